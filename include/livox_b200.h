@@ -1,0 +1,271 @@
+/*
+ * livox_b200.h -- C ABI of the B200 (sm_100a) per-frame LiDAR SLAM hot path.
+ *
+ * Every entry point is `extern "C"`, takes plain device pointers, sizes and a cudaStream_t passed as
+ * `void*`, enqueues its kernels on that stream and returns an int status:
+ *     LW_OK (0), LW_EINVAL (bad argument), LW_ECAPACITY (a capacity is exceeded),
+ *     LW_ETIMEOUT (a bounded device wait gave up), LW_ECUDA (a CUDA call failed).
+ * lw_last_error() returns a message for the calling thread's last failure.
+ * The library never allocates device memory: the caller (the Python `livox_warp` package, or any other
+ * host) allocates every buffer and passes pointers and capacities.
+ *
+ * Conventions shared with the reference implementation (python/livox_warp in nhaumann/livox-warp):
+ *   - voxel keys pack three 21-bit biased axis indices into an int64 (gpu.py:231-239), -1 is an empty slot;
+ *   - slot hash = (key * 0x9E3779B97F4A7C15) ^ (>> 29 arithmetic), & 0x7FFFFFFF, & mask (gpu.py:247-251);
+ *   - open addressing with at most 64 linear probes (gpu.py:254-265);
+ *   - attr packs reflectivity (bits 0-7), noise tag (8-15), return index (16-23), device (24-31)
+ *     (sources.py:1-9).
+ * Deviations, all chosen so that the GPU path is deterministic and matches the CPU oracle bit for bit:
+ *   - per-voxel sums are exact int64 fixed point (LW_FIX_* units) instead of float32 atomics of
+ *     undefined order; means and covariances are derived from them in float64;
+ *   - "the first thread to claim" becomes "the lowest point index", and the 4096-point caps take the
+ *     first points in index order.
+ */
+#ifndef LIVOX_B200_H
+#define LIVOX_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------------- */
+#define LW_OK 0
+#define LW_EINVAL (-1)
+#define LW_ECAPACITY (-2)
+#define LW_ETIMEOUT (-3)
+#define LW_ECUDA (-4)
+
+/* ---- fixed-point units of the voxel sums ------------------------------------------------------ */
+#define LW_FIX_R 4294967296.0        /* registration map: units per metre of (point - voxel centre), 2^32 */
+#define LW_FIX_RR 1099511627776.0    /* registration map: units per m^2 of the outer products, 2^40 */
+#define LW_FIX_W 1048576.0           /* integration / cluster maps: units per metre of world xyz, 2^20 */
+#define LW_REG_CAP 4096              /* points a registration voxel sums (odom.py:83) */
+#define LW_MAP_CAP 4096              /* points an integration voxel sums (gpu.py:55) */
+#define LW_ACC_STRIDE 64             /* entries of one Gauss-Newton accumulator (odom.py:72-82) */
+#define LW_REC_FLOATS 20             /* floats of a registration voxel's derived record */
+#define LW_POSE_SLOTS 65536          /* pose table entries (gpu.py:56) */
+
+/* accumulator layout (odom.py:74-82; localize.py shares it) */
+#define LW_ACC_H 0
+#define LW_ACC_B 21
+#define LW_ACC_COUNT 27
+#define LW_ACC_ERR 28
+#define LW_ACC_RMS 29
+#define LW_ACC_WEIGHT 30
+#define LW_ACC_RANGE 31
+#define LW_ACC_HG 32
+
+/* ---- library ---------------------------------------------------------------------------------- */
+const char* lw_version(void);
+const char* lw_last_error(void);
+/* Number of SMs of the current device (the persistent kernels launch one CTA per SM). */
+int lw_device_sms(int* out_sms);
+
+/* ---- registration voxel map (odom.py:468-474) -------------------------------------------------- */
+typedef struct lw_regmap {
+    int64_t* keys;   /* [cap] voxel key or -1 */
+    int32_t* cnt;    /* [cap] points summed into the voxel (<= LW_REG_CAP) */
+    int64_t* sum;    /* [cap*3] sum of (w - voxel centre), LW_FIX_R units */
+    int64_t* outer;  /* [cap*6] sum of (w - c)(w - c)^T upper triangle xx,xy,xz,yy,yz,zz, LW_FIX_RR units */
+    float* rec;      /* [cap*LW_REC_FLOATS] derived record: mean(3), count, M(6), Mg(6), q(3), surface */
+    int32_t* bcnt;   /* [cap] scratch, 0 between calls */
+    int32_t* first;  /* [cap] scratch, INT32_MAX between calls */
+    int32_t* stats;  /* [2] voxels claimed, points that found no slot in the probe window */
+    int64_t cap;     /* slots, a power of two */
+} lw_regmap;
+
+/* What a registration voxel's record is derived with (odom.py:337-368, 759-761). */
+typedef struct lw_rec_params {
+    float voxel;   /* registration voxel (m) */
+    float tight2;  /* (TIGHT_FRACTION * voxel / sqrt(12))^2 */
+    float noise2;  /* sensor range noise variance */
+    float alpha;   /* weight of loose directions */
+} lw_rec_params;
+
+/* ---- odometry (odom.py:458-803) --------------------------------------------------------------- */
+typedef struct lw_odom_params {
+    double frame_dt, reg_voxel, min_range, max_range, noise, alpha, damping, velocity_smooth;
+    double degen_thr, prior_info, kf_dist, kf_angle_deg;
+    int32_t max_iter, warmup, min_points, min_corr, ret_mask, deskew, redeskew, frame_cap;
+} lw_odom_params;
+
+/* Device-resident odometry state; the host reads it back only when it asks for stats or poses. */
+typedef struct lw_odom_state {
+    double T[16];       /* pose of the last finalised frame (sensor to world, row major) */
+    double T_prev[16];
+    double T_key[16];   /* pose of the last keyframe */
+    double delta[16];   /* constant-velocity motion per frame */
+    double xi_s[6];     /* smoothed body twist */
+    double T_pred[16];  /* the current registration's start / prior pose */
+    double T_reg[16];   /* the current registration's result */
+    double t_mid;       /* mid-frame time of the frame being finalised */
+    double rms, cond;   /* stats of the last registration */
+    float xi[6];        /* body twist of the last frame (rho, theta), what deskew uses */
+    float xi_used[6];   /* twist the current frame was deskewed with */
+    int32_t has_prev, has_key, map_frames, frame_k;
+    int32_t m, n_ds, warm, ok;
+    int32_t run_reg, do_insert, redo, err;
+    int32_t iters, corr, degen, weak;
+    int32_t frames, skipped, keyframes, traj_len;
+} lw_odom_state;
+
+/* One finalised frame in the device trajectory log. */
+typedef struct lw_traj_rec {
+    double T[16];
+    double t_mid;
+    int32_t k, ok, iters, corr;
+} lw_traj_rec;
+
+/* Frame buffers owned by Odometry (odom.py:476-490). */
+typedef struct lw_frame_buf {
+    float* f_raw;     /* [cap*4] x, y, z, t as measured */
+    float* f_xyz;     /* [cap*4] x, y, z (deskewed to mid-frame), t */
+    uint32_t* f_attr; /* [cap] */
+    float* f_t;       /* [cap] */
+    int32_t* f_frame; /* [cap] */
+    int32_t* count;   /* [1] points in the open frame (may exceed cap: the excess is dropped) */
+    int64_t* ds_keys; /* [ds_cap] thinning table, -1 between frames */
+    int32_t* ds_win;  /* [ds_cap] lowest point index per thinning voxel, INT32_MAX between frames */
+    int32_t* ds_slot; /* [cap] per point: its thinning slot when kept, else -1 */
+    int32_t* tiles;   /* [cap/1024 + 1] per-tile kept counts */
+    float* ds_xyz;    /* [cap*4] thinned points x, y, z, range */
+    int64_t cap;      /* frame capacity */
+    int64_t ds_cap;   /* thinning slots, a power of two >= cap */
+} lw_frame_buf;
+
+/* Scratch of the persistent Gauss-Newton kernel. */
+typedef struct lw_gn_scratch {
+    double* part;      /* [2 * grid * LW_ACC_STRIDE] per-CTA partial accumulators, double buffered */
+    uint32_t* bar;     /* [2] grid barrier counter and generation; zero before the first use */
+    int32_t* err;      /* [1] set when a bounded wait gives up */
+    int32_t grid;      /* CTAs (<= the SM count, one per SM) */
+} lw_gn_scratch;
+
+/* Pose table of the Pipeline (gpu.py:1196-1206); written on the device by the odometry. */
+typedef struct lw_pose_table {
+    float* poses;         /* [LW_POSE_SLOTS*16] row-major sensor-to-world */
+    float* tw;            /* [LW_POSE_SLOTS*6] rho, theta per frame */
+    int32_t* owner_frame; /* [LW_POSE_SLOTS] */
+    int32_t* owner_epoch; /* [LW_POSE_SLOTS] */
+} lw_pose_table;
+
+/* Append the staged points with k_min <= floor(max(t,0)/frame_dt) <= k_open to the open frame, in
+ * staged order (odom.py:97-123, called from Odometry.push odom.py:626-638). xyz is [n*xyz_stride]. */
+int lw_frame_append(const float* xyz, int32_t xyz_stride, const uint32_t* attr, const float* t, int64_t n,
+                    double inv_dt, int32_t k_min, int32_t k_open, lw_frame_buf* fb, void* stream);
+
+/* Zero the open frame's point count (odom.py:614, 636). */
+int lw_frame_reset(lw_frame_buf* fb, void* stream);
+
+/* Finalise the open frame k (odom.py:642-657 with _estimate :659-680, _register :752-803, _insert :719,
+ * _update_velocity :682): deskew, thin, Gauss-Newton on the device, re-deskew and re-register when the
+ * solved motion differs, keyframe insert, velocity update, pose-table entry and trajectory record.
+ * `m_ub` bounds the frame's point count (grid sizing only). No host synchronisation. */
+int lw_odom_finalize(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_odom_state* st, lw_frame_buf* fb,
+                     lw_regmap* reg, lw_gn_scratch* gn, lw_pose_table* pt, int32_t epoch,
+                     lw_traj_rec* traj, int64_t traj_cap, void* stream);
+
+/* Write a pose and twist for frames k0 .. k1-1 into the pose table (odom.py:615-625, 637): what the live
+ * view draws frames with before they are solved. mode bit 0: the current pose T instead of the prediction
+ * T*delta; bit 1: a zero twist instead of xi. */
+int lw_odom_predict_poses(int32_t k0, int32_t k1, int32_t current, const lw_odom_state* st, lw_pose_table* pt,
+                          int32_t epoch, void* stream);
+
+/* Reset the odometry state to pose T0 (odom.py:561-579) and, when `clear_map`, the registration map. */
+int lw_odom_reset(const double* T0_host, lw_odom_state* st, lw_regmap* reg, int32_t clear_map, void* stream);
+
+/* Forget the frame clock only (odom.py:581-589). */
+int lw_odom_restart_clock(lw_odom_state* st, void* stream);
+
+/* ---- the parts of the frame, exposed one by one ------------------------------------------------ */
+
+/* Deskew m points (odom.py:163-178, gpu.py:268-283): s = clamp((t - t_mid) * inv_dt, -1, 1),
+ * p' = rotvec(theta s) p + rho s. raw and out are [m*4] (x, y, z, t); m is a device count. */
+int lw_deskew(const float* raw, float* out, const int32_t* m_dev, int64_t m_ub, double t_mid, double inv_dt,
+              const float* twist6_host, void* stream);
+
+/* Thin the deskewed frame: keep the lowest-index point of every half-voxel (odom.py:126-160, 731-737);
+ * writes fb->ds_xyz in point order and n_ds_dev. */
+int lw_thin(lw_frame_buf* fb, const int32_t* m_dev, int64_t m_ub, double inv_v, double min_range,
+            double max_range, int32_t ret_mask, int32_t* n_ds_dev, void* stream);
+
+/* Add n points posed by T to the registration map (odom.py:186-230) and refresh the derived record of
+ * every voxel touched. xyz is [n*4]; n_dev is a device count or NULL (then n_ub is the count);
+ * pslot is [n_ub] scratch. */
+int lw_reg_insert(const float* xyz4, const uint32_t* attr, const int32_t* n_dev, int64_t n_ub,
+                  const double* T_host, double voxel, double max_range, int32_t ret_mask, lw_regmap* reg,
+                  const lw_rec_params* rp, int32_t* pslot, void* stream);
+
+/* Recompute every occupied voxel's record (after the record parameters change). */
+int lw_reg_refresh_all(lw_regmap* reg, const lw_rec_params* rp, void* stream);
+
+/* One Gauss-Newton accumulation pass (odom.py:275-375 then k_reduce :378-384) at pose T: out[64] in the
+ * LW_ACC_* layout (float64). reach / max_d2 / kappa as odom.py:765-767. The Jacobian is taken about the
+ * world origin, as the reference does. */
+int lw_icp_accumulate(const float* ds4, const int32_t* n_dev, int64_t n_ub, const double* T_host,
+                      const lw_regmap* reg, float voxel, int32_t reach, float max_d2, float kappa,
+                      lw_gn_scratch* gn, double* out64, void* stream);
+
+/* The whole Gauss-Newton loop of odom.py:752-803 on the device, from st->T_pred; result in st->T_reg,
+ * st->ok and the stats. One persistent cooperative launch, one grid barrier per iteration. */
+int lw_icp_solve(const float* ds4, const int32_t* n_dev, const lw_odom_params* prm, lw_odom_state* st,
+                 const lw_regmap* reg, lw_gn_scratch* gn, void* stream);
+
+/* ---- integration map (gpu.py:1213-1219) ------------------------------------------------------- */
+typedef struct lw_map {
+    int64_t* keys;   /* [cap] */
+    int32_t* cnt;    /* [cap] hits (keeps counting past LW_MAP_CAP) */
+    int64_t* acc;    /* [cap*4] sum of world x, y, z (LW_FIX_W units) and reflectivity over the first LW_MAP_CAP hits */
+    float* last;     /* [cap] latest hit time */
+    float* first;    /* [cap] earliest hit time (1e30 when empty) */
+    int32_t* miss;   /* [cap] carving misses */
+    int32_t* bcnt;   /* [cap] scratch, 0 between calls */
+    int32_t* lead;   /* [cap] scratch, INT32_MAX between calls */
+    int32_t* stats;  /* [2] occupied, dropped */
+    int64_t cap;
+} lw_map;
+
+/* The filter set of gpu.View (gpu.py:76-98) that the map kernels read. */
+typedef struct lw_view {
+    float now, persist, min_range, max_range;
+    int32_t min_refl, noise_mask, ret_mask, crop_on;
+    float crop_lo[3], crop_hi[3];
+    float inv_frame_dt;
+    int32_t epoch;
+    float inv_voxel;
+    int32_t map_mask, dyn_on;
+    float dyn_settle;
+    int32_t carve_on;
+    float carve_ratio;
+    int32_t carve_min;
+    float carve_stale;
+} lw_view;
+
+/* Accumulate n points through their frames' poses into the map (gpu.py:373-412). n_dev may be NULL
+ * (then n_ub is the count); pslot is [n_ub] scratch. */
+int lw_map_insert(const float* xyz, int32_t xyz_stride, const uint32_t* attr, const float* t,
+                  const int32_t* frame, const int32_t* n_dev, int64_t n_ub, const float* poses,
+                  const lw_view* v, float inv_voxel, lw_map* map, int32_t* pslot, void* stream);
+
+/* Free-space carving of every `every`-th return (gpu.py:469-593). */
+int lw_carve(const float* xyz, int32_t xyz_stride, const uint32_t* attr, const int32_t* frame,
+             const int32_t* n_dev, int64_t n_ub, const float* poses, int32_t every, float inv_voxel,
+             float max_range, int32_t max_steps, lw_map* map, void* stream);
+
+/* Classify the map's voxels into the visible set (gpu.py:699-747) and compact it in slot order
+ * (gpu.py:1495-1504). Writes count_dev[0]. tiles is [cap/1024 + 1] scratch. */
+int lw_map_build(const lw_map* map, const lw_view* v, int32_t min_count, float* out_xyz, uint32_t* out_attr,
+                 float* out_t, int32_t* out_dyn, int32_t* tiles, int32_t* count_dev, void* stream);
+
+/* Frame id of each staged point, floor(max(t, 0) * inv_dt), all 0 when inv_dt <= 0 (gpu.py:340-348). */
+int lw_frame_ids(const float* t, int64_t n, float inv_dt, int32_t* out, void* stream);
+
+/* Clear the integration map (gpu.py:1305-1313). */
+int lw_map_clear(lw_map* map, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LIVOX_B200_H */

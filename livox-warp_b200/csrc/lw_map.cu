@@ -1,0 +1,550 @@
+// Integration voxel map, free-space carving and the map's visible set on sm_100a.
+//
+// Reference: python/livox_warp/gpu.py -- keep_raw :155-167, k_map_insert :373-412, map_centroid :415-419,
+// local_plane :422-466, k_carve :469-593, transient / ghost :286-299, settled_near :596-634,
+// k_classify_map :699-747, the scan + scatter of Pipeline.build :1495-1504, clear_map :1305-1313.
+//
+// Determinism: the map's sums are exact int64 fixed point and the 4096-hit cap sums the first hits in point
+// order, so keys, counts, sums, centroids and therefore every carving decision are independent of thread
+// order and agree bit for bit with the CPU oracle.
+#include "lw_common.cuh"
+#include "lw_linalg.cuh"
+
+namespace lw {
+
+constexpr int MTILE = 1024;
+
+// Carving constants (gpu.py:66-73)
+constexpr float CARVE_MIN_RANGE = 0.05f;
+constexpr float CARVE_MARGIN_VOXELS = 3.0f;
+constexpr float CARVE_MARGIN_FRACTION = 0.03f;
+constexpr float CARVE_GRAZING_VOXELS = 1.5f;
+constexpr float CARVE_MIN_COSINE = 0.05f;
+constexpr float CARVE_PIERCE_PLANE = 0.6f;
+constexpr float CARVE_PIERCE_POINT = 0.5f;
+
+__device__ __forceinline__ bool keep_raw(float x, float y, float z, uint32_t a, const lw_view& v) {
+    float r = len3(x, y, z);
+    if (r < v.min_range || r > v.max_range) return false;
+    if (refl_of(a) < v.min_refl) return false;
+    if (((v.noise_mask >> (tag_of(a) & 3)) & 1) == 0) return false;
+    if (((v.ret_mask >> (ret_of(a) & 3)) & 1) == 0) return false;
+    return true;
+}
+
+template <int STRIDE>
+__device__ __forceinline__ void load_xyz(const float* __restrict__ xyz, int64_t i, float& x, float& y, float& z) {
+    if (STRIDE == 4) {
+        float4 p = __ldg(reinterpret_cast<const float4*>(xyz) + i);
+        x = p.x;
+        y = p.y;
+        z = p.z;
+    } else {
+        x = xyz[i * 3 + 0];
+        y = xyz[i * 3 + 1];
+        z = xyz[i * 3 + 2];
+    }
+}
+
+struct MapIns {
+    float inv_voxel;
+    int mask;
+};
+
+// =====================================================================================================
+// Map insert: A claims and counts, B sums (first LW_MAP_CAP hits in order) and updates the hit times,
+// D publishes the counts and resets the scratch.
+// =====================================================================================================
+
+template <int STRIDE>
+__device__ __forceinline__ bool map_point(const float* __restrict__ xyz, const uint32_t* __restrict__ attr,
+                                          const int32_t* __restrict__ frame, const float* __restrict__ poses,
+                                          const lw_view& v, int64_t i, float inv, float& wx, float& wy, float& wz) {
+    float x, y, z;
+    load_xyz<STRIDE>(xyz, i, x, y, z);
+    if (!keep_raw(x, y, z, attr[i], v)) return false;
+    const float* T = poses + (int64_t)(frame[i] & (LW_POSE_SLOTS - 1)) * 16;
+    xform(T, x, y, z, wx, wy, wz);
+    return true;
+}
+
+template <int STRIDE>
+__global__ void k_map_a(const float* __restrict__ xyz, const uint32_t* __restrict__ attr,
+                        const int32_t* __restrict__ frame, const int* n_dev, int64_t n_ub,
+                        const float* __restrict__ poses, lw_view v, MapIns mi, lw_map map, int* __restrict__ pslot) {
+    int64_t n = n_dev ? (int64_t)*n_dev : n_ub;
+    if (n > n_ub) n = n_ub;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float wx, wy, wz;
+        int s = -1;
+        if (map_point<STRIDE>(xyz, attr, frame, poses, v, i, mi.inv_voxel, wx, wy, wz)) {
+            int64_t key = key_ijk(ifloor(wx * mi.inv_voxel), ifloor(wy * mi.inv_voxel), ifloor(wz * mi.inv_voxel));
+            bool claimed;
+            s = claim_slot(key, map.keys, mi.mask, &claimed);
+            if (claimed) atomicAdd(map.stats + 0, 1);
+            if (s < 0) {
+                atomicAdd(map.stats + 1, 1);  // table full along this probe chain
+            } else {
+                atomicAdd(map.bcnt + s, 1);
+                atomicMin(map.lead + s, (int)i);
+            }
+        }
+        pslot[i] = s;
+    }
+}
+
+__device__ __forceinline__ void map_add(lw_map& map, int s, float wx, float wy, float wz, uint32_t a) {
+    const float FW = (float)LW_FIX_W;
+    atomic_add_i64(map.acc + 4 * (int64_t)s + 0, to_fix(wx, FW));
+    atomic_add_i64(map.acc + 4 * (int64_t)s + 1, to_fix(wy, FW));
+    atomic_add_i64(map.acc + 4 * (int64_t)s + 2, to_fix(wz, FW));
+    atomic_add_i64(map.acc + 4 * (int64_t)s + 3, (int64_t)refl_of(a));
+}
+
+template <int STRIDE>
+__global__ void k_map_b(const float* __restrict__ xyz, const uint32_t* __restrict__ attr,
+                        const float* __restrict__ t, const int32_t* __restrict__ frame, const int* n_dev, int64_t n_ub,
+                        const float* __restrict__ poses, lw_view v, MapIns mi, lw_map map,
+                        const int* __restrict__ pslot) {
+    int64_t n = n_dev ? (int64_t)*n_dev : n_ub;
+    if (n > n_ub) n = n_ub;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int s = pslot[i];
+        if (s < 0) continue;
+        float wx, wy, wz;
+        map_point<STRIDE>(xyz, attr, frame, poses, v, i, mi.inv_voxel, wx, wy, wz);
+        int pre = map.cnt[s];
+        int tot = pre + map.bcnt[s];
+        if (tot <= LW_MAP_CAP) {
+            map_add(map, s, wx, wy, wz, attr[i]);
+        } else if (pre < LW_MAP_CAP && map.lead[s] == (int)i) {
+            // this batch crosses the cap: the lowest-index point sums the first (cap - pre) hits in order
+            int room = LW_MAP_CAP - pre;
+            for (int64_t j = i; j < n && room > 0; ++j) {
+                if (pslot[j] != s) continue;
+                float ux, uy, uz;
+                map_point<STRIDE>(xyz, attr, frame, poses, v, j, mi.inv_voxel, ux, uy, uz);
+                map_add(map, s, ux, uy, uz, attr[j]);
+                --room;
+            }
+        }
+        float ti = t[i];
+        atomic_max_float(map.last + s, ti);
+        atomic_min_float(map.first + s, ti);
+    }
+}
+
+__global__ void k_map_d(const int* n_dev, int64_t n_ub, lw_map map, const int* __restrict__ pslot) {
+    int64_t n = n_dev ? (int64_t)*n_dev : n_ub;
+    if (n > n_ub) n = n_ub;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int s = pslot[i];
+        if (s < 0 || map.lead[s] != (int)i) continue;
+        map.cnt[s] += map.bcnt[s];  // hits keep counting past the cap (carving compares them with misses)
+        map.bcnt[s] = 0;
+        map.lead[s] = NO_INDEX;
+    }
+}
+
+// =====================================================================================================
+// Carving
+// =====================================================================================================
+
+__device__ __forceinline__ void centroid(const lw_map& map, int s, float& x, float& y, float& z) {
+    int c = map.cnt[s];
+    double n = (double)(c < LW_MAP_CAP ? c : LW_MAP_CAP) * LW_FIX_W;
+    x = (float)((double)map.acc[4 * (int64_t)s + 0] / n);
+    y = (float)((double)map.acc[4 * (int64_t)s + 1] / n);
+    z = (float)((double)map.acc[4 * (int64_t)s + 2] / n);
+}
+
+// Normal of the surface through voxel (ix, iy, iz) from a PCA of the occupied 3x3x3 neighbourhood's centroids
+// taken relative to `o` (gpu.py:422-466); w = 2 surface, 1 at least 4 occupied but no surface, 0 fewer.
+__device__ float4 local_plane(int ix, int iy, int iz, float ox, float oy, float oz, const lw_map& map, int mask) {
+    double cs[3] = {0.0, 0.0, 0.0}, cc[6] = {0, 0, 0, 0, 0, 0};
+    int cn = 0;
+    for (int gx = -1; gx <= 1; ++gx)
+        for (int gy = -1; gy <= 1; ++gy)
+            for (int gz = -1; gz <= 1; ++gz) {
+                int sn = find_slot(key_ijk(ix + gx, iy + gy, iz + gz), map.keys, mask);
+                if (sn >= 0 && map.cnt[sn] > 0) {
+                    float cx, cy, cz;
+                    centroid(map, sn, cx, cy, cz);
+                    double qx = (double)(cx - ox), qy = (double)(cy - oy), qz = (double)(cz - oz);
+                    cs[0] += qx;
+                    cs[1] += qy;
+                    cs[2] += qz;
+                    cc[0] += qx * qx;
+                    cc[1] += qx * qy;
+                    cc[2] += qx * qz;
+                    cc[3] += qy * qy;
+                    cc[4] += qy * qz;
+                    cc[5] += qz * qz;
+                    ++cn;
+                }
+            }
+    if (cn < 4) return make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+    double inv = 1.0 / (double)cn;
+    double mu[3] = {cs[0] * inv, cs[1] * inv, cs[2] * inv};
+    double C[9];
+    const int up[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C[i * 3 + j] = cc[up[i * 3 + j]] * inv - mu[i] * mu[j];
+    double ev[3], Q[9];
+    jacobi_eig<3>(C, ev, Q);
+    int k = 0;
+    if (ev[1] < ev[k]) k = 1;
+    if (ev[2] < ev[k]) k = 2;
+    int j = (k + 1) % 3, j2 = (k + 2) % 3;
+    double mid = fmin(ev[j], ev[j2]);
+    float ok = ev[k] < 0.25 * mid ? 2.0f : 1.0f;
+    return make_float4((float)Q[0 * 3 + k], (float)Q[1 * 3 + k], (float)Q[2 * 3 + k], ok);
+}
+
+template <int STRIDE>
+__global__ void k_carve(const float* __restrict__ xyz, const uint32_t* __restrict__ attr,
+                        const int32_t* __restrict__ frame, const int* n_dev, int64_t n_ub,
+                        const float* __restrict__ poses, int every, float inv_voxel, float max_range, int max_steps,
+                        lw_map map) {
+    int64_t n = n_dev ? (int64_t)*n_dev : n_ub;
+    if (n > n_ub) n = n_ub;
+    const int mask = (int)(map.cap - 1);
+    const int64_t nrays = (n + every - 1) / every;
+    for (int64_t ray = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; ray < nrays;
+         ray += (int64_t)gridDim.x * blockDim.x) {
+        int64_t i = ray * every;
+        if (tag_of(attr[i]) != 0) continue;
+        const float* T = poses + (int64_t)(frame[i] & (LW_POSE_SLOTS - 1)) * 16;
+        float ox = T[3], oy = T[7], oz = T[11];
+        float px, py, pz, wx, wy, wz;
+        load_xyz<STRIDE>(xyz, i, px, py, pz);
+        xform(T, px, py, pz, wx, wy, wz);
+        float dx = wx - ox, dy = wy - oy, dz = wz - oz;
+        float L = len3(dx, dy, dz);
+        if (L < CARVE_MIN_RANGE || L > max_range) continue;
+        dx = dx / L;
+        dy = dy / L;
+        dz = dz / L;
+        float voxel = 1.0f / inv_voxel;
+        float margin = fmaxf(CARVE_MARGIN_VOXELS * voxel, CARVE_MARGIN_FRACTION * L);
+        float4 pe = local_plane(ifloor(wx * inv_voxel), ifloor(wy * inv_voxel), ifloor(wz * inv_voxel), wx, wy, wz,
+                                map, mask);
+        if (pe.w > 0.5f) {
+            float cosine = fabsf(pe.x * dx + pe.y * dy + pe.z * dz);
+            margin = fmaxf(margin, CARVE_GRAZING_VOXELS * voxel / fmaxf(cosine, CARVE_MIN_COSINE));
+        }
+        float stop = (L - margin) * inv_voxel;
+        if (stop <= 1.0f) continue;
+        float posx = ox * inv_voxel, posy = oy * inv_voxel, posz = oz * inv_voxel;
+        int ix = ifloor(posx), iy = ifloor(posy), iz = ifloor(posz);
+        int sx = 1, sy = 1, sz = 1;
+        float tmx = 1.0e30f, tmy = 1.0e30f, tmz = 1.0e30f, tdx = 1.0e30f, tdy = 1.0e30f, tdz = 1.0e30f;
+        if (dx > 1.0e-9f) {
+            tmx = ((float)(ix + 1) - posx) / dx;
+            tdx = 1.0f / dx;
+        } else if (dx < -1.0e-9f) {
+            sx = -1;
+            tmx = (posx - (float)ix) / (-dx);
+            tdx = -1.0f / dx;
+        }
+        if (dy > 1.0e-9f) {
+            tmy = ((float)(iy + 1) - posy) / dy;
+            tdy = 1.0f / dy;
+        } else if (dy < -1.0e-9f) {
+            sy = -1;
+            tmy = (posy - (float)iy) / (-dy);
+            tdy = -1.0f / dy;
+        }
+        if (dz > 1.0e-9f) {
+            tmz = ((float)(iz + 1) - posz) / dz;
+            tdz = 1.0f / dz;
+        } else if (dz < -1.0e-9f) {
+            sz = -1;
+            tmz = (posz - (float)iz) / (-dz);
+            tdz = -1.0f / dz;
+        }
+        for (int step = 0; step < max_steps; ++step) {
+            float tt;
+            if (tmx < tmy && tmx < tmz) {
+                tt = tmx;
+                ix += sx;
+                tmx += tdx;
+            } else if (tmy < tmz) {
+                tt = tmy;
+                iy += sy;
+                tmy += tdy;
+            } else {
+                tt = tmz;
+                iz += sz;
+                tmz += tdz;
+            }
+            if (tt >= stop) break;
+            int s = find_slot(key_ijk(ix, iy, iz), map.keys, mask);
+            if (s < 0 || map.cnt[s] <= 0) continue;
+            float cx, cy, cz;
+            centroid(map, s, cx, cy, cz);
+            float rx = cx - ox, ry = cy - oy, rz = cz - oz;
+            bool pierced = false;
+            float4 pl = local_plane(ix, iy, iz, cx, cy, cz, map, mask);
+            if (pl.w > 1.5f) {
+                float dn = dx * pl.x + dy * pl.y + dz * pl.z;
+                if (fabsf(dn) > 1.0e-4f) {
+                    float f = (rx * pl.x + ry * pl.y + rz * pl.z) / dn;
+                    float xx = dx * f - rx, xy = dy * f - ry, xz = dz * f - rz;  // plane crossing rel. to centroid
+                    if (len3(xx, xy, xz) < CARVE_PIERCE_PLANE * voxel) pierced = true;
+                }
+            } else {
+                float g = rx * dx + ry * dy + rz * dz;
+                float qx = rx - g * dx, qy = ry - g * dy, qz = rz - g * dz;
+                if (len3(qx, qy, qz) < CARVE_PIERCE_POINT * voxel) pierced = true;
+            }
+            if (pierced) atomicAdd(map.miss + s, every);
+        }
+    }
+}
+
+// =====================================================================================================
+// Visible set of the map (k_classify_map) compacted in slot order.
+// =====================================================================================================
+
+__device__ __forceinline__ int transient(int c, int miss, const lw_view& v) {
+    if (miss < v.carve_min) return 0;
+    return (float)miss > v.carve_ratio * (float)c ? 1 : 0;
+}
+
+__device__ __forceinline__ int ghost(int c, int miss, float last, const lw_view& v) {
+    if (v.now - last < v.carve_stale) return 0;
+    return transient(c, miss, v);
+}
+
+__device__ __forceinline__ int in_crop(float x, float y, float z, const lw_view& v) {
+    if (v.crop_on == 0) return 1;
+    if (x < v.crop_lo[0] || y < v.crop_lo[1] || z < v.crop_lo[2]) return 0;
+    if (x > v.crop_hi[0] || y > v.crop_hi[1] || z > v.crop_hi[2]) return 0;
+    return 1;
+}
+
+__device__ int settled_near(int ix, int iy, int iz, const lw_view& v, const lw_map& map) {
+    for (int nb = 0; nb < 7; ++nb) {
+        int jx = ix, jy = iy, jz = iz;
+        if (nb == 1) jx = ix - 1;
+        else if (nb == 2) jx = ix + 1;
+        else if (nb == 3) jy = iy - 1;
+        else if (nb == 4) jy = iy + 1;
+        else if (nb == 5) jz = iz - 1;
+        else if (nb == 6) jz = iz + 1;
+        int s = find_slot(key_ijk(jx, jy, jz), map.keys, v.map_mask);
+        if (s >= 0) {
+            float age = v.now - map.first[s];
+            if (age < 0.0f) age = 1.0e9f;  // clock restarted: history predates the new clock
+            if (age >= v.dyn_settle && transient(map.cnt[s], map.miss[s], v) == 0) return 1;
+        }
+    }
+    return 0;
+}
+
+__device__ __forceinline__ bool classify_flag(const lw_map& map, int64_t s, const lw_view& v, int min_count, float& wx,
+                                              float& wy, float& wz) {
+    if (map.keys[s] == EMPTY_KEY) return false;
+    int c = map.cnt[s];
+    if (c < min_count) return false;
+    float last = map.last[s];
+    if (v.persist > 0.0f && v.now - last > v.persist) return false;
+    if (v.carve_on != 0 && ghost(c, map.miss[s], last, v) != 0) return false;
+    if (c <= 0) return false;
+    centroid(map, (int)s, wx, wy, wz);
+    return in_crop(wx, wy, wz, v) != 0;
+}
+
+__global__ void k_classify_count(lw_map map, lw_view v, int min_count, int* __restrict__ tiles) {
+    int64_t s = (int64_t)blockIdx.x * MTILE + threadIdx.x;
+    int f = 0;
+    if (s < map.cap) {
+        float wx, wy, wz;
+        f = classify_flag(map, s, v, min_count, wx, wy, wz) ? 1 : 0;
+    }
+    int c = __syncthreads_count(f);
+    if (threadIdx.x == 0) tiles[blockIdx.x] = c;
+}
+
+// In-place exclusive scan of nt tile counts by one CTA; tiles[nt] receives the total.
+__global__ void k_scan_tiles(int* tiles, int nt, int* total_out) {
+    __shared__ int sm[33];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nt; base += blockDim.x) {
+        int j = base + threadIdx.x;
+        int v = j < nt ? tiles[j] : 0;
+        // inclusive warp scan, then across warps
+        int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        int inc = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            int u = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += u;
+        }
+        if (lane == 31) sm[w] = inc;
+        __syncthreads();
+        if (w == 0) {
+            int nw = blockDim.x >> 5;
+            int x = lane < nw ? sm[lane] : 0;
+            int xi = x;
+            for (int o = 1; o < 32; o <<= 1) {
+                int u = __shfl_up_sync(0xffffffffu, xi, o);
+                if (lane >= o) xi += u;
+            }
+            if (lane < nw) sm[lane] = xi - x;
+            if (lane == 31) sm[32] = xi;
+        }
+        __syncthreads();
+        int excl = carry + sm[w] + inc - v;
+        if (j < nt) tiles[j] = excl;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += sm[32];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        tiles[nt] = carry;
+        if (total_out) *total_out = carry;
+    }
+}
+
+__global__ void k_classify_scatter(lw_map map, lw_view v, int min_count, const int* __restrict__ tiles,
+                                   float* __restrict__ out_xyz, uint32_t* __restrict__ out_attr,
+                                   float* __restrict__ out_t, int* __restrict__ out_dyn) {
+    __shared__ int sm[33];
+    int64_t s = (int64_t)blockIdx.x * MTILE + threadIdx.x;
+    int f = 0;
+    float wx = 0.f, wy = 0.f, wz = 0.f;
+    if (s < map.cap) f = classify_flag(map, s, v, min_count, wx, wy, wz) ? 1 : 0;
+    int tot;
+    int r = block_rank(f, sm, &tot);
+    if (!f) return;
+    int j = tiles[blockIdx.x] + r;
+    int c = map.cnt[s];
+    int n = c < LW_MAP_CAP ? c : LW_MAP_CAP;
+    int refl = (int)((double)map.acc[4 * s + 3] / (double)n + 0.5);
+    if (refl > 255) refl = 255;
+    out_xyz[3 * (int64_t)j + 0] = wx;
+    out_xyz[3 * (int64_t)j + 1] = wy;
+    out_xyz[3 * (int64_t)j + 2] = wz;
+    out_attr[j] = (uint32_t)refl;  // mean reflectivity only: tag, return and device mean nothing for a voxel
+    out_t[j] = map.last[s];
+    int dyn = 0;
+    if (transient(c, map.miss[s], v) != 0)
+        dyn = 1;
+    else if (settled_near(ifloor(wx * v.inv_voxel), ifloor(wy * v.inv_voxel), ifloor(wz * v.inv_voxel), v, map) == 0)
+        dyn = 1;
+    out_dyn[j] = dyn;
+}
+
+// Frame id of each staged point: floor(max(t, 0) * inv_dt), 0 when inv_dt <= 0 (gpu.py:340-348).
+__global__ void k_frame_of(const float* __restrict__ t, int64_t n, float inv_dt, int32_t* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = inv_dt <= 0.0f ? 0 : (int)floorf(fmaxf(t[i], 0.0f) * inv_dt);
+}
+
+__global__ void k_map_clear(lw_map map) {
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < map.cap; s += (int64_t)gridDim.x * blockDim.x) {
+        map.keys[s] = EMPTY_KEY;
+        map.cnt[s] = 0;
+        map.acc[4 * s + 0] = map.acc[4 * s + 1] = map.acc[4 * s + 2] = map.acc[4 * s + 3] = 0;
+        map.last[s] = 0.0f;
+        map.first[s] = 1.0e30f;
+        map.miss[s] = 0;
+        map.bcnt[s] = 0;
+        map.lead[s] = NO_INDEX;
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 2) map.stats[threadIdx.x] = 0;
+}
+
+}  // namespace lw
+
+using namespace lw;
+
+static int check_map(const lw_map* map, const char* who) {
+    if (!map || !map->keys || !map->cnt || !map->acc || !map->last || !map->first || !map->miss || !map->bcnt ||
+        !map->lead || !map->stats)
+        return set_error(LW_EINVAL, "%s: incomplete map", who);
+    if (map->cap <= 0 || (map->cap & (map->cap - 1)) != 0)
+        return set_error(LW_EINVAL, "%s: map capacity %lld is not a power of two", who, (long long)map->cap);
+    return LW_OK;
+}
+
+extern "C" {
+
+int lw_map_insert(const float* xyz, int32_t xyz_stride, const uint32_t* attr, const float* t, const int32_t* frame,
+                  const int32_t* n_dev, int64_t n_ub, const float* poses, const lw_view* v, float inv_voxel,
+                  lw_map* map, int32_t* pslot, void* stream) {
+    int r = check_map(map, "lw_map_insert");
+    if (r != LW_OK) return r;
+    if (!xyz || !attr || !t || !frame || !poses || !v || !pslot || (xyz_stride != 3 && xyz_stride != 4))
+        return set_error(LW_EINVAL, "lw_map_insert: bad arguments");
+    if (n_ub <= 0) return LW_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    MapIns mi{inv_voxel, (int)(map->cap - 1)};
+    int grid = blocks_for(n_ub, 256, 8 * device_sms());
+    if (xyz_stride == 4) {
+        k_map_a<4><<<grid, 256, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, *v, mi, *map, pslot);
+        k_map_b<4><<<grid, 256, 0, s>>>(xyz, attr, t, frame, n_dev, n_ub, poses, *v, mi, *map, pslot);
+    } else {
+        k_map_a<3><<<grid, 256, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, *v, mi, *map, pslot);
+        k_map_b<3><<<grid, 256, 0, s>>>(xyz, attr, t, frame, n_dev, n_ub, poses, *v, mi, *map, pslot);
+    }
+    k_map_d<<<grid, 256, 0, s>>>(n_dev, n_ub, *map, pslot);
+    LW_LAUNCHED("lw_map_insert");
+    return LW_OK;
+}
+
+int lw_carve(const float* xyz, int32_t xyz_stride, const uint32_t* attr, const int32_t* frame, const int32_t* n_dev,
+             int64_t n_ub, const float* poses, int32_t every, float inv_voxel, float max_range, int32_t max_steps,
+             lw_map* map, void* stream) {
+    int r = check_map(map, "lw_carve");
+    if (r != LW_OK) return r;
+    if (!xyz || !attr || !frame || !poses || (xyz_stride != 3 && xyz_stride != 4))
+        return set_error(LW_EINVAL, "lw_carve: bad arguments");
+    if (n_ub <= 0) return LW_OK;
+    if (every < 1) every = 1;
+    cudaStream_t s = (cudaStream_t)stream;
+    int64_t rays = (n_ub + every - 1) / every;
+    int grid = blocks_for(rays, 128, 16 * device_sms());
+    if (xyz_stride == 4)
+        k_carve<4><<<grid, 128, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, every, inv_voxel, max_range, max_steps, *map);
+    else
+        k_carve<3><<<grid, 128, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, every, inv_voxel, max_range, max_steps, *map);
+    LW_LAUNCHED("lw_carve");
+    return LW_OK;
+}
+
+int lw_map_build(const lw_map* map, const lw_view* v, int32_t min_count, float* out_xyz, uint32_t* out_attr,
+                 float* out_t, int32_t* out_dyn, int32_t* tiles, int32_t* count_dev, void* stream) {
+    int r = check_map(map, "lw_map_build");
+    if (r != LW_OK) return r;
+    if (!v || !out_xyz || !out_attr || !out_t || !out_dyn || !tiles || !count_dev)
+        return set_error(LW_EINVAL, "lw_map_build: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    int nt = blocks_for(map->cap, MTILE);
+    k_classify_count<<<nt, MTILE, 0, s>>>(*map, *v, min_count, tiles);
+    k_scan_tiles<<<1, 1024, 0, s>>>(tiles, nt, count_dev);
+    k_classify_scatter<<<nt, MTILE, 0, s>>>(*map, *v, min_count, tiles, out_xyz, out_attr, out_t, out_dyn);
+    LW_LAUNCHED("lw_map_build");
+    return LW_OK;
+}
+
+int lw_frame_ids(const float* t, int64_t n, float inv_dt, int32_t* out, void* stream) {
+    if (!t || !out) return set_error(LW_EINVAL, "lw_frame_ids: null argument");
+    if (n <= 0) return LW_OK;
+    k_frame_of<<<blocks_for(n, 256, 8 * device_sms()), 256, 0, (cudaStream_t)stream>>>(t, n, inv_dt, out);
+    LW_LAUNCHED("lw_frame_ids");
+    return LW_OK;
+}
+
+int lw_map_clear(lw_map* map, void* stream) {
+    int r = check_map(map, "lw_map_clear");
+    if (r != LW_OK) return r;
+    k_map_clear<<<8 * device_sms(), 256, 0, (cudaStream_t)stream>>>(*map);
+    LW_LAUNCHED("lw_map_clear");
+    return LW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1415 @@
+// Odometry hot path on sm_100a: frame cutting, deskew, half-voxel thinning, the registration voxel map with
+// per-voxel distribution records, scan-to-map point-to-distribution Gauss-Newton (accumulate on every SM,
+// float64 6x6 solve on the device), and the per-frame state machine of odom.py (warm-up, re-deskew,
+// keyframes, constant-velocity prediction) -- all without a host round trip.
+//
+// Reference: python/livox_warp/odom.py (kernels :97-384, host solve :387-455, Odometry :458-803) and the key /
+// hash / deskew helpers of python/livox_warp/gpu.py (:231-283).
+#include "lw_common.cuh"
+#include "lw_linalg.cuh"
+
+namespace lw {
+
+constexpr int TILE = 1024;
+
+// =====================================================================================================
+// Frame append (odom.py:97-123): order-preserving compaction of the staged points that belong to the open
+// frame. Three launches: per-tile counts, scatter at (count + prefix of tiles), count update.
+// =====================================================================================================
+
+__device__ __forceinline__ int frame_of(float t, float inv_dt) { return (int)floorf(fmaxf(t, 0.0f) * inv_dt); }
+
+__global__ void k_append_count(const float* __restrict__ t, int64_t n, float inv_dt, int k_min, int k_open,
+                               int* __restrict__ tiles) {
+    int64_t i = (int64_t)blockIdx.x * TILE + threadIdx.x;
+    int f = 0;
+    if (i < n) {
+        int k = frame_of(t[i], inv_dt);
+        f = (k <= k_open && k >= k_min) ? 1 : 0;
+    }
+    int c = __syncthreads_count(f);
+    if (threadIdx.x == 0) tiles[blockIdx.x] = c;
+}
+
+__device__ __forceinline__ int prefix_of_tiles(const int* __restrict__ tiles, int b) {
+    __shared__ int red[32];
+    int s = 0;
+    for (int j = threadIdx.x; j < b; j += blockDim.x) s += tiles[j];
+    s = warp_sum_i(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    int tot = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+    __syncthreads();
+    return tot;
+}
+
+template <int STRIDE>
+__global__ void k_append_scatter(const float* __restrict__ xyz, const uint32_t* __restrict__ attr,
+                                 const float* __restrict__ t, int64_t n, float inv_dt, int k_min, int k_open,
+                                 const int* __restrict__ tiles, lw_frame_buf fb) {
+    __shared__ int sm[33];
+    int64_t i = (int64_t)blockIdx.x * TILE + threadIdx.x;
+    int f = 0;
+    float ti = 0.0f;
+    if (i < n) {
+        ti = t[i];
+        int k = frame_of(ti, inv_dt);
+        f = (k <= k_open && k >= k_min) ? 1 : 0;
+    }
+    int base = *fb.count + prefix_of_tiles(tiles, blockIdx.x);
+    int tot;
+    int r = block_rank(f, sm, &tot);
+    if (f) {
+        int64_t pos = (int64_t)base + r;
+        if (pos < fb.cap) {
+            float4 v = make_float4(xyz[i * STRIDE + 0], xyz[i * STRIDE + 1], xyz[i * STRIDE + 2], ti);
+            reinterpret_cast<float4*>(fb.f_raw)[pos] = v;
+            fb.f_attr[pos] = attr[i];
+            fb.f_t[pos] = ti;
+            fb.f_frame[pos] = k_open;  // the frame it is deskewed, registered and posed with (odom.py:123)
+        }
+    }
+}
+
+__global__ void k_append_total(const int* __restrict__ tiles, int nt, int* count) {
+    int s = 0;
+    for (int j = threadIdx.x; j < nt; j += blockDim.x) s += tiles[j];
+    s = warp_sum_i(s);
+    __shared__ int red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+        *count += tot;
+    }
+}
+
+// =====================================================================================================
+// Deskew (odom.py:163-178 with gpu.py:268-283). The rotation by the rotation vector theta*s is evaluated in
+// float64 and rounded once, so the CPU oracle reproduces it exactly.
+// =====================================================================================================
+
+__device__ __forceinline__ float4 deskew_point(float4 p, float t_mid, float inv_dt, const float* tw) {
+    float s = fminf(fmaxf((p.w - t_mid) * inv_dt, -1.0f), 1.0f);
+    float rx = tw[3] * s, ry = tw[4] * s, rz = tw[5] * s;
+    float a = len3(rx, ry, rz);
+    float ox = p.x, oy = p.y, oz = p.z;
+    if (!(a < 1.0e-9f)) {
+        double ad = (double)a;
+        double ux = (double)rx / ad, uy = (double)ry / ad, uz = (double)rz / ad;
+        double sh = sin(0.5 * ad), w = cos(0.5 * ad);
+        double vx = ux * sh, vy = uy * sh, vz = uz * sh;
+        double px = p.x, py = p.y, pz = p.z;
+        // p' = p + w t + v x t with t = 2 (v x p)
+        double tx = 2.0 * (vy * pz - vz * py), ty = 2.0 * (vz * px - vx * pz), tz = 2.0 * (vx * py - vy * px);
+        ox = (float)(px + w * tx + (vy * tz - vz * ty));
+        oy = (float)(py + w * ty + (vz * tx - vx * tz));
+        oz = (float)(pz + w * tz + (vx * ty - vy * tx));
+    }
+    return make_float4(ox + tw[0] * s, oy + tw[1] * s, oz + tw[2] * s, p.w);
+}
+
+// =====================================================================================================
+// Thinning (odom.py:126-160): keep the lowest-index point of every half-voxel of the (deskewed) sensor frame.
+// Pass A (fused with deskew) claims keys and records the lowest index per slot; pass B marks the winners and
+// counts them per tile; pass C writes them in point order and clears the table for the next frame.
+// =====================================================================================================
+
+struct ThinArgs {
+    float inv_v, min_range, max_range;
+    int ret_mask;
+    int deskew;      // 1: pass A deskews f_raw into f_xyz first
+    float t_mid, inv_dt;
+};
+
+// The frame's point count and twist come from the state when `st` is set, else from the arguments.
+struct Tw6 {
+    float v[6];
+};
+
+__global__ void k_thin_a(lw_frame_buf fb, const int* __restrict__ m_dev, ThinArgs a, const lw_odom_state* st,
+                         Tw6 tw_arg, const int* gate_deskew, const int* gate_thin, int thin_on) {
+    if (gate_deskew && *gate_deskew == 0) return;
+    const bool thin = thin_on && !(gate_thin && *gate_thin == 0);
+    int64_t m = *m_dev;
+    if (m > fb.cap) m = fb.cap;
+    float tw[6];
+    float t_mid = a.t_mid;
+    if (st) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) tw[k] = st->xi_used[k];
+        t_mid = (float)st->t_mid;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) tw[k] = tw_arg.v[k];
+    }
+    const int mask = (int)(fb.ds_cap - 1);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        float4 p;
+        if (a.deskew) {
+            p = deskew_point(reinterpret_cast<const float4*>(fb.f_raw)[i], t_mid, a.inv_dt, tw);
+            reinterpret_cast<float4*>(fb.f_xyz)[i] = p;
+        } else {
+            p = reinterpret_cast<const float4*>(fb.f_xyz)[i];
+        }
+        if (!thin) continue;
+        int slot = -1;
+        float r = len3(p.x, p.y, p.z);
+        uint32_t at = fb.f_attr[i];
+        if (!(r < a.min_range || r > a.max_range) && tag_of(at) == 0 && ((1 << ret_of(at)) & a.ret_mask) != 0) {
+            int64_t key = key_ijk(ifloor(p.x * a.inv_v), ifloor(p.y * a.inv_v), ifloor(p.z * a.inv_v));
+            bool claimed;
+            slot = claim_slot(key, fb.ds_keys, mask, &claimed);
+            if (slot >= 0) atomicMin(fb.ds_win + slot, (int)i);
+        }
+        fb.ds_slot[i] = slot;
+    }
+}
+
+__global__ void k_thin_b(lw_frame_buf fb, const int* __restrict__ m_dev, const int* gate) {
+    if (gate && *gate == 0) return;
+    int64_t m = *m_dev;
+    if (m > fb.cap) m = fb.cap;
+    int64_t i = (int64_t)blockIdx.x * TILE + threadIdx.x;
+    if ((int64_t)blockIdx.x * TILE >= m) return;  // whole tile past the frame
+    int keep = 0;
+    if (i < m) {
+        int s = fb.ds_slot[i];
+        keep = (s >= 0 && fb.ds_win[s] == (int)i) ? 1 : 0;
+        if (!keep) fb.ds_slot[i] = -1;
+    }
+    int c = __syncthreads_count(keep);
+    if (threadIdx.x == 0) fb.tiles[blockIdx.x] = c;
+}
+
+__global__ void k_thin_c(lw_frame_buf fb, const int* __restrict__ m_dev, int* n_ds, const int* gate) {
+    if (gate && *gate == 0) return;
+    __shared__ int sm[33];
+    int64_t m = *m_dev;
+    if (m > fb.cap) m = fb.cap;
+    const int ntiles = (int)((m + TILE - 1) / TILE);
+    if ((int)blockIdx.x >= ntiles) {
+        if (blockIdx.x == gridDim.x - 1 && ntiles == 0 && threadIdx.x == 0) *n_ds = 0;
+        return;
+    }
+    int64_t i = (int64_t)blockIdx.x * TILE + threadIdx.x;
+    int s = -1;
+    if (i < m) s = fb.ds_slot[i];
+    int keep = s >= 0;
+    int base = prefix_of_tiles(fb.tiles, blockIdx.x);
+    int tot;
+    int r = block_rank(keep, sm, &tot);
+    if (keep) {
+        float4 p = reinterpret_cast<const float4*>(fb.f_xyz)[i];
+        reinterpret_cast<float4*>(fb.ds_xyz)[base + r] = make_float4(p.x, p.y, p.z, len3(p.x, p.y, p.z));
+        fb.ds_keys[s] = EMPTY_KEY;  // each claimed slot has exactly one winner: it clears the slot
+        fb.ds_win[s] = NO_INDEX;
+    }
+    if ((int)blockIdx.x == ntiles - 1 && threadIdx.x == 0) *n_ds = base + tot;
+}
+
+// =====================================================================================================
+// Registration map (odom.py:186-230): per voxel the count and exact fixed-point sums of r = w - centre and
+// r r^T. Deterministic: the slot content does not depend on thread order, and the 4096-point cap takes the
+// first points in index order. Pass D refreshes the record the ICP reads (odom.py:320-368 hoisted out of the
+// per-point loop: a voxel's mean and precision only change when it is inserted into).
+// =====================================================================================================
+
+struct RegArgs {
+    float T[12];  // float row-major 3x4 pose
+    float inv_v, voxel, max_range;
+    int ret_mask;
+};
+
+__device__ __forceinline__ void reg_point(const RegArgs& a, float4 p, int& ix, int& iy, int& iz, float& rx,
+                                          float& ry, float& rz) {
+    float wx, wy, wz;
+    xform(a.T, p.x, p.y, p.z, wx, wy, wz);
+    ix = ifloor(wx * a.inv_v);
+    iy = ifloor(wy * a.inv_v);
+    iz = ifloor(wz * a.inv_v);
+    rx = wx - ((float)ix + 0.5f) * a.voxel;
+    ry = wy - ((float)iy + 0.5f) * a.voxel;
+    rz = wz - ((float)iz + 0.5f) * a.voxel;
+}
+
+__device__ __forceinline__ void reg_add(lw_regmap& reg, int s, float rx, float ry, float rz) {
+    const float FR = (float)LW_FIX_R, FRR = (float)LW_FIX_RR;
+    atomic_add_i64(reg.sum + 3 * s + 0, to_fix(rx, FR));
+    atomic_add_i64(reg.sum + 3 * s + 1, to_fix(ry, FR));
+    atomic_add_i64(reg.sum + 3 * s + 2, to_fix(rz, FR));
+    atomic_add_i64(reg.outer + 6 * s + 0, to_fix(rx * rx, FRR));
+    atomic_add_i64(reg.outer + 6 * s + 1, to_fix(rx * ry, FRR));
+    atomic_add_i64(reg.outer + 6 * s + 2, to_fix(rx * rz, FRR));
+    atomic_add_i64(reg.outer + 6 * s + 3, to_fix(ry * ry, FRR));
+    atomic_add_i64(reg.outer + 6 * s + 4, to_fix(ry * rz, FRR));
+    atomic_add_i64(reg.outer + 6 * s + 5, to_fix(rz * rz, FRR));
+}
+
+// RegArgs from a float64 pose held on the device (the odometry state) or given by the host.
+__device__ __forceinline__ void reg_args_pose(RegArgs& a, const double* T_dev) {
+    if (T_dev)
+        for (int k = 0; k < 12; ++k) a.T[k] = (float)T_dev[k];
+}
+
+__device__ __forceinline__ bool reg_keep(float4 p, uint32_t at, const RegArgs& a) {
+    return !(len3(p.x, p.y, p.z) > a.max_range || tag_of(at) != 0 || ((1 << ret_of(at)) & a.ret_mask) == 0);
+}
+
+__global__ void k_reg_a(const float4* __restrict__ xyz, const uint32_t* __restrict__ attr, const int* n_dev,
+                        int64_t n_ub, RegArgs a, const double* T_dev, lw_regmap reg, int* __restrict__ pslot,
+                        const int* gate) {
+    if (gate && *gate == 0) return;
+    reg_args_pose(a, T_dev);
+    int64_t n = n_dev ? (int64_t)*n_dev : n_ub;
+    if (n > n_ub) n = n_ub;
+    const int mask = (int)(reg.cap - 1);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float4 p = xyz[i];
+        int s = -1;
+        if (reg_keep(p, attr[i], a)) {
+            int ix, iy, iz;
+            float rx, ry, rz;
+            reg_point(a, p, ix, iy, iz, rx, ry, rz);
+            bool claimed;
+            s = claim_slot(key_ijk(ix, iy, iz), reg.keys, mask, &claimed);
+            if (claimed) atomicAdd(reg.stats + 0, 1);
+            if (s < 0) {
+                atomicAdd(reg.stats + 1, 1);
+            } else {
+                atomicAdd(reg.bcnt + s, 1);
+                atomicMin(reg.first + s, (int)i);
+            }
+        }
+        pslot[i] = s;
+    }
+}
+
+__global__ void k_reg_b(const float4* __restrict__ xyz, const int* n_dev, int64_t n_ub, RegArgs a, const double* T_dev,
+                        lw_regmap reg, const int* __restrict__ pslot, const int* gate) {
+    if (gate && *gate == 0) return;
+    reg_args_pose(a, T_dev);
+    int64_t n = n_dev ? (int64_t)*n_dev : n_ub;
+    if (n > n_ub) n = n_ub;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int s = pslot[i];
+        if (s < 0) continue;
+        int pre = reg.cnt[s];
+        int tot = pre + reg.bcnt[s];
+        if (tot <= LW_REG_CAP) {
+            int ix, iy, iz;
+            float rx, ry, rz;
+            reg_point(a, xyz[i], ix, iy, iz, rx, ry, rz);
+            reg_add(reg, s, rx, ry, rz);
+        } else if (pre < LW_REG_CAP && reg.first[s] == (int)i) {
+            // this batch crosses the cap: the lowest-index point adds the first (cap - pre) points in order
+            int room = LW_REG_CAP - pre;
+            for (int64_t j = i; j < n && room > 0; ++j) {
+                if (pslot[j] != s) continue;
+                int ix, iy, iz;
+                float rx, ry, rz;
+                reg_point(a, xyz[j], ix, iy, iz, rx, ry, rz);
+                reg_add(reg, s, rx, ry, rz);
+                --room;
+            }
+        }
+    }
+}
+
+// The derived record of one voxel (odom.py:325-368): the mean in world coordinates and the precision matrices
+// M (all directions) and Mg (surface-normal directions only), plus the direction the metric rms is measured
+// along. Evaluated in float64 from the exact sums.
+__device__ void reg_record(lw_regmap& reg, int s, const lw_rec_params& rp) {
+    float* out = reg.rec + (int64_t)s * LW_REC_FLOATS;
+    int c = reg.cnt[s];
+    if (c <= 0) {
+        for (int k = 0; k < LW_REC_FLOATS; ++k) out[k] = 0.0f;
+        return;
+    }
+    int64_t key = reg.keys[s];
+    int ix = (int)(key & KEY_MASK) - (int)KEY_BIAS;
+    int iy = (int)((key >> 21) & KEY_MASK) - (int)KEY_BIAS;
+    int iz = (int)((key >> 42) & KEY_MASK) - (int)KEY_BIAS;
+    double cf = (double)c;
+    double mr[3], C[9];
+    for (int k = 0; k < 3; ++k) mr[k] = (double)reg.sum[3 * s + k] / (cf * LW_FIX_R);
+    const int up[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C[i * 3 + j] = (double)reg.outer[6 * s + up[i * 3 + j]] / (cf * LW_FIX_RR) - mr[i] * mr[j];
+    double vox = (double)rp.voxel;
+    out[0] = (float)(((double)ix + 0.5) * vox + mr[0]);
+    out[1] = (float)(((double)iy + 0.5) * vox + mr[1]);
+    out[2] = (float)(((double)iz + 0.5) * vox + mr[2]);
+    out[3] = (float)c;
+    double ev[3], Q[9];
+    jacobi_eig<3>(C, ev, Q);
+    double tight2 = rp.tight2, noise2 = rp.noise2, alpha = rp.alpha;
+    int nt = 0;
+    for (int k = 0; k < 3; ++k) nt += ev[k] < tight2 ? 1 : 0;
+    double M[6] = {0, 0, 0, 0, 0, 0}, Mg[6] = {0, 0, 0, 0, 0, 0}, q[3] = {0, 0, 0};
+    float surf = 0.0f;
+    if (c >= 5 && nt <= 1) {
+        int kmin = 0;
+        if (ev[1] < ev[kmin]) kmin = 1;
+        if (ev[2] < ev[kmin]) kmin = 2;
+        for (int k = 0; k < 3; ++k) {
+            double qa[3] = {Q[0 * 3 + k], Q[1 * 3 + k], Q[2 * 3 + k]};
+            double e = fmax(ev[k], 0.0) + noise2;
+            double wa = 1.0 / e;
+            bool tight = !(ev[k] >= tight2);
+            if (!tight) wa = alpha / e;  // a direction the surface extends along: a weak pull only
+            double o6[6] = {qa[0] * qa[0], qa[0] * qa[1], qa[0] * qa[2], qa[1] * qa[1], qa[1] * qa[2], qa[2] * qa[2]};
+            for (int j = 0; j < 6; ++j) {
+                M[j] += wa * o6[j];
+                if (tight) Mg[j] += wa * o6[j];
+            }
+            if (k == kmin) {
+                q[0] = qa[0];
+                q[1] = qa[1];
+                q[2] = qa[2];
+            }
+        }
+        surf = 1.0f;
+    } else {
+        double wa = alpha / (0.25 * vox * vox + noise2);  // too few points, or a line / blob: weak isotropic pull
+        M[0] = M[3] = M[5] = wa;
+    }
+    for (int j = 0; j < 6; ++j) {
+        out[4 + j] = (float)M[j];
+        out[10 + j] = (float)Mg[j];
+    }
+    out[16] = (float)q[0];
+    out[17] = (float)q[1];
+    out[18] = (float)q[2];
+    out[19] = surf;
+}
+
+__global__ void k_reg_d(const int* n_dev, int64_t n_ub, lw_regmap reg, const int* __restrict__ pslot,
+                        lw_rec_params rp, const int* gate) {
+    if (gate && *gate == 0) return;
+    int64_t n = n_dev ? (int64_t)*n_dev : n_ub;
+    if (n > n_ub) n = n_ub;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int s = pslot[i];
+        if (s < 0 || reg.first[s] != (int)i) continue;
+        int tot = reg.cnt[s] + reg.bcnt[s];
+        reg.cnt[s] = tot < LW_REG_CAP ? tot : LW_REG_CAP;
+        reg.bcnt[s] = 0;
+        reg.first[s] = NO_INDEX;
+        reg_record(reg, s, rp);
+    }
+}
+
+__global__ void k_reg_refresh_all(lw_regmap reg, lw_rec_params rp) {
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < reg.cap; s += (int64_t)gridDim.x * blockDim.x)
+        if (reg.keys[s] != EMPTY_KEY) reg_record(reg, (int)s, rp);
+}
+
+// =====================================================================================================
+// Gauss-Newton accumulation (odom.py:275-375). A group of G lanes serves one thinned point: the lanes split
+// the (2 reach + 1)^3 neighbour voxels between them (independent probes in flight per lane), reduce to the
+// closest mean in reference order, and the group leader adds the point's weighted terms. The Jacobian is taken
+// about a point near the frame (the predicted sensor position) so float32 keeps its precision far from the
+// world origin; the float64 reduction maps H, b and Hg back to the reference's twist about the world origin.
+// =====================================================================================================
+
+constexpr int GN_THREADS = 256;
+constexpr int GN_G = 8;  // lanes per point
+constexpr int NTERMS = 53;
+
+struct IcpPose {
+    float R[9];   // rotation
+    float tr[3];  // translation minus the centre c
+    float c[3];   // centre (world)
+};
+
+struct IcpConsts {
+    float inv_v, max_d2, kappa2;
+    int reach, mask;
+};
+
+__device__ __forceinline__ int probe_rest(int64_t key, int h, int mask, const int64_t* __restrict__ keys) {
+#pragma unroll 1
+    for (int p = 1; p < PROBES; ++p) {
+        int s = (h + p) & mask;
+        int64_t k = __ldg(keys + s);
+        if (k == key) return s;
+        if (k == EMPTY_KEY) return -1;
+    }
+    return -1;
+}
+
+template <int R>
+__device__ __forceinline__ void icp_search(int lane_g, float wx, float wy, float wz, const IcpConsts& k,
+                                           const int64_t* __restrict__ keys, const float* __restrict__ rec,
+                                           float& best_d2, int& best_o, int& best_s) {
+    constexpr int S = 2 * R + 1;
+    constexpr int N = S * S * S;
+    constexpr int PER = (N + GN_G - 1) / GN_G;
+    constexpr int B = 4;
+    const int bx = ifloor(wx * k.inv_v), by = ifloor(wy * k.inv_v), bz = ifloor(wz * k.inv_v);
+#pragma unroll
+    for (int j0 = 0; j0 < PER; j0 += B) {
+        int64_t key[B];
+        int h[B];
+        int64_t k0[B];
+        int o[B];
+        bool val[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            o[u] = lane_g + (j0 + u) * GN_G;
+            val[u] = (j0 + u) < PER && o[u] < N;
+            if (val[u]) {
+                int dz = o[u] % S - R, dy = (o[u] / S) % S - R, dx = o[u] / (S * S) - R;
+                key[u] = key_ijk(bx + dx, by + dy, bz + dz);
+                h[u] = slot_hash(key[u]) & k.mask;
+                k0[u] = __ldg(keys + h[u]);
+            }
+        }
+        int s[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            s[u] = -1;
+            if (val[u]) {
+                if (k0[u] == key[u]) s[u] = h[u];
+                else if (k0[u] != EMPTY_KEY) s[u] = probe_rest(key[u], h[u], k.mask, keys);
+            }
+        }
+        float4 hd[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+            if (s[u] >= 0) hd[u] = __ldg(reinterpret_cast<const float4*>(rec + (int64_t)s[u] * LW_REC_FLOATS));
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            if (s[u] >= 0 && hd[u].w > 0.0f) {
+                float dx = wx - hd[u].x, dy = wy - hd[u].y, dz = wz - hd[u].z;
+                float d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 < best_d2) {
+                    best_d2 = d2;
+                    best_o = o[u];
+                    best_s = s[u];
+                }
+            }
+        }
+    }
+}
+
+// Accumulate one point's terms (odom.py:233-272, 335-375) into a[NTERMS].
+__device__ __forceinline__ void icp_terms(float* a, const float* __restrict__ rec, int s, float wx, float wy, float wz,
+                                          float lx, float ly, float lz, float range, float kappa2) {
+    const float* rr = rec + (int64_t)s * LW_REC_FLOATS;
+    float4 h0 = __ldg(reinterpret_cast<const float4*>(rr));
+    float4 h1 = __ldg(reinterpret_cast<const float4*>(rr + 4));
+    float4 h2 = __ldg(reinterpret_cast<const float4*>(rr + 8));
+    float4 h3 = __ldg(reinterpret_cast<const float4*>(rr + 12));
+    float4 h4 = __ldg(reinterpret_cast<const float4*>(rr + 16));
+    const float M[6] = {h1.x, h1.y, h1.z, h1.w, h2.x, h2.y};
+    const float Mg[6] = {h2.z, h2.w, h3.x, h3.y, h3.z, h3.w};
+    float r0 = wx - h0.x, r1 = wy - h0.y, r2 = wz - h0.z;
+    // M r
+    float Mr0 = fmaf(M[0], r0, fmaf(M[1], r1, M[2] * r2));
+    float Mr1 = fmaf(M[1], r0, fmaf(M[3], r1, M[4] * r2));
+    float Mr2 = fmaf(M[2], r0, fmaf(M[4], r1, M[5] * r2));
+    float d2 = fmaf(r0, Mr0, fmaf(r1, Mr1, r2 * Mr2));
+    float wgt = 1.0f / (1.0f + d2 / kappa2);
+    wgt = wgt * wgt;  // Geman-McClure
+    float rn = (h4.w > 0.5f) ? fmaf(r0, h4.x, fmaf(r1, h4.y, r2 * h4.z)) : sqrtf(fmaf(r0, r0, fmaf(r1, r1, r2 * r2)));
+    // Jacobian columns (odom.py:305-307) at the re-centred point l
+    const float C[6][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f},
+                           {0.f, -lz, ly},  {lz, 0.f, -lx}, {-ly, lx, 0.f}};
+    float MC[6][3], GC[6][3];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        MC[q][0] = fmaf(M[0], C[q][0], fmaf(M[1], C[q][1], M[2] * C[q][2]));
+        MC[q][1] = fmaf(M[1], C[q][0], fmaf(M[3], C[q][1], M[4] * C[q][2]));
+        MC[q][2] = fmaf(M[2], C[q][0], fmaf(M[4], C[q][1], M[5] * C[q][2]));
+        GC[q][0] = fmaf(Mg[0], C[q][0], fmaf(Mg[1], C[q][1], Mg[2] * C[q][2]));
+        GC[q][1] = fmaf(Mg[1], C[q][0], fmaf(Mg[3], C[q][1], Mg[4] * C[q][2]));
+        GC[q][2] = fmaf(Mg[2], C[q][0], fmaf(Mg[4], C[q][1], Mg[5] * C[q][2]));
+    }
+    int idx = 0;
+#pragma unroll
+    for (int p = 0; p < 6; ++p)
+#pragma unroll
+        for (int q = p; q < 6; ++q) {
+            a[LW_ACC_H + idx] = fmaf(wgt, fmaf(C[p][0], MC[q][0], fmaf(C[p][1], MC[q][1], C[p][2] * MC[q][2])), a[LW_ACC_H + idx]);
+            a[LW_ACC_HG + idx] = fmaf(wgt, fmaf(C[p][0], GC[q][0], fmaf(C[p][1], GC[q][1], C[p][2] * GC[q][2])), a[LW_ACC_HG + idx]);
+            ++idx;
+        }
+#pragma unroll
+    for (int p = 0; p < 6; ++p)
+        a[LW_ACC_B + p] = fmaf(wgt, fmaf(C[p][0], Mr0, fmaf(C[p][1], Mr1, C[p][2] * Mr2)), a[LW_ACC_B + p]);
+    a[LW_ACC_COUNT] += 1.0f;
+    a[LW_ACC_ERR] = fmaf(wgt, d2, a[LW_ACC_ERR]);
+    a[LW_ACC_RMS] = fmaf(wgt, rn * rn, a[LW_ACC_RMS]);
+    a[LW_ACC_WEIGHT] += wgt;
+    a[LW_ACC_RANGE] += range;
+}
+
+// One accumulation pass of this CTA over its share of the thinned points; writes the CTA's float64 partial.
+__device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P, const IcpConsts& k,
+                         const int64_t* __restrict__ keys, const float* __restrict__ rec, double* __restrict__ part) {
+    __shared__ float red[GN_THREADS / 32][NTERMS];
+    float a[NTERMS];
+#pragma unroll
+    for (int t = 0; t < NTERMS; ++t) a[t] = 0.0f;
+    const int lane = threadIdx.x & 31;
+    const int lane_g = lane & (GN_G - 1);
+    const int group = (blockIdx.x * GN_THREADS + threadIdx.x) / GN_G;
+    const int ngroups = gridDim.x * GN_THREADS / GN_G;
+    for (int j = group; j < n; j += ngroups) {
+        float4 p = __ldg(ds + j);
+        float lx = P.R[0] * p.x + P.R[1] * p.y + P.R[2] * p.z + P.tr[0];
+        float ly = P.R[3] * p.x + P.R[4] * p.y + P.R[5] * p.z + P.tr[1];
+        float lz = P.R[6] * p.x + P.R[7] * p.y + P.R[8] * p.z + P.tr[2];
+        float wx = lx + P.c[0], wy = ly + P.c[1], wz = lz + P.c[2];
+        float bd = k.max_d2;
+        int bo = 0x7FFFFFFF, bs = -1;
+        if (k.reach == 2)
+            icp_search<2>(lane_g, wx, wy, wz, k, keys, rec, bd, bo, bs);
+        else
+            icp_search<1>(lane_g, wx, wy, wz, k, keys, rec, bd, bo, bs);
+#pragma unroll
+        for (int off = GN_G / 2; off > 0; off >>= 1) {
+            float od = __shfl_xor_sync(0xffffffffu, bd, off);
+            int oo = __shfl_xor_sync(0xffffffffu, bo, off);
+            int os = __shfl_xor_sync(0xffffffffu, bs, off);
+            if (od < bd || (od == bd && oo < bo)) {
+                bd = od;
+                bo = oo;
+                bs = os;
+            }
+        }
+        if (lane_g == 0 && bs >= 0) icp_terms(a, rec, bs, wx, wy, wz, lx, ly, lz, p.w, k.kappa2);
+    }
+    // group leaders -> lane 0 of each warp
+#pragma unroll
+    for (int t = 0; t < NTERMS; ++t) {
+        float v = a[t];
+#pragma unroll
+        for (int off = 16; off >= GN_G; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        a[t] = v;
+    }
+    if (lane == 0)
+#pragma unroll
+        for (int t = 0; t < NTERMS; ++t) red[threadIdx.x >> 5][t] = a[t];
+    __syncthreads();
+    if (threadIdx.x < NTERMS) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < GN_THREADS / 32; ++w) s += (double)red[w][threadIdx.x];
+        part[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void sym6_from(const double* up, double* H) {
+    int idx = 0;
+    for (int p = 0; p < 6; ++p)
+        for (int q = p; q < 6; ++q) {
+            H[p * 6 + q] = up[idx];
+            H[q * 6 + p] = up[idx];
+            ++idx;
+        }
+}
+
+// Reduce the CTA partials in a fixed order and map the re-centred sums back to the world-origin twist:
+// J_world = J_c A with A = [[I, -[c]x], [0, I]], so H = A^T H_c A and b = A^T b_c.
+__device__ void reduce_partials(const double* __restrict__ part, int grid, const double* c, double* v64) {
+    __shared__ double vs[LW_ACC_STRIDE];
+    if (threadIdx.x < LW_ACC_STRIDE) {
+        double s = 0.0;
+        if (threadIdx.x < NTERMS)
+            for (int b = 0; b < grid; ++b) s += part[(int64_t)b * LW_ACC_STRIDE + threadIdx.x];
+        vs[threadIdx.x] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double A[36];
+        for (int i = 0; i < 36; ++i) A[i] = (i % 7 == 0) ? 1.0 : 0.0;
+        // -[c]x in the upper right block
+        A[0 * 6 + 3] = 0.0;   A[0 * 6 + 4] = c[2];  A[0 * 6 + 5] = -c[1];
+        A[1 * 6 + 3] = -c[2]; A[1 * 6 + 4] = 0.0;   A[1 * 6 + 5] = c[0];
+        A[2 * 6 + 3] = c[1];  A[2 * 6 + 4] = -c[0]; A[2 * 6 + 5] = 0.0;
+        for (int t = 0; t < LW_ACC_STRIDE; ++t) v64[t] = vs[t];
+        for (int which = 0; which < 2; ++which) {
+            int off = which == 0 ? LW_ACC_H : LW_ACC_HG;
+            double H[36], AH[36];
+            sym6_from(vs + off, H);
+            for (int i = 0; i < 6; ++i)
+                for (int j = 0; j < 6; ++j) {
+                    double s = 0.0;
+                    for (int k = 0; k < 6; ++k) s += H[i * 6 + k] * A[k * 6 + j];
+                    AH[i * 6 + j] = s;
+                }
+            int idx = 0;
+            for (int p = 0; p < 6; ++p)
+                for (int q = p; q < 6; ++q) {
+                    double s = 0.0;
+                    for (int k = 0; k < 6; ++k) s += A[k * 6 + p] * AH[k * 6 + q];
+                    v64[off + idx] = s;
+                    ++idx;
+                }
+        }
+        for (int p = 0; p < 6; ++p) {
+            double s = 0.0;
+            for (int k = 0; k < 6; ++k) s += A[k * 6 + p] * vs[LW_ACC_B + k];
+            v64[LW_ACC_B + p] = s;
+        }
+    }
+    __syncthreads();
+}
+
+__device__ void make_pose(const double* T, const double* c, IcpPose& P) {
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) P.R[i * 3 + j] = (float)T[i * 4 + j];
+        P.tr[i] = (float)(T[i * 4 + 3] - c[i]);
+        P.c[i] = (float)c[i];
+    }
+}
+
+__device__ __forceinline__ void schedule(int it, float voxel, int& reach, float& max_d2, float& kappa) {
+    reach = it < 3 ? 2 : 1;  // wide search first, then local refinement (odom.py:765-767)
+    float d = ((float)reach + 0.5f) * voxel;
+    max_d2 = d * d;
+    kappa = fmaxf(2.0f, (float)(6.0 * pow(0.7, (double)it)));
+}
+
+// ---- the float64 step (odom.py:772-796) ----------------------------------------------------------------
+
+// Sensor basis (odom.py:425-433): SB = [[R, [c]x R / L], [0, R / L]] and its inverse [[R^T, -R^T [c]x], [0, L R^T]].
+__device__ void sensor_basis(const double* T, double L, double* SB, double* SBi) {
+    double R[9], c[3] = {T[3], T[7], T[11]};
+    mat44_rot(T, R);
+    double cx[9] = {0.0, -c[2], c[1], c[2], 0.0, -c[0], -c[1], c[0], 0.0};
+    for (int i = 0; i < 36; ++i) SB[i] = SBi[i] = 0.0;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double cr = 0.0, rc = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                cr += cx[i * 3 + k] * R[k * 3 + j];
+                rc += R[k * 3 + i] * cx[k * 3 + j];  // (R^T [c]x)_ij
+            }
+            SB[i * 6 + j] = R[i * 3 + j];
+            SB[i * 6 + 3 + j] = cr / L;
+            SB[(3 + i) * 6 + 3 + j] = R[i * 3 + j] / L;
+            SBi[i * 6 + j] = R[j * 3 + i];
+            SBi[i * 6 + 3 + j] = -rc;
+            SBi[(3 + i) * 6 + 3 + j] = L * R[j * 3 + i];
+        }
+}
+
+__device__ __forceinline__ void matmul6(const double* A, const double* B, double* C, bool At = false) {
+    double t[36];
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+            double s = 0.0;
+            for (int k = 0; k < 6; ++k) s += (At ? A[k * 6 + i] : A[i * 6 + k]) * B[k * 6 + j];
+            t[i * 6 + j] = s;
+        }
+    for (int i = 0; i < 36; ++i) C[i] = t[i];
+}
+
+__device__ __forceinline__ void matvec6(const double* A, const double* x, double* y, bool At = false) {
+    double t[6];
+    for (int i = 0; i < 6; ++i) {
+        double s = 0.0;
+        for (int k = 0; k < 6; ++k) s += (At ? A[k * 6 + i] : A[i * 6 + k]) * x[k];
+        t[i] = s;
+    }
+    for (int i = 0; i < 6; ++i) y[i] = t[i];
+}
+
+struct StepOut {
+    int status;  // 0 continue, 1 converged, 2 too few correspondences, 3 singular
+    int corr, degen;
+    double rms;
+};
+
+// One Gauss-Newton update of T (odom.py:769-796). H (world twist) is returned for the conditioning stat.
+__device__ __noinline__ StepOut gn_step(const double* v, double* T, const double* T_pred, const lw_odom_params& prm,
+                                        double* H) {
+    StepOut o;
+    o.corr = (int)v[LW_ACC_COUNT];
+    o.degen = 0;
+    o.rms = 0.0;
+    if (o.corr < prm.min_corr) {
+        o.status = 2;
+        return o;
+    }
+    double b[6], Hg[36], A[36], rhs[6];
+    sym6_from(v + LW_ACC_H, H);
+    sym6_from(v + LW_ACC_HG, Hg);
+    for (int k = 0; k < 6; ++k) b[k] = v[LW_ACC_B + k];
+    double L = fmax(v[LW_ACC_RANGE] / (double)o.corr, 1.0);
+    o.rms = sqrt(fmax(v[LW_ACC_RMS], 0.0) / fmax(v[LW_ACC_WEIGHT], 1e-9));
+    double dmean = 0.0;
+    for (int k = 0; k < 6; ++k) dmean += H[k * 7];
+    dmean /= 6.0;
+    for (int i = 0; i < 36; ++i) A[i] = H[i];
+    for (int k = 0; k < 6; ++k) {
+        A[k * 7] += 1e-9 * dmean + prm.damping * H[k * 7];
+        rhs[k] = -b[k];
+    }
+    // the left twist from T back onto the prediction (odom.py:397-401)
+    double Ti[16], Mp[16], xi[6];
+    mat44_inv_rigid(T, Ti);
+    mat44_mul(T_pred, Ti, Mp);
+    body_twist(Mp, xi);
+    double SB[36], SBi[36];
+    sensor_basis(T, L, SB, SBi);
+    if (prm.prior_info > 0.0) {
+        double P[36], Pxi[6];
+        matmul6(SBi, SBi, P, true);
+        for (int i = 0; i < 36; ++i) P[i] *= prm.prior_info;
+        matvec6(P, xi, Pxi);
+        for (int i = 0; i < 36; ++i) A[i] += P[i];
+        for (int k = 0; k < 6; ++k) rhs[k] += Pxi[k];
+    }
+    double delta[6];
+    if (prm.degen_thr > 0.0) {
+        // odom.py:436-455: hold the directions the surface normals do not constrain at the prediction
+        double G[36], V[36], lam[6], tmp[36];
+        matmul6(Hg, SB, tmp);
+        matmul6(SB, tmp, G, true);
+        jacobi_eig<6>(G, lam, V);
+        bool good[6];
+        int ng = 0;
+        for (int k = 0; k < 6; ++k) {
+            good[k] = lam[k] >= prm.degen_thr;
+            ng += good[k] ? 1 : 0;
+        }
+        o.degen = 6 - ng;
+        if (ng == 6) {
+            if (!lu_solve<6>(A, rhs, delta)) {
+                o.status = 3;
+                return o;
+            }
+        } else {
+            double z[6], d0[6];
+            matvec6(SBi, xi, z);  // solve(J, to_pred)
+            for (int i = 0; i < 6; ++i) d0[i] = 0.0;
+            for (int k = 0; k < 6; ++k) {
+                if (good[k]) continue;
+                double pr = 0.0;
+                for (int i = 0; i < 6; ++i) pr += V[i * 6 + k] * z[i];
+                for (int i = 0; i < 6; ++i) d0[i] += V[i * 6 + k] * pr;
+            }
+            if (ng > 0) {
+                double As[36], Jr[6], Asd[6], g[6], Ag[36], y[6], Vg[36];
+                int cols[6], nc = 0;
+                for (int k = 0; k < 6; ++k)
+                    if (good[k]) cols[nc++] = k;
+                matmul6(A, SB, tmp);
+                matmul6(SB, tmp, As, true);
+                matvec6(SB, rhs, Jr, true);
+                matvec6(As, d0, Asd);
+                for (int i = 0; i < 6; ++i)
+                    for (int a = 0; a < nc; ++a) Vg[i * 6 + a] = V[i * 6 + cols[a]];
+                for (int a = 0; a < nc; ++a) {
+                    double s = 0.0;
+                    for (int i = 0; i < 6; ++i) s += Vg[i * 6 + a] * (Jr[i] - Asd[i]);
+                    g[a] = s;
+                    for (int c2 = 0; c2 < nc; ++c2) {
+                        double s2 = 0.0;
+                        for (int i = 0; i < 6; ++i) {
+                            double t2 = 0.0;
+                            for (int j = 0; j < 6; ++j) t2 += As[i * 6 + j] * Vg[j * 6 + c2];
+                            s2 += Vg[i * 6 + a] * t2;
+                        }
+                        Ag[a * 6 + c2] = s2;
+                    }
+                }
+                if (!lu_solve<6>(Ag, g, y, nc)) {
+                    o.status = 3;
+                    return o;
+                }
+                for (int i = 0; i < 6; ++i)
+                    for (int a = 0; a < nc; ++a) d0[i] += Vg[i * 6 + a] * y[a];
+            }
+            matvec6(SB, d0, delta);
+        }
+    } else if (!lu_solve<6>(A, rhs, delta)) {
+        o.status = 3;
+        return o;
+    }
+    apply_twist(T, delta);
+    double nt = sqrt(delta[0] * delta[0] + delta[1] * delta[1] + delta[2] * delta[2]);
+    double nr = sqrt(delta[3] * delta[3] + delta[4] * delta[4] + delta[5] * delta[5]);
+    o.status = (nt < 1e-4 && nr < 1e-4) ? 1 : 0;  // STEP_TOL (odom.py:88)
+    return o;
+}
+
+// min/max eigenvalue of H normalised by its diagonal (odom.py:797-800)
+__device__ __noinline__ double conditioning(const double* H) {
+    double dg[6], Hn[36], ev[6], V[36];
+    for (int k = 0; k < 6; ++k) dg[k] = sqrt(fmax(H[k * 7], 1e-12));
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) Hn[i * 6 + j] = H[i * 6 + j] / (dg[i] * dg[j]);
+    jacobi_eig<6>(Hn, ev, V);
+    double lo = ev[0], hi = ev[0];
+    for (int k = 1; k < 6; ++k) {
+        lo = fmin(lo, ev[k]);
+        hi = fmax(hi, ev[k]);
+    }
+    return fmax(lo, 0.0) / fmax(hi, 1e-12);
+}
+
+// The whole registration loop (odom.py:752-803) in one cooperative launch. Every CTA reduces the partials
+// and computes the same float64 step, so one grid barrier per iteration suffices.
+__global__ void __launch_bounds__(GN_THREADS, 1)
+    k_gn(const float4* __restrict__ ds, const int* __restrict__ n_dev, lw_odom_params prm, lw_odom_state* st,
+         const int64_t* __restrict__ keys, const float* __restrict__ rec, int mask, lw_gn_scratch gn, int which) {
+    const int* gate = which == 0 ? &st->run_reg : (which == 1 ? &st->redo : nullptr);
+    if (gate && *gate == 0) return;  // uniform: every CTA reads the same flag before any barrier
+    __shared__ double sT[16], sTp[16], sc[3], v64[LW_ACC_STRIDE];
+    __shared__ int s_stop, s_corr, s_iters, s_degen;
+    __shared__ double s_rms;
+    const int n = *n_dev;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 16; ++i) sT[i] = sTp[i] = st->T_pred[i];
+        sc[0] = st->T_pred[3];
+        sc[1] = st->T_pred[7];
+        sc[2] = st->T_pred[11];
+        s_stop = 0;
+        s_corr = 0;
+        s_iters = 0;
+        s_degen = 0;
+        s_rms = 0.0;
+    }
+    __syncthreads();
+    if (n < prm.min_corr) {  // odom.py:754-757
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            for (int i = 0; i < 16; ++i) st->T_reg[i] = sTp[i];
+            st->ok = 0;
+            st->n_ds = n;
+        }
+        return;
+    }
+    const float voxel = (float)prm.reg_voxel;
+    IcpConsts k;
+    k.inv_v = (float)(1.0 / prm.reg_voxel);
+    k.mask = mask;
+    double H[36];
+    for (int i = 0; i < 36; ++i) H[i] = (i % 7 == 0) ? 1.0 : 0.0;
+    for (int it = 0; it < prm.max_iter; ++it) {
+        float kappa;
+        schedule(it, voxel, k.reach, k.max_d2, kappa);
+        k.kappa2 = kappa * kappa;
+        IcpPose P;
+        make_pose(sT, sc, P);
+        double* part = gn.part + (int64_t)(it & 1) * gn.grid * LW_ACC_STRIDE;
+        icp_pass(ds, n, P, k, keys, rec, part + (int64_t)blockIdx.x * LW_ACC_STRIDE);
+        if (!grid_barrier(gn.bar, gn.err, 1)) return;
+        reduce_partials(part, gn.grid, sc, v64);
+        if (threadIdx.x == 0) {
+            StepOut o = gn_step(v64, sT, sTp, prm, H);
+            s_corr = o.corr;
+            if (o.status != 2) s_rms = o.rms;
+            if (o.status == 0 || o.status == 1) {
+                s_iters = it + 1;
+                s_degen = o.degen;
+            }
+            s_stop = o.status != 0;
+        }
+        __syncthreads();
+        if (s_stop) break;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        bool ok = s_corr >= prm.min_corr;
+        double cond = st->cond;
+        if (ok) cond = conditioning(H);
+        for (int i = 0; i < 16; ++i) st->T_reg[i] = sT[i];
+        st->ok = ok ? 1 : 0;
+        st->n_ds = n;
+        st->iters = s_iters;
+        st->corr = s_corr;
+        st->rms = s_rms;
+        st->cond = cond;
+        st->degen = s_degen;
+        st->weak = (cond < 1e-3 || s_degen > 0) ? 1 : 0;  // WEAK_COND (odom.py:90)
+    }
+}
+
+// Standalone accumulation at a host pose, for the parity tests and the batched callers.
+__global__ void __launch_bounds__(GN_THREADS, 1)
+    k_acc_once(const float4* __restrict__ ds, const int* __restrict__ n_dev, int64_t n_ub, IcpPose P, IcpConsts k,
+               const int64_t* __restrict__ keys, const float* __restrict__ rec, double* part) {
+    int n = n_dev ? *n_dev : (int)n_ub;
+    icp_pass(ds, n, P, k, keys, rec, part + (int64_t)blockIdx.x * LW_ACC_STRIDE);
+}
+
+__global__ void k_acc_reduce(const double* part, int grid, double c0, double c1, double c2, double* out) {
+    __shared__ double v64[LW_ACC_STRIDE];
+    double c[3] = {c0, c1, c2};
+    reduce_partials(part, grid, c, v64);
+    if (threadIdx.x < LW_ACC_STRIDE) out[threadIdx.x] = v64[threadIdx.x];
+}
+
+// =====================================================================================================
+// Frame state machine (odom.py:642-694, 712-727) on one thread.
+// =====================================================================================================
+
+__global__ void k_ctl_begin(int k, lw_odom_params prm, lw_odom_state* st, const int* count) {
+    int m = *count;
+    if (m > prm.frame_cap) m = prm.frame_cap;
+    st->m = m;
+    st->frame_k = k;
+    int warm = st->map_frames < prm.warmup;
+    st->warm = warm;
+    st->t_mid = ((double)k + 0.5) * prm.frame_dt;
+    for (int j = 0; j < 6; ++j) st->xi_used[j] = (prm.deskew && !warm) ? st->xi[j] : 0.0f;
+    double Ts[16];
+    if (warm) {
+        for (int i = 0; i < 16; ++i) Ts[i] = st->T[i];
+    } else {
+        mat44_mul(st->T, st->delta, Ts);  // predict() (odom.py:591-592)
+    }
+    for (int i = 0; i < 16; ++i) st->T_pred[i] = st->T_reg[i] = Ts[i];
+    st->redo = 0;
+    st->do_insert = 0;
+    st->run_reg = 0;
+    if (m < prm.min_points) {
+        st->skipped += 1;
+        st->ok = 0;
+    } else if (warm) {
+        st->ok = 1;  // the map is still filling in: assume the sensor holds still
+    } else {
+        st->run_reg = 1;
+    }
+}
+
+// After the first registration: deskew again with the frame's own motion when it differs (odom.py:673-679).
+__global__ void k_ctl_mid(lw_odom_params prm, lw_odom_state* st) {
+    st->redo = 0;
+    if (!(st->run_reg && st->ok && prm.deskew && prm.redeskew && st->has_prev)) return;
+    double Ti[16], D[16], xn[6];
+    mat44_inv_rigid(st->T_prev, Ti);
+    mat44_mul(Ti, st->T_reg, D);
+    body_twist(D, xn);
+    float xf[6];
+    for (int j = 0; j < 6; ++j) xf[j] = (float)xn[j];
+    float dr0 = xf[3] - st->xi_used[3], dr1 = xf[4] - st->xi_used[4], dr2 = xf[5] - st->xi_used[5];
+    float dt0 = xf[0] - st->xi_used[0], dt1 = xf[1] - st->xi_used[1], dt2 = xf[2] - st->xi_used[2];
+    float nr = sqrtf(dr0 * dr0 + dr1 * dr1 + dr2 * dr2), nt = sqrtf(dt0 * dt0 + dt1 * dt1 + dt2 * dt2);
+    if (nr > 2e-3f || nt > 5e-3f) {  // REDESKEW_ROT / REDESKEW_TRANS (odom.py:92-93)
+        for (int j = 0; j < 6; ++j) st->xi_used[j] = xf[j];
+        for (int i = 0; i < 16; ++i) st->T_pred[i] = st->T_reg[i];
+        st->redo = 1;
+    }
+}
+
+// Keyframe decision, velocity update, pose table and trajectory (odom.py:648-657, 682-694, 712-717).
+__global__ void k_ctl_end(lw_odom_params prm, lw_odom_state* st, lw_pose_table pt, int epoch, lw_traj_rec* traj,
+                          int64_t traj_cap) {
+    double T[16];
+    for (int i = 0; i < 16; ++i) T[i] = st->T_reg[i];
+    int warm = st->warm;
+    int ins = 0;
+    if (st->ok) {
+        if (warm || !st->has_key) {
+            ins = 1;
+        } else {
+            double Ki[16], D[16], R[9], rv[3];
+            mat44_inv_rigid(st->T_key, Ki);
+            mat44_mul(Ki, T, D);
+            mat44_rot(D, R);
+            mat_to_rotvec(R, rv);
+            double ang = sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]) * (180.0 / 3.14159265358979323846);
+            double dist = sqrt(D[3] * D[3] + D[7] * D[7] + D[11] * D[11]);
+            ins = (dist >= prm.kf_dist || ang >= prm.kf_angle_deg) ? 1 : 0;
+        }
+    }
+    st->do_insert = ins;
+    if (ins) {
+        st->map_frames += 1;
+        for (int i = 0; i < 16; ++i) st->T_key[i] = T[i];
+        st->has_key = 1;
+        st->keyframes += 1;
+    }
+    if (st->has_prev && !warm) {
+        double Ti[16], D[16];
+        mat44_inv_rigid(st->T_prev, Ti);
+        mat44_mul(Ti, T, D);
+        double jump = sqrt(D[3] * D[3] + D[7] * D[7] + D[11] * D[11]);
+        if (jump < 1.5) {  // MAX_FRAME_JUMP (odom.py:94)
+            double xd[6];
+            body_twist(D, xd);
+            for (int j = 0; j < 6; ++j) st->xi[j] = (float)xd[j];
+            if (prm.velocity_smooth > 0.0) {
+                double a = prm.velocity_smooth;
+                for (int j = 0; j < 6; ++j) st->xi_s[j] = a * st->xi_s[j] + (1.0 - a) * (double)st->xi[j];
+                twist_matrix(st->xi_s, st->delta);
+            } else {
+                for (int i = 0; i < 16; ++i) st->delta[i] = D[i];
+            }
+        } else {  // a failure, not motion: predict rest from here
+            mat44_eye(st->delta);
+            for (int j = 0; j < 6; ++j) {
+                st->xi[j] = 0.0f;
+                st->xi_s[j] = 0.0;
+            }
+        }
+    }
+    for (int i = 0; i < 16; ++i) st->T_prev[i] = st->T[i] = T[i];
+    st->has_prev = 1;
+    int k = st->frame_k;
+    int j = k & (LW_POSE_SLOTS - 1);
+    for (int i = 0; i < 16; ++i) pt.poses[j * 16 + i] = (float)T[i];
+    for (int i = 0; i < 6; ++i) pt.tw[j * 6 + i] = st->xi_used[i];
+    pt.owner_frame[j] = k;
+    pt.owner_epoch[j] = epoch;
+    if (traj && traj_cap > 0) {
+        lw_traj_rec* r = traj + (st->traj_len % traj_cap);
+        for (int i = 0; i < 16; ++i) r->T[i] = T[i];
+        r->t_mid = st->t_mid;
+        r->k = k;
+        r->ok = st->ok;
+        r->iters = st->run_reg ? st->iters : 0;
+        r->corr = st->run_reg ? st->corr : 0;
+    }
+    st->traj_len += 1;
+    st->frames += 1;
+}
+
+__global__ void k_predict_poses(int k0, int k1, int current, const lw_odom_state* st, lw_pose_table pt, int epoch) {
+    __shared__ float P[16];
+    if (threadIdx.x == 0) {
+        double Tp[16];
+        if (current & 1) {
+            for (int i = 0; i < 16; ++i) Tp[i] = st->T[i];
+        } else {
+            mat44_mul(st->T, st->delta, Tp);
+        }
+        for (int i = 0; i < 16; ++i) P[i] = (float)Tp[i];
+    }
+    __syncthreads();
+    if (k1 - k0 > LW_POSE_SLOTS) k0 = k1 - LW_POSE_SLOTS;
+    for (int k = k0 + (int)(blockIdx.x * blockDim.x + threadIdx.x); k < k1; k += gridDim.x * blockDim.x) {
+        int j = k & (LW_POSE_SLOTS - 1);
+        for (int i = 0; i < 16; ++i) pt.poses[j * 16 + i] = P[i];
+        for (int i = 0; i < 6; ++i) pt.tw[j * 6 + i] = (current & 2) ? 0.0f : st->xi[i];
+        pt.owner_frame[j] = k;
+        pt.owner_epoch[j] = epoch;
+    }
+}
+
+__global__ void k_reset_state(lw_odom_state* st, lw_odom_state init) { *st = init; }
+
+__global__ void k_zero_count(int* c) { *c = 0; }
+
+__global__ void k_restart_clock(lw_odom_state* st) {
+    st->has_prev = 0;
+    mat44_eye(st->delta);
+    for (int j = 0; j < 6; ++j) {
+        st->xi[j] = 0.0f;
+        st->xi_s[j] = 0.0;
+    }
+}
+
+__global__ void k_fill_i64(int64_t* a, int64_t n, int64_t v) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) a[i] = v;
+}
+__global__ void k_fill_i32(int32_t* a, int64_t n, int32_t v) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) a[i] = v;
+}
+
+}  // namespace lw
+
+// =========================================================================================================
+// C ABI
+// =========================================================================================================
+using namespace lw;
+
+static int gn_grid(const lw_gn_scratch* gn) {
+    int sms = device_sms();
+    int g = gn->grid;
+    if (g <= 0 || g > sms) g = sms;
+    return g;
+}
+
+static ThinArgs thin_args(const lw_odom_params* prm) {
+    ThinArgs a;
+    a.inv_v = (float)(2.0 / prm->reg_voxel);
+    a.min_range = (float)prm->min_range;
+    a.max_range = (float)prm->max_range;
+    a.ret_mask = prm->ret_mask;
+    a.deskew = 1;
+    a.t_mid = 0.0f;
+    a.inv_dt = (float)(1.0 / prm->frame_dt);
+    return a;
+}
+
+static lw_rec_params rec_params(const lw_odom_params* prm) {
+    lw_rec_params rp;
+    rp.voxel = (float)prm->reg_voxel;
+    double tf = 0.6 * prm->reg_voxel / sqrt(12.0);  // TIGHT_FRACTION (odom.py:89, 761)
+    rp.tight2 = (float)(tf * tf);
+    rp.noise2 = (float)(prm->noise * prm->noise);
+    rp.alpha = (float)prm->alpha;
+    return rp;
+}
+
+static int launch_gn(const float* ds4, const int32_t* n_dev, const lw_odom_params* prm, lw_odom_state* st,
+                     const lw_regmap* reg, lw_gn_scratch* gn, int which, cudaStream_t s) {
+    int grid = gn_grid(gn);
+    lw_gn_scratch g = *gn;
+    g.grid = grid;
+    const float4* dsp = reinterpret_cast<const float4*>(ds4);
+    int mask = (int)(reg->cap - 1);
+    const int64_t* keys = reg->keys;
+    const float* rec = reg->rec;
+    lw_odom_params p = *prm;
+    void* args[] = {(void*)&dsp, (void*)&n_dev, (void*)&p, (void*)&st, (void*)&keys, (void*)&rec,
+                    (void*)&mask, (void*)&g, (void*)&which};
+    LW_CUDA(cudaLaunchCooperativeKernel((const void*)k_gn, dim3(grid), dim3(GN_THREADS), args, 0, s));
+    return LW_OK;
+}
+
+extern "C" {
+
+int lw_frame_append(const float* xyz, int32_t xyz_stride, const uint32_t* attr, const float* t, int64_t n,
+                    double inv_dt, int32_t k_min, int32_t k_open, lw_frame_buf* fb, void* stream) {
+    if (n <= 0) return LW_OK;
+    if (!xyz || !attr || !t || !fb || (xyz_stride != 3 && xyz_stride != 4))
+        return set_error(LW_EINVAL, "lw_frame_append: bad arguments (stride %d)", xyz_stride);
+    cudaStream_t s = (cudaStream_t)stream;
+    int nt = blocks_for(n, TILE);
+    if ((int64_t)nt > fb->cap / TILE + 1 && nt > 1) {
+        // the tile scratch holds cap/TILE + 1 counts; a larger batch is appended in frame-sized chunks
+        int64_t chunk = (fb->cap / TILE) * TILE;
+        if (chunk <= 0) chunk = TILE;
+        for (int64_t off = 0; off < n; off += chunk) {
+            int64_t c = n - off < chunk ? n - off : chunk;
+            int r = lw_frame_append(xyz + off * xyz_stride, xyz_stride, attr + off, t + off, c, inv_dt, k_min, k_open,
+                                    fb, stream);
+            if (r != LW_OK) return r;
+        }
+        return LW_OK;
+    }
+    float idt = (float)inv_dt;
+    k_append_count<<<nt, TILE, 0, s>>>(t, n, idt, k_min, k_open, fb->tiles);
+    if (xyz_stride == 3)
+        k_append_scatter<3><<<nt, TILE, 0, s>>>(xyz, attr, t, n, idt, k_min, k_open, fb->tiles, *fb);
+    else
+        k_append_scatter<4><<<nt, TILE, 0, s>>>(xyz, attr, t, n, idt, k_min, k_open, fb->tiles, *fb);
+    k_append_total<<<1, 256, 0, s>>>(fb->tiles, nt, fb->count);
+    LW_LAUNCHED("lw_frame_append");
+    return LW_OK;
+}
+
+int lw_frame_reset(lw_frame_buf* fb, void* stream) {
+    k_zero_count<<<1, 1, 0, (cudaStream_t)stream>>>(fb->count);
+    LW_LAUNCHED("lw_frame_reset");
+    return LW_OK;
+}
+
+
+int lw_deskew(const float* raw, float* out, const int32_t* m_dev, int64_t m_ub, double t_mid, double inv_dt,
+              const float* twist6_host, void* stream) {
+    if (!raw || !out || !m_dev || !twist6_host) return set_error(LW_EINVAL, "lw_deskew: null argument");
+    if (m_ub <= 0) return LW_OK;
+    lw_frame_buf fb{};
+    fb.f_raw = const_cast<float*>(raw);
+    fb.f_xyz = out;
+    fb.cap = m_ub;
+    ThinArgs a{};
+    a.deskew = 1;
+    a.t_mid = (float)t_mid;
+    a.inv_dt = (float)inv_dt;
+    Tw6 tw;
+    for (int k = 0; k < 6; ++k) tw.v[k] = twist6_host[k];
+    int grid = blocks_for(m_ub, 256, 8 * device_sms());
+    k_thin_a<<<grid, 256, 0, (cudaStream_t)stream>>>(fb, m_dev, a, nullptr, tw, nullptr, nullptr, 0);
+    LW_LAUNCHED("lw_deskew");
+    return LW_OK;
+}
+
+int lw_thin(lw_frame_buf* fb, const int32_t* m_dev, int64_t m_ub, double inv_v, double min_range, double max_range,
+            int32_t ret_mask, int32_t* n_ds_dev, void* stream) {
+    if (!fb || !m_dev || !n_ds_dev) return set_error(LW_EINVAL, "lw_thin: null argument");
+    if (m_ub > fb->cap) m_ub = fb->cap;
+    cudaStream_t s = (cudaStream_t)stream;
+    ThinArgs a{};
+    a.inv_v = (float)inv_v;
+    a.min_range = (float)min_range;
+    a.max_range = (float)max_range;
+    a.ret_mask = ret_mask;
+    a.deskew = 0;
+    Tw6 tw{};
+    int grid = blocks_for(m_ub, 256, 8 * device_sms());
+    int nt = blocks_for(m_ub, TILE);
+    k_thin_a<<<grid, 256, 0, s>>>(*fb, m_dev, a, nullptr, tw, nullptr, nullptr, 1);
+    k_thin_b<<<nt, TILE, 0, s>>>(*fb, m_dev, nullptr);
+    k_thin_c<<<nt, TILE, 0, s>>>(*fb, m_dev, n_ds_dev, nullptr);
+    LW_LAUNCHED("lw_thin");
+    return LW_OK;
+}
+
+static RegArgs reg_args(const double* T_host, double reg_voxel, double max_range, int ret_mask) {
+    RegArgs a;
+    for (int k = 0; k < 12; ++k) a.T[k] = T_host ? (float)T_host[k] : 0.0f;
+    a.inv_v = (float)(1.0 / reg_voxel);
+    a.voxel = (float)reg_voxel;
+    a.max_range = (float)max_range;
+    a.ret_mask = ret_mask;
+    return a;
+}
+
+static int reg_insert_launch(const float* xyz4, const uint32_t* attr, const int32_t* n_dev, int64_t n_ub,
+                             const double* T_host, const double* T_dev, double voxel, double max_range,
+                             int32_t ret_mask, lw_regmap* reg, const lw_rec_params* rp, int32_t* pslot,
+                             const int* gate, cudaStream_t s) {
+    RegArgs a = reg_args(T_host, voxel, max_range, ret_mask);
+    int grid = blocks_for(n_ub, 256, 8 * device_sms());
+    const float4* p4 = reinterpret_cast<const float4*>(xyz4);
+    k_reg_a<<<grid, 256, 0, s>>>(p4, attr, n_dev, n_ub, a, T_dev, *reg, pslot, gate);
+    k_reg_b<<<grid, 256, 0, s>>>(p4, n_dev, n_ub, a, T_dev, *reg, pslot, gate);
+    k_reg_d<<<grid, 256, 0, s>>>(n_dev, n_ub, *reg, pslot, *rp, gate);
+    LW_LAUNCHED("reg insert");
+    return LW_OK;
+}
+
+int lw_reg_insert(const float* xyz4, const uint32_t* attr, const int32_t* n_dev, int64_t n_ub, const double* T_host,
+                  double voxel, double max_range, int32_t ret_mask, lw_regmap* reg, const lw_rec_params* rp,
+                  int32_t* pslot, void* stream) {
+    if (!xyz4 || !attr || !reg || !rp || !pslot || !T_host) return set_error(LW_EINVAL, "lw_reg_insert: null argument");
+    if ((reg->cap & (reg->cap - 1)) != 0) return set_error(LW_EINVAL, "lw_reg_insert: capacity not a power of two");
+    if (n_ub <= 0) return LW_OK;
+    return reg_insert_launch(xyz4, attr, n_dev, n_ub, T_host, nullptr, voxel, max_range, ret_mask, reg, rp, pslot,
+                             nullptr, (cudaStream_t)stream);
+}
+
+int lw_reg_refresh_all(lw_regmap* reg, const lw_rec_params* rp, void* stream) {
+    if (!reg || !rp) return set_error(LW_EINVAL, "lw_reg_refresh_all: null argument");
+    k_reg_refresh_all<<<4 * device_sms(), 256, 0, (cudaStream_t)stream>>>(*reg, *rp);
+    LW_LAUNCHED("lw_reg_refresh_all");
+    return LW_OK;
+}
+
+int lw_icp_accumulate(const float* ds4, const int32_t* n_dev, int64_t n_ub, const double* T_host, const lw_regmap* reg,
+                      float voxel, int32_t reach, float max_d2, float kappa, lw_gn_scratch* gn, double* out64,
+                      void* stream) {
+    if (!ds4 || !T_host || !reg || !gn || !out64) return set_error(LW_EINVAL, "lw_icp_accumulate: null argument");
+    if (reach != 1 && reach != 2) return set_error(LW_EINVAL, "lw_icp_accumulate: reach must be 1 or 2");
+    cudaStream_t s = (cudaStream_t)stream;
+    int grid = gn_grid(gn);
+    IcpPose P;
+    double c[3] = {T_host[3], T_host[7], T_host[11]};
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) P.R[i * 3 + j] = (float)T_host[i * 4 + j];
+        P.tr[i] = (float)(T_host[i * 4 + 3] - c[i]);
+        P.c[i] = (float)c[i];
+    }
+    double cf[3] = {(double)P.c[0], (double)P.c[1], (double)P.c[2]};
+    IcpConsts k;
+    k.inv_v = (float)(1.0 / (double)voxel);
+    k.max_d2 = max_d2;
+    k.kappa2 = kappa * kappa;
+    k.reach = reach;
+    k.mask = (int)(reg->cap - 1);
+    k_acc_once<<<grid, GN_THREADS, 0, s>>>(reinterpret_cast<const float4*>(ds4), n_dev, n_ub, P, k, reg->keys,
+                                           reg->rec, gn->part);
+    k_acc_reduce<<<1, LW_ACC_STRIDE, 0, s>>>(gn->part, grid, cf[0], cf[1], cf[2], out64);
+    LW_LAUNCHED("lw_icp_accumulate");
+    return LW_OK;
+}
+
+int lw_icp_solve(const float* ds4, const int32_t* n_dev, const lw_odom_params* prm, lw_odom_state* st,
+                 const lw_regmap* reg, lw_gn_scratch* gn, void* stream) {
+    if (!ds4 || !n_dev || !prm || !st || !reg || !gn) return set_error(LW_EINVAL, "lw_icp_solve: null argument");
+    return launch_gn(ds4, n_dev, prm, st, reg, gn, 2, (cudaStream_t)stream);  // ungated
+}
+
+int lw_odom_finalize(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_odom_state* st, lw_frame_buf* fb,
+                     lw_regmap* reg, lw_gn_scratch* gn, lw_pose_table* pt, int32_t epoch, lw_traj_rec* traj,
+                     int64_t traj_cap, void* stream) {
+    if (!prm || !st || !fb || !reg || !gn || !pt) return set_error(LW_EINVAL, "lw_odom_finalize: null argument");
+    if ((reg->cap & (reg->cap - 1)) != 0 || (fb->ds_cap & (fb->ds_cap - 1)) != 0 || fb->ds_cap < fb->cap)
+        return set_error(LW_EINVAL, "lw_odom_finalize: table capacities must be powers of two (ds_cap >= cap)");
+    if (prm->frame_cap != fb->cap) return set_error(LW_EINVAL, "lw_odom_finalize: frame_cap != frame buffer capacity");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (m_ub > fb->cap) m_ub = fb->cap;
+    if (m_ub < 1) m_ub = 1;
+    const int sms = device_sms();
+    const int grid = blocks_for(m_ub, 256, 8 * sms);
+    const int nt = blocks_for(m_ub, TILE);
+    ThinArgs ta = thin_args(prm);
+    Tw6 tw{};
+    lw_rec_params rp = rec_params(prm);
+
+    k_ctl_begin<<<1, 1, 0, s>>>(k, *prm, st, fb->count);
+    // first registration: deskew with the predicted motion, thin, Gauss-Newton
+    k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, ta, st, tw, nullptr, &st->run_reg, 1);
+    k_thin_b<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->run_reg);
+    k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->run_reg);
+    int r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 0, s);
+    if (r != LW_OK) return r;
+    // re-deskew with the solved motion and register again when it moved enough
+    k_ctl_mid<<<1, 1, 0, s>>>(*prm, st);
+    k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, ta, st, tw, &st->redo, &st->redo, 1);
+    k_thin_b<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->redo);
+    k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->redo);
+    r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 1, s);
+    if (r != LW_OK) return r;
+    // keyframe, velocity, pose table, trajectory
+    k_ctl_end<<<1, 1, 0, s>>>(*prm, st, *pt, epoch, traj, traj_cap);
+    // keyframe insert with the frame's final pose (odom.py:719-727), through the state's float64 pose
+    RegArgs a = reg_args(nullptr, prm->reg_voxel, prm->max_range, prm->ret_mask);
+    const float4* p4 = reinterpret_cast<const float4*>(fb->f_xyz);
+    k_reg_a<<<grid, 256, 0, s>>>(p4, fb->f_attr, &st->m, m_ub, a, st->T, *reg, fb->ds_slot, &st->do_insert);
+    k_reg_b<<<grid, 256, 0, s>>>(p4, &st->m, m_ub, a, st->T, *reg, fb->ds_slot, &st->do_insert);
+    k_reg_d<<<grid, 256, 0, s>>>(&st->m, m_ub, *reg, fb->ds_slot, rp, &st->do_insert);
+    LW_LAUNCHED("lw_odom_finalize");
+    return LW_OK;
+}
+
+int lw_odom_predict_poses(int32_t k0, int32_t k1, int32_t current, const lw_odom_state* st, lw_pose_table* pt,
+                          int32_t epoch, void* stream) {
+    if (!st || !pt) return set_error(LW_EINVAL, "lw_odom_predict_poses: null argument");
+    if (k1 <= k0) return LW_OK;
+    int64_t n = (int64_t)k1 - k0;
+    if (n > LW_POSE_SLOTS) n = LW_POSE_SLOTS;
+    k_predict_poses<<<blocks_for(n, 256, 256), 256, 0, (cudaStream_t)stream>>>(k0, k1, current, st, *pt, epoch);
+    LW_LAUNCHED("lw_odom_predict_poses");
+    return LW_OK;
+}
+
+int lw_odom_reset(const double* T0_host, lw_odom_state* st, lw_regmap* reg, int32_t clear_map, void* stream) {
+    if (!T0_host || !st) return set_error(LW_EINVAL, "lw_odom_reset: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    lw_odom_state init;
+    memset(&init, 0, sizeof(init));
+    for (int i = 0; i < 16; ++i) {
+        init.T[i] = T0_host[i];
+        double e = (i % 5 == 0) ? 1.0 : 0.0;
+        init.delta[i] = e;
+        init.T_prev[i] = init.T_key[i] = init.T_pred[i] = init.T_reg[i] = e;
+    }
+    init.cond = 1.0;
+    k_reset_state<<<1, 1, 0, s>>>(st, init);
+    if (clear_map && reg) {
+        int g = 8 * device_sms();
+        k_fill_i64<<<g, 256, 0, s>>>(reg->keys, reg->cap, -1);
+        LW_CUDA(cudaMemsetAsync(reg->cnt, 0, reg->cap * sizeof(int32_t), s));
+        LW_CUDA(cudaMemsetAsync(reg->sum, 0, reg->cap * 3 * sizeof(int64_t), s));
+        LW_CUDA(cudaMemsetAsync(reg->outer, 0, reg->cap * 6 * sizeof(int64_t), s));
+        LW_CUDA(cudaMemsetAsync(reg->rec, 0, reg->cap * LW_REC_FLOATS * sizeof(float), s));
+        LW_CUDA(cudaMemsetAsync(reg->bcnt, 0, reg->cap * sizeof(int32_t), s));
+        k_fill_i32<<<g, 256, 0, s>>>(reg->first, reg->cap, NO_INDEX);
+        LW_CUDA(cudaMemsetAsync(reg->stats, 0, 2 * sizeof(int32_t), s));
+    }
+    LW_LAUNCHED("lw_odom_reset");
+    return LW_OK;
+}
+
+int lw_odom_restart_clock(lw_odom_state* st, void* stream) {
+    if (!st) return set_error(LW_EINVAL, "lw_odom_restart_clock: null argument");
+    k_restart_clock<<<1, 1, 0, (cudaStream_t)stream>>>(st);
+    LW_LAUNCHED("lw_odom_restart_clock");
+    return LW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,179 @@
+"""ctypes binding of liblivoxb200.so, the sm_100a C ABI declared in include/livox_b200.h.
+
+The structs below mirror the header field for field. Every call passes raw device pointers (torch CUDA tensors'
+data_ptr()) and the CUDA stream; a non-zero status raises LwError with the library's message. There is no CPU
+fallback: importing this module without the built library, or calling into it without a CUDA device, raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import torch
+
+LIB_PATH = Path(__file__).resolve().parent / "liblivoxb200.so"
+
+LW_OK, LW_EINVAL, LW_ECAPACITY, LW_ETIMEOUT, LW_ECUDA = 0, -1, -2, -3, -4
+FIX_R, FIX_RR, FIX_W = 2.0 ** 32, 2.0 ** 40, 2.0 ** 20
+REG_CAP = MAP_CAP = 4096
+ACC_STRIDE = 64
+REC_FLOATS = 20
+POSE_SLOTS = 1 << 16
+ACC_H, ACC_B, ACC_COUNT, ACC_ERR, ACC_RMS, ACC_WEIGHT, ACC_RANGE, ACC_HG = 0, 21, 27, 28, 29, 30, 31, 32
+INT32_MAX = 0x7FFFFFFF
+
+
+class LwError(RuntimeError):
+    """A status other than LW_OK from the CUDA library."""
+
+
+P = C.c_void_p
+i32, i64, f32, f64 = C.c_int32, C.c_int64, C.c_float, C.c_double
+
+
+class RegMap(C.Structure):
+    _fields_ = [("keys", P), ("cnt", P), ("sum", P), ("outer", P), ("rec", P), ("bcnt", P), ("first", P),
+                ("stats", P), ("cap", i64)]
+
+
+class RecParams(C.Structure):
+    _fields_ = [("voxel", f32), ("tight2", f32), ("noise2", f32), ("alpha", f32)]
+
+
+class OdomParams(C.Structure):
+    _fields_ = [(n, f64) for n in ("frame_dt", "reg_voxel", "min_range", "max_range", "noise", "alpha", "damping",
+                                    "velocity_smooth", "degen_thr", "prior_info", "kf_dist", "kf_angle_deg")] + \
+               [(n, i32) for n in ("max_iter", "warmup", "min_points", "min_corr", "ret_mask", "deskew", "redeskew",
+                                    "frame_cap")]
+
+
+class OdomState(C.Structure):
+    _fields_ = [("T", f64 * 16), ("T_prev", f64 * 16), ("T_key", f64 * 16), ("delta", f64 * 16), ("xi_s", f64 * 6),
+                ("T_pred", f64 * 16), ("T_reg", f64 * 16), ("t_mid", f64), ("rms", f64), ("cond", f64),
+                ("xi", f32 * 6), ("xi_used", f32 * 6)] + \
+               [(n, i32) for n in ("has_prev", "has_key", "map_frames", "frame_k", "m", "n_ds", "warm", "ok",
+                                    "run_reg", "do_insert", "redo", "err", "iters", "corr", "degen", "weak", "frames",
+                                    "skipped", "keyframes", "traj_len")]
+
+
+class TrajRec(C.Structure):
+    _fields_ = [("T", f64 * 16), ("t_mid", f64), ("k", i32), ("ok", i32), ("iters", i32), ("corr", i32)]
+
+
+class FrameBuf(C.Structure):
+    _fields_ = [("f_raw", P), ("f_xyz", P), ("f_attr", P), ("f_t", P), ("f_frame", P), ("count", P), ("ds_keys", P),
+                ("ds_win", P), ("ds_slot", P), ("tiles", P), ("ds_xyz", P), ("cap", i64), ("ds_cap", i64)]
+
+
+class GnScratch(C.Structure):
+    _fields_ = [("part", P), ("bar", P), ("err", P), ("grid", i32)]
+
+
+class PoseTable(C.Structure):
+    _fields_ = [("poses", P), ("tw", P), ("owner_frame", P), ("owner_epoch", P)]
+
+
+class Map(C.Structure):
+    _fields_ = [("keys", P), ("cnt", P), ("acc", P), ("last", P), ("first", P), ("miss", P), ("bcnt", P),
+                ("lead", P), ("stats", P), ("cap", i64)]
+
+
+class View(C.Structure):
+    """gpu.View (gpu.py:76-98): the filters and labels the map kernels read."""
+
+    _fields_ = [("now", f32), ("persist", f32), ("min_range", f32), ("max_range", f32), ("min_refl", i32),
+                ("noise_mask", i32), ("ret_mask", i32), ("crop_on", i32), ("crop_lo", f32 * 3), ("crop_hi", f32 * 3),
+                ("inv_frame_dt", f32), ("epoch", i32), ("inv_voxel", f32), ("map_mask", i32), ("dyn_on", i32),
+                ("dyn_settle", f32), ("carve_on", i32), ("carve_ratio", f32), ("carve_min", i32),
+                ("carve_stale", f32)]
+
+    def __setattr__(self, name, value):
+        if name in ("crop_lo", "crop_hi"):
+            value = (f32 * 3)(*[float(x) for x in value])
+        super().__setattr__(name, value)
+
+
+# (name, restype, argtypes) of every exported entry point
+_SIGS = {
+    "lw_version": (C.c_char_p, []),
+    "lw_last_error": (C.c_char_p, []),
+    "lw_device_sms": (i32, [C.POINTER(i32)]),
+    "lw_frame_append": (i32, [P, i32, P, P, i64, f64, i32, i32, C.POINTER(FrameBuf), P]),
+    "lw_frame_reset": (i32, [C.POINTER(FrameBuf), P]),
+    "lw_odom_finalize": (i32, [i32, i64, C.POINTER(OdomParams), P, C.POINTER(FrameBuf), C.POINTER(RegMap),
+                               C.POINTER(GnScratch), C.POINTER(PoseTable), i32, P, i64, P]),
+    "lw_odom_predict_poses": (i32, [i32, i32, i32, P, C.POINTER(PoseTable), i32, P]),
+    "lw_odom_reset": (i32, [C.POINTER(f64), P, C.POINTER(RegMap), i32, P]),
+    "lw_odom_restart_clock": (i32, [P, P]),
+    "lw_deskew": (i32, [P, P, P, i64, f64, f64, C.POINTER(f32), P]),
+    "lw_thin": (i32, [C.POINTER(FrameBuf), P, i64, f64, f64, f64, i32, P, P]),
+    "lw_reg_insert": (i32, [P, P, P, i64, C.POINTER(f64), f64, f64, i32, C.POINTER(RegMap), C.POINTER(RecParams),
+                              P, P]),
+    "lw_reg_refresh_all": (i32, [C.POINTER(RegMap), C.POINTER(RecParams), P]),
+    "lw_icp_accumulate": (i32, [P, P, i64, C.POINTER(f64), C.POINTER(RegMap), f32, i32, f32, f32,
+                                C.POINTER(GnScratch), P, P]),
+    "lw_icp_solve": (i32, [P, P, C.POINTER(OdomParams), P, C.POINTER(RegMap), C.POINTER(GnScratch), P]),
+    "lw_map_insert": (i32, [P, i32, P, P, P, P, i64, P, C.POINTER(View), f32, C.POINTER(Map), P, P]),
+    "lw_carve": (i32, [P, i32, P, P, P, i64, P, i32, f32, f32, i32, C.POINTER(Map), P]),
+    "lw_map_build": (i32, [C.POINTER(Map), C.POINTER(View), i32, P, P, P, P, P, P, P]),
+    "lw_map_clear": (i32, [C.POINTER(Map), P]),
+    "lw_frame_ids": (i32, [P, i64, f32, P, P]),
+}
+
+_lib = None
+
+
+def exported_names() -> list[str]:
+    return list(_SIGS)
+
+
+def load(require_cuda: bool = True) -> C.CDLL:
+    """Load the library (once). Raises if it is missing, or if require_cuda and no CUDA device is present."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python livox-warp_b200/csrc/build.py` "
+                          "(there is no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    if require_cuda and not torch.cuda.is_available():
+        raise RuntimeError("livox_warp needs a CUDA device (sm_100a); there is no CPU fallback")
+    return lib
+
+
+def check(status: int, what: str = ""):
+    if status != LW_OK:
+        msg = _lib.lw_last_error().decode(errors="replace") if _lib is not None else ""
+        raise LwError(f"{what or 'livox_warp'}: status {status}: {msg}")
+
+
+def call(name: str, *args):
+    lib = load()
+    check(getattr(lib, name)(*args), name)
+
+
+def ptr(t: torch.Tensor | None):
+    """Device pointer of a tensor (None -> NULL)."""
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def stream_ptr(stream=None) -> C.c_void_p:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def f64_array(values) -> C.Array:
+    vals = [float(v) for v in values]
+    return (f64 * len(vals))(*vals)
+
+
+def f32_array(values) -> C.Array:
+    vals = [float(v) for v in values]
+    return (f32 * len(vals))(*vals)

@@ -1,0 +1,381 @@
+"""Seeded synthetic LiDAR input: a Mid-40-like rosette traced into analytic scenes (the stand-in for the reference's
+Warp ray-casting simulator, python/livox_warp/sources.py, which cannot run without NVIDIA Warp).
+
+Scan pattern. The direction of the return fired at time t is a rose curve r = 0.5 * fov * sin(k * phi) with
+fov = 38.4 deg and k = 7/3, phi = ROSE_RATE * t advancing uniformly, and the whole curve turned by a precession
+angle psi = PRECESSION_RATE * t so that successive roses fill the field of view (the Mid-40's pattern is
+non-repetitive). The rose closes after phi = 3 pi; at ROSE_RATE one closed rose takes 10 ms, and the precession
+turns it by the golden angle per rose, so a 0.1 s frame holds ten rotated roses.
+
+Scenes are unions of axis-aligned solid boxes inside an axis-aligned room (an inside-out box), plus vertical
+cylinders that may move (walkers). A return is the first hit along the ray, with Gaussian range noise, a
+uniform reflectivity 0-255, noise tag 0 and return index 0 (1 for the second return of a dual-return scan).
+Sensor axes: x forward (the rosette's centre), y left, z up. Poses are sensor-to-world 4x4 matrices.
+Everything is numpy float64 with a seeded PCG64 generator; the returned points are float32.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+from scipy.spatial.transform import Rotation
+
+FOV_DEG = 38.4
+ROSE_K = 7.0 / 3.0
+ROSE_RATE = 3.0 * math.pi / 0.01          # rad/s of phi: one closed rose per 10 ms
+PRECESSION_RATE = 2.399963229728653 / 0.01  # the golden angle per rose
+
+
+def rosette_dirs(t: np.ndarray) -> np.ndarray:
+    """Unit ray directions (sensor frame) for firing times t (s)."""
+    t = np.asarray(t, dtype=np.float64)
+    phi = ROSE_RATE * t
+    psi = PRECESSION_RATE * t
+    r = 0.5 * math.radians(FOV_DEG) * np.sin(ROSE_K * phi)  # signed angular radius
+    ang = phi + psi
+    u, v = r * np.cos(ang), r * np.sin(ang)
+    rho = np.abs(r)
+    s = np.where(rho > 1e-12, np.sin(rho) / np.maximum(rho, 1e-12), 1.0)
+    d = np.stack([np.cos(rho), s * u, s * v], axis=1)
+    return d / np.linalg.norm(d, axis=1, keepdims=True)
+
+
+@dataclass
+class Cylinder:
+    """A vertical cylinder (a walker) whose axis moves back and forth along a segment at constant speed."""
+
+    p0: np.ndarray      # xy of one end of its path
+    p1: np.ndarray      # xy of the other end
+    speed: float        # m/s along the path
+    radius: float = 0.25
+    z0: float = 0.0
+    height: float = 1.8
+    phase: float = 0.0  # s
+
+    def centre(self, t: np.ndarray) -> np.ndarray:
+        L = float(np.linalg.norm(self.p1 - self.p0))
+        if L < 1e-9 or self.speed <= 0:
+            return np.broadcast_to(self.p0, (np.size(t), 2)).copy()
+        s = (np.asarray(t, dtype=np.float64) + self.phase) * self.speed
+        u = np.mod(s, 2 * L)
+        u = np.where(u > L, 2 * L - u, u) / L  # ping-pong
+        return self.p0[None, :] + u[:, None] * (self.p1 - self.p0)[None, :]
+
+
+@dataclass
+class Scene:
+    room_lo: np.ndarray
+    room_hi: np.ndarray
+    boxes: np.ndarray                   # (K, 6) x0, y0, z0, x1, y1, z1 (solid)
+    cylinders: list = field(default_factory=list)
+
+    def free(self, p: np.ndarray, margin: float) -> np.ndarray:
+        """Points at least `margin` from every box and inside the room by `margin`."""
+        p = np.atleast_2d(p)
+        ok = np.all((p > self.room_lo + margin) & (p < self.room_hi - margin), axis=1)
+        for b in self.boxes:
+            inside = np.all((p > b[:3] - margin) & (p < b[3:] + margin), axis=1)
+            ok &= ~inside
+        return ok
+
+
+def box_room(seed: int, size=(8.0, 6.0, 3.0), n_boxes: int = 20, side=(0.3, 1.5)) -> Scene:
+    """An 8 x 6 x 3 m room with n axis-aligned boxes of 0.3-1.5 m sides standing on the floor."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.zeros(3), np.asarray(size, dtype=np.float64)
+    boxes = []
+    for _ in range(n_boxes):
+        s = rng.uniform(side[0], side[1], 3)
+        c = rng.uniform(lo[:2] + 0.2, hi[:2] - 0.2)
+        b0 = np.array([c[0] - s[0] / 2, c[1] - s[1] / 2, 0.0])
+        boxes.append(np.concatenate([np.maximum(b0, lo), np.minimum(b0 + s, hi)]))
+    return Scene(lo, hi, np.array(boxes))
+
+
+def office(seed: int, size=(40.0, 30.0, 3.0), rooms=(4, 3), n_boxes: int = 200, walkers: int = 0,
+           walker_speed: float = 1.2) -> Scene:
+    """A multi-room office: outer walls, a grid of 0.1 m internal walls with 1 m door gaps, n boxes and walkers."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.zeros(3), np.asarray(size, dtype=np.float64)
+    H = hi[2]
+    walls = []
+    th = 0.1
+    nx, ny = rooms
+    for i in range(1, nx):  # walls of constant x, with one door per room they bound
+        x = hi[0] * i / nx
+        edges = np.linspace(0, hi[1], ny + 1)
+        for j in range(ny):
+            d = rng.uniform(edges[j] + 0.8, edges[j + 1] - 1.8)
+            walls.append([x - th / 2, edges[j], 0, x + th / 2, d, H])
+            walls.append([x - th / 2, d + 1.0, 0, x + th / 2, edges[j + 1], H])
+    for j in range(1, ny):
+        y = hi[1] * j / ny
+        edges = np.linspace(0, hi[0], nx + 1)
+        for i in range(nx):
+            d = rng.uniform(edges[i] + 0.8, edges[i + 1] - 1.8)
+            walls.append([edges[i], y - th / 2, 0, d, y + th / 2, H])
+            walls.append([d + 1.0, y - th / 2, 0, edges[i + 1], y + th / 2, H])
+    wall_scene = Scene(lo, hi, np.array(walls, dtype=np.float64))
+    boxes = list(walls)
+    placed, attempts = 0, 0
+    while placed < n_boxes:
+        attempts += 1
+        if attempts > 200000:
+            raise RuntimeError("could not place the office boxes")
+        s = rng.uniform(0.3, 1.5, 3)
+        c = rng.uniform(lo[:2] + 0.5, hi[:2] - 0.5)
+        b = np.array([c[0] - s[0] / 2, c[1] - s[1] / 2, 0.0, c[0] + s[0] / 2, c[1] + s[1] / 2, s[2]])
+        # keep the doors and a corridor along every wall free (boxes may touch each other)
+        mg = 0.7 + 0.5 * s[:2].max()
+        if np.any(c - mg < lo[:2]) or np.any(c + mg > hi[:2]):
+            continue
+        W = wall_scene.boxes
+        if np.any(np.all((c[None, :] > W[:, :2] - mg) & (c[None, :] < W[:, 3:5] + mg), axis=1)):
+            continue
+        boxes.append(b)
+        placed += 1
+    scene = Scene(lo, hi, np.array(boxes, dtype=np.float64))
+    for w in range(walkers):
+        for _ in range(20000):
+            a = rng.uniform(lo[:2] + 1.0, hi[:2] - 1.0)
+            ang = rng.uniform(0, 2 * math.pi)
+            b = a + 4.0 * np.array([math.cos(ang), math.sin(ang)])
+            seg = np.linspace(0, 1, 20)[:, None] * (b - a) + a
+            pts = np.concatenate([seg, np.full((20, 1), 0.9)], axis=1)
+            if scene.free(pts, margin=0.4).all():
+                scene.cylinders.append(Cylinder(a, b, walker_speed, phase=rng.uniform(0, 10)))
+                break
+    return scene
+
+
+# ---- ray casting -----------------------------------------------------------------------------------------
+
+
+def raycast(o: np.ndarray, d: np.ndarray, scene: Scene, t: np.ndarray, chunk: int = 8192) -> np.ndarray:
+    """Distance to the first surface along each ray (inf where none); o, d (n, 3), d unit; t firing times."""
+    n = len(o)
+    out = np.full(n, np.inf)
+    B = scene.boxes
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        oo, dd = o[a:b], d[a:b]
+        inv = 1.0 / np.where(np.abs(dd) < 1e-12, np.copysign(1e-12, dd), dd)
+        # the room from inside: the exit distance
+        t_room = np.min(np.where(dd > 0, (scene.room_hi - oo) * inv, (scene.room_lo - oo) * inv), axis=1)
+        best = t_room
+        if len(B):
+            t1 = (B[None, :, :3] - oo[:, None, :]) * inv[:, None, :]
+            t2 = (B[None, :, 3:] - oo[:, None, :]) * inv[:, None, :]
+            tn = np.max(np.minimum(t1, t2), axis=2)
+            tf = np.min(np.maximum(t1, t2), axis=2)
+            hit = (tn <= tf) & (tn > 1e-6)
+            tb = np.where(hit, tn, np.inf).min(axis=1)
+            best = np.minimum(best, tb)
+        for cyl in scene.cylinders:
+            c = cyl.centre(t[a:b])
+            ox, oy = oo[:, 0] - c[:, 0], oo[:, 1] - c[:, 1]
+            A = dd[:, 0] ** 2 + dd[:, 1] ** 2
+            Bq = 2 * (ox * dd[:, 0] + oy * dd[:, 1])
+            Cq = ox ** 2 + oy ** 2 - cyl.radius ** 2
+            disc = Bq ** 2 - 4 * A * Cq
+            ok = (disc >= 0) & (A > 1e-12)
+            sq = np.sqrt(np.maximum(disc, 0))
+            tc = (-Bq - sq) / np.maximum(2 * A, 1e-12)
+            z = oo[:, 2] + tc * dd[:, 2]
+            ok &= (tc > 1e-6) & (z >= cyl.z0) & (z <= cyl.z0 + cyl.height)
+            best = np.minimum(best, np.where(ok, tc, np.inf))
+        out[a:b] = best
+    return out
+
+
+# ---- trajectories -----------------------------------------------------------------------------------------
+
+
+def _pose(R: np.ndarray, p: np.ndarray) -> np.ndarray:
+    T = np.zeros(R.shape[:-2] + (4, 4))
+    T[..., :3, :3] = R
+    T[..., :3, 3] = p
+    T[..., 3, 3] = 1.0
+    return T
+
+
+class ConstantVelocity:
+    """At rest at T0 until t_start, then constant body velocity (v forward m/s, yaw rate rad/s)."""
+
+    def __init__(self, T0: np.ndarray, t_start: float, v: float, yaw_rate: float):
+        self.T0, self.t_start, self.v, self.w = np.asarray(T0, np.float64), t_start, v, yaw_rate
+
+    def poses(self, t: np.ndarray) -> np.ndarray:
+        s = np.maximum(np.asarray(t, np.float64) - self.t_start, 0.0)
+        yaw = self.w * s
+        # integrate a unicycle: forward speed v along the heading, heading turning at w
+        if abs(self.w) > 1e-12:
+            dx = self.v / self.w * np.sin(yaw)
+            dy = self.v / self.w * (1 - np.cos(yaw))
+        else:
+            dx, dy = self.v * s, np.zeros_like(s)
+        Rz = Rotation.from_euler("z", yaw[:, None]).as_matrix()
+        R0 = self.T0[:3, :3]
+        R = R0[None] @ Rz
+        p = self.T0[:3, 3][None, :] + (R0[None] @ np.stack([dx, dy, np.zeros_like(dx)], axis=1)[..., None])[..., 0]
+        return _pose(R, p)
+
+
+class Handheld:
+    """A smooth handheld path: rest for `rest` s, then a Catmull-Rom spline through random free waypoints,
+    timed so the speed stays under v_max, with yaw a smooth random function under w_max and small pitch/roll.
+    """
+
+    def __init__(self, scene: Scene, seed: int, duration: float, v_max: float = 1.0, w_max_deg: float = 60.0,
+                 rest: float = 1.0, height=(1.2, 1.7), margin: float = 0.7):
+        rng = np.random.default_rng(seed)
+        self.rest, self.duration = rest, duration
+        pts = []
+        while len(pts) < 2 or self._length(pts) < v_max * (duration - rest) * 0.8:
+            for _ in range(10000):
+                c = rng.uniform(scene.room_lo + margin, scene.room_hi - margin)
+                c[2] = rng.uniform(*height)
+                if scene.free(c, margin)[0] and (not pts or np.linalg.norm(c - pts[-1]) > 1.0):
+                    seg = np.linspace(0, 1, 25)[:, None] * (c - pts[-1]) + pts[-1] if pts else c[None]
+                    if scene.free(seg, margin * 0.8).all():
+                        pts.append(c)
+                        break
+            else:
+                raise RuntimeError("could not place a waypoint")
+            if len(pts) > 400:
+                break
+        P = np.array(pts)
+        P = np.vstack([P[0], P, P[-1]])  # clamp the spline ends
+        self.P = P
+        # sample the spline densely, arc-length parametrise, time at a speed profile under v_max
+        us = np.linspace(0, len(P) - 3, (len(P) - 3) * 200 + 1)
+        xyz = self._spline(us)
+        seglen = np.linalg.norm(np.diff(xyz, axis=0), axis=1)
+        s = np.concatenate([[0.0], np.cumsum(seglen)])
+        T_move = duration - rest
+        v = min(v_max * 0.95, s[-1] / max(T_move * 0.6, 1e-3))
+        ramp = 0.8  # s to reach cruise speed, so the first moving frames look like a hand starting to move
+        def s_of(tau):
+            tau = np.clip(tau, 0, None)
+            return np.where(tau < ramp, v * tau * tau / (2 * ramp), v * (tau - ramp / 2))
+        self._s, self._xyz, self._s_of = s, xyz, s_of
+        # yaw: sum of random sinusoids scaled to w_max
+        self.freqs = rng.uniform(0.05, 0.3, 4)
+        self.phases = rng.uniform(0, 2 * math.pi, 4)
+        amps = rng.uniform(0.5, 1.0, 4)
+        tt = np.linspace(0, duration, 4000)
+        w = sum(a * 2 * math.pi * f * np.cos(2 * math.pi * f * tt + ph)
+                for a, f, ph in zip(amps, self.freqs, self.phases))
+        self.amps = amps * (math.radians(w_max_deg) * 0.95 / max(np.abs(w).max(), 1e-9))
+        self.yaw0 = rng.uniform(0, 2 * math.pi)
+        self.tilt = rng.uniform(-1, 1, 4) * math.radians(4.0)
+
+    @staticmethod
+    def _length(pts):
+        return sum(np.linalg.norm(b - a) for a, b in zip(pts[:-1], pts[1:]))
+
+    def _spline(self, u):
+        P = self.P
+        i = np.clip(np.floor(u).astype(int), 0, len(P) - 4)
+        f = (u - i)[:, None]
+        p0, p1, p2, p3 = P[i], P[i + 1], P[i + 2], P[i + 3]
+        return 0.5 * ((2 * p1) + (-p0 + p2) * f + (2 * p0 - 5 * p1 + 4 * p2 - p3) * f ** 2 +
+                      (-p0 + 3 * p1 - 3 * p2 + p3) * f ** 3)
+
+    def poses(self, t: np.ndarray) -> np.ndarray:
+        t = np.asarray(t, np.float64)
+        tau = np.clip(t - self.rest, 0.0, None)
+        s = np.minimum(self._s_of(tau), self._s[-1])
+        idx = np.clip(np.searchsorted(self._s, s), 1, len(self._s) - 1)
+        f = ((s - self._s[idx - 1]) / np.maximum(self._s[idx] - self._s[idx - 1], 1e-12))[:, None]
+        p = self._xyz[idx - 1] * (1 - f) + self._xyz[idx] * f
+        tm = np.where(t > self.rest, t - self.rest, 0.0)
+        yaw = self.yaw0 + sum(a * (np.sin(2 * math.pi * fr * tm + ph) - math.sin(ph))
+                              for a, fr, ph in zip(self.amps, self.freqs, self.phases))
+        pitch = self.tilt[0] * np.sin(0.3 * tm) + self.tilt[1] * np.sin(0.17 * tm) * (tm > 0)
+        roll = self.tilt[2] * np.sin(0.23 * tm) + self.tilt[3] * np.sin(0.11 * tm) * (tm > 0)
+        R = Rotation.from_euler("zyx", np.stack([yaw, pitch, roll], axis=1)).as_matrix()
+        return _pose(R, p)
+
+
+# ---- scans ------------------------------------------------------------------------------------------------
+
+
+def scan(scene: Scene, traj, t0: float, t1: float, rate: float, seed: int, noise: float = 0.02,
+         dual: bool = False, max_range: float = 200.0):
+    """Returns fired at `rate` per second over [t0, t1): (xyz float32 (n,3) in each return's own sensor frame,
+    attr uint32, t float32). With dual, each ray gives two returns (index 0 and 1) with independent noise."""
+    i0 = int(math.ceil(t0 * rate - 1e-9))
+    i1 = int(math.ceil(t1 * rate - 1e-9))
+    idx = np.arange(i0, i1, dtype=np.int64)
+    t = idx / rate
+    d = rosette_dirs(t)
+    T = traj.poses(t)
+    o = T[:, :3, 3]
+    dw = (T[:, :3, :3] @ d[..., None])[..., 0]
+    rng = np.random.default_rng([seed, i0])
+    rng_hit = raycast(o, dw, scene, t)
+    ok = np.isfinite(rng_hit) & (rng_hit < max_range)
+    n_ret = 2 if dual else 1
+    xs, ats, ts = [], [], []
+    for r in range(n_ret):
+        rr = rng_hit + rng.normal(0.0, noise, len(t))
+        refl = rng.integers(0, 256, len(t)).astype(np.uint32)
+        xyz = d * rr[:, None]
+        attr = refl | (np.uint32(r) << np.uint32(16))
+        xs.append(xyz[ok])
+        ats.append(attr[ok])
+        ts.append(t[ok])
+    if dual:
+        # interleave the two returns of each ray, in firing order
+        xyz = np.stack(xs, axis=1).reshape(-1, 3)
+        attr = np.stack(ats, axis=1).reshape(-1)
+        tt = np.stack(ts, axis=1).reshape(-1)
+    else:
+        xyz, attr, tt = xs[0], ats[0], ts[0]
+    return xyz.astype(np.float32), attr.astype(np.uint32), tt.astype(np.float32)
+
+
+def frames(scene: Scene, traj, n_frames: int, rate: float, seed: int, frame_dt: float = 0.1, start: int = 0,
+           **kw):
+    """Per-frame scans [(xyz, attr, t)] of frames start .. start + n_frames - 1."""
+    return [scan(scene, traj, (start + k) * frame_dt, (start + k + 1) * frame_dt, rate, seed, **kw)
+            for k in range(n_frames)]
+
+
+def sample_surfaces(scene: Scene, spacing: float, seed: int, jitter: float = 0.0):
+    """Points on every visible face of the scene's room and boxes on a `spacing` grid, with unit normals and a
+    planarity of 1 (the prior map of a global-localisation case). Faces inside other boxes are kept."""
+    rng = np.random.default_rng(seed)
+    pts, nrm = [], []
+
+    def face(origin, u, v, n):
+        lu, lv = np.linalg.norm(u), np.linalg.norm(v)
+        nu, nv = max(int(lu / spacing), 1), max(int(lv / spacing), 1)
+        a, b = np.meshgrid((np.arange(nu) + 0.5) / nu, (np.arange(nv) + 0.5) / nv, indexing="ij")
+        p = origin + a.reshape(-1, 1) * u + b.reshape(-1, 1) * v
+        if jitter:
+            p = p + rng.normal(0, jitter, p.shape)
+        pts.append(p)
+        nrm.append(np.broadcast_to(n, p.shape))
+
+    lo, hi = scene.room_lo, scene.room_hi
+    ex, ey, ez = np.eye(3)
+    size = hi - lo
+    face(lo, ex * size[0], ey * size[1], ez)                         # floor
+    face(lo + ez * size[2], ex * size[0], ey * size[1], -ez)         # ceiling
+    face(lo, ex * size[0], ez * size[2], ey)                         # y = lo wall
+    face(lo + ey * size[1], ex * size[0], ez * size[2], -ey)
+    face(lo, ey * size[1], ez * size[2], ex)
+    face(lo + ex * size[0], ey * size[1], ez * size[2], -ex)
+    for b in scene.boxes:
+        b0, b1 = b[:3], b[3:]
+        s = b1 - b0
+        face(b0 + ez * s[2], ex * s[0], ey * s[1], ez)
+        face(b0, ex * s[0], ez * s[2], -ey)
+        face(b0 + ey * s[1], ex * s[0], ez * s[2], ey)
+        face(b0, ey * s[1], ez * s[2], -ex)
+        face(b0 + ex * s[0], ey * s[1], ez * s[2], ex)
+    return np.concatenate(pts).astype(np.float32), np.concatenate(nrm).astype(np.float32)

@@ -1,0 +1,620 @@
+// lw_oracle.cpp -- CPU restatement of the livox-warp per-frame hot path. TEST INFRASTRUCTURE ONLY: it is the
+// checker the GPU path is compared against (tests/, the smoke check and the CPU baseline of bench.py); no
+// product code links or calls it.
+//
+// It follows the reference's Warp kernels (python/livox_warp in nhaumann/livox-warp) as a serial program:
+//   keys / hash / probing      gpu.py:231-265          deskew              gpu.py:268-283, odom.py:163-178
+//   thinning                   odom.py:126-160         registration insert odom.py:186-230
+//   ICP accumulation           odom.py:233-375         integration insert  gpu.py:373-412
+//   carving + local_plane      gpu.py:415-593          map classification  gpu.py:286-299, 596-634, 699-747
+// The reference's nondeterministic choices are fixed the way the GPU build fixes them: the lowest point index
+// claims a thinning voxel, per-voxel sums are exact int64 fixed point (the units of include/livox_b200.h),
+// and 4096-point caps keep the first points in index order. Float expressions are written in the evaluation
+// order the GPU kernels use and compiled with -ffp-contract=off, so integer outputs match bit for bit.
+// Parity of this restatement against the reference itself is unpinned: the reference needs NVIDIA Warp,
+// which is not installed, and ships no golden vectors for these kernels.
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+#include <algorithm>
+#include <unordered_map>
+#include <vector>
+
+namespace {
+
+constexpr int64_t BIAS = 1LL << 20;
+constexpr int64_t KMASK = (1LL << 21) - 1;
+constexpr uint64_t MULT = 0x9E3779B97F4A7C15ULL;
+constexpr int PROBES = 64;
+constexpr double FIX_R = 4294967296.0, FIX_RR = 1099511627776.0, FIX_W = 1048576.0;
+constexpr int REG_CAP = 4096, MAP_CAP = 4096, REC = 20, POSE_SLOTS = 65536;
+
+inline int64_t key_ijk(int ix, int iy, int iz) {
+    int64_t x = ((int64_t)ix + BIAS) & KMASK, y = ((int64_t)iy + BIAS) & KMASK, z = ((int64_t)iz + BIAS) & KMASK;
+    return x | (y << 21) | (z << 42);
+}
+inline int slot_hash(int64_t k) {
+    int64_t h = (int64_t)((uint64_t)k * MULT);
+    h = h ^ (h >> 29);
+    return (int)(h & 0x7FFFFFFFLL);
+}
+inline int ifloor(float v) { return (int)floorf(v); }
+inline float len3(float x, float y, float z) { return sqrtf(x * x + y * y + z * z); }
+inline int refl_of(uint32_t a) { return (int)(a & 255u); }
+inline int tag_of(uint32_t a) { return (int)((a >> 8) & 255u); }
+inline int ret_of(uint32_t a) { return (int)((a >> 16) & 255u); }
+
+int find_slot(int64_t key, const int64_t* keys, int mask) {
+    int h = slot_hash(key) & mask;
+    for (int p = 0; p < PROBES; ++p) {
+        int s = (h + p) & mask;
+        if (keys[s] == key) return s;
+        if (keys[s] == -1) return -1;
+    }
+    return -1;
+}
+// serial claim: returns the slot and whether it was empty, -1 when the window is full
+int claim(int64_t key, int64_t* keys, int mask, bool* claimed) {
+    int h = slot_hash(key) & mask;
+    *claimed = false;
+    for (int p = 0; p < PROBES; ++p) {
+        int s = (h + p) & mask;
+        if (keys[s] == key) return s;
+        if (keys[s] == -1) {
+            keys[s] = key;
+            *claimed = true;
+            return s;
+        }
+    }
+    return -1;
+}
+
+// Cyclic Jacobi for a symmetric N x N matrix (Golub & Van Loan Alg. 8.5.2 / 8.5.1), the same sweep order and
+// stopping rule as the device solver so the two agree bit for bit.
+template <int N>
+void jacobi(double* A, double* ev, double* V) {
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) V[i * N + j] = (i == j) ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 24; ++sweep) {
+        double off = 0.0, tot = 0.0;
+        for (int i = 0; i < N; ++i)
+            for (int j = 0; j < N; ++j) {
+                double a2 = A[i * N + j] * A[i * N + j];
+                tot += a2;
+                if (i != j) off += a2;
+            }
+        if (off <= 1e-30 * tot || off == 0.0) break;
+        for (int p = 0; p < N - 1; ++p)
+            for (int q = p + 1; q < N; ++q) {
+                double apq = A[p * N + q];
+                if (apq == 0.0) continue;
+                double tau = (A[q * N + q] - A[p * N + p]) / (2.0 * apq);
+                double t = (tau >= 0.0) ? 1.0 / (tau + sqrt(1.0 + tau * tau)) : -1.0 / (-tau + sqrt(1.0 + tau * tau));
+                double c = 1.0 / sqrt(1.0 + t * t), s = t * c;
+                for (int k = 0; k < N; ++k) {
+                    double akp = A[k * N + p], akq = A[k * N + q];
+                    A[k * N + p] = c * akp - s * akq;
+                    A[k * N + q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < N; ++k) {
+                    double apk = A[p * N + k], aqk = A[q * N + k];
+                    A[p * N + k] = c * apk - s * aqk;
+                    A[q * N + k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < N; ++k) {
+                    double vkp = V[k * N + p], vkq = V[k * N + q];
+                    V[k * N + p] = c * vkp - s * vkq;
+                    V[k * N + q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    for (int i = 0; i < N; ++i) ev[i] = A[i * N + i];
+}
+
+inline void xform(const float* T, float x, float y, float z, float& ox, float& oy, float& oz) {
+    ox = T[0] * x + T[1] * y + T[2] * z + T[3];
+    oy = T[4] * x + T[5] * y + T[6] * z + T[7];
+    oz = T[8] * x + T[9] * y + T[10] * z + T[11];
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- primitives -----------------------------------------------------------------------------------------
+int64_t or_key_ijk(int ix, int iy, int iz) { return key_ijk(ix, iy, iz); }
+int or_slot_hash(int64_t k) { return slot_hash(k); }
+
+void or_voxel_keys(const float* xyz, int64_t n, float inv, int64_t* out) {
+    for (int64_t i = 0; i < n; ++i)
+        out[i] = key_ijk(ifloor(xyz[3 * i] * inv), ifloor(xyz[3 * i + 1] * inv), ifloor(xyz[3 * i + 2] * inv));
+}
+
+// ---- deskew (odom.py:163-178, gpu.py:268-283); raw/out are [m*4] (x, y, z, t) -----------------------------
+void or_deskew(const float* raw, int64_t m, float t_mid, float inv_dt, const float* tw, float* out) {
+    for (int64_t i = 0; i < m; ++i) {
+        const float* p = raw + 4 * i;
+        float s = fminf(fmaxf((p[3] - t_mid) * inv_dt, -1.0f), 1.0f);
+        float rx = tw[3] * s, ry = tw[4] * s, rz = tw[5] * s;
+        float a = len3(rx, ry, rz);
+        float ox = p[0], oy = p[1], oz = p[2];
+        if (!(a < 1.0e-9f)) {
+            double ad = a;
+            double ux = rx / ad, uy = ry / ad, uz = rz / ad;
+            double sh = sin(0.5 * ad), w = cos(0.5 * ad);
+            double vx = ux * sh, vy = uy * sh, vz = uz * sh;
+            double px = p[0], py = p[1], pz = p[2];
+            double tx = 2.0 * (vy * pz - vz * py), ty = 2.0 * (vz * px - vx * pz), tz = 2.0 * (vx * py - vy * px);
+            ox = (float)(px + w * tx + (vy * tz - vz * ty));
+            oy = (float)(py + w * ty + (vz * tx - vx * tz));
+            oz = (float)(pz + w * tz + (vx * ty - vy * tx));
+        }
+        out[4 * i + 0] = ox + tw[0] * s;
+        out[4 * i + 1] = oy + tw[1] * s;
+        out[4 * i + 2] = oz + tw[2] * s;
+        out[4 * i + 3] = p[3];
+    }
+}
+
+// ---- thinning (odom.py:126-160): the first point (in index order) of each half-voxel; out [*4] x,y,z,range --
+int64_t or_thin(const float* xyz4, const uint32_t* attr, int64_t m, float inv_v, float min_range, float max_range,
+                int ret_mask, float* out4) {
+    std::unordered_map<int64_t, char> seen;
+    seen.reserve((size_t)m * 2);
+    int64_t k = 0;
+    for (int64_t i = 0; i < m; ++i) {
+        const float* p = xyz4 + 4 * i;
+        float r = len3(p[0], p[1], p[2]);
+        if (r < min_range || r > max_range) continue;
+        if (tag_of(attr[i]) != 0 || ((1 << ret_of(attr[i])) & ret_mask) == 0) continue;
+        int64_t key = key_ijk(ifloor(p[0] * inv_v), ifloor(p[1] * inv_v), ifloor(p[2] * inv_v));
+        if (!seen.emplace(key, 1).second) continue;
+        out4[4 * k + 0] = p[0];
+        out4[4 * k + 1] = p[1];
+        out4[4 * k + 2] = p[2];
+        out4[4 * k + 3] = r;
+        ++k;
+    }
+    return k;
+}
+
+// ---- registration map (odom.py:186-230): serial insert in point order ----------------------------------
+// T is a float row-major 3x4. Tables: keys [cap], cnt [cap], sum [cap*3], outer [cap*6], stats [2].
+void or_reg_insert(const float* xyz4, const uint32_t* attr, int64_t n, const float* T, float inv_v, float voxel,
+                   float max_range, int ret_mask, int64_t cap, int64_t* keys, int32_t* cnt, int64_t* sum,
+                   int64_t* outer, int32_t* stats) {
+    const int mask = (int)(cap - 1);
+    for (int64_t i = 0; i < n; ++i) {
+        const float* p = xyz4 + 4 * i;
+        if (len3(p[0], p[1], p[2]) > max_range || tag_of(attr[i]) != 0 || ((1 << ret_of(attr[i])) & ret_mask) == 0)
+            continue;
+        float wx, wy, wz;
+        xform(T, p[0], p[1], p[2], wx, wy, wz);
+        int ix = ifloor(wx * inv_v), iy = ifloor(wy * inv_v), iz = ifloor(wz * inv_v);
+        float rx = wx - ((float)ix + 0.5f) * voxel, ry = wy - ((float)iy + 0.5f) * voxel, rz = wz - ((float)iz + 0.5f) * voxel;
+        bool claimed;
+        int s = claim(key_ijk(ix, iy, iz), keys, mask, &claimed);
+        if (claimed) stats[0] += 1;
+        if (s < 0) {
+            stats[1] += 1;
+            continue;
+        }
+        if (cnt[s] < REG_CAP) {
+            const float FR = (float)FIX_R, FRR = (float)FIX_RR;
+            sum[3 * s + 0] += llrintf(rx * FR);
+            sum[3 * s + 1] += llrintf(ry * FR);
+            sum[3 * s + 2] += llrintf(rz * FR);
+            outer[6 * s + 0] += llrintf(rx * rx * FRR);
+            outer[6 * s + 1] += llrintf(rx * ry * FRR);
+            outer[6 * s + 2] += llrintf(rx * rz * FRR);
+            outer[6 * s + 3] += llrintf(ry * ry * FRR);
+            outer[6 * s + 4] += llrintf(ry * rz * FRR);
+            outer[6 * s + 5] += llrintf(rz * rz * FRR);
+            cnt[s] += 1;
+        }
+    }
+}
+
+// The per-voxel record the ICP reads: mean, precision M, surface-normal precision Mg, rms direction
+// (odom.py:325-368, evaluated in float64 from the exact sums). rec [cap*20].
+void or_reg_records(int64_t cap, const int64_t* keys, const int32_t* cnt, const int64_t* sum, const int64_t* outer,
+                    float voxel, float tight2f, float noise2f, float alphaf, float* rec) {
+    for (int64_t s = 0; s < cap; ++s) {
+        float* out = rec + s * REC;
+        int c = cnt[s];
+        if (keys[s] == -1 || c <= 0) {
+            for (int k = 0; k < REC; ++k) out[k] = 0.0f;
+            continue;
+        }
+        int64_t key = keys[s];
+        int ix = (int)(key & KMASK) - (int)BIAS, iy = (int)((key >> 21) & KMASK) - (int)BIAS,
+            iz = (int)((key >> 42) & KMASK) - (int)BIAS;
+        double cf = c, mr[3], C[9];
+        for (int k = 0; k < 3; ++k) mr[k] = (double)sum[3 * s + k] / (cf * FIX_R);
+        const int up[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) C[i * 3 + j] = (double)outer[6 * s + up[i * 3 + j]] / (cf * FIX_RR) - mr[i] * mr[j];
+        double vox = voxel;
+        out[0] = (float)(((double)ix + 0.5) * vox + mr[0]);
+        out[1] = (float)(((double)iy + 0.5) * vox + mr[1]);
+        out[2] = (float)(((double)iz + 0.5) * vox + mr[2]);
+        out[3] = (float)c;
+        double ev[3], Q[9];
+        jacobi<3>(C, ev, Q);
+        double tight2 = tight2f, noise2 = noise2f, alpha = alphaf;
+        int nt = 0;
+        for (int k = 0; k < 3; ++k) nt += ev[k] < tight2 ? 1 : 0;
+        double M[6] = {0, 0, 0, 0, 0, 0}, Mg[6] = {0, 0, 0, 0, 0, 0}, q[3] = {0, 0, 0};
+        float surf = 0.0f;
+        if (c >= 5 && nt <= 1) {
+            int kmin = 0;
+            if (ev[1] < ev[kmin]) kmin = 1;
+            if (ev[2] < ev[kmin]) kmin = 2;
+            for (int k = 0; k < 3; ++k) {
+                double qa[3] = {Q[k], Q[3 + k], Q[6 + k]};
+                double e = fmax(ev[k], 0.0) + noise2, wa = 1.0 / e;
+                bool tight = !(ev[k] >= tight2);
+                if (!tight) wa = alpha / e;
+                double o6[6] = {qa[0] * qa[0], qa[0] * qa[1], qa[0] * qa[2], qa[1] * qa[1], qa[1] * qa[2], qa[2] * qa[2]};
+                for (int j = 0; j < 6; ++j) {
+                    M[j] += wa * o6[j];
+                    if (tight) Mg[j] += wa * o6[j];
+                }
+                if (k == kmin) {
+                    q[0] = qa[0];
+                    q[1] = qa[1];
+                    q[2] = qa[2];
+                }
+            }
+            surf = 1.0f;
+        } else {
+            double wa = alpha / (0.25 * vox * vox + noise2);
+            M[0] = M[3] = M[5] = wa;
+        }
+        for (int j = 0; j < 6; ++j) {
+            out[4 + j] = (float)M[j];
+            out[10 + j] = (float)Mg[j];
+        }
+        out[16] = (float)q[0];
+        out[17] = (float)q[1];
+        out[18] = (float)q[2];
+        out[19] = surf;
+    }
+}
+
+// ---- one Gauss-Newton accumulation (odom.py:233-375, k_reduce :378-384) in float64 --------------------
+// T64 row-major 4x4 (float64). The correspondence search follows the reference: closest voxel mean among the
+// (2 reach + 1)^3 voxels, first strictly smaller distance in (dx, dy, dz) order, within max_d2. out[64].
+// Points are split over `threads` OpenMP threads in contiguous ranges; partial sums are added in thread order.
+void or_icp_accumulate(const float* ds4, int64_t n, const double* T64, int64_t cap, const int64_t* keys,
+                       const float* rec, double inv_v, int reach, double max_d2, double kappa, int threads,
+                       double* out) {
+    const int mask = (int)(cap - 1);
+    if (threads < 1) threads = 1;
+    std::vector<double> part((size_t)threads * 64, 0.0);
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (int th = 0; th < threads; ++th) {
+        double* a = part.data() + (size_t)th * 64;
+        int64_t lo = n * th / threads, hi = n * (th + 1) / threads;
+        for (int64_t i = lo; i < hi; ++i) {
+            const float* p = ds4 + 4 * i;
+            double px = p[0], py = p[1], pz = p[2];
+            double w[3];
+            for (int r = 0; r < 3; ++r) w[r] = T64[r * 4 + 0] * px + T64[r * 4 + 1] * py + T64[r * 4 + 2] * pz + T64[r * 4 + 3];
+            int bx = (int)floor(w[0] * inv_v), by = (int)floor(w[1] * inv_v), bz = (int)floor(w[2] * inv_v);
+            double best_d2 = max_d2;
+            int best_s = -1;
+            for (int dx = -reach; dx <= reach; ++dx)
+                for (int dy = -reach; dy <= reach; ++dy)
+                    for (int dz = -reach; dz <= reach; ++dz) {
+                        int s = find_slot(key_ijk(bx + dx, by + dy, bz + dz), keys, mask);
+                        if (s < 0) continue;
+                        const float* rr = rec + (int64_t)s * REC;
+                        if (!(rr[3] > 0.0f)) continue;
+                        double ex = w[0] - rr[0], ey = w[1] - rr[1], ez = w[2] - rr[2];
+                        double d2 = ex * ex + ey * ey + ez * ez;
+                        if (d2 < best_d2) {
+                            best_d2 = d2;
+                            best_s = s;
+                        }
+                    }
+            if (best_s < 0) continue;
+            const float* rr = rec + (int64_t)best_s * REC;
+            double r[3] = {w[0] - rr[0], w[1] - rr[1], w[2] - rr[2]};
+            const int up[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+            double M[9], G[9];
+            for (int k = 0; k < 9; ++k) {
+                M[k] = rr[4 + up[k]];
+                G[k] = rr[10 + up[k]];
+            }
+            double Mr[3];
+            for (int k = 0; k < 3; ++k) Mr[k] = M[k * 3] * r[0] + M[k * 3 + 1] * r[1] + M[k * 3 + 2] * r[2];
+            double d2 = r[0] * Mr[0] + r[1] * Mr[1] + r[2] * Mr[2];
+            double wgt = 1.0 / (1.0 + d2 / (kappa * kappa));
+            wgt = wgt * wgt;
+            double rn = rr[19] > 0.5f ? r[0] * rr[16] + r[1] * rr[17] + r[2] * rr[18] : sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+            double J[3][6] = {{1, 0, 0, 0, w[2], -w[1]}, {0, 1, 0, -w[2], 0, w[0]}, {0, 0, 1, w[1], -w[0], 0}};
+            int idx = 0;
+            for (int pp = 0; pp < 6; ++pp)
+                for (int qq = pp; qq < 6; ++qq) {
+                    double v = 0.0, vg = 0.0;
+                    for (int aa = 0; aa < 3; ++aa)
+                        for (int bb = 0; bb < 3; ++bb) {
+                            v += M[aa * 3 + bb] * J[aa][pp] * J[bb][qq];
+                            vg += G[aa * 3 + bb] * J[aa][pp] * J[bb][qq];
+                        }
+                    a[0 + idx] += wgt * v;
+                    a[32 + idx] += wgt * vg;
+                    ++idx;
+                }
+            for (int pp = 0; pp < 6; ++pp) a[21 + pp] += wgt * (Mr[0] * J[0][pp] + Mr[1] * J[1][pp] + Mr[2] * J[2][pp]);
+            a[27] += 1.0;
+            a[28] += wgt * d2;
+            a[29] += wgt * rn * rn;
+            a[30] += wgt;
+            a[31] += p[3];
+        }
+    }
+    for (int k = 0; k < 64; ++k) out[k] = 0.0;
+    for (int th = 0; th < threads; ++th)
+        for (int k = 0; k < 64; ++k) out[k] += part[(size_t)th * 64 + k];
+}
+
+// ---- integration map (gpu.py:155-167 keep_raw, :373-412) -----------------------------------------------
+struct View {
+    float now, persist, min_range, max_range;
+    int32_t min_refl, noise_mask, ret_mask, crop_on;
+    float crop_lo[3], crop_hi[3];
+    float inv_frame_dt;
+    int32_t epoch;
+    float inv_voxel;
+    int32_t map_mask, dyn_on;
+    float dyn_settle;
+    int32_t carve_on;
+    float carve_ratio;
+    int32_t carve_min;
+    float carve_stale;
+};
+
+static bool keep_raw(float x, float y, float z, uint32_t a, const View& v) {
+    float r = len3(x, y, z);
+    if (r < v.min_range || r > v.max_range) return false;
+    if (refl_of(a) < v.min_refl) return false;
+    if (((v.noise_mask >> (tag_of(a) & 3)) & 1) == 0) return false;
+    if (((v.ret_mask >> (ret_of(a) & 3)) & 1) == 0) return false;
+    return true;
+}
+
+// xyz [n*stride]; poses [65536*16] float; map arrays as lw_map.
+void or_map_insert(const float* xyz, int stride, const uint32_t* attr, const float* t, const int32_t* frame, int64_t n,
+                   const float* poses, const View* v, float inv_voxel, int64_t cap, int64_t* keys, int32_t* cnt,
+                   int64_t* acc, float* last, float* first, int32_t* stats) {
+    const int mask = (int)(cap - 1);
+    for (int64_t i = 0; i < n; ++i) {
+        float x = xyz[i * stride], y = xyz[i * stride + 1], z = xyz[i * stride + 2];
+        if (!keep_raw(x, y, z, attr[i], *v)) continue;
+        const float* T = poses + (int64_t)(frame[i] & (POSE_SLOTS - 1)) * 16;
+        float wx, wy, wz;
+        xform(T, x, y, z, wx, wy, wz);
+        bool claimed;
+        int s = claim(key_ijk(ifloor(wx * inv_voxel), ifloor(wy * inv_voxel), ifloor(wz * inv_voxel)), keys, mask, &claimed);
+        if (claimed) stats[0] += 1;
+        if (s < 0) {
+            stats[1] += 1;
+            continue;
+        }
+        int old = cnt[s]++;
+        if (old < MAP_CAP) {
+            const float FW = (float)FIX_W;
+            acc[4 * s + 0] += llrintf(wx * FW);
+            acc[4 * s + 1] += llrintf(wy * FW);
+            acc[4 * s + 2] += llrintf(wz * FW);
+            acc[4 * s + 3] += refl_of(attr[i]);
+        }
+        last[s] = std::max(last[s], t[i]);
+        first[s] = std::min(first[s], t[i]);
+    }
+}
+
+// ---- carving (gpu.py:415-593) -------------------------------------------------------------------------
+struct MapView {
+    const int64_t* keys;
+    const int32_t* cnt;
+    const int64_t* acc;
+    int mask;
+};
+
+static void centroid(const MapView& m, int s, float& x, float& y, float& z) {
+    int c = m.cnt[s];
+    double n = (double)(c < MAP_CAP ? c : MAP_CAP) * FIX_W;
+    x = (float)((double)m.acc[4 * (int64_t)s + 0] / n);
+    y = (float)((double)m.acc[4 * (int64_t)s + 1] / n);
+    z = (float)((double)m.acc[4 * (int64_t)s + 2] / n);
+}
+
+static void local_plane(int ix, int iy, int iz, float ox, float oy, float oz, const MapView& m, float out[4]) {
+    double cs[3] = {0, 0, 0}, cc[6] = {0, 0, 0, 0, 0, 0};
+    int cn = 0;
+    for (int gx = -1; gx <= 1; ++gx)
+        for (int gy = -1; gy <= 1; ++gy)
+            for (int gz = -1; gz <= 1; ++gz) {
+                int sn = find_slot(key_ijk(ix + gx, iy + gy, iz + gz), m.keys, m.mask);
+                if (sn < 0 || m.cnt[sn] <= 0) continue;
+                float cx, cy, cz;
+                centroid(m, sn, cx, cy, cz);
+                double qx = (double)(cx - ox), qy = (double)(cy - oy), qz = (double)(cz - oz);
+                cs[0] += qx;
+                cs[1] += qy;
+                cs[2] += qz;
+                cc[0] += qx * qx;
+                cc[1] += qx * qy;
+                cc[2] += qx * qz;
+                cc[3] += qy * qy;
+                cc[4] += qy * qz;
+                cc[5] += qz * qz;
+                ++cn;
+            }
+    if (cn < 4) {
+        out[0] = 0.0f;
+        out[1] = 0.0f;
+        out[2] = 1.0f;
+        out[3] = 0.0f;
+        return;
+    }
+    double inv = 1.0 / (double)cn;
+    double mu[3] = {cs[0] * inv, cs[1] * inv, cs[2] * inv}, C[9];
+    const int up[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C[i * 3 + j] = cc[up[i * 3 + j]] * inv - mu[i] * mu[j];
+    double ev[3], Q[9];
+    jacobi<3>(C, ev, Q);
+    int k = 0;
+    if (ev[1] < ev[k]) k = 1;
+    if (ev[2] < ev[k]) k = 2;
+    int j = (k + 1) % 3, j2 = (k + 2) % 3;
+    double mid = fmin(ev[j], ev[j2]);
+    out[0] = (float)Q[k];
+    out[1] = (float)Q[3 + k];
+    out[2] = (float)Q[6 + k];
+    out[3] = ev[k] < 0.25 * mid ? 2.0f : 1.0f;
+}
+
+void or_carve(const float* xyz, int stride, const uint32_t* attr, const int32_t* frame, int64_t n, const float* poses,
+              int every, float inv_voxel, float max_range, int max_steps, int64_t cap, const int64_t* keys,
+              const int32_t* cnt, const int64_t* acc, int32_t* miss, int threads) {
+    MapView m{keys, cnt, acc, (int)(cap - 1)};
+    if (every < 1) every = 1;
+    const int64_t nrays = (n + every - 1) / every;
+    if (threads < 1) threads = 1;
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 256)
+    for (int64_t ray = 0; ray < nrays; ++ray) {
+        int64_t i = ray * every;
+        if (tag_of(attr[i]) != 0) continue;
+        const float* T = poses + (int64_t)(frame[i] & (POSE_SLOTS - 1)) * 16;
+        float ox = T[3], oy = T[7], oz = T[11];
+        float wx, wy, wz;
+        xform(T, xyz[i * stride], xyz[i * stride + 1], xyz[i * stride + 2], wx, wy, wz);
+        float dx = wx - ox, dy = wy - oy, dz = wz - oz;
+        float L = len3(dx, dy, dz);
+        if (L < 0.05f || L > max_range) continue;
+        dx = dx / L;
+        dy = dy / L;
+        dz = dz / L;
+        float voxel = 1.0f / inv_voxel;
+        float margin = fmaxf(3.0f * voxel, 0.03f * L);
+        float pe[4];
+        local_plane(ifloor(wx * inv_voxel), ifloor(wy * inv_voxel), ifloor(wz * inv_voxel), wx, wy, wz, m, pe);
+        if (pe[3] > 0.5f) {
+            float cosine = fabsf(pe[0] * dx + pe[1] * dy + pe[2] * dz);
+            margin = fmaxf(margin, 1.5f * voxel / fmaxf(cosine, 0.05f));
+        }
+        float stop = (L - margin) * inv_voxel;
+        if (stop <= 1.0f) continue;
+        float posx = ox * inv_voxel, posy = oy * inv_voxel, posz = oz * inv_voxel;
+        int ix = ifloor(posx), iy = ifloor(posy), iz = ifloor(posz);
+        int sx = 1, sy = 1, sz = 1;
+        float tmx = 1.0e30f, tmy = 1.0e30f, tmz = 1.0e30f, tdx = 1.0e30f, tdy = 1.0e30f, tdz = 1.0e30f;
+        if (dx > 1.0e-9f) { tmx = ((float)(ix + 1) - posx) / dx; tdx = 1.0f / dx; }
+        else if (dx < -1.0e-9f) { sx = -1; tmx = (posx - (float)ix) / (-dx); tdx = -1.0f / dx; }
+        if (dy > 1.0e-9f) { tmy = ((float)(iy + 1) - posy) / dy; tdy = 1.0f / dy; }
+        else if (dy < -1.0e-9f) { sy = -1; tmy = (posy - (float)iy) / (-dy); tdy = -1.0f / dy; }
+        if (dz > 1.0e-9f) { tmz = ((float)(iz + 1) - posz) / dz; tdz = 1.0f / dz; }
+        else if (dz < -1.0e-9f) { sz = -1; tmz = (posz - (float)iz) / (-dz); tdz = -1.0f / dz; }
+        for (int step = 0; step < max_steps; ++step) {
+            float tt;
+            if (tmx < tmy && tmx < tmz) { tt = tmx; ix += sx; tmx += tdx; }
+            else if (tmy < tmz) { tt = tmy; iy += sy; tmy += tdy; }
+            else { tt = tmz; iz += sz; tmz += tdz; }
+            if (tt >= stop) break;
+            int s = find_slot(key_ijk(ix, iy, iz), keys, m.mask);
+            if (s < 0 || cnt[s] <= 0) continue;
+            float cx, cy, cz;
+            centroid(m, s, cx, cy, cz);
+            float rx = cx - ox, ry = cy - oy, rz = cz - oz;
+            bool pierced = false;
+            float pl[4];
+            local_plane(ix, iy, iz, cx, cy, cz, m, pl);
+            if (pl[3] > 1.5f) {
+                float dn = dx * pl[0] + dy * pl[1] + dz * pl[2];
+                if (fabsf(dn) > 1.0e-4f) {
+                    float f = (rx * pl[0] + ry * pl[1] + rz * pl[2]) / dn;
+                    float xx = dx * f - rx, xy = dy * f - ry, xz = dz * f - rz;
+                    if (len3(xx, xy, xz) < 0.6f * voxel) pierced = true;
+                }
+            } else {
+                float g = rx * dx + ry * dy + rz * dz;
+                float qx = rx - g * dx, qy = ry - g * dy, qz = rz - g * dz;
+                if (len3(qx, qy, qz) < 0.5f * voxel) pierced = true;
+            }
+            if (pierced) {
+#pragma omp atomic
+                miss[s] += every;
+            }
+        }
+    }
+}
+
+// ---- visible set of the map (gpu.py:286-299, 596-634, 699-747), in slot order ---------------------------
+static int transient(int c, int miss, const View& v) {
+    if (miss < v.carve_min) return 0;
+    return (float)miss > v.carve_ratio * (float)c ? 1 : 0;
+}
+
+int64_t or_map_build(int64_t cap, const int64_t* keys, const int32_t* cnt, const int64_t* acc, const float* last,
+                     const float* first, const int32_t* miss, const View* vp, int min_count, float* out_xyz,
+                     uint32_t* out_attr, float* out_t, int32_t* out_dyn) {
+    const View& v = *vp;
+    MapView m{keys, cnt, acc, (int)(cap - 1)};
+    int64_t k = 0;
+    for (int64_t s = 0; s < cap; ++s) {
+        if (keys[s] == -1) continue;
+        int c = cnt[s];
+        if (c < min_count) continue;
+        if (v.persist > 0.0f && v.now - last[s] > v.persist) continue;
+        int gh = (v.now - last[s] < v.carve_stale) ? 0 : transient(c, miss[s], v);
+        if (v.carve_on != 0 && gh != 0) continue;
+        if (c <= 0) continue;
+        float wx, wy, wz;
+        centroid(m, (int)s, wx, wy, wz);
+        if (v.crop_on != 0) {
+            if (wx < v.crop_lo[0] || wy < v.crop_lo[1] || wz < v.crop_lo[2]) continue;
+            if (wx > v.crop_hi[0] || wy > v.crop_hi[1] || wz > v.crop_hi[2]) continue;
+        }
+        int nn = c < MAP_CAP ? c : MAP_CAP;
+        int refl = (int)((double)acc[4 * s + 3] / (double)nn + 0.5);
+        if (refl > 255) refl = 255;
+        out_xyz[3 * k] = wx;
+        out_xyz[3 * k + 1] = wy;
+        out_xyz[3 * k + 2] = wz;
+        out_attr[k] = (uint32_t)refl;
+        out_t[k] = last[s];
+        int dyn = 0;
+        if (transient(c, miss[s], v)) {
+            dyn = 1;
+        } else {
+            int ix = ifloor(wx * v.inv_voxel), iy = ifloor(wy * v.inv_voxel), iz = ifloor(wz * v.inv_voxel);
+            int settled = 0;
+            for (int nb = 0; nb < 7 && !settled; ++nb) {
+                int jx = ix, jy = iy, jz = iz;
+                if (nb == 1) jx = ix - 1;
+                else if (nb == 2) jx = ix + 1;
+                else if (nb == 3) jy = iy - 1;
+                else if (nb == 4) jy = iy + 1;
+                else if (nb == 5) jz = iz - 1;
+                else if (nb == 6) jz = iz + 1;
+                int sn = find_slot(key_ijk(jx, jy, jz), keys, v.map_mask);
+                if (sn >= 0) {
+                    float age = v.now - first[sn];
+                    if (age < 0.0f) age = 1.0e9f;
+                    if (age >= v.dyn_settle && transient(cnt[sn], miss[sn], v) == 0) settled = 1;
+                }
+            }
+            dyn = settled ? 0 : 1;
+        }
+        out_dyn[k] = dyn;
+        ++k;
+    }
+    return k;
+}
+
+}  // extern "C"

@@ -1,0 +1,435 @@
+"""CPU oracle of the livox-warp per-frame hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module, and only as the checker or
+the timed CPU baseline; the product (livox-warp_b200/livox_warp) never imports it.
+
+Two layers:
+  * liblworacle.so (lw_oracle.cpp): the reference's Warp kernels restated as serial C++ -- keys and hashing,
+    deskew, thinning, registration insert and per-voxel records, the ICP accumulation in float64, the
+    integration insert, carving and the map's visible set;
+  * this file: the host-side float64 Gauss-Newton step of odom.py (_sym6 :390-394, _twist_between :397-401,
+    _apply_twist :404-409, _body_twist :412-414, _twist_matrix :417-422, _sensor_basis :425-433,
+    _constrained_step :436-455, _register :752-803) and the frame state machine of Odometry
+    (_finalize :642-657, _estimate :659-680, _update_velocity :682-694, _is_keyframe :712-717), written with
+    numpy and scipy exactly as the reference's host code is -- so the pose oracle is float64 end to end.
+
+Parity of the kernel restatement against the reference is unpinned (NVIDIA Warp is not installed here and the
+reference ships no golden vectors for its kernels); the host step is pinned against the reference's own
+functions through tests/golden/host_solve.npz (see tests/golden/make_golden.py).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from pathlib import Path
+
+import numpy as np
+from scipy.spatial.transform import Rotation
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liblworacle.so"
+
+FIX_R, FIX_RR, FIX_W = 2.0 ** 32, 2.0 ** 40, 2.0 ** 20
+POSE_SLOTS = 1 << 16
+ACC_H, ACC_B, ACC_COUNT, ACC_ERR, ACC_RMS, ACC_WEIGHT, ACC_RANGE, ACC_HG = 0, 21, 27, 28, 29, 30, 31, 32
+WIDE_ITERS = 3
+KAPPA_START, KAPPA_DECAY, KAPPA_MIN = 6.0, 0.7, 2.0
+STEP_TOL = 1e-4
+TIGHT_FRACTION = 0.6
+WEAK_COND = 1e-3
+REDESKEW_ROT, REDESKEW_TRANS = 2e-3, 5e-3
+MAX_FRAME_JUMP = 1.5
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            import importlib.util
+            spec = importlib.util.spec_from_file_location("lw_oracle_build", HERE / "build.py")
+            mod = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(mod)
+            mod.build()
+        _lib = C.CDLL(str(LIB))
+        P = C.c_void_p
+        i64, i32, f32, f64 = C.c_int64, C.c_int32, C.c_float, C.c_double
+        sig = {
+            "or_key_ijk": (i64, [i32, i32, i32]),
+            "or_slot_hash": (i32, [i64]),
+            "or_voxel_keys": (None, [P, i64, f32, P]),
+            "or_deskew": (None, [P, i64, f32, f32, P, P]),
+            "or_thin": (i64, [P, P, i64, f32, f32, f32, i32, P]),
+            "or_reg_insert": (None, [P, P, i64, P, f32, f32, f32, i32, i64, P, P, P, P, P]),
+            "or_reg_records": (None, [i64, P, P, P, P, f32, f32, f32, f32, P]),
+            "or_icp_accumulate": (None, [P, i64, P, i64, P, P, f64, i32, f64, f64, i32, P]),
+            "or_map_insert": (None, [P, i32, P, P, P, i64, P, P, f32, i64, P, P, P, P, P, P]),
+            "or_carve": (None, [P, i32, P, P, i64, P, i32, f32, f32, i32, i64, P, P, P, P, i32]),
+            "or_map_build": (i64, [i64, P, P, P, P, P, P, P, i32, P, P, P, P]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(_lib, name)
+            fn.restype = res
+            fn.argtypes = args
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"], "oracle arrays must be contiguous"
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def threads() -> int:
+    return int(os.environ.get("LW_ORACLE_THREADS", os.cpu_count() or 1))
+
+
+# ---- kernels ------------------------------------------------------------------------------------------------
+
+
+def voxel_keys(xyz: np.ndarray, inv: float) -> np.ndarray:
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+    out = np.empty(len(xyz), np.int64)
+    lib().or_voxel_keys(_p(xyz), len(xyz), inv, _p(out))
+    return out
+
+
+def deskew(raw4: np.ndarray, t_mid: float, inv_dt: float, twist) -> np.ndarray:
+    raw4 = np.ascontiguousarray(raw4, dtype=np.float32)
+    out = np.empty_like(raw4)
+    tw = np.ascontiguousarray(twist, dtype=np.float32)
+    lib().or_deskew(_p(raw4), len(raw4), np.float32(t_mid), np.float32(inv_dt), _p(tw), _p(out))
+    return out
+
+
+def thin(xyz4: np.ndarray, attr: np.ndarray, inv_v: float, min_range: float, max_range: float, ret_mask: int):
+    xyz4 = np.ascontiguousarray(xyz4, dtype=np.float32)
+    attr = np.ascontiguousarray(attr, dtype=np.uint32)
+    out = np.empty_like(xyz4)
+    n = lib().or_thin(_p(xyz4), _p(attr), len(xyz4), inv_v, min_range, max_range, ret_mask, _p(out))
+    return out[:n]
+
+
+class RegMap:
+    """The registration map as the oracle keeps it (same slot layout as the device tables)."""
+
+    def __init__(self, cap: int):
+        self.cap = cap
+        self.keys = np.full(cap, -1, np.int64)
+        self.cnt = np.zeros(cap, np.int32)
+        self.sum = np.zeros((cap, 3), np.int64)
+        self.outer = np.zeros((cap, 6), np.int64)
+        self.stats = np.zeros(2, np.int32)
+        self.rec = np.zeros((cap, 20), np.float32)
+
+    def insert(self, xyz4, attr, T, voxel: float, max_range: float, ret_mask: int):
+        xyz4 = np.ascontiguousarray(xyz4, dtype=np.float32)
+        attr = np.ascontiguousarray(attr, dtype=np.uint32)
+        T12 = np.ascontiguousarray(np.asarray(T, np.float64).reshape(4, 4)[:3].astype(np.float32))
+        lib().or_reg_insert(_p(xyz4), _p(attr), len(xyz4), _p(T12), np.float32(1.0 / voxel), np.float32(voxel),
+                            max_range, ret_mask, self.cap, _p(self.keys), _p(self.cnt), _p(self.sum),
+                            _p(self.outer), _p(self.stats))
+
+    def records(self, voxel: float, noise: float, alpha: float):
+        tight2 = (TIGHT_FRACTION * voxel / math.sqrt(12.0)) ** 2
+        lib().or_reg_records(self.cap, _p(self.keys), _p(self.cnt), _p(self.sum), _p(self.outer), voxel, tight2,
+                             noise * noise, alpha, _p(self.rec))
+        return self.rec
+
+    def as_dict(self):
+        occ = self.keys != -1
+        return {int(k): (int(c), tuple(s), tuple(o)) for k, c, s, o in
+                zip(self.keys[occ], self.cnt[occ], self.sum[occ], self.outer[occ])}
+
+
+def icp_accumulate(ds4: np.ndarray, T: np.ndarray, reg: RegMap, voxel: float, reach: int, max_d2: float,
+                   kappa: float, nthreads: int | None = None) -> np.ndarray:
+    ds4 = np.ascontiguousarray(ds4, dtype=np.float32)
+    T = np.ascontiguousarray(np.asarray(T, np.float64).reshape(16))
+    out = np.zeros(64)
+    lib().or_icp_accumulate(_p(ds4), len(ds4), _p(T), reg.cap, _p(reg.keys), _p(reg.rec), 1.0 / voxel, reach,
+                            max_d2, kappa, nthreads or threads(), _p(out))
+    return out
+
+
+# ---- integration map -------------------------------------------------------------------------------------
+
+
+class Map:
+    def __init__(self, cap: int):
+        self.cap = cap
+        self.keys = np.full(cap, -1, np.int64)
+        self.cnt = np.zeros(cap, np.int32)
+        self.acc = np.zeros((cap, 4), np.int64)
+        self.last = np.zeros(cap, np.float32)
+        self.first = np.full(cap, 1.0e30, np.float32)
+        self.miss = np.zeros(cap, np.int32)
+        self.stats = np.zeros(2, np.int32)
+
+    def insert(self, xyz, attr, t, frame, poses, view, voxel: float):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+        stride = xyz.shape[1]
+        attr = np.ascontiguousarray(attr, dtype=np.uint32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        frame = np.ascontiguousarray(frame, dtype=np.int32)
+        poses = np.ascontiguousarray(poses, dtype=np.float32).reshape(POSE_SLOTS, 16)
+        lib().or_map_insert(_p(xyz), stride, _p(attr), _p(t), _p(frame), len(t), _p(poses), C.byref(view),
+                            np.float32(1.0 / max(voxel, 1e-4)), self.cap, _p(self.keys), _p(self.cnt), _p(self.acc),
+                            _p(self.last), _p(self.first), _p(self.stats))
+
+    def carve(self, xyz, attr, frame, poses, voxel, every=2, max_range=40.0, max_steps=4096, nthreads=None):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+        attr = np.ascontiguousarray(attr, dtype=np.uint32)
+        frame = np.ascontiguousarray(frame, dtype=np.int32)
+        poses = np.ascontiguousarray(poses, dtype=np.float32).reshape(POSE_SLOTS, 16)
+        lib().or_carve(_p(xyz), xyz.shape[1], _p(attr), _p(frame), len(frame), _p(poses), max(1, int(every)),
+                       np.float32(1.0 / max(voxel, 1e-4)), max_range, max_steps, self.cap, _p(self.keys),
+                       _p(self.cnt), _p(self.acc), _p(self.miss), nthreads or threads())
+
+    def build(self, view, min_count: int = 1):
+        n = self.cap
+        xyz = np.zeros((n, 3), np.float32)
+        attr = np.zeros(n, np.uint32)
+        t = np.zeros(n, np.float32)
+        dyn = np.zeros(n, np.int32)
+        k = lib().or_map_build(self.cap, _p(self.keys), _p(self.cnt), _p(self.acc), _p(self.last), _p(self.first),
+                               _p(self.miss), C.byref(view), min_count, _p(xyz), _p(attr), _p(t), _p(dyn))
+        return xyz[:k], attr[:k], t[:k], dyn[:k]
+
+    def as_dict(self):
+        occ = self.keys != -1
+        return {int(k): (int(c), tuple(a), float(l), float(f), int(m)) for k, c, a, l, f, m in
+                zip(self.keys[occ], self.cnt[occ], self.acc[occ], self.last[occ], self.first[occ], self.miss[occ])}
+
+
+# ---- the host-side float64 step (odom.py:387-455) -----------------------------------------------------------
+
+_TRIU6 = np.triu_indices(6)
+
+
+def sym6(upper: np.ndarray) -> np.ndarray:
+    H = np.zeros((6, 6))
+    H[_TRIU6] = upper
+    return H + np.triu(H, 1).T
+
+
+def twist_between(T_from, T_to):
+    M = T_to @ np.linalg.inv(T_from)
+    return np.concatenate([M[:3, 3], Rotation.from_matrix(M[:3, :3]).as_rotvec()])
+
+
+def apply_twist(T, delta):
+    Rz = Rotation.from_rotvec(delta[3:]).as_matrix()
+    out = T.copy()
+    out[:3, :3] = Rz @ T[:3, :3]
+    out[:3, 3] = Rz @ T[:3, 3] + delta[:3]
+    return out
+
+
+def body_twist(d):
+    return np.concatenate([d[:3, 3], Rotation.from_matrix(d[:3, :3]).as_rotvec()]).astype(np.float32)
+
+
+def twist_matrix(xi):
+    out = np.eye(4)
+    out[:3, :3] = Rotation.from_rotvec(np.asarray(xi[3:], dtype=np.float64)).as_matrix()
+    out[:3, 3] = xi[:3]
+    return out
+
+
+def sensor_basis(T, L):
+    c = T[:3, 3]
+    J = np.eye(6)
+    J[:3, 3:] = np.array([[0.0, -c[2], c[1]], [c[2], 0.0, -c[0]], [-c[1], c[0], 0.0]])
+    B = np.zeros((6, 6))
+    B[:3, :3] = B[3:, 3:] = T[:3, :3]
+    return J @ B @ np.diag([1.0, 1.0, 1.0, 1.0 / L, 1.0 / L, 1.0 / L])
+
+
+def constrained_step(A, rhs, Hg, T, L, thr, to_pred):
+    J = sensor_basis(T, L)
+    lam, V = np.linalg.eigh(J.T @ Hg @ J)
+    good = lam >= thr
+    if good.all():
+        return np.linalg.solve(A, rhs), (lam, V, good)
+    Vd = V[:, ~good]
+    d0 = Vd @ (Vd.T @ np.linalg.solve(J, to_pred))
+    if good.any():
+        Vg = V[:, good]
+        As = J.T @ A @ J
+        d0 = d0 + Vg @ np.linalg.solve(Vg.T @ As @ Vg, Vg.T @ (J.T @ rhs - As @ d0))
+    return J @ d0, (lam, V, good)
+
+
+class Params:
+    """Odometry tuning with the reference's defaults (odom.py:499-525)."""
+
+    def __init__(self, **kw):
+        self.frame_dt = 0.1
+        self.reg_voxel = 0.15
+        self.max_iter = 16
+        self.warmup = 8
+        self.min_points = 200
+        self.min_corr = 60
+        self.min_range = 0.3
+        self.max_range = 60.0
+        self.noise = 0.02
+        self.ret_mask = 0b1111
+        self.alpha = 0.05
+        self.damping = 1.0e-3
+        self.velocity_smooth = 0.85
+        self.degen_thr = 3000.0
+        self.prior_info = 2000.0
+        self.kf_dist = 0.05
+        self.kf_angle = 1.0
+        self.deskew = True
+        self.redeskew = True
+        for k, v in kw.items():
+            setattr(self, k, v)
+
+
+def schedule(it: int, voxel: float):
+    """reach, max_d2 and kappa of iteration `it`, rounded to float32 the way the kernels receive them."""
+    reach = 2 if it < WIDE_ITERS else 1
+    d = np.float32(np.float32(reach) + np.float32(0.5)) * np.float32(voxel)
+    max_d2 = float(np.float32(d * d))
+    kappa = float(np.float32(max(KAPPA_MIN, KAPPA_START * (KAPPA_DECAY ** it))))
+    return reach, max_d2, kappa
+
+
+def register(ds4: np.ndarray, T_pred: np.ndarray, reg: RegMap, p: Params, nthreads: int | None = None):
+    """odom.py:752-803 with the float64 accumulation; returns (T, ok, stats dict)."""
+    n_ds = len(ds4)
+    stats = {"ds": n_ds}
+    if n_ds < p.min_corr:
+        return T_pred.copy(), False, stats
+    T = T_pred.copy()
+    voxel = p.reg_voxel
+    iters, corr, rms, cond, n_degen = 0, 0, 0.0, 1.0, 0
+    H = np.eye(6)
+    for it in range(p.max_iter):
+        reach, max_d2, kappa = schedule(it, voxel)
+        v = icp_accumulate(ds4, T, reg, voxel, reach, max_d2, kappa, nthreads)
+        corr = int(v[ACC_COUNT])
+        if corr < p.min_corr:
+            break
+        H, b, Hg = sym6(v[ACC_H:ACC_H + 21]), v[ACC_B:ACC_B + 6], sym6(v[ACC_HG:ACC_HG + 21])
+        L = max(v[ACC_RANGE] / corr, 1.0)
+        rms = math.sqrt(max(v[ACC_RMS], 0.0) / max(v[ACC_WEIGHT], 1e-9))
+        dg = np.diag(H)
+        A = H + np.diag(1e-9 * dg.mean() + p.damping * dg)
+        rhs = -b
+        xi = twist_between(T, T_pred)
+        if p.prior_info > 0.0:
+            Ji = np.linalg.inv(sensor_basis(T, L))
+            P = p.prior_info * (Ji.T @ Ji)
+            A = A + P
+            rhs = rhs + P @ xi
+        try:
+            if p.degen_thr > 0.0:
+                delta, (_, _, kept) = constrained_step(A, rhs, Hg, T, L, p.degen_thr, xi)
+                n_degen = int((~kept).sum())
+            else:
+                delta = np.linalg.solve(A, rhs)
+        except np.linalg.LinAlgError:
+            break
+        T = apply_twist(T, delta)
+        iters = it + 1
+        if np.linalg.norm(delta[:3]) < STEP_TOL and np.linalg.norm(delta[3:]) < STEP_TOL:
+            break
+    if corr >= p.min_corr:
+        dg = np.sqrt(np.maximum(np.diag(H), 1e-12))
+        ev = np.linalg.eigvalsh(H / np.outer(dg, dg))
+        cond = float(max(ev[0], 0.0) / max(ev[-1], 1e-12))
+    stats.update(iters=iters, corr=corr, rms=rms, cond=cond, weak=cond < WEAK_COND or n_degen > 0, degen=n_degen)
+    return T, corr >= p.min_corr, stats
+
+
+class Odometry:
+    """The frame pipeline of odom.py:642-727 on the oracle, fed one frame at a time."""
+
+    def __init__(self, reg_slots: int, p: Params, T0=None):
+        self.p = p
+        self.reg = RegMap(reg_slots)
+        self.T = np.eye(4) if T0 is None else np.asarray(T0, np.float64)
+        self.T_prev = None
+        self.delta = np.eye(4)
+        self.xi = np.zeros(6, np.float32)
+        self.xi_s = np.zeros(6)
+        self.map_frames = 0
+        self.T_key = None
+        self.traj = []
+        self.stats = {}
+
+    def predict(self):
+        return self.T @ self.delta
+
+    def _deskew(self, raw4, t_mid, xi):
+        return deskew(raw4, np.float32(t_mid), np.float32(1.0 / self.p.frame_dt), xi)
+
+    def _register(self, xyz4, attr, T_pred):
+        p = self.p
+        ds = thin(xyz4, attr, np.float32(2.0 / p.reg_voxel), p.min_range, p.max_range, p.ret_mask)
+        return register(ds, T_pred, self.reg, p)
+
+    def frame(self, k: int, raw4: np.ndarray, attr: np.ndarray):
+        """Finalise frame k from its raw points (x, y, z, t); returns (T, xyz4 deskewed, ok)."""
+        p = self.p
+        m = len(raw4)
+        warm = self.map_frames < p.warmup
+        t_mid = (k + 0.5) * p.frame_dt
+        xi = self.xi if (p.deskew and not warm) else np.zeros(6, np.float32)
+        xyz4 = self._deskew(raw4, t_mid, xi) if m > 0 else raw4
+        T = self.T if warm else self.predict()
+        ok = True
+        if m < p.min_points:
+            ok = False
+        elif not warm:
+            T, ok, st = self._register(xyz4, attr, T)
+            self.stats.update(st)
+            if ok and p.deskew and p.redeskew and self.T_prev is not None:
+                xi_new = body_twist(np.linalg.inv(self.T_prev) @ T)
+                if (np.linalg.norm(xi_new[3:] - xi[3:]) > REDESKEW_ROT
+                        or np.linalg.norm(xi_new[:3] - xi[:3]) > REDESKEW_TRANS):
+                    xi = xi_new
+                    xyz4 = self._deskew(raw4, t_mid, xi)
+                    T, ok, st = self._register(xyz4, attr, T)
+                    self.stats.update(st)
+        if ok and (warm or self._is_keyframe(T)):
+            self.reg.insert(xyz4, attr, T, p.reg_voxel, p.max_range, p.ret_mask)
+            self.reg.records(p.reg_voxel, p.noise, p.alpha)
+            self.map_frames += 1
+            self.T_key = T.copy()
+        if self.T_prev is not None and not warm:
+            self._update_velocity(np.linalg.inv(self.T_prev) @ T)
+        self.T_prev = self.T = T
+        self.traj.append((k, t_mid, T.copy()))
+        return T, xyz4, ok
+
+    def _is_keyframe(self, T):
+        if self.T_key is None:
+            return True
+        d = np.linalg.inv(self.T_key) @ T
+        ang = math.degrees(np.linalg.norm(Rotation.from_matrix(d[:3, :3]).as_rotvec()))
+        return np.linalg.norm(d[:3, 3]) >= self.p.kf_dist or ang >= self.p.kf_angle
+
+    def _update_velocity(self, d):
+        if np.linalg.norm(d[:3, 3]) < MAX_FRAME_JUMP:
+            self.delta = d
+            self.xi = body_twist(d)
+            if self.p.velocity_smooth > 0.0:
+                a = self.p.velocity_smooth
+                self.xi_s = a * self.xi_s + (1.0 - a) * self.xi.astype(np.float64)
+                self.delta = twist_matrix(self.xi_s)
+        else:
+            self.delta = np.eye(4)
+            self.xi = np.zeros(6, np.float32)
+            self.xi_s = np.zeros(6)
+
+
+def pose_error(A: np.ndarray, B: np.ndarray):
+    """(metres, degrees) between two 4x4 poses."""
+    d = np.linalg.inv(A) @ B
+    return float(np.linalg.norm(d[:3, 3])), float(np.degrees(np.linalg.norm(Rotation.from_matrix(d[:3, :3]).as_rotvec())))

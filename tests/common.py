@@ -1,0 +1,62 @@
+"""Shared seeded inputs of the tests: the scenes and scans of the benchmark configurations at test sizes."""
+
+from __future__ import annotations
+
+import functools
+
+import numpy as np
+
+from livox_warp import synth
+
+FRAME_DT = 0.1
+
+
+@functools.lru_cache(maxsize=None)
+def room(seed: int = 1):
+    return synth.box_room(seed)
+
+
+@functools.lru_cache(maxsize=None)
+def handheld(seed: int = 2, duration: float = 20.0, scene_seed: int = 1):
+    return synth.Handheld(room(scene_seed), seed, duration)
+
+
+@functools.lru_cache(maxsize=None)
+def handheld_frames(n: int, seed: int = 3, traj_seed: int = 2, duration: float = 20.0, rate: float = 100000.0):
+    sc = room(1)
+    tr = handheld(traj_seed, duration)
+    return synth.frames(sc, tr, n, rate, seed)
+
+
+def frame_ids(t: np.ndarray, inv_dt: float = 10.0) -> np.ndarray:
+    """floor(max(t, 0) * inv_dt) in float32, as the frame-id kernel computes it."""
+    return np.floor(np.maximum(np.asarray(t, np.float32), np.float32(0)) * np.float32(inv_dt)).astype(np.int32)
+
+
+def mid_pose(traj, k: int) -> np.ndarray:
+    return traj.poses(np.array([(k + 0.5) * FRAME_DT]))[0]
+
+
+def raw4(xyz, t) -> np.ndarray:
+    return np.ascontiguousarray(np.concatenate([xyz, t[:, None]], axis=1).astype(np.float32))
+
+
+def look_at(p, target) -> np.ndarray:
+    """Sensor-to-world pose at p with the sensor's x axis toward target (no roll)."""
+    import math
+
+    from scipy.spatial.transform import Rotation
+
+    p = np.asarray(p, np.float64)
+    d = np.asarray(target, np.float64) - p
+    yaw = math.atan2(d[1], d[0])
+    pitch = -math.atan2(d[2], np.linalg.norm(d[:2]))
+    T = np.eye(4)
+    T[:3, :3] = Rotation.from_euler("zyx", [yaw, pitch, 0.0]).as_matrix()
+    T[:3, 3] = p
+    return T
+
+
+def config1_pose() -> np.ndarray:
+    """The single-frame ICP case's start pose: a corner of the box room, looking across it and slightly down."""
+    return look_at([0.8, 0.8, 1.6], [7.0, 5.0, 1.0])
