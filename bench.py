@@ -1,0 +1,431 @@
+#!/usr/bin/env python
+"""Benchmark of the per-frame SLAM hot path on B200: sequence odometry frames/s.
+
+Workload (the sequence-odometry configuration): a seeded 8 x 6 x 3 m box room with 20 boxes, a Mid-40-like
+rosette at 100k points/s (about 10k points per 0.1 s frame) along a smooth handheld trajectory (a spline
+through random waypoints, <= 1 m/s and <= 60 deg/s, after 1 s at rest). Each step is one frame through the
+whole path: frame cut, deskew, half-voxel thinning, scan-to-map Gauss-Newton (float64 6x6 solve on the device),
+re-deskew, keyframe insert into the 0.15 m registration map, velocity update, then insertion of the frame into
+the 0.1 m integration map (2^22 slots) and free-space carving of every ray.
+
+  value  frames/s with the frames already resident in HBM, device time (CUDA events per step), L2 flushed
+         between steps by a 256 MB write outside the timed events;
+  e2e    the same through the public API from host (numpy) buffers: pinned H2D of each frame, the pose read
+         back (D2H) every frame, CUDA events around all steps;
+  roofline  the dominant kernel's algorithmic bytes / its live average launch time vs the measured HBM peak;
+  cpu_baseline  the CPU oracle (a C++ / numpy restatement of the reference's kernels and host solve, OpenMP)
+         on a bounded sample of the same frames.
+
+`--impl reference` times the reference's CPU implementation of the path instead: NVIDIA Warp (the reference's
+only runtime) is not installed, so that arm runs the CPU restatement, on every host core.
+Multi-GPU: the path does not shard (each frame registers against the map of the frames before it), so
+`--gpus N` runs N independent replicas, one per GPU, and `value` sums their frames.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path[:0] = [str(ROOT), str(ROOT / "livox-warp_b200")]
+
+RATE = 100000.0
+FRAME_DT = 0.1
+REG_VOXEL = 0.15
+MAP_VOXEL = 0.1
+MAP_SLOTS = 1 << 22
+REG_SLOTS = 1 << 21
+FRAME_CAP = 1 << 18
+SEED = 2026
+L2_FLUSH_BYTES = 256 << 20
+
+
+# ---- workload --------------------------------------------------------------------------------------------------
+
+
+def _gen_chunk(args):
+    seed, duration, k0, k1 = args
+    from livox_warp import synth
+
+    scene = synth.box_room(seed)
+    traj = synth.Handheld(scene, seed + 1, duration)
+    return synth.frames(scene, traj, k1 - k0, RATE, seed + 2, start=k0)
+
+
+def workload(n_frames: int, seed: int = SEED, procs: int | None = None):
+    """The frames 0 .. n_frames-1 of the sequence (generated in a spawn pool before any CUDA call)."""
+    from livox_warp import synth
+
+    duration = n_frames * FRAME_DT + 2.0
+    procs = procs or min(8, os.cpu_count() or 1)
+    step = max(1, math.ceil(n_frames / (procs * 4)))
+    chunks = [(seed, duration, k, min(k + step, n_frames)) for k in range(0, n_frames, step)]
+    if procs > 1 and len(chunks) > 1:
+        with mp.get_context("spawn").Pool(procs) as pool:
+            parts = pool.map(_gen_chunk, chunks)
+    else:
+        parts = [_gen_chunk(c) for c in chunks]
+    frames = [f for p in parts for f in p]
+    scene = synth.box_room(seed)
+    traj = synth.Handheld(scene, seed + 1, duration)
+    return frames, traj
+
+
+# ---- clocks --------------------------------------------------------------------------------------------------
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and the throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = np.array([float(r[1]) for r in rows if r[1].replace(".", "").isdigit()] or [0.0])
+        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for r in rows for j in range(4) if r[5 + j].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+# ---- the device arm ----------------------------------------------------------------------------------------------
+
+
+def make_engine(device):
+    from livox_warp import gpu
+    from livox_warp.odom import Odometry
+
+    pipe = gpu.Pipeline(ring_capacity=1 << 16, map_capacity=MAP_SLOTS, device=device)
+    odom = Odometry(pipe, reg_slots=REG_SLOTS, frame_cap=FRAME_CAP)
+    odom.reg_voxel = REG_VOXEL
+    view = gpu.make_view(now=0.0, voxel=MAP_VOXEL, map_cap=MAP_SLOTS)
+    odom.integrate(view, MAP_VOXEL, carve_every=1)
+    return pipe, odom
+
+
+def run_device(frames, traj, warmup: int, steps: int, device, clocks: "Clocks | None"):
+    import torch
+
+    from livox_warp import _lib
+
+    pipe, odom = make_engine(device)
+    T0 = traj.poses(np.array([0.5 * FRAME_DT]))[0]
+    odom.reset(T0)
+    dev = [(torch.from_numpy(x).to(device), torch.from_numpy(a.view(np.int32)).to(device),
+            torch.from_numpy(t).to(device), len(t), float(t.min()), float(t.max())) for x, a, t in frames]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream(device)
+
+    def step(k):
+        sx, sa, st, n, t0, t1 = dev[k]
+        sf = pipe._stage_frame if pipe._stage_frame is not None and pipe._stage_frame.numel() >= n else None
+        if sf is None:
+            pipe._ensure_stage(n)
+            sf = pipe._stage_frame
+        _lib.call("lw_frame_ids", _lib.ptr(st), n, float(1.0 / FRAME_DT), _lib.ptr(sf), _lib.stream_ptr())
+        odom.push(sx, sa, st, n, t0, t1)
+
+    for k in range(warmup):
+        step(k)
+    torch.cuda.synchronize(device)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    _lib.prof_reset()
+    _lib.prof_enable(True)
+    _lib.launches(reset=True)
+    if clocks:
+        clocks.start()
+    torch.cuda.synchronize(device)
+    for j in range(steps):
+        flush.fill_(float(j))  # L2 flush, outside the step's events
+        evs[j][0].record(stream)
+        step(warmup + j)
+        evs[j][1].record(stream)
+    torch.cuda.synchronize(device)
+    clk = clocks.stop() if clocks else None
+    launches = _lib.launches()
+    _lib.prof_enable(False)
+    step_ms = np.array([a.elapsed_time(b) for a, b in evs])
+    names = ("gn", "carve", "map_insert", "thin", "reg_insert", "frame_append", "control")
+    prof = {n: _lib.prof_read(n) for n in names}
+    odom.flush()
+    torch.cuda.synchronize(device)
+    return {"step_ms": step_ms, "prof": prof, "launches": launches, "clocks": clk, "odom": odom, "pipe": pipe}
+
+
+def run_e2e(frames, traj, warmup: int, steps: int, device):
+    """Through the public API from host buffers: stage (pinned H2D), push, pose read back every frame."""
+    import torch
+
+    pipe, odom = make_engine(device)
+    odom.reset(traj.poses(np.array([0.5 * FRAME_DT]))[0])
+    pose_host = torch.empty(16, dtype=torch.float64, pin_memory=True)
+    stream = torch.cuda.current_stream(device)
+
+    def step(k):
+        x, a, t = frames[k]
+        sx, sa, st, sf = pipe.stage(x, a, t, len(t), 1.0 / FRAME_DT)
+        odom.push(sx, sa, st, len(t), float(t.min()), float(t.max()))
+        pose_host.copy_(odom._state[:128].view(torch.float64), non_blocking=True)
+        stream.synchronize()  # the caller consumes the frame's pose
+        return pose_host.numpy()
+
+    for k in range(warmup):
+        step(k)
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for j in range(steps):
+        step(warmup + j)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    ms = e0.elapsed_time(e1)
+    n_pts = np.mean([len(frames[warmup + j][2]) for j in range(steps)])
+    return {"ms": ms, "h2d": int(round(n_pts * 20)), "d2h": 128}
+
+
+def roofline(res, frames, traj, warmup, steps, peak):
+    """The dominant kernel's achieved GB/s: algorithmic bytes per launch / live average launch time."""
+    from livox_warp import roofline as rl
+
+    prof = res["prof"]
+    name = max(prof, key=lambda n: prof[n][0])
+    ms, cnt = prof[name]
+    odom, pipe = res["odom"], res["pipe"]
+    recs = {r[0]: r for r in odom.traj_records()}
+    reg_keys = odom.reg_keys.cpu().numpy()
+    reg_keys = reg_keys[reg_keys != -1]
+    map_keys = pipe.map_keys.cpu().numpy()
+    map_keys = map_keys[map_keys != -1]
+    sample = list(range(warmup, warmup + steps, max(1, steps // 12)))
+    per_launch = []
+    for k in sample:
+        if k not in recs:
+            continue
+        _, _, T, ok, iters, corr = recs[k]
+        x = frames[k][0]
+        if name == "gn":
+            ds = rl.thin_host(x, REG_VOXEL)
+            per_launch.append(rl.gn_bytes(ds, T, reg_keys, REG_VOXEL, max(iters, 1), odom._gn.grid))
+        elif name == "carve":
+            per_launch.append(rl.carve_bytes(x, T, map_keys, MAP_VOXEL))
+        else:
+            per_launch.append(rl.map_insert_bytes(x, T, MAP_VOXEL))
+    if name == "gn":
+        launches_per_frame = 2  # the first registration and the (usually gated-off) re-registration
+        bytes_per_launch = float(np.mean(per_launch)) / launches_per_frame
+    else:
+        bytes_per_launch = float(np.mean(per_launch))
+    avg_ms = ms / max(cnt, 1)
+    achieved = bytes_per_launch / (avg_ms * 1e-3) / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 3), "peak": peak["hbm_gbs"], "unit": "GB/s",
+            "frac": round(achieved / peak["hbm_gbs"], 5), "traffic": None,
+            "peak_source": peak["source"], "avg_launch_us": round(avg_ms * 1e3, 2), "launches": int(cnt),
+            "algorithmic_bytes_per_launch": int(bytes_per_launch),
+            "kernel_ms_share": {n: round(prof[n][0] / max(sum(v[0] for v in prof.values()), 1e-9), 4) for n in prof}}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured (MEASURED_PEAKS.json)"}
+    return {"hbm_gbs": 6650.0, "source": "fallback 6.65 TB/s"}
+
+
+# ---- the CPU arms ------------------------------------------------------------------------------------------------
+
+
+def cpu_pipeline(frames, traj, warmup: int, budget_s: float, max_frames: int, threads: int):
+    """The oracle's frame pipeline (odometry + integration insert + carving) over frames 0..; the first `warmup`
+    frames untimed, then frames until max_frames or budget_s of CPU time. Returns (frames timed, seconds)."""
+    os.environ["LW_ORACLE_THREADS"] = str(threads)
+    from oracle import oracle
+
+    p = oracle.Params(reg_voxel=REG_VOXEL)
+    T0 = traj.poses(np.array([0.5 * FRAME_DT]))[0]
+    od = oracle.Odometry(REG_SLOTS, p, T0)
+    om = oracle.Map(MAP_SLOTS)
+    poses = np.tile(np.eye(4, dtype=np.float32).reshape(1, 16), (oracle.POSE_SLOTS, 1))
+    view = _oracle_view(oracle)
+    timed, t_total = 0, 0.0
+    for k, (x, a, t) in enumerate(frames):
+        t0 = time.perf_counter()
+        raw = np.ascontiguousarray(np.concatenate([x, t[:, None]], 1), dtype=np.float32)
+        T, xyz4, ok = od.frame(k, raw, a)
+        poses[k & (oracle.POSE_SLOTS - 1)] = T.astype(np.float32).reshape(16)
+        fid = np.full(len(t), k, np.int32)
+        om.insert(xyz4, a, t, fid, poses, view, MAP_VOXEL)
+        om.carve(xyz4, a, fid, poses, MAP_VOXEL, every=1, nthreads=threads)
+        dt = time.perf_counter() - t0
+        if k >= warmup:
+            timed += 1
+            t_total += dt
+            if timed >= max_frames or t_total >= budget_s:
+                break
+    return timed, t_total
+
+
+def _oracle_view(oracle):
+    from livox_warp import _lib
+
+    v = _lib.View()
+    v.now, v.persist, v.min_range, v.max_range = 0.0, 0.0, 0.1, 500.0
+    v.min_refl, v.noise_mask, v.ret_mask, v.crop_on = 0, 0b1111, 0b1111, 0
+    v.crop_lo, v.crop_hi = (-1e9, -1e9, -1e9), (1e9, 1e9, 1e9)
+    v.inv_voxel, v.map_mask = 1.0 / MAP_VOXEL, MAP_SLOTS - 1
+    return v
+
+
+# ---- main -------------------------------------------------------------------------------------------------------
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=580)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
+    ap.add_argument("--no-e2e", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    n_frames = a.warmup + a.steps + 1
+    metric = "ICP sequence odometry frames/s (deskew + GN ICP + keyframe insert + map insert + carve)"
+    config = {"workload": "sequence odometry: box room 8x6x3 m, 20 boxes, rosette 100k pts/s (~10k pts/frame), "
+                          "handheld spline <=1 m/s <=60 deg/s, reg voxel 0.15 m (2^21 slots), "
+                          "integration voxel 0.1 m (2^22 slots), carve every ray",
+              "frames": n_frames, "points_per_frame": None, "l2": "flushed between steps (256 MB write)",
+              "parallelism": f"replicas x{a.gpus}"}
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        frames, traj = workload(n_frames)
+        from oracle import oracle as _o
+
+        threads = _o.host_cores()
+        budget = max(30.0, min(150.0, 0.25 * a.steps))
+        timed, secs = cpu_pipeline(frames, traj, a.warmup, budget, a.steps, threads)
+        v = timed / secs
+        line = {"impl": "reference", "metric": metric, "value": round(v, 3), "unit": "frames/s", "n_gpus": a.gpus,
+                "steps": timed, "warmup": a.warmup, "ms_per_step": round(1e3 * secs / max(timed, 1), 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
+                "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": round(v, 3), "unit": "frames/s", "cores": threads, "kind": "port",
+                                 "sample": f"frames {a.warmup}..{a.warmup + timed - 1} of the sequence after "
+                                           f"{a.warmup} untimed frames; NVIDIA Warp (the reference runtime) is not "
+                                           "installed, so this is the CPU restatement of its kernels and host "
+                                           "solve"},
+                "e2e": {"value": round(v, 3), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    frames, traj = workload(n_frames)  # before any CUDA call (spawn pool)
+    config["points_per_frame"] = int(np.mean([len(f[2]) for f in frames]))
+    import torch
+    import torch.distributed as dist
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+    clocks = Clocks(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    res = run_device(frames, traj, a.warmup, a.steps, device, clocks)
+    ms_total = float(res["step_ms"].sum())
+    if world > 1:
+        t = torch.tensor([ms_total], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    value = world * a.steps / (ms_total * 1e-3)
+    e2e = None
+    if not a.no_e2e:
+        e = run_e2e(frames, traj, a.warmup, a.steps, device)
+        e_ms = e["ms"]
+        if world > 1:
+            t = torch.tensor([e_ms], dtype=torch.float64, device=device)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e2e = {"value": round(world * a.steps / (e_ms * 1e-3), 3), "unit": "frames/s",
+               "h2d_bytes_per_step": e["h2d"], "d2h_bytes_per_step": e["d2h"]}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    roof = roofline(res, frames, traj, a.warmup, a.steps, measured_peak())
+    from oracle import oracle as _o
+
+    threads = _o.host_cores()
+    n_cpu = max(3, min(60, a.steps))
+    timed, secs = cpu_pipeline(frames, traj, a.warmup, a.cpu_budget, n_cpu, threads)
+    pts = config["points_per_frame"]
+    line = {"metric": metric, "value": round(value, 3), "unit": "frames/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms_total / a.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 solve)", "data": "synthetic",
+            "config": config, "points_per_s": round(value * pts, 1),
+            "step_ms_p50_p99": [round(float(np.percentile(res["step_ms"], 50)), 4),
+                                round(float(np.percentile(res["step_ms"], 99)), 4)],
+            "roofline": roof,
+            "cpu_baseline": {"value": round(timed / secs, 3), "unit": "frames/s", "cores": threads, "kind": "port",
+                             "sample": f"{timed} frames ({a.warmup}..{a.warmup + timed - 1}) of the same sequence "
+                                       f"through the CPU oracle (C++/OpenMP kernels + numpy float64 solve), "
+                                       f"{secs:.1f} s"},
+            "e2e": e2e, "gpu_launches": int(res["launches"]), "clocks": res["clocks"]}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -63,6 +63,15 @@ const char* lw_last_error(void);
 /* Number of SMs of the current device (the persistent kernels launch one CTA per SM). */
 int lw_device_sms(int* out_sms);
 
+/* Opt-in launch timing: when enabled, the entry points bracket their main kernels with CUDA events on the
+ * launching stream ("gn", "thin", "reg_insert", "map_insert", "carve", "frame_append", "control", "map_build");
+ * lw_prof_read waits for them and returns the summed milliseconds and the launch count of one name. */
+int lw_prof_enable(int on);
+int lw_prof_read(const char* name, double* ms, int64_t* count);
+int lw_prof_reset(void);
+/* Kernels this library has launched since the last reset (reset when `reset` is non-zero). */
+int64_t lw_launches(int reset);
+
 /* ---- registration voxel map (odom.py:468-474) -------------------------------------------------- */
 typedef struct lw_regmap {
     int64_t* keys;   /* [cap] voxel key or -1 */

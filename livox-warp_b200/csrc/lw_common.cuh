@@ -28,6 +28,24 @@ int check_cuda(cudaError_t e, const char* what);
 
 int device_sms();
 
+// Kernel launches issued by the entry points since the last lw_launches_reset (a benchmark's claim of how many
+// of this library's kernels ran).
+void count_launches(int n);
+
+// Brackets the launches issued in its lifetime with CUDA events on `s` when timing is enabled (lw_prof_enable).
+class ProfScope {
+  public:
+    ProfScope(const char* name, cudaStream_t s);
+    ~ProfScope();
+    ProfScope(const ProfScope&) = delete;
+    ProfScope& operator=(const ProfScope&) = delete;
+
+  private:
+    const char* name_;
+    cudaStream_t s_;
+    void* a_;
+};
+
 // ---- voxel keys (gpu.py:59-64, 231-265) ----------------------------------------------------------------
 constexpr int64_t KEY_BIAS = 1LL << 20;
 constexpr int64_t KEY_MASK = (1LL << 21) - 1;

@@ -484,6 +484,7 @@ int lw_map_insert(const float* xyz, int32_t xyz_stride, const uint32_t* attr, co
     cudaStream_t s = (cudaStream_t)stream;
     MapIns mi{inv_voxel, (int)(map->cap - 1)};
     int grid = blocks_for(n_ub, 256, 8 * device_sms());
+    ProfScope prof("map_insert", s);
     if (xyz_stride == 4) {
         k_map_a<4><<<grid, 256, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, *v, mi, *map, pslot);
         k_map_b<4><<<grid, 256, 0, s>>>(xyz, attr, t, frame, n_dev, n_ub, poses, *v, mi, *map, pslot);
@@ -493,6 +494,7 @@ int lw_map_insert(const float* xyz, int32_t xyz_stride, const uint32_t* attr, co
     }
     k_map_d<<<grid, 256, 0, s>>>(n_dev, n_ub, *map, pslot);
     LW_LAUNCHED("lw_map_insert");
+    count_launches(3);
     return LW_OK;
 }
 
@@ -508,11 +510,13 @@ int lw_carve(const float* xyz, int32_t xyz_stride, const uint32_t* attr, const i
     cudaStream_t s = (cudaStream_t)stream;
     int64_t rays = (n_ub + every - 1) / every;
     int grid = blocks_for(rays, 128, 16 * device_sms());
+    ProfScope prof("carve", s);
     if (xyz_stride == 4)
         k_carve<4><<<grid, 128, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, every, inv_voxel, max_range, max_steps, *map);
     else
         k_carve<3><<<grid, 128, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, every, inv_voxel, max_range, max_steps, *map);
     LW_LAUNCHED("lw_carve");
+    count_launches(1);
     return LW_OK;
 }
 
@@ -524,10 +528,12 @@ int lw_map_build(const lw_map* map, const lw_view* v, int32_t min_count, float* 
         return set_error(LW_EINVAL, "lw_map_build: null argument");
     cudaStream_t s = (cudaStream_t)stream;
     int nt = blocks_for(map->cap, MTILE);
+    ProfScope prof("map_build", s);
     k_classify_count<<<nt, MTILE, 0, s>>>(*map, *v, min_count, tiles);
     k_scan_tiles<<<1, 1024, 0, s>>>(tiles, nt, count_dev);
     k_classify_scatter<<<nt, MTILE, 0, s>>>(*map, *v, min_count, tiles, out_xyz, out_attr, out_t, out_dyn);
     LW_LAUNCHED("lw_map_build");
+    count_launches(3);
     return LW_OK;
 }
 
@@ -536,6 +542,7 @@ int lw_frame_ids(const float* t, int64_t n, float inv_dt, int32_t* out, void* st
     if (n <= 0) return LW_OK;
     k_frame_of<<<blocks_for(n, 256, 8 * device_sms()), 256, 0, (cudaStream_t)stream>>>(t, n, inv_dt, out);
     LW_LAUNCHED("lw_frame_ids");
+    count_launches(1);
     return LW_OK;
 }
 
@@ -544,6 +551,7 @@ int lw_map_clear(lw_map* map, void* stream) {
     if (r != LW_OK) return r;
     k_map_clear<<<8 * device_sms(), 256, 0, (cudaStream_t)stream>>>(*map);
     LW_LAUNCHED("lw_map_clear");
+    count_launches(1);
     return LW_OK;
 }
 

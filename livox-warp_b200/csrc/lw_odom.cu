@@ -571,11 +571,13 @@ __device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P,
             icp_search<2>(lane_g, wx, wy, wz, k, keys, rec, bd, bo, bs);
         else
             icp_search<1>(lane_g, wx, wy, wz, k, keys, rec, bd, bo, bs);
+        // groups of one warp may run different trip counts: shuffle within this group's lanes only
+        const unsigned gmask = ((1u << GN_G) - 1u) << (lane & ~(GN_G - 1));
 #pragma unroll
         for (int off = GN_G / 2; off > 0; off >>= 1) {
-            float od = __shfl_xor_sync(0xffffffffu, bd, off);
-            int oo = __shfl_xor_sync(0xffffffffu, bo, off);
-            int os = __shfl_xor_sync(0xffffffffu, bs, off);
+            float od = __shfl_xor_sync(gmask, bd, off);
+            int oo = __shfl_xor_sync(gmask, bo, off);
+            int os = __shfl_xor_sync(gmask, bs, off);
             if (od < bd || (od == bd && oo < bo)) {
                 bd = od;
                 bo = oo;
@@ -1165,6 +1167,7 @@ static int launch_gn(const float* ds4, const int32_t* n_dev, const lw_odom_param
     void* args[] = {(void*)&dsp, (void*)&n_dev, (void*)&p, (void*)&st, (void*)&keys, (void*)&rec,
                     (void*)&mask, (void*)&g, (void*)&which};
     LW_CUDA(cudaLaunchCooperativeKernel((const void*)k_gn, dim3(grid), dim3(GN_THREADS), args, 0, s));
+    count_launches(1);
     return LW_OK;
 }
 
@@ -1190,6 +1193,7 @@ int lw_frame_append(const float* xyz, int32_t xyz_stride, const uint32_t* attr, 
         return LW_OK;
     }
     float idt = (float)inv_dt;
+    ProfScope prof("frame_append", s);
     k_append_count<<<nt, TILE, 0, s>>>(t, n, idt, k_min, k_open, fb->tiles);
     if (xyz_stride == 3)
         k_append_scatter<3><<<nt, TILE, 0, s>>>(xyz, attr, t, n, idt, k_min, k_open, fb->tiles, *fb);
@@ -1197,12 +1201,14 @@ int lw_frame_append(const float* xyz, int32_t xyz_stride, const uint32_t* attr, 
         k_append_scatter<4><<<nt, TILE, 0, s>>>(xyz, attr, t, n, idt, k_min, k_open, fb->tiles, *fb);
     k_append_total<<<1, 256, 0, s>>>(fb->tiles, nt, fb->count);
     LW_LAUNCHED("lw_frame_append");
+    count_launches(3);
     return LW_OK;
 }
 
 int lw_frame_reset(lw_frame_buf* fb, void* stream) {
     k_zero_count<<<1, 1, 0, (cudaStream_t)stream>>>(fb->count);
     LW_LAUNCHED("lw_frame_reset");
+    count_launches(1);
     return LW_OK;
 }
 
@@ -1224,6 +1230,7 @@ int lw_deskew(const float* raw, float* out, const int32_t* m_dev, int64_t m_ub, 
     int grid = blocks_for(m_ub, 256, 8 * device_sms());
     k_thin_a<<<grid, 256, 0, (cudaStream_t)stream>>>(fb, m_dev, a, nullptr, tw, nullptr, nullptr, 0);
     LW_LAUNCHED("lw_deskew");
+    count_launches(1);
     return LW_OK;
 }
 
@@ -1245,6 +1252,7 @@ int lw_thin(lw_frame_buf* fb, const int32_t* m_dev, int64_t m_ub, double inv_v, 
     k_thin_b<<<nt, TILE, 0, s>>>(*fb, m_dev, nullptr);
     k_thin_c<<<nt, TILE, 0, s>>>(*fb, m_dev, n_ds_dev, nullptr);
     LW_LAUNCHED("lw_thin");
+    count_launches(3);
     return LW_OK;
 }
 
@@ -1269,6 +1277,7 @@ static int reg_insert_launch(const float* xyz4, const uint32_t* attr, const int3
     k_reg_b<<<grid, 256, 0, s>>>(p4, n_dev, n_ub, a, T_dev, *reg, pslot, gate);
     k_reg_d<<<grid, 256, 0, s>>>(n_dev, n_ub, *reg, pslot, *rp, gate);
     LW_LAUNCHED("reg insert");
+    count_launches(3);
     return LW_OK;
 }
 
@@ -1286,6 +1295,7 @@ int lw_reg_refresh_all(lw_regmap* reg, const lw_rec_params* rp, void* stream) {
     if (!reg || !rp) return set_error(LW_EINVAL, "lw_reg_refresh_all: null argument");
     k_reg_refresh_all<<<4 * device_sms(), 256, 0, (cudaStream_t)stream>>>(*reg, *rp);
     LW_LAUNCHED("lw_reg_refresh_all");
+    count_launches(1);
     return LW_OK;
 }
 
@@ -1314,12 +1324,14 @@ int lw_icp_accumulate(const float* ds4, const int32_t* n_dev, int64_t n_ub, cons
                                            reg->rec, gn->part);
     k_acc_reduce<<<1, LW_ACC_STRIDE, 0, s>>>(gn->part, grid, cf[0], cf[1], cf[2], out64);
     LW_LAUNCHED("lw_icp_accumulate");
+    count_launches(2);
     return LW_OK;
 }
 
 int lw_icp_solve(const float* ds4, const int32_t* n_dev, const lw_odom_params* prm, lw_odom_state* st,
                  const lw_regmap* reg, lw_gn_scratch* gn, void* stream) {
     if (!ds4 || !n_dev || !prm || !st || !reg || !gn) return set_error(LW_EINVAL, "lw_icp_solve: null argument");
+    ProfScope prof("gn", (cudaStream_t)stream);
     return launch_gn(ds4, n_dev, prm, st, reg, gn, 2, (cudaStream_t)stream);  // ungated
 }
 
@@ -1340,29 +1352,55 @@ int lw_odom_finalize(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_odom
     Tw6 tw{};
     lw_rec_params rp = rec_params(prm);
 
-    k_ctl_begin<<<1, 1, 0, s>>>(k, *prm, st, fb->count);
+    {
+        ProfScope prof("control", s);
+        k_ctl_begin<<<1, 1, 0, s>>>(k, *prm, st, fb->count);
+    }
     // first registration: deskew with the predicted motion, thin, Gauss-Newton
-    k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, ta, st, tw, nullptr, &st->run_reg, 1);
-    k_thin_b<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->run_reg);
-    k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->run_reg);
-    int r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 0, s);
+    {
+        ProfScope prof("thin", s);
+        k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, ta, st, tw, nullptr, &st->run_reg, 1);
+        k_thin_b<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->run_reg);
+        k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->run_reg);
+    }
+    int r;
+    {
+        ProfScope prof("gn", s);
+        r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 0, s);
+    }
     if (r != LW_OK) return r;
     // re-deskew with the solved motion and register again when it moved enough
-    k_ctl_mid<<<1, 1, 0, s>>>(*prm, st);
-    k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, ta, st, tw, &st->redo, &st->redo, 1);
-    k_thin_b<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->redo);
-    k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->redo);
-    r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 1, s);
+    {
+        ProfScope prof("control", s);
+        k_ctl_mid<<<1, 1, 0, s>>>(*prm, st);
+    }
+    {
+        ProfScope prof("thin", s);
+        k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, ta, st, tw, &st->redo, &st->redo, 1);
+        k_thin_b<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->redo);
+        k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->redo);
+    }
+    {
+        ProfScope prof("gn", s);
+        r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 1, s);
+    }
     if (r != LW_OK) return r;
     // keyframe, velocity, pose table, trajectory
-    k_ctl_end<<<1, 1, 0, s>>>(*prm, st, *pt, epoch, traj, traj_cap);
+    {
+        ProfScope prof("control", s);
+        k_ctl_end<<<1, 1, 0, s>>>(*prm, st, *pt, epoch, traj, traj_cap);
+    }
     // keyframe insert with the frame's final pose (odom.py:719-727), through the state's float64 pose
     RegArgs a = reg_args(nullptr, prm->reg_voxel, prm->max_range, prm->ret_mask);
     const float4* p4 = reinterpret_cast<const float4*>(fb->f_xyz);
-    k_reg_a<<<grid, 256, 0, s>>>(p4, fb->f_attr, &st->m, m_ub, a, st->T, *reg, fb->ds_slot, &st->do_insert);
-    k_reg_b<<<grid, 256, 0, s>>>(p4, &st->m, m_ub, a, st->T, *reg, fb->ds_slot, &st->do_insert);
-    k_reg_d<<<grid, 256, 0, s>>>(&st->m, m_ub, *reg, fb->ds_slot, rp, &st->do_insert);
+    {
+        ProfScope prof("reg_insert", s);
+        k_reg_a<<<grid, 256, 0, s>>>(p4, fb->f_attr, &st->m, m_ub, a, st->T, *reg, fb->ds_slot, &st->do_insert);
+        k_reg_b<<<grid, 256, 0, s>>>(p4, &st->m, m_ub, a, st->T, *reg, fb->ds_slot, &st->do_insert);
+        k_reg_d<<<grid, 256, 0, s>>>(&st->m, m_ub, *reg, fb->ds_slot, rp, &st->do_insert);
+    }
     LW_LAUNCHED("lw_odom_finalize");
+    count_launches(12);  // plus the two Gauss-Newton launches counted by launch_gn
     return LW_OK;
 }
 
@@ -1374,6 +1412,7 @@ int lw_odom_predict_poses(int32_t k0, int32_t k1, int32_t current, const lw_odom
     if (n > LW_POSE_SLOTS) n = LW_POSE_SLOTS;
     k_predict_poses<<<blocks_for(n, 256, 256), 256, 0, (cudaStream_t)stream>>>(k0, k1, current, st, *pt, epoch);
     LW_LAUNCHED("lw_odom_predict_poses");
+    count_launches(1);
     return LW_OK;
 }
 
@@ -1402,6 +1441,7 @@ int lw_odom_reset(const double* T0_host, lw_odom_state* st, lw_regmap* reg, int3
         LW_CUDA(cudaMemsetAsync(reg->stats, 0, 2 * sizeof(int32_t), s));
     }
     LW_LAUNCHED("lw_odom_reset");
+    count_launches(clear_map && reg ? 3 : 1);
     return LW_OK;
 }
 
@@ -1409,6 +1449,7 @@ int lw_odom_restart_clock(lw_odom_state* st, void* stream) {
     if (!st) return set_error(LW_EINVAL, "lw_odom_restart_clock: null argument");
     k_restart_clock<<<1, 1, 0, (cudaStream_t)stream>>>(st);
     LW_LAUNCHED("lw_odom_restart_clock");
+    count_launches(1);
     return LW_OK;
 }
 

@@ -100,6 +100,10 @@ _SIGS = {
     "lw_version": (C.c_char_p, []),
     "lw_last_error": (C.c_char_p, []),
     "lw_device_sms": (i32, [C.POINTER(i32)]),
+    "lw_prof_enable": (i32, [i32]),
+    "lw_prof_read": (i32, [C.c_char_p, C.POINTER(f64), C.POINTER(i64)]),
+    "lw_prof_reset": (i32, []),
+    "lw_launches": (i64, [i32]),
     "lw_frame_append": (i32, [P, i32, P, P, i64, f64, i32, i32, C.POINTER(FrameBuf), P]),
     "lw_frame_reset": (i32, [C.POINTER(FrameBuf), P]),
     "lw_odom_finalize": (i32, [i32, i64, C.POINTER(OdomParams), P, C.POINTER(FrameBuf), C.POINTER(RegMap),
@@ -177,3 +181,23 @@ def f64_array(values) -> C.Array:
 def f32_array(values) -> C.Array:
     vals = [float(v) for v in values]
     return (f32 * len(vals))(*vals)
+
+
+def prof_enable(on: bool = True):
+    call("lw_prof_enable", int(on))
+
+
+def prof_read(name: str) -> tuple[float, int]:
+    """(summed ms, launches) of the named launches since the last reset (waits for them)."""
+    ms, cnt = f64(0.0), i64(0)
+    call("lw_prof_read", name.encode(), C.byref(ms), C.byref(cnt))
+    return ms.value, cnt.value
+
+
+def prof_reset():
+    call("lw_prof_reset")
+
+
+def launches(reset: bool = False) -> int:
+    """Kernels launched by the library since the last reset."""
+    return int(load().lw_launches(int(reset)))

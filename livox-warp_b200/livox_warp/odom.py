@@ -109,6 +109,10 @@ class Odometry:
         self.redeskew = True
         self.epoch = 0
         self._rec_key = None
+        self._integrate = None
+        # the frame's point count as the device state holds it (an int32 view into the state buffer)
+        off = _lib.OdomState.m.offset
+        self._m_dev = self._state[off:off + 4].view(torch.int32)
         self.reset(np.eye(4, dtype=np.float64))
 
     # ---- parameters ---------------------------------------------------------------------------------------
@@ -285,6 +289,13 @@ class Odometry:
             self._poses(self.k_open, self.k_open + 1, 0)
             self.k_pred = max(self.k_pred, self.k_open)
 
+    def integrate(self, view, voxel: float, carve_every: int = 1, max_range: float = 40.0, max_steps: int = 4096):
+        """Insert every finalised frame into the pipeline's integration map and carve its rays, on the device,
+        straight after registration (what the viewer's on_frame does: app.py:557-563) -- without a host round
+        trip. carve_every = 0 inserts without carving; view = None turns it off."""
+        self._integrate = None if view is None else (view, float(voxel), int(carve_every), float(max_range),
+                                                     int(max_steps))
+
     def flush(self, on_frame=None):
         """Finalise the open frame now (the end of a recording)."""
         if self.k_open is not None and self._m_ub > 0:
@@ -296,6 +307,15 @@ class Odometry:
         _lib.call("lw_odom_finalize", int(k), max(self._m_ub, 1), _byref(self.params()), _lib.ptr(self._state),
                   _byref(self.fbuf), _byref(self.regmap), _byref(self.gn), _byref(self.pipe.pose_table), self.epoch,
                   _lib.ptr(self._traj), TRAJ_CAP, self._sp())
+        if self._integrate is not None:
+            view, voxel, every, max_range, max_steps = self._integrate
+            m_ub = max(self._m_ub, 1)
+            with torch.cuda.stream(self.stream):
+                self.pipe.map_insert(self.f_xyz, self.f_attr, self.f_t, self.f_frame, m_ub, view, voxel,
+                                     n_dev=self._m_dev)
+                if every > 0:
+                    self.pipe.carve(self.f_xyz, self.f_attr, self.f_frame, m_ub, voxel, every, max_range, max_steps,
+                                    n_dev=self._m_dev)
         if on_frame is not None:
             st = self.read_state()
             self._ms = (time.perf_counter() - t0) * 1e3

@@ -1,0 +1,99 @@
+"""Algorithmic (compulsory) bytes of the per-frame kernels: the numerator of the roofline the benchmark reports.
+
+Each input is read once, each output written once, and each touched table record is read (and written, if
+modified) once per launch. The distinct records a launch must touch are counted here on the host with numpy
+from the frame's points, its solved pose and the table's occupied keys, per kernel:
+
+  Gauss-Newton registration (one launch = every iteration of a frame), per iteration:
+      16 B per thinned point (x, y, z, range)
+    +  8 B per distinct neighbour key probed (the union of the (2 reach + 1)^3 neighbourhoods)
+    + 16 B per distinct occupied voxel among them (its mean and count)
+    + 64 B per distinct voxel a point is matched to (its precision record)
+    + 2 * 64 * 8 B per CTA (the float64 partials written and read back)
+  carving (one launch = one frame's rays):
+      20 B per traced ray (x, y, z, attr, frame id)
+    + 12 B per distinct voxel the rays visit (key + hit count)
+    + 32 B per distinct occupied voxel among them (the fixed-point centroid sums)
+    +  4 B per miss counter written (bounded by the occupied visited voxels)
+  integration insert (one launch = one batch):
+      24 B per point (x, y, z, attr, t, frame id) + 2 * 64 B per distinct voxel touched (key, count, sums, times)
+
+The counts use the solved pose for every iteration and sample each ray every quarter voxel, so they are
+estimates of the compulsory traffic, not measurements: ncu's dram__bytes is the measured counterpart.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+BIAS = 1 << 20
+KMASK = (1 << 21) - 1
+
+
+def keys_of(ijk: np.ndarray) -> np.ndarray:
+    ijk = ijk.astype(np.int64)
+    return (((ijk[:, 0] + BIAS) & KMASK) | (((ijk[:, 1] + BIAS) & KMASK) << 21) |
+            (((ijk[:, 2] + BIAS) & KMASK) << 42))
+
+
+def _world(xyz: np.ndarray, T: np.ndarray) -> np.ndarray:
+    return xyz[:, :3].astype(np.float64) @ T[:3, :3].T + T[:3, 3]
+
+
+def thin_host(xyz_sensor: np.ndarray, voxel: float, min_range: float = 0.3, max_range: float = 60.0) -> np.ndarray:
+    """First point of every half-voxel (the thinning rule), on the host."""
+    r = np.linalg.norm(xyz_sensor[:, :3], axis=1)
+    ok = (r >= min_range) & (r <= max_range)
+    idx = np.nonzero(ok)[0]
+    k = keys_of(np.floor(xyz_sensor[idx, :3] * (2.0 / voxel)).astype(np.int64))
+    _, first = np.unique(k, return_index=True)
+    return xyz_sensor[idx[np.sort(first)]]
+
+
+def gn_bytes(ds_sensor: np.ndarray, T: np.ndarray, occupied_keys: np.ndarray, voxel: float, iters: int,
+             grid: int, wide_iters: int = 3) -> float:
+    """Compulsory bytes of one registration launch (all its iterations)."""
+    w = _world(ds_sensor, T)
+    base = np.floor(w / voxel).astype(np.int64)
+    occ = np.sort(occupied_keys)
+    total = 0.0
+    own = keys_of(base)
+    matched = np.unique(own[np.isin(own, occ, assume_unique=False)])
+    for reach in (2, 1):
+        n_it = min(iters, wide_iters) if reach == 2 else max(iters - wide_iters, 0)
+        if n_it == 0:
+            continue
+        r = np.arange(-reach, reach + 1)
+        off = np.stack(np.meshgrid(r, r, r, indexing="ij"), -1).reshape(-1, 3)
+        probed = np.unique(keys_of((base[:, None, :] + off[None, :, :]).reshape(-1, 3)))
+        v_occ = np.count_nonzero(np.isin(probed, occ))
+        per_it = 16 * len(ds_sensor) + 8 * len(probed) + 16 * v_occ + 64 * len(matched) + 2 * grid * 64 * 8
+        total += n_it * per_it
+    return float(total)
+
+
+def carve_bytes(xyz_sensor: np.ndarray, T: np.ndarray, occupied_keys: np.ndarray, voxel: float, every: int = 1,
+                max_range: float = 40.0) -> float:
+    """Compulsory bytes of one carving launch over a frame's rays."""
+    p = xyz_sensor[::every, :3].astype(np.float64)
+    w = _world(p, T)
+    o = T[:3, 3]
+    d = w - o
+    L = np.linalg.norm(d, axis=1)
+    ok = (L >= 0.05) & (L <= max_range)
+    d, L = d[ok] / L[ok, None], L[ok]
+    stop = L - np.maximum(3.0 * voxel, 0.03 * L)
+    step = voxel / 4.0
+    n_s = np.maximum((stop / step).astype(np.int64), 0)
+    ray = np.repeat(np.arange(len(L)), n_s)
+    t = (np.arange(n_s.sum()) - np.repeat(np.cumsum(n_s) - n_s, n_s) + 0.5) * step
+    pts = o + d[ray] * t[:, None]
+    visited = np.unique(keys_of(np.floor(pts / voxel).astype(np.int64)))
+    occ = np.count_nonzero(np.isin(visited, np.sort(occupied_keys)))
+    return float(20 * len(p) + 12 * len(visited) + 32 * occ + 4 * occ)
+
+
+def map_insert_bytes(xyz_sensor: np.ndarray, T: np.ndarray, voxel: float) -> float:
+    w = _world(xyz_sensor, T)
+    touched = np.unique(keys_of(np.floor(w / voxel).astype(np.int64)))
+    return float(24 * len(w) + 2 * 64 * len(touched))

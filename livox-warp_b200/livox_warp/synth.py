@@ -224,12 +224,13 @@ class ConstantVelocity:
 
 
 class Handheld:
-    """A smooth handheld path: rest for `rest` s, then a Catmull-Rom spline through random free waypoints,
-    timed so the speed stays under v_max, with yaw a smooth random function under w_max and small pitch/roll.
+    """A smooth handheld path: rest for `rest` s, then a Catmull-Rom spline through random free waypoints at a
+    cruise speed under v_max, with the sensor turned toward a look-at point drifting around the room's middle
+    (yaw rate under w_max, yaw acceleration under a_max), pitched ~10 deg down, with small pitch/roll sway.
     """
 
     def __init__(self, scene: Scene, seed: int, duration: float, v_max: float = 1.0, w_max_deg: float = 60.0,
-                 rest: float = 1.0, height=(1.2, 1.7), margin: float = 0.7):
+                 rest: float = 1.0, height=(1.2, 1.7), margin: float = 0.7, a_max_deg: float = 120.0):
         rng = np.random.default_rng(seed)
         self.rest, self.duration = rest, duration
         pts = []
@@ -255,22 +256,52 @@ class Handheld:
         seglen = np.linalg.norm(np.diff(xyz, axis=0), axis=1)
         s = np.concatenate([[0.0], np.cumsum(seglen)])
         T_move = duration - rest
-        v = min(v_max * 0.95, s[-1] / max(T_move * 0.6, 1e-3))
+        v = min(v_max * 0.7, s[-1] / max(T_move * 0.6, 1e-3))  # cruise; the spline's bends stay under v_max
         ramp = 0.8  # s to reach cruise speed, so the first moving frames look like a hand starting to move
         def s_of(tau):
             tau = np.clip(tau, 0, None)
             return np.where(tau < ramp, v * tau * tau / (2 * ramp), v * (tau - ramp / 2))
         self._s, self._xyz, self._s_of = s, xyz, s_of
-        # yaw: sum of random sinusoids scaled to w_max
-        self.freqs = rng.uniform(0.05, 0.3, 4)
-        self.phases = rng.uniform(0, 2 * math.pi, 4)
-        amps = rng.uniform(0.5, 1.0, 4)
-        tt = np.linspace(0, duration, 4000)
-        w = sum(a * 2 * math.pi * f * np.cos(2 * math.pi * f * tt + ph)
-                for a, f, ph in zip(amps, self.freqs, self.phases))
-        self.amps = amps * (math.radians(w_max_deg) * 0.95 / max(np.abs(w).max(), 1e-9))
-        self.yaw0 = rng.uniform(0, 2 * math.pi)
-        self.tilt = rng.uniform(-1, 1, 4) * math.radians(4.0)
+        # yaw: a handheld scan keeps the room in view -- the sensor points from where it is toward a look-at
+        # point that drifts around the room's middle, smoothed over 1 s (causal) and rate-limited to w_max, plus
+        # a small random sway; a slight downward pitch sees the floor ahead
+        self.dt = 0.002
+        tt = np.arange(0.0, duration + 1.0, self.dt)
+        pos = self._position(tt)
+        mid = 0.5 * (scene.room_lo + scene.room_hi)
+        half = 0.15 * (scene.room_hi - scene.room_lo)
+        lf, lph = rng.uniform(0.02, 0.06, 2), rng.uniform(0, 2 * math.pi, 2)
+        centre = np.stack([mid[0] + half[0] * np.sin(2 * math.pi * lf[0] * tt + lph[0]),
+                           mid[1] + half[1] * np.sin(2 * math.pi * lf[1] * tt + lph[1])], axis=1)
+        # look across the room: through a point near its middle, toward the far side
+        away = centre - pos[:, :2]
+        near = np.linalg.norm(away, axis=1) < 0.8
+        heading = np.arctan2(away[:, 1], away[:, 0])
+        for i in range(1, len(heading)):  # right at the middle: keep the last direction
+            if near[i]:
+                heading[i] = heading[i - 1]
+        heading = np.unwrap(heading)
+        heading[tt <= rest] = heading[int(np.searchsorted(tt, rest))]  # at rest the sensor holds still
+        win = max(1, int(1.0 / self.dt))
+        smooth = np.convolve(np.pad(heading, (win - 1, 0), mode="edge"), np.ones(win) / win, mode="valid")
+        sway_f, sway_ph = rng.uniform(0.1, 0.3, 2), rng.uniform(0, 2 * math.pi, 2)
+        sway = sum(math.radians(8.0) * np.sin(2 * math.pi * f * tt + ph) for f, ph in zip(sway_f, sway_ph))
+        want = smooth + sway * (tt > rest)
+        # a critically damped follower with the yaw rate capped at w_max and the yaw acceleration at a_max, so
+        # turns start and stop the way a hand moves (no step in angular velocity)
+        wmax = math.radians(w_max_deg) * 0.95
+        amax = math.radians(a_max_deg)
+        yaw = np.empty_like(want)
+        yaw[0] = want[0]
+        rate = 0.0
+        k_p = 4.0  # 1/s: how fast the follower closes a heading error
+        for i in range(1, len(want)):
+            target = np.clip(k_p * (want[i] - yaw[i - 1]), -wmax, wmax)
+            rate += np.clip(target - rate, -amax * self.dt, amax * self.dt)
+            yaw[i] = yaw[i - 1] + rate * self.dt
+        self._yaw = yaw
+        self.tilt = rng.uniform(-1, 1, 4) * math.radians(3.0)
+        self.pitch0 = math.radians(10.0)
 
     @staticmethod
     def _length(pts):
@@ -284,18 +315,20 @@ class Handheld:
         return 0.5 * ((2 * p1) + (-p0 + p2) * f + (2 * p0 - 5 * p1 + 4 * p2 - p3) * f ** 2 +
                       (-p0 + 3 * p1 - 3 * p2 + p3) * f ** 3)
 
-    def poses(self, t: np.ndarray) -> np.ndarray:
-        t = np.asarray(t, np.float64)
-        tau = np.clip(t - self.rest, 0.0, None)
+    def _position(self, t: np.ndarray) -> np.ndarray:
+        tau = np.clip(np.asarray(t, np.float64) - self.rest, 0.0, None)
         s = np.minimum(self._s_of(tau), self._s[-1])
         idx = np.clip(np.searchsorted(self._s, s), 1, len(self._s) - 1)
         f = ((s - self._s[idx - 1]) / np.maximum(self._s[idx] - self._s[idx - 1], 1e-12))[:, None]
-        p = self._xyz[idx - 1] * (1 - f) + self._xyz[idx] * f
+        return self._xyz[idx - 1] * (1 - f) + self._xyz[idx] * f
+
+    def poses(self, t: np.ndarray) -> np.ndarray:
+        t = np.asarray(t, np.float64)
+        p = self._position(t)
+        yaw = np.interp(t, np.arange(len(self._yaw)) * self.dt, self._yaw)
         tm = np.where(t > self.rest, t - self.rest, 0.0)
-        yaw = self.yaw0 + sum(a * (np.sin(2 * math.pi * fr * tm + ph) - math.sin(ph))
-                              for a, fr, ph in zip(self.amps, self.freqs, self.phases))
-        pitch = self.tilt[0] * np.sin(0.3 * tm) + self.tilt[1] * np.sin(0.17 * tm) * (tm > 0)
-        roll = self.tilt[2] * np.sin(0.23 * tm) + self.tilt[3] * np.sin(0.11 * tm) * (tm > 0)
+        pitch = self.pitch0 + self.tilt[0] * np.sin(0.3 * tm) + self.tilt[1] * np.sin(0.17 * tm)
+        roll = self.tilt[2] * np.sin(0.23 * tm) + self.tilt[3] * np.sin(0.11 * tm)
         R = Rotation.from_euler("zyx", np.stack([yaw, pitch, roll], axis=1)).as_matrix()
         return _pose(R, p)
 

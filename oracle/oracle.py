@@ -48,6 +48,9 @@ _lib = None
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
+        # the OpenMP runtime reads these when the library loads: never spin-wait on a shared host
+        os.environ.setdefault("OMP_WAIT_POLICY", "PASSIVE")
+        os.environ.setdefault("GOMP_SPINCOUNT", "0")
         if not LIB.exists():
             import importlib.util
             spec = importlib.util.spec_from_file_location("lw_oracle_build", HERE / "build.py")
@@ -82,8 +85,24 @@ def _p(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
 
 
+def host_cores() -> int:
+    """CPUs this process may really use: its affinity set, capped by a cgroup CPU quota when one is set."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        n = os.cpu_count() or 1
+    try:
+        quota, period = open("/sys/fs/cgroup/cpu.max").read().split()[:2]
+        if quota != "max":
+            n = min(n, max(1, int(int(quota) // int(period))))
+    except (OSError, ValueError):
+        pass
+    return max(1, n)
+
+
 def threads() -> int:
-    return int(os.environ.get("LW_ORACLE_THREADS", os.cpu_count() or 1))
+    """OpenMP threads of the oracle: LW_ORACLE_THREADS, else the usable cores (at most 8)."""
+    return int(os.environ.get("LW_ORACLE_THREADS", min(host_cores(), 8)))
 
 
 # ---- kernels ------------------------------------------------------------------------------------------------

@@ -1,0 +1,118 @@
+"""Generate the golden fixtures of tests/golden/ from the reference's own code (run in a container that has the
+reference checkout; the fixtures are committed, the GPU tests only read them).
+
+    python tests/golden/make_golden.py /path/to/livox-warp
+
+The reference's modules import NVIDIA Warp at the top, which is not installed, so they cannot be imported.
+Their pure numpy / scipy functions are executed from source instead: this script parses each module with `ast`,
+takes the named function definitions (and the module constants they read) verbatim, and runs them in a fresh
+namespace on seeded inputs. What they produce pins the CPU oracle's restatement (oracle/oracle.py) and the
+device solve:
+
+  host_solve.npz    odom.py _sym6, _twist_between, _apply_twist, _body_twist, _twist_matrix, _sensor_basis,
+                    _constrained_step; localize.py _twist_apply, _rotz, pose_difference; gpu.py mount_matrix.
+"""
+
+from __future__ import annotations
+
+import ast
+import sys
+from pathlib import Path
+
+import numpy as np
+from scipy.spatial.transform import Rotation
+
+HERE = Path(__file__).resolve().parent
+
+
+def extract(src_path: Path, names: list[str], consts: list[str] = ()) -> dict:
+    """Run the named top-level functions / assignments of a module in a namespace with numpy and scipy."""
+    tree = ast.parse(src_path.read_text())
+    keep = []
+    for node in tree.body:
+        if isinstance(node, ast.FunctionDef) and node.name in names:
+            keep.append(node)
+        elif isinstance(node, ast.Assign) and any(isinstance(t, ast.Name) and t.id in consts for t in node.targets):
+            keep.append(node)
+    found = {n.name for n in keep if isinstance(n, ast.FunctionDef)}
+    missing = set(names) - found
+    if missing:
+        raise KeyError(f"{src_path.name}: not found {sorted(missing)}")
+    mod = ast.Module(body=keep, type_ignores=[])
+    ns = {"np": np, "Rotation": Rotation, "math": __import__("math")}
+    exec(compile(mod, str(src_path), "exec"), ns)
+    return ns
+
+
+def random_pose(rng, t_scale=5.0, r_scale=1.0):
+    T = np.eye(4)
+    T[:3, :3] = Rotation.from_rotvec(rng.normal(0, r_scale, 3)).as_matrix()
+    T[:3, 3] = rng.normal(0, t_scale, 3)
+    return T
+
+
+def host_solve(ref: Path) -> dict:
+    pkg = ref / "python" / "livox_warp"
+    odom = extract(pkg / "odom.py", ["_sym6", "_twist_between", "_apply_twist", "_body_twist", "_twist_matrix",
+                                      "_sensor_basis", "_constrained_step"], ["_TRIU6"])
+    loc = extract(pkg / "localize.py", ["_twist_apply", "_rotz", "pose_difference"])
+    gpu = extract(pkg / "gpu.py", ["mount_matrix"])
+    rng = np.random.default_rng(20261203)
+    out = {}
+    n = 24
+    up = rng.normal(0, 1, (n, 21))
+    out["sym6_in"], out["sym6_out"] = up, np.stack([odom["_sym6"](u) for u in up])
+    A = np.stack([random_pose(rng) for _ in range(n)])
+    B = np.stack([A[i] @ random_pose(rng, 0.1, 0.05) for i in range(n)])
+    out["tb_from"], out["tb_to"] = A, B
+    out["tb_out"] = np.stack([odom["_twist_between"](A[i], B[i]) for i in range(n)])
+    d = rng.normal(0, 0.05, (n, 6))
+    out["apply_T"], out["apply_delta"] = A, d
+    out["apply_out"] = np.stack([odom["_apply_twist"](A[i], d[i]) for i in range(n)])
+    out["apply_loc_out"] = np.stack([loc["_twist_apply"](A[i], d[i]) for i in range(n)])
+    D = np.stack([random_pose(rng, 0.1, 0.05) for _ in range(n)])
+    out["body_in"], out["body_out"] = D, np.stack([odom["_body_twist"](x) for x in D])
+    xi = rng.normal(0, 0.05, (n, 6))
+    out["twm_in"], out["twm_out"] = xi, np.stack([odom["_twist_matrix"](x) for x in xi])
+    L = rng.uniform(1.0, 8.0, n)
+    out["sb_T"], out["sb_L"] = A, L
+    out["sb_out"] = np.stack([odom["_sensor_basis"](A[i], L[i]) for i in range(n)])
+    # constrained steps: normal equations of random point-to-plane problems, some with degenerate directions
+    cs_A, cs_rhs, cs_Hg, cs_T, cs_L, cs_thr, cs_pred, cs_out, cs_kept = [], [], [], [], [], [], [], [], []
+    for i in range(n):
+        J = rng.normal(0, 1, (200, 6))
+        if i % 3 == 1:
+            J[:, 3] *= 1e-4  # a direction the geometry hardly constrains
+        if i % 3 == 2:
+            J[:, 0] *= 1e-4
+            J[:, 4] *= 1e-4
+        H = J.T @ J * (5.0e4 if i % 3 == 0 else 50.0)
+        Hg = H * rng.uniform(0.5, 1.0)
+        rhs = rng.normal(0, 10, 6)
+        T = A[i]
+        pred = rng.normal(0, 0.01, 6)
+        thr = 3000.0
+        dg = np.diag(H)
+        Am = H + np.diag(1e-9 * dg.mean() + 1e-3 * dg)
+        step, (_, _, kept) = odom["_constrained_step"](Am, rhs, Hg, T, L[i], thr, pred)
+        cs_A.append(Am), cs_rhs.append(rhs), cs_Hg.append(Hg), cs_T.append(T), cs_L.append(L[i])
+        cs_thr.append(thr), cs_pred.append(pred), cs_out.append(step), cs_kept.append(kept)
+    out.update(cs_A=np.stack(cs_A), cs_rhs=np.stack(cs_rhs), cs_Hg=np.stack(cs_Hg), cs_T=np.stack(cs_T),
+               cs_L=np.array(cs_L), cs_thr=np.array(cs_thr), cs_pred=np.stack(cs_pred), cs_out=np.stack(cs_out),
+               cs_kept=np.stack(cs_kept))
+    ang = rng.uniform(-np.pi, np.pi, n)
+    out["rotz_in"], out["rotz_out"] = ang, np.stack([loc["_rotz"](a) for a in ang])
+    out["pd_out"] = np.array([loc["pose_difference"](A[i], B[i]) for i in range(n)])
+    mm = rng.uniform(-30, 30, (n, 6))
+    out["mount_in"], out["mount_out"] = mm, np.stack([gpu["mount_matrix"](*m) for m in mm])
+    return out
+
+
+def main():
+    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    np.savez_compressed(HERE / "host_solve.npz", **host_solve(ref))
+    print("wrote", HERE / "host_solve.npz")
+
+
+if __name__ == "__main__":
+    main()

@@ -70,7 +70,7 @@ def test_map_insert_and_carve_bit_exact(stride4):
     _feed(pipe, om, poses, frames, traj, 10, view, every=1, stride4=stride4)
     torch.cuda.synchronize()
     g, o = _gpu_dict(pipe), om.as_dict()
-    assert len(g) == len(o) > 1000
+    assert len(g) == len(o) > 300
     assert g == o
     assert np.array_equal(pipe.map_stats.cpu().numpy(), om.stats)
     assert sum(v[4] for v in g.values()) > 0, "no ray pierced anything: the carving test is vacuous"
@@ -141,4 +141,4 @@ def test_map_clear():
     pipe.clear_map()
     torch.cuda.synchronize()
     assert int((pipe.map_keys != -1).sum()) == 0 and int(pipe.map_stats.abs().sum()) == 0
-    assert float(pipe.map_first.min()) == 1.0e30
+    assert float(pipe.map_first.min()) == float(np.float32(1.0e30))

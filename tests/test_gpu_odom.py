@@ -54,7 +54,7 @@ def test_thin_bit_exact(voxel):
     g = th(torch.from_numpy(x4).cuda(), torch.from_numpy(a.view(np.int32)).cuda(), float(inv_v), 0.3, 60.0,
            0b0011).cpu().numpy()
     o = oracle.thin(x4, a, inv_v, 0.3, 60.0, 0b0011)
-    assert len(g) == len(o) > 500
+    assert len(g) == len(o) > 200
     assert np.array_equal(g, o)
     # the thinning table is clean for the next frame
     assert int((th.ds_keys != -1).sum()) == 0
