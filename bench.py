@@ -48,7 +48,9 @@ MAP_VOXEL = 0.1
 MAP_SLOTS = 1 << 22
 REG_SLOTS = 1 << 21
 FRAME_CAP = 1 << 18
-SEED = 2026
+ROOM_SEED = 1   # the box room
+PATH_SEED = 31  # the handheld path (a sequence the float64 oracle tracks for the whole 60 s)
+SCAN_SEED = 3
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -56,30 +58,30 @@ L2_FLUSH_BYTES = 256 << 20
 
 
 def _gen_chunk(args):
-    seed, duration, k0, k1 = args
+    duration, k0, k1 = args
     from livox_warp import synth
 
-    scene = synth.box_room(seed)
-    traj = synth.Handheld(scene, seed + 1, duration)
-    return synth.frames(scene, traj, k1 - k0, RATE, seed + 2, start=k0)
+    scene = synth.box_room(ROOM_SEED)
+    traj = synth.Handheld(scene, PATH_SEED, duration)
+    return synth.frames(scene, traj, k1 - k0, RATE, SCAN_SEED, start=k0)
 
 
-def workload(n_frames: int, seed: int = SEED, procs: int | None = None):
+def workload(n_frames: int, procs: int | None = None):
     """The frames 0 .. n_frames-1 of the sequence (generated in a spawn pool before any CUDA call)."""
     from livox_warp import synth
 
-    duration = n_frames * FRAME_DT + 2.0
+    duration = max(n_frames * FRAME_DT + 2.0, 62.0)  # the path of the 600-frame sequence, whatever n_frames
     procs = procs or min(8, os.cpu_count() or 1)
     step = max(1, math.ceil(n_frames / (procs * 4)))
-    chunks = [(seed, duration, k, min(k + step, n_frames)) for k in range(0, n_frames, step)]
+    chunks = [(duration, k, min(k + step, n_frames)) for k in range(0, n_frames, step)]
     if procs > 1 and len(chunks) > 1:
         with mp.get_context("spawn").Pool(procs) as pool:
             parts = pool.map(_gen_chunk, chunks)
     else:
         parts = [_gen_chunk(c) for c in chunks]
     frames = [f for p in parts for f in p]
-    scene = synth.box_room(seed)
-    traj = synth.Handheld(scene, seed + 1, duration)
+    scene = synth.box_room(ROOM_SEED)
+    traj = synth.Handheld(scene, PATH_SEED, duration)
     return frames, traj
 
 
@@ -267,6 +269,26 @@ def roofline(res, frames, traj, warmup, steps, peak):
             "kernel_ms_share": {n: round(prof[n][0] / max(sum(v[0] for v in prof.values()), 1e-9), 4) for n in prof}}
 
 
+def pose_drift(odom, traj, oracle_poses: dict) -> dict:
+    """Registered poses against the simulated ground truth (every frame) and against the float64 oracle run on
+    the frames the CPU baseline processed."""
+    from scipy.spatial.transform import Rotation
+
+    def pose_error(A, B):
+        d = np.linalg.inv(A) @ B
+        return float(np.linalg.norm(d[:3, 3])), float(np.degrees(np.linalg.norm(Rotation.from_matrix(d[:3, :3]).as_rotvec())))
+
+    recs = odom.traj
+    gt = [pose_error(traj.poses(np.array([tm]))[0], T) for k, tm, T in recs]
+    orc = [pose_error(oracle_poses[k], T) for k, tm, T in recs if k in oracle_poses]
+    g = np.array(gt)
+    o = np.array(orc) if orc else np.zeros((1, 2))
+    return {"frames": len(recs), "gt_rmse_m": round(float(np.sqrt((g[:, 0] ** 2).mean())), 4),
+            "gt_max_m": round(float(g[:, 0].max()), 4), "gt_rot_rmse_deg": round(float(np.sqrt((g[:, 1] ** 2).mean())), 3),
+            "vs_fp64_oracle_frames": len(orc), "vs_fp64_oracle_max_m": round(float(o[:, 0].max()), 6),
+            "vs_fp64_oracle_max_deg": round(float(o[:, 1].max()), 5)}
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -291,6 +313,7 @@ def cpu_pipeline(frames, traj, warmup: int, budget_s: float, max_frames: int, th
     poses = np.tile(np.eye(4, dtype=np.float32).reshape(1, 16), (oracle.POSE_SLOTS, 1))
     view = _oracle_view(oracle)
     timed, t_total = 0, 0.0
+    poses_out = {}
     for k, (x, a, t) in enumerate(frames):
         t0 = time.perf_counter()
         raw = np.ascontiguousarray(np.concatenate([x, t[:, None]], 1), dtype=np.float32)
@@ -300,12 +323,13 @@ def cpu_pipeline(frames, traj, warmup: int, budget_s: float, max_frames: int, th
         om.insert(xyz4, a, t, fid, poses, view, MAP_VOXEL)
         om.carve(xyz4, a, fid, poses, MAP_VOXEL, every=1, nthreads=threads)
         dt = time.perf_counter() - t0
+        poses_out[k] = T
         if k >= warmup:
             timed += 1
             t_total += dt
             if timed >= max_frames or t_total >= budget_s:
                 break
-    return timed, t_total
+    return timed, t_total, poses_out
 
 
 def _oracle_view(oracle):
@@ -353,7 +377,7 @@ def main():
 
         threads = _o.host_cores()
         budget = max(30.0, min(150.0, 0.25 * a.steps))
-        timed, secs = cpu_pipeline(frames, traj, a.warmup, budget, a.steps, threads)
+        timed, secs, _ = cpu_pipeline(frames, traj, a.warmup, budget, a.steps, threads)
         v = timed / secs
         line = {"impl": "reference", "metric": metric, "value": round(v, 3), "unit": "frames/s", "n_gpus": a.gpus,
                 "steps": timed, "warmup": a.warmup, "ms_per_step": round(1e3 * secs / max(timed, 1), 3),
@@ -410,8 +434,9 @@ def main():
 
     threads = _o.host_cores()
     n_cpu = max(3, min(60, a.steps))
-    timed, secs = cpu_pipeline(frames, traj, a.warmup, a.cpu_budget, n_cpu, threads)
+    timed, secs, opose = cpu_pipeline(frames, traj, a.warmup, a.cpu_budget, n_cpu, threads)
     pts = config["points_per_frame"]
+    drift = pose_drift(res["odom"], traj, opose)
     line = {"metric": metric, "value": round(value, 3), "unit": "frames/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(ms_total / a.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 solve)", "data": "synthetic",
@@ -423,7 +448,7 @@ def main():
                              "sample": f"{timed} frames ({a.warmup}..{a.warmup + timed - 1}) of the same sequence "
                                        f"through the CPU oracle (C++/OpenMP kernels + numpy float64 solve), "
                                        f"{secs:.1f} s"},
-            "e2e": e2e, "gpu_launches": int(res["launches"]), "clocks": res["clocks"]}
+            "e2e": e2e, "gpu_launches": int(res["launches"]), "clocks": res["clocks"], "pose_drift": drift}
     print(json.dumps(line))
 
 
