@@ -200,6 +200,19 @@ int lw_deskew(const float* raw, float* out, const int32_t* m_dev, int64_t m_ub, 
 int lw_thin(lw_frame_buf* fb, const int32_t* m_dev, int64_t m_ub, double inv_v, double min_range,
             double max_range, int32_t ret_mask, int32_t* n_ds_dev, void* stream);
 
+/* Thinning for callers that cannot allocate device memory; it has no counterpart in the reference.
+ * A real-time sensor thread, or a host whose device memory is fixed at start-up (a driver callback, a plugin
+ * under a memory budget), must not call cudaMalloc on the frame path: an allocation can wait behind other
+ * device work for an unbounded time. This variant of lw_thin takes only the caller's points (xyz4 [m*4] with
+ * x, y, z, any; attr [m]) and output (ds4_out [m*4], *n_ds_dev); its tables live in one file-scope device
+ * array of about 1.8 MB that every GPU which loads the library holds until the process exits. At most 65536
+ * points per call: more is rejected with LW_ECAPACITY before any work is queued. The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. It allocates nothing. Calls share the one array and each clears its tables
+ * first, so calls that overlap on the GPU (two streams at once) race: serialise them. */
+int lw_thin_noalloc(const float* xyz4, const uint32_t* attr, int64_t m, double inv_v, double min_range,
+                    double max_range, int32_t ret_mask, float* ds4_out, int32_t* n_ds_dev, void* stream);
+
 /* Add n points posed by T to the registration map (odom.py:186-230) and refresh the derived record of
  * every voxel touched. xyz is [n*4]; n_dev is a device count or NULL (then n_ub is the count);
  * pslot is [n_ub] scratch. */

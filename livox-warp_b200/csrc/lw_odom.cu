@@ -5,6 +5,7 @@
 //
 // Reference: python/livox_warp/odom.py (kernels :97-384, host solve :387-455, Odometry :458-803) and the key /
 // hash / deskew helpers of python/livox_warp/gpu.py (:231-283).
+#include <mutex>
 #include "lw_common.cuh"
 #include "lw_linalg.cuh"
 
@@ -1454,3 +1455,100 @@ int lw_odom_restart_clock(lw_odom_state* st, void* stream) {
 }
 
 }  // extern "C"
+
+// =========================================================================================================
+// Thinning for callers that cannot allocate device memory.
+//
+// A host that embeds this library inside a real-time sensor thread, or inside a process whose device memory is
+// fixed at start-up (a driver callback, a plugin under a memory budget), must not call cudaMalloc on the frame
+// path: an allocation can block behind other work on the device and its latency is unbounded. This variant of
+// lw_thin takes only the caller's input points and output buffer; its working tables live in one file-scope
+// device array that every GPU holds from the moment the library is loaded until the process exits.
+// =========================================================================================================
+
+namespace lw {
+
+constexpr int64_t NOALLOC_THIN_MAX = 1 << 16;    // points one call may thin
+constexpr int64_t NOALLOC_THIN_SLOTS = 1 << 17;  // hash slots (a power of two >= twice the points)
+constexpr int64_t NOALLOC_THIN_TILES = NOALLOC_THIN_MAX / TILE + 2;
+// layout (in int64 units): keys [SLOTS] | win [SLOTS/2] | slot [MAX/2] | tiles + m [(TILES + 2)/2]
+constexpr int64_t NOALLOC_THIN_WORDS =
+    NOALLOC_THIN_SLOTS + NOALLOC_THIN_SLOTS / 2 + NOALLOC_THIN_MAX / 2 + (NOALLOC_THIN_TILES + 2) / 2 + 1;
+
+static __device__ __align__(256) int64_t g_thin_scratch[NOALLOC_THIN_WORDS];  // ~1.8 MB per device
+
+__global__ void k_noalloc_thin_reset(int64_t* keys, int32_t* win, int32_t* m_dev, int32_t m) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < NOALLOC_THIN_SLOTS;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        keys[i] = EMPTY_KEY;
+        win[i] = NO_INDEX;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *m_dev = m;
+}
+
+// The array's device address, looked up once per device with that device current (host code may not use
+// the symbol itself: on the host it names a stand-in, not device memory).
+static int noalloc_thin_scratch(int64_t** out) {
+    static std::mutex mu;
+    static int64_t* addr[256] = {};
+    int dev = 0;
+    LW_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return set_error(LW_EINVAL, "lw_thin_noalloc: device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> g(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_thin_scratch);
+        if (e != cudaSuccess) return check_cuda(e, "lw_thin_noalloc: cudaGetSymbolAddress");
+        addr[dev] = (int64_t*)p;
+    }
+    *out = addr[dev];
+    return LW_OK;
+}
+
+}  // namespace lw
+
+extern "C" int lw_thin_noalloc(const float* xyz4, const uint32_t* attr, int64_t m, double inv_v, double min_range,
+                               double max_range, int32_t ret_mask, float* ds4_out, int32_t* n_ds_dev, void* stream) {
+    using namespace lw;
+    if (!xyz4 || !attr || !ds4_out || !n_ds_dev) return set_error(LW_EINVAL, "lw_thin_noalloc: null argument");
+    if (m < 0 || m > NOALLOC_THIN_MAX)
+        return set_error(LW_ECAPACITY, "lw_thin_noalloc: %lld points exceed the fixed maximum of %lld per call",
+                         (long long)m, (long long)NOALLOC_THIN_MAX);
+    int64_t* base = nullptr;
+    int r = noalloc_thin_scratch(&base);
+    if (r != LW_OK) return r;
+    cudaStream_t s = (cudaStream_t)stream;
+    int64_t* keys = base;
+    int32_t* win = reinterpret_cast<int32_t*>(base + NOALLOC_THIN_SLOTS);
+    int32_t* slot = reinterpret_cast<int32_t*>(base + NOALLOC_THIN_SLOTS + NOALLOC_THIN_SLOTS / 2);
+    int32_t* tiles = reinterpret_cast<int32_t*>(base + NOALLOC_THIN_SLOTS + NOALLOC_THIN_SLOTS / 2 + NOALLOC_THIN_MAX / 2);
+    int32_t* m_dev = tiles + NOALLOC_THIN_TILES;
+    // the array keeps whatever the last call left: start every call from a cleared table
+    k_noalloc_thin_reset<<<64, 256, 0, s>>>(keys, win, m_dev, (int32_t)m);
+    lw_frame_buf fb{};
+    fb.f_xyz = const_cast<float*>(xyz4);
+    fb.f_attr = const_cast<uint32_t*>(attr);
+    fb.ds_keys = keys;
+    fb.ds_win = win;
+    fb.ds_slot = slot;
+    fb.tiles = tiles;
+    fb.ds_xyz = ds4_out;
+    fb.cap = m > 0 ? m : 1;
+    fb.ds_cap = NOALLOC_THIN_SLOTS;
+    ThinArgs a{};
+    a.inv_v = (float)inv_v;
+    a.min_range = (float)min_range;
+    a.max_range = (float)max_range;
+    a.ret_mask = ret_mask;
+    a.deskew = 0;
+    Tw6 tw{};
+    int64_t mu = m > 0 ? m : 1;
+    int grid = blocks_for(mu, 256, 8 * device_sms());
+    int nt = blocks_for(mu, TILE);
+    k_thin_a<<<grid, 256, 0, s>>>(fb, m_dev, a, nullptr, tw, nullptr, nullptr, 1);
+    k_thin_b<<<nt, TILE, 0, s>>>(fb, m_dev, nullptr);
+    k_thin_c<<<nt, TILE, 0, s>>>(fb, m_dev, n_ds_dev, nullptr);
+    LW_LAUNCHED("lw_thin_noalloc");
+    count_launches(4);
+    return LW_OK;
+}

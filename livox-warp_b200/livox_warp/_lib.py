@@ -113,6 +113,7 @@ _SIGS = {
     "lw_odom_restart_clock": (i32, [P, P]),
     "lw_deskew": (i32, [P, P, P, i64, f64, f64, C.POINTER(f32), P]),
     "lw_thin": (i32, [C.POINTER(FrameBuf), P, i64, f64, f64, f64, i32, P, P]),
+    "lw_thin_noalloc": (i32, [P, P, i64, f64, f64, f64, i32, P, P, P]),
     "lw_reg_insert": (i32, [P, P, P, i64, C.POINTER(f64), f64, f64, i32, C.POINTER(RegMap), C.POINTER(RecParams),
                               P, P]),
     "lw_reg_refresh_all": (i32, [C.POINTER(RegMap), C.POINTER(RecParams), P]),
