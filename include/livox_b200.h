@@ -287,6 +287,52 @@ int lw_frame_ids(const float* t, int64_t n, float inv_dt, int32_t* out, void* st
 /* Clear the integration map (gpu.py:1305-1313). */
 int lw_map_clear(lw_map* map, void* stream);
 
+/* ---- perception (perception.py) -------------------------------------------------------------- */
+
+/* Ground labels of n points (perception.py:29-111, Perception.ground :458-483): grid minimum per toroidal
+ * 2048 x 2048 cell, support within `thick`, the lowest supported minimum of the 5 x 5 cells around a point plus
+ * slope_step per cell of Chebyshev distance, ground when within `thresh`; hag = height above that ground.
+ * cell_min [2048*2048] (1e30) and cell_sup [2048*2048] (0) must hold their cleared values between calls; the call
+ * restores the cells it touched. nrm [n*3] is read only with use_normals. */
+int lw_ground(const float* xyz, int32_t xyz_stride, const float* nrm, const int32_t* n_dev, int64_t n_ub, float cell,
+              float thick, int32_t min_sup, float thresh, float slope_step, int32_t use_normals, float nz_min,
+              float* cell_min, int32_t* cell_sup, int32_t* out_gnd, float* out_hag, void* stream);
+
+/* Buffers of the Euclidean clustering; "between calls" values are restored by every call. */
+typedef struct lw_cluster_buf {
+    int64_t* keys;       /* [cap] voxel keys, -1 between calls */
+    int64_t* acc;        /* [cap*4] fixed-point x, y, z sums (LW_FIX_W) and point count, 0 between calls */
+    int32_t* first;      /* [cap] lowest point index per voxel, INT32_MAX between calls */
+    int32_t* vidx;       /* [cap] node of a slot */
+    int32_t* slot_of_pt; /* [pt_cap] */
+    int32_t* tiles;      /* [pt_cap/1024 + 2] */
+    int32_t* node_slot;  /* [pt_cap] slot of a node */
+    float* v_xyz;        /* [pt_cap*3] node centroids */
+    int32_t* v_w;        /* [pt_cap] node point counts */
+    int32_t* edge_off;   /* [pt_cap + 1] */
+    int32_t* edges;      /* [edge_cap] neighbour lists */
+    int32_t* label;      /* [pt_cap] component of a node: its smallest node index */
+    int64_t* st_sum;     /* [pt_cap*4] per-root fixed-point sums and count, 0 between calls */
+    float* st_lo;        /* [pt_cap*3] per-root minimum corner, +1e30 between calls */
+    float* st_hi;        /* [pt_cap*3] per-root maximum corner, -1e30 between calls */
+    int32_t* dense;      /* [pt_cap] dense cluster id of a root, -1 */
+    float* out_cnt;      /* [max_out] points per cluster */
+    float* out_cen;      /* [max_out*3] centroids */
+    float* out_lo;       /* [max_out*3] */
+    float* out_hi;       /* [max_out*3] */
+    int32_t* m;          /* [1] nodes of the last call */
+    int32_t* n_clusters; /* [2] clusters kept, clusters before the max_out cap */
+    int32_t* err;        /* [1] non-zero when a buffer was too small or a bounded loop gave up */
+    int64_t cap, pt_cap, edge_cap;
+} lw_cluster_buf;
+
+/* Connected components of the (non-ground) points' voxels (perception.py:114-271, Perception.cluster :487-567):
+ * voxels of size `voxel` linked when their centroids are within `connect`; clusters with >= min_pts points get
+ * dense ids 0.. in node order (a node's order is its first point's), at most max_out; out_cid [n] per point. */
+int lw_cluster(const float* xyz, int32_t xyz_stride, const int32_t* gnd, int32_t use_ground, const int32_t* n_dev,
+               int64_t n_ub, float voxel, float connect, float min_pts, int32_t max_out, lw_cluster_buf* cb,
+               int32_t* out_cid, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,6 +13,7 @@
 namespace lw {
 
 constexpr int MTILE = 1024;
+constexpr int DDA_BATCH = 8;  // voxels of a ray whose hash probes are issued together
 
 // Carving constants (gpu.py:66-73)
 constexpr float CARVE_MIN_RANGE = 0.05f;
@@ -160,29 +161,75 @@ __device__ __forceinline__ void centroid(const lw_map& map, int s, float& x, flo
 
 // Normal of the surface through voxel (ix, iy, iz) from a PCA of the occupied 3x3x3 neighbourhood's centroids
 // taken relative to `o` (gpu.py:422-466); w = 2 surface, 1 at least 4 occupied but no surface, 0 fewer.
+// Find the slots of n keys at once: every first probe is issued before any is waited on; collisions (rare at
+// the map's load factor) continue one by one. -1 where the key is absent.
+template <int N>
+__device__ __forceinline__ void find_slots(const int64_t* key, int* slot, const int64_t* __restrict__ keys, int mask) {
+    int h[N];
+    int64_t k0[N];
+#pragma unroll
+    for (int u = 0; u < N; ++u) {
+        h[u] = slot_hash(key[u]) & mask;
+        k0[u] = __ldg(keys + h[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < N; ++u) {
+        if (k0[u] == key[u]) {
+            slot[u] = h[u];
+        } else if (k0[u] == EMPTY_KEY) {
+            slot[u] = -1;
+        } else {
+            int s = -1;
+#pragma unroll 1
+            for (int p = 1; p < PROBES; ++p) {
+                int t = (h[u] + p) & mask;
+                int64_t kk = __ldg(keys + t);
+                if (kk == key[u]) {
+                    s = t;
+                    break;
+                }
+                if (kk == EMPTY_KEY) break;
+            }
+            slot[u] = s;
+        }
+    }
+}
+
+// Normal of the surface through voxel (ix, iy, iz) from a PCA of the occupied 3x3x3 neighbourhood's centroids
+// taken relative to `o` (gpu.py:422-466); w = 2 surface, 1 at least 4 occupied but no surface, 0 fewer.
+// The neighbours are visited in the reference's (gx, gy, gz) order; each gx slab's 9 probes go out together.
 __device__ float4 local_plane(int ix, int iy, int iz, float ox, float oy, float oz, const lw_map& map, int mask) {
     double cs[3] = {0.0, 0.0, 0.0}, cc[6] = {0, 0, 0, 0, 0, 0};
     int cn = 0;
-    for (int gx = -1; gx <= 1; ++gx)
-        for (int gy = -1; gy <= 1; ++gy)
-            for (int gz = -1; gz <= 1; ++gz) {
-                int sn = find_slot(key_ijk(ix + gx, iy + gy, iz + gz), map.keys, mask);
-                if (sn >= 0 && map.cnt[sn] > 0) {
-                    float cx, cy, cz;
-                    centroid(map, sn, cx, cy, cz);
-                    double qx = (double)(cx - ox), qy = (double)(cy - oy), qz = (double)(cz - oz);
-                    cs[0] += qx;
-                    cs[1] += qy;
-                    cs[2] += qz;
-                    cc[0] += qx * qx;
-                    cc[1] += qx * qy;
-                    cc[2] += qx * qz;
-                    cc[3] += qy * qy;
-                    cc[4] += qy * qz;
-                    cc[5] += qz * qz;
-                    ++cn;
-                }
+#pragma unroll 1
+    for (int gx = -1; gx <= 1; ++gx) {
+        int64_t key[9];
+        int slot[9];
+#pragma unroll
+        for (int u = 0; u < 9; ++u) key[u] = key_ijk(ix + gx, iy + u / 3 - 1, iz + u % 3 - 1);
+        find_slots<9>(key, slot, map.keys, mask);
+        int cnt[9];
+#pragma unroll
+        for (int u = 0; u < 9; ++u) cnt[u] = slot[u] >= 0 ? __ldg(map.cnt + slot[u]) : 0;
+#pragma unroll
+        for (int u = 0; u < 9; ++u) {
+            if (cnt[u] > 0) {
+                float cx, cy, cz;
+                centroid(map, slot[u], cx, cy, cz);
+                double qx = (double)(cx - ox), qy = (double)(cy - oy), qz = (double)(cz - oz);
+                cs[0] += qx;
+                cs[1] += qy;
+                cs[2] += qz;
+                cc[0] += qx * qx;
+                cc[1] += qx * qy;
+                cc[2] += qx * qz;
+                cc[3] += qy * qy;
+                cc[4] += qy * qz;
+                cc[5] += qz * qz;
+                ++cn;
             }
+        }
+    }
     if (cn < 4) return make_float4(0.0f, 0.0f, 1.0f, 0.0f);
     double inv = 1.0 / (double)cn;
     double mu[3] = {cs[0] * inv, cs[1] * inv, cs[2] * inv};
@@ -263,42 +310,70 @@ __global__ void k_carve(const float* __restrict__ xyz, const uint32_t* __restric
             tmz = (posz - (float)iz) / (-dz);
             tdz = -1.0f / dz;
         }
-        for (int step = 0; step < max_steps; ++step) {
-            float tt;
-            if (tmx < tmy && tmx < tmz) {
-                tt = tmx;
-                ix += sx;
-                tmx += tdx;
-            } else if (tmy < tmz) {
-                tt = tmy;
-                iy += sy;
-                tmy += tdy;
-            } else {
-                tt = tmz;
-                iz += sz;
-                tmz += tdz;
-            }
-            if (tt >= stop) break;
-            int s = find_slot(key_ijk(ix, iy, iz), map.keys, mask);
-            if (s < 0 || map.cnt[s] <= 0) continue;
-            float cx, cy, cz;
-            centroid(map, s, cx, cy, cz);
-            float rx = cx - ox, ry = cy - oy, rz = cz - oz;
-            bool pierced = false;
-            float4 pl = local_plane(ix, iy, iz, cx, cy, cz, map, mask);
-            if (pl.w > 1.5f) {
-                float dn = dx * pl.x + dy * pl.y + dz * pl.z;
-                if (fabsf(dn) > 1.0e-4f) {
-                    float f = (rx * pl.x + ry * pl.y + rz * pl.z) / dn;
-                    float xx = dx * f - rx, xy = dy * f - ry, xz = dz * f - rz;  // plane crossing rel. to centroid
-                    if (len3(xx, xy, xz) < CARVE_PIERCE_PLANE * voxel) pierced = true;
+        // walk the ray DDA_BATCH voxels at a time: the voxel sequence does not depend on the map, so the batch's
+        // hash probes are issued together; the voxels are then examined in ray order
+        bool done = false;
+#pragma unroll 1
+        for (int step0 = 0; step0 < max_steps && !done; step0 += DDA_BATCH) {
+            int64_t key[DDA_BATCH];
+            int vx[DDA_BATCH], vy[DDA_BATCH], vz[DDA_BATCH];
+            int nb = 0;
+#pragma unroll
+            for (int u = 0; u < DDA_BATCH; ++u) {
+                key[u] = EMPTY_KEY;
+                vx[u] = vy[u] = vz[u] = 0;
+                if (!done && step0 + u < max_steps) {
+                    float tt;
+                    if (tmx < tmy && tmx < tmz) {
+                        tt = tmx;
+                        ix += sx;
+                        tmx += tdx;
+                    } else if (tmy < tmz) {
+                        tt = tmy;
+                        iy += sy;
+                        tmy += tdy;
+                    } else {
+                        tt = tmz;
+                        iz += sz;
+                        tmz += tdz;
+                    }
+                    if (tt >= stop) {
+                        done = true;
+                    } else {
+                        key[u] = key_ijk(ix, iy, iz);
+                        vx[u] = ix;
+                        vy[u] = iy;
+                        vz[u] = iz;
+                        nb = u + 1;
+                    }
                 }
-            } else {
-                float g = rx * dx + ry * dy + rz * dz;
-                float qx = rx - g * dx, qy = ry - g * dy, qz = rz - g * dz;
-                if (len3(qx, qy, qz) < CARVE_PIERCE_POINT * voxel) pierced = true;
             }
-            if (pierced) atomicAdd(map.miss + s, every);
+            if (step0 + DDA_BATCH >= max_steps) done = true;
+            int slot[DDA_BATCH];
+            find_slots<DDA_BATCH>(key, slot, map.keys, mask);
+#pragma unroll 1
+            for (int u = 0; u < nb; ++u) {
+                int s = slot[u];
+                if (s < 0 || __ldg(map.cnt + s) <= 0) continue;
+                float cx, cy, cz;
+                centroid(map, s, cx, cy, cz);
+                float rx = cx - ox, ry = cy - oy, rz = cz - oz;
+                bool pierced = false;
+                float4 pl = local_plane(vx[u], vy[u], vz[u], cx, cy, cz, map, mask);
+                if (pl.w > 1.5f) {
+                    float dn = dx * pl.x + dy * pl.y + dz * pl.z;
+                    if (fabsf(dn) > 1.0e-4f) {
+                        float f = (rx * pl.x + ry * pl.y + rz * pl.z) / dn;
+                        float xx = dx * f - rx, xy = dy * f - ry, xz = dz * f - rz;  // plane crossing rel. to centroid
+                        if (len3(xx, xy, xz) < CARVE_PIERCE_PLANE * voxel) pierced = true;
+                    }
+                } else {
+                    float g = rx * dx + ry * dy + rz * dz;
+                    float qx = rx - g * dx, qy = ry - g * dy, qz = rz - g * dz;
+                    if (len3(qx, qy, qz) < CARVE_PIERCE_POINT * voxel) pierced = true;
+                }
+                if (pierced) atomicAdd(map.miss + s, every);
+            }
         }
     }
 }

@@ -417,7 +417,7 @@ __global__ void k_reg_refresh_all(lw_regmap reg, lw_rec_params rp) {
 // =====================================================================================================
 
 constexpr int GN_THREADS = 256;
-constexpr int GN_G = 8;  // lanes per point
+constexpr int GN_G = 16;  // lanes per point
 constexpr int NTERMS = 53;
 
 struct IcpPose {
@@ -552,14 +552,19 @@ __device__ __forceinline__ void icp_terms(float* a, const float* __restrict__ re
 // One accumulation pass of this CTA over its share of the thinned points; writes the CTA's float64 partial.
 __device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P, const IcpConsts& k,
                          const int64_t* __restrict__ keys, const float* __restrict__ rec, double* __restrict__ part) {
-    __shared__ float red[GN_THREADS / 32][NTERMS];
-    float a[NTERMS];
-#pragma unroll
-    for (int t = 0; t < NTERMS; ++t) a[t] = 0.0f;
+    constexpr int GROUPS = GN_THREADS / GN_G;
+    // one row of float accumulators per group, written by the group's leader lane (registers stay free for the
+    // search); summed over the groups in a fixed order at the end
+    __shared__ float gacc[GROUPS][NTERMS + 1];
+    for (int e = threadIdx.x; e < GROUPS * (NTERMS + 1); e += blockDim.x) (&gacc[0][0])[e] = 0.0f;
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int lane_g = lane & (GN_G - 1);
-    const int group = (blockIdx.x * GN_THREADS + threadIdx.x) / GN_G;
-    const int ngroups = gridDim.x * GN_THREADS / GN_G;
+    const int gl = threadIdx.x / GN_G;
+    const int group = blockIdx.x * GROUPS + gl;
+    const int ngroups = gridDim.x * GROUPS;
+    // groups of one warp may run different trip counts: shuffle within this group's lanes only
+    const unsigned gmask = (GN_G == 32 ? 0xffffffffu : ((1u << GN_G) - 1u)) << (lane & ~(GN_G - 1));
     for (int j = group; j < n; j += ngroups) {
         float4 p = __ldg(ds + j);
         float lx = P.R[0] * p.x + P.R[1] * p.y + P.R[2] * p.z + P.tr[0];
@@ -572,8 +577,6 @@ __device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P,
             icp_search<2>(lane_g, wx, wy, wz, k, keys, rec, bd, bo, bs);
         else
             icp_search<1>(lane_g, wx, wy, wz, k, keys, rec, bd, bo, bs);
-        // groups of one warp may run different trip counts: shuffle within this group's lanes only
-        const unsigned gmask = ((1u << GN_G) - 1u) << (lane & ~(GN_G - 1));
 #pragma unroll
         for (int off = GN_G / 2; off > 0; off >>= 1) {
             float od = __shfl_xor_sync(gmask, bd, off);
@@ -585,24 +588,13 @@ __device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P,
                 bs = os;
             }
         }
-        if (lane_g == 0 && bs >= 0) icp_terms(a, rec, bs, wx, wy, wz, lx, ly, lz, p.w, k.kappa2);
+        if (lane_g == 0 && bs >= 0) icp_terms(gacc[gl], rec, bs, wx, wy, wz, lx, ly, lz, p.w, k.kappa2);
     }
-    // group leaders -> lane 0 of each warp
-#pragma unroll
-    for (int t = 0; t < NTERMS; ++t) {
-        float v = a[t];
-#pragma unroll
-        for (int off = 16; off >= GN_G; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        a[t] = v;
-    }
-    if (lane == 0)
-#pragma unroll
-        for (int t = 0; t < NTERMS; ++t) red[threadIdx.x >> 5][t] = a[t];
     __syncthreads();
     if (threadIdx.x < NTERMS) {
         double s = 0.0;
 #pragma unroll
-        for (int w = 0; w < GN_THREADS / 32; ++w) s += (double)red[w][threadIdx.x];
+        for (int g = 0; g < GROUPS; ++g) s += (double)gacc[g][threadIdx.x];
         part[threadIdx.x] = s;
     }
     __syncthreads();
@@ -860,6 +852,347 @@ __device__ __noinline__ double conditioning(const double* H) {
     return fmax(lo, 0.0) / fmax(hi, 1e-12);
 }
 
+// ---- the block-cooperative float64 step --------------------------------------------------------------------
+// Every CTA of the persistent kernel runs the same step on the same reduced accumulator (so one grid barrier per
+// iteration suffices). The 6x6 products are spread over 36 threads (one element each); the positive-definiteness
+// tests and solves are 6x6 Cholesky factorisations held in registers. Only a frame with a degenerate direction
+// takes the eigen-decomposition path (odom.py:436-455) on one thread.
+
+struct GnSmem {
+    double part4[4][LW_ACC_STRIDE];
+    double v[LW_ACC_STRIDE];
+    double HA[2][36];
+    double H[36], Hg[36], b[6];
+    double A[36], SB[36], SBi[36], P[36], tmp[36], G[36];
+    double rhs[6], xi[6], delta[6];
+    double T[16], Tp[16], c[3];
+    double L, rms, dmean;
+    int status, corr, degen;
+};
+
+// Reduce the CTA partials: four fixed quarters of the CTAs per term, then the quarters in order.
+__device__ void gn_reduce(const double* __restrict__ part, int grid, GnSmem& S) {
+    const int t = threadIdx.x & (LW_ACC_STRIDE - 1), q = threadIdx.x >> 6;
+    if (q < 4) {
+        double acc = 0.0;
+        // other CTAs wrote these in this launch: read them from L2 (__ldcg), never from a stale L1 line
+        if (t < NTERMS) {
+#pragma unroll 8
+            for (int b = q; b < grid; b += 4) acc += __ldcg(part + (int64_t)b * LW_ACC_STRIDE + t);
+        }
+        S.part4[q][t] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x < LW_ACC_STRIDE) {
+        const int u = threadIdx.x;
+        S.v[u] = ((S.part4[0][u] + S.part4[1][u]) + S.part4[2][u]) + S.part4[3][u];
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ int sym_idx(int p, int q) {
+    // index of (p, q) in the row-major upper triangle of a 6x6 matrix
+    if (p > q) {
+        int t = p;
+        p = q;
+        q = t;
+    }
+    return p * 6 - (p * (p - 1)) / 2 + (q - p);
+}
+
+// -[c]x, the upper-right block of the map from the world-origin twist to the re-centred one
+__device__ __forceinline__ double kmat(const double* c, int i, int j) {
+    const double K[9] = {0.0, c[2], -c[1], -c[2], 0.0, c[0], c[1], -c[0], 0.0};
+    return K[i * 3 + j];
+}
+
+// H = A^T H_c A, Hg likewise, b = A^T b_c with A = [[I, -[c]x], [0, I]] (odom.py's twist is about the origin).
+__device__ void gn_world(GnSmem& S) {
+    const int tid = threadIdx.x;
+    if (tid < 72) {
+        const int w = tid / 36, e = tid % 36, p = e / 6, q = e % 6;
+        const double* up = S.v + (w == 0 ? LW_ACC_H : LW_ACC_HG);
+        double x = up[sym_idx(p, q)];
+        if (q >= 3)
+            for (int k = 0; k < 3; ++k) x += up[sym_idx(p, k)] * kmat(S.c, k, q - 3);
+        S.HA[w][e] = x;
+    }
+    __syncthreads();
+    if (tid < 72) {
+        const int w = tid / 36, e = tid % 36, p = e / 6, q = e % 6;
+        double x = S.HA[w][e];
+        if (p >= 3)
+            for (int k = 0; k < 3; ++k) x += kmat(S.c, k, p - 3) * S.HA[w][k * 6 + q];
+        (w == 0 ? S.H : S.Hg)[e] = x;
+    } else if (tid < 78) {
+        const int p = tid - 72;
+        double x = S.v[LW_ACC_B + p];
+        if (p >= 3)
+            for (int k = 0; k < 3; ++k) x += kmat(S.c, k, p - 3) * S.v[LW_ACC_B + k];
+        S.b[p] = x;
+    }
+    __syncthreads();
+}
+
+// Cholesky of a symmetric 6x6 (row major) shifted by -shift on the diagonal, in registers; false unless it is
+// positive definite.
+__device__ __forceinline__ bool chol6(const double* M, double shift, double* Lf) {
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        double d = M[j * 6 + j] - shift;
+#pragma unroll
+        for (int k = 0; k < j; ++k) d -= Lf[j * 6 + k] * Lf[j * 6 + k];
+        if (!(d > 0.0)) return false;
+        d = sqrt(d);
+        Lf[j * 6 + j] = d;
+#pragma unroll
+        for (int i = j + 1; i < 6; ++i) {
+            double x = M[i * 6 + j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) x -= Lf[i * 6 + k] * Lf[j * 6 + k];
+            Lf[i * 6 + j] = x / d;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void chol6_solve(const double* Lf, const double* rhs, double* x) {
+    double y[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double s = rhs[i];
+#pragma unroll
+        for (int k = 0; k < i; ++k) s -= Lf[i * 6 + k] * y[k];
+        y[i] = s / Lf[i * 6 + i];
+    }
+#pragma unroll
+    for (int i = 5; i >= 0; --i) {
+        double s = y[i];
+#pragma unroll
+        for (int k = i + 1; k < 6; ++k) s -= Lf[k * 6 + i] * x[k];
+        x[i] = s / Lf[i * 6 + i];
+    }
+}
+
+// The degenerate branch of odom.py:436-455 (some direction below degen_thr): eigen-decompose G and hold the
+// weak directions at the prediction. One thread; rare.
+__device__ __noinline__ int gn_degenerate(GnSmem& S, double thr, double* delta) {
+    double Gc[36], V[36], lam[6];
+    for (int i = 0; i < 36; ++i) Gc[i] = S.G[i];
+    jacobi_eig<6>(Gc, lam, V);
+    bool good[6];
+    int ng = 0;
+    for (int k = 0; k < 6; ++k) {
+        good[k] = lam[k] >= thr;
+        ng += good[k] ? 1 : 0;
+    }
+    S.degen = 6 - ng;
+    if (ng == 6) {
+        double Lf[36];
+        if (!chol6(S.A, 0.0, Lf)) return 3;
+        chol6_solve(Lf, S.rhs, delta);
+        return 0;
+    }
+    double z[6], d0[6];
+    matvec6(S.SBi, S.xi, z);  // solve(J, to_pred)
+    for (int i = 0; i < 6; ++i) d0[i] = 0.0;
+    for (int k = 0; k < 6; ++k) {
+        if (good[k]) continue;
+        double pr = 0.0;
+        for (int i = 0; i < 6; ++i) pr += V[i * 6 + k] * z[i];
+        for (int i = 0; i < 6; ++i) d0[i] += V[i * 6 + k] * pr;
+    }
+    if (ng > 0) {
+        double As[36], tmp[36], Jr[6], Asd[6], g[6], Ag[36], y[6], Vg[36];
+        int cols[6], nc = 0;
+        for (int k = 0; k < 6; ++k)
+            if (good[k]) cols[nc++] = k;
+        matmul6(S.A, S.SB, tmp);
+        matmul6(S.SB, tmp, As, true);
+        matvec6(S.SB, S.rhs, Jr, true);
+        matvec6(As, d0, Asd);
+        for (int i = 0; i < 6; ++i)
+            for (int a = 0; a < nc; ++a) Vg[i * 6 + a] = V[i * 6 + cols[a]];
+        for (int a = 0; a < nc; ++a) {
+            double s = 0.0;
+            for (int i = 0; i < 6; ++i) s += Vg[i * 6 + a] * (Jr[i] - Asd[i]);
+            g[a] = s;
+            for (int c2 = 0; c2 < nc; ++c2) {
+                double s2 = 0.0;
+                for (int i = 0; i < 6; ++i) {
+                    double t2 = 0.0;
+                    for (int j = 0; j < 6; ++j) t2 += As[i * 6 + j] * Vg[j * 6 + c2];
+                    s2 += Vg[i * 6 + a] * t2;
+                }
+                Ag[a * 6 + c2] = s2;
+            }
+        }
+        if (!lu_solve<6>(Ag, g, y, nc)) return 3;
+        for (int i = 0; i < 6; ++i)
+            for (int a = 0; a < nc; ++a) d0[i] += Vg[i * 6 + a] * y[a];
+    }
+    matvec6(S.SB, d0, delta);
+    return 0;
+}
+
+// One Gauss-Newton update of S.T (odom.py:769-796) by the whole block. S.status: 0 continue, 1 converged,
+// 2 too few correspondences, 3 singular.
+__device__ void gn_step_block(GnSmem& S, const lw_odom_params& prm) {
+    const int tid = threadIdx.x;
+    gn_world(S);
+    if (tid == 0) {
+        S.corr = (int)S.v[LW_ACC_COUNT];
+        S.status = S.corr < prm.min_corr ? 2 : 0;
+        S.degen = 0;
+        if (S.status == 0) {
+            S.L = fmax(S.v[LW_ACC_RANGE] / (double)S.corr, 1.0);
+            S.rms = sqrt(fmax(S.v[LW_ACC_RMS], 0.0) / fmax(S.v[LW_ACC_WEIGHT], 1e-9));
+            double dm = 0.0;
+            for (int k = 0; k < 6; ++k) dm += S.H[k * 7];
+            S.dmean = dm / 6.0;
+            double Ti[16], Mp[16];
+            mat44_inv_rigid(S.T, Ti);  // the left twist from T back onto the prediction (odom.py:397-401)
+            mat44_mul(S.Tp, Ti, Mp);
+            body_twist(Mp, S.xi);
+        }
+    }
+    __syncthreads();
+    if (S.status != 0) return;
+    if (tid < 36) {
+        const int p = tid / 6, q = tid % 6, bi = p / 3, bj = q / 3, i = p % 3, j = q % 3;
+        double a = S.H[tid];
+        if (p == q) a += 1e-9 * S.dmean + prm.damping * S.H[tid];
+        S.A[tid] = a;
+        // sensor basis (odom.py:425-433): SB = [[R, [c]x R / L], [0, R / L]], SB^-1 = [[R^T, -R^T [c]x], [0, L R^T]]
+        const double c0 = S.T[3], c1 = S.T[7], c2 = S.T[11];
+        const double cx[9] = {0.0, -c2, c1, c2, 0.0, -c0, -c1, c0, 0.0};
+        double sb = 0.0, sbi = 0.0;
+        if (bi == 0 && bj == 0) {
+            sb = S.T[i * 4 + j];
+            sbi = S.T[j * 4 + i];
+        } else if (bi == 0 && bj == 1) {
+            double cr = 0.0, rc = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                cr += cx[i * 3 + k] * S.T[k * 4 + j];
+                rc += S.T[k * 4 + i] * cx[k * 3 + j];
+            }
+            sb = cr / S.L;
+            sbi = -rc;
+        } else if (bi == 1 && bj == 1) {
+            sb = S.T[i * 4 + j] / S.L;
+            sbi = S.L * S.T[j * 4 + i];
+        }
+        S.SB[tid] = sb;
+        S.SBi[tid] = sbi;
+    } else if (tid < 42) {
+        S.rhs[tid - 36] = -S.b[tid - 36];
+    }
+    __syncthreads();
+    if (tid < 36) {
+        const int p = tid / 6, q = tid % 6;
+        double x = 0.0, y = 0.0;
+        for (int k = 0; k < 6; ++k) {
+            x += S.SBi[k * 6 + p] * S.SBi[k * 6 + q];
+            y += S.Hg[p * 6 + k] * S.SB[k * 6 + q];
+        }
+        S.P[tid] = prm.prior_info > 0.0 ? prm.prior_info * x : 0.0;
+        S.tmp[tid] = y;
+    }
+    __syncthreads();
+    if (tid < 36) {
+        const int p = tid / 6, q = tid % 6;
+        double g = 0.0;
+        for (int k = 0; k < 6; ++k) g += S.SB[k * 6 + p] * S.tmp[k * 6 + q];
+        S.G[tid] = g;
+        if (prm.prior_info > 0.0) S.A[tid] += S.P[tid];
+    } else if (tid < 42 && prm.prior_info > 0.0) {
+        const int i = tid - 36;
+        double x = 0.0;
+        for (int k = 0; k < 6; ++k) x += S.P[i * 6 + k] * S.xi[k];
+        S.rhs[i] += x;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double delta[6], Lf[36];
+        int st = 0;
+        double Gs[36];
+        for (int i = 0; i < 36; ++i) Gs[i] = S.G[i];
+        if (prm.degen_thr > 0.0 && !chol6(Gs, prm.degen_thr, Lf)) {
+            st = gn_degenerate(S, prm.degen_thr, delta);  // some direction below the threshold
+        } else {
+            double As[36];
+            for (int i = 0; i < 36; ++i) As[i] = S.A[i];
+            if (!chol6(As, 0.0, Lf)) {
+                st = 3;
+            } else {
+                chol6_solve(Lf, S.rhs, delta);
+            }
+        }
+        if (st == 0) {
+            apply_twist(S.T, delta);
+            double nt = sqrt(delta[0] * delta[0] + delta[1] * delta[1] + delta[2] * delta[2]);
+            double nr = sqrt(delta[3] * delta[3] + delta[4] * delta[4] + delta[5] * delta[5]);
+            st = (nt < 1e-4 && nr < 1e-4) ? 1 : 0;  // STEP_TOL (odom.py:88)
+        }
+        S.status = st;
+    }
+    __syncthreads();
+}
+
+// Eigenvalues of a symmetric 6x6 by cyclic Jacobi without vectors, fully unrolled so the matrix stays in
+// registers; min over max of the diagonally normalised H is the conditioning stat (odom.py:797-800).
+__device__ __noinline__ double conditioning_fast(const double* Hs) {
+    double dg[6], A[36];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) dg[k] = sqrt(fmax(Hs[k * 7], 1e-12));
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = 0; j < 6; ++j) A[i * 6 + j] = Hs[i * 6 + j] / (dg[i] * dg[j]);
+    for (int sweep = 0; sweep < 24; ++sweep) {
+        double off = 0.0, tot = 0.0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                double a2 = A[i * 6 + j] * A[i * 6 + j];
+                tot += a2;
+                if (i != j) off += a2;
+            }
+        if (off <= 1e-30 * tot || off == 0.0) break;
+#pragma unroll
+        for (int p = 0; p < 5; ++p)
+#pragma unroll
+            for (int q = p + 1; q < 6; ++q) {
+                double apq = A[p * 6 + q];
+                if (apq != 0.0) {
+                    double tau = (A[q * 6 + q] - A[p * 6 + p]) / (2.0 * apq);
+                    double t = (tau >= 0.0) ? 1.0 / (tau + sqrt(1.0 + tau * tau)) : -1.0 / (-tau + sqrt(1.0 + tau * tau));
+                    double c = 1.0 / sqrt(1.0 + t * t), s = t * c;
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) {
+                        double akp = A[k * 6 + p], akq = A[k * 6 + q];
+                        A[k * 6 + p] = c * akp - s * akq;
+                        A[k * 6 + q] = s * akp + c * akq;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) {
+                        double apk = A[p * 6 + k], aqk = A[q * 6 + k];
+                        A[p * 6 + k] = c * apk - s * aqk;
+                        A[q * 6 + k] = s * apk + c * aqk;
+                    }
+                }
+            }
+    }
+    double lo = A[0], hi = A[0];
+#pragma unroll
+    for (int k = 1; k < 6; ++k) {
+        lo = fmin(lo, A[k * 7]);
+        hi = fmax(hi, A[k * 7]);
+    }
+    return fmax(lo, 0.0) / fmax(hi, 1e-12);
+}
+
 // The whole registration loop (odom.py:752-803) in one cooperative launch. Every CTA reduces the partials
 // and computes the same float64 step, so one grid barrier per iteration suffices.
 __global__ void __launch_bounds__(GN_THREADS, 1)
@@ -867,25 +1200,25 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
          const int64_t* __restrict__ keys, const float* __restrict__ rec, int mask, lw_gn_scratch gn, int which) {
     const int* gate = which == 0 ? &st->run_reg : (which == 1 ? &st->redo : nullptr);
     if (gate && *gate == 0) return;  // uniform: every CTA reads the same flag before any barrier
-    __shared__ double sT[16], sTp[16], sc[3], v64[LW_ACC_STRIDE];
-    __shared__ int s_stop, s_corr, s_iters, s_degen;
+    __shared__ GnSmem S;
+    __shared__ int s_iters, s_degen, s_corr;
     __shared__ double s_rms;
     const int n = *n_dev;
     if (threadIdx.x == 0) {
-        for (int i = 0; i < 16; ++i) sT[i] = sTp[i] = st->T_pred[i];
-        sc[0] = st->T_pred[3];
-        sc[1] = st->T_pred[7];
-        sc[2] = st->T_pred[11];
-        s_stop = 0;
-        s_corr = 0;
+        for (int i = 0; i < 16; ++i) S.T[i] = S.Tp[i] = st->T_pred[i];
+        S.c[0] = st->T_pred[3];
+        S.c[1] = st->T_pred[7];
+        S.c[2] = st->T_pred[11];
         s_iters = 0;
         s_degen = 0;
+        s_corr = 0;
         s_rms = 0.0;
+        for (int i = 0; i < 36; ++i) S.H[i] = (i % 7 == 0) ? 1.0 : 0.0;
     }
     __syncthreads();
     if (n < prm.min_corr) {  // odom.py:754-757
         if (blockIdx.x == 0 && threadIdx.x == 0) {
-            for (int i = 0; i < 16; ++i) st->T_reg[i] = sTp[i];
+            for (int i = 0; i < 16; ++i) st->T_reg[i] = S.Tp[i];
             st->ok = 0;
             st->n_ds = n;
         }
@@ -895,36 +1228,33 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
     IcpConsts k;
     k.inv_v = (float)(1.0 / prm.reg_voxel);
     k.mask = mask;
-    double H[36];
-    for (int i = 0; i < 36; ++i) H[i] = (i % 7 == 0) ? 1.0 : 0.0;
     for (int it = 0; it < prm.max_iter; ++it) {
         float kappa;
         schedule(it, voxel, k.reach, k.max_d2, kappa);
         k.kappa2 = kappa * kappa;
         IcpPose P;
-        make_pose(sT, sc, P);
+        make_pose(S.T, S.c, P);
         double* part = gn.part + (int64_t)(it & 1) * gn.grid * LW_ACC_STRIDE;
         icp_pass(ds, n, P, k, keys, rec, part + (int64_t)blockIdx.x * LW_ACC_STRIDE);
         if (!grid_barrier(gn.bar, gn.err, 1)) return;
-        reduce_partials(part, gn.grid, sc, v64);
+        gn_reduce(part, gn.grid, S);
+        gn_step_block(S, prm);
         if (threadIdx.x == 0) {
-            StepOut o = gn_step(v64, sT, sTp, prm, H);
-            s_corr = o.corr;
-            if (o.status != 2) s_rms = o.rms;
-            if (o.status == 0 || o.status == 1) {
+            s_corr = S.corr;
+            if (S.status != 2) s_rms = S.rms;
+            if (S.status == 0 || S.status == 1) {
                 s_iters = it + 1;
-                s_degen = o.degen;
+                s_degen = S.degen;
             }
-            s_stop = o.status != 0;
         }
         __syncthreads();
-        if (s_stop) break;
+        if (S.status != 0) break;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         bool ok = s_corr >= prm.min_corr;
         double cond = st->cond;
-        if (ok) cond = conditioning(H);
-        for (int i = 0; i < 16; ++i) st->T_reg[i] = sT[i];
+        if (ok) cond = conditioning_fast(S.H);
+        for (int i = 0; i < 16; ++i) st->T_reg[i] = S.T[i];
         st->ok = ok ? 1 : 0;
         st->n_ds = n;
         st->iters = s_iters;

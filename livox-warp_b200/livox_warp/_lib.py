@@ -80,6 +80,13 @@ class Map(C.Structure):
                 ("lead", P), ("stats", P), ("cap", i64)]
 
 
+class ClusterBuf(C.Structure):
+    PTRS = ("keys", "acc", "first", "vidx", "slot_of_pt", "tiles", "node_slot", "v_xyz", "v_w", "edge_off", "edges",
+            "label", "st_sum", "st_lo", "st_hi", "dense", "out_cnt", "out_cen", "out_lo", "out_hi", "m", "n_clusters",
+            "err")
+    _fields_ = [(n, P) for n in PTRS] + [("cap", i64), ("pt_cap", i64), ("edge_cap", i64)]
+
+
 class View(C.Structure):
     """gpu.View (gpu.py:76-98): the filters and labels the map kernels read."""
 
@@ -125,6 +132,8 @@ _SIGS = {
     "lw_map_build": (i32, [C.POINTER(Map), C.POINTER(View), i32, P, P, P, P, P, P, P]),
     "lw_map_clear": (i32, [C.POINTER(Map), P]),
     "lw_frame_ids": (i32, [P, i64, f32, P, P]),
+    "lw_ground": (i32, [P, i32, P, P, i64, f32, f32, i32, f32, f32, i32, f32, P, P, P, P, P]),
+    "lw_cluster": (i32, [P, i32, P, i32, P, i64, f32, f32, f32, i32, C.POINTER(ClusterBuf), P, P]),
 }
 
 _lib = None

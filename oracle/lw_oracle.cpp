@@ -17,6 +17,8 @@
 #include <stdint.h>
 #include <string.h>
 #include <algorithm>
+#include <array>
+#include <functional>
 #include <unordered_map>
 #include <vector>
 
@@ -615,6 +617,156 @@ int64_t or_map_build(int64_t cap, const int64_t* keys, const int32_t* cnt, const
         ++k;
     }
     return k;
+}
+
+
+// ---- ground (perception.py:29-111, Perception.ground :458-483) -------------------------------------------------
+// xyz [n*stride]; nrm [n*3] or null. The grid starts cleared on every call (the GPU keeps it cleared between calls).
+void or_ground(const float* xyz, int stride, const float* nrm, int64_t n, float cell, float thick, int min_sup,
+               float thresh, float slope_step, int use_normals, float nz_min, int32_t* out_gnd, float* out_hag) {
+    const int G = 2048;
+    const float inv = 1.0f / fmaxf(cell, 0.05f);
+    std::vector<float> cmin((size_t)G * G, 1.0e30f);
+    std::vector<int32_t> csup((size_t)G * G, 0);
+    auto cell_of = [&](float x, float y) { return (ifloor(y * inv) & (G - 1)) * G + (ifloor(x * inv) & (G - 1)); };
+    for (int64_t i = 0; i < n; ++i) {
+        int c = cell_of(xyz[i * stride], xyz[i * stride + 1]);
+        cmin[c] = std::min(cmin[c], xyz[i * stride + 2]);
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        int c = cell_of(xyz[i * stride], xyz[i * stride + 1]);
+        if (xyz[i * stride + 2] - cmin[c] < thick) csup[c] += 1;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        float x = xyz[i * stride], y = xyz[i * stride + 1], z = xyz[i * stride + 2];
+        int cx = ifloor(x * inv), cy = ifloor(y * inv);
+        float g = 1.0e30f, g_floor = 1.0e30f;
+        for (int dy = -2; dy <= 2; ++dy)
+            for (int dx = -2; dx <= 2; ++dx) {
+                int c = ((cy + dy) & (G - 1)) * G + ((cx + dx) & (G - 1));
+                if (csup[c] >= min_sup) {
+                    float cand = cmin[c] + slope_step * (float)std::max(std::abs(dx), std::abs(dy));
+                    if (cand < g) {
+                        g = cand;
+                        g_floor = cmin[c];
+                    }
+                }
+            }
+        if (g > 1.0e29f) {
+            out_gnd[i] = 0;
+            out_hag[i] = 0.0f;
+            continue;
+        }
+        float h = z - g;
+        int is_gnd = 0;
+        if (h < thresh) {
+            is_gnd = 1;
+            if (use_normals && h > 0.2f * thresh && fabsf(nrm[i * 3 + 2]) < nz_min) is_gnd = 0;
+        }
+        out_gnd[i] = is_gnd;
+        out_hag[i] = is_gnd ? h : z - g_floor;
+    }
+}
+
+// ---- clusters (perception.py:114-271, 487-567) --------------------------------------------------------------
+// Nodes are the occupied voxels in the order of their first point; components label a node by the smallest node
+// index linked to it (what min-label propagation converges to); clusters are the roots with >= min_pts points,
+// numbered in node order (at most max_out). Outputs: cid [n], labels [m] (returned count m via *m_out), cluster
+// stats cnt [max_out], cen/lo/hi [max_out*3]; returns the number of clusters (before the cap) in *k_all.
+int64_t or_cluster(const float* xyz, int stride, const int32_t* gnd, int use_ground, int64_t n, float voxel,
+                   float connect, float min_pts, int max_out, int32_t* out_cid, int32_t* labels, int64_t* m_out,
+                   float* out_cnt, float* out_cen, float* out_lo, float* out_hi, int64_t* k_all) {
+    const float inv = 1.0f / fmaxf(voxel, 0.01f);
+    const float FW = (float)FIX_W;
+    std::unordered_map<int64_t, int> node_of;
+    std::vector<int64_t> nkey;
+    std::vector<std::array<int64_t, 4>> nacc;
+    std::vector<int> pt_node(n, -1);
+    for (int64_t i = 0; i < n; ++i) {
+        if (use_ground && gnd[i] != 0) continue;
+        float x = xyz[i * stride], y = xyz[i * stride + 1], z = xyz[i * stride + 2];
+        int64_t key = key_ijk(ifloor(x * inv), ifloor(y * inv), ifloor(z * inv));
+        auto it = node_of.find(key);
+        int j;
+        if (it == node_of.end()) {
+            j = (int)nkey.size();
+            node_of.emplace(key, j);
+            nkey.push_back(key);
+            nacc.push_back({0, 0, 0, 0});
+        } else {
+            j = it->second;
+        }
+        nacc[j][0] += llrintf(x * FW);
+        nacc[j][1] += llrintf(y * FW);
+        nacc[j][2] += llrintf(z * FW);
+        nacc[j][3] += 1;
+        pt_node[i] = j;
+    }
+    const int m = (int)nkey.size();
+    *m_out = m;
+    std::vector<float> cen((size_t)m * 3);
+    for (int j = 0; j < m; ++j)
+        for (int d = 0; d < 3; ++d) cen[3 * j + d] = (float)((double)nacc[j][d] / ((double)nacc[j][3] * FIX_W));
+    int reach = (int)ceilf(connect * inv);
+    if (reach < 1) reach = 1;
+    const float c2 = connect * connect;
+    std::vector<int> parent(m);
+    for (int j = 0; j < m; ++j) parent[j] = j;
+    std::function<int(int)> find = [&](int x) {
+        while (parent[x] != x) {
+            parent[x] = parent[parent[x]];
+            x = parent[x];
+        }
+        return x;
+    };
+    for (int j = 0; j < m; ++j) {
+        int64_t key = nkey[j];
+        int ix = (int)(key & KMASK) - (int)BIAS, iy = (int)((key >> 21) & KMASK) - (int)BIAS,
+            iz = (int)((key >> 42) & KMASK) - (int)BIAS;
+        for (int dx = -reach; dx <= reach; ++dx)
+            for (int dy = -reach; dy <= reach; ++dy)
+                for (int dz = -reach; dz <= reach; ++dz) {
+                    if (!dx && !dy && !dz) continue;
+                    auto it = node_of.find(key_ijk(ix + dx, iy + dy, iz + dz));
+                    if (it == node_of.end()) continue;
+                    int k = it->second;
+                    float ex = cen[3 * k] - cen[3 * j], ey = cen[3 * k + 1] - cen[3 * j + 1], ez = cen[3 * k + 2] - cen[3 * j + 2];
+                    if (ex * ex + ey * ey + ez * ez <= c2) {
+                        int a = find(j), b = find(k);
+                        if (a != b) parent[std::max(a, b)] = std::min(a, b);
+                    }
+                }
+    }
+    for (int j = 0; j < m; ++j) labels[j] = find(j);
+    std::vector<std::array<int64_t, 4>> ssum(m, {0, 0, 0, 0});
+    std::vector<float> lo((size_t)m * 3, 1.0e30f), hi((size_t)m * 3, -1.0e30f);
+    for (int j = 0; j < m; ++j) {
+        int r = labels[j];
+        for (int d = 0; d < 4; ++d) ssum[r][d] += nacc[j][d];
+        for (int d = 0; d < 3; ++d) {
+            lo[3 * r + d] = std::min(lo[3 * r + d], cen[3 * j + d]);
+            hi[3 * r + d] = std::max(hi[3 * r + d], cen[3 * j + d]);
+        }
+    }
+    std::vector<int> dense(m, -1);
+    int64_t k = 0;
+    for (int j = 0; j < m; ++j) {
+        if (labels[j] != j || (float)ssum[j][3] < min_pts) continue;
+        if (k < max_out) {
+            dense[j] = (int)k;
+            double w = (double)ssum[j][3];
+            out_cnt[k] = (float)ssum[j][3];
+            for (int d = 0; d < 3; ++d) {
+                out_cen[3 * k + d] = (float)((double)ssum[j][d] / (w * FIX_W));
+                out_lo[3 * k + d] = lo[3 * j + d];
+                out_hi[3 * k + d] = hi[3 * j + d];
+            }
+        }
+        ++k;
+    }
+    *k_all = k;
+    for (int64_t i = 0; i < n; ++i) out_cid[i] = pt_node[i] < 0 ? -1 : dense[labels[pt_node[i]]];
+    return k < max_out ? k : max_out;
 }
 
 }  // extern "C"

@@ -72,6 +72,8 @@ def lib() -> C.CDLL:
             "or_map_insert": (None, [P, i32, P, P, P, i64, P, P, f32, i64, P, P, P, P, P, P]),
             "or_carve": (None, [P, i32, P, P, i64, P, i32, f32, f32, i32, i64, P, P, P, P, i32]),
             "or_map_build": (i64, [i64, P, P, P, P, P, P, P, i32, P, P, P, P]),
+            "or_ground": (None, [P, i32, P, i64, f32, f32, i32, f32, f32, i32, f32, P, P]),
+            "or_cluster": (i64, [P, i32, P, i32, i64, f32, f32, f32, i32, P, P, P, P, P, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(_lib, name)
@@ -221,6 +223,40 @@ class Map:
         occ = self.keys != -1
         return {int(k): (int(c), tuple(a), float(l), float(f), int(m)) for k, c, a, l, f, m in
                 zip(self.keys[occ], self.cnt[occ], self.acc[occ], self.last[occ], self.first[occ], self.miss[occ])}
+
+
+# ---- perception ---------------------------------------------------------------------------------------------
+
+
+def ground(xyz, cell=0.5, thick=0.15, min_sup=3, thresh=0.2, slope_step=0.3, nrm=None, nz_min=0.7):
+    """perception.py:29-111: (gnd int32, hag float32) per point."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+    n = len(xyz)
+    gnd = np.zeros(n, np.int32)
+    hag = np.zeros(n, np.float32)
+    nrm_a = None if nrm is None else np.ascontiguousarray(nrm, dtype=np.float32)
+    lib().or_ground(_p(xyz), xyz.shape[1], None if nrm_a is None else _p(nrm_a), n, cell, thick, min_sup, thresh,
+                    slope_step, int(nrm_a is not None), nz_min, _p(gnd), _p(hag))
+    return gnd, hag
+
+
+def cluster(xyz, gnd=None, voxel=0.1, connect=0.35, min_pts=30, max_out=4096):
+    """perception.py:114-271: (cid per point, node labels, clusters [(cnt, cen, lo, hi)], clusters before cap)."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+    n = len(xyz)
+    g = np.zeros(n, np.int32) if gnd is None else np.ascontiguousarray(gnd, dtype=np.int32)
+    cid = np.zeros(n, np.int32)
+    labels = np.zeros(max(n, 1), np.int32)
+    m = np.zeros(1, np.int64)
+    k_all = np.zeros(1, np.int64)
+    cnt = np.zeros(max_out, np.float32)
+    cen = np.zeros((max_out, 3), np.float32)
+    lo = np.zeros((max_out, 3), np.float32)
+    hi = np.zeros((max_out, 3), np.float32)
+    k = lib().or_cluster(_p(xyz), xyz.shape[1], _p(g), int(gnd is not None), n, voxel, connect, float(min_pts),
+                         max_out, _p(cid), _p(labels), _p(m), _p(cnt), _p(cen), _p(lo), _p(hi), _p(k_all))
+    clusters = [(float(cnt[j]), cen[j].copy(), lo[j].copy(), hi[j].copy()) for j in range(k)]
+    return cid, labels[:int(m[0])], clusters, int(k_all[0])
 
 
 # ---- the host-side float64 step (odom.py:387-455) -----------------------------------------------------------
