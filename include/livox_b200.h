@@ -333,6 +333,67 @@ int lw_cluster(const float* xyz, int32_t xyz_stride, const int32_t* gnd, int32_t
                int64_t n_ub, float voxel, float connect, float min_pts, int32_t max_out, lw_cluster_buf* cb,
                int32_t* out_cid, void* stream);
 
+/* ---- prior-map grid and batched localisation ICP (mapgrid.py, localize.py) -------------------------- */
+
+/* A dense grid over a prior map (mapgrid.py:1-33, 207-296): the n map points sorted by cell (start[c] ..
+ * start[c+1] are cell c's points), a jump-flooded nearest point per cell and a byte distance field in cm. */
+typedef struct lw_prior_grid {
+    float* xyz;       /* [n*3] map points, sorted by cell */
+    float* nrm;       /* [n*3] unit normals */
+    float* planar;    /* [n] planarity */
+    int32_t* start;   /* [ncell+1] */
+    int32_t* nn;      /* [ncell] flooded nearest point or -1 */
+    uint8_t* df;      /* [ncell] distance to it in cm, 255 beyond the band */
+    uint64_t* seed;   /* [ncell] build scratch */
+    int32_t* nn2;     /* [ncell] build scratch */
+    float origin[3];
+    float cell, inv_cell;
+    int32_t nx, ny, nz, pad_;
+    int64_t n, ncell;
+} lw_prior_grid;
+
+/* Build nn and df from the sorted points (k_seed, k_unpack, k_jfa x (8, 4, 2, 1, 1), k_df: mapgrid.py:105-170,
+ * 272-296). Seeds are 64-bit (no 2^23-point limit) and the flood is double buffered (deterministic). */
+int lw_prior_grid_build(lw_prior_grid* g, void* stream);
+
+/* Distance of n points (pts [n*3]) posed by T (row-major 4x4, host) to the nearest map point, 1e3 beyond the
+ * band (mapgrid.py:173-194, PriorGrid.distances :298-305). */
+int lw_prior_distances(const lw_prior_grid* g, const float* pts, int64_t n, const double* T_host, float* out,
+                       void* stream);
+
+/* Buffers of the batched ICP: every hypothesis has its own range of points (tile_lo .. scan_end; hypotheses may
+ * share one scan) and pose (T, in and out). The points are cut into tiles of `tile` points that never span two
+ * hypotheses: hypothesis h owns tiles hyp_tile[h] .. hyp_tile[h+1]. */
+typedef struct lw_loc_batch {
+    float* pts;         /* [pts_cap*4] x, y, z, unused */
+    int32_t* scan_end;  /* [n_hyp] end (exclusive) of each hypothesis' points */
+    int32_t* tile_hyp;  /* [n_tiles] hypothesis of each tile */
+    int32_t* tile_lo;   /* [n_tiles] first point of each tile */
+    int32_t* hyp_tile;  /* [n_hyp+1] first tile of each hypothesis */
+    double* T;          /* [n_hyp*16] row-major poses, updated in place */
+    double* tile_part;  /* [n_tiles*32] float64 tile partials (scratch) */
+    int32_t* moved;     /* [moved_cap] largest step of each iteration (scratch) */
+    int32_t* count;     /* [n_hyp] matched points in the last iteration */
+    int32_t* eval;      /* [n_hyp*3] points within 3 / 5 / 10 cm of the map at the final pose */
+    uint32_t* bar;      /* [2] grid barrier, zero before the first use */
+    int32_t* err;       /* [1] set when a bounded wait gave up */
+    int32_t* iters_run; /* [1] iterations run over all stages */
+    int32_t* dims;      /* [2] n_hyp, n_tiles read on the device (a graph replayed over changing batches), or NULL */
+    int64_t pts_cap;    /* points the pts buffer holds; tiles and scan ends are clamped to it */
+    int32_t moved_cap, grid_cap;
+} lw_loc_batch;
+
+/* Point-to-plane ICP of every hypothesis at once against the grid (k_icp_batch / k_reduce_batch / the host
+ * solve of GlobalLocalizer._icp, localize.py:126-179, 517-553, then k_eval_batch :182-205), in one cooperative
+ * launch: stages k = 0..n_stages-1 of iters[k] iterations with correspondence distance dmax[k] (max_d2 and the
+ * Geman-McClure c2 = (dmax/2)^2 are formed in double and rounded to float, as the reference's host does); a
+ * hypothesis with fewer than min_count matches keeps its pose; a stage ends when no hypothesis moved 2e-4
+ * (n_stages = 0 only evaluates). With b->dims set, n_hyp and n_tiles are capacities and the counts are read on
+ * the device. tile: 128, 256 or 512 points per CTA; grid <= 0 picks one full wave. */
+int lw_loc_icp_batch(const lw_prior_grid* g, lw_loc_batch* b, int32_t n_hyp, int32_t n_tiles, int32_t tile,
+                     int32_t n_stages, const double* dmax, const int32_t* iters, float alpha, int32_t min_count,
+                     int32_t grid, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,583 @@
+// Prior-map grid and batched point-to-plane ICP for global localisation, on sm_100a.
+//
+// Reference: python/livox_warp/mapgrid.py -- Grid / grid_flat / grid_at / cell_centre :35-65, nearest_point :68-102,
+// k_seed :105-114, k_unpack :117-125, k_jfa :128-158, k_df :161-170, PriorGrid.build :272-296;
+// python/livox_warp/localize.py -- k_icp_batch :126-167, k_reduce_batch :170-179, k_eval_batch :182-205,
+// GlobalLocalizer._icp :517-553, _evaluate :555-565.
+//
+// The grid build seeds each cell with a 64-bit key (distance in mm << 32 | point index) instead of the
+// reference's 32-bit (mm << 23 | index), which held at most 2^23 - 1 map points, and floods between two
+// buffers instead of in place, so the flood's result does not depend on thread timing.
+//
+// The batched ICP runs every hypothesis -- each with its own scan, of any length -- in one cooperative launch:
+// tiles of one hypothesis' points accumulate float32 terms into float64 tile partials; after a grid barrier
+// each hypothesis sums its tiles in a fixed order and solves its 6x6 system (Cholesky, float64); after a second
+// barrier every CTA reads the largest step of the iteration and the schedule stage ends when it is below 2e-4
+// (localize.py:536-552). The evaluation counts of localize.py:182-205 follow in the same launch.
+#include "lw_common.cuh"
+#include "lw_linalg.cuh"
+
+namespace lw {
+
+// ---- grid geometry (mapgrid.py:35-65) --------------------------------------------------------------------
+__device__ __forceinline__ int64_t grid_flat(const lw_prior_grid& g, int ix, int iy, int iz) {
+    if (ix < 0 || iy < 0 || iz < 0 || ix >= g.nx || iy >= g.ny || iz >= g.nz) return -1;
+    return ((int64_t)iz * g.ny + iy) * g.nx + ix;
+}
+
+__device__ __forceinline__ void grid_idx(const lw_prior_grid& g, float x, float y, float z, int& ix, int& iy, int& iz) {
+    ix = ifloor((x - g.origin[0]) * g.inv_cell);
+    iy = ifloor((y - g.origin[1]) * g.inv_cell);
+    iz = ifloor((z - g.origin[2]) * g.inv_cell);
+}
+
+__device__ __forceinline__ void cell_centre(const lw_prior_grid& g, int64_t c, float& x, float& y, float& z) {
+    int64_t ix = c % g.nx, r = c / g.nx;
+    int64_t iy = r % g.ny, iz = r / g.ny;
+    x = g.origin[0] + ((float)ix + 0.5f) * g.cell;
+    y = g.origin[1] + ((float)iy + 0.5f) * g.cell;
+    z = g.origin[2] + ((float)iz + 0.5f) * g.cell;
+}
+
+__device__ __forceinline__ float3 ld_pt(const float* __restrict__ xyz, int64_t i) {
+    return make_float3(__ldg(xyz + 3 * i), __ldg(xyz + 3 * i + 1), __ldg(xyz + 3 * i + 2));
+}
+
+// The map point nearest to w: exact within one cell (every such point lies in the 27 cells around w), otherwise
+// the closest of those cells' flooded seeds, or -1 beyond the band (mapgrid.py:68-102).
+__device__ int nearest_point(const lw_prior_grid& g, float wx, float wy, float wz) {
+    int ix, iy, iz;
+    grid_idx(g, wx, wy, wz, ix, iy, iz);
+    int best = -1;
+    float bd = g.cell * g.cell;
+    int seed = -1;
+    float sd = 1.0e30f;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                int64_t c = grid_flat(g, ix + dx, iy + dy, iz + dz);
+                if (c < 0) continue;
+                int k0 = __ldg(g.start + c), k1 = __ldg(g.start + c + 1);
+                for (int k = k0; k < k1; ++k) {
+                    float3 q = ld_pt(g.xyz, k);
+                    float ex = wx - q.x, ey = wy - q.y, ez = wz - q.z;
+                    float d2 = ex * ex + ey * ey + ez * ez;
+                    if (d2 < bd) {
+                        bd = d2;
+                        best = k;
+                    }
+                }
+                if (best < 0) {
+                    int s = __ldg(g.nn + c);
+                    if (s >= 0) {
+                        float3 q = ld_pt(g.xyz, s);
+                        float ex = wx - q.x, ey = wy - q.y, ez = wz - q.z;
+                        float d2 = ex * ex + ey * ey + ez * ez;
+                        if (d2 < sd) {
+                            sd = d2;
+                            seed = s;
+                        }
+                    }
+                }
+            }
+    return best >= 0 ? best : seed;
+}
+
+// ---- grid build (mapgrid.py:105-170, 272-296) -------------------------------------------------------------
+__global__ void k_seed_clear(lw_prior_grid g) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < g.ncell; c += (int64_t)gridDim.x * blockDim.x)
+        g.seed[c] = ~0ULL;
+}
+
+__global__ void k_seed(lw_prior_grid g) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += (int64_t)gridDim.x * blockDim.x) {
+        float3 p = ld_pt(g.xyz, i);
+        int ix, iy, iz;
+        grid_idx(g, p.x, p.y, p.z, ix, iy, iz);
+        int64_t c = grid_flat(g, ix, iy, iz);
+        if (c < 0) continue;
+        float cx, cy, cz;
+        cell_centre(g, c, cx, cy, cz);
+        int dmm = (int)(len3(p.x - cx, p.y - cy, p.z - cz) * 1000.0f);
+        if (dmm > 255) dmm = 255;
+        atomicMin((unsigned long long*)(g.seed + c), ((unsigned long long)dmm << 32) | (unsigned long long)i);
+    }
+}
+
+__global__ void k_unpack(lw_prior_grid g) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < g.ncell; c += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t v = g.seed[c];
+        g.nn[c] = v == ~0ULL ? -1 : (int32_t)(v & 0xFFFFFFFFULL);
+    }
+}
+
+// One flood step from `in` to `out`: the nearest of the seeds held `step` cells away in the 26 directions.
+__global__ void k_jfa(lw_prior_grid g, const int32_t* __restrict__ in, int32_t* __restrict__ out, int step) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < g.ncell; c += (int64_t)gridDim.x * blockDim.x) {
+        float px, py, pz;
+        cell_centre(g, c, px, py, pz);
+        int ix = (int)(c % g.nx), iy = (int)((c / g.nx) % g.ny), iz = (int)(c / ((int64_t)g.nx * g.ny));
+        int best = in[c];
+        float bd = 1.0e30f;
+        if (best >= 0) {
+            float3 q = ld_pt(g.xyz, best);
+            float ex = px - q.x, ey = py - q.y, ez = pz - q.z;
+            bd = ex * ex + ey * ey + ez * ez;
+        }
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    int64_t j = grid_flat(g, ix + dx * step, iy + dy * step, iz + dz * step);
+                    if (j < 0 || j == c) continue;
+                    int s = in[j];
+                    if (s < 0 || s == best) continue;
+                    float3 q = ld_pt(g.xyz, s);
+                    float ex = px - q.x, ey = py - q.y, ez = pz - q.z;
+                    float d2 = ex * ex + ey * ey + ez * ez;
+                    if (d2 < bd) {
+                        bd = d2;
+                        best = s;
+                    }
+                }
+        out[c] = best;
+    }
+}
+
+__global__ void k_df(lw_prior_grid g) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < g.ncell; c += (int64_t)gridDim.x * blockDim.x) {
+        int s = g.nn[c];
+        if (s < 0) {
+            g.df[c] = 255;
+            continue;
+        }
+        float px, py, pz;
+        cell_centre(g, c, px, py, pz);
+        float3 q = ld_pt(g.xyz, s);
+        float d = len3(px - q.x, py - q.y, pz - q.z) * 100.0f;
+        int v = (int)(d + 0.5f);
+        g.df[c] = (uint8_t)(v < 255 ? v : 255);
+    }
+}
+
+// Distance of each point (posed by T) to the nearest map point, 1e3 beyond the band (mapgrid.py:173-194).
+struct Pose12 {
+    float m[12];
+};
+
+__global__ void k_distances(lw_prior_grid g, const float* __restrict__ pts, int64_t n, Pose12 T, float* __restrict__ out) {
+    const float* M = T.m;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float wx, wy, wz;
+        xform(M, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], wx, wy, wz);
+        int s = nearest_point(g, wx, wy, wz);
+        float d = 1.0e3f;
+        if (s >= 0) {
+            float3 q = ld_pt(g.xyz, s);
+            d = len3(wx - q.x, wy - q.y, wz - q.z);
+        }
+        out[i] = d;
+    }
+}
+
+// ---- batched point-to-plane ICP (localize.py:126-205, 517-565) --------------------------------------------
+
+constexpr int LTERMS = 30;  // H 21, b 6, count, err, weight
+constexpr float PLANAR = 0.5f;  // mapgrid.py:32
+
+struct LocPose {
+    float R[9], tr[3], c[3];
+};
+
+// Per-hypothesis float pose, re-centred on the hypothesis' translation (float32 keeps its precision). The poses
+// change between iterations of the same launch, so they are read through L2 (__ldcg), never the L1 cache.
+__device__ __forceinline__ void loc_pose(const double* T, LocPose& P) {
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) P.R[i * 3 + j] = (float)__ldcg(T + i * 4 + j);
+        const double t = __ldcg(T + i * 4 + 3);
+        P.c[i] = (float)t;
+        P.tr[i] = (float)(t - (double)P.c[i]);
+    }
+}
+
+// The hypothesis and point range of a tile, checked against the batch: h = -1 for a tile to skip.
+__device__ __forceinline__ void tile_range(const lw_loc_batch& b, int tile, int n_hyp, int& h, int& lo, int& hi) {
+    h = __ldg(b.tile_hyp + tile);
+    lo = __ldg(b.tile_lo + tile);
+    if (h < 0 || h >= n_hyp || lo < 0) {
+        h = -1;
+        lo = hi = 0;
+        return;
+    }
+    hi = (int)min((int64_t)__ldg(b.scan_end + h), b.pts_cap);
+}
+
+// One (hypothesis, point) pair's terms (localize.py:144-167) into a[LTERMS].
+__device__ __forceinline__ void loc_terms(const lw_prior_grid& g, const LocPose& P, float4 p, float max_d2, float c2,
+                                          float alpha, float* a) {
+    float lx = P.R[0] * p.x + P.R[1] * p.y + P.R[2] * p.z + P.tr[0];
+    float ly = P.R[3] * p.x + P.R[4] * p.y + P.R[5] * p.z + P.tr[1];
+    float lz = P.R[6] * p.x + P.R[7] * p.y + P.R[8] * p.z + P.tr[2];
+    float wx = lx + P.c[0], wy = ly + P.c[1], wz = lz + P.c[2];
+    int s = nearest_point(g, wx, wy, wz);
+    if (s < 0) return;
+    float3 q = ld_pt(g.xyz, s);
+    float r0 = wx - q.x, r1 = wy - q.y, r2 = wz - q.z;
+    if (r0 * r0 + r1 * r1 + r2 * r2 > max_d2) return;
+    float3 nv = ld_pt(g.nrm, s);
+    float M[6];
+    if (__ldg(g.planar + s) > PLANAR && len3(nv.x, nv.y, nv.z) > 0.5f) {
+        // the normal at full weight, along the surface only a little
+        float b = 1.0f - alpha;
+        M[0] = nv.x * nv.x * b + alpha;
+        M[1] = nv.x * nv.y * b;
+        M[2] = nv.x * nv.z * b;
+        M[3] = nv.y * nv.y * b + alpha;
+        M[4] = nv.y * nv.z * b;
+        M[5] = nv.z * nv.z * b + alpha;
+    } else {
+        // an edge or clutter: a weak point-to-point pull
+        M[0] = M[3] = M[5] = alpha * 4.0f;
+        M[1] = M[2] = M[4] = 0.0f;
+    }
+    float Mr0 = fmaf(M[0], r0, fmaf(M[1], r1, M[2] * r2));
+    float Mr1 = fmaf(M[1], r0, fmaf(M[3], r1, M[4] * r2));
+    float Mr2 = fmaf(M[2], r0, fmaf(M[4], r1, M[5] * r2));
+    float d2 = fmaf(r0, Mr0, fmaf(r1, Mr1, r2 * Mr2));
+    float wgt = 1.0f / (1.0f + d2 / c2);
+    wgt = wgt * wgt;  // Geman-McClure
+    const float C[6][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f},
+                           {0.f, -lz, ly},  {lz, 0.f, -lx}, {-ly, lx, 0.f}};
+    float MC[6][3];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        MC[k][0] = fmaf(M[0], C[k][0], fmaf(M[1], C[k][1], M[2] * C[k][2]));
+        MC[k][1] = fmaf(M[1], C[k][0], fmaf(M[3], C[k][1], M[4] * C[k][2]));
+        MC[k][2] = fmaf(M[2], C[k][0], fmaf(M[4], C[k][1], M[5] * C[k][2]));
+    }
+    int idx = 0;
+#pragma unroll
+    for (int pp = 0; pp < 6; ++pp)
+#pragma unroll
+        for (int qq = pp; qq < 6; ++qq) {
+            a[idx] = fmaf(wgt, fmaf(C[pp][0], MC[qq][0], fmaf(C[pp][1], MC[qq][1], C[pp][2] * MC[qq][2])), a[idx]);
+            ++idx;
+        }
+#pragma unroll
+    for (int pp = 0; pp < 6; ++pp) a[21 + pp] = fmaf(wgt, fmaf(C[pp][0], Mr0, fmaf(C[pp][1], Mr1, C[pp][2] * Mr2)), a[21 + pp]);
+    a[27] += 1.0f;
+    a[28] = fmaf(wgt, d2, a[28]);
+    a[29] += wgt;
+}
+
+struct LocArgs {
+    int n_hyp, n_tiles, n_stages;  // counts, or capacities when b.dims is set
+    float max_d2[8], c2[8];
+    int iters[8];
+    float alpha;
+    float radii[3];
+    int min_count;  // a hypothesis with fewer matched points skips its update (localize.py:538)
+};
+
+__global__ void __launch_bounds__(512, 1)
+    k_loc_icp(lw_prior_grid g, lw_loc_batch b, LocArgs la) {
+    extern __shared__ float smem[];  // [LTERMS][blockDim/32] per-term warp partials
+    __shared__ double sv[32];
+    __shared__ int s_stop;
+    const int tid = threadIdx.x;
+    const int n_hyp = b.dims ? min(__ldg(b.dims), la.n_hyp) : la.n_hyp;
+    const int n_tiles = b.dims ? min(__ldg(b.dims + 1), la.n_tiles) : la.n_tiles;
+    int it_total = 0;
+    for (int stage = 0; stage < la.n_stages; ++stage) {
+        const float max_d2 = la.max_d2[stage];
+        const float c2 = la.c2[stage];
+        for (int it = 0; it < la.iters[stage]; ++it, ++it_total) {
+            // phase A: tiles -> float64 partials
+            for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+                int h, lo, hi;
+                tile_range(b, tile, n_hyp, h, lo, hi);
+                LocPose P;
+                if (h >= 0) loc_pose(b.T + 16 * h, P);
+                float a[LTERMS];
+#pragma unroll
+                for (int k = 0; k < LTERMS; ++k) a[k] = 0.0f;
+                const int i = lo + tid;
+                if (h >= 0 && i < hi && i < lo + (int)blockDim.x)
+                    loc_terms(g, P, __ldg(reinterpret_cast<const float4*>(b.pts) + i), max_d2, c2, la.alpha, a);
+                // warp sums of the 30 terms, then the warps in order (one pass through shared memory)
+                const int lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+                for (int k = 0; k < LTERMS; ++k) {
+                    float v = a[k];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    if (lane == 0) smem[k * nw + w] = v;
+                }
+                __syncthreads();
+                if (tid < LTERMS) {
+                    double sum = 0.0;
+                    for (int ww = 0; ww < nw; ++ww) sum += (double)smem[tid * nw + ww];
+                    b.tile_part[(int64_t)tile * 32 + tid] = sum;
+                }
+                __syncthreads();
+            }
+            if (!grid_barrier(b.bar, b.err, 1)) return;
+            // phase B: per hypothesis, sum its tiles in order and solve (localize.py:537-550)
+            for (int h = blockIdx.x; h < n_hyp; h += gridDim.x) {
+                const int t0 = max(b.hyp_tile[h], 0), t1 = min(b.hyp_tile[h + 1], n_tiles);
+                if (tid < LTERMS) {
+                    double s = 0.0;
+                    for (int t = t0; t < t1; ++t) s += __ldcg(b.tile_part + (int64_t)t * 32 + tid);
+                    sv[tid] = s;
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    double moved = 0.0;
+                    b.count[h] = (int)sv[27];
+                    if (sv[27] >= (double)la.min_count) {
+                        // re-centred sums -> the twist about the world origin: H = A^T Hc A, b = A^T bc
+                        double c[3] = {(double)(float)__ldcg(b.T + 16 * h + 3), (double)(float)__ldcg(b.T + 16 * h + 7),
+                                       (double)(float)__ldcg(b.T + 16 * h + 11)};
+                        double Hc[36], H[36], bc[6], bw[6];
+                        int idx = 0;
+                        for (int p = 0; p < 6; ++p)
+                            for (int q = p; q < 6; ++q) {
+                                Hc[p * 6 + q] = Hc[q * 6 + p] = sv[idx];
+                                ++idx;
+                            }
+                        for (int p = 0; p < 6; ++p) bc[p] = sv[21 + p];
+                        const double K[9] = {0.0, c[2], -c[1], -c[2], 0.0, c[0], c[1], -c[0], 0.0};
+                        double HA[36];
+                        for (int p = 0; p < 6; ++p)
+                            for (int q = 0; q < 6; ++q) {
+                                double x = Hc[p * 6 + q];
+                                if (q >= 3)
+                                    for (int k = 0; k < 3; ++k) x += Hc[p * 6 + k] * K[k * 3 + q - 3];
+                                HA[p * 6 + q] = x;
+                            }
+                        for (int p = 0; p < 6; ++p) {
+                            for (int q = 0; q < 6; ++q) {
+                                double x = HA[p * 6 + q];
+                                if (p >= 3)
+                                    for (int k = 0; k < 3; ++k) x += K[k * 3 + p - 3] * HA[k * 6 + q];
+                                H[p * 6 + q] = x;
+                            }
+                            double x = bc[p];
+                            if (p >= 3)
+                                for (int k = 0; k < 3; ++k) x += K[k * 3 + p - 3] * bc[k];
+                            bw[p] = x;
+                        }
+                        // A = H + diag(1e-3 dg + 1e-9), delta = solve(A, -b)
+                        double Lf[36], rhs[6], delta[6];
+                        for (int p = 0; p < 6; ++p) {
+                            H[p * 7] += 1e-3 * H[p * 7] + 1e-9;
+                            rhs[p] = -bw[p];
+                        }
+                        bool ok = true;
+                        for (int j = 0; j < 6 && ok; ++j) {
+                            double d = H[j * 6 + j];
+                            for (int k = 0; k < j; ++k) d -= Lf[j * 6 + k] * Lf[j * 6 + k];
+                            if (!(d > 0.0)) {
+                                ok = false;
+                                break;
+                            }
+                            d = sqrt(d);
+                            Lf[j * 6 + j] = d;
+                            for (int r = j + 1; r < 6; ++r) {
+                                double x = H[r * 6 + j];
+                                for (int k = 0; k < j; ++k) x -= Lf[r * 6 + k] * Lf[j * 6 + k];
+                                Lf[r * 6 + j] = x / d;
+                            }
+                        }
+                        if (ok) {
+                            double y[6];
+                            for (int r = 0; r < 6; ++r) {
+                                double s = rhs[r];
+                                for (int k = 0; k < r; ++k) s -= Lf[r * 6 + k] * y[k];
+                                y[r] = s / Lf[r * 6 + r];
+                            }
+                            for (int r = 5; r >= 0; --r) {
+                                double s = y[r];
+                                for (int k = r + 1; k < 6; ++k) s -= Lf[k * 6 + r] * delta[k];
+                                delta[r] = s / Lf[r * 6 + r];
+                            }
+                            double T[16];
+                            for (int k = 0; k < 16; ++k) T[k] = __ldcg(b.T + 16 * h + k);
+                            apply_twist(T, delta);
+                            for (int k = 0; k < 16; ++k) b.T[16 * h + k] = T[k];
+                            double nt = sqrt(delta[0] * delta[0] + delta[1] * delta[1] + delta[2] * delta[2]);
+                            double nr = sqrt(delta[3] * delta[3] + delta[4] * delta[4] + delta[5] * delta[5]);
+                            moved = fmax(nt, 5.0 * nr);
+                        }
+                    }
+                    // the largest step of the iteration, as ordered bits of a non-negative float
+                    atomicMax(b.moved + it_total, __float_as_int((float)moved));
+                }
+                __syncthreads();
+            }
+            if (!grid_barrier(b.bar, b.err, 2)) return;
+            if (tid == 0) s_stop = __int_as_float(__ldcg(b.moved + it_total)) < 2e-4f ? 1 : 0;
+            __syncthreads();
+            if (s_stop) {
+                ++it_total;
+                break;
+            }
+        }
+    }
+    // evaluation (localize.py:182-205): points within each radius of their nearest map point, per hypothesis
+    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        int h, lo, hi;
+        tile_range(b, tile, n_hyp, h, lo, hi);
+        float M[12];
+        for (int k = 0; k < 12; ++k) M[k] = h >= 0 ? (float)__ldcg(b.T + 16 * h + k) : 0.0f;
+        int c0 = 0, c1 = 0, c2 = 0;
+        const int i = lo + tid;
+        if (h >= 0 && i < hi && i < lo + (int)blockDim.x) {
+            float4 p = __ldg(reinterpret_cast<const float4*>(b.pts) + i);
+            float wx, wy, wz;
+            xform(M, p.x, p.y, p.z, wx, wy, wz);
+            int s = nearest_point(g, wx, wy, wz);
+            if (s >= 0) {
+                float3 q = ld_pt(g.xyz, s);
+                float d = len3(wx - q.x, wy - q.y, wz - q.z);
+                c0 = d < la.radii[0];
+                c1 = d < la.radii[1];
+                c2 = d < la.radii[2];
+            }
+        }
+        int t0 = __syncthreads_count(c0), t1 = __syncthreads_count(c1), t2 = __syncthreads_count(c2);
+        if (tid == 0 && h >= 0) {
+            atomicAdd(b.eval + 3 * h + 0, t0);
+            atomicAdd(b.eval + 3 * h + 1, t1);
+            atomicAdd(b.eval + 3 * h + 2, t2);
+        }
+    }
+    if (blockIdx.x == 0 && tid == 0) *b.iters_run = it_total;
+}
+
+// Clears what the launch accumulates into. The barrier's arrival count is zeroed too: a launch that gave up at a
+// barrier may have left it part counted (its generation word needs no reset).
+__global__ void k_loc_reset(lw_loc_batch b, int n_hyp, int max_iters) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < max_iters; i += gridDim.x * blockDim.x) b.moved[i] = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n_hyp; i += gridDim.x * blockDim.x) b.eval[i] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *b.err = 0;
+        b.bar[0] = 0u;
+    }
+}
+
+}  // namespace lw
+
+using namespace lw;
+
+static int check_grid(const lw_prior_grid* g, const char* who) {
+    if (!g || !g->xyz || !g->start || !g->nn || g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || g->cell <= 0.0f)
+        return set_error(LW_EINVAL, "%s: incomplete prior grid", who);
+    if ((int64_t)g->nx * g->ny * g->nz != g->ncell) return set_error(LW_EINVAL, "%s: ncell != nx*ny*nz", who);
+    if (g->n >= 0x7FFFFFFF) return set_error(LW_ECAPACITY, "%s: %lld map points exceed int32 indices", who, (long long)g->n);
+    return LW_OK;
+}
+
+extern "C" {
+
+int lw_prior_grid_build(lw_prior_grid* g, void* stream) {
+    int r = check_grid(g, "lw_prior_grid_build");
+    if (r != LW_OK) return r;
+    if (!g->seed || !g->nn2 || !g->df) return set_error(LW_EINVAL, "lw_prior_grid_build: missing build scratch");
+    cudaStream_t s = (cudaStream_t)stream;
+    int gc = blocks_for(g->ncell, 256, 16 * device_sms());
+    int gp = blocks_for(g->n, 256, 16 * device_sms());
+    ProfScope prof("grid_build", s);
+    k_seed_clear<<<gc, 256, 0, s>>>(*g);
+    k_seed<<<gp, 256, 0, s>>>(*g);
+    k_unpack<<<gc, 256, 0, s>>>(*g);
+    const int steps[5] = {8, 4, 2, 1, 1};  // mapgrid.py:31
+    int32_t* a = g->nn;
+    int32_t* bbuf = g->nn2;
+    for (int k = 0; k < 5; ++k) {
+        k_jfa<<<gc, 256, 0, s>>>(*g, a, bbuf, steps[k]);
+        int32_t* t = a;
+        a = bbuf;
+        bbuf = t;
+    }
+    if (a != g->nn) LW_CUDA(cudaMemcpyAsync(g->nn, a, g->ncell * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    k_df<<<gc, 256, 0, s>>>(*g);
+    LW_LAUNCHED("lw_prior_grid_build");
+    count_launches(9);
+    return LW_OK;
+}
+
+int lw_prior_distances(const lw_prior_grid* g, const float* pts, int64_t n, const double* T_host, float* out,
+                       void* stream) {
+    int r = check_grid(g, "lw_prior_distances");
+    if (r != LW_OK) return r;
+    if (!pts || !T_host || !out) return set_error(LW_EINVAL, "lw_prior_distances: null argument");
+    if (n <= 0) return LW_OK;
+    Pose12 T;
+    for (int k = 0; k < 12; ++k) T.m[k] = (float)T_host[k];
+    k_distances<<<blocks_for(n, 256, 16 * device_sms()), 256, 0, (cudaStream_t)stream>>>(*g, pts, n, T, out);
+    LW_LAUNCHED("lw_prior_distances");
+    count_launches(1);
+    return LW_OK;
+}
+
+int lw_loc_icp_batch(const lw_prior_grid* g, lw_loc_batch* b, int32_t n_hyp, int32_t n_tiles, int32_t tile,
+                     int32_t n_stages, const double* dmax, const int32_t* iters, float alpha, int32_t min_count,
+                     int32_t grid, void* stream) {
+    int r = check_grid(g, "lw_loc_icp_batch");
+    if (r != LW_OK) return r;
+    if (!b || (n_stages > 0 && (!dmax || !iters)) || n_stages < 0 || n_stages > 8 || n_hyp < 1 || n_tiles < 1)
+        return set_error(LW_EINVAL, "lw_loc_icp_batch: bad arguments");
+    if (!b->pts || !b->scan_end || !b->tile_hyp || !b->tile_lo || !b->hyp_tile || !b->T || !b->tile_part ||
+        !b->moved || !b->count || !b->eval || !b->bar || !b->err || !b->iters_run || b->pts_cap < 0)
+        return set_error(LW_EINVAL, "lw_loc_icp_batch: incomplete batch buffers");
+    if (tile != 128 && tile != 256 && tile != 512) return set_error(LW_EINVAL, "lw_loc_icp_batch: tile must be 128/256/512");
+    if (!g->nrm || !g->planar) return set_error(LW_EINVAL, "lw_loc_icp_batch: the grid needs normals and planarity");
+    LocArgs la{};
+    la.n_hyp = n_hyp;
+    la.n_tiles = n_tiles;
+    la.n_stages = n_stages;
+    int total_iters = 0;
+    for (int k = 0; k < n_stages; ++k) {
+        if (iters[k] < 0 || !(dmax[k] > 0.0)) return set_error(LW_EINVAL, "lw_loc_icp_batch: stage %d", k);
+        la.max_d2[k] = (float)(dmax[k] * dmax[k]);  // localize.py:541: dmax * dmax
+        const double half = dmax[k] * 0.5;
+        la.c2[k] = (float)(half * half);  // localize.py:530: (dmax * 0.5) ** 2
+        la.iters[k] = iters[k];
+        total_iters += iters[k];
+    }
+    if (total_iters > b->moved_cap) return set_error(LW_ECAPACITY, "lw_loc_icp_batch: %d iterations > moved_cap", total_iters);
+    la.alpha = alpha;
+    la.radii[0] = 0.03f;  // EVAL_RADII (localize.py:47)
+    la.radii[1] = 0.05f;
+    la.radii[2] = 0.10f;
+    la.min_count = min_count;
+    cudaStream_t s = (cudaStream_t)stream;
+    int sms = device_sms();
+    int per_sm = 0;
+    const size_t dyn = (size_t)LTERMS * (tile / 32) * sizeof(float);
+    LW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_loc_icp, tile, dyn));
+    if (per_sm < 1) return set_error(LW_EINVAL, "lw_loc_icp_batch: tile %d does not fit on an SM", tile);
+    int max_grid = per_sm * sms;
+    if (grid <= 0 || grid > max_grid) grid = max_grid;
+    if (grid > b->grid_cap) grid = b->grid_cap;
+    ProfScope prof("loc_icp", s);
+    k_loc_reset<<<16, 256, 0, s>>>(*b, n_hyp, total_iters);
+    // a cooperative launch (every CTA resident: the grid barriers rely on it), made through cudaLaunchKernelEx
+    // so that it can also be captured into a CUDA graph
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(tile);
+    cfg.dynamicSmemBytes = dyn;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    LW_CUDA(cudaLaunchKernelEx(&cfg, k_loc_icp, *g, *b, la));
+    LW_LAUNCHED("lw_loc_icp_batch");
+    count_launches(2);
+    return LW_OK;
+}
+
+}  // extern "C"

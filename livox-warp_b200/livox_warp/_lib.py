@@ -87,6 +87,20 @@ class ClusterBuf(C.Structure):
     _fields_ = [(n, P) for n in PTRS] + [("cap", i64), ("pt_cap", i64), ("edge_cap", i64)]
 
 
+class PriorGrid(C.Structure):
+    """mapgrid.Grid (mapgrid.py:35-43) plus the map arrays the grid kernels read."""
+
+    _fields_ = [("xyz", P), ("nrm", P), ("planar", P), ("start", P), ("nn", P), ("df", P), ("seed", P), ("nn2", P),
+                ("origin", f32 * 3), ("cell", f32), ("inv_cell", f32), ("nx", i32), ("ny", i32), ("nz", i32),
+                ("pad_", i32), ("n", i64), ("ncell", i64)]
+
+
+class LocBatch(C.Structure):
+    PTRS = ("pts", "scan_end", "tile_hyp", "tile_lo", "hyp_tile", "T", "tile_part", "moved", "count", "eval", "bar",
+            "err", "iters_run", "dims")
+    _fields_ = [(n, P) for n in PTRS] + [("pts_cap", i64), ("moved_cap", i32), ("grid_cap", i32)]
+
+
 class View(C.Structure):
     """gpu.View (gpu.py:76-98): the filters and labels the map kernels read."""
 
@@ -134,6 +148,10 @@ _SIGS = {
     "lw_frame_ids": (i32, [P, i64, f32, P, P]),
     "lw_ground": (i32, [P, i32, P, P, i64, f32, f32, i32, f32, f32, i32, f32, P, P, P, P, P]),
     "lw_cluster": (i32, [P, i32, P, i32, P, i64, f32, f32, f32, i32, C.POINTER(ClusterBuf), P, P]),
+    "lw_prior_grid_build": (i32, [C.POINTER(PriorGrid), P]),
+    "lw_prior_distances": (i32, [C.POINTER(PriorGrid), P, i64, C.POINTER(f64), P, P]),
+    "lw_loc_icp_batch": (i32, [C.POINTER(PriorGrid), C.POINTER(LocBatch), i32, i32, i32, i32, C.POINTER(f64),
+                               C.POINTER(i32), f32, i32, i32, P]),
 }
 
 _lib = None

@@ -412,3 +412,66 @@ def sample_surfaces(scene: Scene, spacing: float, seed: int, jitter: float = 0.0
         face(b0, ey * s[1], ez * s[2], -ex)
         face(b0 + ex * s[0], ey * s[1], ez * s[2], ex)
     return np.concatenate(pts).astype(np.float32), np.concatenate(nrm).astype(np.float32)
+
+
+# ---- global localisation cases -----------------------------------------------------------------------------------
+
+
+def spin_scan(scene: Scene, T: np.ndarray, n: int, seed: int, noise: float = 0.01, elev_deg=(-7.0, 52.0),
+              max_range: float = 40.0) -> np.ndarray:
+    """A static 360-degree scan from pose T (sensor to world): n rays with azimuth uniform in [0, 2 pi) and
+    elevation uniform in elev_deg (a Mid-360-like field of view), Gaussian range noise; the (m <= n) hits in the
+    sensor frame, float32."""
+    rng = np.random.default_rng(seed)
+    az = rng.uniform(0.0, 2.0 * math.pi, n)
+    el = np.radians(rng.uniform(elev_deg[0], elev_deg[1], n))
+    d = np.stack([np.cos(el) * np.cos(az), np.cos(el) * np.sin(az), np.sin(el)], axis=1)
+    T = np.asarray(T, dtype=np.float64)
+    o = np.broadcast_to(T[:3, 3], (n, 3))
+    dw = d @ T[:3, :3].T
+    r = raycast(np.ascontiguousarray(o), dw, scene, np.zeros(n))
+    ok = np.isfinite(r) & (r < max_range)
+    rr = r + rng.normal(0.0, noise, n)
+    return (d * rr[:, None])[ok].astype(np.float32)
+
+
+def free_poses(scene: Scene, n: int, seed: int, z: float = 1.2, margin: float = 0.6, grid: float = 0.0):
+    """n sensor poses in free space at height z with yaw uniform in [0, 2 pi): (T (n, 4, 4) sensor to world).
+    With grid > 0 the positions lie on that xy grid (distinct cells, drawn without replacement)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    if grid > 0:
+        xs = np.arange(scene.room_lo[0] + grid, scene.room_hi[0], grid)
+        ys = np.arange(scene.room_lo[1] + grid, scene.room_hi[1], grid)
+        P = np.stack(np.meshgrid(xs, ys, indexing="ij"), axis=-1).reshape(-1, 2)
+        P = np.concatenate([P, np.full((len(P), 1), z)], axis=1)
+        P = P[scene.free(P, margin)]
+        if len(P) < n:
+            raise RuntimeError(f"only {len(P)} free grid positions for {n} poses")
+        P = P[rng.choice(len(P), n, replace=False)]
+    else:
+        P = np.zeros((0, 3))
+        while len(P) < n:
+            c = np.concatenate([rng.uniform(scene.room_lo[:2], scene.room_hi[:2], (4 * n, 2)),
+                                np.full((4 * n, 1), z)], axis=1)
+            P = np.concatenate([P, c[scene.free(c, margin)]])[:n]
+    yaw = rng.uniform(0.0, 2.0 * math.pi, n)
+    for p, a in zip(P, yaw):
+        out.append(_pose(Rotation.from_euler("z", a).as_matrix(), p))
+    return np.stack(out)
+
+
+def perturb(T: np.ndarray, seed: int, trans: float, yaw_deg: float, tilt_deg: float = 0.0) -> np.ndarray:
+    """Poses T (n, 4, 4) moved by a uniform xy offset of at most `trans` per axis, a yaw of at most yaw_deg and
+    a roll / pitch of at most tilt_deg (a coarse search's quantisation error)."""
+    rng = np.random.default_rng(seed)
+    T = np.array(T, dtype=np.float64, copy=True)
+    n = len(T)
+    dxy = rng.uniform(-trans, trans, (n, 2))
+    ang = np.radians(np.stack([rng.uniform(-tilt_deg, tilt_deg, n), rng.uniform(-tilt_deg, tilt_deg, n),
+                               rng.uniform(-yaw_deg, yaw_deg, n)], axis=1))
+    for i in range(n):
+        R = Rotation.from_euler("xyz", ang[i]).as_matrix()
+        T[i, :3, :3] = R @ T[i, :3, :3]
+        T[i, :2, 3] += dxy[i]
+    return T

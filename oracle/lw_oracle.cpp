@@ -7,6 +7,8 @@
 //   thinning                   odom.py:126-160         registration insert odom.py:186-230
 //   ICP accumulation           odom.py:233-375         integration insert  gpu.py:373-412
 //   carving + local_plane      gpu.py:415-593          map classification  gpu.py:286-299, 596-634, 699-747
+//   ground grid                perception.py:29-111    clusters            perception.py:114-271
+//   prior grid + nearest_point mapgrid.py:35-194       batched ICP + eval  localize.py:126-205, 517-565
 // The reference's nondeterministic choices are fixed the way the GPU build fixes them: the lowest point index
 // claims a thinning voxel, per-voxel sums are exact int64 fixed point (the units of include/livox_b200.h),
 // and 4096-point caps keep the first points in index order. Float expressions are written in the evaluation
@@ -767,6 +769,329 @@ int64_t or_cluster(const float* xyz, int stride, const int32_t* gnd, int use_gro
     *k_all = k;
     for (int64_t i = 0; i < n; ++i) out_cid[i] = pt_node[i] < 0 ? -1 : dense[labels[pt_node[i]]];
     return k < max_out ? k : max_out;
+}
+
+
+// ---- prior-map grid (mapgrid.py) -----------------------------------------------------------------------------
+// The grid geometry, nearest_point and the build follow mapgrid.py:35-170 with two deliberate differences that the
+// GPU build shares: the seed key is 64 bits (distance mm << 32 | index; the reference's 32-bit key held 2^23 - 1
+// points), and each flood step reads one buffer and writes another (the reference floods in place, so its result
+// depends on thread timing).
+
+typedef struct or_grid {
+    const float* xyz;
+    const float* nrm;
+    const float* planar;
+    const int32_t* start;
+    const int32_t* nn;
+    float origin[3];
+    float cell, inv_cell;
+    int32_t nx, ny, nz, pad_;
+} or_grid;
+
+}  // extern "C"
+
+static inline int64_t og_flat(const or_grid& g, int ix, int iy, int iz) {  // grid_flat mapgrid.py:46-50
+    if (ix < 0 || iy < 0 || iz < 0 || ix >= g.nx || iy >= g.ny || iz >= g.nz) return -1;
+    return ((int64_t)iz * g.ny + iy) * g.nx + ix;
+}
+static inline void og_centre(const or_grid& g, int64_t c, float& x, float& y, float& z) {  // cell_centre :59-65
+    int64_t ix = c % g.nx, r = c / g.nx;
+    int64_t iy = r % g.ny, iz = r / g.ny;
+    x = g.origin[0] + ((float)ix + 0.5f) * g.cell;
+    y = g.origin[1] + ((float)iy + 0.5f) * g.cell;
+    z = g.origin[2] + ((float)iz + 0.5f) * g.cell;
+}
+// nearest_point mapgrid.py:68-102
+static int og_nearest(const or_grid& g, float wx, float wy, float wz) {
+    int ix = ifloor((wx - g.origin[0]) * g.inv_cell);
+    int iy = ifloor((wy - g.origin[1]) * g.inv_cell);
+    int iz = ifloor((wz - g.origin[2]) * g.inv_cell);
+    int best = -1, seed = -1;
+    float bd = g.cell * g.cell, sd = 1.0e30f;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                int64_t c = og_flat(g, ix + dx, iy + dy, iz + dz);
+                if (c < 0) continue;
+                for (int k = g.start[c]; k < g.start[c + 1]; ++k) {
+                    const float* q = g.xyz + 3 * (int64_t)k;
+                    float ex = wx - q[0], ey = wy - q[1], ez = wz - q[2];
+                    float d2 = ex * ex + ey * ey + ez * ez;
+                    if (d2 < bd) {
+                        bd = d2;
+                        best = k;
+                    }
+                }
+                if (best < 0) {
+                    int s = g.nn[c];
+                    if (s >= 0) {
+                        const float* q = g.xyz + 3 * (int64_t)s;
+                        float ex = wx - q[0], ey = wy - q[1], ez = wz - q[2];
+                        float d2 = ex * ex + ey * ey + ez * ez;
+                        if (d2 < sd) {
+                            sd = d2;
+                            seed = s;
+                        }
+                    }
+                }
+            }
+    return best >= 0 ? best : seed;
+}
+
+extern "C" {
+
+// k_seed, k_unpack, k_jfa x JFA_STEPS, k_df (mapgrid.py:105-170, PriorGrid.build :272-296) into nn and df.
+void or_grid_build(const or_grid* gp, int64_t n, int32_t* nn, uint8_t* df, int threads) {
+    const or_grid& g = *gp;
+    const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
+    std::vector<uint64_t> seed(ncell, ~0ULL);
+    for (int64_t i = 0; i < n; ++i) {
+        const float* p = g.xyz + 3 * i;
+        int64_t c = og_flat(g, ifloor((p[0] - g.origin[0]) * g.inv_cell), ifloor((p[1] - g.origin[1]) * g.inv_cell),
+                            ifloor((p[2] - g.origin[2]) * g.inv_cell));
+        if (c < 0) continue;
+        float cx, cy, cz;
+        og_centre(g, c, cx, cy, cz);
+        int dmm = (int)(len3(p[0] - cx, p[1] - cy, p[2] - cz) * 1000.0f);
+        if (dmm > 255) dmm = 255;
+        uint64_t key = ((uint64_t)dmm << 32) | (uint64_t)i;
+        if (key < seed[c]) seed[c] = key;
+    }
+    std::vector<int32_t> a(ncell), b(ncell);
+    for (int64_t c = 0; c < ncell; ++c) a[c] = seed[c] == ~0ULL ? -1 : (int32_t)(seed[c] & 0xFFFFFFFFULL);
+    const int steps[5] = {8, 4, 2, 1, 1};
+    for (int st = 0; st < 5; ++st) {
+        const int step = steps[st];
+#pragma omp parallel for num_threads(threads) schedule(static)
+        for (int64_t c = 0; c < ncell; ++c) {
+            float px, py, pz;
+            og_centre(g, c, px, py, pz);
+            int ix = (int)(c % g.nx), iy = (int)((c / g.nx) % g.ny), iz = (int)(c / ((int64_t)g.nx * g.ny));
+            int best = a[c];
+            float bd = 1.0e30f;
+            if (best >= 0) {
+                const float* q = g.xyz + 3 * (int64_t)best;
+                float ex = px - q[0], ey = py - q[1], ez = pz - q[2];
+                bd = ex * ex + ey * ey + ez * ez;
+            }
+            for (int dz = -1; dz <= 1; ++dz)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        int64_t j = og_flat(g, ix + dx * step, iy + dy * step, iz + dz * step);
+                        if (j < 0 || j == c) continue;
+                        int s = a[j];
+                        if (s < 0 || s == best) continue;
+                        const float* q = g.xyz + 3 * (int64_t)s;
+                        float ex = px - q[0], ey = py - q[1], ez = pz - q[2];
+                        float d2 = ex * ex + ey * ey + ez * ez;
+                        if (d2 < bd) {
+                            bd = d2;
+                            best = s;
+                        }
+                    }
+            b[c] = best;
+        }
+        a.swap(b);
+    }
+    for (int64_t c = 0; c < ncell; ++c) {
+        nn[c] = a[c];
+        if (a[c] < 0) {
+            df[c] = 255;
+            continue;
+        }
+        float px, py, pz;
+        og_centre(g, c, px, py, pz);
+        const float* q = g.xyz + 3 * (int64_t)a[c];
+        float d = len3(px - q[0], py - q[1], pz - q[2]) * 100.0f;
+        int v = (int)(d + 0.5f);
+        df[c] = (uint8_t)(v < 255 ? v : 255);
+    }
+}
+
+// nearest_point for n query points (mapgrid.py:68-102).
+void or_nearest(const or_grid* g, const float* w, int64_t n, int32_t* out, int threads) {
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (int64_t i = 0; i < n; ++i) out[i] = og_nearest(*g, w[3 * i], w[3 * i + 1], w[3 * i + 2]);
+}
+
+// k_changes_T (mapgrid.py:173-194): distance of each point posed by T (float32, as the kernel's mat44) to the map.
+void or_prior_distances(const or_grid* g, const float* pts, int64_t n, const double* T, float* out, int threads) {
+    float M[12];
+    for (int k = 0; k < 12; ++k) M[k] = (float)T[k];
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        const float* p = pts + 3 * i;
+        float wx = M[0] * p[0] + M[1] * p[1] + M[2] * p[2] + M[3];
+        float wy = M[4] * p[0] + M[5] * p[1] + M[6] * p[2] + M[7];
+        float wz = M[8] * p[0] + M[9] * p[1] + M[10] * p[2] + M[11];
+        int s = og_nearest(*g, wx, wy, wz);
+        float d = 1.0e3f;
+        if (s >= 0) {
+            const float* q = g->xyz + 3 * (int64_t)s;
+            d = len3(wx - q[0], wy - q[1], wz - q[2]);
+        }
+        out[i] = d;
+    }
+}
+
+}  // extern "C"
+
+// ---- batched point-to-plane ICP (localize.py) ------------------------------------------------------------------
+
+// solve A x = r by Gaussian elimination with partial pivoting (numpy.linalg.solve); false when A is singular
+static bool or_solve6(double A[36], double r[6], double x[6]) {
+    int piv[6] = {0, 1, 2, 3, 4, 5};
+    for (int c = 0; c < 6; ++c) {
+        int p = c;
+        for (int k = c + 1; k < 6; ++k)
+            if (fabs(A[piv[k] * 6 + c]) > fabs(A[piv[p] * 6 + c])) p = k;
+        std::swap(piv[c], piv[p]);
+        double d = A[piv[c] * 6 + c];
+        if (d == 0.0) return false;
+        for (int k = c + 1; k < 6; ++k) {
+            double f = A[piv[k] * 6 + c] / d;
+            for (int j = c; j < 6; ++j) A[piv[k] * 6 + j] -= f * A[piv[c] * 6 + j];
+            r[piv[k]] -= f * r[piv[c]];
+        }
+    }
+    for (int c = 5; c >= 0; --c) {
+        double s = r[piv[c]];
+        for (int j = c + 1; j < 6; ++j) s -= A[piv[c] * 6 + j] * x[j];
+        x[c] = s / A[piv[c] * 6 + c];
+    }
+    return true;
+}
+
+// _twist_apply (localize.py:227-233): T <- [exp(delta_r), delta_t] T, the rotation by Rodrigues' formula.
+static void or_twist_apply(double* T, const double* d) {
+    double th = sqrt(d[3] * d[3] + d[4] * d[4] + d[5] * d[5]);
+    double R[9];
+    if (th < 1e-12) {
+        const double I[9] = {1, -d[5], d[4], d[5], 1, -d[3], -d[4], d[3], 1};
+        for (int k = 0; k < 9; ++k) R[k] = I[k];
+    } else {
+        double x = d[3] / th, y = d[4] / th, z = d[5] / th, s = sin(th), c = cos(th), v = 1.0 - c;
+        const double Q[9] = {c + x * x * v, x * y * v - z * s, x * z * v + y * s,
+                             y * x * v + z * s, c + y * y * v, y * z * v - x * s,
+                             z * x * v - y * s, z * y * v + x * s, c + z * z * v};
+        for (int k = 0; k < 9; ++k) R[k] = Q[k];
+    }
+    double o[12];
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) o[i * 4 + j] = R[i * 3] * T[j] + R[i * 3 + 1] * T[4 + j] + R[i * 3 + 2] * T[8 + j];
+        o[i * 4 + 3] = R[i * 3] * T[3] + R[i * 3 + 1] * T[7] + R[i * 3 + 2] * T[11] + d[i];
+    }
+    for (int k = 0; k < 12; ++k) T[k] = o[k];
+}
+
+static inline void or_posef(const double* T, float* M) {
+    for (int k = 0; k < 12; ++k) M[k] = (float)T[k];
+}
+static inline void or_xform(const float* M, const float* p, float& wx, float& wy, float& wz) {
+    wx = M[0] * p[0] + M[1] * p[1] + M[2] * p[2] + M[3];
+    wy = M[4] * p[0] + M[5] * p[1] + M[6] * p[2] + M[7];
+    wz = M[8] * p[0] + M[9] * p[1] + M[10] * p[2] + M[11];
+}
+
+extern "C" {
+
+// GlobalLocalizer._icp (localize.py:517-553) with k_icp_batch / k_reduce_batch (:126-179) in float64: every
+// hypothesis h registers pts4[scan_lo[h] .. scan_hi[h]) (x, y, z, unused) from T[16h..] (row-major, updated).
+// The correspondences are chosen in float32 as the kernel does (the pose cast to float32, w = T p); the terms
+// are formed and summed in float64. max_d2 and c2 are the float32 values the kernel receives.
+void or_loc_icp(const or_grid* gp, const float* pts4, const int32_t* scan_lo, const int32_t* scan_hi, int n_hyp,
+                double* T, int n_stages, const float* max_d2, const float* c2, const int32_t* iters, float alpha,
+                int min_count, int32_t* count, int32_t* iters_run, int threads) {
+    const or_grid& g = *gp;
+    const float PLANAR_F = 0.5f;
+    int run = 0;
+    std::vector<double> moved(n_hyp);
+    for (int st = 0; st < n_stages; ++st) {
+        for (int it = 0; it < iters[st]; ++it) {
+            ++run;
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 1)
+            for (int h = 0; h < n_hyp; ++h) {
+                float M[12];
+                or_posef(T + 16 * h, M);
+                double H[36] = {0}, bv[6] = {0};
+                int64_t cnt = 0;
+                for (int64_t i = scan_lo[h]; i < scan_hi[h]; ++i) {
+                    float wx, wy, wz;
+                    or_xform(M, pts4 + 4 * i, wx, wy, wz);
+                    int s = og_nearest(g, wx, wy, wz);
+                    if (s < 0) continue;
+                    const float* q = g.xyz + 3 * (int64_t)s;
+                    float rx = wx - q[0], ry = wy - q[1], rz = wz - q[2];
+                    if (rx * rx + ry * ry + rz * rz > max_d2[st]) continue;
+                    const float* nv = g.nrm + 3 * (int64_t)s;
+                    double Mm[9];
+                    if (g.planar[s] > PLANAR_F && len3(nv[0], nv[1], nv[2]) > 0.5f) {
+                        double a = alpha, b1 = 1.0 - (double)alpha, n3[3] = {nv[0], nv[1], nv[2]};
+                        for (int r = 0; r < 3; ++r)
+                            for (int c = 0; c < 3; ++c) Mm[r * 3 + c] = n3[r] * n3[c] * b1 + (r == c ? a : 0.0);
+                    } else {
+                        for (int k = 0; k < 9; ++k) Mm[k] = (k % 4 == 0) ? 4.0 * alpha : 0.0;
+                    }
+                    double r3[3] = {rx, ry, rz}, Mr[3];
+                    for (int r = 0; r < 3; ++r) Mr[r] = Mm[r * 3] * r3[0] + Mm[r * 3 + 1] * r3[1] + Mm[r * 3 + 2] * r3[2];
+                    double d2 = r3[0] * Mr[0] + r3[1] * Mr[1] + r3[2] * Mr[2];
+                    double wgt = 1.0 / (1.0 + d2 / (double)c2[st]);
+                    wgt *= wgt;
+                    const double W[3] = {wx, wy, wz};
+                    // J = [I | -[w]x] (localize.py:160-162)
+                    const double J[3][6] = {{1, 0, 0, 0, W[2], -W[1]}, {0, 1, 0, -W[2], 0, W[0]}, {0, 0, 1, W[1], -W[0], 0}};
+                    double MJ[3][6];
+                    for (int r = 0; r < 3; ++r)
+                        for (int c = 0; c < 6; ++c) MJ[r][c] = Mm[r * 3] * J[0][c] + Mm[r * 3 + 1] * J[1][c] + Mm[r * 3 + 2] * J[2][c];
+                    for (int p = 0; p < 6; ++p) {
+                        for (int qq = 0; qq < 6; ++qq) H[p * 6 + qq] += wgt * (J[0][p] * MJ[0][qq] + J[1][p] * MJ[1][qq] + J[2][p] * MJ[2][qq]);
+                        bv[p] += wgt * (J[0][p] * Mr[0] + J[1][p] * Mr[1] + J[2][p] * Mr[2]);
+                    }
+                    ++cnt;
+                }
+                count[h] = (int32_t)cnt;
+                moved[h] = 0.0;
+                if (cnt < min_count) continue;
+                double A[36], rhs[6], delta[6];
+                for (int k = 0; k < 36; ++k) A[k] = H[k];
+                for (int p = 0; p < 6; ++p) {
+                    A[p * 7] += 1e-3 * H[p * 7] + 1e-9;
+                    rhs[p] = -bv[p];
+                }
+                if (!or_solve6(A, rhs, delta)) continue;
+                or_twist_apply(T + 16 * h, delta);
+                double nt = sqrt(delta[0] * delta[0] + delta[1] * delta[1] + delta[2] * delta[2]);
+                double nr = sqrt(delta[3] * delta[3] + delta[4] * delta[4] + delta[5] * delta[5]);
+                moved[h] = std::max(nt, 5.0 * nr);
+            }
+            double mv = 0.0;
+            for (int h = 0; h < n_hyp; ++h) mv = std::max(mv, moved[h]);
+            if (mv < 2e-4) break;
+        }
+    }
+    *iters_run = run;
+}
+
+// k_eval_batch (localize.py:182-205): per hypothesis, the points within radii[k] of their nearest map point.
+void or_loc_eval(const or_grid* gp, const float* pts4, const int32_t* scan_lo, const int32_t* scan_hi, int n_hyp,
+                 const double* T, const float* radii, int32_t* counts, int threads) {
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 1)
+    for (int h = 0; h < n_hyp; ++h) {
+        float M[12];
+        or_posef(T + 16 * h, M);
+        int32_t c[3] = {0, 0, 0};
+        for (int64_t i = scan_lo[h]; i < scan_hi[h]; ++i) {
+            float wx, wy, wz;
+            or_xform(M, pts4 + 4 * i, wx, wy, wz);
+            int s = og_nearest(*gp, wx, wy, wz);
+            if (s < 0) continue;
+            const float* q = gp->xyz + 3 * (int64_t)s;
+            float d = len3(wx - q[0], wy - q[1], wz - q[2]);
+            for (int k = 0; k < 3; ++k) c[k] += d < radii[k];
+        }
+        for (int k = 0; k < 3; ++k) counts[3 * h + k] = c[k];
+    }
 }
 
 }  // extern "C"

@@ -13,6 +13,9 @@ Two layers:
     (_finalize :642-657, _estimate :659-680, _update_velocity :682-694, _is_keyframe :712-717), written with
     numpy and scipy exactly as the reference's host code is -- so the pose oracle is float64 end to end.
 
+The prior-map grid and the batched localisation ICP (mapgrid.py, localize.py) follow at the end of this file:
+prepare (mapgrid.py:216-243) in numpy, the kernels in lw_oracle.cpp, the ICP's terms and solve in float64.
+
 Parity of the kernel restatement against the reference is unpinned (NVIDIA Warp is not installed here and the
 reference ships no golden vectors for its kernels); the host step is pinned against the reference's own
 functions through tests/golden/host_solve.npz (see tests/golden/make_golden.py).
@@ -45,6 +48,12 @@ MAX_FRAME_JUMP = 1.5
 _lib = None
 
 
+class OrGrid(C.Structure):
+    _fields_ = [("xyz", C.c_void_p), ("nrm", C.c_void_p), ("planar", C.c_void_p), ("start", C.c_void_p),
+                ("nn", C.c_void_p), ("origin", C.c_float * 3), ("cell", C.c_float), ("inv_cell", C.c_float),
+                ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("pad_", C.c_int32)]
+
+
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
@@ -74,6 +83,11 @@ def lib() -> C.CDLL:
             "or_map_build": (i64, [i64, P, P, P, P, P, P, P, i32, P, P, P, P]),
             "or_ground": (None, [P, i32, P, i64, f32, f32, i32, f32, f32, i32, f32, P, P]),
             "or_cluster": (i64, [P, i32, P, i32, i64, f32, f32, f32, i32, P, P, P, P, P, P, P, P]),
+            "or_grid_build": (None, [C.POINTER(OrGrid), i64, P, P, i32]),
+            "or_nearest": (None, [C.POINTER(OrGrid), P, i64, P, i32]),
+            "or_prior_distances": (None, [C.POINTER(OrGrid), P, i64, P, P, i32]),
+            "or_loc_icp": (None, [C.POINTER(OrGrid), P, P, P, i32, P, i32, P, P, P, f32, i32, P, P, i32]),
+            "or_loc_eval": (None, [C.POINTER(OrGrid), P, P, P, i32, P, P, P, i32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(_lib, name)
@@ -488,3 +502,103 @@ def pose_error(A: np.ndarray, B: np.ndarray):
     """(metres, degrees) between two 4x4 poses."""
     d = np.linalg.inv(A) @ B
     return float(np.linalg.norm(d[:3, 3])), float(np.degrees(np.linalg.norm(Rotation.from_matrix(d[:3, :3]).as_rotvec())))
+
+
+# ---- prior-map grid and batched localisation (mapgrid.py, localize.py) ------------------------------------------
+
+GRID_CELL = 0.05  # mapgrid.py:24
+EVAL_RADII = (0.03, 0.05, 0.10)  # localize.py:47
+
+
+def prior_prepare(xyz, normal, planarity=None, cell: float = GRID_CELL, pad: float = 0.6) -> dict:
+    """PriorGrid.prepare (mapgrid.py:216-243): points sorted by cell (stable), unit normals, the cell prefix."""
+    xyz = np.asarray(xyz, dtype=np.float32)
+    n = len(xyz)
+    nrm = np.asarray(normal, dtype=np.float32)
+    planar = np.asarray(planarity if planarity is not None else np.ones(n), dtype=np.float32)
+    lo, hi = xyz.min(0), xyz.max(0)
+    origin = (lo - pad).astype(np.float32)
+    dims = np.ceil((hi + pad - origin) / cell).astype(np.int64)
+    ijk = np.floor((xyz - origin) / cell).astype(np.int64)
+    key = (ijk[:, 2] * dims[1] + ijk[:, 1]) * dims[0] + ijk[:, 0]
+    order = np.argsort(key, kind="stable")
+    ncell = int(np.prod(dims))
+    start = np.zeros(ncell + 1, np.int32)
+    np.cumsum(np.bincount(key, minlength=ncell), out=start[1:])
+    nrm = nrm[order]
+    nrm = np.ascontiguousarray(nrm / np.maximum(np.linalg.norm(nrm, axis=1, keepdims=True), 1e-6), dtype=np.float32)
+    return {"xyz": np.ascontiguousarray(xyz[order]), "normal": nrm, "planarity": np.ascontiguousarray(planar[order]),
+            "origin": origin, "cell": float(cell), "dims": dims, "start": start}
+
+
+class PriorGrid:
+    """The grid of a prepared prior map with its flooded nearest points (nn) and distance field (df)."""
+
+    def __init__(self, prep: dict, build: bool = True):
+        self.prep = prep
+        self.xyz = np.ascontiguousarray(prep["xyz"], dtype=np.float32)
+        self.nrm = np.ascontiguousarray(prep["normal"], dtype=np.float32)
+        self.planar = np.ascontiguousarray(prep["planarity"], dtype=np.float32)
+        self.start = np.ascontiguousarray(prep["start"], dtype=np.int32)
+        self.dims = np.asarray(prep["dims"], dtype=np.int64)
+        self.ncell = int(np.prod(self.dims))
+        self.nn = np.full(self.ncell, -1, np.int32)
+        self.df = np.full(self.ncell, 255, np.uint8)
+        g = OrGrid()
+        g.xyz, g.nrm, g.planar, g.start, g.nn = _p(self.xyz), _p(self.nrm), _p(self.planar), _p(self.start), _p(self.nn)
+        g.origin = (C.c_float * 3)(*[float(v) for v in prep["origin"]])
+        g.cell = float(prep["cell"])
+        g.inv_cell = float(np.float32(1.0 / prep["cell"]))
+        g.nx, g.ny, g.nz = (int(d) for d in self.dims)
+        self.g = g
+        if build:
+            lib().or_grid_build(C.byref(g), len(self.xyz), _p(self.nn), _p(self.df), threads())
+
+    def nearest(self, w) -> np.ndarray:
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        out = np.empty(len(w), np.int32)
+        lib().or_nearest(C.byref(self.g), _p(w), len(w), _p(out), threads())
+        return out
+
+    def distances(self, pts, T) -> np.ndarray:
+        pts = np.ascontiguousarray(pts, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        out = np.empty(len(pts), np.float32)
+        lib().or_prior_distances(C.byref(self.g), _p(pts), len(pts), _p(T), _p(out), threads())
+        return out
+
+    def icp(self, pts4, lo, hi, T, schedule, alpha=0.05, min_count=30, nthreads=None):
+        """GlobalLocalizer._icp (localize.py:517-553) for every hypothesis' own range of pts4: (T, count, iters)."""
+        pts4 = np.ascontiguousarray(pts4, dtype=np.float32)
+        lo = np.ascontiguousarray(lo, dtype=np.int32)
+        hi = np.ascontiguousarray(hi, dtype=np.int32)
+        T = np.array(T, dtype=np.float64, order="C").reshape(-1, 4, 4)
+        k = len(T)
+        max_d2 = np.array([np.float32(d * d) for d, _ in schedule], np.float32)
+        c2 = np.array([np.float32((d * 0.5) ** 2) for d, _ in schedule], np.float32)
+        iters = np.array([it for _, it in schedule], np.int32)
+        count = np.zeros(k, np.int32)
+        run = np.zeros(1, np.int32)
+        lib().or_loc_icp(C.byref(self.g), _p(pts4), _p(lo), _p(hi), k, _p(T), len(schedule), _p(max_d2), _p(c2),
+                         _p(iters), alpha, min_count, _p(count), _p(run), nthreads or threads())
+        return T, count, int(run[0])
+
+    def evaluate(self, pts4, lo, hi, T, nthreads=None) -> np.ndarray:
+        """k_eval_batch (localize.py:182-205): points within each of EVAL_RADII of the map, per hypothesis."""
+        pts4 = np.ascontiguousarray(pts4, dtype=np.float32)
+        T = np.ascontiguousarray(np.asarray(T, dtype=np.float64).reshape(-1, 16))
+        k = len(T)
+        counts = np.zeros((k, 3), np.int32)
+        radii = np.array(EVAL_RADII, np.float32)
+        lib().or_loc_eval(C.byref(self.g), _p(pts4), _p(np.ascontiguousarray(lo, dtype=np.int32)),
+                          _p(np.ascontiguousarray(hi, dtype=np.int32)), k, _p(T), _p(radii), _p(counts),
+                          nthreads or threads())
+        return counts
+
+
+def thin_5cm(xyz) -> np.ndarray:
+    """One point per 5 cm voxel, the first in scan order (localize.py:579-581)."""
+    pts = np.asarray(xyz, dtype=np.float32)
+    key = np.floor(pts / 0.05).astype(np.int64)
+    _, first = np.unique(key, axis=0, return_index=True)
+    return pts[np.sort(first)]

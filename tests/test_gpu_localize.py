@@ -1,0 +1,220 @@
+"""Prior grid and batched localisation ICP on the GPU against the CPU oracle.
+
+The grid (flooded nearest points and distance field) and every nearest-point query are integer results and
+must match the oracle bit for bit. The batched ICP is compared pose by pose with the oracle's float64
+restatement of GlobalLocalizer._icp (localize.py:517-553): within 1 mm / 0.01 deg, the same iteration count
+within one (the stop test moved < 2e-4 can fall either side of an iteration by float rounding), and the
+evaluation counts within 0.5 % of the scan.
+"""
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+POSE_TOL_M, POSE_TOL_DEG = 1e-3, 0.01
+
+
+def _pose_err(A, B):
+    d = np.linalg.inv(A) @ B
+    ang = math.degrees(math.acos(np.clip((np.trace(d[:3, :3]) - 1) / 2, -1, 1)))
+    return float(np.linalg.norm(A[:3, 3] - B[:3, 3])), ang
+
+
+@pytest.fixture(scope="module")
+def room():
+    from livox_warp import synth
+    from livox_warp.mapgrid import PriorGrid
+
+    sc = synth.box_room(3)
+    xyz, nrm = synth.sample_surfaces(sc, 0.02, 0, jitter=0.002)
+    planar = np.ones(len(xyz), np.float32)
+    planar[::7] = 0.3  # some clutter points: the point-to-point branch
+    host = PriorGrid.prepare({"xyz": xyz, "normal": nrm, "planarity": planar})
+    grid = PriorGrid(host)
+    grid.build()
+    og = oracle.PriorGrid(oracle.prior_prepare(xyz, nrm, planar))
+    return sc, grid, og
+
+
+def test_prepare_matches_oracle(room):
+    _, grid, og = room
+    h = grid._host
+    assert np.array_equal(h["xyz"], og.xyz) and np.array_equal(h["start"], og.start)
+    assert np.array_equal(h["normal"], og.nrm) and np.array_equal(h["planarity"], og.planar)
+    assert np.array_equal(h["origin"], og.prep["origin"]) and np.array_equal(h["dims"], og.dims)
+
+
+def test_grid_build_bit_exact(room):
+    _, grid, og = room
+    assert np.array_equal(grid.nn.cpu().numpy(), og.nn)
+    assert np.array_equal(grid.df.cpu().numpy(), og.df)
+    assert (og.nn >= 0).mean() > 0.3 and (og.df < 255).any()
+
+
+def test_distances_bit_exact(room):
+    sc, grid, og = room
+    rng = np.random.default_rng(4)
+    # queries near surfaces, in the flooded band and far outside the grid
+    q = og.xyz[rng.choice(len(og.xyz), 20000)] + rng.normal(0, 0.08, (20000, 3)).astype(np.float32)
+    q = np.concatenate([q, rng.uniform(-5, 15, (5000, 3)).astype(np.float32)]).astype(np.float32)
+    T = np.eye(4)
+    T[:3, :3] = np.array([[0.0, -1.0, 0.0], [1.0, 0.0, 0.0], [0.0, 0.0, 1.0]])
+    T[:3, 3] = [7.0, -1.0, 0.0]
+    Ti = np.linalg.inv(T)
+    pts = (q.astype(np.float64) @ Ti[:3, :3].T + Ti[:3, 3]).astype(np.float32)
+    dev = torch.from_numpy(pts).cuda()
+    out = torch.empty(len(pts), dtype=torch.float32, device="cuda")
+    grid.distances(dev, len(pts), T, out)
+    got = out.cpu().numpy()
+    want = og.distances(pts, T)
+    assert np.array_equal(got, want)
+    assert (want >= 1e3).any() and (want < 0.05).mean() > 0.3
+
+
+def _hypotheses(sc, n, seed, trans=0.15, yaw=4.0, sizes=(2000, 20000)):
+    from livox_warp import synth
+
+    T_true = synth.free_poses(sc, n, seed, z=1.2, margin=0.5)
+    T0 = synth.perturb(T_true, seed + 1, trans, yaw, tilt_deg=1.0)
+    rng = np.random.default_rng(seed + 2)
+    scans = [synth.spin_scan(sc, T_true[h], int(rng.integers(sizes[0], sizes[1] + 1)), seed + 10 + h)
+             for h in range(n)]
+    return T_true, T0, scans
+
+
+def _oracle_batch(og, scans, T0, schedule):
+    pts4 = np.zeros((sum(len(s) for s in scans), 4), np.float32)
+    hi = np.cumsum([len(s) for s in scans])
+    lo = hi - [len(s) for s in scans]
+    for s, a in zip(scans, lo):
+        pts4[a:a + len(s), :3] = s
+    T, count, iters = og.icp(pts4, lo, hi, T0, schedule)
+    ev = og.evaluate(pts4, lo, hi, T)
+    return T, count, iters, ev
+
+
+@pytest.mark.parametrize("tile", [128, 256, 512])
+def test_batch_uneven_scans_match_oracle(room, tile):
+    from livox_warp.localize import SCHEDULE_ICP, GlobalLocalizer
+
+    sc, grid, og = room
+    T_true, T0, scans = _hypotheses(sc, 12, 40)
+    loc = GlobalLocalizer(grid, hyp_cap=64, pts_cap=1 << 19)
+    res = loc.register_batch(scans, T0, SCHEDULE_ICP, tile=tile)
+    oT, ocount, oiters, oev = _oracle_batch(og, scans, T0, SCHEDULE_ICP)
+    assert abs(res.iters - oiters) <= 1
+    for h in range(len(scans)):
+        dt, da = _pose_err(res.T[h], oT[h])
+        assert dt < POSE_TOL_M and da < POSE_TOL_DEG, (h, dt, da)
+        n = len(scans[h])
+        assert abs(int(res.count[h]) - int(ocount[h])) <= max(2, n // 200), h
+        ev = np.rint(res.fit[h] * n).astype(np.int64)
+        assert np.all(np.abs(ev - oev[h]) <= max(2, n // 200)), (h, ev, oev[h])
+    # the registration itself: the noise-free poses are found
+    ok = [(_pose_err(res.T[h], T_true[h])[0] < 0.05) for h in range(len(scans))]
+    assert np.mean(ok) >= 0.75
+
+
+def test_shared_scan_refine_and_starts(room):
+    """refine (localize.py:569-612): one shared thinned scan, T0 plus offset starts in the same batch."""
+    from livox_warp import synth
+    from livox_warp.localize import SCHEDULE_REFINE, GlobalLocalizer, thin_5cm
+
+    sc, grid, og = room
+    T_true = synth.free_poses(sc, 1, 77, z=1.3, margin=0.6)[0]
+    xyz = synth.spin_scan(sc, T_true, 60000, 78)
+    T0 = synth.perturb(T_true[None], 79, 0.08, 2.0)[0]
+    loc = GlobalLocalizer(grid, hyp_cap=64, pts_cap=1 << 19)
+    starts = [(0.3, 0.0, 0.0), (0.0, -0.3, 0.0, 5.0)]
+    T, fit, info = loc.refine(xyz, T0, starts=starts)
+    pts = oracle.thin_5cm(xyz)
+    assert info["n"] == len(pts)
+    assert np.array_equal(thin_5cm(xyz), pts)
+    # the oracle refines the same three starts
+    c_map = T0[:3, :3] @ pts.mean(axis=0).astype(np.float64) + T0[:3, 3]
+    inits = [T0]
+    for off in starts:
+        Ti = T0.copy()
+        off = np.asarray(off, dtype=np.float64)
+        if len(off) > 3 and off[3] != 0.0:
+            c, s = math.cos(math.radians(off[3])), math.sin(math.radians(off[3]))
+            Rz = np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]])
+            Ti[:3, :3] = Rz @ Ti[:3, :3]
+            Ti[:3, 3] = Rz @ (Ti[:3, 3] - c_map) + c_map
+        Ti[:3, 3] += off[:3]
+        inits.append(Ti)
+    oT, _, _, oev = _oracle_batch(og, [pts] * len(inits), np.stack(inits), SCHEDULE_REFINE)
+    ofit = oev / len(pts)
+    best = 0
+    for i in range(1, len(inits)):
+        if ofit[i, 0] > ofit[best, 0] + (0.05 if best == 0 else 0.0):
+            best = i
+    assert info["switched"] == (best != 0)
+    dt, da = _pose_err(T, oT[best])
+    assert dt < POSE_TOL_M and da < POSE_TOL_DEG
+    assert np.all(np.abs(fit - ofit[best]) <= 0.005)
+    assert _pose_err(T, T_true)[0] < 0.03
+    start_fit = og.evaluate(np.concatenate([pts, np.zeros((len(pts), 1), np.float32)], 1), [0], [len(pts)], T0[None])
+    assert abs(info["fit_start"] - start_fit[0, 0] / len(pts)) < 1e-9
+
+
+def test_graph_replay_equals_direct_launch(room):
+    """A captured launch reading its counts on the device gives the direct launch's results bit for bit, for
+    batches of different shapes replayed through the same graph."""
+    from livox_warp.localize import SCHEDULE_ICP, GlobalLocalizer
+
+    sc, grid, og = room
+    loc = GlobalLocalizer(grid, hyp_cap=64, pts_cap=1 << 19)
+    for seed, n in ((50, 10), (60, 6)):
+        T_true, T0, scans = _hypotheses(sc, n, seed)
+        direct = loc.register_batch(scans, T0, SCHEDULE_ICP, tile=256)
+        lo, hi = loc._upload_pts(scans, torch.cuda.current_stream())
+        replay = loc.register_graph(lo, hi, SCHEDULE_ICP, tile=256)
+        got = replay(lo, hi, T0)
+        assert np.array_equal(got.T, direct.T)
+        assert np.array_equal(got.count, direct.count) and np.array_equal(got.fit, direct.fit)
+        assert got.iters == direct.iters
+
+
+def test_degenerate_hypotheses_keep_pose(room):
+    """A hypothesis with no points, or with fewer than 30 matches, keeps its pose; the others still converge."""
+    from livox_warp.localize import SCHEDULE_ICP, GlobalLocalizer
+
+    sc, grid, og = room
+    T_true, T0, scans = _hypotheses(sc, 4, 90)
+    far = np.eye(4)
+    far[:3, 3] = [500.0, 500.0, 500.0]
+    scans = scans + [np.zeros((0, 3), np.float32), scans[0][:20]]
+    T0 = np.concatenate([T0, far[None], T0[:1]])
+    loc = GlobalLocalizer(grid, hyp_cap=64, pts_cap=1 << 19)
+    res = loc.register_batch(scans, T0, SCHEDULE_ICP, tile=128)
+    assert np.array_equal(res.T[4], far) and np.array_equal(res.T[5], T0[5])
+    assert res.count[4] == 0 and res.count[5] <= 20
+    oT, _, _, _ = _oracle_batch(og, scans, T0, SCHEDULE_ICP)
+    for h in range(4):
+        dt, da = _pose_err(res.T[h], oT[h])
+        assert dt < POSE_TOL_M and da < POSE_TOL_DEG
+
+
+def test_argument_errors(room):
+    import ctypes as C
+
+    from livox_warp import _lib
+    from livox_warp.localize import GlobalLocalizer
+
+    sc, grid, og = room
+    loc = GlobalLocalizer(grid, hyp_cap=8, pts_cap=1 << 17)
+    with pytest.raises(_lib.LwError):
+        loc._launch(1, 1, 384, ((0.1, 2),), torch.cuda.current_stream())  # tile must be 128/256/512
+    with pytest.raises(_lib.LwError):
+        loc._launch(1, 1, 256, ((0.1, 200), (0.1, 200)), torch.cuda.current_stream())  # > moved_cap iterations
+    with pytest.raises(ValueError):
+        loc.register_batch([np.zeros((10, 3), np.float32)] * 9, np.tile(np.eye(4), (9, 1, 1)))
+    with pytest.raises(RuntimeError):
+        loc.refine(np.zeros((50, 3), np.float32), np.eye(4))
