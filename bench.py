@@ -18,6 +18,12 @@ the 0.1 m integration map (2^22 slots) and free-space carving of every ray.
 
 `--impl reference` times the reference's CPU implementation of the path instead: NVIDIA Warp (the reference's
 only runtime) is not installed, so that arm runs the CPU restatement, on every host core.
+`--workload localize` measures the batched global localisation instead: a 20.3M-point prior map sampled every
+15 mm on the surfaces of a seeded 40 x 30 x 3 m office (walls with doors, 200 boxes), 256 hypotheses, each with
+its own static 360-degree scan of U[2k, 20k] points taken at a free pose (z = 1.2 m, yaw uniform), started from
+that pose snapped to a 0.5 m xy grid and a 5 deg heading grid; one step = one batched registration of all 256
+(the schedule (0.40, 8), (0.20, 8), (0.10, 8), (0.05, 10)) plus the evaluation, in one graph-replayed launch.
+
 Multi-GPU: the path does not shard (each frame registers against the map of the frames before it), so
 `--gpus N` runs N independent replicas, one per GPU, and `value` sums their frames.
 """
@@ -52,6 +58,12 @@ ROOM_SEED = 1   # the box room
 PATH_SEED = 31  # the handheld path (a sequence the float64 oracle tracks for the whole 60 s)
 SCAN_SEED = 3
 L2_FLUSH_BYTES = 256 << 20
+LOC_SEED = 1          # the office
+LOC_SPACING = 0.015   # prior-map sample spacing: 20.3M points on the office's surfaces
+LOC_HYP = 256
+LOC_PTS = (2000, 20000)
+LOC_Z = 1.2
+LOC_POSE_SEED = 11
 
 
 # ---- workload --------------------------------------------------------------------------------------------------
@@ -343,6 +355,225 @@ def _oracle_view(oracle):
     return v
 
 
+# ---- batched global localisation -----------------------------------------------------------------------------------
+
+
+def _loc_scans(args):
+    from livox_warp import synth
+
+    T, sizes, seeds = args
+    scene = synth.office(LOC_SEED)
+    return [synth.spin_scan(scene, T[i], int(sizes[i]), int(seeds[i])) for i in range(len(T))]
+
+
+def loc_workload(procs: int | None = None):
+    """Prior map, packed scans (N, 4), per-hypothesis row ranges, true and initial poses (before any CUDA call)."""
+    from livox_warp import synth
+
+    scene = synth.office(LOC_SEED)
+    xyz, nrm = synth.sample_surfaces(scene, LOC_SPACING, LOC_SEED, jitter=0.002)
+    T_true = synth.free_poses(scene, LOC_HYP, LOC_POSE_SEED, z=LOC_Z, margin=0.6)
+    rng = np.random.default_rng(LOC_POSE_SEED + 1)
+    sizes = rng.integers(LOC_PTS[0], LOC_PTS[1] + 1, LOC_HYP)
+    seeds = 1000 + np.arange(LOC_HYP)
+    procs = procs or min(8, os.cpu_count() or 1)
+    parts = np.array_split(np.arange(LOC_HYP), procs * 2)
+    jobs = [(T_true[p], sizes[p], seeds[p]) for p in parts if len(p)]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        scans = [s for chunk in pool.map(_loc_scans, jobs) for s in chunk]
+    n = np.array([len(x) for x in scans], dtype=np.int64)
+    hi = np.cumsum(n)
+    lo = hi - n
+    pts4 = np.zeros((int(hi[-1]), 4), np.float32)
+    for x, a in zip(scans, lo):
+        pts4[a:a + len(x), :3] = x
+    # the hypotheses: the true pose snapped to a 0.5 m xy grid and a 5 deg heading grid (a coarse search's cells)
+    T0 = T_true.copy()
+    yaw = np.arctan2(T_true[:, 1, 0], T_true[:, 0, 0])
+    yq = np.round(np.degrees(yaw) / 5.0) * np.radians(5.0)
+    for h in range(LOC_HYP):
+        c, s_ = math.cos(yq[h]), math.sin(yq[h])
+        T0[h, :3, :3] = np.array([[c, -s_, 0.0], [s_, c, 0.0], [0.0, 0.0, 1.0]])
+        T0[h, :2, 3] = np.round(T_true[h, :2, 3] / 0.5) * 0.5
+    return {"xyz": xyz, "nrm": nrm, "pts4": pts4, "lo": lo, "hi": hi, "T_true": T_true, "T0": T0}
+
+
+def _loc_success(T, T_true):
+    from livox_warp.localize import pose_difference
+
+    err = np.array([pose_difference(T_true[h], T[h]) for h in range(len(T))])
+    ok = (err[:, 0] < 0.1) & (err[:, 1] < 1.0)
+    return float(ok.mean()), err
+
+
+def loc_oracle(og, w, idx, threads):
+    """The oracle's batched ICP + evaluation of hypotheses idx: (T, count, iters, eval, seconds)."""
+    from livox_warp.localize import SCHEDULE_ICP
+
+    os.environ["LW_ORACLE_THREADS"] = str(threads)
+    n = w["hi"][idx] - w["lo"][idx]
+    hi = np.cumsum(n)
+    lo = hi - n
+    pts4 = np.concatenate([w["pts4"][w["lo"][h]:w["hi"][h]] for h in idx])
+    t0 = time.perf_counter()
+    T, count, iters = og.icp(pts4, lo, hi, w["T0"][idx], SCHEDULE_ICP, nthreads=threads)
+    ev = og.evaluate(pts4, lo, hi, T, nthreads=threads)
+    return T, count, iters, ev, time.perf_counter() - t0
+
+
+def run_localize(a, rank: int, world: int, local: int):
+    from oracle import oracle as _o
+
+    w = loc_workload()
+    metric = "batched global localisation hypotheses/s (point-to-plane ICP schedule + evaluation)"
+    config = {"workload": f"global localisation: office 40x30x3 m (walls, doors, 200 boxes), prior map "
+                          f"{len(w['xyz']):,} pts at {LOC_SPACING * 1e3:.0f} mm with normals, {LOC_HYP} hypotheses "
+                          f"(xy on a 0.5 m grid, yaw on 5 deg, z {LOC_Z} m) each with its own 360-degree scan of "
+                          f"U[{LOC_PTS[0]}, {LOC_PTS[1]}] pts",
+              "map_points": int(len(w["xyz"])), "hypotheses": LOC_HYP, "scan_points_total": int(len(w["pts4"])),
+              "schedule": "(0.40,8),(0.20,8),(0.10,8),(0.05,10)", "l2": "flushed between steps (256 MB write)",
+              "parallelism": f"replicas x{a.gpus}"}
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        threads = _o.host_cores()
+        og = _o.PriorGrid(_o.prior_prepare(w["xyz"], w["nrm"]))
+        k = min(LOC_HYP, max(threads, 8))
+        T, count, iters, ev, secs = loc_oracle(og, w, np.arange(k), threads)
+        v = k / secs
+        line = {"impl": "reference", "metric": metric, "value": round(v, 3), "unit": "hypotheses/s",
+                "n_gpus": a.gpus, "steps": 1, "warmup": 0, "ms_per_step": round(1e3 * secs, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
+                "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": round(v, 3), "unit": "hypotheses/s", "cores": threads, "kind": "port",
+                                 "sample": f"the first {k} hypotheses as one batch through the CPU restatement "
+                                           "(NVIDIA Warp is not installed)"},
+                "e2e": {"value": round(v, 3), "unit": "hypotheses/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+    import torch
+
+    from livox_warp import _lib
+    from livox_warp import roofline as rl
+    from livox_warp.localize import SCHEDULE_ICP, GlobalLocalizer
+    from livox_warp.mapgrid import PriorGrid
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    t0 = time.perf_counter()
+    grid = PriorGrid({"xyz": w["xyz"], "normal": w["nrm"]}, device)
+    prep_s = time.perf_counter() - t0
+    grid.build()
+    n_all = len(w["pts4"])
+    loc = GlobalLocalizer(grid, device, hyp_cap=LOC_HYP, pts_cap=n_all)
+    stream = torch.cuda.current_stream(device)
+    pinned = torch.from_numpy(w["pts4"]).pin_memory()
+    # autotune (tile per CTA) through the public call, then capture the launch in a graph
+    res = loc.register_packed(pinned, w["lo"], w["hi"], w["T0"])
+    tile = res.tile
+    replay = loc.register_graph(w["lo"], w["hi"], SCHEDULE_ICP, tile)
+    b = loc.batch
+    T0_dev = torch.from_numpy(w["T0"].reshape(LOC_HYP, 16).copy()).to(device)
+    b.pts[:n_all].copy_(pinned.to(device))
+    b.stage(w["lo"], w["hi"], tile, stream)
+    g = loc._graphs[(tuple(SCHEDULE_ICP), tile)]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+
+    def dev_step():
+        b.T[:LOC_HYP].copy_(T0_dev)
+        g.replay()
+
+    for _ in range(a.warmup):
+        dev_step()
+    torch.cuda.synchronize(device)
+    clocks = Clocks(local)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    clocks.start()
+    torch.cuda.synchronize(device)
+    for j in range(a.steps):
+        flush.fill_(float(j))
+        evs[j][0].record(stream)
+        dev_step()
+        evs[j][1].record(stream)
+    torch.cuda.synchronize(device)
+    clk = clocks.stop()
+    step_ms = np.array([x.elapsed_time(y) for x, y in evs])
+    T_dev = b.T[:LOC_HYP].cpu().numpy().reshape(LOC_HYP, 4, 4)
+    iters = int(b.outs[b.o_it].item())
+    ms_total = float(step_ms.sum())
+    value = world * a.steps * LOC_HYP / (ms_total * 1e-3)
+    # e2e: from pinned host scans through register_packed (H2D of scans, tiles and poses; D2H of poses and fits)
+    for _ in range(3):
+        loc.register_packed(pinned, w["lo"], w["hi"], w["T0"], tile=tile)
+    torch.cuda.synchronize(device)
+    e_steps = max(3, min(a.steps, 20))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e_steps):
+        r = loc.register_packed(pinned, w["lo"], w["hi"], w["T0"], tile=tile)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    e_ms = e0.elapsed_time(e1)
+    nt = int(b.h_ints[1])
+    h2d = n_all * 16 + LOC_HYP * 128 + 4 * (2 + LOC_HYP + LOC_HYP + 1 + 2 * nt)
+    d2h = LOC_HYP * 128 + 4 * (4 * LOC_HYP + 2)
+    # the timed region replays the captured graph (k_loc_reset + k_loc_icp) once per step; graph replays do not
+    # pass through the library's host-side launch counter
+    launches = 2 * a.steps
+    if rank != 0:
+        return
+    success, err = _loc_success(r.T, w["T_true"])
+    assert np.array_equal(r.T, T_dev), "graph replay and the public call disagree"
+    # roofline of k_loc_icp: algorithmic bytes / the measured step time (the step is that one launch)
+    peak = measured_peak()
+    lb = rl.loc_bytes(grid._host["start"], grid.origin, grid.dims, grid.cell, w["pts4"], w["lo"], w["hi"], T_dev,
+                      iters, nt)
+    avg_ms = ms_total / a.steps
+    ach = lb["bytes"] / (avg_ms * 1e-3) / 1e9
+    roof = {"kernel": "k_loc_icp", "bound": "hbm", "achieved": round(ach, 3), "peak": peak["hbm_gbs"],
+            "unit": "GB/s", "frac": round(ach / peak["hbm_gbs"], 5), "traffic": None,
+            "peak_source": peak["source"], "avg_launch_us": round(avg_ms * 1e3, 2), "iterations": iters,
+            "algorithmic_bytes_per_launch": int(lb["bytes"]), "distinct_cells": lb["cells"],
+            "distinct_map_points": lb["visited_points"], "tile": tile}
+    # parity and the CPU baseline: the first 16 hypotheses as one batch, GPU and oracle
+    threads = _o.host_cores()
+    # the oracle's grid over the same prepared arrays; its flooded seeds are the device's, which the parity
+    # tests hold bit-exact to the oracle's own flood (flooding 43M cells on the host would take a minute)
+    og = _o.PriorGrid(grid._host, build=False)
+    og.nn[:] = grid.nn.cpu().numpy()
+    idx = np.arange(16)
+    oT, ocount, oiters, oev, secs = loc_oracle(og, w, idx, threads)
+    n16 = w["hi"][idx] - w["lo"][idx]
+    hi16 = np.cumsum(n16)
+    lo16 = hi16 - n16
+    p16 = torch.from_numpy(np.concatenate([w["pts4"][w["lo"][h]:w["hi"][h]] for h in idx])).pin_memory()
+    g16 = loc.register_packed(p16, lo16, hi16, w["T0"][idx], tile=tile)
+    from livox_warp.localize import pose_difference
+
+    pd = np.array([pose_difference(oT[h], g16.T[h]) for h in range(16)])
+    line = {"metric": metric, "value": round(value, 3), "unit": "hypotheses/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(avg_ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 tile sums, solve and poses)",
+            "data": "synthetic", "config": config,
+            "success_rate": round(success, 4), "pose_err_median_m": round(float(np.median(err[:, 0])), 4),
+            "pose_err_median_deg": round(float(np.median(err[:, 1])), 4),
+            "step_ms_p50_p99": [round(float(np.percentile(step_ms, 50)), 4),
+                                round(float(np.percentile(step_ms, 99)), 4)],
+            "roofline": roof,
+            "cpu_baseline": {"value": round(16 / secs, 3), "unit": "hypotheses/s", "cores": threads, "kind": "port",
+                             "sample": f"the first 16 hypotheses as one batch through the CPU oracle "
+                                       f"(C++/OpenMP, float64 terms), {secs:.1f} s"},
+            "vs_fp64_oracle": {"hypotheses": 16, "max_m": round(float(pd[:, 0].max()), 7),
+                               "max_deg": round(float(pd[:, 1].max()), 6), "iters_gpu": g16.iters,
+                               "iters_oracle": oiters},
+            "e2e": {"value": round(world * e_steps * LOC_HYP / (e_ms * 1e-3), 3), "unit": "hypotheses/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches), "graph": True, "clocks": clk, "prepare_s": round(prep_s, 2),
+            "grid_build_s": round(grid.build_s, 3)}
+    print(json.dumps(line))
+
+
 # ---- main -------------------------------------------------------------------------------------------------------
 
 
@@ -354,6 +585,7 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", choices=("sequence", "localize"), default="sequence")
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -361,6 +593,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.workload == "localize":
+        run_localize(a, rank, world, local)
+        return
     n_frames = a.warmup + a.steps + 1
     metric = "ICP sequence odometry frames/s (deskew + GN ICP + keyframe insert + map insert + carve)"
     config = {"workload": "sequence odometry: box room 8x6x3 m, 20 boxes, rosette 100k pts/s (~10k pts/frame), "

@@ -336,11 +336,11 @@ int lw_cluster(const float* xyz, int32_t xyz_stride, const int32_t* gnd, int32_t
 /* ---- prior-map grid and batched localisation ICP (mapgrid.py, localize.py) -------------------------- */
 
 /* A dense grid over a prior map (mapgrid.py:1-33, 207-296): the n map points sorted by cell (start[c] ..
- * start[c+1] are cell c's points), a jump-flooded nearest point per cell and a byte distance field in cm. */
+ * start[c+1] are cell c's points), a jump-flooded nearest point per cell and a byte distance field in cm. A map
+ * point is one 16-byte record (x, y, z, planarity), so the nearest-point scans gather one aligned vector each. */
 typedef struct lw_prior_grid {
-    float* xyz;       /* [n*3] map points, sorted by cell */
+    float* xyz;       /* [n*4] map points sorted by cell: x, y, z, planarity (16-byte aligned) */
     float* nrm;       /* [n*3] unit normals */
-    float* planar;    /* [n] planarity */
     int32_t* start;   /* [ncell+1] */
     int32_t* nn;      /* [ncell] flooded nearest point or -1 */
     uint8_t* df;      /* [ncell] distance to it in cm, 255 beyond the band */

@@ -39,40 +39,80 @@ __device__ __forceinline__ void cell_centre(const lw_prior_grid& g, int64_t c, f
     z = g.origin[2] + ((float)iz + 0.5f) * g.cell;
 }
 
-__device__ __forceinline__ float3 ld_pt(const float* __restrict__ xyz, int64_t i) {
-    return make_float3(__ldg(xyz + 3 * i), __ldg(xyz + 3 * i + 1), __ldg(xyz + 3 * i + 2));
-}
+__device__ __forceinline__ float4 ld_pt(const float4* __restrict__ xyzp, int64_t i) { return __ldg(xyzp + i); }
 
-// The map point nearest to w: exact within one cell (every such point lies in the 27 cells around w), otherwise
-// the closest of those cells' flooded seeds, or -1 beyond the band (mapgrid.py:68-102).
+constexpr float BOX_SLACK = 1.0e-4f;  // m: covers the float rounding of cell assignment and of the box offsets
+
+// The map point nearest to w (mapgrid.py:68-102): exact within one cell -- the first point, in the reference's
+// scan order (dz, dy, dx, then index), at the smallest distance below one cell -- otherwise the closest of the
+// 27 cells' flooded seeds, or -1 beyond the band.
+//
+// Same result, fewer reads: the own cell is scanned first, and its smallest distance ub bounds the answer; a
+// neighbour cell whose box lies farther than ub from w (less BOX_SLACK) holds no point that could be the first
+// minimum, so its points are skipped. The seeds are still compared for every cell while nothing within one cell
+// has been found, as the reference does. The own cell's contribution in the scan order is its own first minimum.
 __device__ int nearest_point(const lw_prior_grid& g, float wx, float wy, float wz) {
+    const float4* __restrict__ P = reinterpret_cast<const float4*>(g.xyz);
     int ix, iy, iz;
     grid_idx(g, wx, wy, wz, ix, iy, iz);
+    const float cell2 = g.cell * g.cell;
+    // w's offsets from its own cell's lower faces
+    const float fx = (wx - g.origin[0]) - (float)ix * g.cell;
+    const float fy = (wy - g.origin[1]) - (float)iy * g.cell;
+    const float fz = (wz - g.origin[2]) - (float)iz * g.cell;
+    int own = -1;
+    float own_d2 = cell2;
+    const int64_t c0 = grid_flat(g, ix, iy, iz);
+    if (c0 >= 0) {
+        const int k0 = __ldg(g.start + c0), k1 = __ldg(g.start + c0 + 1);
+        for (int k = k0; k < k1; ++k) {
+            const float4 q = ld_pt(P, k);
+            const float ex = wx - q.x, ey = wy - q.y, ez = wz - q.z;
+            const float d2 = ex * ex + ey * ey + ez * ez;
+            if (d2 < own_d2) {
+                own_d2 = d2;
+                own = k;
+            }
+        }
+    }
+    const float ub = own_d2 * 1.00001f;
     int best = -1;
-    float bd = g.cell * g.cell;
+    float bd = cell2;
     int seed = -1;
     float sd = 1.0e30f;
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
+    for (int dz = -1; dz <= 1; ++dz) {
+        const float lz = fmaxf((dz < 0 ? fz : (dz > 0 ? g.cell - fz : 0.0f)) - BOX_SLACK, 0.0f);
+        for (int dy = -1; dy <= 1; ++dy) {
+            const float ly = fmaxf((dy < 0 ? fy : (dy > 0 ? g.cell - fy : 0.0f)) - BOX_SLACK, 0.0f);
             for (int dx = -1; dx <= 1; ++dx) {
-                int64_t c = grid_flat(g, ix + dx, iy + dy, iz + dz);
+                const int64_t c = grid_flat(g, ix + dx, iy + dy, iz + dz);
                 if (c < 0) continue;
-                int k0 = __ldg(g.start + c), k1 = __ldg(g.start + c + 1);
-                for (int k = k0; k < k1; ++k) {
-                    float3 q = ld_pt(g.xyz, k);
-                    float ex = wx - q.x, ey = wy - q.y, ez = wz - q.z;
-                    float d2 = ex * ex + ey * ey + ez * ez;
-                    if (d2 < bd) {
-                        bd = d2;
-                        best = k;
+                if (dx == 0 && dy == 0 && dz == 0) {
+                    if (own >= 0 && own_d2 < bd) {
+                        bd = own_d2;
+                        best = own;
+                    }
+                } else {
+                    const float lx = fmaxf((dx < 0 ? fx : (dx > 0 ? g.cell - fx : 0.0f)) - BOX_SLACK, 0.0f);
+                    if (lx * lx + ly * ly + lz * lz <= ub) {
+                        const int k0 = __ldg(g.start + c), k1 = __ldg(g.start + c + 1);
+                        for (int k = k0; k < k1; ++k) {
+                            const float4 q = ld_pt(P, k);
+                            const float ex = wx - q.x, ey = wy - q.y, ez = wz - q.z;
+                            const float d2 = ex * ex + ey * ey + ez * ez;
+                            if (d2 < bd) {
+                                bd = d2;
+                                best = k;
+                            }
+                        }
                     }
                 }
                 if (best < 0) {
-                    int s = __ldg(g.nn + c);
+                    const int s = __ldg(g.nn + c);
                     if (s >= 0) {
-                        float3 q = ld_pt(g.xyz, s);
-                        float ex = wx - q.x, ey = wy - q.y, ez = wz - q.z;
-                        float d2 = ex * ex + ey * ey + ez * ez;
+                        const float4 q = ld_pt(P, s);
+                        const float ex = wx - q.x, ey = wy - q.y, ez = wz - q.z;
+                        const float d2 = ex * ex + ey * ey + ez * ez;
                         if (d2 < sd) {
                             sd = d2;
                             seed = s;
@@ -80,6 +120,8 @@ __device__ int nearest_point(const lw_prior_grid& g, float wx, float wy, float w
                     }
                 }
             }
+        }
+    }
     return best >= 0 ? best : seed;
 }
 
@@ -91,7 +133,7 @@ __global__ void k_seed_clear(lw_prior_grid g) {
 
 __global__ void k_seed(lw_prior_grid g) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += (int64_t)gridDim.x * blockDim.x) {
-        float3 p = ld_pt(g.xyz, i);
+        const float4 p = ld_pt(reinterpret_cast<const float4*>(g.xyz), i);
         int ix, iy, iz;
         grid_idx(g, p.x, p.y, p.z, ix, iy, iz);
         int64_t c = grid_flat(g, ix, iy, iz);
@@ -120,7 +162,7 @@ __global__ void k_jfa(lw_prior_grid g, const int32_t* __restrict__ in, int32_t* 
         int best = in[c];
         float bd = 1.0e30f;
         if (best >= 0) {
-            float3 q = ld_pt(g.xyz, best);
+            const float4 q = ld_pt(reinterpret_cast<const float4*>(g.xyz), best);
             float ex = px - q.x, ey = py - q.y, ez = pz - q.z;
             bd = ex * ex + ey * ey + ez * ez;
         }
@@ -131,7 +173,7 @@ __global__ void k_jfa(lw_prior_grid g, const int32_t* __restrict__ in, int32_t* 
                     if (j < 0 || j == c) continue;
                     int s = in[j];
                     if (s < 0 || s == best) continue;
-                    float3 q = ld_pt(g.xyz, s);
+                    const float4 q = ld_pt(reinterpret_cast<const float4*>(g.xyz), s);
                     float ex = px - q.x, ey = py - q.y, ez = pz - q.z;
                     float d2 = ex * ex + ey * ey + ez * ez;
                     if (d2 < bd) {
@@ -152,7 +194,7 @@ __global__ void k_df(lw_prior_grid g) {
         }
         float px, py, pz;
         cell_centre(g, c, px, py, pz);
-        float3 q = ld_pt(g.xyz, s);
+        const float4 q = ld_pt(reinterpret_cast<const float4*>(g.xyz), s);
         float d = len3(px - q.x, py - q.y, pz - q.z) * 100.0f;
         int v = (int)(d + 0.5f);
         g.df[c] = (uint8_t)(v < 255 ? v : 255);
@@ -172,7 +214,7 @@ __global__ void k_distances(lw_prior_grid g, const float* __restrict__ pts, int6
         int s = nearest_point(g, wx, wy, wz);
         float d = 1.0e3f;
         if (s >= 0) {
-            float3 q = ld_pt(g.xyz, s);
+            const float4 q = ld_pt(reinterpret_cast<const float4*>(g.xyz), s);
             d = len3(wx - q.x, wy - q.y, wz - q.z);
         }
         out[i] = d;
@@ -220,12 +262,13 @@ __device__ __forceinline__ void loc_terms(const lw_prior_grid& g, const LocPose&
     float wx = lx + P.c[0], wy = ly + P.c[1], wz = lz + P.c[2];
     int s = nearest_point(g, wx, wy, wz);
     if (s < 0) return;
-    float3 q = ld_pt(g.xyz, s);
+    const float4 q = ld_pt(reinterpret_cast<const float4*>(g.xyz), s);
     float r0 = wx - q.x, r1 = wy - q.y, r2 = wz - q.z;
     if (r0 * r0 + r1 * r1 + r2 * r2 > max_d2) return;
-    float3 nv = ld_pt(g.nrm, s);
+    const float3 nv = make_float3(__ldg(g.nrm + 3 * (int64_t)s), __ldg(g.nrm + 3 * (int64_t)s + 1),
+                                  __ldg(g.nrm + 3 * (int64_t)s + 2));
     float M[6];
-    if (__ldg(g.planar + s) > PLANAR && len3(nv.x, nv.y, nv.z) > 0.5f) {
+    if (q.w > PLANAR && len3(nv.x, nv.y, nv.z) > 0.5f) {
         // the normal at full weight, along the surface only a little
         float b = 1.0f - alpha;
         M[0] = nv.x * nv.x * b + alpha;
@@ -437,7 +480,7 @@ __global__ void __launch_bounds__(512, 1)
             xform(M, p.x, p.y, p.z, wx, wy, wz);
             int s = nearest_point(g, wx, wy, wz);
             if (s >= 0) {
-                float3 q = ld_pt(g.xyz, s);
+                const float4 q = ld_pt(reinterpret_cast<const float4*>(g.xyz), s);
                 float d = len3(wx - q.x, wy - q.y, wz - q.z);
                 c0 = d < la.radii[0];
                 c1 = d < la.radii[1];
@@ -473,6 +516,7 @@ static int check_grid(const lw_prior_grid* g, const char* who) {
     if (!g || !g->xyz || !g->start || !g->nn || g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || g->cell <= 0.0f)
         return set_error(LW_EINVAL, "%s: incomplete prior grid", who);
     if ((int64_t)g->nx * g->ny * g->nz != g->ncell) return set_error(LW_EINVAL, "%s: ncell != nx*ny*nz", who);
+    if (((uintptr_t)g->xyz & 15) != 0) return set_error(LW_EINVAL, "%s: xyz must be 16-byte aligned", who);
     if (g->n >= 0x7FFFFFFF) return set_error(LW_ECAPACITY, "%s: %lld map points exceed int32 indices", who, (long long)g->n);
     return LW_OK;
 }
@@ -531,7 +575,7 @@ int lw_loc_icp_batch(const lw_prior_grid* g, lw_loc_batch* b, int32_t n_hyp, int
         !b->moved || !b->count || !b->eval || !b->bar || !b->err || !b->iters_run || b->pts_cap < 0)
         return set_error(LW_EINVAL, "lw_loc_icp_batch: incomplete batch buffers");
     if (tile != 128 && tile != 256 && tile != 512) return set_error(LW_EINVAL, "lw_loc_icp_batch: tile must be 128/256/512");
-    if (!g->nrm || !g->planar) return set_error(LW_EINVAL, "lw_loc_icp_batch: the grid needs normals and planarity");
+    if (!g->nrm) return set_error(LW_EINVAL, "lw_loc_icp_batch: the grid needs normals");
     LocArgs la{};
     la.n_hyp = n_hyp;
     la.n_tiles = n_tiles;

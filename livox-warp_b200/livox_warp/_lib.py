@@ -90,7 +90,7 @@ class ClusterBuf(C.Structure):
 class PriorGrid(C.Structure):
     """mapgrid.Grid (mapgrid.py:35-43) plus the map arrays the grid kernels read."""
 
-    _fields_ = [("xyz", P), ("nrm", P), ("planar", P), ("start", P), ("nn", P), ("df", P), ("seed", P), ("nn2", P),
+    _fields_ = [("xyz", P), ("nrm", P), ("start", P), ("nn", P), ("df", P), ("seed", P), ("nn2", P),
                 ("origin", f32 * 3), ("cell", f32), ("inv_cell", f32), ("nx", i32), ("ny", i32), ("nz", i32),
                 ("pad_", i32), ("n", i64), ("ncell", i64)]
 

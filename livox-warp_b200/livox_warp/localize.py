@@ -371,6 +371,26 @@ class GlobalLocalizer:
         lo, hi = self._upload_pts([np.asarray(s, dtype=np.float32) for s in scans], stream)
         return self._run(lo, hi, T0s, schedule, stream, tile)
 
+    def register_packed(self, pts4: torch.Tensor, lo, hi, T0s, schedule=SCHEDULE_ICP, stream=None,
+                        tile: int | None = None) -> BatchResult:
+        """register_batch for scans already packed one after another in `pts4` ((N, 4) float32: x, y, z, unused;
+        a pinned host tensor is copied asynchronously, a device tensor in place); hypothesis h owns rows
+        lo[h] .. hi[h]."""
+        stream = stream if stream is not None else torch.cuda.current_stream(self.device)
+        b = self.batch
+        n = pts4.shape[0]
+        if pts4.dtype != torch.float32 or pts4.dim() != 2 or pts4.shape[1] != 4 or not pts4.is_contiguous():
+            raise ValueError("pts4 must be a contiguous (N, 4) float32 tensor")
+        if n > b.pts_cap:
+            raise ValueError(f"{n} points exceed the batch's {b.pts_cap}")
+        lo = np.asarray(lo, dtype=np.int64)
+        hi = np.asarray(hi, dtype=np.int64)
+        if len(lo) != len(T0s) or len(hi) != len(T0s) or (len(lo) and (lo.min() < 0 or hi.max() > n)):
+            raise ValueError("lo / hi must give each hypothesis a row range of pts4")
+        with torch.cuda.stream(stream):
+            b.pts[:n].copy_(pts4, non_blocking=True)
+        return self._run(lo, hi, T0s, schedule, stream, tile)
+
     def register_graph(self, lo, hi, schedule=SCHEDULE_ICP, tile: int = 256, stream=None):
         """A CUDA graph of the batched launch for the staged batch's shape class: the hypothesis and tile counts
         are read on the device (lw_loc_batch.dims), so one capture replays over any batch up to the buffers'

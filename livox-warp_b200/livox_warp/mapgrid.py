@@ -7,9 +7,10 @@ Per cell the grid holds
     ~0.8 m, so queries farther from the map still get a nearest point;
   - `df`: that distance in cm as a byte, 255 beyond the band.
 
-Device layout (HBM): xyz and nrm as packed float32 triples, planarity float32, start int32 [ncell+1], nn int32
-[ncell], df uint8 [ncell]: n * 28 + ncell * 9 bytes. The build's two scratch arrays (a uint64 seed and a second
-int32 flood buffer, ncell * 12 bytes) are freed when build() returns.
+Device layout (HBM): each map point is one 16-byte record (x, y, z, planarity) so that a nearest-point scan
+gathers one aligned vector per point; nrm packed float32 triples (read only for a matched point); start int32
+[ncell+1], nn int32 [ncell], df uint8 [ncell]: n * 28 + ncell * 9 bytes. The build's two scratch arrays (a
+uint64 seed and a second int32 flood buffer, ncell * 12 bytes) are freed when build() returns.
 
 Differences from the reference, both in the build: seeds are 64-bit keys (distance mm << 32 | index), so a map
 may hold up to 2^31 - 2 points instead of 2^23 - 1 (mapgrid.py:26-30, 223-224); and each flood step reads one
@@ -100,9 +101,8 @@ class PriorGrid:
         self.cell = float(host["cell"])
         self.levels = host["levels"]
         d = self.device
-        self.xyz = torch.empty((self.n, 3), dtype=torch.float32, device=d)
+        self.xyzp = torch.empty((self.n, 4), dtype=torch.float32, device=d)  # x, y, z, planarity
         self.nrm = torch.empty((self.n, 3), dtype=torch.float32, device=d)
-        self.planar = torch.empty(self.n, dtype=torch.float32, device=d)
         self.start = torch.empty(self.ncell + 1, dtype=torch.int32, device=d)
         self.nn = torch.empty(self.ncell, dtype=torch.int32, device=d)
         self.df = torch.empty(self.ncell, dtype=torch.uint8, device=d)
@@ -112,7 +112,7 @@ class PriorGrid:
 
     def _struct(self, seed, nn2) -> _lib.PriorGrid:
         g = _lib.PriorGrid()
-        g.xyz, g.nrm, g.planar = _lib.ptr(self.xyz), _lib.ptr(self.nrm), _lib.ptr(self.planar)
+        g.xyz, g.nrm = _lib.ptr(self.xyzp), _lib.ptr(self.nrm)
         g.start, g.nn, g.df = _lib.ptr(self.start), _lib.ptr(self.nn), _lib.ptr(self.df)
         g.seed, g.nn2 = _lib.ptr(seed), _lib.ptr(nn2)
         g.origin = (_lib.f32 * 3)(*[float(v) for v in self.origin])
@@ -127,8 +127,17 @@ class PriorGrid:
         """The lw_prior_grid the localisation launches read."""
         return self._g
 
+    @property
+    def xyz(self) -> torch.Tensor:
+        """The sorted map points (a view of the (x, y, z, planarity) records)."""
+        return self.xyzp[:, :3]
+
+    @property
+    def planar(self) -> torch.Tensor:
+        return self.xyzp[:, 3]
+
     def gpu_bytes(self) -> int:
-        return self.n * (12 + 12 + 4) + (self.ncell + 1) * 4 + self.ncell * (4 + 1)
+        return self.n * (16 + 12) + (self.ncell + 1) * 4 + self.ncell * (4 + 1)
 
     def build(self, stream=None):
         """Upload the points and build the grid, every op on `stream`; returns when it is done."""
@@ -136,9 +145,11 @@ class PriorGrid:
         s = stream if stream is not None else torch.cuda.current_stream(self.device)
         h = self._host
         with torch.cuda.stream(s):
-            self.xyz.copy_(torch.from_numpy(h["xyz"]))
+            rec = np.empty((self.n, 4), np.float32)
+            rec[:, :3] = h["xyz"]
+            rec[:, 3] = h["planarity"]
+            self.xyzp.copy_(torch.from_numpy(rec))
             self.nrm.copy_(torch.from_numpy(h["normal"]))
-            self.planar.copy_(torch.from_numpy(h["planarity"]))
             self.start.copy_(torch.from_numpy(h["start"]))
             seed = torch.empty(self.ncell, dtype=torch.int64, device=self.device)
             nn2 = torch.empty(self.ncell, dtype=torch.int32, device=self.device)

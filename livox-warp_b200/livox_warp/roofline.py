@@ -18,6 +18,15 @@ from the frame's points, its solved pose and the table's occupied keys, per kern
   integration insert (one launch = one batch):
       24 B per point (x, y, z, attr, t, frame id) + 2 * 64 B per distinct voxel touched (key, count, sums, times)
 
+  batched localisation ICP (one launch = every iteration of every hypothesis, then the evaluation), per
+  iteration and for the evaluation pass:
+      16 B per scan point of every hypothesis (x, y, z, pad)
+    +  8 B per distinct grid cell probed (its start pair; the flooded seed is read only where a query has
+       no point within one cell and is not counted)
+    + 12 B per distinct map point in those cells (its xyz)
+    + 16 B per distinct map point matched (its normal and planarity; the ICP iterations only)
+    + 2 * 32 * 8 B per tile (the float64 tile partials written and read back)
+
 The counts use the solved pose for every iteration and sample each ray every quarter voxel, so they are
 estimates of the compulsory traffic, not measurements: ncu's dram__bytes is the measured counterpart.
 """
@@ -97,3 +106,34 @@ def map_insert_bytes(xyz_sensor: np.ndarray, T: np.ndarray, voxel: float) -> flo
     w = _world(xyz_sensor, T)
     touched = np.unique(keys_of(np.floor(w / voxel).astype(np.int64)))
     return float(24 * len(w) + 2 * 64 * len(touched))
+
+
+def loc_bytes(start: np.ndarray, origin: np.ndarray, dims: np.ndarray, cell: float, pts4: np.ndarray,
+              lo: np.ndarray, hi: np.ndarray, T: np.ndarray, iters: int, n_tiles: int) -> dict:
+    """Compulsory bytes of one batched localisation launch, counted at the final poses T (k, 4, 4)."""
+    cells, matched_cells = [], []
+    r = np.arange(-1, 2)
+    off = np.stack(np.meshgrid(r, r, r, indexing="ij"), -1).reshape(-1, 3)
+    dims = np.asarray(dims, dtype=np.int64)
+    for h in range(len(T)):
+        p = pts4[lo[h]:hi[h], :3].astype(np.float64)
+        if len(p) == 0:
+            continue
+        w = p @ T[h, :3, :3].T + T[h, :3, 3]
+        ijk = np.floor((w - origin) / cell).astype(np.int64)
+        own = ijk
+        ok = np.all((own >= 0) & (own < dims), axis=1)
+        matched_cells.append(((own[ok, 2] * dims[1] + own[ok, 1]) * dims[0] + own[ok, 0]))
+        nb = (ijk[:, None, :] + off[None, :, :]).reshape(-1, 3)
+        ok = np.all((nb >= 0) & (nb < dims), axis=1)
+        nb = nb[ok]
+        cells.append(np.unique((nb[:, 2] * dims[1] + nb[:, 1]) * dims[0] + nb[:, 0]))
+    c = np.unique(np.concatenate(cells)) if cells else np.zeros(0, np.int64)
+    mc = np.unique(np.concatenate(matched_cells)) if matched_cells else np.zeros(0, np.int64)
+    visited = int((start[c + 1] - start[c]).sum())
+    matched = int((start[mc + 1] - start[mc]).sum())  # points sharing a cell with a query: the matches' bound
+    n_pts = int(np.maximum(np.asarray(hi) - np.asarray(lo), 0).sum())
+    per_iter = 16 * n_pts + 8 * len(c) + 12 * visited + 16 * matched + 2 * 32 * 8 * n_tiles
+    eval_pass = 16 * n_pts + 8 * len(c) + 12 * visited
+    return {"bytes": float(iters * per_iter + eval_pass), "per_iter": float(per_iter), "cells": int(len(c)),
+            "visited_points": visited, "matched_points_bound": matched}
