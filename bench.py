@@ -366,18 +366,18 @@ def _loc_scans(args):
     return [synth.spin_scan(scene, T[i], int(sizes[i]), int(seeds[i])) for i in range(len(T))]
 
 
-def loc_workload(procs: int | None = None):
+def loc_workload(n_hyp: int = LOC_HYP, spacing: float = LOC_SPACING, procs: int | None = None):
     """Prior map, packed scans (N, 4), per-hypothesis row ranges, true and initial poses (before any CUDA call)."""
     from livox_warp import synth
 
     scene = synth.office(LOC_SEED)
-    xyz, nrm = synth.sample_surfaces(scene, LOC_SPACING, LOC_SEED, jitter=0.002)
-    T_true = synth.free_poses(scene, LOC_HYP, LOC_POSE_SEED, z=LOC_Z, margin=0.6)
+    xyz, nrm = synth.sample_surfaces(scene, spacing, LOC_SEED, jitter=0.002)
+    T_true = synth.free_poses(scene, LOC_HYP, LOC_POSE_SEED, z=LOC_Z, margin=0.6)[:n_hyp]
     rng = np.random.default_rng(LOC_POSE_SEED + 1)
-    sizes = rng.integers(LOC_PTS[0], LOC_PTS[1] + 1, LOC_HYP)
-    seeds = 1000 + np.arange(LOC_HYP)
+    sizes = rng.integers(LOC_PTS[0], LOC_PTS[1] + 1, LOC_HYP)[:n_hyp]
+    seeds = 1000 + np.arange(n_hyp)
     procs = procs or min(8, os.cpu_count() or 1)
-    parts = np.array_split(np.arange(LOC_HYP), procs * 2)
+    parts = np.array_split(np.arange(n_hyp), procs * 2)
     jobs = [(T_true[p], sizes[p], seeds[p]) for p in parts if len(p)]
     with mp.get_context("spawn").Pool(procs) as pool:
         scans = [s for chunk in pool.map(_loc_scans, jobs) for s in chunk]
@@ -391,7 +391,7 @@ def loc_workload(procs: int | None = None):
     T0 = T_true.copy()
     yaw = np.arctan2(T_true[:, 1, 0], T_true[:, 0, 0])
     yq = np.round(np.degrees(yaw) / 5.0) * np.radians(5.0)
-    for h in range(LOC_HYP):
+    for h in range(n_hyp):
         c, s_ = math.cos(yq[h]), math.sin(yq[h])
         T0[h, :3, :3] = np.array([[c, -s_, 0.0], [s_, c, 0.0], [0.0, 0.0, 1.0]])
         T0[h, :2, 3] = np.round(T_true[h, :2, 3] / 0.5) * 0.5
@@ -424,13 +424,14 @@ def loc_oracle(og, w, idx, threads):
 def run_localize(a, rank: int, world: int, local: int):
     from oracle import oracle as _o
 
-    w = loc_workload()
+    w = loc_workload(a.loc_hyp, a.loc_spacing)
+    K = len(w["T0"])
     metric = "batched global localisation hypotheses/s (point-to-plane ICP schedule + evaluation)"
     config = {"workload": f"global localisation: office 40x30x3 m (walls, doors, 200 boxes), prior map "
-                          f"{len(w['xyz']):,} pts at {LOC_SPACING * 1e3:.0f} mm with normals, {LOC_HYP} hypotheses "
+                          f"{len(w['xyz']):,} pts at {a.loc_spacing * 1e3:.0f} mm with normals, {K} hypotheses "
                           f"(xy on a 0.5 m grid, yaw on 5 deg, z {LOC_Z} m) each with its own 360-degree scan of "
                           f"U[{LOC_PTS[0]}, {LOC_PTS[1]}] pts",
-              "map_points": int(len(w["xyz"])), "hypotheses": LOC_HYP, "scan_points_total": int(len(w["pts4"])),
+              "map_points": int(len(w["xyz"])), "hypotheses": K, "scan_points_total": int(len(w["pts4"])),
               "schedule": "(0.40,8),(0.20,8),(0.10,8),(0.05,10)", "l2": "flushed between steps (256 MB write)",
               "parallelism": f"replicas x{a.gpus}"}
     if a.impl == "reference":
@@ -438,7 +439,7 @@ def run_localize(a, rank: int, world: int, local: int):
             return
         threads = _o.host_cores()
         og = _o.PriorGrid(_o.prior_prepare(w["xyz"], w["nrm"]))
-        k = min(LOC_HYP, max(threads, 8))
+        k = min(K, max(threads, 8))
         T, count, iters, ev, secs = loc_oracle(og, w, np.arange(k), threads)
         v = k / secs
         line = {"impl": "reference", "metric": metric, "value": round(v, 3), "unit": "hypotheses/s",
@@ -466,22 +467,22 @@ def run_localize(a, rank: int, world: int, local: int):
     prep_s = time.perf_counter() - t0
     grid.build()
     n_all = len(w["pts4"])
-    loc = GlobalLocalizer(grid, device, hyp_cap=LOC_HYP, pts_cap=n_all)
+    loc = GlobalLocalizer(grid, device, hyp_cap=K, pts_cap=n_all)
     stream = torch.cuda.current_stream(device)
     pinned = torch.from_numpy(w["pts4"]).pin_memory()
     # autotune (tile per CTA) through the public call, then capture the launch in a graph
     res = loc.register_packed(pinned, w["lo"], w["hi"], w["T0"])
-    tile = res.tile
-    replay = loc.register_graph(w["lo"], w["hi"], SCHEDULE_ICP, tile)
+    tile, minb = res.tile, res.blocks_per_sm
+    replay = loc.register_graph(w["lo"], w["hi"], SCHEDULE_ICP, tile, blocks_per_sm=minb)
     b = loc.batch
-    T0_dev = torch.from_numpy(w["T0"].reshape(LOC_HYP, 16).copy()).to(device)
+    T0_dev = torch.from_numpy(w["T0"].reshape(K, 16).copy()).to(device)
     b.pts[:n_all].copy_(pinned.to(device))
     b.stage(w["lo"], w["hi"], tile, stream)
-    g = loc._graphs[(tuple(SCHEDULE_ICP), tile)]
+    g = loc._graphs[(tuple(SCHEDULE_ICP), tile, minb)]
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
 
     def dev_step():
-        b.T[:LOC_HYP].copy_(T0_dev)
+        b.T[:K].copy_(T0_dev)
         g.replay()
 
     for _ in range(a.warmup):
@@ -499,25 +500,25 @@ def run_localize(a, rank: int, world: int, local: int):
     torch.cuda.synchronize(device)
     clk = clocks.stop()
     step_ms = np.array([x.elapsed_time(y) for x, y in evs])
-    T_dev = b.T[:LOC_HYP].cpu().numpy().reshape(LOC_HYP, 4, 4)
+    T_dev = b.T[:K].cpu().numpy().reshape(K, 4, 4)
     iters = int(b.outs[b.o_it].item())
     ms_total = float(step_ms.sum())
-    value = world * a.steps * LOC_HYP / (ms_total * 1e-3)
+    value = world * a.steps * K / (ms_total * 1e-3)
     # e2e: from pinned host scans through register_packed (H2D of scans, tiles and poses; D2H of poses and fits)
     for _ in range(3):
-        loc.register_packed(pinned, w["lo"], w["hi"], w["T0"], tile=tile)
+        loc.register_packed(pinned, w["lo"], w["hi"], w["T0"], tile=tile, blocks_per_sm=minb)
     torch.cuda.synchronize(device)
     e_steps = max(3, min(a.steps, 20))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(e_steps):
-        r = loc.register_packed(pinned, w["lo"], w["hi"], w["T0"], tile=tile)
+        r = loc.register_packed(pinned, w["lo"], w["hi"], w["T0"], tile=tile, blocks_per_sm=minb)
     e1.record(stream)
     torch.cuda.synchronize(device)
     e_ms = e0.elapsed_time(e1)
     nt = int(b.h_ints[1])
-    h2d = n_all * 16 + LOC_HYP * 128 + 4 * (2 + LOC_HYP + LOC_HYP + 1 + 2 * nt)
-    d2h = LOC_HYP * 128 + 4 * (4 * LOC_HYP + 2)
+    h2d = n_all * 16 + K * 128 + 4 * (2 + K + K + 1 + 2 * nt)
+    d2h = K * 128 + 4 * (4 * K + 2)
     # the timed region replays the captured graph (k_loc_reset + k_loc_icp) once per step; graph replays do not
     # pass through the library's host-side launch counter
     launches = 2 * a.steps
@@ -535,23 +536,25 @@ def run_localize(a, rank: int, world: int, local: int):
             "unit": "GB/s", "frac": round(ach / peak["hbm_gbs"], 5), "traffic": None,
             "peak_source": peak["source"], "avg_launch_us": round(avg_ms * 1e3, 2), "iterations": iters,
             "algorithmic_bytes_per_launch": int(lb["bytes"]), "distinct_cells": lb["cells"],
-            "distinct_map_points": lb["visited_points"], "tile": tile}
+            "distinct_map_points": lb["visited_points"], "tile": tile,
+            "blocks_per_sm": minb, "autotune_ms": {f"{t}x{m}": round(v, 3) for (t, m), v in
+                                                   next(iter(loc.tuner.trials.values()), {}).items()}}
     # parity and the CPU baseline: the first 16 hypotheses as one batch, GPU and oracle
     threads = _o.host_cores()
     # the oracle's grid over the same prepared arrays; its flooded seeds are the device's, which the parity
     # tests hold bit-exact to the oracle's own flood (flooding 43M cells on the host would take a minute)
     og = _o.PriorGrid(grid._host, build=False)
     og.nn[:] = grid.nn.cpu().numpy()
-    idx = np.arange(16)
+    idx = np.arange(min(16, K))
     oT, ocount, oiters, oev, secs = loc_oracle(og, w, idx, threads)
     n16 = w["hi"][idx] - w["lo"][idx]
     hi16 = np.cumsum(n16)
     lo16 = hi16 - n16
     p16 = torch.from_numpy(np.concatenate([w["pts4"][w["lo"][h]:w["hi"][h]] for h in idx])).pin_memory()
-    g16 = loc.register_packed(p16, lo16, hi16, w["T0"][idx], tile=tile)
+    g16 = loc.register_packed(p16, lo16, hi16, w["T0"][idx], tile=tile, blocks_per_sm=minb)
     from livox_warp.localize import pose_difference
 
-    pd = np.array([pose_difference(oT[h], g16.T[h]) for h in range(16)])
+    pd = np.array([pose_difference(oT[h], g16.T[h]) for h in range(len(idx))])
     line = {"metric": metric, "value": round(value, 3), "unit": "hypotheses/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(avg_ms, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 tile sums, solve and poses)",
@@ -561,13 +564,14 @@ def run_localize(a, rank: int, world: int, local: int):
             "step_ms_p50_p99": [round(float(np.percentile(step_ms, 50)), 4),
                                 round(float(np.percentile(step_ms, 99)), 4)],
             "roofline": roof,
-            "cpu_baseline": {"value": round(16 / secs, 3), "unit": "hypotheses/s", "cores": threads, "kind": "port",
-                             "sample": f"the first 16 hypotheses as one batch through the CPU oracle "
+            "cpu_baseline": {"value": round(len(idx) / secs, 3), "unit": "hypotheses/s", "cores": threads,
+                             "kind": "port",
+                             "sample": f"the first {len(idx)} hypotheses as one batch through the CPU oracle "
                                        f"(C++/OpenMP, float64 terms), {secs:.1f} s"},
-            "vs_fp64_oracle": {"hypotheses": 16, "max_m": round(float(pd[:, 0].max()), 7),
+            "vs_fp64_oracle": {"hypotheses": len(idx), "max_m": round(float(pd[:, 0].max()), 7),
                                "max_deg": round(float(pd[:, 1].max()), 6), "iters_gpu": g16.iters,
                                "iters_oracle": oiters},
-            "e2e": {"value": round(world * e_steps * LOC_HYP / (e_ms * 1e-3), 3), "unit": "hypotheses/s",
+            "e2e": {"value": round(world * e_steps * K / (e_ms * 1e-3), 3), "unit": "hypotheses/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches), "graph": True, "clocks": clk, "prepare_s": round(prep_s, 2),
             "grid_build_s": round(grid.build_s, 3)}
@@ -586,6 +590,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", choices=("sequence", "localize"), default="sequence")
+    ap.add_argument("--loc-hyp", type=int, default=256, help="localize: hypotheses (a smaller profiling case)")
+    ap.add_argument("--loc-spacing", type=float, default=0.015, help="localize: prior-map sample spacing (m)")
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -362,8 +362,8 @@ int lw_prior_distances(const lw_prior_grid* g, const float* pts, int64_t n, cons
                        void* stream);
 
 /* Buffers of the batched ICP: every hypothesis has its own range of points (tile_lo .. scan_end; hypotheses may
- * share one scan) and pose (T, in and out). The points are cut into tiles of `tile` points that never span two
- * hypotheses: hypothesis h owns tiles hyp_tile[h] .. hyp_tile[h+1]. */
+ * share one scan) and pose (T, in and out). The points are cut into tiles of at most `tile` points that never
+ * span two hypotheses: hypothesis h owns tiles hyp_tile[h] .. hyp_tile[h+1]. */
 typedef struct lw_loc_batch {
     float* pts;         /* [pts_cap*4] x, y, z, unused */
     int32_t* scan_end;  /* [n_hyp] end (exclusive) of each hypothesis' points */
@@ -373,6 +373,7 @@ typedef struct lw_loc_batch {
     double* T;          /* [n_hyp*16] row-major poses, updated in place */
     double* tile_part;  /* [n_tiles*32] float64 tile partials (scratch) */
     int32_t* moved;     /* [moved_cap] largest step of each iteration (scratch) */
+    int32_t* next;      /* [moved_cap + 1] tile counters of the iterations and the evaluation (scratch) */
     int32_t* count;     /* [n_hyp] matched points in the last iteration */
     int32_t* eval;      /* [n_hyp*3] points within 3 / 5 / 10 cm of the map at the final pose */
     uint32_t* bar;      /* [2] grid barrier, zero before the first use */
@@ -389,10 +390,12 @@ typedef struct lw_loc_batch {
  * Geman-McClure c2 = (dmax/2)^2 are formed in double and rounded to float, as the reference's host does); a
  * hypothesis with fewer than min_count matches keeps its pose; a stage ends when no hypothesis moved 2e-4
  * (n_stages = 0 only evaluates). With b->dims set, n_hyp and n_tiles are capacities and the counts are read on
- * the device. tile: 128, 256 or 512 points per CTA; grid <= 0 picks one full wave. */
+ * the device. tile: points per tile (a multiple of 32 up to 2048), each tile worked by one warp; the host's tiling
+ * must use the same value. blocks_per_sm: the register budget, 2 or 3 resident 256-thread CTAs per SM (0 = 3).
+ * grid <= 0 picks one full wave. */
 int lw_loc_icp_batch(const lw_prior_grid* g, lw_loc_batch* b, int32_t n_hyp, int32_t n_tiles, int32_t tile,
                      int32_t n_stages, const double* dmax, const int32_t* iters, float alpha, int32_t min_count,
-                     int32_t grid, void* stream);
+                     int32_t blocks_per_sm, int32_t grid, void* stream);
 
 #ifdef __cplusplus
 }

@@ -288,25 +288,35 @@ __device__ __forceinline__ void loc_terms(const lw_prior_grid& g, const LocPose&
     float d2 = fmaf(r0, Mr0, fmaf(r1, Mr1, r2 * Mr2));
     float wgt = 1.0f / (1.0f + d2 / c2);
     wgt = wgt * wgt;  // Geman-McClure
-    const float C[6][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f},
-                           {0.f, -lz, ly},  {lz, 0.f, -lx}, {-ly, lx, 0.f}};
-    float MC[6][3];
+    // J = [I | A] with A = -[l]x, so H = w [[M, M A], [A^T M, A^T M A]] and b = w [M r; A^T M r]
+    // (the upper triangle in row-major order, the layout of accumulate(), odom.py:244-259)
+    const float A[3][3] = {{0.f, lz, -ly}, {-lz, 0.f, lx}, {ly, -lx, 0.f}};
+    const float Ms[3][3] = {{M[0], M[1], M[2]}, {M[1], M[3], M[4]}, {M[2], M[4], M[5]}};
+    float MA[3][3];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        MC[k][0] = fmaf(M[0], C[k][0], fmaf(M[1], C[k][1], M[2] * C[k][2]));
-        MC[k][1] = fmaf(M[1], C[k][0], fmaf(M[3], C[k][1], M[4] * C[k][2]));
-        MC[k][2] = fmaf(M[2], C[k][0], fmaf(M[4], C[k][1], M[5] * C[k][2]));
-    }
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) MA[r][j] = fmaf(Ms[r][0], A[0][j], fmaf(Ms[r][1], A[1][j], Ms[r][2] * A[2][j]));
     int idx = 0;
 #pragma unroll
     for (int pp = 0; pp < 6; ++pp)
 #pragma unroll
         for (int qq = pp; qq < 6; ++qq) {
-            a[idx] = fmaf(wgt, fmaf(C[pp][0], MC[qq][0], fmaf(C[pp][1], MC[qq][1], C[pp][2] * MC[qq][2])), a[idx]);
+            float h;
+            if (qq < 3)
+                h = Ms[pp][qq];
+            else if (pp < 3)
+                h = MA[pp][qq - 3];
+            else
+                h = fmaf(A[0][pp - 3], MA[0][qq - 3], fmaf(A[1][pp - 3], MA[1][qq - 3], A[2][pp - 3] * MA[2][qq - 3]));
+            a[idx] = fmaf(wgt, h, a[idx]);
             ++idx;
         }
+    a[21] = fmaf(wgt, Mr0, a[21]);
+    a[22] = fmaf(wgt, Mr1, a[22]);
+    a[23] = fmaf(wgt, Mr2, a[23]);
 #pragma unroll
-    for (int pp = 0; pp < 6; ++pp) a[21 + pp] = fmaf(wgt, fmaf(C[pp][0], Mr0, fmaf(C[pp][1], Mr1, C[pp][2] * Mr2)), a[21 + pp]);
+    for (int j = 0; j < 3; ++j) a[24 + j] = fmaf(wgt, fmaf(A[0][j], Mr0, fmaf(A[1][j], Mr1, A[2][j] * Mr2)), a[24 + j]);
     a[27] += 1.0f;
     a[28] = fmaf(wgt, d2, a[28]);
     a[29] += wgt;
@@ -314,6 +324,7 @@ __device__ __forceinline__ void loc_terms(const lw_prior_grid& g, const LocPose&
 
 struct LocArgs {
     int n_hyp, n_tiles, n_stages;  // counts, or capacities when b.dims is set
+    int tile;                      // points per warp tile
     float max_d2[8], c2[8];
     int iters[8];
     float alpha;
@@ -321,12 +332,42 @@ struct LocArgs {
     int min_count;  // a hypothesis with fewer matched points skips its update (localize.py:538)
 };
 
-__global__ void __launch_bounds__(512, 1)
+constexpr int LOC_BLOCK = 256;
+constexpr unsigned FULL = 0xffffffffu;
+
+// Reduce-scatter over a warp: afterwards lane j holds the sum over the 32 lanes of v[j]. Each of the five steps
+// hands half of the remaining slots to the partner lane (31 shuffles in all, against 5 per slot for 32 butterfly
+// reductions).
+__device__ __forceinline__ float warp_reduce_scatter32(float (&v)[32], int lane) {
+#pragma unroll
+    for (int half = 16; half >= 1; half >>= 1) {
+        const bool up = (lane & half) != 0;
+#pragma unroll
+        for (int k = 0; k < half; ++k) {
+            const float send = up ? v[k] : v[k + half];
+            const float keep = up ? v[k + half] : v[k];
+            v[k] = keep + __shfl_xor_sync(FULL, send, half);
+        }
+    }
+    return v[0];
+}
+
+// The next tile of pass `pass` for the calling warp (one atomic per tile, broadcast to the warp).
+__device__ __forceinline__ int next_tile(const lw_loc_batch& b, int pass, int lane) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(b.next + pass, 1);
+    return __shfl_sync(FULL, t, 0);
+}
+
+// MINB: CTAs of LOC_BLOCK threads the register budget must let reside per SM -- 2 (up to 128 registers, no
+// spills) or 3 (80 registers, a few spilled words, half again as many warps to hide the gathers' latency).
+template <int MINB>
+__global__ void __launch_bounds__(LOC_BLOCK, MINB)
     k_loc_icp(lw_prior_grid g, lw_loc_batch b, LocArgs la) {
-    extern __shared__ float smem[];  // [LTERMS][blockDim/32] per-term warp partials
     __shared__ double sv[32];
     __shared__ int s_stop;
     const int tid = threadIdx.x;
+    const int lane = tid & 31;
     const int n_hyp = b.dims ? min(__ldg(b.dims), la.n_hyp) : la.n_hyp;
     const int n_tiles = b.dims ? min(__ldg(b.dims + 1), la.n_tiles) : la.n_tiles;
     int it_total = 0;
@@ -334,34 +375,25 @@ __global__ void __launch_bounds__(512, 1)
         const float max_d2 = la.max_d2[stage];
         const float c2 = la.c2[stage];
         for (int it = 0; it < la.iters[stage]; ++it, ++it_total) {
-            // phase A: tiles -> float64 partials
-            for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+            // phase A: warp tiles, handed out in order of arrival, -> float64 tile partials. A tile's partial
+            // does not depend on which warp computed it, so the sums of phase B are deterministic.
+            for (;;) {
+                const int tile = next_tile(b, it_total, lane);
+                if (tile >= n_tiles) break;
                 int h, lo, hi;
                 tile_range(b, tile, n_hyp, h, lo, hi);
-                LocPose P;
-                if (h >= 0) loc_pose(b.T + 16 * h, P);
-                float a[LTERMS];
+                float v[32];
 #pragma unroll
-                for (int k = 0; k < LTERMS; ++k) a[k] = 0.0f;
-                const int i = lo + tid;
-                if (h >= 0 && i < hi && i < lo + (int)blockDim.x)
-                    loc_terms(g, P, __ldg(reinterpret_cast<const float4*>(b.pts) + i), max_d2, c2, la.alpha, a);
-                // warp sums of the 30 terms, then the warps in order (one pass through shared memory)
-                const int lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-                for (int k = 0; k < LTERMS; ++k) {
-                    float v = a[k];
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                    if (lane == 0) smem[k * nw + w] = v;
+                for (int k = 0; k < 32; ++k) v[k] = 0.0f;
+                if (h >= 0) {
+                    LocPose P;
+                    loc_pose(b.T + 16 * h, P);
+                    const int end = min(hi, lo + la.tile);
+                    for (int i = lo + lane; i < end; i += 32)
+                        loc_terms(g, P, __ldg(reinterpret_cast<const float4*>(b.pts) + i), max_d2, c2, la.alpha, v);
                 }
-                __syncthreads();
-                if (tid < LTERMS) {
-                    double sum = 0.0;
-                    for (int ww = 0; ww < nw; ++ww) sum += (double)smem[tid * nw + ww];
-                    b.tile_part[(int64_t)tile * 32 + tid] = sum;
-                }
-                __syncthreads();
+                const float sum = warp_reduce_scatter32(v, lane);
+                if (lane < LTERMS) b.tile_part[(int64_t)tile * 32 + lane] = (double)sum;
             }
             if (!grid_barrier(b.bar, b.err, 1)) return;
             // phase B: per hypothesis, sum its tiles in order and solve (localize.py:537-550)
@@ -467,14 +499,17 @@ __global__ void __launch_bounds__(512, 1)
         }
     }
     // evaluation (localize.py:182-205): points within each radius of their nearest map point, per hypothesis
-    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    for (;;) {
+        const int tile = next_tile(b, it_total, lane);
+        if (tile >= n_tiles) break;
         int h, lo, hi;
         tile_range(b, tile, n_hyp, h, lo, hi);
+        if (h < 0) continue;
         float M[12];
-        for (int k = 0; k < 12; ++k) M[k] = h >= 0 ? (float)__ldcg(b.T + 16 * h + k) : 0.0f;
+        for (int k = 0; k < 12; ++k) M[k] = (float)__ldcg(b.T + 16 * h + k);
         int c0 = 0, c1 = 0, c2 = 0;
-        const int i = lo + tid;
-        if (h >= 0 && i < hi && i < lo + (int)blockDim.x) {
+        const int end = min(hi, lo + la.tile);
+        for (int i = lo + lane; i < end; i += 32) {
             float4 p = __ldg(reinterpret_cast<const float4*>(b.pts) + i);
             float wx, wy, wz;
             xform(M, p.x, p.y, p.z, wx, wy, wz);
@@ -482,16 +517,18 @@ __global__ void __launch_bounds__(512, 1)
             if (s >= 0) {
                 const float4 q = ld_pt(reinterpret_cast<const float4*>(g.xyz), s);
                 float d = len3(wx - q.x, wy - q.y, wz - q.z);
-                c0 = d < la.radii[0];
-                c1 = d < la.radii[1];
-                c2 = d < la.radii[2];
+                c0 += d < la.radii[0];
+                c1 += d < la.radii[1];
+                c2 += d < la.radii[2];
             }
         }
-        int t0 = __syncthreads_count(c0), t1 = __syncthreads_count(c1), t2 = __syncthreads_count(c2);
-        if (tid == 0 && h >= 0) {
-            atomicAdd(b.eval + 3 * h + 0, t0);
-            atomicAdd(b.eval + 3 * h + 1, t1);
-            atomicAdd(b.eval + 3 * h + 2, t2);
+        c0 = __reduce_add_sync(FULL, c0);
+        c1 = __reduce_add_sync(FULL, c1);
+        c2 = __reduce_add_sync(FULL, c2);
+        if (lane == 0) {
+            atomicAdd(b.eval + 3 * h + 0, c0);
+            atomicAdd(b.eval + 3 * h + 1, c1);
+            atomicAdd(b.eval + 3 * h + 2, c2);
         }
     }
     if (blockIdx.x == 0 && tid == 0) *b.iters_run = it_total;
@@ -501,6 +538,7 @@ __global__ void __launch_bounds__(512, 1)
 // barrier may have left it part counted (its generation word needs no reset).
 __global__ void k_loc_reset(lw_loc_batch b, int n_hyp, int max_iters) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < max_iters; i += gridDim.x * blockDim.x) b.moved[i] = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= max_iters; i += gridDim.x * blockDim.x) b.next[i] = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n_hyp; i += gridDim.x * blockDim.x) b.eval[i] = 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *b.err = 0;
@@ -566,20 +604,22 @@ int lw_prior_distances(const lw_prior_grid* g, const float* pts, int64_t n, cons
 
 int lw_loc_icp_batch(const lw_prior_grid* g, lw_loc_batch* b, int32_t n_hyp, int32_t n_tiles, int32_t tile,
                      int32_t n_stages, const double* dmax, const int32_t* iters, float alpha, int32_t min_count,
-                     int32_t grid, void* stream) {
+                     int32_t blocks_per_sm, int32_t grid, void* stream) {
     int r = check_grid(g, "lw_loc_icp_batch");
     if (r != LW_OK) return r;
     if (!b || (n_stages > 0 && (!dmax || !iters)) || n_stages < 0 || n_stages > 8 || n_hyp < 1 || n_tiles < 1)
         return set_error(LW_EINVAL, "lw_loc_icp_batch: bad arguments");
     if (!b->pts || !b->scan_end || !b->tile_hyp || !b->tile_lo || !b->hyp_tile || !b->T || !b->tile_part ||
-        !b->moved || !b->count || !b->eval || !b->bar || !b->err || !b->iters_run || b->pts_cap < 0)
+        !b->moved || !b->next || !b->count || !b->eval || !b->bar || !b->err || !b->iters_run || b->pts_cap < 0)
         return set_error(LW_EINVAL, "lw_loc_icp_batch: incomplete batch buffers");
-    if (tile != 128 && tile != 256 && tile != 512) return set_error(LW_EINVAL, "lw_loc_icp_batch: tile must be 128/256/512");
+    if (tile < 32 || tile > 2048 || tile % 32 != 0)
+        return set_error(LW_EINVAL, "lw_loc_icp_batch: tile must be a multiple of 32 in [32, 2048]");
     if (!g->nrm) return set_error(LW_EINVAL, "lw_loc_icp_batch: the grid needs normals");
     LocArgs la{};
     la.n_hyp = n_hyp;
     la.n_tiles = n_tiles;
     la.n_stages = n_stages;
+    la.tile = tile;
     int total_iters = 0;
     for (int k = 0; k < n_stages; ++k) {
         if (iters[k] < 0 || !(dmax[k] > 0.0)) return set_error(LW_EINVAL, "lw_loc_icp_batch: stage %d", k);
@@ -597,10 +637,13 @@ int lw_loc_icp_batch(const lw_prior_grid* g, lw_loc_batch* b, int32_t n_hyp, int
     la.min_count = min_count;
     cudaStream_t s = (cudaStream_t)stream;
     int sms = device_sms();
+    if (blocks_per_sm == 0) blocks_per_sm = 3;
+    if (blocks_per_sm != 2 && blocks_per_sm != 3)
+        return set_error(LW_EINVAL, "lw_loc_icp_batch: blocks_per_sm must be 0, 2 or 3");
+    const void* fn = blocks_per_sm == 2 ? (const void*)k_loc_icp<2> : (const void*)k_loc_icp<3>;
     int per_sm = 0;
-    const size_t dyn = (size_t)LTERMS * (tile / 32) * sizeof(float);
-    LW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_loc_icp, tile, dyn));
-    if (per_sm < 1) return set_error(LW_EINVAL, "lw_loc_icp_batch: tile %d does not fit on an SM", tile);
+    LW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, LOC_BLOCK, 0));
+    if (per_sm < 1) return set_error(LW_EINVAL, "lw_loc_icp_batch: the kernel does not fit on an SM");
     int max_grid = per_sm * sms;
     if (grid <= 0 || grid > max_grid) grid = max_grid;
     if (grid > b->grid_cap) grid = b->grid_cap;
@@ -610,15 +653,18 @@ int lw_loc_icp_batch(const lw_prior_grid* g, lw_loc_batch* b, int32_t n_hyp, int
     // so that it can also be captured into a CUDA graph
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(tile);
-    cfg.dynamicSmemBytes = dyn;
+    cfg.blockDim = dim3(LOC_BLOCK);
+    cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    LW_CUDA(cudaLaunchKernelEx(&cfg, k_loc_icp, *g, *b, la));
+    if (blocks_per_sm == 2)
+        LW_CUDA(cudaLaunchKernelEx(&cfg, k_loc_icp<2>, *g, *b, la));
+    else
+        LW_CUDA(cudaLaunchKernelEx(&cfg, k_loc_icp<3>, *g, *b, la));
     LW_LAUNCHED("lw_loc_icp_batch");
     count_launches(2);
     return LW_OK;

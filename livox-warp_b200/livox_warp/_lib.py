@@ -96,8 +96,8 @@ class PriorGrid(C.Structure):
 
 
 class LocBatch(C.Structure):
-    PTRS = ("pts", "scan_end", "tile_hyp", "tile_lo", "hyp_tile", "T", "tile_part", "moved", "count", "eval", "bar",
-            "err", "iters_run", "dims")
+    PTRS = ("pts", "scan_end", "tile_hyp", "tile_lo", "hyp_tile", "T", "tile_part", "moved", "next", "count", "eval",
+            "bar", "err", "iters_run", "dims")
     _fields_ = [(n, P) for n in PTRS] + [("pts_cap", i64), ("moved_cap", i32), ("grid_cap", i32)]
 
 
@@ -151,7 +151,7 @@ _SIGS = {
     "lw_prior_grid_build": (i32, [C.POINTER(PriorGrid), P]),
     "lw_prior_distances": (i32, [C.POINTER(PriorGrid), P, i64, C.POINTER(f64), P, P]),
     "lw_loc_icp_batch": (i32, [C.POINTER(PriorGrid), C.POINTER(LocBatch), i32, i32, i32, i32, C.POINTER(f64),
-                               C.POINTER(i32), f32, i32, i32, P]),
+                               C.POINTER(i32), f32, i32, i32, i32, P]),
 }
 
 _lib = None

@@ -12,8 +12,9 @@ Precision: the residuals and Jacobians run in float32 on points re-centred on th
 tile sums, the normal equations, the Cholesky solve and the poses are float64 (the reference sends float32
 poses to the device and solves with numpy in float64).
 
-Tile size (points per CTA: 128, 256 or 512) is chosen by `Autotuner`, which times the candidates once per
-batch shape class and caches the winner (in memory, and in a JSON file when LW_AUTOTUNE_CACHE names one).
+The launch shape -- points per warp tile (64, 128, 256 or 512) and the register budget (2 or 3 resident
+256-thread CTAs per SM) -- is chosen by `Autotuner`, which times the candidates once per batch shape class and
+caches the winner (in memory, and in a JSON file when LW_AUTOTUNE_CACHE names one).
 """
 
 from __future__ import annotations
@@ -36,7 +37,9 @@ SCHEDULE_ICP = ((0.40, 8), (0.20, 8), (0.10, 8), (0.05, 10))  # GlobalLocalizer.
 SCHEDULE_REFINE = ((0.30, 6), (0.12, 8), (0.05, 8))  # GlobalLocalizer.refine default, localize.py:569
 ALPHA = 0.05  # along-surface weight of a planar correspondence, localize.py:523
 MIN_COUNT = 30  # matches below which a hypothesis keeps its pose, localize.py:538
-TILES = (128, 256, 512)
+TILES = (64, 128, 256, 512)  # points per warp tile the autotuner tries
+BUDGETS = (2, 3)  # resident CTAs per SM the kernel's register budget is compiled for
+CANDIDATES = tuple((t, m) for t in TILES for m in BUDGETS)
 
 
 def rotz(a: float) -> np.ndarray:
@@ -86,23 +89,25 @@ class BatchResult:
     fit: np.ndarray  # (k, 3) fractions of each scan within EVAL_RADII of the map
     count: np.ndarray  # (k,) matched points in the last iteration
     iters: int  # iterations run (all stages)
-    tile: int  # points per CTA the launch used
+    tile: int  # points per warp tile the launch used
+    blocks_per_sm: int = 3  # the register budget the launch used
 
 
 class Autotuner:
-    """Chooses the tile size of the batched ICP per batch shape class: each candidate is timed once with CUDA
-    events on the caller's stream (the poses restored between trials) and the fastest is cached."""
+    """Chooses the launch shape (tile, blocks_per_sm) of the batched ICP per batch shape class: each candidate is
+    timed once with CUDA events on the caller's stream (the poses restored between trials) and the fastest is
+    cached."""
 
     def __init__(self, path: str | None = None):
         self.path = path if path is not None else os.environ.get("LW_AUTOTUNE_CACHE")
-        self.table: dict[str, int] = {}
+        self.table: dict[str, tuple[int, int]] = {}
         if self.path and os.path.exists(self.path):
             try:
                 with open(self.path) as f:
-                    self.table = {k: int(v) for k, v in json.load(f).items()}
-            except (OSError, ValueError):
+                    self.table = {k: (int(v[0]), int(v[1])) for k, v in json.load(f).items()}
+            except (OSError, ValueError, TypeError, IndexError):
                 self.table = {}
-        self.trials: dict[str, dict[int, float]] = {}
+        self.trials: dict[str, dict[tuple[int, int], float]] = {}
 
     @staticmethod
     def key(n_hyp: int, n_pts: int, schedule) -> str:
@@ -111,11 +116,11 @@ class Autotuner:
         sched = ",".join(f"{d:g}x{i}" for d, i in schedule)
         return f"h{1 << max(0, int(n_hyp - 1).bit_length())}-p{1 << max(0, int(mean - 1).bit_length())}-{sched}"
 
-    def choose(self, key: str, run) -> int:
-        """The cached tile for `key`, else time run(tile) -> ms for every candidate and keep the fastest."""
+    def choose(self, key: str, run) -> tuple[int, int]:
+        """The cached shape for `key`, else time run(shape) -> ms for every candidate and keep the fastest."""
         if key in self.table:
             return self.table[key]
-        times = {t: run(t) for t in TILES}
+        times = {c: run(c) for c in CANDIDATES}
         best = min(times, key=times.get)
         self.trials[key] = times
         self.table[key] = best
@@ -156,6 +161,7 @@ class LocBatch:
         self.h_T = torch.zeros((H, 16), dtype=torch.float64).pin_memory()
         self.tile_part = torch.zeros(NT * 32, dtype=torch.float64, device=d)
         self.moved = torch.zeros(self.ITERS_CAP, dtype=torch.int32, device=d)
+        self.next = torch.zeros(self.ITERS_CAP + 1, dtype=torch.int32, device=d)
         self.bar = torch.zeros(2, dtype=torch.int32, device=d)
         self.s = self._struct(dims=False)
         self.s_dims = self._struct(dims=True)
@@ -172,6 +178,7 @@ class LocBatch:
         b.T = _lib.ptr(self.T)
         b.tile_part = _lib.ptr(self.tile_part)
         b.moved = _lib.ptr(self.moved)
+        b.next = _lib.ptr(self.next)
         b.count = C.c_void_p(ob)
         b.eval = C.c_void_p(ob + 4 * self.o_ev)
         b.iters_run = C.c_void_p(ob + 4 * self.o_it)
@@ -226,12 +233,12 @@ class GlobalLocalizer:
 
     # ---- the launch ------------------------------------------------------------------------------
 
-    def _launch(self, n_hyp: int, n_tiles: int, tile: int, schedule, stream, dims: bool = False):
+    def _launch(self, n_hyp: int, n_tiles: int, tile: int, schedule, stream, dims: bool = False, minb: int = 3):
         b = self.batch
         dm = (_lib.f64 * max(1, len(schedule)))(*[float(d) for d, _ in schedule] or [0.0])
         it = (_lib.i32 * max(1, len(schedule)))(*[int(i) for _, i in schedule] or [0])
         _lib.call("lw_loc_icp_batch", C.byref(self.grid.struct), C.byref(b.s_dims if dims else b.s), int(n_hyp),
-                  int(n_tiles), int(tile), len(schedule), dm, it, ALPHA, MIN_COUNT, 0, _lib.stream_ptr(stream))
+                  int(n_tiles), int(tile), len(schedule), dm, it, ALPHA, MIN_COUNT, int(minb), 0, _lib.stream_ptr(stream))
 
     def _put_T(self, Ts, stream):
         b = self.batch
@@ -255,8 +262,9 @@ class GlobalLocalizer:
         ev = o[b.o_ev:b.o_ev + 3 * k].reshape(k, 3).copy()
         return T, count, ev, int(o[b.o_it])
 
-    def _run(self, lo, hi, Ts, schedule, stream, tile: int | None = None) -> BatchResult:
-        """ICP then evaluation of hypotheses h over points [lo[h], hi[h]) already in the batch's pts."""
+    def _run(self, lo, hi, Ts, schedule, stream, tile: int | None = None, minb: int | None = None) -> BatchResult:
+        """ICP then evaluation of hypotheses h over points [lo[h], hi[h]) already in the batch's pts. With tile
+        None the autotuner picks the launch shape; with tile given, minb None means the default budget (3)."""
         k = len(Ts)
         stream = stream if stream is not None else torch.cuda.current_stream(self.device)
         lo = np.asarray(lo, dtype=np.int64)
@@ -265,26 +273,28 @@ class GlobalLocalizer:
         if tile is None:
             key = Autotuner.key(k, n_pts, schedule)
 
-            def trial(t):
+            def trial(shape):
+                t, m = shape
                 nt = self.batch.stage(lo, hi, t, stream)
                 self._put_T(Ts, stream)
-                self._launch(k, nt, t, schedule, stream)  # warm
+                self._launch(k, nt, t, schedule, stream, minb=m)  # warm
                 self._put_T(Ts, stream)
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                self._launch(k, nt, t, schedule, stream)
+                self._launch(k, nt, t, schedule, stream, minb=m)
                 e1.record(stream)
                 e1.synchronize()
                 return e0.elapsed_time(e1)
 
-            tile = self.tuner.choose(key, trial)
+            tile, minb = self.tuner.choose(key, trial)
+        minb = 3 if minb is None else minb
         nt = self.batch.stage(lo, hi, tile, stream)
         self._put_T(Ts, stream)
-        self._launch(k, nt, tile, schedule, stream)
+        self._launch(k, nt, tile, schedule, stream, minb=minb)
         T, count, ev, iters = self._get(k, stream)
         self.last_tile = tile
         n_h = np.maximum(hi - lo, 1).astype(np.float64)
-        return BatchResult(T, ev / n_h[:, None], count, iters, tile)
+        return BatchResult(T, ev / n_h[:, None], count, iters, tile, minb)
 
     def _upload_pts(self, parts, stream) -> tuple[np.ndarray, np.ndarray]:
         """Pack point sets (each (n, 3) float32) one after another into the batch's pts; returns (lo, hi)."""
@@ -334,7 +344,8 @@ class GlobalLocalizer:
         self._upload_pts([pts], stream)
         k = len(inits)
         res = self._run(np.zeros(k, np.int64), np.full(k, n, np.int64), inits, schedule, stream)
-        start = self._run(np.zeros(1, np.int64), np.full(1, n, np.int64), [T0], (), stream, tile=res.tile)
+        start = self._run(np.zeros(1, np.int64), np.full(1, n, np.int64), [T0], (), stream, tile=res.tile,
+                          minb=res.blocks_per_sm)
         fits = res.fit
         best = 0
         for i in range(1, k):
@@ -362,17 +373,18 @@ class GlobalLocalizer:
 
     # ---- many hypotheses, uneven scans --------------------------------------------------------------
 
-    def register_batch(self, scans, T0s, schedule=SCHEDULE_ICP, stream=None, tile: int | None = None) -> BatchResult:
+    def register_batch(self, scans, T0s, schedule=SCHEDULE_ICP, stream=None, tile: int | None = None,
+                       blocks_per_sm: int | None = None) -> BatchResult:
         """Register hypothesis h's own scan (scans[h], (n_h, 3) float32 in the sensor frame) from T0s[h], all
         in one launch; returns the refined poses, their fits and the matched counts."""
         stream = stream if stream is not None else torch.cuda.current_stream(self.device)
         if len(scans) != len(T0s):
             raise ValueError("one scan per hypothesis")
         lo, hi = self._upload_pts([np.asarray(s, dtype=np.float32) for s in scans], stream)
-        return self._run(lo, hi, T0s, schedule, stream, tile)
+        return self._run(lo, hi, T0s, schedule, stream, tile, blocks_per_sm)
 
     def register_packed(self, pts4: torch.Tensor, lo, hi, T0s, schedule=SCHEDULE_ICP, stream=None,
-                        tile: int | None = None) -> BatchResult:
+                        tile: int | None = None, blocks_per_sm: int | None = None) -> BatchResult:
         """register_batch for scans already packed one after another in `pts4` ((N, 4) float32: x, y, z, unused;
         a pinned host tensor is copied asynchronously, a device tensor in place); hypothesis h owns rows
         lo[h] .. hi[h]."""
@@ -389,14 +401,14 @@ class GlobalLocalizer:
             raise ValueError("lo / hi must give each hypothesis a row range of pts4")
         with torch.cuda.stream(stream):
             b.pts[:n].copy_(pts4, non_blocking=True)
-        return self._run(lo, hi, T0s, schedule, stream, tile)
+        return self._run(lo, hi, T0s, schedule, stream, tile, blocks_per_sm)
 
-    def register_graph(self, lo, hi, schedule=SCHEDULE_ICP, tile: int = 256, stream=None):
+    def register_graph(self, lo, hi, schedule=SCHEDULE_ICP, tile: int = 256, stream=None, blocks_per_sm: int = 3):
         """A CUDA graph of the batched launch for the staged batch's shape class: the hypothesis and tile counts
         are read on the device (lw_loc_batch.dims), so one capture replays over any batch up to the buffers'
         capacity with that schedule and tile. Returns a callable that stages (lo, hi, T0s) and replays it."""
         stream = stream if stream is not None else torch.cuda.current_stream(self.device)
-        key = (tuple(schedule), tile)
+        key = (tuple(schedule), tile, blocks_per_sm)
         g = self._graphs.get(key)
         b = self.batch
         if g is None:
@@ -407,7 +419,7 @@ class GlobalLocalizer:
             cap = torch.cuda.Stream(self.device)
             cap.wait_stream(stream)
             with torch.cuda.graph(g, stream=cap, capture_error_mode="thread_local"):
-                self._launch(b.hyp_cap, b.tiles_cap, tile, schedule, cap, dims=True)
+                self._launch(b.hyp_cap, b.tiles_cap, tile, schedule, cap, dims=True, minb=blocks_per_sm)
             stream.wait_stream(cap)
             self._graphs[key] = g
 
@@ -418,6 +430,6 @@ class GlobalLocalizer:
                 g.replay()
             T, count, ev, iters = self._get(len(T0s), stream)
             n_h = np.maximum(np.asarray(hi) - np.asarray(lo), 1).astype(np.float64)
-            return BatchResult(T, ev / n_h[:, None], count, iters, tile)
+            return BatchResult(T, ev / n_h[:, None], count, iters, tile, blocks_per_sm)
 
         return replay

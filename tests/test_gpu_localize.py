@@ -99,14 +99,14 @@ def _oracle_batch(og, scans, T0, schedule):
     return T, count, iters, ev
 
 
-@pytest.mark.parametrize("tile", [128, 256, 512])
-def test_batch_uneven_scans_match_oracle(room, tile):
+@pytest.mark.parametrize("tile,minb", [(64, 3), (128, 2), (512, 3)])
+def test_batch_uneven_scans_match_oracle(room, tile, minb):
     from livox_warp.localize import SCHEDULE_ICP, GlobalLocalizer
 
     sc, grid, og = room
     T_true, T0, scans = _hypotheses(sc, 12, 40)
     loc = GlobalLocalizer(grid, hyp_cap=64, pts_cap=1 << 19)
-    res = loc.register_batch(scans, T0, SCHEDULE_ICP, tile=tile)
+    res = loc.register_batch(scans, T0, SCHEDULE_ICP, tile=tile, blocks_per_sm=minb)
     oT, ocount, oiters, oev = _oracle_batch(og, scans, T0, SCHEDULE_ICP)
     assert abs(res.iters - oiters) <= 1
     for h in range(len(scans)):
@@ -211,9 +211,11 @@ def test_argument_errors(room):
     sc, grid, og = room
     loc = GlobalLocalizer(grid, hyp_cap=8, pts_cap=1 << 17)
     with pytest.raises(_lib.LwError):
-        loc._launch(1, 1, 384, ((0.1, 2),), torch.cuda.current_stream())  # tile must be 128/256/512
+        loc._launch(1, 1, 100, ((0.1, 2),), torch.cuda.current_stream())  # tile must be a multiple of 32
     with pytest.raises(_lib.LwError):
         loc._launch(1, 1, 256, ((0.1, 200), (0.1, 200)), torch.cuda.current_stream())  # > moved_cap iterations
+    with pytest.raises(_lib.LwError):
+        loc._launch(1, 1, 256, ((0.1, 2),), torch.cuda.current_stream(), minb=5)  # register budget 2 or 3
     with pytest.raises(ValueError):
         loc.register_batch([np.zeros((10, 3), np.float32)] * 9, np.tile(np.eye(4), (9, 1, 1)))
     with pytest.raises(RuntimeError):
