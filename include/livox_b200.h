@@ -391,7 +391,7 @@ typedef struct lw_loc_batch {
  * hypothesis with fewer than min_count matches keeps its pose; a stage ends when no hypothesis moved 2e-4
  * (n_stages = 0 only evaluates). With b->dims set, n_hyp and n_tiles are capacities and the counts are read on
  * the device. tile: points per tile (a multiple of 32 up to 2048), each tile worked by one warp; the host's tiling
- * must use the same value. blocks_per_sm: the register budget, 2 or 3 resident 256-thread CTAs per SM (0 = 3).
+ * must use the same value. blocks_per_sm: the register budget, 2 to 6 resident 256-thread CTAs per SM (0 = 3).
  * grid <= 0 picks one full wave. */
 int lw_loc_icp_batch(const lw_prior_grid* g, lw_loc_batch* b, int32_t n_hyp, int32_t n_tiles, int32_t tile,
                      int32_t n_stages, const double* dmax, const int32_t* iters, float alpha, int32_t min_count,

@@ -253,7 +253,9 @@ __device__ __forceinline__ void tile_range(const lw_loc_batch& b, int tile, int 
     hi = (int)min((int64_t)__ldg(b.scan_end + h), b.pts_cap);
 }
 
-// One (hypothesis, point) pair's terms (localize.py:144-167) into a[LTERMS].
+// One (hypothesis, point) pair's terms (localize.py:144-167) added to a[k * S], k < LTERMS (S = 1: registers;
+// S = 32: a warp's per-lane columns in shared memory).
+template <int S>
 __device__ __forceinline__ void loc_terms(const lw_prior_grid& g, const LocPose& P, float4 p, float max_d2, float c2,
                                           float alpha, float* a) {
     float lx = P.R[0] * p.x + P.R[1] * p.y + P.R[2] * p.z + P.tr[0];
@@ -309,17 +311,102 @@ __device__ __forceinline__ void loc_terms(const lw_prior_grid& g, const LocPose&
                 h = MA[pp][qq - 3];
             else
                 h = fmaf(A[0][pp - 3], MA[0][qq - 3], fmaf(A[1][pp - 3], MA[1][qq - 3], A[2][pp - 3] * MA[2][qq - 3]));
-            a[idx] = fmaf(wgt, h, a[idx]);
+            a[idx * S] = fmaf(wgt, h, a[idx * S]);
             ++idx;
         }
-    a[21] = fmaf(wgt, Mr0, a[21]);
-    a[22] = fmaf(wgt, Mr1, a[22]);
-    a[23] = fmaf(wgt, Mr2, a[23]);
+    a[21 * S] = fmaf(wgt, Mr0, a[21 * S]);
+    a[22 * S] = fmaf(wgt, Mr1, a[22 * S]);
+    a[23 * S] = fmaf(wgt, Mr2, a[23 * S]);
 #pragma unroll
-    for (int j = 0; j < 3; ++j) a[24 + j] = fmaf(wgt, fmaf(A[0][j], Mr0, fmaf(A[1][j], Mr1, A[2][j] * Mr2)), a[24 + j]);
-    a[27] += 1.0f;
-    a[28] = fmaf(wgt, d2, a[28]);
-    a[29] += wgt;
+    for (int j = 0; j < 3; ++j)
+        a[(24 + j) * S] = fmaf(wgt, fmaf(A[0][j], Mr0, fmaf(A[1][j], Mr1, A[2][j] * Mr2)), a[(24 + j) * S]);
+    a[27 * S] += 1.0f;
+    a[28 * S] = fmaf(wgt, d2, a[28 * S]);
+    a[29 * S] += wgt;
+}
+
+// The float64 step of hypothesis h from its summed terms sv (localize.py:537-550) applied to its pose; returns
+// the step's size max(|dt|, 5 |dr|), 0 when it is skipped. Kept out of line: it runs on one thread per
+// hypothesis per iteration, and inlined its arrays would set the register budget of the whole kernel.
+__device__ __noinline__ double loc_solve(const double* sv, double* Th, int min_count) {
+    double moved = 0.0;
+    if (sv[27] >= (double)min_count) {
+        // re-centred sums -> the twist about the world origin: H = A^T Hc A, b = A^T bc
+        double c[3] = {(double)(float)__ldcg(Th + 3), (double)(float)__ldcg(Th + 7),
+                       (double)(float)__ldcg(Th + 11)};
+        double Hc[36], H[36], bc[6], bw[6];
+        int idx = 0;
+        for (int p = 0; p < 6; ++p)
+            for (int q = p; q < 6; ++q) {
+                Hc[p * 6 + q] = Hc[q * 6 + p] = sv[idx];
+                ++idx;
+            }
+        for (int p = 0; p < 6; ++p) bc[p] = sv[21 + p];
+        const double K[9] = {0.0, c[2], -c[1], -c[2], 0.0, c[0], c[1], -c[0], 0.0};
+        double HA[36];
+        for (int p = 0; p < 6; ++p)
+            for (int q = 0; q < 6; ++q) {
+                double x = Hc[p * 6 + q];
+                if (q >= 3)
+                    for (int k = 0; k < 3; ++k) x += Hc[p * 6 + k] * K[k * 3 + q - 3];
+                HA[p * 6 + q] = x;
+            }
+        for (int p = 0; p < 6; ++p) {
+            for (int q = 0; q < 6; ++q) {
+                double x = HA[p * 6 + q];
+                if (p >= 3)
+                    for (int k = 0; k < 3; ++k) x += K[k * 3 + p - 3] * HA[k * 6 + q];
+                H[p * 6 + q] = x;
+            }
+            double x = bc[p];
+            if (p >= 3)
+                for (int k = 0; k < 3; ++k) x += K[k * 3 + p - 3] * bc[k];
+            bw[p] = x;
+        }
+        // A = H + diag(1e-3 dg + 1e-9), delta = solve(A, -b)
+        double Lf[36], rhs[6], delta[6];
+        for (int p = 0; p < 6; ++p) {
+            H[p * 7] += 1e-3 * H[p * 7] + 1e-9;
+            rhs[p] = -bw[p];
+        }
+        bool ok = true;
+        for (int j = 0; j < 6 && ok; ++j) {
+            double d = H[j * 6 + j];
+            for (int k = 0; k < j; ++k) d -= Lf[j * 6 + k] * Lf[j * 6 + k];
+            if (!(d > 0.0)) {
+                ok = false;
+                break;
+            }
+            d = sqrt(d);
+            Lf[j * 6 + j] = d;
+            for (int r = j + 1; r < 6; ++r) {
+                double x = H[r * 6 + j];
+                for (int k = 0; k < j; ++k) x -= Lf[r * 6 + k] * Lf[j * 6 + k];
+                Lf[r * 6 + j] = x / d;
+            }
+        }
+        if (ok) {
+            double y[6];
+            for (int r = 0; r < 6; ++r) {
+                double s = rhs[r];
+                for (int k = 0; k < r; ++k) s -= Lf[r * 6 + k] * y[k];
+                y[r] = s / Lf[r * 6 + r];
+            }
+            for (int r = 5; r >= 0; --r) {
+                double s = y[r];
+                for (int k = r + 1; k < 6; ++k) s -= Lf[k * 6 + r] * delta[k];
+                delta[r] = s / Lf[r * 6 + r];
+            }
+            double T[16];
+            for (int k = 0; k < 16; ++k) T[k] = __ldcg(Th + k);
+            apply_twist(T, delta);
+            for (int k = 0; k < 16; ++k) Th[k] = T[k];
+            double nt = sqrt(delta[0] * delta[0] + delta[1] * delta[1] + delta[2] * delta[2]);
+            double nr = sqrt(delta[3] * delta[3] + delta[4] * delta[4] + delta[5] * delta[5]);
+            moved = fmax(nt, 5.0 * nr);
+        }
+    }
+    return moved;
 }
 
 struct LocArgs {
@@ -359,11 +446,16 @@ __device__ __forceinline__ int next_tile(const lw_loc_batch& b, int pass, int la
     return __shfl_sync(FULL, t, 0);
 }
 
-// MINB: CTAs of LOC_BLOCK threads the register budget must let reside per SM -- 2 (up to 128 registers, no
-// spills) or 3 (80 registers, a few spilled words, half again as many warps to hide the gathers' latency).
+// MINB: CTAs of LOC_BLOCK threads the register budget must let reside per SM. With 2 or 3 the per-lane term
+// sums of a tile and the tile's pose live in registers; with 4 to 6 they live in shared memory (a [30][32]
+// column block and one pose per warp, 31 KB per CTA), which frees ~47 registers across the nearest-point search
+// so that two to three times the 2-CTA warp count stays resident.
 template <int MINB>
 __global__ void __launch_bounds__(LOC_BLOCK, MINB)
     k_loc_icp(lw_prior_grid g, lw_loc_batch b, LocArgs la) {
+    constexpr bool SMEM_ACC = MINB >= 4;
+    __shared__ float s_acc[SMEM_ACC ? LOC_BLOCK / 32 : 1][SMEM_ACC ? LTERMS : 1][32];
+    __shared__ LocPose s_pose[SMEM_ACC ? LOC_BLOCK / 32 : 1];
     __shared__ double sv[32];
     __shared__ int s_stop;
     const int tid = threadIdx.x;
@@ -386,11 +478,28 @@ __global__ void __launch_bounds__(LOC_BLOCK, MINB)
 #pragma unroll
                 for (int k = 0; k < 32; ++k) v[k] = 0.0f;
                 if (h >= 0) {
-                    LocPose P;
-                    loc_pose(b.T + 16 * h, P);
+                    // the tile's pose is the same for the whole warp: with SMEM_ACC it is kept in shared memory
+                    // (broadcast reads) instead of 15 registers per lane
+                    LocPose Pr;
+                    LocPose& P = SMEM_ACC ? s_pose[tid >> 5] : Pr;
+                    if (!SMEM_ACC || lane == 0) loc_pose(b.T + 16 * h, P);
+                    __syncwarp();
                     const int end = min(hi, lo + la.tile);
-                    for (int i = lo + lane; i < end; i += 32)
-                        loc_terms(g, P, __ldg(reinterpret_cast<const float4*>(b.pts) + i), max_d2, c2, la.alpha, v);
+                    if constexpr (SMEM_ACC) {
+                        float* col = &s_acc[tid >> 5][0][lane];
+#pragma unroll
+                        for (int k = 0; k < LTERMS; ++k) col[k * 32] = 0.0f;
+                        for (int i = lo + lane; i < end; i += 32)
+                            loc_terms<32>(g, P, __ldg(reinterpret_cast<const float4*>(b.pts) + i), max_d2, c2,
+                                          la.alpha, col);
+#pragma unroll
+                        for (int k = 0; k < LTERMS; ++k) v[k] = col[k * 32];
+                        __syncwarp();  // the pose slot is rewritten by the warp's next tile
+                    } else {
+                        for (int i = lo + lane; i < end; i += 32)
+                            loc_terms<1>(g, P, __ldg(reinterpret_cast<const float4*>(b.pts) + i), max_d2, c2,
+                                         la.alpha, v);
+                    }
                 }
                 const float sum = warp_reduce_scatter32(v, lane);
                 if (lane < LTERMS) b.tile_part[(int64_t)tile * 32 + lane] = (double)sum;
@@ -406,84 +515,8 @@ __global__ void __launch_bounds__(LOC_BLOCK, MINB)
                 }
                 __syncthreads();
                 if (tid == 0) {
-                    double moved = 0.0;
                     b.count[h] = (int)sv[27];
-                    if (sv[27] >= (double)la.min_count) {
-                        // re-centred sums -> the twist about the world origin: H = A^T Hc A, b = A^T bc
-                        double c[3] = {(double)(float)__ldcg(b.T + 16 * h + 3), (double)(float)__ldcg(b.T + 16 * h + 7),
-                                       (double)(float)__ldcg(b.T + 16 * h + 11)};
-                        double Hc[36], H[36], bc[6], bw[6];
-                        int idx = 0;
-                        for (int p = 0; p < 6; ++p)
-                            for (int q = p; q < 6; ++q) {
-                                Hc[p * 6 + q] = Hc[q * 6 + p] = sv[idx];
-                                ++idx;
-                            }
-                        for (int p = 0; p < 6; ++p) bc[p] = sv[21 + p];
-                        const double K[9] = {0.0, c[2], -c[1], -c[2], 0.0, c[0], c[1], -c[0], 0.0};
-                        double HA[36];
-                        for (int p = 0; p < 6; ++p)
-                            for (int q = 0; q < 6; ++q) {
-                                double x = Hc[p * 6 + q];
-                                if (q >= 3)
-                                    for (int k = 0; k < 3; ++k) x += Hc[p * 6 + k] * K[k * 3 + q - 3];
-                                HA[p * 6 + q] = x;
-                            }
-                        for (int p = 0; p < 6; ++p) {
-                            for (int q = 0; q < 6; ++q) {
-                                double x = HA[p * 6 + q];
-                                if (p >= 3)
-                                    for (int k = 0; k < 3; ++k) x += K[k * 3 + p - 3] * HA[k * 6 + q];
-                                H[p * 6 + q] = x;
-                            }
-                            double x = bc[p];
-                            if (p >= 3)
-                                for (int k = 0; k < 3; ++k) x += K[k * 3 + p - 3] * bc[k];
-                            bw[p] = x;
-                        }
-                        // A = H + diag(1e-3 dg + 1e-9), delta = solve(A, -b)
-                        double Lf[36], rhs[6], delta[6];
-                        for (int p = 0; p < 6; ++p) {
-                            H[p * 7] += 1e-3 * H[p * 7] + 1e-9;
-                            rhs[p] = -bw[p];
-                        }
-                        bool ok = true;
-                        for (int j = 0; j < 6 && ok; ++j) {
-                            double d = H[j * 6 + j];
-                            for (int k = 0; k < j; ++k) d -= Lf[j * 6 + k] * Lf[j * 6 + k];
-                            if (!(d > 0.0)) {
-                                ok = false;
-                                break;
-                            }
-                            d = sqrt(d);
-                            Lf[j * 6 + j] = d;
-                            for (int r = j + 1; r < 6; ++r) {
-                                double x = H[r * 6 + j];
-                                for (int k = 0; k < j; ++k) x -= Lf[r * 6 + k] * Lf[j * 6 + k];
-                                Lf[r * 6 + j] = x / d;
-                            }
-                        }
-                        if (ok) {
-                            double y[6];
-                            for (int r = 0; r < 6; ++r) {
-                                double s = rhs[r];
-                                for (int k = 0; k < r; ++k) s -= Lf[r * 6 + k] * y[k];
-                                y[r] = s / Lf[r * 6 + r];
-                            }
-                            for (int r = 5; r >= 0; --r) {
-                                double s = y[r];
-                                for (int k = r + 1; k < 6; ++k) s -= Lf[k * 6 + r] * delta[k];
-                                delta[r] = s / Lf[r * 6 + r];
-                            }
-                            double T[16];
-                            for (int k = 0; k < 16; ++k) T[k] = __ldcg(b.T + 16 * h + k);
-                            apply_twist(T, delta);
-                            for (int k = 0; k < 16; ++k) b.T[16 * h + k] = T[k];
-                            double nt = sqrt(delta[0] * delta[0] + delta[1] * delta[1] + delta[2] * delta[2]);
-                            double nr = sqrt(delta[3] * delta[3] + delta[4] * delta[4] + delta[5] * delta[5]);
-                            moved = fmax(nt, 5.0 * nr);
-                        }
-                    }
+                    const double moved = loc_solve(sv, b.T + 16 * h, la.min_count);
                     // the largest step of the iteration, as ordered bits of a non-negative float
                     atomicMax(b.moved + it_total, __float_as_int((float)moved));
                 }
@@ -638,9 +671,13 @@ int lw_loc_icp_batch(const lw_prior_grid* g, lw_loc_batch* b, int32_t n_hyp, int
     cudaStream_t s = (cudaStream_t)stream;
     int sms = device_sms();
     if (blocks_per_sm == 0) blocks_per_sm = 3;
-    if (blocks_per_sm != 2 && blocks_per_sm != 3)
-        return set_error(LW_EINVAL, "lw_loc_icp_batch: blocks_per_sm must be 0, 2 or 3");
-    const void* fn = blocks_per_sm == 2 ? (const void*)k_loc_icp<2> : (const void*)k_loc_icp<3>;
+    if (blocks_per_sm < 2 || blocks_per_sm > 6)
+        return set_error(LW_EINVAL, "lw_loc_icp_batch: blocks_per_sm must be 0 or 2..6");
+    const void* fn = blocks_per_sm == 2   ? (const void*)k_loc_icp<2>
+                     : blocks_per_sm == 3 ? (const void*)k_loc_icp<3>
+                     : blocks_per_sm == 4 ? (const void*)k_loc_icp<4>
+                     : blocks_per_sm == 5 ? (const void*)k_loc_icp<5>
+                                          : (const void*)k_loc_icp<6>;
     int per_sm = 0;
     LW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, LOC_BLOCK, 0));
     if (per_sm < 1) return set_error(LW_EINVAL, "lw_loc_icp_batch: the kernel does not fit on an SM");
@@ -661,10 +698,13 @@ int lw_loc_icp_batch(const lw_prior_grid* g, lw_loc_batch* b, int32_t n_hyp, int
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (blocks_per_sm == 2)
-        LW_CUDA(cudaLaunchKernelEx(&cfg, k_loc_icp<2>, *g, *b, la));
-    else
-        LW_CUDA(cudaLaunchKernelEx(&cfg, k_loc_icp<3>, *g, *b, la));
+    switch (blocks_per_sm) {
+        case 2: LW_CUDA(cudaLaunchKernelEx(&cfg, k_loc_icp<2>, *g, *b, la)); break;
+        case 3: LW_CUDA(cudaLaunchKernelEx(&cfg, k_loc_icp<3>, *g, *b, la)); break;
+        case 4: LW_CUDA(cudaLaunchKernelEx(&cfg, k_loc_icp<4>, *g, *b, la)); break;
+        case 5: LW_CUDA(cudaLaunchKernelEx(&cfg, k_loc_icp<5>, *g, *b, la)); break;
+        default: LW_CUDA(cudaLaunchKernelEx(&cfg, k_loc_icp<6>, *g, *b, la)); break;
+    }
     LW_LAUNCHED("lw_loc_icp_batch");
     count_launches(2);
     return LW_OK;

@@ -12,8 +12,8 @@ Precision: the residuals and Jacobians run in float32 on points re-centred on th
 tile sums, the normal equations, the Cholesky solve and the poses are float64 (the reference sends float32
 poses to the device and solves with numpy in float64).
 
-The launch shape -- points per warp tile (64, 128, 256 or 512) and the register budget (2 or 3 resident
-256-thread CTAs per SM) -- is chosen by `Autotuner`, which times the candidates once per batch shape class and
+The launch shape -- points per warp tile (32, 64 or 128) and the register budget (3 to 6 resident 256-thread
+CTAs per SM) -- is chosen by `Autotuner`, which times the candidates once per batch shape class and
 caches the winner (in memory, and in a JSON file when LW_AUTOTUNE_CACHE names one).
 """
 
@@ -37,8 +37,8 @@ SCHEDULE_ICP = ((0.40, 8), (0.20, 8), (0.10, 8), (0.05, 10))  # GlobalLocalizer.
 SCHEDULE_REFINE = ((0.30, 6), (0.12, 8), (0.05, 8))  # GlobalLocalizer.refine default, localize.py:569
 ALPHA = 0.05  # along-surface weight of a planar correspondence, localize.py:523
 MIN_COUNT = 30  # matches below which a hypothesis keeps its pose, localize.py:538
-TILES = (64, 128, 256, 512)  # points per warp tile the autotuner tries
-BUDGETS = (2, 3)  # resident CTAs per SM the kernel's register budget is compiled for
+TILES = (32, 64, 128)  # points per warp tile the autotuner tries
+BUDGETS = (3, 4, 5, 6)  # resident CTAs per SM of the register budgets it tries (the library also has 2)
 CANDIDATES = tuple((t, m) for t in TILES for m in BUDGETS)
 
 

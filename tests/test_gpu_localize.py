@@ -99,7 +99,7 @@ def _oracle_batch(og, scans, T0, schedule):
     return T, count, iters, ev
 
 
-@pytest.mark.parametrize("tile,minb", [(64, 3), (128, 2), (512, 3)])
+@pytest.mark.parametrize("tile,minb", [(32, 6), (32, 4), (64, 5), (128, 2), (512, 3)])
 def test_batch_uneven_scans_match_oracle(room, tile, minb):
     from livox_warp.localize import SCHEDULE_ICP, GlobalLocalizer
 
@@ -215,7 +215,7 @@ def test_argument_errors(room):
     with pytest.raises(_lib.LwError):
         loc._launch(1, 1, 256, ((0.1, 200), (0.1, 200)), torch.cuda.current_stream())  # > moved_cap iterations
     with pytest.raises(_lib.LwError):
-        loc._launch(1, 1, 256, ((0.1, 2),), torch.cuda.current_stream(), minb=5)  # register budget 2 or 3
+        loc._launch(1, 1, 256, ((0.1, 2),), torch.cuda.current_stream(), minb=7)  # register budget 2..6
     with pytest.raises(ValueError):
         loc.register_batch([np.zeros((10, 3), np.float32)] * 9, np.tile(np.eye(4), (9, 1, 1)))
     with pytest.raises(RuntimeError):
