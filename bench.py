@@ -18,6 +18,12 @@ the 0.1 m integration map (2^22 slots) and free-space carving of every ray.
 
 `--impl reference` times the reference's CPU implementation of the path instead: NVIDIA Warp (the reference's
 only runtime) is not installed, so that arm runs the CPU restatement, on every host core.
+`--workload frame` measures the full perception frame: a dual-return rosette (100k rays/s, two returns each: ~20k
+points per frame) on a handheld path through a seeded 40 x 30 x 3 m office with 10 walkers (r 0.25 m, h 1.8 m,
+1.2 m/s); per frame deskew + Gauss-Newton ICP + keyframe insert, integration-map insert and carving of every ray
+(walker ghosts), the map's visible set, the 0.5 m ground grid (slope allowance 0.3) and clusters of the non-ground
+points at 0.2 m voxels (connect 0.35 m, 30 points), read back to the host; latency p50 / p99 per frame.
+
 `--workload localize` measures the batched global localisation instead: a 20.3M-point prior map sampled every
 15 mm on the surfaces of a seeded 40 x 30 x 3 m office (walls with doors, 200 boxes), 256 hypotheses, each with
 its own static 360-degree scan of U[2k, 20k] points taken at a free pose (z = 1.2 m, yaw uniform), started from
@@ -64,6 +70,9 @@ LOC_HYP = 256
 LOC_PTS = (2000, 20000)
 LOC_Z = 1.2
 LOC_POSE_SEED = 11
+FRAME_SCENE_SEED = 4   # the office with walkers
+FRAME_PATH_SEED = 5
+FRAME_RAYS = 100000.0  # rays/s; two returns each
 
 
 # ---- workload --------------------------------------------------------------------------------------------------
@@ -355,6 +364,185 @@ def _oracle_view(oracle):
     return v
 
 
+# ---- full perception frame --------------------------------------------------------------------------------------
+
+
+def _frame_chunk(args):
+    from livox_warp import synth
+
+    duration, k0, k1 = args
+    scene = synth.office(FRAME_SCENE_SEED, walkers=10)
+    traj = synth.Handheld(scene, FRAME_PATH_SEED, duration)
+    return synth.frames(scene, traj, k1 - k0, FRAME_RAYS, SCAN_SEED, start=k0, dual=True)
+
+
+def frame_workload(n_frames: int, procs: int | None = None):
+    from livox_warp import synth
+
+    duration = n_frames * FRAME_DT + 2.0
+    procs = procs or min(8, os.cpu_count() or 1)
+    step = max(1, math.ceil(n_frames / (procs * 4)))
+    chunks = [(duration, k, min(k + step, n_frames)) for k in range(0, n_frames, step)]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        parts = pool.map(_frame_chunk, chunks)
+    scene = synth.office(FRAME_SCENE_SEED, walkers=10)
+    return [f for p in parts for f in p], synth.Handheld(scene, FRAME_PATH_SEED, duration)
+
+
+FRAME_GROUND = dict(cell=0.5, thick=0.15, min_sup=3, thresh=0.2, slope_step=0.3)
+FRAME_CLUSTER = dict(voxel=0.2, connect=0.35, min_pts=30)
+
+
+def cpu_frame_pipeline(frames, traj, warmup: int, budget_s: float, max_frames: int, threads: int):
+    """The oracle's full frame (odometry, insert, carve, visible set, ground, clusters); frames after `warmup`
+    are timed until max_frames or budget_s. Returns (frames timed, seconds)."""
+    os.environ["LW_ORACLE_THREADS"] = str(threads)
+    from oracle import oracle
+
+    p = oracle.Params(reg_voxel=REG_VOXEL)
+    od = oracle.Odometry(REG_SLOTS, p, traj.poses(np.array([0.5 * FRAME_DT]))[0])
+    om = oracle.Map(MAP_SLOTS)
+    poses = np.tile(np.eye(4, dtype=np.float32).reshape(1, 16), (oracle.POSE_SLOTS, 1))
+    view = _oracle_view(oracle)
+    view.carve_on = 1
+    timed, total = 0, 0.0
+    for k, (x, a, t) in enumerate(frames):
+        t0 = time.perf_counter()
+        raw = np.ascontiguousarray(np.concatenate([x, t[:, None]], 1), dtype=np.float32)
+        T, xyz4, ok = od.frame(k, raw, a)
+        poses[k & (oracle.POSE_SLOTS - 1)] = T.astype(np.float32).reshape(16)
+        fid = np.full(len(t), k, np.int32)
+        om.insert(xyz4, a, t, fid, poses, view, MAP_VOXEL)
+        om.carve(xyz4, a, fid, poses, MAP_VOXEL, every=1, nthreads=threads)
+        view.now = (k + 1) * FRAME_DT
+        vis = om.build(view)[0]
+        gnd, _ = oracle.ground(vis, **FRAME_GROUND)
+        oracle.cluster(vis, gnd, **FRAME_CLUSTER)
+        dt = time.perf_counter() - t0
+        if k >= warmup:
+            timed += 1
+            total += dt
+            if timed >= max_frames or total >= budget_s:
+                break
+    return timed, total
+
+
+def run_frame(a, rank: int, world: int, local: int):
+    n_frames = a.warmup + a.steps + 1
+    frames, traj = frame_workload(n_frames)
+    metric = "full perception frame latency p50 (stage + odometry + insert + carve + visible set + ground + clusters)"
+    config = {"workload": "full perception frame: office 40x30x3 m, 10 walkers (r 0.25 m, h 1.8 m, 1.2 m/s), "
+                          "dual-return rosette 100k rays/s (~20k pts/frame), handheld path, reg voxel 0.15 m, map voxel "
+                          "0.1 m (2^22 slots) with carving, ground 0.5 m slope 0.3, clusters 0.2 m connect 0.35 m",
+              "frames": n_frames, "points_per_frame": int(np.mean([len(f[2]) for f in frames])),
+              "l2": "not flushed: each frame's latency is measured as the pipeline runs",
+              "parallelism": f"replicas x{a.gpus}"}
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import oracle as _o
+
+        threads = _o.host_cores()
+        timed, secs = cpu_frame_pipeline(frames, traj, a.warmup, max(20.0, min(120.0, 0.2 * a.steps)), a.steps,
+                                         threads)
+        ms = 1e3 * secs / max(timed, 1)
+        print(json.dumps({"impl": "reference", "metric": metric, "value": round(ms, 3), "unit": "ms",
+                          "n_gpus": a.gpus, "steps": timed, "warmup": a.warmup, "ms_per_step": round(ms, 3),
+                          "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
+                          "data": "synthetic", "config": config,
+                          "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": threads, "kind": "port",
+                                           "sample": f"{timed} frames after {a.warmup} untimed, CPU restatement"},
+                          "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+    import torch
+
+    from livox_warp import _lib, gpu
+    from livox_warp.odom import Odometry
+    from livox_warp.perception import Perception
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    pipe = gpu.Pipeline(ring_capacity=1 << 16, map_capacity=MAP_SLOTS, device=device)
+    odom = Odometry(pipe, reg_slots=REG_SLOTS, frame_cap=FRAME_CAP)
+    odom.reg_voxel = REG_VOXEL
+    view = gpu.make_view(now=0.0, voxel=MAP_VOXEL, map_cap=MAP_SLOTS, carve_on=1)
+    odom.integrate(view, MAP_VOXEL, carve_every=1)
+    perc = Perception(pipe, cluster_slots=1 << 20)
+    odom.reset(traj.poses(np.array([0.5 * FRAME_DT]))[0])
+    stream = torch.cuda.current_stream(device)
+    lat_host, lat_dev, n_clusters = [], [], []
+
+    def step(k):
+        x, at, t = frames[k]
+        sx, sa, st, sf = pipe.stage(x, at, t, len(t), 1.0 / FRAME_DT)
+        odom.push(sx, sa, st, len(t), float(t.min()), float(t.max()))  # completes frame k - 1
+        view.now = (k + 1) * FRAME_DT
+        pipe.build(view, map_on=True)
+        perc.ground(**FRAME_GROUND)
+        return perc.cluster(**FRAME_CLUSTER)  # read back to the host
+
+    for k in range(a.warmup):
+        step(k)
+    torch.cuda.synchronize(device)
+    clocks = Clocks(local)
+    clocks.start()
+    _lib.launches(reset=True)
+    h2d = d2h = 0
+    for j in range(a.steps):
+        k = a.warmup + j
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        cl = step(k)
+        e1.record(stream)
+        e1.synchronize()
+        lat_host.append((time.perf_counter() - t0) * 1e3)
+        lat_dev.append(e0.elapsed_time(e1))
+        n_clusters.append(len(cl))
+        h2d += len(frames[k][2]) * 20
+        d2h += 12 + len(cl) * 40 + 12
+    clk = clocks.stop()
+    launches = _lib.launches()
+    if rank != 0:
+        return
+    # parity of the last frame's labels: the oracle's ground and clusters on the same visible set
+    from oracle import oracle as _o
+
+    n = pipe.count
+    vis = pipe.c_xyz[:n].cpu().numpy()
+    og, _ = _o.ground(vis, **FRAME_GROUND)
+    ocid, _, ocl, _ = _o.cluster(vis, og, **FRAME_CLUSTER)
+    gnd_ok = bool(np.array_equal(pipe.gnd[:n].cpu().numpy(), og))
+    cid_ok = bool(np.array_equal(pipe.cid[:n].cpu().numpy(), ocid)) and len(ocl) == len(cl)
+    threads = _o.host_cores()
+    timed, secs = cpu_frame_pipeline(frames, traj, a.warmup, a.cpu_budget, max(3, min(40, a.steps)), threads)
+    lh, ld = np.array(lat_host), np.array(lat_dev)
+    recs = odom.traj
+    from livox_warp.localize import pose_difference
+
+    gt = np.array([pose_difference(traj.poses(np.array([tm]))[0], T) for _, tm, T in recs])
+    line = {"metric": metric, "value": round(float(np.percentile(lh, 50)), 4), "unit": "ms", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(float(lh.mean()), 4),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 solve)",
+            "data": "synthetic", "config": config,
+            "latency_ms": {"p50": round(float(np.percentile(lh, 50)), 4), "p99": round(float(np.percentile(lh, 99)), 4),
+                           "max": round(float(lh.max()), 4), "device_p50": round(float(np.percentile(ld, 50)), 4),
+                           "device_p99": round(float(np.percentile(ld, 99)), 4)},
+            "frames_per_s": round(1e3 * a.steps / float(lh.sum()), 3),
+            "visible_points_last": int(n), "clusters_mean": round(float(np.mean(n_clusters)), 2),
+            "labels_bit_exact_last_frame": {"gnd": gnd_ok, "cid": cid_ok},
+            "pose_vs_gt": {"rmse_m": round(float(np.sqrt((gt[:, 0] ** 2).mean())), 4),
+                           "max_m": round(float(gt[:, 0].max()), 4), "max_deg": round(float(gt[:, 1].max()), 3)},
+            "cpu_baseline": {"value": round(1e3 * secs / max(timed, 1), 3), "unit": "ms", "cores": threads,
+                             "kind": "port", "sample": f"{timed} frames of the same sequence through the CPU oracle "
+                                                       f"(odometry, insert, carve, visible set, ground, clusters)"},
+            "e2e": {"value": round(float(np.percentile(lh, 50)), 4), "unit": "ms",
+                    "h2d_bytes_per_step": int(h2d / a.steps), "d2h_bytes_per_step": int(d2h / a.steps)},
+            "gpu_launches": int(launches), "clocks": clk}
+    print(json.dumps(line))
+
+
 # ---- batched global localisation -----------------------------------------------------------------------------------
 
 
@@ -589,7 +777,7 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=("sequence", "localize"), default="sequence")
+    ap.add_argument("--workload", choices=("sequence", "localize", "frame"), default="sequence")
     ap.add_argument("--loc-hyp", type=int, default=256, help="localize: hypotheses (a smaller profiling case)")
     ap.add_argument("--loc-spacing", type=float, default=0.015, help="localize: prior-map sample spacing (m)")
     a = ap.parse_args()
@@ -601,6 +789,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.workload == "localize":
         run_localize(a, rank, world, local)
+        return
+    if a.workload == "frame":
+        run_frame(a, rank, world, local)
         return
     n_frames = a.warmup + a.steps + 1
     metric = "ICP sequence odometry frames/s (deskew + GN ICP + keyframe insert + map insert + carve)"
