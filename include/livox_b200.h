@@ -118,6 +118,7 @@ typedef struct lw_odom_state {
     int32_t run_reg, do_insert, redo, err;
     int32_t iters, corr, degen, weak;
     int32_t frames, skipped, keyframes, traj_len;
+    int32_t iters_first, pad_; /* Gauss-Newton iterations of the frame's first registration (from the prediction) */
 } lw_odom_state;
 
 /* One finalised frame in the device trajectory log. */
@@ -125,6 +126,7 @@ typedef struct lw_traj_rec {
     double T[16];
     double t_mid;
     int32_t k, ok, iters, corr;
+    int32_t iters_first, pad_; /* iterations of the first registration; iters is the last one's */
 } lw_traj_rec;
 
 /* Frame buffers owned by Odometry (odom.py:476-490). */
@@ -396,6 +398,108 @@ typedef struct lw_loc_batch {
 int lw_loc_icp_batch(const lw_prior_grid* g, lw_loc_batch* b, int32_t n_hyp, int32_t n_tiles, int32_t tile,
                      int32_t n_stages, const double* dmax, const int32_t* iters, float alpha, int32_t min_count,
                      int32_t blocks_per_sm, int32_t grid, void* stream);
+
+/* ---- learned initial pose (no counterpart in the reference: its odometry predicts with constant velocity) ---- */
+
+/* A point-set network proposing the ICP start pose: a shared per-point MLP 3 -> 64 -> 128 -> 256 (ReLU), a max
+ * over the LW_NET_P points of each set, the frame's and the map patch's codes concatenated (512), then
+ * 512 -> 128 (ReLU) -> 6: an se(3) step (tx, ty, tz, rx, ry, rz) in the predicted sensor frame, so that
+ * T = T_pred * exp(step). Weights and activations are bf16 with float32 accumulation; layers 2 and 3 run on the
+ * tensor cores (tcgen05.mma, accumulators in TMEM). Parameters live in one flat float32 master buffer (Adam)
+ * with a bf16 copy the kernels read, at the LW_NET_OFF_* element offsets. */
+#define LW_NET_P 1024
+#define LW_NET_OFF_W1 0        /* [64][3]   */
+#define LW_NET_OFF_B1 192      /* [64]      */
+#define LW_NET_OFF_W2 256      /* [128][64] */
+#define LW_NET_OFF_B2 8448     /* [128]     */
+#define LW_NET_OFF_W3 8576     /* [256][128] */
+#define LW_NET_OFF_B3 41344    /* [256]     */
+#define LW_NET_OFF_WH1 41600   /* [128][512] */
+#define LW_NET_OFF_BH1 107136  /* [128]     */
+#define LW_NET_OFF_WH2 107264  /* [6][128]  */
+#define LW_NET_OFF_BH2 108032  /* [6]       */
+#define LW_NET_NPARAM 108040   /* padded to a multiple of 8 */
+
+typedef struct lw_initnet {
+    float* master;    /* [LW_NET_NPARAM] float32 weights (what Adam updates) */
+    uint16_t* w;      /* [LW_NET_NPARAM] bf16 copy the kernels read (16-byte aligned) */
+    float* grad;      /* [LW_NET_NPARAM] gradient of the last backward pass */
+    float* adam_m;    /* [LW_NET_NPARAM] */
+    float* adam_v;    /* [LW_NET_NPARAM] */
+    float* out_scale; /* [6] output scale: step = network output * out_scale */
+    float in_scale;   /* input points are multiplied by this (1 / metres) */
+    int32_t pad_;
+} lw_initnet;
+
+/* Forward pass of n samples: sets [2n][LW_NET_P][4] (x, y, z, unused; set 2s is sample s's frame, 2s+1 its map
+ * patch, both in the predicted sensor frame). Writes pooled [2n][256] (the max of each channel), argmax [2n][256]
+ * (the first point attaining it), hid [n][128] (the head's hidden layer, bf16 values) and step [n][6]
+ * (out_scale applied). err [1] is set when a bounded wait gave up. */
+int lw_net_forward(const lw_initnet* net, const float* sets, int32_t n, float* pooled, int32_t* argmax, float* hid,
+                   float* step, int32_t* err, void* stream);
+
+/* Scratch of the backward pass for up to n_cap samples (sizes in floats unless stated). */
+typedef struct lw_net_scratch {
+    float* dz3;       /* [2n*256] */
+    uint16_t* h2g;    /* [2n*256*128] bf16: layer-2 activations of each channel's argmax point */
+    float* d2t;       /* [128][2n*256] */
+    float* h1t;       /* [65][2n*256]: layer-1 activations, then a row of ones */
+    float* d1t;       /* [64][2n*256] */
+    float* xt;        /* [4][2n*256]: the scaled inputs, then a row of ones */
+    float* dzh;       /* [n][128] */
+    float* dout;      /* [n][6] */
+    float* dpool;     /* [2n][256] */
+    float* part;      /* [64 * 8448] split-K partials */
+    float* loss;      /* [n] per-sample loss */
+    int32_t n_cap;
+    int32_t pad_;
+} lw_net_scratch;
+
+/* Loss sum_s sum_j w[j] * (out[s][j] - target[s][j] / out_scale[j])^2 / n and its gradient with respect to the
+ * bf16 weights, into net->grad (backpropagation through the max: only each channel's argmax point receives
+ * gradient). target [n][6] is the true step. Per-sample losses in scr->loss. */
+int lw_net_backward(const lw_initnet* net, const float* sets, int32_t n, const float* pooled, const int32_t* argmax,
+                    const float* hid, const float* step, const float* target, const float* w_loss,
+                    lw_net_scratch* scr, void* stream);
+
+/* One Adam step (t >= 1) on the master weights with decoupled weight decay, then the bf16 copy. */
+int lw_net_adam(lw_initnet* net, int32_t t, float lr, float beta1, float beta2, float eps, float weight_decay,
+                void* stream);
+
+/* Deterministic initialisation (He-uniform weights from `seed`, zero biases and moments, out_scale untouched). */
+int lw_net_init(lw_initnet* net, uint64_t seed, void* stream);
+
+/* The two point sets of the current frame, in the frame of pose T (row-major 4x4 float64 on the device, e.g. the
+ * state's T_pred). Frame set: LW_NET_P points taken at an even stride from the thinned frame (ds_xyz, n_ds on the
+ * device). Map set, with voxel > 0 (the registration voxel): for each frame-set point, the nearest registration
+ * voxel mean among the 27 voxels around it at T (the point itself where none is occupied); with voxel <= 0: the
+ * registration voxel means within `radius` of T's origin, in slot order at an even stride (cand [reg cap] and
+ * tiles [reg cap / 1024 + 2] are then scratch). sets_out [2][LW_NET_P][4]; count [2] receives the frame's point
+ * count and the patch's candidate count. */
+int lw_net_sets(const float* ds_xyz, const int32_t* n_ds, const lw_regmap* reg, const double* T, float radius,
+                float voxel, float* sets_out, int32_t* cand, int32_t* tiles, int32_t* count, void* stream);
+
+/* lw_odom_finalize with the learned start pose: after the frame is deskewed and thinned with the predicted
+ * motion, the network sees the frame and the map patch around the constant-velocity prediction T_pred and the
+ * registration starts from (and its prior is anchored at) T_pred * exp(step) instead. work: sets [2*LW_NET_P*4],
+ * pooled [512], argmax [512] (int), hid [128], step [6], err [1] (int) floats, cand / tiles as lw_net_sets. */
+typedef struct lw_net_work {
+    float* sets;
+    float* pooled;
+    int32_t* argmax;
+    float* hid;
+    float* step;
+    int32_t* err;
+    int32_t* cand;
+    int32_t* tiles;
+    int32_t* count;
+    float radius; /* map patch radius when voxel <= 0 */
+    float voxel;  /* > 0: the map set is the nearest registration voxel mean of each frame-set point */
+} lw_net_work;
+
+int lw_odom_finalize_net(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_odom_state* st, lw_frame_buf* fb,
+                         lw_regmap* reg, lw_gn_scratch* gn, lw_pose_table* pt, int32_t epoch, lw_traj_rec* traj,
+                         int64_t traj_cap, const lw_initnet* net, lw_net_work* work, void* stream);
 
 #ifdef __cplusplus
 }

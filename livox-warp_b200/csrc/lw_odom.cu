@@ -8,6 +8,7 @@
 #include <mutex>
 #include "lw_common.cuh"
 #include "lw_linalg.cuh"
+#include "lw_net.cuh"
 
 namespace lw {
 
@@ -1258,6 +1259,7 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         st->ok = ok ? 1 : 0;
         st->n_ds = n;
         st->iters = s_iters;
+        if (which == 0) st->iters_first = s_iters;
         st->corr = s_corr;
         st->rms = s_rms;
         st->cond = cond;
@@ -1304,6 +1306,7 @@ __global__ void k_ctl_begin(int k, lw_odom_params prm, lw_odom_state* st, const 
     st->redo = 0;
     st->do_insert = 0;
     st->run_reg = 0;
+    st->iters_first = 0;
     if (m < prm.min_points) {
         st->skipped += 1;
         st->ok = 0;
@@ -1401,6 +1404,7 @@ __global__ void k_ctl_end(lw_odom_params prm, lw_odom_state* st, lw_pose_table p
         r->k = k;
         r->ok = st->ok;
         r->iters = st->run_reg ? st->iters : 0;
+        r->iters_first = st->run_reg ? st->iters_first : 0;
         r->corr = st->run_reg ? st->corr : 0;
     }
     st->traj_len += 1;
@@ -1666,9 +1670,11 @@ int lw_icp_solve(const float* ds4, const int32_t* n_dev, const lw_odom_params* p
     return launch_gn(ds4, n_dev, prm, st, reg, gn, 2, (cudaStream_t)stream);  // ungated
 }
 
-int lw_odom_finalize(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_odom_state* st, lw_frame_buf* fb,
-                     lw_regmap* reg, lw_gn_scratch* gn, lw_pose_table* pt, int32_t epoch, lw_traj_rec* traj,
-                     int64_t traj_cap, void* stream) {
+// The frame's queue of launches; with `net`, the learned start pose replaces the constant-velocity one between
+// the first thinning and the first registration.
+static int finalize_impl(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_odom_state* st, lw_frame_buf* fb,
+                         lw_regmap* reg, lw_gn_scratch* gn, lw_pose_table* pt, int32_t epoch, lw_traj_rec* traj,
+                         int64_t traj_cap, const lw_initnet* net, lw_net_work* work, void* stream) {
     if (!prm || !st || !fb || !reg || !gn || !pt) return set_error(LW_EINVAL, "lw_odom_finalize: null argument");
     if ((reg->cap & (reg->cap - 1)) != 0 || (fb->ds_cap & (fb->ds_cap - 1)) != 0 || fb->ds_cap < fb->cap)
         return set_error(LW_EINVAL, "lw_odom_finalize: table capacities must be powers of two (ds_cap >= cap)");
@@ -1695,6 +1701,17 @@ int lw_odom_finalize(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_odom
         k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->run_reg);
     }
     int r;
+    if (net) {
+        // the network sees the frame and the map patch around the constant-velocity prediction
+        ProfScope prof("net", s);
+        r = net_sets_launch(fb->ds_xyz, &st->n_ds, *reg, st->T_pred, work->radius, work->voxel, work->sets,
+                            work->cand, work->tiles, work->count, s);
+        if (r != LW_OK) return r;
+        r = net_forward_launch(*net, work->sets, 1, work->pooled, work->argmax, work->hid, work->step, work->err, s);
+        if (r != LW_OK) return r;
+        r = net_apply_launch(st, work->step, work->err, s);
+        if (r != LW_OK) return r;
+    }
     {
         ProfScope prof("gn", s);
         r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 0, s);
@@ -1733,6 +1750,23 @@ int lw_odom_finalize(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_odom
     LW_LAUNCHED("lw_odom_finalize");
     count_launches(12);  // plus the two Gauss-Newton launches counted by launch_gn
     return LW_OK;
+}
+
+int lw_odom_finalize(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_odom_state* st, lw_frame_buf* fb,
+                     lw_regmap* reg, lw_gn_scratch* gn, lw_pose_table* pt, int32_t epoch, lw_traj_rec* traj,
+                     int64_t traj_cap, void* stream) {
+    return finalize_impl(k, m_ub, prm, st, fb, reg, gn, pt, epoch, traj, traj_cap, nullptr, nullptr, stream);
+}
+
+int lw_odom_finalize_net(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_odom_state* st, lw_frame_buf* fb,
+                         lw_regmap* reg, lw_gn_scratch* gn, lw_pose_table* pt, int32_t epoch, lw_traj_rec* traj,
+                         int64_t traj_cap, const lw_initnet* net, lw_net_work* work, void* stream) {
+    if (!net || !net->w || !net->out_scale || !work || !work->sets || !work->pooled || !work->argmax || !work->hid ||
+        !work->step || !work->err || !work->count || (!(work->voxel > 0.0f) && (!work->cand || !work->tiles)))
+        return set_error(LW_EINVAL, "lw_odom_finalize_net: incomplete network or work buffers");
+    if (((uintptr_t)net->w & 15) != 0 || ((uintptr_t)work->sets & 15) != 0)
+        return set_error(LW_EINVAL, "lw_odom_finalize_net: weights and sets must be 16-byte aligned");
+    return finalize_impl(k, m_ub, prm, st, fb, reg, gn, pt, epoch, traj, traj_cap, net, work, stream);
 }
 
 int lw_odom_predict_poses(int32_t k0, int32_t k1, int32_t current, const lw_odom_state* st, lw_pose_table* pt,

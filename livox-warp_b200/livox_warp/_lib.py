@@ -55,11 +55,12 @@ class OdomState(C.Structure):
                 ("xi", f32 * 6), ("xi_used", f32 * 6)] + \
                [(n, i32) for n in ("has_prev", "has_key", "map_frames", "frame_k", "m", "n_ds", "warm", "ok",
                                     "run_reg", "do_insert", "redo", "err", "iters", "corr", "degen", "weak", "frames",
-                                    "skipped", "keyframes", "traj_len")]
+                                    "skipped", "keyframes", "traj_len", "iters_first", "pad_")]
 
 
 class TrajRec(C.Structure):
-    _fields_ = [("T", f64 * 16), ("t_mid", f64), ("k", i32), ("ok", i32), ("iters", i32), ("corr", i32)]
+    _fields_ = [("T", f64 * 16), ("t_mid", f64), ("k", i32), ("ok", i32), ("iters", i32), ("corr", i32),
+                ("iters_first", i32), ("pad_", i32)]
 
 
 class FrameBuf(C.Structure):
@@ -99,6 +100,27 @@ class LocBatch(C.Structure):
     PTRS = ("pts", "scan_end", "tile_hyp", "tile_lo", "hyp_tile", "T", "tile_part", "moved", "next", "count", "eval",
             "bar", "err", "iters_run", "dims")
     _fields_ = [(n, P) for n in PTRS] + [("pts_cap", i64), ("moved_cap", i32), ("grid_cap", i32)]
+
+
+NET_P = 1024
+NET_OFF = {"W1": 0, "B1": 192, "W2": 256, "B2": 8448, "W3": 8576, "B3": 41344, "WH1": 41600, "BH1": 107136,
+           "WH2": 107264, "BH2": 108032}
+NET_NPARAM = 108040
+
+
+class InitNet(C.Structure):
+    _fields_ = [("master", P), ("w", P), ("grad", P), ("adam_m", P), ("adam_v", P), ("out_scale", P),
+                ("in_scale", f32), ("pad_", i32)]
+
+
+class NetScratch(C.Structure):
+    PTRS = ("dz3", "h2g", "d2t", "h1t", "d1t", "xt", "dzh", "dout", "dpool", "part", "loss")
+    _fields_ = [(n, P) for n in PTRS] + [("n_cap", i32), ("pad_", i32)]
+
+
+class NetWork(C.Structure):
+    PTRS = ("sets", "pooled", "argmax", "hid", "step", "err", "cand", "tiles", "count")
+    _fields_ = [(n, P) for n in PTRS] + [("radius", f32), ("voxel", f32)]
 
 
 class View(C.Structure):
@@ -149,6 +171,14 @@ _SIGS = {
     "lw_ground": (i32, [P, i32, P, P, i64, f32, f32, i32, f32, f32, i32, f32, P, P, P, P, P]),
     "lw_cluster": (i32, [P, i32, P, i32, P, i64, f32, f32, f32, i32, C.POINTER(ClusterBuf), P, P]),
     "lw_prior_grid_build": (i32, [C.POINTER(PriorGrid), P]),
+    "lw_net_init": (i32, [C.POINTER(InitNet), C.c_uint64, P]),
+    "lw_net_forward": (i32, [C.POINTER(InitNet), P, i32, P, P, P, P, P, P]),
+    "lw_net_backward": (i32, [C.POINTER(InitNet), P, i32, P, P, P, P, P, P, C.POINTER(NetScratch), P]),
+    "lw_net_adam": (i32, [C.POINTER(InitNet), i32, f32, f32, f32, f32, f32, P]),
+    "lw_net_sets": (i32, [P, P, C.POINTER(RegMap), P, f32, f32, P, P, P, P, P]),
+    "lw_odom_finalize_net": (i32, [i32, i64, C.POINTER(OdomParams), P, C.POINTER(FrameBuf), C.POINTER(RegMap),
+                                   C.POINTER(GnScratch), C.POINTER(PoseTable), i32, P, i64, C.POINTER(InitNet),
+                                   C.POINTER(NetWork), P]),
     "lw_prior_distances": (i32, [C.POINTER(PriorGrid), P, i64, C.POINTER(f64), P, P]),
     "lw_loc_icp_batch": (i32, [C.POINTER(PriorGrid), C.POINTER(LocBatch), i32, i32, i32, i32, C.POINTER(f64),
                                C.POINTER(i32), f32, i32, i32, i32, P]),

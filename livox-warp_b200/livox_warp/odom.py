@@ -110,6 +110,7 @@ class Odometry:
         self.epoch = 0
         self._rec_key = None
         self._integrate = None
+        self._net = None  # (InitNet, lw_net_work, its buffers) when the learned start pose is on
         # the frame's point count as the device state holds it (an int32 view into the state buffer)
         off = _lib.OdomState.m.offset
         self._m_dev = self._state[off:off + 4].view(torch.int32)
@@ -296,6 +297,40 @@ class Odometry:
         self._integrate = None if view is None else (view, float(voxel), int(carve_every), float(max_range),
                                                      int(max_steps))
 
+    def learned_init(self, net, radius: float = 12.0, nearest: bool = True):
+        """Start each frame's registration from the network's proposal (livox_warp.initnet.InitNet) instead of
+        the constant-velocity prediction; None turns it off. The network sees the thinned frame and, for each of
+        its points, the nearest registration voxel mean (nearest=False: the voxel means within `radius` m),
+        both in the predicted sensor frame -- the sets it was trained on."""
+        if net is None:
+            self._net = None
+            return
+        d = self.device
+        bufs = {"sets": torch.zeros((2, _lib.NET_P, 4), dtype=torch.float32, device=d),
+                "pooled": torch.zeros(512, dtype=torch.float32, device=d),
+                "argmax": torch.zeros(512, dtype=torch.int32, device=d),
+                "hid": torch.zeros(128, dtype=torch.float32, device=d),
+                "step": torch.zeros(6, dtype=torch.float32, device=d),
+                "err": torch.zeros(1, dtype=torch.int32, device=d),
+                "cand": torch.zeros(self.reg_cap, dtype=torch.int32, device=d),
+                "tiles": torch.zeros(self.reg_cap // 1024 + 2, dtype=torch.int32, device=d),
+                "count": torch.zeros(2, dtype=torch.int32, device=d)}
+        work = _lib.NetWork(*(_lib.ptr(bufs[k]).value for k in _lib.NetWork.PTRS), float(radius),
+                            float(self.reg_voxel) if nearest else 0.0)
+        self._net = (net, work, bufs)
+
+    def iteration_log(self) -> np.ndarray:
+        """(k, iterations of the first registration, iterations of the last) of every logged frame that
+        registered."""
+        n = self.read_state().traj_len
+        k = min(n, TRAJ_CAP)
+        with torch.cuda.stream(self.stream):
+            raw = self._traj.cpu().numpy().tobytes()
+        recs = (_lib.TrajRec * TRAJ_CAP).from_buffer_copy(raw)
+        rows = [(int(r.k), int(r.iters_first), int(r.iters)) for r in (recs[j % TRAJ_CAP] for j in range(n - k, n))
+                if r.ok and r.iters_first > 0]
+        return np.array(rows, dtype=np.int64).reshape(-1, 3)
+
     def flush(self, on_frame=None):
         """Finalise the open frame now (the end of a recording)."""
         if self.k_open is not None and self._m_ub > 0:
@@ -304,9 +339,16 @@ class Odometry:
 
     def _finalize(self, k: int, on_frame):
         t0 = time.perf_counter()
-        _lib.call("lw_odom_finalize", int(k), max(self._m_ub, 1), _byref(self.params()), _lib.ptr(self._state),
-                  _byref(self.fbuf), _byref(self.regmap), _byref(self.gn), _byref(self.pipe.pose_table), self.epoch,
-                  _lib.ptr(self._traj), TRAJ_CAP, self._sp())
+        if self._net is None:
+            _lib.call("lw_odom_finalize", int(k), max(self._m_ub, 1), _byref(self.params()), _lib.ptr(self._state),
+                      _byref(self.fbuf), _byref(self.regmap), _byref(self.gn), _byref(self.pipe.pose_table),
+                      self.epoch, _lib.ptr(self._traj), TRAJ_CAP, self._sp())
+        else:
+            net, work, _ = self._net
+            _lib.call("lw_odom_finalize_net", int(k), max(self._m_ub, 1), _byref(self.params()),
+                      _lib.ptr(self._state), _byref(self.fbuf), _byref(self.regmap), _byref(self.gn),
+                      _byref(self.pipe.pose_table), self.epoch, _lib.ptr(self._traj), TRAJ_CAP, _byref(net.struct),
+                      _byref(work), self._sp())
         if self._integrate is not None:
             view, voxel, every, max_range, max_steps = self._integrate
             m_ub = max(self._m_ub, 1)

@@ -602,3 +602,91 @@ def thin_5cm(xyz) -> np.ndarray:
     key = np.floor(pts / 0.05).astype(np.int64)
     _, first = np.unique(key, axis=0, return_index=True)
     return pts[np.sort(first)]
+
+
+# ---- the learned start-pose network (float64 with the kernels' bf16 rounding points) ------------------------------
+
+NET_P = 1024
+NET_NPARAM = 108040
+_NET_SEG = (("W1", 0, (64, 3)), ("b1", 192, (64,)), ("W2", 256, (128, 64)), ("b2", 8448, (128,)),
+            ("W3", 8576, (256, 128)), ("b3", 41344, (256,)), ("Wh1", 41600, (128, 512)), ("bh1", 107136, (128,)),
+            ("Wh2", 107264, (6, 128)), ("bh2", 108032, (6,)))
+
+
+def bf16r(x) -> np.ndarray:
+    """Round float32 values to bf16 (round to nearest even), returned as float32."""
+    a = np.ascontiguousarray(x, dtype=np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return r.view(np.float32).reshape(a.shape)
+
+
+def net_params(w_bf16: np.ndarray) -> dict:
+    """The bf16 weight vector (as uint16 or float32 values) split into its tensors, float64."""
+    w = np.asarray(w_bf16)
+    if w.dtype in (np.uint16, np.int16):
+        w = (w.astype(np.uint32) << 16).view(np.float32)
+    w = w.astype(np.float64)
+    return {name: w[o:o + int(np.prod(shape))].reshape(shape) for name, o, shape in _NET_SEG}
+
+
+def net_forward(w_bf16, sets: np.ndarray, in_scale: float, out_scale) -> dict:
+    """Forward pass of n samples: sets (2n, P, >=3). Layer activations rounded to bf16 where the kernels round."""
+    p = net_params(w_bf16)
+    X = (np.asarray(sets, np.float32)[..., :3] * np.float32(in_scale)).astype(np.float64)
+    z1 = X @ p["W1"].T + p["b1"]
+    h1 = bf16r(np.maximum(z1, 0.0).astype(np.float32)).astype(np.float64)
+    z2 = h1 @ p["W2"].T + p["b2"]
+    h2 = bf16r(np.maximum(z2, 0.0).astype(np.float32)).astype(np.float64)
+    z3 = np.maximum(h2 @ p["W3"].T + p["b3"], 0.0)
+    pooled = z3.max(axis=1)
+    argmax = z3.argmax(axis=1)  # first point attaining the maximum
+    n = len(sets) // 2
+    x = bf16r(pooled.reshape(n, 512).astype(np.float32)).astype(np.float64)
+    zh = x @ p["Wh1"].T + p["bh1"]
+    hid = bf16r(np.maximum(zh, 0.0).astype(np.float32)).astype(np.float64)
+    out = hid @ p["Wh2"].T + p["bh2"]
+    step = out * np.asarray(out_scale, np.float64)
+    return {"pooled": pooled, "argmax": argmax, "hid": hid, "out": out, "step": step, "x": x, "X": X}
+
+
+def net_backward(w_bf16, sets: np.ndarray, fwd: dict, target: np.ndarray, w_loss, out_scale) -> tuple:
+    """(gradient [NPARAM] with respect to the bf16 weights, loss) of sum_j w_j (out_j - target_j / scale_j)^2 / n,
+    through the max by each channel's argmax point only."""
+    p = net_params(w_bf16)
+    sc = np.asarray(out_scale, np.float64)
+    wl = np.asarray(w_loss, np.float64)
+    n = len(target)
+    diff = fwd["out"] - np.asarray(target, np.float64) / sc
+    loss = float((wl * diff * diff).sum() / n)
+    dout = 2.0 * wl * diff / n
+    g = {k: np.zeros_like(v) for k, v in p.items()}
+    g["Wh2"] = dout.T @ fwd["hid"]
+    g["bh2"] = dout.sum(0)
+    dzh = (dout @ p["Wh2"]) * (fwd["hid"] > 0)
+    g["Wh1"] = dzh.T @ fwd["x"]
+    g["bh1"] = dzh.sum(0)
+    dpool = (dzh @ p["Wh1"]).reshape(2 * n, 256)
+    X = fwd["X"]
+    for s in range(2 * n):
+        for c in range(256):
+            if not fwd["pooled"][s, c] > 0.0:
+                continue
+            gz = dpool[s, c]
+            x = X[s, fwd["argmax"][s, c]]
+            z1 = x @ p["W1"].T + p["b1"]
+            h1 = bf16r(np.maximum(z1, 0.0).astype(np.float32)).astype(np.float64)
+            z2 = h1 @ p["W2"].T + p["b2"]
+            h2 = bf16r(np.maximum(z2, 0.0).astype(np.float32)).astype(np.float64)
+            g["W3"][c] += gz * h2
+            g["b3"][c] += gz
+            d2 = gz * p["W3"][c] * (z2 > 0)
+            g["W2"] += np.outer(d2, h1)
+            g["b2"] += d2
+            d1 = (d2 @ p["W2"]) * (z1 > 0)
+            g["W1"] += np.outer(d1, x)
+            g["b1"] += d1
+    out = np.zeros(NET_NPARAM)
+    for name, o, shape in _NET_SEG:
+        out[o:o + int(np.prod(shape))] = g[name].reshape(-1)
+    return out, loss

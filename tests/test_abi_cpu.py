@@ -51,7 +51,8 @@ def test_struct_layouts_match_header(tmp_path):
                "lw_odom_state": _lib.OdomState, "lw_traj_rec": _lib.TrajRec, "lw_frame_buf": _lib.FrameBuf,
                "lw_gn_scratch": _lib.GnScratch, "lw_pose_table": _lib.PoseTable, "lw_map": _lib.Map,
                "lw_view": _lib.View, "lw_cluster_buf": _lib.ClusterBuf, "lw_prior_grid": _lib.PriorGrid,
-               "lw_loc_batch": _lib.LocBatch}
+               "lw_loc_batch": _lib.LocBatch, "lw_initnet": _lib.InitNet, "lw_net_scratch": _lib.NetScratch,
+               "lw_net_work": _lib.NetWork}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for cname, py in mirrors.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
