@@ -871,15 +871,30 @@ struct GnSmem {
     int status, corr, degen;
 };
 
-// Reduce the CTA partials: four fixed quarters of the CTAs per term, then the quarters in order.
+// Reduce the CTA partials: four fixed quarters of the CTAs per term, then the quarters in order. The loads of a
+// quarter are issued 20 at a time (one L2 round trip per batch) and summed in CTA order. A thread with no term
+// (t >= NTERMS) computes the twist from the current pose back to the prediction meanwhile (odom.py:397-401).
 __device__ void gn_reduce(const double* __restrict__ part, int grid, GnSmem& S) {
     const int t = threadIdx.x & (LW_ACC_STRIDE - 1), q = threadIdx.x >> 6;
     if (q < 4) {
         double acc = 0.0;
         // other CTAs wrote these in this launch: read them from L2 (__ldcg), never from a stale L1 line
         if (t < NTERMS) {
+            int b = q;
+            for (; b + 4 * 19 < grid; b += 4 * 20) {
+                double x[20];
+#pragma unroll
+                for (int j = 0; j < 20; ++j) x[j] = __ldcg(part + (int64_t)(b + 4 * j) * LW_ACC_STRIDE + t);
+#pragma unroll
+                for (int j = 0; j < 20; ++j) acc += x[j];
+            }
 #pragma unroll 8
-            for (int b = q; b < grid; b += 4) acc += __ldcg(part + (int64_t)b * LW_ACC_STRIDE + t);
+            for (; b < grid; b += 4) acc += __ldcg(part + (int64_t)b * LW_ACC_STRIDE + t);
+        } else if (threadIdx.x == GN_THREADS - 1) {
+            double Ti[16], Mp[16];
+            mat44_inv_rigid(S.T, Ti);
+            mat44_mul(S.Tp, Ti, Mp);
+            body_twist(Mp, S.xi);
         }
         S.part4[q][t] = acc;
     }
@@ -1050,11 +1065,7 @@ __device__ void gn_step_block(GnSmem& S, const lw_odom_params& prm) {
             S.rms = sqrt(fmax(S.v[LW_ACC_RMS], 0.0) / fmax(S.v[LW_ACC_WEIGHT], 1e-9));
             double dm = 0.0;
             for (int k = 0; k < 6; ++k) dm += S.H[k * 7];
-            S.dmean = dm / 6.0;
-            double Ti[16], Mp[16];
-            mat44_inv_rigid(S.T, Ti);  // the left twist from T back onto the prediction (odom.py:397-401)
-            mat44_mul(S.Tp, Ti, Mp);
-            body_twist(Mp, S.xi);
+            S.dmean = dm / 6.0;  // S.xi (the twist back onto the prediction) was formed during the reduce
         }
     }
     __syncthreads();
@@ -1091,13 +1102,24 @@ __device__ void gn_step_block(GnSmem& S, const lw_odom_params& prm) {
     __syncthreads();
     if (tid < 36) {
         const int p = tid / 6, q = tid % 6;
-        double x = 0.0, y = 0.0;
-        for (int k = 0; k < 6; ++k) {
-            x += S.SBi[k * 6 + p] * S.SBi[k * 6 + q];
-            y += S.Hg[p * 6 + k] * S.SB[k * 6 + q];
+        double y = 0.0;
+        for (int k = 0; k < 6; ++k) y += S.Hg[p * 6 + k] * S.SB[k * 6 + q];
+        S.tmp[tid] = y;
+        // SBi^T SBi in closed form (R R^T = I): [[I, -C], [C, C^T C + L^2 I]] with C = [c]x
+        const int bi = p / 3, bj = q / 3, i = p % 3, j = q % 3;
+        const double c[3] = {S.T[3], S.T[7], S.T[11]};
+        double x;
+        if (bi == 0 && bj == 0) {
+            x = i == j ? 1.0 : 0.0;
+        } else if (bi == 0) {
+            x = kmat(c, i, j);  // -C[i][j] (kmat holds -C)
+        } else if (bj == 0) {
+            x = -kmat(c, i, j);
+        } else {
+            // (C^T C)[i][j] = |c|^2 delta_ij - c_i c_j
+            x = (i == j ? c[0] * c[0] + c[1] * c[1] + c[2] * c[2] + S.L * S.L : 0.0) - c[i] * c[j];
         }
         S.P[tid] = prm.prior_info > 0.0 ? prm.prior_info * x : 0.0;
-        S.tmp[tid] = y;
     }
     __syncthreads();
     if (tid < 36) {
@@ -1113,21 +1135,28 @@ __device__ void gn_step_block(GnSmem& S, const lw_odom_params& prm) {
         S.rhs[i] += x;
     }
     __syncthreads();
-    if (tid == 0) {
-        double delta[6], Lf[36];
-        int st = 0;
-        double Gs[36];
+    // the degeneracy test (G - thr I positive definite) on another warp while thread 0 factors A
+    __shared__ int s_g_ok;
+    if (tid == 32) {
+        double Gs[36], Lg[36];
         for (int i = 0; i < 36; ++i) Gs[i] = S.G[i];
-        if (prm.degen_thr > 0.0 && !chol6(Gs, prm.degen_thr, Lf)) {
+        s_g_ok = !(prm.degen_thr > 0.0) || chol6(Gs, prm.degen_thr, Lg);
+    }
+    double delta[6];
+    int a_ok = 0;
+    if (tid == 0) {
+        double As[36], Lf[36];
+        for (int i = 0; i < 36; ++i) As[i] = S.A[i];
+        a_ok = chol6(As, 0.0, Lf);
+        if (a_ok) chol6_solve(Lf, S.rhs, delta);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int st = 0;
+        if (!s_g_ok) {
             st = gn_degenerate(S, prm.degen_thr, delta);  // some direction below the threshold
-        } else {
-            double As[36];
-            for (int i = 0; i < 36; ++i) As[i] = S.A[i];
-            if (!chol6(As, 0.0, Lf)) {
-                st = 3;
-            } else {
-                chol6_solve(Lf, S.rhs, delta);
-            }
+        } else if (!a_ok) {
+            st = 3;
         }
         if (st == 0) {
             apply_twist(S.T, delta);
