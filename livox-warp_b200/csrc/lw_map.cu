@@ -13,7 +13,6 @@
 namespace lw {
 
 constexpr int MTILE = 1024;
-constexpr int DDA_BATCH = 8;  // voxels of a ray whose hash probes are issued together
 
 // Carving constants (gpu.py:66-73)
 constexpr float CARVE_MIN_RANGE = 0.05f;
@@ -248,39 +247,57 @@ __device__ float4 local_plane(int ix, int iy, int iz, float ox, float oy, float 
     return make_float4((float)Q[0 * 3 + k], (float)Q[1 * 3 + k], (float)Q[2 * 3 + k], ok);
 }
 
+// local_plane kept out of line: it runs once per ray and once per occupied voxel a ray meets, and inlined its
+// float64 PCA would set the register budget of the whole ray walk
+__device__ __noinline__ float4 local_plane_nl(int ix, int iy, int iz, float ox, float oy, float oz, lw_map map,
+                                              int mask) {
+    return local_plane(ix, iy, iz, ox, oy, oz, map, mask);
+}
+
+// One warp per ray (gpu.py:469-593). Every lane steps the same DDA (identical float operations, so the voxel
+// sequence is the single-thread one); lane j takes steps 32c + j of chunk c, probes its voxel and, when it is
+// occupied, fits its local plane and tests whether the ray pierces it. The misses are integer atomics, so the map
+// gets the same counts in any order.
 template <int STRIDE>
-__global__ void k_carve(const float* __restrict__ xyz, const uint32_t* __restrict__ attr,
-                        const int32_t* __restrict__ frame, const int* n_dev, int64_t n_ub,
-                        const float* __restrict__ poses, int every, float inv_voxel, float max_range, int max_steps,
-                        lw_map map) {
+__global__ void __launch_bounds__(128) k_carve(const float* __restrict__ xyz, const uint32_t* __restrict__ attr,
+                                               const int32_t* __restrict__ frame, const int* n_dev, int64_t n_ub,
+                                               const float* __restrict__ poses, int every, float inv_voxel,
+                                               float max_range, int max_steps, lw_map map) {
     int64_t n = n_dev ? (int64_t)*n_dev : n_ub;
     if (n > n_ub) n = n_ub;
     const int mask = (int)(map.cap - 1);
     const int64_t nrays = (n + every - 1) / every;
-    for (int64_t ray = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; ray < nrays;
-         ray += (int64_t)gridDim.x * blockDim.x) {
-        int64_t i = ray * every;
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t ray = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ray < nrays; ray += nwarps) {
+        const int64_t i = ray * every;
         if (tag_of(attr[i]) != 0) continue;
         const float* T = poses + (int64_t)(frame[i] & (LW_POSE_SLOTS - 1)) * 16;
-        float ox = T[3], oy = T[7], oz = T[11];
+        const float ox = T[3], oy = T[7], oz = T[11];
         float px, py, pz, wx, wy, wz;
         load_xyz<STRIDE>(xyz, i, px, py, pz);
         xform(T, px, py, pz, wx, wy, wz);
         float dx = wx - ox, dy = wy - oy, dz = wz - oz;
-        float L = len3(dx, dy, dz);
+        const float L = len3(dx, dy, dz);
         if (L < CARVE_MIN_RANGE || L > max_range) continue;
         dx = dx / L;
         dy = dy / L;
         dz = dz / L;
-        float voxel = 1.0f / inv_voxel;
+        const float voxel = 1.0f / inv_voxel;
         float margin = fmaxf(CARVE_MARGIN_VOXELS * voxel, CARVE_MARGIN_FRACTION * L);
-        float4 pe = local_plane(ifloor(wx * inv_voxel), ifloor(wy * inv_voxel), ifloor(wz * inv_voxel), wx, wy, wz,
+        float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (lane == 0)
+            pe = local_plane_nl(ifloor(wx * inv_voxel), ifloor(wy * inv_voxel), ifloor(wz * inv_voxel), wx, wy, wz,
                                 map, mask);
+        pe.x = __shfl_sync(0xffffffffu, pe.x, 0);
+        pe.y = __shfl_sync(0xffffffffu, pe.y, 0);
+        pe.z = __shfl_sync(0xffffffffu, pe.z, 0);
+        pe.w = __shfl_sync(0xffffffffu, pe.w, 0);
         if (pe.w > 0.5f) {
             float cosine = fabsf(pe.x * dx + pe.y * dy + pe.z * dz);
             margin = fmaxf(margin, CARVE_GRAZING_VOXELS * voxel / fmaxf(cosine, CARVE_MIN_COSINE));
         }
-        float stop = (L - margin) * inv_voxel;
+        const float stop = (L - margin) * inv_voxel;
         if (stop <= 1.0f) continue;
         float posx = ox * inv_voxel, posy = oy * inv_voxel, posz = oz * inv_voxel;
         int ix = ifloor(posx), iy = ifloor(posy), iz = ifloor(posz);
@@ -310,70 +327,64 @@ __global__ void k_carve(const float* __restrict__ xyz, const uint32_t* __restric
             tmz = (posz - (float)iz) / (-dz);
             tdz = -1.0f / dz;
         }
-        // walk the ray DDA_BATCH voxels at a time: the voxel sequence does not depend on the map, so the batch's
-        // hash probes are issued together; the voxels are then examined in ray order
         bool done = false;
 #pragma unroll 1
-        for (int step0 = 0; step0 < max_steps && !done; step0 += DDA_BATCH) {
-            int64_t key[DDA_BATCH];
-            int vx[DDA_BATCH], vy[DDA_BATCH], vz[DDA_BATCH];
-            int nb = 0;
-#pragma unroll
-            for (int u = 0; u < DDA_BATCH; ++u) {
-                key[u] = EMPTY_KEY;
-                vx[u] = vy[u] = vz[u] = 0;
-                if (!done && step0 + u < max_steps) {
-                    float tt;
-                    if (tmx < tmy && tmx < tmz) {
-                        tt = tmx;
-                        ix += sx;
-                        tmx += tdx;
-                    } else if (tmy < tmz) {
-                        tt = tmy;
-                        iy += sy;
-                        tmy += tdy;
-                    } else {
-                        tt = tmz;
-                        iz += sz;
-                        tmz += tdz;
-                    }
-                    if (tt >= stop) {
-                        done = true;
-                    } else {
-                        key[u] = key_ijk(ix, iy, iz);
-                        vx[u] = ix;
-                        vy[u] = iy;
-                        vz[u] = iz;
-                        nb = u + 1;
-                    }
-                }
-            }
-            if (step0 + DDA_BATCH >= max_steps) done = true;
-            int slot[DDA_BATCH];
-            find_slots<DDA_BATCH>(key, slot, map.keys, mask);
+        for (int c0 = 0; c0 < max_steps && !done; c0 += 32) {
+            int vx = 0, vy = 0, vz = 0;
+            bool mine = false;
+            // every lane takes the same 32 steps (warp-uniform control flow); lane u keeps step c0 + u
 #pragma unroll 1
-            for (int u = 0; u < nb; ++u) {
-                int s = slot[u];
-                if (s < 0 || __ldg(map.cnt + s) <= 0) continue;
-                float cx, cy, cz;
-                centroid(map, s, cx, cy, cz);
-                float rx = cx - ox, ry = cy - oy, rz = cz - oz;
-                bool pierced = false;
-                float4 pl = local_plane(vx[u], vy[u], vz[u], cx, cy, cz, map, mask);
-                if (pl.w > 1.5f) {
-                    float dn = dx * pl.x + dy * pl.y + dz * pl.z;
-                    if (fabsf(dn) > 1.0e-4f) {
-                        float f = (rx * pl.x + ry * pl.y + rz * pl.z) / dn;
-                        float xx = dx * f - rx, xy = dy * f - ry, xz = dz * f - rz;  // plane crossing rel. to centroid
-                        if (len3(xx, xy, xz) < CARVE_PIERCE_PLANE * voxel) pierced = true;
-                    }
-                } else {
-                    float g = rx * dx + ry * dy + rz * dz;
-                    float qx = rx - g * dx, qy = ry - g * dy, qz = rz - g * dz;
-                    if (len3(qx, qy, qz) < CARVE_PIERCE_POINT * voxel) pierced = true;
+            for (int u = 0; u < 32; ++u) {
+                if (c0 + u >= max_steps) {
+                    done = true;
+                    break;
                 }
-                if (pierced) atomicAdd(map.miss + s, every);
+                float tt;
+                if (tmx < tmy && tmx < tmz) {
+                    tt = tmx;
+                    ix += sx;
+                    tmx += tdx;
+                } else if (tmy < tmz) {
+                    tt = tmy;
+                    iy += sy;
+                    tmy += tdy;
+                } else {
+                    tt = tmz;
+                    iz += sz;
+                    tmz += tdz;
+                }
+                if (tt >= stop) {
+                    done = true;
+                    break;
+                }
+                if (u == lane) {
+                    vx = ix;
+                    vy = iy;
+                    vz = iz;
+                    mine = true;
+                }
             }
+            if (!mine) continue;
+            const int s = find_slot(key_ijk(vx, vy, vz), map.keys, mask);
+            if (s < 0 || __ldg(map.cnt + s) <= 0) continue;
+            float cx, cy, cz;
+            centroid(map, s, cx, cy, cz);
+            const float rx = cx - ox, ry = cy - oy, rz = cz - oz;
+            bool pierced = false;
+            const float4 pl = local_plane_nl(vx, vy, vz, cx, cy, cz, map, mask);
+            if (pl.w > 1.5f) {
+                const float dn = dx * pl.x + dy * pl.y + dz * pl.z;
+                if (fabsf(dn) > 1.0e-4f) {
+                    const float f = (rx * pl.x + ry * pl.y + rz * pl.z) / dn;
+                    const float xx = dx * f - rx, xy = dy * f - ry, xz = dz * f - rz;  // plane crossing rel. to centroid
+                    if (len3(xx, xy, xz) < CARVE_PIERCE_PLANE * voxel) pierced = true;
+                }
+            } else {
+                const float g = rx * dx + ry * dy + rz * dz;
+                const float qx = rx - g * dx, qy = ry - g * dy, qz = rz - g * dz;
+                if (len3(qx, qy, qz) < CARVE_PIERCE_POINT * voxel) pierced = true;
+            }
+            if (pierced) atomicAdd(map.miss + s, every);
         }
     }
 }
@@ -584,7 +595,7 @@ int lw_carve(const float* xyz, int32_t xyz_stride, const uint32_t* attr, const i
     if (every < 1) every = 1;
     cudaStream_t s = (cudaStream_t)stream;
     int64_t rays = (n_ub + every - 1) / every;
-    int grid = blocks_for(rays, 128, 16 * device_sms());
+    int grid = blocks_for(rays * 32, 128, 24 * device_sms());  // a warp per ray
     ProfScope prof("carve", s);
     if (xyz_stride == 4)
         k_carve<4><<<grid, 128, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, every, inv_voxel, max_range, max_steps, *map);
