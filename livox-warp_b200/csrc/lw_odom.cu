@@ -551,8 +551,15 @@ __device__ __forceinline__ void icp_terms(float* a, const float* __restrict__ re
 }
 
 // One accumulation pass of this CTA over its share of the thinned points; writes the CTA's float64 partial.
+// Fixed point of the cross-CTA sums of the Gauss-Newton loop: 2^-16 units. The largest term a frame can produce
+// (rotation block of H: weight 1 x precision <= 2500 m^-2 x lever arm^2 <= 3600 m^2 x 2^18 points) is 2.4e12, so
+// the sum of all CTAs' terms stays below 2^62; a partial that would not fit flags an error instead of wrapping.
+constexpr double GN_FIX = 65536.0;
+constexpr double GN_FIX_MAX = 4.0e18 / 256.0;  // per-CTA bound: 256 CTAs stay below 2^62
+
 __device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P, const IcpConsts& k,
-                         const int64_t* __restrict__ keys, const float* __restrict__ rec, double* __restrict__ part) {
+                         const int64_t* __restrict__ keys, const float* __restrict__ rec, double* __restrict__ part,
+                         long long* __restrict__ fixed = nullptr, int* err = nullptr) {
     constexpr int GROUPS = GN_THREADS / GN_G;
     // one row of float accumulators per group, written by the group's leader lane (registers stay free for the
     // search); summed over the groups in a fixed order at the end
@@ -596,7 +603,17 @@ __device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P,
         double s = 0.0;
 #pragma unroll
         for (int g = 0; g < GROUPS; ++g) s += (double)gacc[g][threadIdx.x];
-        part[threadIdx.x] = s;
+        if (fixed) {
+            // integer atomics commute: every CTA reads back the same exact sum, whatever the arrival order
+            double q = rint(s * GN_FIX);
+            if (!(fabs(q) < GN_FIX_MAX)) {
+                atomicExch(err, 4);
+                q = 0.0;
+            }
+            atomicAdd((unsigned long long*)(fixed + threadIdx.x), (unsigned long long)(long long)q);
+        } else {
+            part[threadIdx.x] = s;
+        }
     }
     __syncthreads();
 }
@@ -860,7 +877,6 @@ __device__ __noinline__ double conditioning(const double* H) {
 // takes the eigen-decomposition path (odom.py:436-455) on one thread.
 
 struct GnSmem {
-    double part4[4][LW_ACC_STRIDE];
     double v[LW_ACC_STRIDE];
     double HA[2][36];
     double H[36], Hg[36], b[6];
@@ -871,37 +887,16 @@ struct GnSmem {
     int status, corr, degen;
 };
 
-// Reduce the CTA partials: four fixed quarters of the CTAs per term, then the quarters in order. The loads of a
-// quarter are issued 20 at a time (one L2 round trip per batch) and summed in CTA order. A thread with no term
-// (t >= NTERMS) computes the twist from the current pose back to the prediction meanwhile (odom.py:397-401).
-__device__ void gn_reduce(const double* __restrict__ part, int grid, GnSmem& S) {
-    const int t = threadIdx.x & (LW_ACC_STRIDE - 1), q = threadIdx.x >> 6;
-    if (q < 4) {
-        double acc = 0.0;
-        // other CTAs wrote these in this launch: read them from L2 (__ldcg), never from a stale L1 line
-        if (t < NTERMS) {
-            int b = q;
-            for (; b + 4 * 19 < grid; b += 4 * 20) {
-                double x[20];
-#pragma unroll
-                for (int j = 0; j < 20; ++j) x[j] = __ldcg(part + (int64_t)(b + 4 * j) * LW_ACC_STRIDE + t);
-#pragma unroll
-                for (int j = 0; j < 20; ++j) acc += x[j];
-            }
-#pragma unroll 8
-            for (; b < grid; b += 4) acc += __ldcg(part + (int64_t)b * LW_ACC_STRIDE + t);
-        } else if (threadIdx.x == GN_THREADS - 1) {
-            double Ti[16], Mp[16];
-            mat44_inv_rigid(S.T, Ti);
-            mat44_mul(S.Tp, Ti, Mp);
-            body_twist(Mp, S.xi);
-        }
-        S.part4[q][t] = acc;
-    }
-    __syncthreads();
-    if (threadIdx.x < LW_ACC_STRIDE) {
-        const int u = threadIdx.x;
-        S.v[u] = ((S.part4[0][u] + S.part4[1][u]) + S.part4[2][u]) + S.part4[3][u];
+// The cross-CTA sums from the fixed-point accumulator (one load per term); a thread without a term forms the twist
+// from the current pose back to the prediction meanwhile (odom.py:397-401).
+__device__ void gn_reduce_fixed(const long long* __restrict__ fixed, GnSmem& S) {
+    const int t = threadIdx.x;
+    if (t < LW_ACC_STRIDE) S.v[t] = t < NTERMS ? (double)__ldcg(fixed + t) * (1.0 / GN_FIX) : 0.0;
+    if (t == GN_THREADS - 1) {
+        double Ti[16], Mp[16];
+        mat44_inv_rigid(S.T, Ti);
+        mat44_mul(S.Tp, Ti, Mp);
+        body_twist(Mp, S.xi);
     }
     __syncthreads();
 }
@@ -1264,10 +1259,15 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         k.kappa2 = kappa * kappa;
         IcpPose P;
         make_pose(S.T, S.c, P);
-        double* part = gn.part + (int64_t)(it & 1) * gn.grid * LW_ACC_STRIDE;
-        icp_pass(ds, n, P, k, keys, rec, part + (int64_t)blockIdx.x * LW_ACC_STRIDE);
+        // cross-CTA sums in fixed point, three buffers in turn: iteration `it` adds into buffer it % 3 before the
+        // barrier and reads it after; CTA 0 then clears buffer (it + 2) % 3, which nobody reads any more (its last
+        // readers passed this barrier) and nobody adds to before the next barrier
+        long long* fixed = reinterpret_cast<long long*>(gn.part) + (it % 3) * LW_ACC_STRIDE;
+        icp_pass(ds, n, P, k, keys, rec, nullptr, fixed, gn.err);
         if (!grid_barrier(gn.bar, gn.err, 1)) return;
-        gn_reduce(part, gn.grid, S);
+        if (blockIdx.x == 0 && threadIdx.x < LW_ACC_STRIDE)
+            reinterpret_cast<long long*>(gn.part)[((it + 2) % 3) * LW_ACC_STRIDE + threadIdx.x] = 0;
+        gn_reduce_fixed(fixed, S);
         gn_step_block(S, prm);
         if (threadIdx.x == 0) {
             s_corr = S.corr;
@@ -1368,7 +1368,11 @@ __global__ void k_ctl_mid(lw_odom_params prm, lw_odom_state* st) {
 
 // Keyframe decision, velocity update, pose table and trajectory (odom.py:648-657, 682-694, 712-717).
 __global__ void k_ctl_end(lw_odom_params prm, lw_odom_state* st, lw_pose_table pt, int epoch, lw_traj_rec* traj,
-                          int64_t traj_cap) {
+                          int64_t traj_cap, const int* gn_err) {
+    if (*gn_err != 0) {  // a registration gave up (a bounded wait ran out, or its sums overflowed): not trusted
+        st->err = *gn_err;
+        st->ok = 0;
+    }
     double T[16];
     for (int i = 0; i < 16; ++i) T[i] = st->T_reg[i];
     int warm = st->warm;
@@ -1530,6 +1534,8 @@ static int launch_gn(const float* ds4, const int32_t* n_dev, const lw_odom_param
     lw_odom_params p = *prm;
     void* args[] = {(void*)&dsp, (void*)&n_dev, (void*)&p, (void*)&st, (void*)&keys, (void*)&rec,
                     (void*)&mask, (void*)&g, (void*)&which};
+    // the fixed-point accumulators of the first two iterations start at zero (the kernel clears the rest)
+    LW_CUDA(cudaMemsetAsync(gn->part, 0, 3 * LW_ACC_STRIDE * sizeof(long long), s));
     LW_CUDA(cudaLaunchCooperativeKernel((const void*)k_gn, dim3(grid), dim3(GN_THREADS), args, 0, s));
     count_launches(1);
     return LW_OK;
@@ -1765,7 +1771,7 @@ static int finalize_impl(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_
     // keyframe, velocity, pose table, trajectory
     {
         ProfScope prof("control", s);
-        k_ctl_end<<<1, 1, 0, s>>>(*prm, st, *pt, epoch, traj, traj_cap);
+        k_ctl_end<<<1, 1, 0, s>>>(*prm, st, *pt, epoch, traj, traj_cap, gn->err);
     }
     // keyframe insert with the frame's final pose (odom.py:719-727), through the state's float64 pose
     RegArgs a = reg_args(nullptr, prm->reg_voxel, prm->max_range, prm->ret_mask);

@@ -167,6 +167,8 @@ class Odometry:
         """Forget the map and the trajectory; the next frame is posed at T0 (odom.py:561-579)."""
         T0 = np.asarray(T0, dtype=np.float64).reshape(16)
         _lib.call("lw_odom_reset", _lib.f64_array(T0), _lib.ptr(self._state), _byref(self.regmap), 1, self._sp())
+        with torch.cuda.stream(self.stream):
+            self._gn.err.zero_()  # a registration that gave up stays flagged until the next reset
         _lib.call("lw_frame_reset", _byref(self.fbuf), self._sp())
         self._rec_key = (self.reg_voxel, self.noise, self.alpha)
         self.k_open = None
@@ -229,7 +231,7 @@ class Odometry:
                    map_overflow=int(rs[1]), skipped=st.skipped, warm=st.map_frames < self.warmup,
                    speed=float(np.linalg.norm(xi[:3]) / self.frame_dt),
                    turn=float(math.degrees(np.linalg.norm(xi[3:])) / self.frame_dt), gaps=self._gaps,
-                   degen=st.degen, keyframes=st.keyframes)
+                   degen=st.degen, keyframes=st.keyframes, err=st.err)
         return out
 
     # ---- per batch --------------------------------------------------------------------------------------------
