@@ -28,7 +28,10 @@ __device__ __forceinline__ void jacobi_eig(double* A, double* ev, double* V) {
                 if (i != j) off += a2;
             }
         if (off <= 1e-30 * tot || off == 0.0) break;
+        // the rotations unrolled: every index is then a constant and A, V stay in registers
+#pragma unroll
         for (int p = 0; p < N - 1; ++p) {
+#pragma unroll
             for (int q = p + 1; q < N; ++q) {
                 double apq = A[p * N + q];
                 if (apq == 0.0) continue;

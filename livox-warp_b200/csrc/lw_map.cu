@@ -196,37 +196,34 @@ __device__ __forceinline__ void find_slots(const int64_t* key, int* slot, const 
 
 // Normal of the surface through voxel (ix, iy, iz) from a PCA of the occupied 3x3x3 neighbourhood's centroids
 // taken relative to `o` (gpu.py:422-466); w = 2 surface, 1 at least 4 occupied but no surface, 0 fewer.
-// The neighbours are visited in the reference's (gx, gy, gz) order; each gx slab's 9 probes go out together.
+// All 27 probes go out together; the occupied neighbours are then summed in the reference's (gx, gy, gz) order.
 __device__ float4 local_plane(int ix, int iy, int iz, float ox, float oy, float oz, const lw_map& map, int mask) {
     double cs[3] = {0.0, 0.0, 0.0}, cc[6] = {0, 0, 0, 0, 0, 0};
     int cn = 0;
+    int64_t key[27];
+    int slot[27];
+#pragma unroll
+    for (int u = 0; u < 27; ++u) key[u] = key_ijk(ix + u / 9 - 1, iy + (u / 3) % 3 - 1, iz + u % 3 - 1);
+    find_slots<27>(key, slot, map.keys, mask);
+    int cnt[27];
+#pragma unroll
+    for (int u = 0; u < 27; ++u) cnt[u] = slot[u] >= 0 ? __ldg(map.cnt + slot[u]) : 0;
 #pragma unroll 1
-    for (int gx = -1; gx <= 1; ++gx) {
-        int64_t key[9];
-        int slot[9];
-#pragma unroll
-        for (int u = 0; u < 9; ++u) key[u] = key_ijk(ix + gx, iy + u / 3 - 1, iz + u % 3 - 1);
-        find_slots<9>(key, slot, map.keys, mask);
-        int cnt[9];
-#pragma unroll
-        for (int u = 0; u < 9; ++u) cnt[u] = slot[u] >= 0 ? __ldg(map.cnt + slot[u]) : 0;
-#pragma unroll
-        for (int u = 0; u < 9; ++u) {
-            if (cnt[u] > 0) {
-                float cx, cy, cz;
-                centroid(map, slot[u], cx, cy, cz);
-                double qx = (double)(cx - ox), qy = (double)(cy - oy), qz = (double)(cz - oz);
-                cs[0] += qx;
-                cs[1] += qy;
-                cs[2] += qz;
-                cc[0] += qx * qx;
-                cc[1] += qx * qy;
-                cc[2] += qx * qz;
-                cc[3] += qy * qy;
-                cc[4] += qy * qz;
-                cc[5] += qz * qz;
-                ++cn;
-            }
+    for (int u = 0; u < 27; ++u) {
+        if (cnt[u] > 0) {
+            float cx, cy, cz;
+            centroid(map, slot[u], cx, cy, cz);
+            double qx = (double)(cx - ox), qy = (double)(cy - oy), qz = (double)(cz - oz);
+            cs[0] += qx;
+            cs[1] += qy;
+            cs[2] += qz;
+            cc[0] += qx * qx;
+            cc[1] += qx * qy;
+            cc[2] += qx * qz;
+            cc[3] += qy * qy;
+            cc[4] += qy * qz;
+            cc[5] += qz * qz;
+            ++cn;
         }
     }
     if (cn < 4) return make_float4(0.0f, 0.0f, 1.0f, 0.0f);
