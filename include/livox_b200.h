@@ -273,10 +273,11 @@ int lw_map_insert(const float* xyz, int32_t xyz_stride, const uint32_t* attr, co
                   const int32_t* frame, const int32_t* n_dev, int64_t n_ub, const float* poses,
                   const lw_view* v, float inv_voxel, lw_map* map, int32_t* pslot, void* stream);
 
-/* Free-space carving of every `every`-th return (gpu.py:469-593). */
+/* Free-space carving of every `every`-th return (gpu.py:469-593). ray_stop is [ceil(n_ub / every)] scratch (the
+ * stopping distance of each ray, found from its end point's local plane before the rays are walked). */
 int lw_carve(const float* xyz, int32_t xyz_stride, const uint32_t* attr, const int32_t* frame,
              const int32_t* n_dev, int64_t n_ub, const float* poses, int32_t every, float inv_voxel,
-             float max_range, int32_t max_steps, lw_map* map, void* stream);
+             float max_range, int32_t max_steps, lw_map* map, float* ray_stop, void* stream);
 
 /* Classify the map's voxels into the visible set (gpu.py:699-747) and compact it in slot order
  * (gpu.py:1495-1504). Writes count_dev[0]. tiles is [cap/1024 + 1] scratch. */

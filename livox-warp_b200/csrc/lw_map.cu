@@ -251,51 +251,84 @@ __device__ __noinline__ float4 local_plane_nl(int ix, int iy, int iz, float ox, 
     return local_plane(ix, iy, iz, ox, oy, oz, map, mask);
 }
 
-// One warp per ray (gpu.py:469-593). Every lane steps the same DDA (identical float operations, so the voxel
-// sequence is the single-thread one); lane j takes steps 32c + j of chunk c, probes its voxel and, when it is
-// occupied, fits its local plane and tests whether the ray pierces it. The misses are integer atomics, so the map
-// gets the same counts in any order.
+// A ray of the carving pass: origin and unit direction through its pose; false when it is not carved (a noise
+// return, out of range).
+template <int STRIDE>
+__device__ __forceinline__ bool carve_ray(const float* __restrict__ xyz, const uint32_t* __restrict__ attr,
+                                          const int32_t* __restrict__ frame, const float* __restrict__ poses, int64_t i,
+                                          float max_range, float& ox, float& oy, float& oz, float& wx, float& wy,
+                                          float& wz, float& dx, float& dy, float& dz, float& L) {
+    if (tag_of(attr[i]) != 0) return false;
+    const float* T = poses + (int64_t)(frame[i] & (LW_POSE_SLOTS - 1)) * 16;
+    ox = T[3];
+    oy = T[7];
+    oz = T[11];
+    float px, py, pz;
+    load_xyz<STRIDE>(xyz, i, px, py, pz);
+    xform(T, px, py, pz, wx, wy, wz);
+    dx = wx - ox;
+    dy = wy - oy;
+    dz = wz - oz;
+    L = len3(dx, dy, dz);
+    if (L < CARVE_MIN_RANGE || L > max_range) return false;
+    dx = dx / L;
+    dy = dy / L;
+    dz = dz / L;
+    return true;
+}
+
+// Carving, pass 1 (gpu.py:469-495): one thread per ray finds where the ray stops -- short of its end point by a
+// margin that grows at grazing incidence on the end point's local plane -- in voxel units; 0 when not carved.
+template <int STRIDE>
+__global__ void k_carve_setup(const float* __restrict__ xyz, const uint32_t* __restrict__ attr,
+                              const int32_t* __restrict__ frame, const int* n_dev, int64_t n_ub,
+                              const float* __restrict__ poses, int every, float inv_voxel, float max_range, lw_map map,
+                              float* __restrict__ ray_stop) {
+    int64_t n = n_dev ? (int64_t)*n_dev : n_ub;
+    if (n > n_ub) n = n_ub;
+    const int mask = (int)(map.cap - 1);
+    const int64_t nrays = (n + every - 1) / every;
+    const float voxel = 1.0f / inv_voxel;
+    for (int64_t ray = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; ray < nrays;
+         ray += (int64_t)gridDim.x * blockDim.x) {
+        float ox, oy, oz, wx, wy, wz, dx, dy, dz, L;
+        float stop = 0.0f;
+        if (carve_ray<STRIDE>(xyz, attr, frame, poses, ray * every, max_range, ox, oy, oz, wx, wy, wz, dx, dy, dz, L)) {
+            float margin = fmaxf(CARVE_MARGIN_VOXELS * voxel, CARVE_MARGIN_FRACTION * L);
+            const float4 pe = local_plane(ifloor(wx * inv_voxel), ifloor(wy * inv_voxel), ifloor(wz * inv_voxel), wx,
+                                          wy, wz, map, mask);
+            if (pe.w > 0.5f) {
+                float cosine = fabsf(pe.x * dx + pe.y * dy + pe.z * dz);
+                margin = fmaxf(margin, CARVE_GRAZING_VOXELS * voxel / fmaxf(cosine, CARVE_MIN_COSINE));
+            }
+            stop = (L - margin) * inv_voxel;
+        }
+        ray_stop[ray] = stop;
+    }
+}
+
+// Carving, pass 2 (gpu.py:496-593): one warp per ray. Every lane steps the same DDA (identical float operations,
+// so the voxel sequence is the single-thread one); lane j takes steps 32c + j of chunk c, probes its voxel and,
+// when it is occupied, fits its local plane and tests whether the ray pierces it. The misses are integer atomics,
+// so the map gets the same counts in any order.
 template <int STRIDE>
 __global__ void __launch_bounds__(128) k_carve(const float* __restrict__ xyz, const uint32_t* __restrict__ attr,
                                                const int32_t* __restrict__ frame, const int* n_dev, int64_t n_ub,
                                                const float* __restrict__ poses, int every, float inv_voxel,
-                                               float max_range, int max_steps, lw_map map) {
+                                               float max_range, int max_steps, lw_map map,
+                                               const float* __restrict__ ray_stop) {
     int64_t n = n_dev ? (int64_t)*n_dev : n_ub;
     if (n > n_ub) n = n_ub;
     const int mask = (int)(map.cap - 1);
     const int64_t nrays = (n + every - 1) / every;
     const int lane = threadIdx.x & 31;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const float voxel = 1.0f / inv_voxel;
     for (int64_t ray = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ray < nrays; ray += nwarps) {
-        const int64_t i = ray * every;
-        if (tag_of(attr[i]) != 0) continue;
-        const float* T = poses + (int64_t)(frame[i] & (LW_POSE_SLOTS - 1)) * 16;
-        const float ox = T[3], oy = T[7], oz = T[11];
-        float px, py, pz, wx, wy, wz;
-        load_xyz<STRIDE>(xyz, i, px, py, pz);
-        xform(T, px, py, pz, wx, wy, wz);
-        float dx = wx - ox, dy = wy - oy, dz = wz - oz;
-        const float L = len3(dx, dy, dz);
-        if (L < CARVE_MIN_RANGE || L > max_range) continue;
-        dx = dx / L;
-        dy = dy / L;
-        dz = dz / L;
-        const float voxel = 1.0f / inv_voxel;
-        float margin = fmaxf(CARVE_MARGIN_VOXELS * voxel, CARVE_MARGIN_FRACTION * L);
-        float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (lane == 0)
-            pe = local_plane_nl(ifloor(wx * inv_voxel), ifloor(wy * inv_voxel), ifloor(wz * inv_voxel), wx, wy, wz,
-                                map, mask);
-        pe.x = __shfl_sync(0xffffffffu, pe.x, 0);
-        pe.y = __shfl_sync(0xffffffffu, pe.y, 0);
-        pe.z = __shfl_sync(0xffffffffu, pe.z, 0);
-        pe.w = __shfl_sync(0xffffffffu, pe.w, 0);
-        if (pe.w > 0.5f) {
-            float cosine = fabsf(pe.x * dx + pe.y * dy + pe.z * dz);
-            margin = fmaxf(margin, CARVE_GRAZING_VOXELS * voxel / fmaxf(cosine, CARVE_MIN_COSINE));
-        }
-        const float stop = (L - margin) * inv_voxel;
+        const float stop = ray_stop[ray];
         if (stop <= 1.0f) continue;
+        float ox, oy, oz, wx, wy, wz, dx, dy, dz, L;
+        carve_ray<STRIDE>(xyz, attr, frame, poses, ray * every, max_range, ox, oy, oz, wx, wy, wz, dx, dy, dz, L);
         float posx = ox * inv_voxel, posy = oy * inv_voxel, posz = oz * inv_voxel;
         int ix = ifloor(posx), iy = ifloor(posy), iz = ifloor(posz);
         int sx = 1, sy = 1, sz = 1;
@@ -583,23 +616,31 @@ int lw_map_insert(const float* xyz, int32_t xyz_stride, const uint32_t* attr, co
 
 int lw_carve(const float* xyz, int32_t xyz_stride, const uint32_t* attr, const int32_t* frame, const int32_t* n_dev,
              int64_t n_ub, const float* poses, int32_t every, float inv_voxel, float max_range, int32_t max_steps,
-             lw_map* map, void* stream) {
+             lw_map* map, float* ray_stop, void* stream) {
     int r = check_map(map, "lw_carve");
     if (r != LW_OK) return r;
-    if (!xyz || !attr || !frame || !poses || (xyz_stride != 3 && xyz_stride != 4))
+    if (!xyz || !attr || !frame || !poses || !ray_stop || (xyz_stride != 3 && xyz_stride != 4))
         return set_error(LW_EINVAL, "lw_carve: bad arguments");
     if (n_ub <= 0) return LW_OK;
     if (every < 1) every = 1;
     cudaStream_t s = (cudaStream_t)stream;
     int64_t rays = (n_ub + every - 1) / every;
+    int grid1 = blocks_for(rays, 64, 16 * device_sms());      // a thread per ray
     int grid = blocks_for(rays * 32, 128, 24 * device_sms());  // a warp per ray
     ProfScope prof("carve", s);
-    if (xyz_stride == 4)
-        k_carve<4><<<grid, 128, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, every, inv_voxel, max_range, max_steps, *map);
-    else
-        k_carve<3><<<grid, 128, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, every, inv_voxel, max_range, max_steps, *map);
+    if (xyz_stride == 4) {
+        k_carve_setup<4><<<grid1, 64, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, every, inv_voxel, max_range, *map,
+                                              ray_stop);
+        k_carve<4><<<grid, 128, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, every, inv_voxel, max_range, max_steps,
+                                        *map, ray_stop);
+    } else {
+        k_carve_setup<3><<<grid1, 64, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, every, inv_voxel, max_range, *map,
+                                              ray_stop);
+        k_carve<3><<<grid, 128, 0, s>>>(xyz, attr, frame, n_dev, n_ub, poses, every, inv_voxel, max_range, max_steps,
+                                        *map, ray_stop);
+    }
     LW_LAUNCHED("lw_carve");
-    count_launches(1);
+    count_launches(2);
     return LW_OK;
 }
 

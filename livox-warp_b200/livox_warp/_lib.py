@@ -164,7 +164,7 @@ _SIGS = {
                                 C.POINTER(GnScratch), P, P]),
     "lw_icp_solve": (i32, [P, P, C.POINTER(OdomParams), P, C.POINTER(RegMap), C.POINTER(GnScratch), P]),
     "lw_map_insert": (i32, [P, i32, P, P, P, P, i64, P, C.POINTER(View), f32, C.POINTER(Map), P, P]),
-    "lw_carve": (i32, [P, i32, P, P, P, i64, P, i32, f32, f32, i32, C.POINTER(Map), P]),
+    "lw_carve": (i32, [P, i32, P, P, P, i64, P, i32, f32, f32, i32, C.POINTER(Map), P, P]),
     "lw_map_build": (i32, [C.POINTER(Map), C.POINTER(View), i32, P, P, P, P, P, P, P]),
     "lw_map_clear": (i32, [C.POINTER(Map), P]),
     "lw_frame_ids": (i32, [P, i64, f32, P, P]),

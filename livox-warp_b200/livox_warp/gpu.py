@@ -314,7 +314,7 @@ class Pipeline:
         sx = _as_xyz(sx, self.device)
         _lib.call("lw_carve", _lib.ptr(sx), sx.shape[1], _lib.ptr(sa), _lib.ptr(sf), _lib.ptr(n_dev), n,
                   _lib.ptr(self.poses), max(1, int(every)), 1.0 / max(voxel, 1e-4), float(max_range), int(max_steps),
-                  C_ref(self.map_struct), _lib.stream_ptr())
+                  C_ref(self.map_struct), _lib.ptr(self._scratch(n)), _lib.stream_ptr())
 
     def ingest(self, xyz, attr, t, n: int, view: View, map_on: bool, voxel: float):
         """Stage, ring and map in one call, without odometry (gpu.py:1454-1462)."""
