@@ -985,6 +985,69 @@ __device__ __forceinline__ void chol6_solve(const double* Lf, const double* rhs,
     }
 }
 
+// A = L L^T (positive definite) and the solution of A x = rhs, with one reciprocal per column: out of line so the
+// factor stays in registers (the caller's register budget is spent on the correspondence search).
+__device__ __noinline__ int chol6_solve_nl(const double* __restrict__ A, const double* __restrict__ rhs, double* x) {
+    double Lf[36], inv[6];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        double d = A[j * 6 + j];
+#pragma unroll
+        for (int k = 0; k < j; ++k) d -= Lf[j * 6 + k] * Lf[j * 6 + k];
+        if (!(d > 0.0)) return 0;
+        const double l = sqrt(d);
+        const double r = 1.0 / l;
+        Lf[j * 6 + j] = l;
+        inv[j] = r;
+#pragma unroll
+        for (int i = j + 1; i < 6; ++i) {
+            double v = A[i * 6 + j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) v -= Lf[i * 6 + k] * Lf[j * 6 + k];
+            Lf[i * 6 + j] = v * r;
+        }
+    }
+    double y[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double v = rhs[i];
+#pragma unroll
+        for (int k = 0; k < i; ++k) v -= Lf[i * 6 + k] * y[k];
+        y[i] = v * inv[i];
+    }
+#pragma unroll
+    for (int i = 5; i >= 0; --i) {
+        double v = y[i];
+#pragma unroll
+        for (int k = i + 1; k < 6; ++k) v -= Lf[k * 6 + i] * x[k];
+        x[i] = v * inv[i];
+    }
+    return 1;
+}
+
+// Whether M - shift I is positive definite (a Cholesky factorisation succeeds), out of line like the solve.
+__device__ __noinline__ int chol6_pd_nl(const double* __restrict__ M, double shift) {
+    double Lf[36];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        double d = M[j * 6 + j] - shift;
+#pragma unroll
+        for (int k = 0; k < j; ++k) d -= Lf[j * 6 + k] * Lf[j * 6 + k];
+        if (!(d > 0.0)) return 0;
+        const double l = sqrt(d);
+        const double r = 1.0 / l;
+        Lf[j * 6 + j] = l;
+#pragma unroll
+        for (int i = j + 1; i < 6; ++i) {
+            double v = M[i * 6 + j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) v -= Lf[i * 6 + k] * Lf[j * 6 + k];
+            Lf[i * 6 + j] = v * r;
+        }
+    }
+    return 1;
+}
+
 // The degenerate branch of odom.py:436-455 (some direction below degen_thr): eigen-decompose G and hold the
 // weak directions at the prediction. One thread; rare.
 __device__ __noinline__ int gn_degenerate(GnSmem& S, double thr, double* delta) {
@@ -1132,19 +1195,10 @@ __device__ void gn_step_block(GnSmem& S, const lw_odom_params& prm) {
     __syncthreads();
     // the degeneracy test (G - thr I positive definite) on another warp while thread 0 factors A
     __shared__ int s_g_ok;
-    if (tid == 32) {
-        double Gs[36], Lg[36];
-        for (int i = 0; i < 36; ++i) Gs[i] = S.G[i];
-        s_g_ok = !(prm.degen_thr > 0.0) || chol6(Gs, prm.degen_thr, Lg);
-    }
+    if (tid == 32) s_g_ok = !(prm.degen_thr > 0.0) || chol6_pd_nl(S.G, prm.degen_thr);
     double delta[6];
     int a_ok = 0;
-    if (tid == 0) {
-        double As[36], Lf[36];
-        for (int i = 0; i < 36; ++i) As[i] = S.A[i];
-        a_ok = chol6(As, 0.0, Lf);
-        if (a_ok) chol6_solve(Lf, S.rhs, delta);
-    }
+    if (tid == 0) a_ok = chol6_solve_nl(S.A, S.rhs, delta);
     __syncthreads();
     if (tid == 0) {
         int st = 0;
