@@ -208,22 +208,39 @@ __device__ float4 local_plane(int ix, int iy, int iz, float ox, float oy, float 
     int cnt[27];
 #pragma unroll
     for (int u = 0; u < 27; ++u) cnt[u] = slot[u] >= 0 ? __ldg(map.cnt + slot[u]) : 0;
+    // the occupied neighbours' sums, fetched nine at a time, then taken in order
 #pragma unroll 1
-    for (int u = 0; u < 27; ++u) {
-        if (cnt[u] > 0) {
-            float cx, cy, cz;
-            centroid(map, slot[u], cx, cy, cz);
-            double qx = (double)(cx - ox), qy = (double)(cy - oy), qz = (double)(cz - oz);
-            cs[0] += qx;
-            cs[1] += qy;
-            cs[2] += qz;
-            cc[0] += qx * qx;
-            cc[1] += qx * qy;
-            cc[2] += qx * qz;
-            cc[3] += qy * qy;
-            cc[4] += qy * qz;
-            cc[5] += qz * qz;
-            ++cn;
+    for (int u0 = 0; u0 < 27; u0 += 9) {
+        long long ax[9], ay[9], az[9];
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+            const int s = slot[u0 + v];
+            const bool occ = cnt[u0 + v] > 0;
+            const long long* a = reinterpret_cast<const long long*>(map.acc) + 4 * (int64_t)s;
+            ax[v] = occ ? __ldg(a + 0) : 0;
+            ay[v] = occ ? __ldg(a + 1) : 0;
+            az[v] = occ ? __ldg(a + 2) : 0;
+        }
+#pragma unroll
+        for (int v = 0; v < 9; ++v) {
+            const int u = u0 + v;
+            if (cnt[u] > 0) {
+                const int c = cnt[u];
+                const double nn = (double)(c < LW_MAP_CAP ? c : LW_MAP_CAP) * LW_FIX_W;
+                const float cx = (float)((double)ax[v] / nn), cy = (float)((double)ay[v] / nn);
+                const float cz = (float)((double)az[v] / nn);
+                double qx = (double)(cx - ox), qy = (double)(cy - oy), qz = (double)(cz - oz);
+                cs[0] += qx;
+                cs[1] += qy;
+                cs[2] += qz;
+                cc[0] += qx * qx;
+                cc[1] += qx * qy;
+                cc[2] += qx * qz;
+                cc[3] += qy * qy;
+                cc[4] += qy * qz;
+                cc[5] += qz * qz;
+                ++cn;
+            }
         }
     }
     if (cn < 4) return make_float4(0.0f, 0.0f, 1.0f, 0.0f);
