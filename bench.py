@@ -324,6 +324,27 @@ def measured_peak():
     return {"hbm_gbs": 6650.0, "source": "fallback 6.65 TB/s"}
 
 
+# ---- replicas ---------------------------------------------------------------------------------------------------
+
+
+def max_over_ranks(x: float, device) -> float:
+    """The largest of every rank's x (a device time): the job takes as long as its slowest replica. One
+    all-reduce on `device` (a CUDA tensor for NCCL, a CPU one for gloo); x itself with one process."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_per_rank: int, world: int, ms_max: float) -> float:
+    """Whole-job throughput of `world` replicas that each processed units_per_rank in at most ms_max."""
+    return world * units_per_rank / (ms_max * 1e-3)
+
+
 # ---- the CPU arms ------------------------------------------------------------------------------------------------
 
 
@@ -975,21 +996,13 @@ def main():
         dist.barrier()
     torch.cuda.synchronize(device)
     res = run_device(frames, traj, a.warmup, a.steps, device, clocks)
-    ms_total = float(res["step_ms"].sum())
-    if world > 1:
-        t = torch.tensor([ms_total], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
-    value = world * a.steps / (ms_total * 1e-3)
+    ms_total = max_over_ranks(float(res["step_ms"].sum()), device)
+    value = replica_rate(a.steps, world, ms_total)
     e2e = None
     if not a.no_e2e:
         e = run_e2e(frames, traj, a.warmup, a.steps, device)
-        e_ms = e["ms"]
-        if world > 1:
-            t = torch.tensor([e_ms], dtype=torch.float64, device=device)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
-        e2e = {"value": round(world * a.steps / (e_ms * 1e-3), 3), "unit": "frames/s",
+        e_ms = max_over_ranks(e["ms"], device)
+        e2e = {"value": round(replica_rate(a.steps, world, e_ms), 3), "unit": "frames/s",
                "h2d_bytes_per_step": e["h2d"], "d2h_bytes_per_step": e["d2h"]}
     if world > 1:
         dist.barrier()

@@ -11,6 +11,9 @@ device solve:
 
   host_solve.npz    odom.py _sym6, _twist_between, _apply_twist, _body_twist, _twist_matrix, _sensor_basis,
                     _constrained_step; localize.py _twist_apply, _rotz, pose_difference; gpu.py mount_matrix.
+  prior_prepare.npz mapgrid.py PriorGrid.prepare (a static method, taken out of its class) with
+                    horizontal_levels and the module constants it reads (CELL, IDX_BITS, MAX_POINTS, PLANAR; the
+                    one Warp call among them, wp.constant, is the identity here).
 """
 
 from __future__ import annotations
@@ -108,10 +111,54 @@ def host_solve(ref: Path) -> dict:
     return out
 
 
+def prior_prepare(ref: Path) -> dict:
+    """PriorGrid.prepare on a seeded small map (a few surfaces with jitter, non-unit normals, planarity)."""
+    import types
+
+    src = ref / "python" / "livox_warp" / "mapgrid.py"
+    tree = ast.parse(src.read_text())
+    keep = []
+    for node in tree.body:
+        if isinstance(node, ast.Assign) and any(isinstance(t, ast.Name) and t.id in ("CELL", "IDX_BITS", "MAX_POINTS",
+                                                                                       "PLANAR") for t in node.targets):
+            keep.append(node)
+        elif isinstance(node, ast.FunctionDef) and node.name == "horizontal_levels":
+            keep.append(node)
+        elif isinstance(node, ast.ClassDef) and node.name == "PriorGrid":
+            for item in node.body:
+                if isinstance(item, ast.FunctionDef) and item.name == "prepare":
+                    item.decorator_list = []
+                    keep.append(item)
+    names = {n.name for n in keep if isinstance(n, ast.FunctionDef)}
+    if names != {"horizontal_levels", "prepare"}:
+        raise KeyError(f"mapgrid.py: found {sorted(names)}")
+    ns = {"np": np, "wp": types.SimpleNamespace(constant=lambda v: v)}
+    exec(compile(ast.Module(body=keep, type_ignores=[]), str(src), "exec"), ns)
+    rng = np.random.default_rng(20261204)
+    pts, nrm = [], []
+    for _ in range(6):  # patches of planes in a 3 x 2 x 1.5 m box
+        c = rng.uniform([0, 0, 0], [3, 2, 1.5])
+        u, v = np.linalg.qr(rng.normal(size=(3, 3)))[0][:, :2].T
+        ab = rng.uniform(-0.6, 0.6, (900, 2))
+        pts.append(c + ab[:, :1] * u + ab[:, 1:] * v + rng.normal(0, 0.003, (900, 3)))
+        nrm.append(np.broadcast_to(np.cross(u, v) * rng.uniform(0.5, 2.0), (900, 3)))
+    xyz = np.concatenate(pts).astype(np.float32)
+    normal = np.concatenate(nrm).astype(np.float32)
+    planarity = rng.uniform(0, 1, len(xyz)).astype(np.float32)
+    out = ns["prepare"]({"xyz": xyz, "normal": normal, "planarity": planarity})
+    lv = out["levels"]
+    return {"in_xyz": xyz, "in_normal": normal, "in_planarity": planarity, "xyz": out["xyz"], "normal": out["normal"],
+            "planarity": out["planarity"], "origin": out["origin"], "dims": out["dims"], "start": out["start"],
+            "lo": out["lo"], "hi": out["hi"], "levels_h": lv[0], "levels_lo": np.float64(lv[1]),
+            "levels_bin": np.float64(lv[2])}
+
+
 def main():
     ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
     np.savez_compressed(HERE / "host_solve.npz", **host_solve(ref))
     print("wrote", HERE / "host_solve.npz")
+    np.savez_compressed(HERE / "prior_prepare.npz", **prior_prepare(ref))
+    print("wrote", HERE / "prior_prepare.npz")
 
 
 if __name__ == "__main__":

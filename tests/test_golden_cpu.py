@@ -62,3 +62,20 @@ def test_pose_difference_and_mount():
 
     for m, want in zip(G["mount_in"], G["mount_out"]):
         assert np.array_equal(gpu.mount_matrix(*m), want)
+
+
+def test_prior_prepare_matches_reference():
+    """PriorGrid.prepare (mapgrid.py:216-243) as the reference computes it, bit for bit: the product's host
+    preparation and the oracle's restatement against tests/golden/prior_prepare.npz."""
+    from livox_warp.mapgrid import PriorGrid
+
+    P = np.load(Path(__file__).resolve().parent / "golden" / "prior_prepare.npz")
+    host = {"xyz": P["in_xyz"], "normal": P["in_normal"], "planarity": P["in_planarity"]}
+    got = PriorGrid.prepare(host)
+    for k in ("xyz", "normal", "planarity", "origin", "dims", "start", "lo", "hi"):
+        assert np.array_equal(np.asarray(got[k]), P[k]), k
+    h, lo, b = got["levels"]
+    assert np.array_equal(h, P["levels_h"]) and lo == float(P["levels_lo"]) and b == float(P["levels_bin"])
+    o = oracle.prior_prepare(P["in_xyz"], P["in_normal"], P["in_planarity"])
+    for k in ("xyz", "normal", "planarity", "origin", "dims", "start"):
+        assert np.array_equal(np.asarray(o[k]), P[k]), k
