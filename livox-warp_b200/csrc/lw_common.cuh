@@ -169,6 +169,31 @@ __device__ __forceinline__ int block_rank(int flag, int* smem32, int* tot) {
     return r;
 }
 
+// A voxel whose point cap is crossed in this batch sums only its first `room` points in index order: the
+// whole warp (every lane active) scans pslot[i0, n) for slot s, 128 entries per round, ranks the hits with
+// ballots and calls add(j) for the first `room` of them. Same points as a serial scan from i0; the adds are
+// integer atomics, so which lane makes them does not change the sums.
+template <class Add>
+__device__ __forceinline__ void warp_fill_first(const int* __restrict__ pslot, int64_t i0, int64_t n, int s,
+                                                int room, Add add) {
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    for (int64_t j0 = i0; j0 < n && room > 0; j0 += 128) {
+        bool hit[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            int64_t j = j0 + 32 * u + lane;
+            hit[u] = j < n && pslot[j] == s;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            unsigned m = __ballot_sync(0xffffffffu, hit[u]);
+            if (hit[u] && __popc(m & below) < room) add(j0 + 32 * u + lane);
+            room -= __popc(m);
+        }
+    }
+}
+
 // ---- bounded grid barrier -------------------------------------------------------------------------------
 // bar[0] counts arrivals, bar[1] is the generation. Every CTA of a cooperative launch calls it; a CTA that
 // waits longer than the spin budget sets *err and returns false (the kernel then exits), so a fault can

@@ -65,6 +65,123 @@ __device__ __forceinline__ void jacobi_eig(double* A, double* ev, double* V) {
     for (int i = 0; i < N; ++i) ev[i] = A[i * N + i];
 }
 
+// The same eigen-decomposition for a symmetric 6x6 by one warp (every lane calls it), on shared memory: the 15
+// rotations of a sweep run as 5 rounds of 3 disjoint (p, q) pairs (the round-robin ordering of parallel Jacobi,
+// Golub & Van Loan Sec. 8.5.5). Within a round lanes 0-2 form the three rotations, then 21 lanes rewrite the
+// upper triangle of J^T A J (each rotated pair's own element set to zero) and the lanes rewrite V J. A is
+// destroyed; ev[k] is A's k-th diagonal element at the end, V's column k its vector (V may be null when VEC is
+// false); rot holds 6 doubles of scratch. One thread running the unrolled cyclic form spends most of its time
+// fetching instructions; this form keeps the code small and the rotations of a round side by side. Same
+// stopping rule as jacobi_eig.
+__device__ __forceinline__ int jac6_pair(int r, int slot, int end) {
+    // round r, slot 0-2 (one byte each, p in the high nibble): (0,5)(1,4)(2,3) / (0,4)(3,5)(1,2) /
+    // (0,3)(2,4)(1,5) / (0,2)(1,3)(4,5) / (0,1)(2,5)(3,4) -- every pair once per sweep
+    const unsigned w = r == 0 ? 0x231405u : r == 1 ? 0x123504u : r == 2 ? 0x152403u : r == 3 ? 0x451302u : 0x342501u;
+    const unsigned pq = (w >> (8 * slot)) & 0xffu;
+    return end == 0 ? (int)(pq >> 4) : (int)(pq & 15u);
+}
+
+template <bool VEC>
+__device__ void jacobi6_warp(double* A, double* V, double* ev, double* rot) {
+    const int lane = threadIdx.x & 31;
+    if (VEC) {
+        V[lane] = (lane % 7 == 0) ? 1.0 : 0.0;
+        if (lane < 4) V[lane + 32] = (lane == 3) ? 1.0 : 0.0;
+    }
+    // this lane's upper-triangle element (lanes 0-20)
+    int ui = 0, uj = 0;
+    {
+        int e = lane;
+        while (ui < 5 && e >= 6 - ui) {
+            e -= 6 - ui;
+            ++ui;
+        }
+        uj = ui + e;
+    }
+    __syncwarp();
+    for (int sweep = 0; sweep < 24; ++sweep) {
+        double a0 = A[lane], a1 = lane < 4 ? A[lane + 32] : 0.0;
+        double tot = a0 * a0 + a1 * a1;
+        double off = (lane % 7 != 0 ? a0 * a0 : 0.0) + (lane < 3 ? a1 * a1 : 0.0);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            tot += __shfl_xor_sync(0xffffffffu, tot, o);
+            off += __shfl_xor_sync(0xffffffffu, off, o);
+        }
+        if (off <= 1e-30 * tot || off == 0.0) break;
+#pragma unroll 1
+        for (int r = 0; r < 5; ++r) {
+            if (lane < 3) {
+                const int p = jac6_pair(r, lane, 0), q = jac6_pair(r, lane, 1);
+                const double apq = A[p * 6 + q];
+                double c = 1.0, sn = 0.0;
+                if (apq != 0.0) {
+                    double tau = (A[q * 6 + q] - A[p * 6 + p]) / (2.0 * apq);
+                    double t = (tau >= 0.0) ? 1.0 / (tau + sqrt(1.0 + tau * tau))
+                                             : -1.0 / (-tau + sqrt(1.0 + tau * tau));
+                    c = 1.0 / sqrt(1.0 + t * t);
+                    sn = t * c;
+                }
+                rot[2 * lane] = c;
+                rot[2 * lane + 1] = sn;
+            }
+            __syncwarp();
+            // index i sits in one pair (p, q) of this round: new_i = a * old_p + b * old_q
+            auto coef = [&](int i, int& p, int& q, double& ca, double& cb) {
+                int sl = 0;
+#pragma unroll
+                for (int k = 1; k < 3; ++k)
+                    if (jac6_pair(r, k, 0) == i || jac6_pair(r, k, 1) == i) sl = k;
+                p = jac6_pair(r, sl, 0);
+                q = jac6_pair(r, sl, 1);
+                const double c = rot[2 * sl], sn = rot[2 * sl + 1];
+                if (i == p) {
+                    ca = c;
+                    cb = -sn;
+                } else {
+                    ca = sn;
+                    cb = c;
+                }
+            };
+            double na = 0.0, nv0 = 0.0, nv1 = 0.0;
+            if (lane < 21) {
+                int pi, qi, pj, qj;
+                double ai, bi, aj, bj;
+                coef(ui, pi, qi, ai, bi);
+                coef(uj, pj, qj, aj, bj);
+                if (ui != uj && pi == pj)
+                    na = 0.0;  // the rotated pair's own element
+                else
+                    na = ai * (aj * A[pi * 6 + pj] + bj * A[pi * 6 + qj]) + bi * (aj * A[qi * 6 + pj] + bj * A[qi * 6 + qj]);
+            }
+            if (VEC) {
+                int pj, qj;
+                double aj, bj;
+                const int k0 = lane / 6, j0 = lane % 6;
+                coef(j0, pj, qj, aj, bj);
+                nv0 = aj * V[k0 * 6 + pj] + bj * V[k0 * 6 + qj];
+                if (lane < 4) {
+                    const int k1 = (lane + 32) / 6, j1 = (lane + 32) % 6;
+                    coef(j1, pj, qj, aj, bj);
+                    nv1 = aj * V[k1 * 6 + pj] + bj * V[k1 * 6 + qj];
+                }
+            }
+            __syncwarp();
+            if (lane < 21) {
+                A[ui * 6 + uj] = na;
+                A[uj * 6 + ui] = na;
+            }
+            if (VEC) {
+                V[lane] = nv0;
+                if (lane < 4) V[lane + 32] = nv1;
+            }
+            __syncwarp();
+        }
+    }
+    if (lane < 6) ev[lane] = A[lane * 7];
+    __syncwarp();
+}
+
 // Solve A x = b (A row major N x N, copied) by LU with partial pivoting; false when a pivot is exactly zero
 // (numpy.linalg.solve raises LinAlgError there).
 template <int N>

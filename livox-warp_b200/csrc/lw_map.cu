@@ -108,29 +108,37 @@ __global__ void k_map_b(const float* __restrict__ xyz, const uint32_t* __restric
                         const int* __restrict__ pslot) {
     int64_t n = n_dev ? (int64_t)*n_dev : n_ub;
     if (n > n_ub) n = n_ub;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int s = pslot[i];
-        if (s < 0) continue;
-        float wx, wy, wz;
-        map_point<STRIDE>(xyz, attr, frame, poses, v, i, mi.inv_voxel, wx, wy, wz);
-        int pre = map.cnt[s];
-        int tot = pre + map.bcnt[s];
-        if (tot <= LW_MAP_CAP) {
-            map_add(map, s, wx, wy, wz, attr[i]);
-        } else if (pre < LW_MAP_CAP && map.lead[s] == (int)i) {
-            // this batch crosses the cap: the lowest-index point sums the first (cap - pre) hits in order
-            int room = LW_MAP_CAP - pre;
-            for (int64_t j = i; j < n && room > 0; ++j) {
-                if (pslot[j] != s) continue;
+    const int lane = threadIdx.x & 31;
+    // warp-uniform trip count (blockDim is a multiple of 32): the cap-crossing fill below needs the whole warp
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
+         base += (int64_t)gridDim.x * blockDim.x) {
+        int64_t i = base + lane;
+        int s = i < n ? pslot[i] : -1;
+        int pre = 0;
+        bool lead = false;
+        if (s >= 0) {
+            float wx, wy, wz;
+            map_point<STRIDE>(xyz, attr, frame, poses, v, i, mi.inv_voxel, wx, wy, wz);
+            pre = map.cnt[s];
+            if (pre + map.bcnt[s] <= LW_MAP_CAP)
+                map_add(map, s, wx, wy, wz, attr[i]);
+            else
+                lead = pre < LW_MAP_CAP && map.lead[s] == (int)i;
+            float ti = t[i];
+            atomic_max_float(map.last + s, ti);
+            atomic_min_float(map.first + s, ti);
+        }
+        // this batch crosses the cap: the voxel sums its first (cap - pre) hits in index order
+        for (unsigned lm = __ballot_sync(0xffffffffu, lead); lm; lm &= lm - 1) {
+            int src = __ffs(lm) - 1;
+            int sl = __shfl_sync(0xffffffffu, s, src);
+            int room = LW_MAP_CAP - __shfl_sync(0xffffffffu, pre, src);
+            warp_fill_first(pslot, base + src, n, sl, room, [&](int64_t j) {
                 float ux, uy, uz;
                 map_point<STRIDE>(xyz, attr, frame, poses, v, j, mi.inv_voxel, ux, uy, uz);
-                map_add(map, s, ux, uy, uz, attr[j]);
-                --room;
-            }
+                map_add(map, sl, ux, uy, uz, attr[j]);
+            });
         }
-        float ti = t[i];
-        atomic_max_float(map.last + s, ti);
-        atomic_min_float(map.first + s, ti);
     }
 }
 

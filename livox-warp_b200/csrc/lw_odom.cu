@@ -295,27 +295,36 @@ __global__ void k_reg_b(const float4* __restrict__ xyz, const int* n_dev, int64_
     reg_args_pose(a, T_dev);
     int64_t n = n_dev ? (int64_t)*n_dev : n_ub;
     if (n > n_ub) n = n_ub;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int s = pslot[i];
-        if (s < 0) continue;
-        int pre = reg.cnt[s];
-        int tot = pre + reg.bcnt[s];
-        if (tot <= LW_REG_CAP) {
-            int ix, iy, iz;
-            float rx, ry, rz;
-            reg_point(a, xyz[i], ix, iy, iz, rx, ry, rz);
-            reg_add(reg, s, rx, ry, rz);
-        } else if (pre < LW_REG_CAP && reg.first[s] == (int)i) {
-            // this batch crosses the cap: the lowest-index point adds the first (cap - pre) points in order
-            int room = LW_REG_CAP - pre;
-            for (int64_t j = i; j < n && room > 0; ++j) {
-                if (pslot[j] != s) continue;
+    const int lane = threadIdx.x & 31;
+    // warp-uniform trip count (blockDim is a multiple of 32): the cap-crossing fill below needs the whole warp
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
+         base += (int64_t)gridDim.x * blockDim.x) {
+        int64_t i = base + lane;
+        int s = i < n ? pslot[i] : -1;
+        int pre = 0;
+        bool lead = false;
+        if (s >= 0) {
+            pre = reg.cnt[s];
+            if (pre + reg.bcnt[s] <= LW_REG_CAP) {
+                int ix, iy, iz;
+                float rx, ry, rz;
+                reg_point(a, xyz[i], ix, iy, iz, rx, ry, rz);
+                reg_add(reg, s, rx, ry, rz);
+            } else {
+                lead = pre < LW_REG_CAP && reg.first[s] == (int)i;
+            }
+        }
+        // this batch crosses the cap: the voxel adds its first (cap - pre) points in index order
+        for (unsigned lm = __ballot_sync(0xffffffffu, lead); lm; lm &= lm - 1) {
+            int src = __ffs(lm) - 1;
+            int sl = __shfl_sync(0xffffffffu, s, src);
+            int room = LW_REG_CAP - __shfl_sync(0xffffffffu, pre, src);
+            warp_fill_first(pslot, base + src, n, sl, room, [&](int64_t j) {
                 int ix, iy, iz;
                 float rx, ry, rz;
                 reg_point(a, xyz[j], ix, iy, iz, rx, ry, rz);
-                reg_add(reg, s, rx, ry, rz);
-                --room;
-            }
+                reg_add(reg, sl, rx, ry, rz);
+            });
         }
     }
 }
@@ -882,6 +891,7 @@ struct GnSmem {
     double H[36], Hg[36], b[6];
     double A[36], SB[36], SBi[36], P[36], tmp[36], G[36];
     double rhs[6], xi[6], delta[6];
+    double EA[36], EV[36], ev[6], rot[6];  // the warp eigen-decomposition (degenerate branch, conditioning)
     double T[16], Tp[16], c[3];
     double L, rms, dmean;
     int status, corr, degen;
@@ -1048,12 +1058,11 @@ __device__ __noinline__ int chol6_pd_nl(const double* __restrict__ M, double shi
     return 1;
 }
 
-// The degenerate branch of odom.py:436-455 (some direction below degen_thr): eigen-decompose G and hold the
-// weak directions at the prediction. One thread; rare.
+// The degenerate branch of odom.py:436-455 (some direction below degen_thr): with G's eigen-decomposition in
+// S.ev / S.EV (warp 0 forms it), hold the weak directions at the prediction. One thread.
 __device__ __noinline__ int gn_degenerate(GnSmem& S, double thr, double* delta) {
-    double Gc[36], V[36], lam[6];
-    for (int i = 0; i < 36; ++i) Gc[i] = S.G[i];
-    jacobi_eig<6>(Gc, lam, V);
+    const double* lam = S.ev;
+    const double* V = S.EV;
     bool good[6];
     int ng = 0;
     for (int k = 0; k < 6; ++k) {
@@ -1200,6 +1209,15 @@ __device__ void gn_step_block(GnSmem& S, const lw_odom_params& prm) {
     int a_ok = 0;
     if (tid == 0) a_ok = chol6_solve_nl(S.A, S.rhs, delta);
     __syncthreads();
+    if (!s_g_ok) {  // block-uniform: G's eigen-decomposition by warp 0
+        if (tid < 32) {
+            S.EA[tid] = S.G[tid];
+            if (tid < 4) S.EA[tid + 32] = S.G[tid + 32];
+            __syncwarp();
+            jacobi6_warp<true>(S.EA, S.EV, S.ev, S.rot);
+        }
+        __syncthreads();
+    }
     if (tid == 0) {
         int st = 0;
         if (!s_g_ok) {
@@ -1216,60 +1234,6 @@ __device__ void gn_step_block(GnSmem& S, const lw_odom_params& prm) {
         S.status = st;
     }
     __syncthreads();
-}
-
-// Eigenvalues of a symmetric 6x6 by cyclic Jacobi without vectors, fully unrolled so the matrix stays in
-// registers; min over max of the diagonally normalised H is the conditioning stat (odom.py:797-800).
-__device__ __noinline__ double conditioning_fast(const double* Hs) {
-    double dg[6], A[36];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) dg[k] = sqrt(fmax(Hs[k * 7], 1e-12));
-#pragma unroll
-    for (int i = 0; i < 6; ++i)
-#pragma unroll
-        for (int j = 0; j < 6; ++j) A[i * 6 + j] = Hs[i * 6 + j] / (dg[i] * dg[j]);
-    for (int sweep = 0; sweep < 24; ++sweep) {
-        double off = 0.0, tot = 0.0;
-#pragma unroll
-        for (int i = 0; i < 6; ++i)
-#pragma unroll
-            for (int j = 0; j < 6; ++j) {
-                double a2 = A[i * 6 + j] * A[i * 6 + j];
-                tot += a2;
-                if (i != j) off += a2;
-            }
-        if (off <= 1e-30 * tot || off == 0.0) break;
-#pragma unroll
-        for (int p = 0; p < 5; ++p)
-#pragma unroll
-            for (int q = p + 1; q < 6; ++q) {
-                double apq = A[p * 6 + q];
-                if (apq != 0.0) {
-                    double tau = (A[q * 6 + q] - A[p * 6 + p]) / (2.0 * apq);
-                    double t = (tau >= 0.0) ? 1.0 / (tau + sqrt(1.0 + tau * tau)) : -1.0 / (-tau + sqrt(1.0 + tau * tau));
-                    double c = 1.0 / sqrt(1.0 + t * t), s = t * c;
-#pragma unroll
-                    for (int k = 0; k < 6; ++k) {
-                        double akp = A[k * 6 + p], akq = A[k * 6 + q];
-                        A[k * 6 + p] = c * akp - s * akq;
-                        A[k * 6 + q] = s * akp + c * akq;
-                    }
-#pragma unroll
-                    for (int k = 0; k < 6; ++k) {
-                        double apk = A[p * 6 + k], aqk = A[q * 6 + k];
-                        A[p * 6 + k] = c * apk - s * aqk;
-                        A[q * 6 + k] = s * apk + c * aqk;
-                    }
-                }
-            }
-    }
-    double lo = A[0], hi = A[0];
-#pragma unroll
-    for (int k = 1; k < 6; ++k) {
-        lo = fmin(lo, A[k * 7]);
-        hi = fmax(hi, A[k * 7]);
-    }
-    return fmax(lo, 0.0) / fmax(hi, 1e-12);
 }
 
 // The whole registration loop (odom.py:752-803) in one cooperative launch. Every CTA reduces the partials
@@ -1334,10 +1298,26 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         __syncthreads();
         if (S.status != 0) break;
     }
+    if (blockIdx.x == 0 && threadIdx.x < 32 && s_corr >= prm.min_corr) {
+        // min/max eigenvalue of H normalised by its diagonal (odom.py:797-800), by warp 0
+        for (int e = threadIdx.x; e < 36; e += 32) {
+            const int i = e / 6, j = e % 6;
+            S.EA[e] = S.H[e] / (sqrt(fmax(S.H[i * 7], 1e-12)) * sqrt(fmax(S.H[j * 7], 1e-12)));
+        }
+        __syncwarp();
+        jacobi6_warp<false>(S.EA, nullptr, S.ev, S.rot);
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         bool ok = s_corr >= prm.min_corr;
         double cond = st->cond;
-        if (ok) cond = conditioning_fast(S.H);
+        if (ok) {
+            double lo = S.ev[0], hi = S.ev[0];
+            for (int k = 1; k < 6; ++k) {
+                lo = fmin(lo, S.ev[k]);
+                hi = fmax(hi, S.ev[k]);
+            }
+            cond = fmax(lo, 0.0) / fmax(hi, 1e-12);
+        }
         for (int i = 0; i < 16; ++i) st->T_reg[i] = S.T[i];
         st->ok = ok ? 1 : 0;
         st->n_ds = n;

@@ -228,37 +228,49 @@ __global__ void k_cl_node_total(const int* tiles, int nt, int* m_dev) {
 
 // Neighbours of node j: nodes whose centroid lies within connect, found through the voxel hash within `reach`
 // voxels (a centroid lies inside its voxel, so no neighbour is farther). Counted, then written in probe order.
+// A warp serves one node: its lanes probe 32 consecutive offsets at a time (independent hash lookups in flight)
+// and a ballot ranks the hits, so the edges land in the same ascending probe order a serial walk gives.
 template <bool WRITE>
 __global__ void k_cl_edges(ClArgs a, lw_cluster_buf cb, int64_t m_ub) {
     int m = *cb.m;
     if (m > m_ub) m = (int)m_ub;
     const int S = 2 * a.reach + 1, N = S * S * S;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int j = warp; j < m; j += nwarps) {
         float px = cb.v_xyz[3 * j], py = cb.v_xyz[3 * j + 1], pz = cb.v_xyz[3 * j + 2];
         int64_t key = cb.keys[cb.node_slot[j]];
         int ix = (int)(key & KEY_MASK) - (int)KEY_BIAS;
         int iy = (int)((key >> 21) & KEY_MASK) - (int)KEY_BIAS;
         int iz = (int)((key >> 42) & KEY_MASK) - (int)KEY_BIAS;
         int cnt = 0;
-        int out = WRITE ? cb.edge_off[j] : 0;
-        for (int o = 0; o < N; ++o) {
-            int dz = o % S - a.reach, dy = (o / S) % S - a.reach, dx = o / (S * S) - a.reach;
-            if (dx == 0 && dy == 0 && dz == 0) continue;
-            int s = find_slot(key_ijk(ix + dx, iy + dy, iz + dz), cb.keys, a.mask);
-            if (s < 0) continue;
-            int k = cb.vidx[s];
-            float ex = cb.v_xyz[3 * k] - px, ey = cb.v_xyz[3 * k + 1] - py, ez = cb.v_xyz[3 * k + 2] - pz;
-            if (ex * ex + ey * ey + ez * ez <= a.connect2) {
-                if (WRITE) {
-                    if (out + cnt < cb.edge_cap)
-                        cb.edges[out + cnt] = k;
-                    else
-                        atomicExch(cb.err, 2);  // edge buffer too small: reported, never overrun
+        const int out = WRITE ? cb.edge_off[j] : 0;
+        for (int o0 = 0; o0 < N; o0 += 32) {
+            const int o = o0 + lane;
+            int k = -1;
+            if (o < N) {
+                int dz = o % S - a.reach, dy = (o / S) % S - a.reach, dx = o / (S * S) - a.reach;
+                if (dx != 0 || dy != 0 || dz != 0) {
+                    int s = find_slot(key_ijk(ix + dx, iy + dy, iz + dz), cb.keys, a.mask);
+                    if (s >= 0) {
+                        int c = cb.vidx[s];
+                        float ex = cb.v_xyz[3 * c] - px, ey = cb.v_xyz[3 * c + 1] - py, ez = cb.v_xyz[3 * c + 2] - pz;
+                        if (ex * ex + ey * ey + ez * ez <= a.connect2) k = c;
+                    }
                 }
-                ++cnt;
             }
+            const unsigned hits = __ballot_sync(0xffffffffu, k >= 0);
+            if (WRITE && k >= 0) {
+                const int e = out + cnt + __popc(hits & below);
+                if (e < cb.edge_cap)
+                    cb.edges[e] = k;
+                else
+                    atomicExch(cb.err, 2);  // edge buffer too small: reported, never overrun
+            }
+            cnt += __popc(hits);
         }
-        if (!WRITE) cb.edge_off[j] = cnt;
+        if (!WRITE && lane == 0) cb.edge_off[j] = cnt;
     }
 }
 
@@ -320,13 +332,17 @@ __global__ void k_cl_uf_init(lw_cluster_buf cb, int64_t m_ub) {
 }
 
 // Hook the larger root under the smaller one for every edge; a CAS that loses a race retries with the new roots.
+// Every component ends rooted at its smallest node whatever order the hooks land in, so a warp serves a node
+// and its lanes take the node's edges side by side.
 __global__ void k_cl_uf_union(lw_cluster_buf cb, int64_t m_ub) {
     int m = *cb.m;
     if (m > m_ub) m = (int)m_ub;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int j = warp; j < m; j += nwarps) {
         int e0 = cb.edge_off[j], e1 = cb.edge_off[j + 1];
         if (e1 > cb.edge_cap) e1 = (int)cb.edge_cap;
-        for (int e = e0; e < e1; ++e) {
+        for (int e = e0 + lane; e < e1; e += 32) {
             int k = cb.edges[e];
             if (k <= j) continue;  // every undirected edge once
             int a = j, b = k;
@@ -515,6 +531,7 @@ int lw_cluster(const float* xyz, int32_t xyz_stride, const int32_t* gnd, int32_t
     const int64_t m_ub = n_ub;  // at most one node per point
     const int sms = device_sms();
     int grid = blocks_for(n_ub, 256, 8 * sms);
+    int gridw = blocks_for(m_ub * 32, 256, 16 * sms);  // a warp per node
     int nt = blocks_for(n_ub, CTILE);
     ProfScope prof("cluster", s);
     if (xyz_stride == 4)
@@ -524,11 +541,11 @@ int lw_cluster(const float* xyz, int32_t xyz_stride, const int32_t* gnd, int32_t
     k_cl_node_count<<<nt, CTILE, 0, s>>>(n_dev, n_ub, *cb);
     k_cl_node_scatter<<<nt, CTILE, 0, s>>>(n_dev, n_ub, nt, *cb);
     k_cl_node_total<<<1, 256, 0, s>>>(cb->tiles, nt, cb->m);
-    k_cl_edges<false><<<grid, 256, 0, s>>>(a, *cb, m_ub);
+    k_cl_edges<false><<<gridw, 256, 0, s>>>(a, *cb, m_ub);
     k_cl_scan_edges<<<1, 1024, 0, s>>>(*cb, m_ub);
-    k_cl_edges<true><<<grid, 256, 0, s>>>(a, *cb, m_ub);
+    k_cl_edges<true><<<gridw, 256, 0, s>>>(a, *cb, m_ub);
     k_cl_uf_init<<<grid, 256, 0, s>>>(*cb, m_ub);
-    k_cl_uf_union<<<grid, 256, 0, s>>>(*cb, m_ub);
+    k_cl_uf_union<<<gridw, 256, 0, s>>>(*cb, m_ub);
     k_cl_uf_flatten<<<grid, 256, 0, s>>>(*cb, m_ub);
     k_cl_stats<<<grid, 256, 0, s>>>(*cb, m_ub);
     k_cl_flag<<<nt, CTILE, 0, s>>>(*cb, a, m_ub);

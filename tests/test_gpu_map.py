@@ -88,18 +88,22 @@ def test_carve_every_other_ray():
     assert _gpu_dict(pipe) == om.as_dict()
 
 
-def test_map_cap_counts_past_4096():
-    """A voxel hit more than 4096 times keeps counting but sums exactly the first 4096 hits in point order."""
+@pytest.mark.parametrize("voxels", [1, 7])
+def test_map_cap_counts_past_4096(voxels):
+    """A voxel hit more than 4096 times keeps counting but sums exactly the first 4096 hits in point order. With
+    several voxels their hits interleave at random, so one warp meets several voxels crossing the cap at once."""
     from livox_warp import gpu
 
     pipe, om, poses = _setup(1 << 12)
     rng = np.random.default_rng(5)
-    n = 9000
-    x = (np.array([1.05, 2.05, 0.55]) + rng.uniform(-0.04, 0.04, (n, 3))).astype(np.float32)
+    n = 9000 * voxels
+    centre = np.array([1.05, 2.05, 0.55]) + 0.1 * np.stack([np.arange(voxels), np.zeros(voxels),
+                                                            np.arange(voxels) % 3], 1)
+    x = (centre[rng.integers(0, voxels, n)] + rng.uniform(-0.04, 0.04, (n, 3))).astype(np.float32)
     a = rng.integers(0, 256, n).astype(np.uint32)
     t = np.linspace(0.0, 0.09, n).astype(np.float32)
     view = gpu.make_view(now=1.0, voxel=VOXEL, map_cap=pipe.map_cap)
-    for half in (slice(0, 3000), slice(3000, n)):  # the second batch crosses the cap
+    for half in (slice(0, 3000 * voxels), slice(3000 * voxels, n)):  # the second batch crosses the cap
         xs, as_, ts = x[half], a[half], t[half]
         sx, sa, st, sf = pipe.stage(xs, as_, ts, len(ts), 0.0)
         pipe.map_insert(sx, sa, st, sf, len(ts), view, VOXEL)
