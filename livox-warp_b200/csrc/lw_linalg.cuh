@@ -71,32 +71,78 @@ __device__ __forceinline__ void jacobi_eig(double* A, double* ev, double* V) {
 // upper triangle of J^T A J (each rotated pair's own element set to zero) and the lanes rewrite V J. A is
 // destroyed; ev[k] is A's k-th diagonal element at the end, V's column k its vector (V may be null when VEC is
 // false); rot holds 6 doubles of scratch. One thread running the unrolled cyclic form spends most of its time
-// fetching instructions; this form keeps the code small and the rotations of a round side by side. Same
-// stopping rule as jacobi_eig.
-__device__ __forceinline__ int jac6_pair(int r, int slot, int end) {
-    // round r, slot 0-2 (one byte each, p in the high nibble): (0,5)(1,4)(2,3) / (0,4)(3,5)(1,2) /
-    // (0,3)(2,4)(1,5) / (0,2)(1,3)(4,5) / (0,1)(2,5)(3,4) -- every pair once per sweep
-    const unsigned w = r == 0 ? 0x231405u : r == 1 ? 0x123504u : r == 2 ? 0x152403u : r == 3 ? 0x451302u : 0x342501u;
-    const unsigned pq = (w >> (8 * slot)) & 0xffu;
-    return end == 0 ? (int)(pq >> 4) : (int)(pq & 15u);
+// fetching instructions; this form keeps the code small and the rotations of a round side by side, and forms
+// each rotation with jac_rotation (no divide or correctly rounded square root). Same stopping rule as jacobi_eig.
+// 1/sqrt(x) and 1/x in float64 for x in [1, 8]: the float32 hardware approximation (relative error below
+// 2^-22) refined by two Newton-Raphson steps, y <- y (3 - x y^2) / 2 and y <- y (2 - x y), each of which squares
+// the relative error (2^-22 -> 2^-44 -> below the float64 rounding). A few dependent multiply-adds instead of the
+// long dependent chains of a correctly rounded divide or square root; the result is within a few ulp.
+__device__ __forceinline__ double rsqrt_nr(double x) {
+    float yf;
+    asm("rsqrt.approx.f32 %0, %1;" : "=f"(yf) : "f"((float)x));
+    double y = (double)yf;
+    y = y * (1.5 - 0.5 * x * y * y);
+    y = y * (1.5 - 0.5 * x * y * y);
+    return y;
+}
+
+__device__ __forceinline__ double rcp_nr(double x) {
+    float yf;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(yf) : "f"((float)x));
+    double y = (double)yf;
+    y = y + y * (1.0 - x * y);
+    y = y + y * (1.0 - x * y);
+    return y;
+}
+
+// The Jacobi rotation (c, s) that annihilates apq (Golub & Van Loan Alg. 8.5.1): t = sign(tau) / (|tau| +
+// sqrt(1 + tau^2)) with tau = (aqq - app) / (2 apq), c = 1 / sqrt(1 + t^2), s = t c. Written as
+// t = sign(tau) |2 apq| / (|d| + sqrt(d^2 + 4 apq^2)) with d = aqq - app, both scaled by the same power of two so
+// the larger has magnitude in [1, 2): every square root and reciprocal then sees an argument in [1, 8] (no
+// overflow for any tau). Same sign convention as jacobi_eig (tau = 0 counts as positive).
+__device__ __forceinline__ void jac_rotation(double app, double aqq, double apq, double& c, double& sn) {
+    c = 1.0;
+    sn = 0.0;
+    const double d = aqq - app, p2 = 2.0 * apq;
+    const double m = fmax(fabs(d), fabs(p2));
+    if (!(m >= 1e-290 && m <= 1e290)) return;  // a zero or absurd element: no rotation
+    const int e = (int)((__double_as_longlong(m) >> 52) & 0x7ff) - 1023;
+    const double sc = __longlong_as_double((long long)(1023 - e) << 52);  // 2^-e, exact
+    const double dd = d * sc, pp = p2 * sc;
+    const double h = dd * dd + pp * pp;
+    const double r = h * rsqrt_nr(h);
+    const bool pos = d == 0.0 || ((d > 0.0) == (p2 > 0.0));
+    const double t = (pos ? 1.0 : -1.0) * fabs(pp) * rcp_nr(fabs(dd) + r);
+    c = rsqrt_nr(1.0 + t * t);
+    sn = t * c;
 }
 
 template <bool VEC>
 __device__ void jacobi6_warp(double* A, double* V, double* ev, double* rot) {
+    // round r's three pairs, one byte each (p in the high nibble): (0,5)(1,4)(2,3) / (0,4)(3,5)(1,2) /
+    // (0,3)(2,4)(1,5) / (0,2)(1,3)(4,5) / (0,1)(2,5)(3,4) -- every pair once per sweep
+    constexpr unsigned PAIRS[5] = {0x231405u, 0x123504u, 0x152403u, 0x451302u, 0x342501u};
+    // the same rounds seen from each index x (6 bits at 6x): slot | (x is q) << 2 | partner << 3
+    constexpr unsigned long long IDX[5] = {0x00010d59a868ULL, 0x000744a4e4a0ULL, 0x000395121a98ULL,
+                                           0x0009aa344650ULL, 0x00055e8a9108ULL};
     const int lane = threadIdx.x & 31;
-    if (VEC) {
-        V[lane] = (lane % 7 == 0) ? 1.0 : 0.0;
-        if (lane < 4) V[lane + 32] = (lane == 3) ? 1.0 : 0.0;
-    }
-    // this lane's upper-triangle element (lanes 0-20)
-    int ui = 0, uj = 0;
+    // this lane's upper-triangle element (lanes 0-20; lanes 21-31 compute a copy of element 20 and store nothing)
+    int ui = 0, uj;
     {
-        int e = lane;
-        while (ui < 5 && e >= 6 - ui) {
+        int e = lane < 21 ? lane : 20;
+        while (e >= 6 - ui) {
             e -= 6 - ui;
             ++ui;
         }
         uj = ui + e;
+    }
+    // this lane's elements of V: lane, and lane + 32 for lanes 0-3 (the others compute a copy of element 35)
+    const int k0 = lane / 6, j0 = lane % 6;
+    const int e1 = lane < 4 ? lane + 32 : 35;
+    const int k1 = e1 / 6, j1 = e1 % 6;
+    if (VEC) {
+        V[lane] = (lane % 7 == 0) ? 1.0 : 0.0;
+        if (lane < 4) V[lane + 32] = (lane == 3) ? 1.0 : 0.0;
     }
     __syncwarp();
     for (int sweep = 0; sweep < 24; ++sweep) {
@@ -109,62 +155,43 @@ __device__ void jacobi6_warp(double* A, double* V, double* ev, double* rot) {
             off += __shfl_xor_sync(0xffffffffu, off, o);
         }
         if (off <= 1e-30 * tot || off == 0.0) break;
-#pragma unroll 1
+#pragma unroll
         for (int r = 0; r < 5; ++r) {
             if (lane < 3) {
-                const int p = jac6_pair(r, lane, 0), q = jac6_pair(r, lane, 1);
-                const double apq = A[p * 6 + q];
-                double c = 1.0, sn = 0.0;
-                if (apq != 0.0) {
-                    double tau = (A[q * 6 + q] - A[p * 6 + p]) / (2.0 * apq);
-                    double t = (tau >= 0.0) ? 1.0 / (tau + sqrt(1.0 + tau * tau))
-                                             : -1.0 / (-tau + sqrt(1.0 + tau * tau));
-                    c = 1.0 / sqrt(1.0 + t * t);
-                    sn = t * c;
-                }
+                const unsigned pq = (PAIRS[r] >> (8 * lane)) & 0xffu;
+                const int p = (int)(pq >> 4), q = (int)(pq & 15u);
+                double c, sn;
+                jac_rotation(A[p * 6 + p], A[q * 6 + q], A[p * 6 + q], c, sn);
                 rot[2 * lane] = c;
                 rot[2 * lane + 1] = sn;
             }
             __syncwarp();
-            // index i sits in one pair (p, q) of this round: new_i = a * old_p + b * old_q
-            auto coef = [&](int i, int& p, int& q, double& ca, double& cb) {
-                int sl = 0;
-#pragma unroll
-                for (int k = 1; k < 3; ++k)
-                    if (jac6_pair(r, k, 0) == i || jac6_pair(r, k, 1) == i) sl = k;
-                p = jac6_pair(r, sl, 0);
-                q = jac6_pair(r, sl, 1);
-                const double c = rot[2 * sl], sn = rot[2 * sl + 1];
-                if (i == p) {
-                    ca = c;
-                    cb = -sn;
-                } else {
-                    ca = sn;
-                    cb = c;
-                }
+            // index x sits in one pair (p, q) of this round: new_x = ca * old_p + cb * old_q
+            auto lookup = [&](int x, int& p, int& q, double& ca, double& cb, int& slot) {
+                const int en = (int)((IDX[r] >> (6 * x)) & 63ULL);
+                slot = en & 3;
+                const int partner = en >> 3;
+                const bool is_q = (en & 4) != 0;
+                const double c = rot[2 * slot], sn = rot[2 * slot + 1];
+                p = is_q ? partner : x;
+                q = is_q ? x : partner;
+                ca = is_q ? sn : c;
+                cb = is_q ? c : -sn;
             };
-            double na = 0.0, nv0 = 0.0, nv1 = 0.0;
-            if (lane < 21) {
-                int pi, qi, pj, qj;
-                double ai, bi, aj, bj;
-                coef(ui, pi, qi, ai, bi);
-                coef(uj, pj, qj, aj, bj);
-                if (ui != uj && pi == pj)
-                    na = 0.0;  // the rotated pair's own element
-                else
-                    na = ai * (aj * A[pi * 6 + pj] + bj * A[pi * 6 + qj]) + bi * (aj * A[qi * 6 + pj] + bj * A[qi * 6 + qj]);
-            }
+            int pi, qi, si, pj, qj, sj;
+            double ai, bi, aj, bj;
+            lookup(ui, pi, qi, ai, bi, si);
+            lookup(uj, pj, qj, aj, bj, sj);
+            double na = ai * (aj * A[pi * 6 + pj] + bj * A[pi * 6 + qj]) + bi * (aj * A[qi * 6 + pj] + bj * A[qi * 6 + qj]);
+            if (ui != uj && si == sj) na = 0.0;  // the rotated pair's own element
+            double nv0 = 0.0, nv1 = 0.0;
             if (VEC) {
-                int pj, qj;
-                double aj, bj;
-                const int k0 = lane / 6, j0 = lane % 6;
-                coef(j0, pj, qj, aj, bj);
-                nv0 = aj * V[k0 * 6 + pj] + bj * V[k0 * 6 + qj];
-                if (lane < 4) {
-                    const int k1 = (lane + 32) / 6, j1 = (lane + 32) % 6;
-                    coef(j1, pj, qj, aj, bj);
-                    nv1 = aj * V[k1 * 6 + pj] + bj * V[k1 * 6 + qj];
-                }
+                int p0, q0, s0, p1, q1, s1;
+                double ca0, cb0, ca1, cb1;
+                lookup(j0, p0, q0, ca0, cb0, s0);
+                lookup(j1, p1, q1, ca1, cb1, s1);
+                nv0 = ca0 * V[k0 * 6 + p0] + cb0 * V[k0 * 6 + q0];
+                nv1 = ca1 * V[k1 * 6 + p1] + cb1 * V[k1 * 6 + q1];
             }
             __syncwarp();
             if (lane < 21) {
