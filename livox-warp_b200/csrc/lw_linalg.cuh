@@ -70,7 +70,8 @@ __device__ __forceinline__ void jacobi_eig(double* A, double* ev, double* V) {
 // Golub & Van Loan Sec. 8.5.5). Within a round lanes 0-2 form the three rotations, then 21 lanes rewrite the
 // upper triangle of J^T A J (each rotated pair's own element set to zero) and the lanes rewrite V J. A is
 // destroyed; ev[k] is A's k-th diagonal element at the end, V's column k its vector (V may be null when VEC is
-// false); rot holds 6 doubles of scratch. One thread running the unrolled cyclic form spends most of its time
+// false); rot holds 6 doubles of scratch. With v_given, V already holds an orthogonal basis Q and A is Q^T M Q:
+// the rotations accumulate onto Q, so V ends as M's eigenvectors. One thread running the unrolled cyclic form spends most of its time
 // fetching instructions; this form keeps the code small and the rotations of a round side by side, and forms
 // each rotation with jac_rotation (no divide or correctly rounded square root). Same stopping rule as jacobi_eig.
 // 1/sqrt(x) and 1/x in float64 for x in [1, 8]: the float32 hardware approximation (relative error below
@@ -118,7 +119,7 @@ __device__ __forceinline__ void jac_rotation(double app, double aqq, double apq,
 }
 
 template <bool VEC>
-__device__ void jacobi6_warp(double* A, double* V, double* ev, double* rot) {
+__device__ void jacobi6_warp(double* A, double* V, double* ev, double* rot, bool v_given) {
     // round r's three pairs, one byte each (p in the high nibble): (0,5)(1,4)(2,3) / (0,4)(3,5)(1,2) /
     // (0,3)(2,4)(1,5) / (0,2)(1,3)(4,5) / (0,1)(2,5)(3,4) -- every pair once per sweep
     constexpr unsigned PAIRS[5] = {0x231405u, 0x123504u, 0x152403u, 0x451302u, 0x342501u};
@@ -140,7 +141,7 @@ __device__ void jacobi6_warp(double* A, double* V, double* ev, double* rot) {
     const int k0 = lane / 6, j0 = lane % 6;
     const int e1 = lane < 4 ? lane + 32 : 35;
     const int k1 = e1 / 6, j1 = e1 % 6;
-    if (VEC) {
+    if (VEC && !v_given) {
         V[lane] = (lane % 7 == 0) ? 1.0 : 0.0;
         if (lane < 4) V[lane + 32] = (lane == 3) ? 1.0 : 0.0;
     }

@@ -892,6 +892,8 @@ struct GnSmem {
     double A[36], SB[36], SBi[36], P[36], tmp[36], G[36];
     double rhs[6], xi[6], delta[6];
     double EA[36], EV[36], ev[6], rot[6];  // the warp eigen-decomposition (degenerate branch, conditioning)
+    double wv[6][6];                        // the degenerate step's vectors
+    int have_v, dstat;                      // EV holds an earlier iteration's vectors; the degenerate step's status
     double T[16], Tp[16], c[3];
     double L, rms, dmean;
     int status, corr, degen;
@@ -1059,63 +1061,134 @@ __device__ __noinline__ int chol6_pd_nl(const double* __restrict__ M, double shi
 }
 
 // The degenerate branch of odom.py:436-455 (some direction below degen_thr): with G's eigen-decomposition in
-// S.ev / S.EV (warp 0 forms it), hold the weak directions at the prediction. One thread.
-__device__ __noinline__ int gn_degenerate(GnSmem& S, double thr, double* delta) {
-    const double* lam = S.ev;
+// S.ev / S.EV, hold the weak directions at the prediction and solve for the rest. Warp 0, every lane: the 6x6
+// products run one element per lane; the small solve on the kept directions runs on lane 0. Writes S.delta,
+// S.degen and S.dstat (0, or 3 when a factorisation fails).
+__device__ void gn_degenerate_warp(GnSmem& S, double thr) {
+    const int lane = threadIdx.x & 31;
     const double* V = S.EV;
-    bool good[6];
-    int ng = 0;
-    for (int k = 0; k < 6; ++k) {
-        good[k] = lam[k] >= thr;
-        ng += good[k] ? 1 : 0;
+    unsigned gm = 0;
+    for (int k = 0; k < 6; ++k)
+        if (S.ev[k] >= thr) gm |= 1u << k;
+    const int ng = __popc(gm);
+    if (lane == 0) {
+        S.degen = 6 - ng;
+        S.dstat = 0;
     }
-    S.degen = 6 - ng;
     if (ng == 6) {
-        double Lf[36];
-        if (!chol6(S.A, 0.0, Lf)) return 3;
-        chol6_solve(Lf, S.rhs, delta);
-        return 0;
-    }
-    double z[6], d0[6];
-    matvec6(S.SBi, S.xi, z);  // solve(J, to_pred)
-    for (int i = 0; i < 6; ++i) d0[i] = 0.0;
-    for (int k = 0; k < 6; ++k) {
-        if (good[k]) continue;
-        double pr = 0.0;
-        for (int i = 0; i < 6; ++i) pr += V[i * 6 + k] * z[i];
-        for (int i = 0; i < 6; ++i) d0[i] += V[i * 6 + k] * pr;
-    }
-    if (ng > 0) {
-        double As[36], tmp[36], Jr[6], Asd[6], g[6], Ag[36], y[6], Vg[36];
-        int cols[6], nc = 0;
-        for (int k = 0; k < 6; ++k)
-            if (good[k]) cols[nc++] = k;
-        matmul6(S.A, S.SB, tmp);
-        matmul6(S.SB, tmp, As, true);
-        matvec6(S.SB, S.rhs, Jr, true);
-        matvec6(As, d0, Asd);
-        for (int i = 0; i < 6; ++i)
-            for (int a = 0; a < nc; ++a) Vg[i * 6 + a] = V[i * 6 + cols[a]];
-        for (int a = 0; a < nc; ++a) {
-            double s = 0.0;
-            for (int i = 0; i < 6; ++i) s += Vg[i * 6 + a] * (Jr[i] - Asd[i]);
-            g[a] = s;
-            for (int c2 = 0; c2 < nc; ++c2) {
-                double s2 = 0.0;
-                for (int i = 0; i < 6; ++i) {
-                    double t2 = 0.0;
-                    for (int j = 0; j < 6; ++j) t2 += As[i * 6 + j] * Vg[j * 6 + c2];
-                    s2 += Vg[i * 6 + a] * t2;
-                }
-                Ag[a * 6 + c2] = s2;
+        if (lane == 0) {
+            double Lf[36], d[6];
+            if (!chol6(S.A, 0.0, Lf)) {
+                S.dstat = 3;
+            } else {
+                chol6_solve(Lf, S.rhs, d);
+                for (int i = 0; i < 6; ++i) S.delta[i] = d[i];
             }
         }
-        if (!lu_solve<6>(Ag, g, y, nc)) return 3;
-        for (int i = 0; i < 6; ++i)
-            for (int a = 0; a < nc; ++a) d0[i] += Vg[i * 6 + a] * y[a];
+        __syncwarp();
+        return;
     }
-    matvec6(S.SB, d0, delta);
-    return 0;
+    double* z = S.wv[0];   // SB^-1 (prediction - current): solve(J, to_pred)
+    double* d0 = S.wv[1];  // the step in the sensor basis
+    double* Jr = S.wv[2];  // SB^T rhs
+    double* pr = S.wv[3];  // weak-direction components of z, then the residual Jr - As d0
+    double* gf = S.wv[4];  // V^T (Jr - As d0)
+    double* yf = S.wv[5];  // the kept directions' solution (zero on the weak ones)
+    double* tmp = S.tmp;   // A SB, then As V
+    double* As = S.P;      // SB^T A SB
+    double* M = S.EA;      // V^T As V
+    if (lane < 6) {
+        double t = 0.0;
+        for (int k = 0; k < 6; ++k) t += S.SBi[lane * 6 + k] * S.xi[k];
+        z[lane] = t;
+    } else if (lane >= 8 && lane < 14) {
+        const int i = lane - 8;
+        double t = 0.0;
+        for (int k = 0; k < 6; ++k) t += S.SB[k * 6 + i] * S.rhs[k];
+        Jr[i] = t;
+    }
+    for (int e = lane; e < 36; e += 32) {
+        const int i = e / 6, j = e % 6;
+        double t = 0.0;
+        for (int k = 0; k < 6; ++k) t += S.A[i * 6 + k] * S.SB[k * 6 + j];
+        tmp[e] = t;
+    }
+    __syncwarp();
+    if (lane < 6) {
+        double t = 0.0;
+        if (!((gm >> lane) & 1u))
+            for (int i = 0; i < 6; ++i) t += V[i * 6 + lane] * z[i];
+        pr[lane] = t;
+    }
+    for (int e = lane; e < 36; e += 32) {
+        const int i = e / 6, j = e % 6;
+        double t = 0.0;
+        for (int k = 0; k < 6; ++k) t += S.SB[k * 6 + i] * tmp[k * 6 + j];
+        As[e] = t;
+    }
+    __syncwarp();
+    if (lane < 6) {
+        double t = 0.0;
+        for (int k = 0; k < 6; ++k)
+            if (!((gm >> k) & 1u)) t += V[lane * 6 + k] * pr[k];
+        d0[lane] = t;
+    }
+    for (int e = lane; e < 36; e += 32) {
+        const int i = e / 6, j = e % 6;
+        double t = 0.0;
+        for (int k = 0; k < 6; ++k) t += As[i * 6 + k] * V[k * 6 + j];
+        tmp[e] = t;
+    }
+    __syncwarp();
+    if (ng > 0) {
+        if (lane < 6) {
+            double t = 0.0;
+            for (int k = 0; k < 6; ++k) t += As[lane * 6 + k] * d0[k];
+            pr[lane] = Jr[lane] - t;
+        }
+        for (int e = lane; e < 36; e += 32) {
+            const int i = e / 6, j = e % 6;
+            double t = 0.0;
+            for (int k = 0; k < 6; ++k) t += V[k * 6 + i] * tmp[k * 6 + j];
+            M[e] = t;
+        }
+        __syncwarp();
+        if (lane < 6) {
+            double t = 0.0;
+            for (int i = 0; i < 6; ++i) t += V[i * 6 + lane] * pr[i];
+            gf[lane] = t;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            int cols[6], nc = 0;
+            for (int k = 0; k < 6; ++k)
+                if ((gm >> k) & 1u) cols[nc++] = k;
+            double Ag[36], g[6], y[6];
+            for (int a = 0; a < nc; ++a) {
+                g[a] = gf[cols[a]];
+                for (int c2 = 0; c2 < nc; ++c2) Ag[a * 6 + c2] = M[cols[a] * 6 + cols[c2]];
+            }
+            for (int k = 0; k < 6; ++k) yf[k] = 0.0;
+            if (!lu_solve<6>(Ag, g, y, nc))
+                S.dstat = 3;
+            else
+                for (int a = 0; a < nc; ++a) yf[cols[a]] = y[a];
+        }
+        __syncwarp();
+        if (lane < 6) {
+            double t = d0[lane];
+            for (int k = 0; k < 6; ++k)
+                if ((gm >> k) & 1u) t += V[lane * 6 + k] * yf[k];
+            d0[lane] = t;
+        }
+        __syncwarp();
+    }
+    if (lane < 6) {
+        double t = 0.0;
+        for (int k = 0; k < 6; ++k) t += S.SB[lane * 6 + k] * d0[k];
+        S.delta[lane] = t;
+    }
+    __syncwarp();
 }
 
 // One Gauss-Newton update of S.T (odom.py:769-796) by the whole block. S.status: 0 continue, 1 converged,
@@ -1209,19 +1282,42 @@ __device__ void gn_step_block(GnSmem& S, const lw_odom_params& prm) {
     int a_ok = 0;
     if (tid == 0) a_ok = chol6_solve_nl(S.A, S.rhs, delta);
     __syncthreads();
-    if (!s_g_ok) {  // block-uniform: G's eigen-decomposition by warp 0
+    if (!s_g_ok) {  // block-uniform: some direction below the threshold, warp 0 takes the degenerate step
         if (tid < 32) {
-            S.EA[tid] = S.G[tid];
-            if (tid < 4) S.EA[tid + 32] = S.G[tid + 32];
+            const bool warm = S.have_v != 0;
+            if (warm) {
+                // start from an earlier iteration's vectors: V^T G V is nearly diagonal, so fewer sweeps
+                for (int e = tid; e < 36; e += 32) {
+                    const int i = e / 6, j = e % 6;
+                    double t = 0.0;
+                    for (int k = 0; k < 6; ++k) t += S.G[i * 6 + k] * S.EV[k * 6 + j];
+                    S.tmp[e] = t;
+                }
+                __syncwarp();
+                for (int e = tid; e < 36; e += 32) {
+                    const int i = e / 6, j = e % 6;
+                    if (i > j) continue;
+                    double t = 0.0;
+                    for (int k = 0; k < 6; ++k) t += S.EV[k * 6 + i] * S.tmp[k * 6 + j];
+                    S.EA[i * 6 + j] = t;
+                    S.EA[j * 6 + i] = t;
+                }
+            } else {
+                S.EA[tid] = S.G[tid];
+                if (tid < 4) S.EA[tid + 32] = S.G[tid + 32];
+            }
             __syncwarp();
-            jacobi6_warp<true>(S.EA, S.EV, S.ev, S.rot);
+            jacobi6_warp<true>(S.EA, S.EV, S.ev, S.rot, warm);
+            if (tid == 0) S.have_v = 1;
+            gn_degenerate_warp(S, prm.degen_thr);
         }
         __syncthreads();
     }
     if (tid == 0) {
         int st = 0;
         if (!s_g_ok) {
-            st = gn_degenerate(S, prm.degen_thr, delta);  // some direction below the threshold
+            st = S.dstat;
+            for (int i = 0; i < 6; ++i) delta[i] = S.delta[i];
         } else if (!a_ok) {
             st = 3;
         }
@@ -1257,6 +1353,7 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         s_corr = 0;
         s_rms = 0.0;
         for (int i = 0; i < 36; ++i) S.H[i] = (i % 7 == 0) ? 1.0 : 0.0;
+        S.have_v = 0;
     }
     __syncthreads();
     if (n < prm.min_corr) {  // odom.py:754-757
@@ -1305,7 +1402,7 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
             S.EA[e] = S.H[e] / (sqrt(fmax(S.H[i * 7], 1e-12)) * sqrt(fmax(S.H[j * 7], 1e-12)));
         }
         __syncwarp();
-        jacobi6_warp<false>(S.EA, nullptr, S.ev, S.rot);
+        jacobi6_warp<false>(S.EA, nullptr, S.ev, S.rot, false);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         bool ok = s_corr >= prm.min_corr;
