@@ -12,7 +12,6 @@
 
 namespace lw {
 
-constexpr int MTILE = 1024;
 
 // Carving constants (gpu.py:66-73)
 constexpr float CARVE_MIN_RANGE = 0.05f;
@@ -484,9 +483,9 @@ __device__ int settled_near(int ix, int iy, int iz, const lw_view& v, const lw_m
     return 0;
 }
 
-__device__ __forceinline__ bool classify_flag(const lw_map& map, int64_t s, const lw_view& v, int min_count, float& wx,
-                                              float& wy, float& wz) {
-    if (map.keys[s] == EMPTY_KEY) return false;
+__device__ __forceinline__ bool classify_flag_key(const lw_map& map, int64_t s, int64_t key, const lw_view& v,
+                                                  int min_count, float& wx, float& wy, float& wz) {
+    if (key == EMPTY_KEY) return false;
     int c = map.cnt[s];
     if (c < min_count) return false;
     float last = map.last[s];
@@ -497,15 +496,69 @@ __device__ __forceinline__ bool classify_flag(const lw_map& map, int64_t s, cons
     return in_crop(wx, wy, wz, v) != 0;
 }
 
-__global__ void k_classify_count(lw_map map, lw_view v, int min_count, int* __restrict__ tiles) {
-    int64_t s = (int64_t)blockIdx.x * MTILE + threadIdx.x;
-    int f = 0;
-    if (s < map.cap) {
-        float wx, wy, wz;
-        f = classify_flag(map, s, v, min_count, wx, wy, wz) ? 1 : 0;
+// The classification runs in tiles of CL_TILE slots, a CTA per tile and CL_PER consecutive slots per thread (their
+// keys in 16-byte loads), so every load of a tile is in flight at once; per-thread counts are scanned across the
+// CTA, which keeps the compaction in slot order.
+constexpr int CL_PER = 8, CL_THREADS = 512, CL_TILE = CL_PER * CL_THREADS;
+
+__device__ __forceinline__ void load_keys(const lw_map& map, int64_t s0, int64_t* k) {
+    if (s0 + CL_PER <= map.cap && (reinterpret_cast<uintptr_t>(map.keys) & 15) == 0) {
+        const longlong2* p = reinterpret_cast<const longlong2*>(map.keys + s0);
+#pragma unroll
+        for (int h = 0; h < CL_PER / 2; ++h) {
+            longlong2 x = p[h];
+            k[2 * h] = x.x;
+            k[2 * h + 1] = x.y;
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < CL_PER; ++u) k[u] = s0 + u < map.cap ? map.keys[s0 + u] : EMPTY_KEY;
     }
-    int c = __syncthreads_count(f);
-    if (threadIdx.x == 0) tiles[blockIdx.x] = c;
+}
+
+// Exclusive scan of per-thread counts over the CTA (blockDim.x <= 1024); the CTA total in *tot.
+__device__ __forceinline__ int block_excl(int v, int* sm, int* tot) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    int inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    if (lane == 31) sm[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        int x = lane < nw ? sm[lane] : 0, xi = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int u = __shfl_up_sync(0xffffffffu, xi, o);
+            if (lane >= o) xi += u;
+        }
+        if (lane < nw) sm[lane] = xi - x;
+        if (lane == 31) sm[32] = xi;
+    }
+    __syncthreads();
+    int r = sm[w] + inc - v;
+    *tot = sm[32];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(CL_THREADS) k_classify_count(lw_map map, lw_view v, int min_count,
+                                                               int* __restrict__ tiles) {
+    __shared__ int sm[33];
+    const int64_t s0 = (int64_t)blockIdx.x * CL_TILE + (int64_t)threadIdx.x * CL_PER;
+    int64_t k[CL_PER];
+    load_keys(map, s0, k);
+    int c = 0;
+#pragma unroll
+    for (int u = 0; u < CL_PER; ++u) {
+        float wx, wy, wz;
+        if (k[u] != EMPTY_KEY && classify_flag_key(map, s0 + u, k[u], v, min_count, wx, wy, wz)) ++c;
+    }
+    int tot;
+    block_excl(c, sm, &tot);
+    if (threadIdx.x == 0) tiles[blockIdx.x] = tot;
 }
 
 // In-place exclusive scan of nt tile counts by one CTA; tiles[nt] receives the total.
@@ -550,33 +603,45 @@ __global__ void k_scan_tiles(int* tiles, int nt, int* total_out) {
     }
 }
 
-__global__ void k_classify_scatter(lw_map map, lw_view v, int min_count, const int* __restrict__ tiles,
-                                   float* __restrict__ out_xyz, uint32_t* __restrict__ out_attr,
-                                   float* __restrict__ out_t, int* __restrict__ out_dyn) {
+__global__ void __launch_bounds__(CL_THREADS) k_classify_scatter(lw_map map, lw_view v, int min_count,
+                                                                 const int* __restrict__ tiles,
+                                                                 float* __restrict__ out_xyz,
+                                                                 uint32_t* __restrict__ out_attr,
+                                                                 float* __restrict__ out_t, int* __restrict__ out_dyn) {
     __shared__ int sm[33];
-    int64_t s = (int64_t)blockIdx.x * MTILE + threadIdx.x;
-    int f = 0;
-    float wx = 0.f, wy = 0.f, wz = 0.f;
-    if (s < map.cap) f = classify_flag(map, s, v, min_count, wx, wy, wz) ? 1 : 0;
+    const int64_t s0 = (int64_t)blockIdx.x * CL_TILE + (int64_t)threadIdx.x * CL_PER;
+    int64_t k[CL_PER];
+    load_keys(map, s0, k);
+    float wx[CL_PER], wy[CL_PER], wz[CL_PER];
+    unsigned flags = 0;
+#pragma unroll
+    for (int u = 0; u < CL_PER; ++u)
+        if (k[u] != EMPTY_KEY && classify_flag_key(map, s0 + u, k[u], v, min_count, wx[u], wy[u], wz[u]))
+            flags |= 1u << u;
     int tot;
-    int r = block_rank(f, sm, &tot);
-    if (!f) return;
-    int j = tiles[blockIdx.x] + r;
-    int c = map.cnt[s];
-    int n = c < LW_MAP_CAP ? c : LW_MAP_CAP;
-    int refl = (int)((double)map.acc[4 * s + 3] / (double)n + 0.5);
-    if (refl > 255) refl = 255;
-    out_xyz[3 * (int64_t)j + 0] = wx;
-    out_xyz[3 * (int64_t)j + 1] = wy;
-    out_xyz[3 * (int64_t)j + 2] = wz;
-    out_attr[j] = (uint32_t)refl;  // mean reflectivity only: tag, return and device mean nothing for a voxel
-    out_t[j] = map.last[s];
-    int dyn = 0;
-    if (transient(c, map.miss[s], v) != 0)
-        dyn = 1;
-    else if (settled_near(ifloor(wx * v.inv_voxel), ifloor(wy * v.inv_voxel), ifloor(wz * v.inv_voxel), v, map) == 0)
-        dyn = 1;
-    out_dyn[j] = dyn;
+    int j = tiles[blockIdx.x] + block_excl(__popc(flags), sm, &tot);
+#pragma unroll
+    for (int u = 0; u < CL_PER; ++u) {
+        if (!((flags >> u) & 1u)) continue;
+        const int64_t s = s0 + u;
+        int c = map.cnt[s];
+        int n = c < LW_MAP_CAP ? c : LW_MAP_CAP;
+        int refl = (int)((double)map.acc[4 * s + 3] / (double)n + 0.5);
+        if (refl > 255) refl = 255;
+        out_xyz[3 * (int64_t)j + 0] = wx[u];
+        out_xyz[3 * (int64_t)j + 1] = wy[u];
+        out_xyz[3 * (int64_t)j + 2] = wz[u];
+        out_attr[j] = (uint32_t)refl;  // mean reflectivity only: tag, return and device mean nothing for a voxel
+        out_t[j] = map.last[s];
+        int dyn = 0;
+        if (transient(c, map.miss[s], v) != 0)
+            dyn = 1;
+        else if (settled_near(ifloor(wx[u] * v.inv_voxel), ifloor(wy[u] * v.inv_voxel), ifloor(wz[u] * v.inv_voxel), v,
+                              map) == 0)
+            dyn = 1;
+        out_dyn[j] = dyn;
+        ++j;
+    }
 }
 
 // Frame id of each staged point: floor(max(t, 0) * inv_dt), 0 when inv_dt <= 0 (gpu.py:340-348).
@@ -676,11 +741,11 @@ int lw_map_build(const lw_map* map, const lw_view* v, int32_t min_count, float* 
     if (!v || !out_xyz || !out_attr || !out_t || !out_dyn || !tiles || !count_dev)
         return set_error(LW_EINVAL, "lw_map_build: null argument");
     cudaStream_t s = (cudaStream_t)stream;
-    int nt = blocks_for(map->cap, MTILE);
+    int nt = blocks_for(map->cap, CL_TILE);  // <= cap / 1024 + 1 tiles: within the caller's buffer
     ProfScope prof("map_build", s);
-    k_classify_count<<<nt, MTILE, 0, s>>>(*map, *v, min_count, tiles);
+    k_classify_count<<<nt, CL_THREADS, 0, s>>>(*map, *v, min_count, tiles);
     k_scan_tiles<<<1, 1024, 0, s>>>(tiles, nt, count_dev);
-    k_classify_scatter<<<nt, MTILE, 0, s>>>(*map, *v, min_count, tiles, out_xyz, out_attr, out_t, out_dyn);
+    k_classify_scatter<<<nt, CL_THREADS, 0, s>>>(*map, *v, min_count, tiles, out_xyz, out_attr, out_t, out_dyn);
     LW_LAUNCHED("lw_map_build");
     count_launches(3);
     return LW_OK;
