@@ -918,6 +918,169 @@ def run_localize(a, rank: int, world: int, local: int):
     print(json.dumps(line))
 
 
+# ---- coarse hypothesis scoring (k_score_grid) --------------------------------------------------------------------
+
+COARSE_SPACING = 0.03  # prior-map sample spacing (m): the scores read only the grid's distance field
+COARSE_PTS = 1024      # scan points per hypothesis (localize.py:352, n_coarse_pts)
+COARSE_HEIGHTS = 8     # sensor heights per gravity candidate (localize.py:346)
+
+
+def coarse_workload():
+    """The office prior map, one 360-degree scan from a free pose and its 1024-point subset (one point per 15 cm
+    voxel first, as localize.py:630-634 spreads it), and 8 sensor heights around the true one."""
+    from livox_warp import synth
+
+    scene = synth.office(LOC_SEED)
+    xyz, nrm = synth.sample_surfaces(scene, COARSE_SPACING, LOC_SEED, jitter=0.002)
+    T = synth.free_poses(scene, 1, LOC_POSE_SEED, z=LOC_Z, margin=0.6)[0]
+    scan = synth.spin_scan(scene, T, 60000, LOC_POSE_SEED + 7)
+    rng = np.random.default_rng(0)
+    _, first = np.unique(np.floor(scan / 0.15).astype(np.int64), axis=0, return_index=True)
+    spread = scan[np.sort(first)]
+    pts = spread[rng.choice(len(spread), min(COARSE_PTS, len(spread)), replace=False)].astype(np.float32)
+    heights = [round(float(T[2, 3]) + 0.08 * k, 3) for k in range(-3, COARSE_HEIGHTS - 3)]
+    return {"xyz": xyz, "nrm": nrm, "T": T, "pts": pts, "heights": heights}
+
+
+def run_coarse(a, rank: int, world: int, local: int):
+    from oracle import oracle as _o
+
+    w = coarse_workload()
+    metric = "coarse global-search hypotheses/s (distance-field soft count of 1024 scan points per hypothesis)"
+    n_yaw, dyaw, tau, free_cm, step = 180, math.radians(2.0), 25.0, 10.0, 0.25
+    config = {"workload": f"coarse global search: office 40x30x3 m prior map ({len(w['xyz']):,} pts at "
+                          f"{COARSE_SPACING * 1e3:.0f} mm, 5 cm grid), every free position on a {step} m xy grid x "
+                          f"{COARSE_HEIGHTS} heights x {n_yaw} headings, {len(w['pts'])} scan points each, "
+                          f"tau {tau:.0f} cm, free {free_cm:.0f} cm (localize.py:413-448)",
+              "scan_points": int(len(w["pts"])), "headings": n_yaw, "heights": COARSE_HEIGHTS,
+              "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{a.gpus}"}
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        from livox_warp.localize import coarse_positions
+        from livox_warp.mapgrid import PriorGrid
+
+        threads = _o.host_cores()
+        prep = PriorGrid.prepare({"xyz": w["xyz"], "normal": w["nrm"]})  # host numpy
+        og = _o.PriorGrid(prep)
+        pos, nx, ny = coarse_positions(prep["lo"], prep["hi"], w["heights"], step)
+        sample = pos[::97]
+        t0 = time.perf_counter()
+        og.score_grid(w["pts"], sample, n_yaw, 0.0, dyaw, tau, free_cm, ref=True, nthreads=threads)
+        secs = time.perf_counter() - t0
+        v = len(sample) * n_yaw / secs
+        print(json.dumps({"impl": "reference", "metric": metric, "value": round(v, 3), "unit": "hypotheses/s",
+                          "n_gpus": a.gpus, "steps": 1, "warmup": 0, "ms_per_step": round(1e3 * secs, 3),
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                          "data": "synthetic", "config": config,
+                          "cpu_baseline": {"value": round(v, 3), "unit": "hypotheses/s", "cores": threads,
+                                           "kind": "port", "sample": f"every 97th position ({len(sample)}) x "
+                                                                     f"{n_yaw} headings through the CPU restatement"},
+                          "e2e": {"value": round(v, 3), "unit": "hypotheses/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+    import torch
+
+    from livox_warp import _lib
+    from livox_warp.localize import GlobalLocalizer, coarse_positions, score_grid
+    from livox_warp.mapgrid import PriorGrid
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    grid = PriorGrid({"xyz": w["xyz"], "normal": w["nrm"]}, device)
+    grid.build()
+    loc = GlobalLocalizer(grid, device, hyp_cap=16, pts_cap=1 << 12)
+    pos, nx, ny = coarse_positions(grid.lo, grid.hi, w["heights"], step)
+    n_hyp = len(pos) * n_yaw
+    stream = torch.cuda.current_stream(device)
+    d_pts = torch.from_numpy(w["pts"]).to(device)
+    d_pos = torch.from_numpy(pos).to(device)
+    out = torch.empty(n_hyp, dtype=torch.float32, device=device)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+
+    def dev_step():
+        score_grid(grid, d_pts, d_pos, n_yaw, 0.0, dyaw, tau, free_cm, out, stream)
+
+    for _ in range(a.warmup):
+        dev_step()
+    torch.cuda.synchronize(device)
+    clocks = Clocks(local)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    _lib.launches(reset=True)
+    clocks.start()
+    torch.cuda.synchronize(device)
+    for j in range(a.steps):
+        flush.fill_(float(j))
+        evs[j][0].record(stream)
+        dev_step()
+        evs[j][1].record(stream)
+    torch.cuda.synchronize(device)
+    clk = clocks.stop()
+    launches = _lib.launches()
+    step_ms = np.array([x.elapsed_time(y) for x, y in evs])
+    ms_total = max_over_ranks(float(step_ms.sum()), device)
+    value = replica_rate(a.steps * n_hyp, world, ms_total)
+    sc = out.cpu().numpy()
+    # e2e through GlobalLocalizer._coarse: host scan in, H2D of scan and positions, every score back to the host
+    for _ in range(2):
+        loc._coarse(stream, w["pts"], w["heights"])
+    torch.cuda.synchronize(device)
+    e_steps = max(3, min(a.steps, 10))
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        pos_e, shape, _, sc_e = loc._coarse(stream, w["pts"], w["heights"])
+    e_s = max_over_ranks(time.perf_counter() - t0, device)
+    if rank != 0:
+        return
+    assert np.array_equal(sc_e, sc), "the public call and the timed launches disagree"
+    # parity on a sample of positions, and the CPU baseline on it (the oracle's grid over the same prepared
+    # arrays; the distance field is the device's, which the parity tests hold bit-exact to the oracle's flood)
+    threads = _o.host_cores()
+    og = _o.PriorGrid(grid._host, build=False)
+    og.df[:] = grid.df.cpu().numpy()
+    sample = np.arange(0, len(pos), 97)
+    t0 = time.perf_counter()
+    want = og.score_grid(w["pts"], pos[sample], n_yaw, 0.0, dyaw, tau, free_cm, nthreads=threads)
+    secs = time.perf_counter() - t0
+    got = sc.reshape(len(pos), n_yaw)[sample].reshape(-1)
+    best = int(np.argmax(sc))
+    bp, by = pos[best // n_yaw], (best % n_yaw) * dyaw
+    T = w["T"]
+    yaw = math.atan2(T[1, 0], T[0, 0]) % (2 * math.pi)
+    avg_ms = ms_total / a.steps
+    # the unique bytes a launch must move: the distance field, the scan, the positions and every score
+    ubytes = int(grid.ncell + 12 * len(w["pts"]) + 12 * len(pos) + 4 * n_hyp)
+    peak = measured_peak()
+    ach = ubytes / (avg_ms * 1e-3) / 1e9
+    roof = {"kernel": "k_score_grid", "bound": "hbm", "achieved": round(ach, 3), "peak": peak["hbm_gbs"],
+            "unit": "GB/s", "frac": round(ach / peak["hbm_gbs"], 5), "traffic": None, "peak_source": peak["source"],
+            "avg_launch_us": round(avg_ms * 1e3, 2), "algorithmic_bytes_per_launch": ubytes,
+            "byte_gathers_per_launch": int(n_hyp * len(w["pts"])),
+            "gathers_per_s": round(n_hyp * len(w["pts"]) / (avg_ms * 1e-3), 1),
+            "limiter": "one 1-byte distance-field gather per (hypothesis, point), served from L1 / L2 (the 5 cm "
+                       "field fits in L2); HBM moves only the unique bytes"}
+    line = {"metric": metric, "value": round(value, 3), "unit": "hypotheses/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(avg_ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 poses, int32 sums", "data": "synthetic",
+            "config": config, "hypotheses_per_step": int(n_hyp),
+            "best_vs_true": {"xy_m": round(float(np.linalg.norm(bp[:2] - T[:2, 3])), 4),
+                             "z_m": round(float(abs(bp[2] - T[2, 3])), 4),
+                             "yaw_deg": round(math.degrees(abs((by - yaw + math.pi) % (2 * math.pi) - math.pi)), 3)},
+            "bit_exact_vs_oracle_sample": bool(np.array_equal(got, want)),
+            "step_ms_p50_p99": [round(float(np.percentile(step_ms, 50)), 4),
+                                round(float(np.percentile(step_ms, 99)), 4)],
+            "roofline": roof,
+            "cpu_baseline": {"value": round(len(sample) * n_yaw / secs, 3), "unit": "hypotheses/s",
+                             "cores": threads, "kind": "port",
+                             "sample": f"every 97th position ({len(sample)}) x {n_yaw} headings through the CPU "
+                                       f"oracle (C++/OpenMP), {secs:.1f} s"},
+            "e2e": {"value": round(world * e_steps * n_hyp / e_s, 3), "unit": "hypotheses/s",
+                    "h2d_bytes_per_step": int(12 * len(w["pts"]) + 12 * len(pos)),
+                    "d2h_bytes_per_step": int(4 * n_hyp)},
+            "gpu_launches": int(launches), "clocks": clk}
+    print(json.dumps(line))
+
+
 # ---- main -------------------------------------------------------------------------------------------------------
 
 
@@ -929,7 +1092,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=("sequence", "localize", "frame", "learned"), default="sequence")
+    ap.add_argument("--workload", choices=("sequence", "localize", "frame", "learned", "coarse"),
+                    default="sequence")
     ap.add_argument("--learn-epochs", type=int, default=40, help="learned: training epochs")
     ap.add_argument("--loc-hyp", type=int, default=256, help="localize: hypotheses (a smaller profiling case)")
     ap.add_argument("--loc-spacing", type=float, default=0.015, help="localize: prior-map sample spacing (m)")
@@ -948,6 +1112,9 @@ def main():
         return
     if a.workload == "learned":
         run_learned(a, rank, world, local)
+        return
+    if a.workload == "coarse":
+        run_coarse(a, rank, world, local)
         return
     n_frames = a.warmup + a.steps + 1
     metric = "ICP sequence odometry frames/s (deskew + GN ICP + keyframe insert + map insert + carve)"

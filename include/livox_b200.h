@@ -364,6 +364,25 @@ int lw_prior_grid_build(lw_prior_grid* g, void* stream);
 int lw_prior_distances(const lw_prior_grid* g, const float* pts, int64_t n, const double* T_host, float* out,
                        void* stream);
 
+/* Coarse search scores (localize.py:55-96, k_score_grid): for every position pos[i] (float xyz, i < n_pos) and
+ * heading yaw0 + j dyaw (j < n_yaw <= LW_SCORE_MAX_YAW), the soft count of the n_pts scan points pts [n_pts*3]
+ * (gravity-aligned sensor frame) near the map: the sum over points whose cell distance d (cm, the grid's df) is
+ * below tau_cm of 1 - d^2 / tau_cm^2, formed exactly from integer sums (the reference adds float32 terms in point
+ * order). out[i*n_yaw + j]; -1 where the position lies outside the grid or within free_cm of a mapped surface.
+ * Needs the built grid (df). */
+#define LW_SCORE_MAX_YAW 1024
+int lw_score_grid(const lw_prior_grid* g, const float* pts, int32_t n_pts, const float* pos, int64_t n_pos,
+                  int32_t n_yaw, float yaw0, float dyaw, float tau_cm, float free_cm, float* out, void* stream);
+
+/* The same soft count for a list of hypotheses hyp [n_hyp*4] = (x, y, z, yaw), 16-byte aligned
+ * (localize.py:99-123, k_score_list). */
+int lw_score_list(const lw_prior_grid* g, const float* pts, int32_t n_pts, const float* hyp, int64_t n_hyp,
+                  float tau_cm, float* out, void* stream);
+
+/* The headings' float32 cosines and sines lw_score_grid poses points with: yaw_j = yaw0 + j dyaw in float32
+ * (localize.py:79), its cosine and sine in float64 rounded to float32. Host only; c and s hold n_yaw floats. */
+void lw_score_yaw_table(int32_t n_yaw, float yaw0, float dyaw, float* c, float* s);
+
 /* Buffers of the batched ICP: every hypothesis has its own range of points (tile_lo .. scan_end; hypotheses may
  * share one scan) and pose (T, in and out). The points are cut into tiles of at most `tile` points that never
  * span two hypotheses: hypothesis h owns tiles hyp_tile[h] .. hyp_tile[h+1]. */

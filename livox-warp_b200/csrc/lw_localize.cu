@@ -14,6 +14,8 @@
 // each hypothesis sums its tiles in a fixed order and solves its 6x6 system (Cholesky, float64); after a second
 // barrier every CTA reads the largest step of the iteration and the schedule stage ends when it is below 2e-4
 // (localize.py:536-552). The evaluation counts of localize.py:182-205 follow in the same launch.
+#include <cmath>
+
 #include "lw_common.cuh"
 #include "lw_linalg.cuh"
 
@@ -583,6 +585,121 @@ __global__ void k_loc_reset(lw_loc_batch b, int n_hyp, int max_iters) {
 
 using namespace lw;
 
+namespace lw {
+
+// ---- coarse hypothesis scores (localize.py:55-123, k_score_grid / k_score_list) -----------------------------
+// A thread per hypothesis, the scan points staged in shared memory in chunks (every thread reads the same point at
+// once). The soft count sum over points with d < tau of (1 - d^2 / tau^2) is kept as two integers -- the number of
+// such points and the sum of d^2 (d is a whole number of cm) -- and formed once at the end in float64: exact and
+// independent of the summation order, where the reference adds float32 terms in point order (the two differ by
+// that sum's rounding only). Headings' cosine and sine come from the host (YawTab) so that every implementation
+// poses the points with the same float32 values.
+constexpr int SC_THREADS = 256;
+constexpr int SC_CHUNK = 1024;
+
+struct YawTab {
+    float c[LW_SCORE_MAX_YAW], s[LW_SCORE_MAX_YAW];
+};
+
+__device__ __forceinline__ void score_chunk(const lw_prior_grid& g, const float* __restrict__ px,
+                                            const float* __restrict__ py, const float* __restrict__ pz, int m,
+                                            float cx, float cy, float cz, float co, float si, float tau, int& n_in,
+                                            int& sum_d2) {
+    const uint8_t* __restrict__ df = g.df;
+#pragma unroll 4
+    for (int k = 0; k < m; ++k) {
+        const float wx = cx + co * px[k] - si * py[k];
+        const float wy = cy + si * px[k] + co * py[k];
+        const float wz = cz + pz[k];
+        int ix, iy, iz;
+        grid_idx(g, wx, wy, wz, ix, iy, iz);
+        const int64_t j = grid_flat(g, ix, iy, iz);
+        if (j >= 0) {
+            const int d = __ldg(df + j);
+            if ((float)d < tau) {
+                ++n_in;
+                sum_d2 += d * d;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void stage_pts(const float* __restrict__ pts, int base, int m, float* px, float* py,
+                                          float* pz) {
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        px[k] = pts[3 * (int64_t)(base + k) + 0];
+        py[k] = pts[3 * (int64_t)(base + k) + 1];
+        pz[k] = pts[3 * (int64_t)(base + k) + 2];
+    }
+}
+
+__device__ __forceinline__ float soft_count(int n_in, int sum_d2, float tau) {
+    return (float)((double)n_in - (double)sum_d2 / ((double)tau * (double)tau));
+}
+
+__global__ void __launch_bounds__(SC_THREADS) k_score_grid(lw_prior_grid g, const float* __restrict__ pts, int n_pts,
+                                                           const float* __restrict__ pos, int64_t n_hyp, int n_yaw,
+                                                           const YawTab yt, float tau, float free_cm,
+                                                           float* __restrict__ out) {
+    __shared__ float px[SC_CHUNK], py[SC_CHUNK], pz[SC_CHUNK];
+    const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool live = h < n_hyp;
+    float cx = 0.f, cy = 0.f, cz = 0.f, co = 1.f, si = 0.f;
+    if (live) {
+        const int64_t ip = h / n_yaw;
+        const int iyaw = (int)(h - ip * n_yaw);
+        cx = pos[3 * ip];
+        cy = pos[3 * ip + 1];
+        cz = pos[3 * ip + 2];
+        co = yt.c[iyaw];
+        si = yt.s[iyaw];
+        int ix, iy, iz;
+        grid_idx(g, cx, cy, cz, ix, iy, iz);
+        const int64_t cc = grid_flat(g, ix, iy, iz);
+        // the sensor outside the grid or inside a mapped surface
+        if (cc < 0 || (float)g.df[cc] < free_cm) {
+            out[h] = -1.0f;
+            live = false;
+        }
+    }
+    int n_in = 0, sum_d2 = 0;
+    for (int base = 0; base < n_pts; base += SC_CHUNK) {
+        const int m = min(SC_CHUNK, n_pts - base);
+        __syncthreads();
+        stage_pts(pts, base, m, px, py, pz);
+        __syncthreads();
+        if (live) score_chunk(g, px, py, pz, m, cx, cy, cz, co, si, tau, n_in, sum_d2);
+    }
+    if (live) out[h] = soft_count(n_in, sum_d2, tau);
+}
+
+__global__ void __launch_bounds__(SC_THREADS) k_score_list(lw_prior_grid g, const float* __restrict__ pts, int n_pts,
+                                                           const float4* __restrict__ hyp, int64_t n_hyp, float tau,
+                                                           float* __restrict__ out) {
+    __shared__ float px[SC_CHUNK], py[SC_CHUNK], pz[SC_CHUNK];
+    const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = h < n_hyp;
+    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+    float co = 1.f, si = 0.f;
+    if (live) {
+        q = hyp[h];
+        // cos / sin in float64, rounded once: the heading as the host would pose it
+        co = (float)cos((double)q.w);
+        si = (float)sin((double)q.w);
+    }
+    int n_in = 0, sum_d2 = 0;
+    for (int base = 0; base < n_pts; base += SC_CHUNK) {
+        const int m = min(SC_CHUNK, n_pts - base);
+        __syncthreads();
+        stage_pts(pts, base, m, px, py, pz);
+        __syncthreads();
+        if (live) score_chunk(g, px, py, pz, m, q.x, q.y, q.z, co, si, tau, n_in, sum_d2);
+    }
+    if (live) out[h] = soft_count(n_in, sum_d2, tau);
+}
+
+}  // namespace lw
+
 static int check_grid(const lw_prior_grid* g, const char* who) {
     if (!g || !g->xyz || !g->start || !g->nn || g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || g->cell <= 0.0f)
         return set_error(LW_EINVAL, "%s: incomplete prior grid", who);
@@ -633,6 +750,54 @@ int lw_prior_distances(const lw_prior_grid* g, const float* pts, int64_t n, cons
     LW_LAUNCHED("lw_prior_distances");
     count_launches(1);
     return LW_OK;
+}
+
+int lw_score_grid(const lw_prior_grid* g, const float* pts, int32_t n_pts, const float* pos, int64_t n_pos,
+                  int32_t n_yaw, float yaw0, float dyaw, float tau_cm, float free_cm, float* out, void* stream) {
+    int r = check_grid(g, "lw_score_grid");
+    if (r != LW_OK) return r;
+    if (!g->df || !pts || !pos || !out || n_pts < 0 || n_pos < 0)
+        return set_error(LW_EINVAL, "lw_score_grid: bad arguments");
+    if (n_yaw < 1 || n_yaw > LW_SCORE_MAX_YAW)
+        return set_error(LW_EINVAL, "lw_score_grid: n_yaw %d outside [1, %d]", n_yaw, LW_SCORE_MAX_YAW);
+    if (!(tau_cm > 0.0f)) return set_error(LW_EINVAL, "lw_score_grid: tau_cm must be positive");
+    if ((int64_t)n_pts * 255 * 255 > 0x7FFFFFFF)
+        return set_error(LW_ECAPACITY, "lw_score_grid: %d points overflow the int32 sums", n_pts);
+    const int64_t n_hyp = n_pos * (int64_t)n_yaw;
+    if (n_hyp == 0) return LW_OK;
+    YawTab yt;
+    lw_score_yaw_table(n_yaw, yaw0, dyaw, yt.c, yt.s);
+    k_score_grid<<<(unsigned)((n_hyp + SC_THREADS - 1) / SC_THREADS), SC_THREADS, 0, (cudaStream_t)stream>>>(
+        *g, pts, n_pts, pos, n_hyp, n_yaw, yt, tau_cm, free_cm, out);
+    LW_LAUNCHED("lw_score_grid");
+    count_launches(1);
+    return LW_OK;
+}
+
+int lw_score_list(const lw_prior_grid* g, const float* pts, int32_t n_pts, const float* hyp, int64_t n_hyp,
+                  float tau_cm, float* out, void* stream) {
+    int r = check_grid(g, "lw_score_list");
+    if (r != LW_OK) return r;
+    if (!g->df || !pts || !hyp || !out || n_pts < 0 || n_hyp < 0)
+        return set_error(LW_EINVAL, "lw_score_list: bad arguments");
+    if (((uintptr_t)hyp & 15) != 0) return set_error(LW_EINVAL, "lw_score_list: hyp must be 16-byte aligned");
+    if (!(tau_cm > 0.0f)) return set_error(LW_EINVAL, "lw_score_list: tau_cm must be positive");
+    if ((int64_t)n_pts * 255 * 255 > 0x7FFFFFFF)
+        return set_error(LW_ECAPACITY, "lw_score_list: %d points overflow the int32 sums", n_pts);
+    if (n_hyp == 0) return LW_OK;
+    k_score_list<<<(unsigned)((n_hyp + SC_THREADS - 1) / SC_THREADS), SC_THREADS, 0, (cudaStream_t)stream>>>(
+        *g, pts, n_pts, reinterpret_cast<const float4*>(hyp), n_hyp, tau_cm, out);
+    LW_LAUNCHED("lw_score_list");
+    count_launches(1);
+    return LW_OK;
+}
+
+void lw_score_yaw_table(int32_t n_yaw, float yaw0, float dyaw, float* c, float* s) {
+    for (int j = 0; j < n_yaw; ++j) {
+        const float yaw = yaw0 + (float)j * dyaw;  // float32, as localize.py:79
+        c[j] = (float)std::cos((double)yaw);
+        s[j] = (float)std::sin((double)yaw);
+    }
 }
 
 int lw_loc_icp_batch(const lw_prior_grid* g, lw_loc_batch* b, int32_t n_hyp, int32_t n_tiles, int32_t tile,

@@ -102,6 +102,7 @@ class LocBatch(C.Structure):
     _fields_ = [(n, P) for n in PTRS] + [("pts_cap", i64), ("moved_cap", i32), ("grid_cap", i32)]
 
 
+SCORE_MAX_YAW = 1024  # headings lw_score_grid takes per launch (LW_SCORE_MAX_YAW)
 NET_P = 1024
 NET_OFF = {"W1": 0, "B1": 192, "W2": 256, "B2": 8448, "W3": 8576, "B3": 41344, "WH1": 41600, "BH1": 107136,
            "WH2": 107264, "BH2": 108032}
@@ -180,6 +181,9 @@ _SIGS = {
                                    C.POINTER(GnScratch), C.POINTER(PoseTable), i32, P, i64, C.POINTER(InitNet),
                                    C.POINTER(NetWork), P]),
     "lw_prior_distances": (i32, [C.POINTER(PriorGrid), P, i64, C.POINTER(f64), P, P]),
+    "lw_score_grid": (i32, [C.POINTER(PriorGrid), P, i32, P, i64, i32, f32, f32, f32, f32, P, P]),
+    "lw_score_list": (i32, [C.POINTER(PriorGrid), P, i32, P, i64, f32, P, P]),
+    "lw_score_yaw_table": (None, [i32, f32, f32, P, P]),
     "lw_loc_icp_batch": (i32, [C.POINTER(PriorGrid), C.POINTER(LocBatch), i32, i32, i32, i32, C.POINTER(f64),
                                C.POINTER(i32), f32, i32, i32, i32, P]),
 }

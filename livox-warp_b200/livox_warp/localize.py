@@ -8,6 +8,10 @@ launch (lw_loc_icp_batch): each hypothesis may have its own scan of any length, 
 SE(3) update happen on the device, and the stage stops when no hypothesis moved 2e-4 (:551), exactly as the
 reference's host loop decides.
 
+The coarse search's hypothesis scores (k_score_grid / k_score_list, localize.py:55-123) are `score_grid` and
+`score_list`: a thread per hypothesis with the scan points in shared memory, the soft count kept as integer sums
+(exact, independent of the summation order) and rounded once.
+
 Precision: the residuals and Jacobians run in float32 on points re-centred on the hypothesis' translation; the
 tile sums, the normal equations, the Cholesky solve and the poses are float64 (the reference sends float32
 poses to the device and solves with numpy in float64).
@@ -212,12 +216,59 @@ class LocBatch:
         return nt
 
 
+def _f32_rows(x, cols: int, name: str) -> torch.Tensor:
+    if not (isinstance(x, torch.Tensor) and x.is_cuda and x.dtype == torch.float32 and x.is_contiguous()
+            and x.dim() == 2 and x.shape[1] == cols):
+        raise ValueError(f"{name} must be a contiguous [n, {cols}] float32 CUDA tensor")
+    return x
+
+
+def score_grid(grid: PriorGrid, pts: torch.Tensor, pos: torch.Tensor, n_yaw: int, yaw0: float, dyaw: float,
+               tau_cm: float, free_cm: float, out: torch.Tensor, stream=None):
+    """k_score_grid (localize.py:55-96): for every position pos[i] ([n, 3]) and heading yaw0 + j dyaw, the soft
+    count of the scan points `pts` ([m, 3], gravity-aligned sensor frame) within tau_cm of the map, into
+    out[i * n_yaw + j]; -1 where the sensor would sit outside the grid or within free_cm of a mapped surface."""
+    _f32_rows(pts, 3, "pts")
+    _f32_rows(pos, 3, "pos")
+    if out.dtype != torch.float32 or not out.is_contiguous() or out.numel() < pos.shape[0] * n_yaw:
+        raise ValueError("out must hold n_pos * n_yaw float32")
+    _lib.call("lw_score_grid", C.byref(grid.struct), _lib.ptr(pts), int(pts.shape[0]), _lib.ptr(pos),
+              int(pos.shape[0]), int(n_yaw), float(yaw0), float(dyaw), float(tau_cm), float(free_cm), _lib.ptr(out),
+              _lib.stream_ptr(stream))
+
+
+def score_list(grid: PriorGrid, pts: torch.Tensor, hyp: torch.Tensor, tau_cm: float, out: torch.Tensor, stream=None):
+    """k_score_list (localize.py:99-123): the same soft count for (x, y, z, yaw) hypotheses `hyp` ([n, 4])."""
+    _f32_rows(pts, 3, "pts")
+    _f32_rows(hyp, 4, "hyp")
+    if out.dtype != torch.float32 or not out.is_contiguous() or out.numel() < hyp.shape[0]:
+        raise ValueError("out must hold n float32")
+    _lib.call("lw_score_list", C.byref(grid.struct), _lib.ptr(pts), int(pts.shape[0]), _lib.ptr(hyp),
+              int(hyp.shape[0]), float(tau_cm), _lib.ptr(out), _lib.stream_ptr(stream))
+
+
+def coarse_positions(lo, hi, heights, xy_step: float) -> tuple[np.ndarray, int, int]:
+    """Every position of the xy grid over [lo, hi] at each height (localize.py:415-419): x outer, y inner, one
+    block per height; returns (pos [n, 3] float32, nx, ny)."""
+    gx = np.arange(lo[0], hi[0] + 1e-6, xy_step)
+    gy = np.arange(lo[1], hi[1] + 1e-6, xy_step)
+    X, Y = np.meshgrid(gx, gy, indexing="ij")
+    pos = np.concatenate([np.stack([X.ravel(), Y.ravel(), np.full(X.size, z)], 1) for z in heights])
+    return pos.astype(np.float32), len(gx), len(gy)
+
+
 class GlobalLocalizer:
     """Batched ICP against a PriorGrid: refine() is the reference's pose-tracking step (localize.py:569-612);
     register_batch() registers many hypotheses, each with its own scan, in one launch."""
 
     PTS_CAP = 1 << 17  # scan points after 5 cm thinning, localize.py:322
     ICP_CAP = 16  # poses refine() takes together, localize.py:325
+    # coarse search tuning (localize.py:344-351)
+    xy_step = 0.25
+    yaw_step_deg = 2.0
+    tau_coarse = 25.0  # cm
+    tau_mid = 12.0
+    free_cm = 10.0  # the sensor sits at least this far from any mapped surface
 
     def __init__(self, grid: PriorGrid, device=None, hyp_cap: int = 1024, pts_cap: int = 1 << 23,
                  tuner: Autotuner | None = None):
@@ -230,6 +281,37 @@ class GlobalLocalizer:
         self.seed = 0  # refine() draws its subset from a fresh generator with this seed
         self.last_tile = 0
         self._graphs: dict = {}
+
+    # ---- the coarse search's scores ------------------------------------------------------------------
+
+    def _coarse(self, stream, pts_g: np.ndarray, heights):
+        """Every free-space position on the xy grid at the given heights x every heading, scored in one launch
+        (localize.py:413-448). Returns (pos, (n_heights, nx, ny, n_yaw), dyaw, scores)."""
+        g = self.grid
+        pos, nx, ny = coarse_positions(g.lo, g.hi, heights, self.xy_step)
+        n_yaw = int(round(360.0 / self.yaw_step_deg))
+        dyaw = math.radians(self.yaw_step_deg)
+        stream = stream if stream is not None else torch.cuda.current_stream(self.device)
+        with torch.cuda.stream(stream):
+            d_pts = torch.from_numpy(np.ascontiguousarray(pts_g, dtype=np.float32)).to(self.device, non_blocking=True)
+            d_pos = torch.from_numpy(pos).to(self.device, non_blocking=True)
+            out = torch.empty(len(pos) * n_yaw, dtype=torch.float32, device=self.device)
+            score_grid(g, d_pts, d_pos, n_yaw, 0.0, dyaw, self.tau_coarse, self.free_cm, out, stream)
+            sc = out.cpu().numpy()
+        return pos, (len(heights), nx, ny, n_yaw), dyaw, sc
+
+    def _score_list(self, stream, pts, m: int, hyps: np.ndarray, tau: float) -> np.ndarray:
+        """The soft counts of (x, y, z, yaw) hypotheses for the first m points of `pts` (localize.py:507-515)."""
+        stream = stream if stream is not None else torch.cuda.current_stream(self.device)
+        with torch.cuda.stream(stream):
+            d_pts = pts if isinstance(pts, torch.Tensor) else torch.from_numpy(
+                np.ascontiguousarray(pts, dtype=np.float32)).to(self.device, non_blocking=True)
+            d_pts = d_pts[:m].contiguous()
+            d_hyp = torch.from_numpy(np.ascontiguousarray(hyps, dtype=np.float32).reshape(-1, 4)).to(
+                self.device, non_blocking=True)
+            out = torch.empty(d_hyp.shape[0], dtype=torch.float32, device=self.device)
+            score_list(self.grid, d_pts, d_hyp, tau, out, stream)
+            return out.cpu().numpy()
 
     # ---- the launch ------------------------------------------------------------------------------
 

@@ -16,6 +16,7 @@
 // Parity of this restatement against the reference itself is unpinned: the reference needs NVIDIA Warp,
 // which is not installed, and ships no golden vectors for these kernels.
 #include <math.h>
+#include <cmath>
 #include <stdint.h>
 #include <string.h>
 #include <algorithm>
@@ -932,6 +933,108 @@ void or_prior_distances(const or_grid* g, const float* pts, int64_t n, const dou
             d = len3(wx - q[0], wy - q[1], wz - q[2]);
         }
         out[i] = d;
+    }
+}
+
+}  // extern "C"
+
+// ---- coarse hypothesis scores (localize.py:55-123, k_score_grid / k_score_list) --------------------------------
+// Two sums. By default the definition the library computes: the soft count formed exactly from the number of
+// points with d < tau and the sum of their d^2 (integers), rounded once. With ref, the reference's own sum: float32
+// terms 1 - d*d*inv_t2 added in point order. Both pose the points with the reference's expressions
+// (localize.py:86-88, 114-116) and the headings' cosines and sines taken in float64 and rounded to float32 (the
+// reference's float32 wp.cos / wp.sin may differ from those by an ulp).
+
+static inline int64_t og_at(const or_grid& g, float x, float y, float z) {  // grid_at mapgrid.py:53-56
+    return og_flat(g, (int)std::floor((x - g.origin[0]) * g.inv_cell), (int)std::floor((y - g.origin[1]) * g.inv_cell),
+                   (int)std::floor((z - g.origin[2]) * g.inv_cell));
+}
+
+static inline void og_score_sums(const or_grid& g, const uint8_t* df, const float* pts, int n_pts, float cx, float cy,
+                                 float cz, float co, float si, float tau, int& n_in, int& sum_d2) {
+    n_in = 0;
+    sum_d2 = 0;
+    for (int k = 0; k < n_pts; ++k) {
+        const float* p = pts + 3 * (int64_t)k;
+        const float wx = cx + co * p[0] - si * p[1];
+        const float wy = cy + si * p[0] + co * p[1];
+        const float wz = cz + p[2];
+        const int64_t j = og_at(g, wx, wy, wz);
+        if (j >= 0) {
+            const int d = df[j];
+            if ((float)d < tau) {
+                ++n_in;
+                sum_d2 += d * d;
+            }
+        }
+    }
+}
+
+static inline float og_score_ref(const or_grid& g, const uint8_t* df, const float* pts, int n_pts, float cx, float cy,
+                                 float cz, float co, float si, float tau) {
+    const float inv_t2 = 1.0f / (tau * tau);
+    float s = 0.0f;
+    for (int k = 0; k < n_pts; ++k) {
+        const float* p = pts + 3 * (int64_t)k;
+        const float wx = cx + co * p[0] - si * p[1];
+        const float wy = cy + si * p[0] + co * p[1];
+        const float wz = cz + p[2];
+        const int64_t j = og_at(g, wx, wy, wz);
+        if (j >= 0) {
+            const float d = (float)df[j];
+            if (d < tau) s += 1.0f - d * d * inv_t2;
+        }
+    }
+    return s;
+}
+
+extern "C" {
+
+void or_score_grid(const or_grid* gp, const uint8_t* df, const float* pts, int n_pts, const float* pos, int64_t n_pos,
+                   int n_yaw, float yaw0, float dyaw, float tau, float free_cm, int ref, float* out, int threads) {
+    const or_grid& g = *gp;
+    std::vector<float> c(n_yaw), sn(n_yaw);
+    for (int j = 0; j < n_yaw; ++j) {
+        const float yaw = yaw0 + (float)j * dyaw;
+        c[j] = (float)std::cos((double)yaw);
+        sn[j] = (float)std::sin((double)yaw);
+    }
+    const int64_t n_hyp = n_pos * n_yaw;
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (int64_t h = 0; h < n_hyp; ++h) {
+        const int64_t ip = h / n_yaw;
+        const int iyaw = (int)(h - ip * n_yaw);
+        const float cx = pos[3 * ip], cy = pos[3 * ip + 1], cz = pos[3 * ip + 2];
+        const int64_t cc = og_at(g, cx, cy, cz);
+        if (cc < 0 || (float)df[cc] < free_cm) {
+            out[h] = -1.0f;
+            continue;
+        }
+        if (ref) {
+            out[h] = og_score_ref(g, df, pts, n_pts, cx, cy, cz, c[iyaw], sn[iyaw], tau);
+        } else {
+            int n_in, sum_d2;
+            og_score_sums(g, df, pts, n_pts, cx, cy, cz, c[iyaw], sn[iyaw], tau, n_in, sum_d2);
+            out[h] = (float)((double)n_in - (double)sum_d2 / ((double)tau * (double)tau));
+        }
+    }
+}
+
+void or_score_list(const or_grid* gp, const uint8_t* df, const float* pts, int n_pts, const float* hyp, int64_t n_hyp,
+                   float tau, int ref, float* out, int threads) {
+    const or_grid& g = *gp;
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (int64_t h = 0; h < n_hyp; ++h) {
+        const float* q = hyp + 4 * h;
+        const float co = (float)std::cos((double)q[3]);
+        const float si = (float)std::sin((double)q[3]);
+        if (ref) {
+            out[h] = og_score_ref(g, df, pts, n_pts, q[0], q[1], q[2], co, si, tau);
+        } else {
+            int n_in, sum_d2;
+            og_score_sums(g, df, pts, n_pts, q[0], q[1], q[2], co, si, tau, n_in, sum_d2);
+            out[h] = (float)((double)n_in - (double)sum_d2 / ((double)tau * (double)tau));
+        }
     }
 }
 

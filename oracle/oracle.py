@@ -88,6 +88,8 @@ def lib() -> C.CDLL:
             "or_prior_distances": (None, [C.POINTER(OrGrid), P, i64, P, P, i32]),
             "or_loc_icp": (None, [C.POINTER(OrGrid), P, P, P, i32, P, i32, P, P, P, f32, i32, P, P, i32]),
             "or_loc_eval": (None, [C.POINTER(OrGrid), P, P, P, i32, P, P, P, i32]),
+            "or_score_grid": (None, [C.POINTER(OrGrid), P, P, i32, P, i64, i32, f32, f32, f32, f32, i32, P, i32]),
+            "or_score_list": (None, [C.POINTER(OrGrid), P, P, i32, P, i64, f32, i32, P, i32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(_lib, name)
@@ -565,6 +567,27 @@ class PriorGrid:
         T = np.ascontiguousarray(T, dtype=np.float64)
         out = np.empty(len(pts), np.float32)
         lib().or_prior_distances(C.byref(self.g), _p(pts), len(pts), _p(T), _p(out), threads())
+        return out
+
+    def score_grid(self, pts, pos, n_yaw: int, yaw0: float, dyaw: float, tau: float, free_cm: float,
+                   ref: bool = False, nthreads: int | None = None) -> np.ndarray:
+        """k_score_grid (localize.py:55-96) over every (position, heading): the exact-sum soft count the library
+        computes, or with ref the reference's float32 sum in point order (same poses)."""
+        pts = np.ascontiguousarray(pts, dtype=np.float32).reshape(-1, 3)
+        pos = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 3)
+        out = np.empty(len(pos) * int(n_yaw), np.float32)
+        lib().or_score_grid(C.byref(self.g), _p(self.df), _p(pts), len(pts), _p(pos), len(pos), int(n_yaw),
+                            float(yaw0), float(dyaw), float(tau), float(free_cm), int(ref), _p(out),
+                            nthreads or threads())
+        return out
+
+    def score_list(self, pts, hyp, tau: float, ref: bool = False, nthreads: int | None = None) -> np.ndarray:
+        """k_score_list (localize.py:99-123) for (x, y, z, yaw) hypotheses."""
+        pts = np.ascontiguousarray(pts, dtype=np.float32).reshape(-1, 3)
+        hyp = np.ascontiguousarray(hyp, dtype=np.float32).reshape(-1, 4)
+        out = np.empty(len(hyp), np.float32)
+        lib().or_score_list(C.byref(self.g), _p(self.df), _p(pts), len(pts), _p(hyp), len(hyp), float(tau), int(ref),
+                            _p(out), nthreads or threads())
         return out
 
     def icp(self, pts4, lo, hi, T, schedule, alpha=0.05, min_count=30, nthreads=None):

@@ -220,3 +220,78 @@ def test_argument_errors(room):
         loc.register_batch([np.zeros((10, 3), np.float32)] * 9, np.tile(np.eye(4), (9, 1, 1)))
     with pytest.raises(RuntimeError):
         loc.refine(np.zeros((50, 3), np.float32), np.eye(4))
+
+
+def _score_case(sc, seed, n_pts):
+    from livox_warp import synth
+
+    T = synth.free_poses(sc, 1, seed)[0]
+    pts = synth.spin_scan(sc, T, 3 * n_pts, seed + 1)[:n_pts]
+    return T, np.ascontiguousarray(pts, dtype=np.float32)
+
+
+@pytest.mark.parametrize("n_pts", [1024, 2500])
+def test_score_grid_bit_exact(room, n_pts):
+    """lw_score_grid against the oracle, every (position, heading) bit for bit: positions inside and outside the
+    grid and inside surfaces (-1), 36 headings, scans of one and of several shared-memory chunks."""
+    from livox_warp.localize import coarse_positions, score_grid
+
+    sc, grid, og = room
+    T, pts = _score_case(sc, 7, n_pts)
+    pos, nx, ny = coarse_positions(grid.lo - 0.5, grid.hi + 0.5, [0.6, 1.2, 1.8], 0.35)
+    n_yaw, yaw0, dyaw = 36, 0.05, math.radians(10.0)
+    out = torch.full((len(pos) * n_yaw,), 7.0, dtype=torch.float32, device="cuda")
+    score_grid(grid, torch.from_numpy(pts).cuda(), torch.from_numpy(pos).cuda(), n_yaw, yaw0, dyaw, 25.0, 10.0, out)
+    got = out.cpu().numpy()
+    want = og.score_grid(pts, pos, n_yaw, yaw0, dyaw, 25.0, 10.0)
+    assert np.array_equal(got, want)
+    assert (want == -1.0).sum() > 100 and (want > 0.5 * n_pts).any()
+
+
+def test_score_list_bit_exact(room):
+    from livox_warp.localize import score_list
+
+    sc, grid, og = room
+    T, pts = _score_case(sc, 11, 2048)
+    rng = np.random.default_rng(2)
+    yaw = math.atan2(T[1, 0], T[0, 0])
+    hyp = np.concatenate([T[:3, 3] + rng.normal(0, 0.3, (5000, 3)), yaw + rng.normal(0, 0.5, (5000, 1))], 1)
+    hyp = hyp.astype(np.float32)
+    out = torch.empty(len(hyp), dtype=torch.float32, device="cuda")
+    score_list(grid, torch.from_numpy(pts).cuda(), torch.from_numpy(hyp).cuda(), 12.0, out)
+    got = out.cpu().numpy()
+    want = og.score_list(pts, hyp, 12.0)
+    assert np.array_equal(got, want)
+    true = og.score_list(pts, np.array([[T[0, 3], T[1, 3], T[2, 3], yaw]], np.float32), 12.0)[0]
+    assert true > 0.8 * len(pts) and true >= np.quantile(want, 0.99)
+
+
+def test_coarse_search_finds_the_pose(room):
+    """GlobalLocalizer._coarse over the whole room (0.25 m, 2 degrees, three heights): the best hypothesis lies
+    within one grid step and two heading steps of the scan's true pose."""
+    from livox_warp.localize import GlobalLocalizer
+
+    sc, grid, og = room
+    T, pts = _score_case(sc, 13, 1024)
+    loc = GlobalLocalizer(grid, hyp_cap=16, pts_cap=1 << 12)
+    pos, shape, dyaw, s = loc._coarse(None, pts, [T[2, 3] - 0.1, T[2, 3], T[2, 3] + 0.1])
+    assert shape[3] == 180 and len(s) == len(pos) * 180
+    best = int(np.argmax(s))
+    p, iyaw = pos[best // 180], best % 180
+    yaw = math.atan2(T[1, 0], T[0, 0]) % (2 * math.pi)
+    dy = abs((iyaw * dyaw - yaw + math.pi) % (2 * math.pi) - math.pi)
+    assert np.linalg.norm(p[:2] - T[:2, 3]) <= 0.25 * 1.5 and dy <= 2 * dyaw + 1e-6, (p, T[:3, 3], dy)
+    ms = loc._score_list(None, pts, len(pts), np.array([[*p, iyaw * dyaw]], np.float32), loc.tau_mid)
+    assert ms[0] == og.score_list(pts, np.array([[*p, iyaw * dyaw]], np.float32), loc.tau_mid)[0]
+
+
+def test_score_grid_rejects_too_many_headings(room):
+    from livox_warp import _lib
+    from livox_warp.localize import score_grid
+
+    sc, grid, og = room
+    pts = torch.zeros((4, 3), dtype=torch.float32, device="cuda")
+    pos = torch.zeros((2, 3), dtype=torch.float32, device="cuda")
+    out = torch.empty(2 * 2000, dtype=torch.float32, device="cuda")
+    with pytest.raises(_lib.LwError, match="n_yaw"):
+        score_grid(grid, pts, pos, 2000, 0.0, 0.01, 25.0, 10.0, out)
