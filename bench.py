@@ -999,7 +999,7 @@ def run_coarse(a, rank: int, world: int, local: int):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
 
     def dev_step():
-        score_grid(grid, d_pts, d_pos, n_yaw, 0.0, dyaw, tau, free_cm, out, stream)
+        score_grid(grid, d_pts, d_pos, n_yaw, 0.0, dyaw, tau, free_cm, out, stream, pos_stride=ny)
 
     for _ in range(a.warmup):
         dev_step()

@@ -369,10 +369,13 @@ int lw_prior_distances(const lw_prior_grid* g, const float* pts, int64_t n, cons
  * (gravity-aligned sensor frame) near the map: the sum over points whose cell distance d (cm, the grid's df) is
  * below tau_cm of 1 - d^2 / tau_cm^2, formed exactly from integer sums (the reference adds float32 terms in point
  * order). out[i*n_yaw + j]; -1 where the position lies outside the grid or within free_cm of a mapped surface.
- * Needs the built grid (df). */
+ * Needs the built grid (df). pos_stride (>= 1) only sets the thread layout: when positions i and i + pos_stride
+ * are neighbours along x (ny for a meshgrid with y inner, as localize.py:415-419 builds), a warp's gathers share
+ * cache lines; 1 for any list. */
 #define LW_SCORE_MAX_YAW 1024
 int lw_score_grid(const lw_prior_grid* g, const float* pts, int32_t n_pts, const float* pos, int64_t n_pos,
-                  int32_t n_yaw, float yaw0, float dyaw, float tau_cm, float free_cm, float* out, void* stream);
+                  int64_t pos_stride, int32_t n_yaw, float yaw0, float dyaw, float tau_cm, float free_cm, float* out,
+                  void* stream);
 
 /* The same soft count for a list of hypotheses hyp [n_hyp*4] = (x, y, z, yaw), 16-byte aligned
  * (localize.py:99-123, k_score_list). */

@@ -224,17 +224,19 @@ def _f32_rows(x, cols: int, name: str) -> torch.Tensor:
 
 
 def score_grid(grid: PriorGrid, pts: torch.Tensor, pos: torch.Tensor, n_yaw: int, yaw0: float, dyaw: float,
-               tau_cm: float, free_cm: float, out: torch.Tensor, stream=None):
+               tau_cm: float, free_cm: float, out: torch.Tensor, stream=None, pos_stride: int = 1):
     """k_score_grid (localize.py:55-96): for every position pos[i] ([n, 3]) and heading yaw0 + j dyaw, the soft
     count of the scan points `pts` ([m, 3], gravity-aligned sensor frame) within tau_cm of the map, into
-    out[i * n_yaw + j]; -1 where the sensor would sit outside the grid or within free_cm of a mapped surface."""
+    out[i * n_yaw + j]; -1 where the sensor would sit outside the grid or within free_cm of a mapped surface.
+    pos_stride: positions i and i + pos_stride are x neighbours (ny for coarse_positions' layout); it changes the
+    thread layout only."""
     _f32_rows(pts, 3, "pts")
     _f32_rows(pos, 3, "pos")
     if out.dtype != torch.float32 or not out.is_contiguous() or out.numel() < pos.shape[0] * n_yaw:
         raise ValueError("out must hold n_pos * n_yaw float32")
     _lib.call("lw_score_grid", C.byref(grid.struct), _lib.ptr(pts), int(pts.shape[0]), _lib.ptr(pos),
-              int(pos.shape[0]), int(n_yaw), float(yaw0), float(dyaw), float(tau_cm), float(free_cm), _lib.ptr(out),
-              _lib.stream_ptr(stream))
+              int(pos.shape[0]), int(pos_stride), int(n_yaw), float(yaw0), float(dyaw), float(tau_cm), float(free_cm),
+              _lib.ptr(out), _lib.stream_ptr(stream))
 
 
 def score_list(grid: PriorGrid, pts: torch.Tensor, hyp: torch.Tensor, tau_cm: float, out: torch.Tensor, stream=None):
@@ -296,7 +298,7 @@ class GlobalLocalizer:
             d_pts = torch.from_numpy(np.ascontiguousarray(pts_g, dtype=np.float32)).to(self.device, non_blocking=True)
             d_pos = torch.from_numpy(pos).to(self.device, non_blocking=True)
             out = torch.empty(len(pos) * n_yaw, dtype=torch.float32, device=self.device)
-            score_grid(g, d_pts, d_pos, n_yaw, 0.0, dyaw, self.tau_coarse, self.free_cm, out, stream)
+            score_grid(g, d_pts, d_pos, n_yaw, 0.0, dyaw, self.tau_coarse, self.free_cm, out, stream, pos_stride=ny)
             sc = out.cpu().numpy()
         return pos, (len(heights), nx, ny, n_yaw), dyaw, sc
 

@@ -230,10 +230,11 @@ def _score_case(sc, seed, n_pts):
     return T, np.ascontiguousarray(pts, dtype=np.float32)
 
 
-@pytest.mark.parametrize("n_pts", [1024, 2500])
-def test_score_grid_bit_exact(room, n_pts):
+@pytest.mark.parametrize("n_pts,stride", [(1024, 1), (2500, 1), (1024, "ny"), (700, 5)])
+def test_score_grid_bit_exact(room, n_pts, stride):
     """lw_score_grid against the oracle, every (position, heading) bit for bit: positions inside and outside the
-    grid and inside surfaces (-1), 36 headings, scans of one and of several shared-memory chunks."""
+    grid and inside surfaces (-1), 36 headings, scans of one and of several shared-memory chunks, each thread
+    layout (x neighbours along a warp, plain list order, a stride that does not divide the positions)."""
     from livox_warp.localize import coarse_positions, score_grid
 
     sc, grid, og = room
@@ -241,7 +242,8 @@ def test_score_grid_bit_exact(room, n_pts):
     pos, nx, ny = coarse_positions(grid.lo - 0.5, grid.hi + 0.5, [0.6, 1.2, 1.8], 0.35)
     n_yaw, yaw0, dyaw = 36, 0.05, math.radians(10.0)
     out = torch.full((len(pos) * n_yaw,), 7.0, dtype=torch.float32, device="cuda")
-    score_grid(grid, torch.from_numpy(pts).cuda(), torch.from_numpy(pos).cuda(), n_yaw, yaw0, dyaw, 25.0, 10.0, out)
+    score_grid(grid, torch.from_numpy(pts).cuda(), torch.from_numpy(pos).cuda(), n_yaw, yaw0, dyaw, 25.0, 10.0, out,
+               pos_stride=ny if stride == "ny" else stride)
     got = out.cpu().numpy()
     want = og.score_grid(pts, pos, n_yaw, yaw0, dyaw, 25.0, 10.0)
     assert np.array_equal(got, want)
@@ -295,3 +297,5 @@ def test_score_grid_rejects_too_many_headings(room):
     out = torch.empty(2 * 2000, dtype=torch.float32, device="cuda")
     with pytest.raises(_lib.LwError, match="n_yaw"):
         score_grid(grid, pts, pos, 2000, 0.0, 0.01, 25.0, 10.0, out)
+    with pytest.raises(_lib.LwError, match="pos_stride"):
+        score_grid(grid, pts, pos, 4, 0.0, 0.01, 25.0, 10.0, out, pos_stride=0)

@@ -71,7 +71,7 @@ def test_score_arguments_checked_before_cuda():
     from livox_warp import _lib
 
     lib = _lib.load(require_cuda=False)
-    assert lib.lw_score_grid(None, None, 0, None, 0, 1, ctypes.c_float(0), ctypes.c_float(0), ctypes.c_float(25),
+    assert lib.lw_score_grid(None, None, 0, None, 0, 1, 1, ctypes.c_float(0), ctypes.c_float(0), ctypes.c_float(25),
                              ctypes.c_float(10), None, None) == _lib.LW_EINVAL
     assert b"lw_score_grid" in lib.lw_last_error()
     assert lib.lw_score_list(None, None, 0, None, 0, ctypes.c_float(12), None, None) == _lib.LW_EINVAL
