@@ -921,13 +921,13 @@ def run_localize(a, rank: int, world: int, local: int):
 # ---- coarse hypothesis scoring (k_score_grid) --------------------------------------------------------------------
 
 COARSE_SPACING = 0.03  # prior-map sample spacing (m): the scores read only the grid's distance field
-COARSE_PTS = 1024      # scan points per hypothesis (localize.py:352, n_coarse_pts)
-COARSE_HEIGHTS = 8     # sensor heights per gravity candidate (localize.py:346)
+COARSE_PTS = 1024      # scan points per hypothesis (localize.py:365, n_coarse_pts)
+COARSE_HEIGHTS = 8     # sensor heights per gravity candidate (localize.py:361)
 
 
 def coarse_workload():
     """The office prior map, one 360-degree scan from a free pose and its 1024-point subset (one point per 15 cm
-    voxel first, as localize.py:630-634 spreads it), and 8 sensor heights around the true one."""
+    voxel first, as localize.py:635-638 spreads it), and 8 sensor heights around the true one."""
     from livox_warp import synth
 
     scene = synth.office(LOC_SEED)
@@ -951,7 +951,7 @@ def run_coarse(a, rank: int, world: int, local: int):
     config = {"workload": f"coarse global search: office 40x30x3 m prior map ({len(w['xyz']):,} pts at "
                           f"{COARSE_SPACING * 1e3:.0f} mm, 5 cm grid), every free position on a {step} m xy grid x "
                           f"{COARSE_HEIGHTS} heights x {n_yaw} headings, {len(w['pts'])} scan points each, "
-                          f"tau {tau:.0f} cm, free {free_cm:.0f} cm (localize.py:413-448)",
+                          f"tau {tau:.0f} cm, free {free_cm:.0f} cm (localize.py:426-448)",
               "scan_points": int(len(w["pts"])), "headings": n_yaw, "heights": COARSE_HEIGHTS,
               "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{a.gpus}"}
     if a.impl == "reference":
@@ -1021,18 +1021,25 @@ def run_coarse(a, rank: int, world: int, local: int):
     ms_total = max_over_ranks(float(step_ms.sum()), device)
     value = replica_rate(a.steps * n_hyp, world, ms_total)
     sc = out.cpu().numpy()
-    # e2e through GlobalLocalizer._coarse: host scan in, H2D of scan and positions, every score back to the host
+    # e2e through the public calls from the host scan: _coarse_candidates (scores and local maxima on the device,
+    # the candidates back) and _coarse (every score back to the host, as the reference's _coarse returns them)
     for _ in range(2):
         loc._coarse(stream, w["pts"], w["heights"])
+        loc._coarse_candidates(stream, w["pts"], w["heights"])
     torch.cuda.synchronize(device)
     e_steps = max(3, min(a.steps, 10))
     t0 = time.perf_counter()
     for _ in range(e_steps):
-        pos_e, shape, _, sc_e = loc._coarse(stream, w["pts"], w["heights"])
+        _, _, _, cand, cand_sc = loc._coarse_candidates(stream, w["pts"], w["heights"])
     e_s = max_over_ranks(time.perf_counter() - t0, device)
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        pos_e, shape, _, sc_e = loc._coarse(stream, w["pts"], w["heights"])
+    e_all_s = max_over_ranks(time.perf_counter() - t0, device)
     if rank != 0:
         return
     assert np.array_equal(sc_e, sc), "the public call and the timed launches disagree"
+    assert np.array_equal(cand_sc, sc[cand]) and int(cand[0]) == int(np.argmax(sc)), "candidates disagree"
     # parity on a sample of positions, and the CPU baseline on it (the oracle's grid over the same prepared
     # arrays; the distance field is the device's, which the parity tests hold bit-exact to the oracle's flood)
     threads = _o.host_cores()
@@ -1076,7 +1083,11 @@ def run_coarse(a, rank: int, world: int, local: int):
                                        f"oracle (C++/OpenMP), {secs:.1f} s"},
             "e2e": {"value": round(world * e_steps * n_hyp / e_s, 3), "unit": "hypotheses/s",
                     "h2d_bytes_per_step": int(12 * len(w["pts"]) + 12 * len(pos)),
-                    "d2h_bytes_per_step": int(4 * n_hyp)},
+                    "d2h_bytes_per_step": int(4 + 12 * loc.last_candidates),
+                    "path": "GlobalLocalizer._coarse_candidates: scores and local maxima on the device"},
+            "e2e_all_scores": {"value": round(world * e_steps * n_hyp / e_all_s, 3), "unit": "hypotheses/s",
+                               "d2h_bytes_per_step": int(4 * n_hyp),
+                               "path": "GlobalLocalizer._coarse: every score back to the host"},
             "gpu_launches": int(launches), "clocks": clk}
     print(json.dumps(line))
 

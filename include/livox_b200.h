@@ -370,7 +370,7 @@ int lw_prior_distances(const lw_prior_grid* g, const float* pts, int64_t n, cons
  * below tau_cm of 1 - d^2 / tau_cm^2, formed exactly from integer sums (the reference adds float32 terms in point
  * order). out[i*n_yaw + j]; -1 where the position lies outside the grid or within free_cm of a mapped surface.
  * Needs the built grid (df). pos_stride (>= 1) only sets the thread layout: when positions i and i + pos_stride
- * are neighbours along x (ny for a meshgrid with y inner, as localize.py:415-419 builds), a warp's gathers share
+ * are neighbours along x (ny for a meshgrid with y inner, as localize.py:428-432 builds), a warp's gathers share
  * cache lines; 1 for any list. */
 #define LW_SCORE_MAX_YAW 1024
 int lw_score_grid(const lw_prior_grid* g, const float* pts, int32_t n_pts, const float* pos, int64_t n_pos,
@@ -382,8 +382,16 @@ int lw_score_grid(const lw_prior_grid* g, const float* pts, int32_t n_pts, const
 int lw_score_list(const lw_prior_grid* g, const float* pts, int32_t n_pts, const float* hyp, int64_t n_hyp,
                   float tau_cm, float* out, void* stream);
 
+/* Local maxima of lw_score_grid's scores laid out as (nz heights, nx, ny, n_yaw) -- the meshgrid order of
+ * localize.py:428-432 -- by the rule of localize.py:450-483 (_local_maxima): a positive score, at least
+ * min_score, no less than any of the 26 (x, y, heading) neighbours at the same height (x / y neighbours outside
+ * the grid skipped, headings wrapping). Appends up to cap survivors as (idx [cap] int64, val [cap]) in no
+ * particular order; count_dev[0] = the number of survivors (may exceed cap). Clears count_dev on the stream. */
+int lw_score_maxima(const float* scores, int32_t nz, int32_t nx, int32_t ny, int32_t n_yaw, float min_score,
+                    int32_t cap, int64_t* idx, float* val, int32_t* count_dev, void* stream);
+
 /* The headings' float32 cosines and sines lw_score_grid poses points with: yaw_j = yaw0 + j dyaw in float32
- * (localize.py:79), its cosine and sine in float64 rounded to float32. Host only; c and s hold n_yaw floats. */
+ * (localize.py:82), its cosine and sine in float64 rounded to float32. Host only; c and s hold n_yaw floats. */
 void lw_score_yaw_table(int32_t n_yaw, float yaw0, float dyaw, float* c, float* s);
 
 /* Buffers of the batched ICP: every hypothesis has its own range of points (tile_lo .. scan_end; hypotheses may

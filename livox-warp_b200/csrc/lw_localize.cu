@@ -716,7 +716,7 @@ __global__ void __launch_bounds__(SC_THREADS, 6) k_score_grid(lw_prior_grid g, c
         if (rows <= 2) {
 #pragma unroll 2
             for (int k = 0; k < m; ++k) {
-                // the reference's expressions (localize.py:86-88), the shared parts once per row
+                // the reference's expressions (localize.py:89), the shared parts once per row
                 const float ax = co * px[k], bx = si * py[k], ey = si * px[k], fy = co * py[k];
                 const float wya = ya + ey + fy, wza = za + pz[k];
                 const int iya = ifloor((wya - g.origin[1]) * g.inv_cell), iza = ifloor((wza - g.origin[2]) * g.inv_cell);
@@ -757,6 +757,48 @@ __global__ void __launch_bounds__(SC_THREADS, 6) k_score_grid(lw_prior_grid g, c
 #pragma unroll
     for (int j = 0; j < SC_POS; ++j)
         if (live[j]) out[(c + stride * (r0 + j)) * n_yaw + iyaw] = soft_count(n_in[j], sum_d2[j], tau);
+}
+
+// Local maxima of the coarse scores (localize.py:450-483, _local_maxima): hypothesis h = ((iz nx + ix) ny + iy)
+// n_yaw + iyaw is one when its score is positive, at least min_score, and no less than any of its 26 neighbours in
+// (x, y, heading) at its height -- neighbours outside the x / y range are skipped, headings wrap. Survivors are
+// appended (index, score) in no particular order; the caller orders them.
+__global__ void k_score_maxima(const float* __restrict__ sc, int nz, int nx, int ny, int n_yaw, float min_score,
+                               int cap, int64_t* __restrict__ idx, float* __restrict__ val, int* __restrict__ count) {
+    const int64_t n = (int64_t)nz * nx * ny * n_yaw;
+    for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < n; h += (int64_t)gridDim.x * blockDim.x) {
+        const float mine = sc[h];
+        if (!(mine > 0.0f) || mine < min_score) continue;
+        const int iyaw = (int)(h % n_yaw);
+        const int64_t p = h / n_yaw;
+        const int iy = (int)(p % ny);
+        const int ix = (int)((p / ny) % nx);
+        const int64_t base = p - (int64_t)iy - (int64_t)ix * ny;  // iz's first position
+        bool best = true;
+        for (int ox = -1; ox <= 1 && best; ++ox) {
+            const int jx = ix + ox;
+            if (jx < 0 || jx >= nx) continue;
+            for (int oy = -1; oy <= 1 && best; ++oy) {
+                const int jy = iy + oy;
+                if (jy < 0 || jy >= ny) continue;
+                const int64_t q = (base + (int64_t)jx * ny + jy) * n_yaw;
+                for (int oa = -1; oa <= 1; ++oa) {
+                    if (ox == 0 && oy == 0 && oa == 0) continue;
+                    const int ja = (iyaw + oa + n_yaw) % n_yaw;
+                    if (__ldg(sc + q + ja) > mine) {
+                        best = false;
+                        break;
+                    }
+                }
+            }
+        }
+        if (!best) continue;
+        const int k = atomicAdd(count, 1);
+        if (k < cap) {
+            idx[k] = h;
+            val[k] = mine;
+        }
+    }
 }
 
 __global__ void __launch_bounds__(SC_THREADS) k_score_list(lw_prior_grid g, const float* __restrict__ pts, int n_pts,
@@ -888,9 +930,25 @@ int lw_score_list(const lw_prior_grid* g, const float* pts, int32_t n_pts, const
     return LW_OK;
 }
 
+int lw_score_maxima(const float* scores, int32_t nz, int32_t nx, int32_t ny, int32_t n_yaw, float min_score,
+                    int32_t cap, int64_t* idx, float* val, int32_t* count_dev, void* stream) {
+    if (!scores || !idx || !val || !count_dev || nz < 0 || nx < 0 || ny < 0 || n_yaw < 1 || cap < 0)
+        return set_error(LW_EINVAL, "lw_score_maxima: bad arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemsetAsync(count_dev, 0, sizeof(int32_t), s) != cudaSuccess)
+        return set_error(LW_ECUDA, "lw_score_maxima: clearing the count failed");
+    const int64_t n = (int64_t)nz * nx * ny * n_yaw;
+    if (n == 0) return LW_OK;
+    k_score_maxima<<<blocks_for(n, 256, 16 * device_sms()), 256, 0, s>>>(scores, nz, nx, ny, n_yaw, min_score, cap,
+                                                                        idx, val, count_dev);
+    LW_LAUNCHED("lw_score_maxima");
+    count_launches(1);
+    return LW_OK;
+}
+
 void lw_score_yaw_table(int32_t n_yaw, float yaw0, float dyaw, float* c, float* s) {
     for (int j = 0; j < n_yaw; ++j) {
-        const float yaw = yaw0 + (float)j * dyaw;  // float32, as localize.py:79
+        const float yaw = yaw0 + (float)j * dyaw;  // float32, as localize.py:82
         c[j] = (float)std::cos((double)yaw);
         s[j] = (float)std::sin((double)yaw);
     }

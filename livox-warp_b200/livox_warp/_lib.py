@@ -184,6 +184,7 @@ _SIGS = {
     "lw_score_grid": (i32, [C.POINTER(PriorGrid), P, i32, P, i64, i64, i32, f32, f32, f32, f32, P, P]),
     "lw_score_list": (i32, [C.POINTER(PriorGrid), P, i32, P, i64, f32, P, P]),
     "lw_score_yaw_table": (None, [i32, f32, f32, P, P]),
+    "lw_score_maxima": (i32, [P, i32, i32, i32, i32, f32, i32, P, P, P, P]),
     "lw_loc_icp_batch": (i32, [C.POINTER(PriorGrid), C.POINTER(LocBatch), i32, i32, i32, i32, C.POINTER(f64),
                                C.POINTER(i32), f32, i32, i32, i32, P]),
 }

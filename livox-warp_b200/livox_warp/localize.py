@@ -250,7 +250,7 @@ def score_list(grid: PriorGrid, pts: torch.Tensor, hyp: torch.Tensor, tau_cm: fl
 
 
 def coarse_positions(lo, hi, heights, xy_step: float) -> tuple[np.ndarray, int, int]:
-    """Every position of the xy grid over [lo, hi] at each height (localize.py:415-419): x outer, y inner, one
+    """Every position of the xy grid over [lo, hi] at each height (localize.py:428-432): x outer, y inner, one
     block per height; returns (pos [n, 3] float32, nx, ny)."""
     gx = np.arange(lo[0], hi[0] + 1e-6, xy_step)
     gy = np.arange(lo[1], hi[1] + 1e-6, xy_step)
@@ -265,12 +265,13 @@ class GlobalLocalizer:
 
     PTS_CAP = 1 << 17  # scan points after 5 cm thinning, localize.py:322
     ICP_CAP = 16  # poses refine() takes together, localize.py:325
-    # coarse search tuning (localize.py:344-351)
+    # coarse search tuning (localize.py:359-364)
     xy_step = 0.25
     yaw_step_deg = 2.0
     tau_coarse = 25.0  # cm
     tau_mid = 12.0
     free_cm = 10.0  # the sensor sits at least this far from any mapped surface
+    keep_coarse = 128  # coarse local maxima re-scored on the finer grid (localize.py:367)
 
     def __init__(self, grid: PriorGrid, device=None, hyp_cap: int = 1024, pts_cap: int = 1 << 23,
                  tuner: Autotuner | None = None):
@@ -282,13 +283,14 @@ class GlobalLocalizer:
         self.tuner = tuner if tuner is not None else Autotuner()
         self.seed = 0  # refine() draws its subset from a fresh generator with this seed
         self.last_tile = 0
+        self.last_candidates = 0
         self._graphs: dict = {}
 
     # ---- the coarse search's scores ------------------------------------------------------------------
 
     def _coarse(self, stream, pts_g: np.ndarray, heights):
         """Every free-space position on the xy grid at the given heights x every heading, scored in one launch
-        (localize.py:413-448). Returns (pos, (n_heights, nx, ny, n_yaw), dyaw, scores)."""
+        (localize.py:426-448). Returns (pos, (n_heights, nx, ny, n_yaw), dyaw, scores)."""
         g = self.grid
         pos, nx, ny = coarse_positions(g.lo, g.hi, heights, self.xy_step)
         n_yaw = int(round(360.0 / self.yaw_step_deg))
@@ -301,6 +303,40 @@ class GlobalLocalizer:
             score_grid(g, d_pts, d_pos, n_yaw, 0.0, dyaw, self.tau_coarse, self.free_cm, out, stream, pos_stride=ny)
             sc = out.cpu().numpy()
         return pos, (len(heights), nx, ny, n_yaw), dyaw, sc
+
+    def _coarse_candidates(self, stream, pts_g: np.ndarray, heights, keep: int | None = None, pool: int = 20000):
+        """The coarse search with its local maxima found on the device: the reference's _coarse then
+        _local_maxima(sc, shape, keep) (localize.py:426-448, 450-483), but only the candidates cross to the host.
+        A candidate scores above zero, no lower than its 26 (x, y, heading) neighbours and at least the pool-th
+        best score (the reference looks for maxima among the `pool` best); ties are ordered by index. Returns
+        (pos, shape, dyaw, best indices, their scores), best first."""
+        g = self.grid
+        keep = self.keep_coarse if keep is None else keep
+        pos, nx, ny = coarse_positions(g.lo, g.hi, heights, self.xy_step)
+        n_yaw = int(round(360.0 / self.yaw_step_deg))
+        dyaw = math.radians(self.yaw_step_deg)
+        shape = (len(heights), nx, ny, n_yaw)
+        stream = stream if stream is not None else torch.cuda.current_stream(self.device)
+        cap = 1 << 16
+        with torch.cuda.stream(stream):
+            d_pts = torch.from_numpy(np.ascontiguousarray(pts_g, dtype=np.float32)).to(self.device, non_blocking=True)
+            d_pos = torch.from_numpy(pos).to(self.device, non_blocking=True)
+            n = len(pos) * n_yaw
+            out = torch.empty(n, dtype=torch.float32, device=self.device)
+            score_grid(g, d_pts, d_pos, n_yaw, 0.0, dyaw, self.tau_coarse, self.free_cm, out, stream, pos_stride=ny)
+            thr = torch.topk(out, min(pool, n), sorted=False).values.min()
+            idx = torch.empty(cap, dtype=torch.int64, device=self.device)
+            val = torch.empty(cap, dtype=torch.float32, device=self.device)
+            cnt = torch.zeros(1, dtype=torch.int32, device=self.device)
+            _lib.call("lw_score_maxima", _lib.ptr(out), shape[0], nx, ny, n_yaw, float(thr.item()), cap,
+                      _lib.ptr(idx), _lib.ptr(val), _lib.ptr(cnt), _lib.stream_ptr(stream))
+            k = int(cnt.item())
+            if k > cap:
+                raise _lib.LwError(f"lw_score_maxima: {k} local maxima exceed {cap}")
+            bi, bv = idx[:k].cpu().numpy(), val[:k].cpu().numpy()
+        self.last_candidates = k  # local maxima found (and copied to the host) by the last call
+        order = np.lexsort((bi, -bv))[:keep]
+        return pos, shape, dyaw, bi[order], bv[order]
 
     def _score_list(self, stream, pts, m: int, hyps: np.ndarray, tau: float) -> np.ndarray:
         """The soft counts of (x, y, z, yaw) hypotheses for the first m points of `pts` (localize.py:507-515)."""

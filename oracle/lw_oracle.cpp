@@ -942,7 +942,7 @@ void or_prior_distances(const or_grid* g, const float* pts, int64_t n, const dou
 // Two sums. By default the definition the library computes: the soft count formed exactly from the number of
 // points with d < tau and the sum of their d^2 (integers), rounded once. With ref, the reference's own sum: float32
 // terms 1 - d*d*inv_t2 added in point order. Both pose the points with the reference's expressions
-// (localize.py:86-88, 114-116) and the headings' cosines and sines taken in float64 and rounded to float32 (the
+// (localize.py:89, 117) and the headings' cosines and sines taken in float64 and rounded to float32 (the
 // reference's float32 wp.cos / wp.sin may differ from those by an ulp).
 
 static inline int64_t og_at(const or_grid& g, float x, float y, float z) {  // grid_at mapgrid.py:53-56
