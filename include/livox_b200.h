@@ -369,7 +369,7 @@ int lw_prior_distances(const lw_prior_grid* g, const float* pts, int64_t n, cons
  * (gravity-aligned sensor frame) near the map: the sum over points whose cell distance d (cm, the grid's df) is
  * below tau_cm of 1 - d^2 / tau_cm^2, formed exactly from integer sums (the reference adds float32 terms in point
  * order). out[i*n_yaw + j]; -1 where the position lies outside the grid or within free_cm of a mapped surface.
- * Needs the built grid (df). pos_stride (>= 1) only sets the thread layout: when positions i and i + pos_stride
+ * Needs the built grid (df); a buffer may be null when its count is 0. pos_stride (>= 1) only sets the thread layout: when positions i and i + pos_stride
  * are neighbours along x (ny for a meshgrid with y inner, as localize.py:428-432 builds), a warp's gathers share
  * cache lines; 1 for any list. */
 #define LW_SCORE_MAX_YAW 1024

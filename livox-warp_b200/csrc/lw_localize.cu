@@ -885,7 +885,7 @@ int lw_score_grid(const lw_prior_grid* g, const float* pts, int32_t n_pts, const
                   void* stream) {
     int r = check_grid(g, "lw_score_grid");
     if (r != LW_OK) return r;
-    if (!g->df || !pts || !pos || !out || n_pts < 0 || n_pos < 0)
+    if (!g->df || n_pts < 0 || n_pos < 0 || (n_pts > 0 && !pts) || (n_pos > 0 && (!pos || !out)))
         return set_error(LW_EINVAL, "lw_score_grid: bad arguments");
     if (n_yaw < 1 || n_yaw > LW_SCORE_MAX_YAW)
         return set_error(LW_EINVAL, "lw_score_grid: n_yaw %d outside [1, %d]", n_yaw, LW_SCORE_MAX_YAW);
@@ -916,7 +916,7 @@ int lw_score_list(const lw_prior_grid* g, const float* pts, int32_t n_pts, const
                   float tau_cm, float* out, void* stream) {
     int r = check_grid(g, "lw_score_list");
     if (r != LW_OK) return r;
-    if (!g->df || !pts || !hyp || !out || n_pts < 0 || n_hyp < 0)
+    if (!g->df || n_pts < 0 || n_hyp < 0 || (n_pts > 0 && !pts) || (n_hyp > 0 && (!hyp || !out)))
         return set_error(LW_EINVAL, "lw_score_list: bad arguments");
     if (((uintptr_t)hyp & 15) != 0) return set_error(LW_EINVAL, "lw_score_list: hyp must be 16-byte aligned");
     if (!(tau_cm > 0.0f)) return set_error(LW_EINVAL, "lw_score_list: tau_cm must be positive");

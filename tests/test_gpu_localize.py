@@ -343,3 +343,23 @@ def test_coarse_candidates_follow_the_local_maximum_rule(room):
     assert np.array_equal(val, s[idx]) and np.all(np.diff(val) <= 0)
     top = loc._coarse_candidates(None, pts, heights)[3]
     assert np.array_equal(top, idx[:loc.keep_coarse])
+
+
+def test_score_empty_inputs(room):
+    """No scan points: every free position scores 0 and the rest -1, as the oracle; no positions or hypotheses:
+    nothing is written."""
+    from livox_warp.localize import coarse_positions, score_grid, score_list
+
+    sc, grid, og = room
+    pos, nx, ny = coarse_positions(grid.lo, grid.hi, [1.2], 0.5)
+    none = torch.zeros((0, 3), dtype=torch.float32, device="cuda")
+    out = torch.full((len(pos) * 8,), 7.0, dtype=torch.float32, device="cuda")
+    score_grid(grid, none, torch.from_numpy(pos).cuda(), 8, 0.0, 0.7, 25.0, 10.0, out, pos_stride=ny)
+    got = out.cpu().numpy()
+    want = og.score_grid(np.zeros((0, 3), np.float32), pos, 8, 0.0, 0.7, 25.0, 10.0)
+    assert np.array_equal(got, want) and set(np.unique(got).tolist()) <= {0.0, -1.0} and (got == 0.0).any()
+    out.fill_(7.0)
+    score_grid(grid, none, torch.zeros((0, 3), dtype=torch.float32, device="cuda"), 8, 0.0, 0.7, 25.0, 10.0, out)
+    h = torch.zeros((0, 4), dtype=torch.float32, device="cuda")
+    score_list(grid, none, h, 12.0, out)
+    assert bool((out == 7.0).all())
