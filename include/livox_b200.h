@@ -287,6 +287,35 @@ int lw_map_build(const lw_map* map, const lw_view* v, int32_t min_count, float* 
 /* Frame id of each staged point, floor(max(t, 0) * inv_dt), all 0 when inv_dt <= 0 (gpu.py:340-348). */
 int lw_frame_ids(const float* t, int64_t n, float inv_dt, int32_t* out, void* stream);
 
+/* Buffers of the neighbourhood pass: an open-addressed voxel table of cap (a power of two) slots and the dense
+ * per-voxel arrays (at most one voxel per point). */
+typedef struct lw_nbr_buf {
+    int64_t* keys;       /* [cap] voxel keys, -1 empty (cleared by each call) */
+    int64_t* acc;        /* [cap*4] fixed-point sums of x, y, z (LW_FIX_W units) and the point count */
+    int32_t* vidx;       /* [cap] dense index of each occupied slot */
+    int32_t* v_slot;     /* [cap] slot of each dense voxel */
+    int32_t* slot_of_pt; /* [pt_cap] voxel slot of each point, -1 when the table was full */
+    float* v_xyz;        /* [cap*3] voxel centroids, in slot order */
+    int32_t* v_w;        /* [cap] points per voxel */
+    float* v_cnt;        /* [cap] point-weighted neighbour count */
+    float* v_nrm;        /* [cap*3] unit normals */
+    float* v_curv;       /* [cap] curvature */
+    int32_t* tiles;      /* [cap/1024 + 1] scan scratch */
+    int32_t* m;          /* [1] voxels */
+    int64_t cap, pt_cap;
+} lw_nbr_buf;
+
+/* Neighbourhoods of the first n points (gpu.py:777-905, Pipeline.neighborhoods :1531-1557): the points are summed
+ * into voxels radius / 3 wide; each voxel's neighbours are the voxels whose centroid lies within `radius`
+ * (0 < radius <= 4 m) of its own, and their point-weighted count, the normal of their covariance's smallest
+ * eigenvalue turned toward `sensor` (host float[3]) and the curvature (smallest eigenvalue / trace) are handed to
+ * every point of the voxel: out_cnt [n] int32 (rounded), with want_normals out_nrm [n*3] and out_curv [n]. Sums
+ * are exact fixed point and float64, so each point's answers do not depend on thread order. A point whose voxel
+ * did not fit in the table gets count 2^30, normal (0, 0, 1), curvature 0. */
+int lw_neighborhoods(const float* xyz, int32_t xyz_stride, const int32_t* n_dev, int64_t n_ub, float radius,
+                     int32_t want_normals, const float* sensor, lw_nbr_buf* nb, int32_t* out_cnt, float* out_nrm,
+                     float* out_curv, void* stream);
+
 /* Clear the integration map (gpu.py:1305-1313). */
 int lw_map_clear(lw_map* map, void* stream);
 

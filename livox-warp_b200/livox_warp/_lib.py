@@ -88,6 +88,11 @@ class ClusterBuf(C.Structure):
     _fields_ = [(n, P) for n in PTRS] + [("cap", i64), ("pt_cap", i64), ("edge_cap", i64)]
 
 
+class NbrBuf(C.Structure):
+    PTRS = ("keys", "acc", "vidx", "v_slot", "slot_of_pt", "v_xyz", "v_w", "v_cnt", "v_nrm", "v_curv", "tiles", "m")
+    _fields_ = [(n, P) for n in PTRS] + [("cap", i64), ("pt_cap", i64)]
+
+
 class PriorGrid(C.Structure):
     """mapgrid.Grid (mapgrid.py:35-43) plus the map arrays the grid kernels read."""
 
@@ -171,6 +176,7 @@ _SIGS = {
     "lw_frame_ids": (i32, [P, i64, f32, P, P]),
     "lw_ground": (i32, [P, i32, P, P, i64, f32, f32, i32, f32, f32, i32, f32, P, P, P, P, P]),
     "lw_cluster": (i32, [P, i32, P, i32, P, i64, f32, f32, f32, i32, C.POINTER(ClusterBuf), P, P]),
+    "lw_neighborhoods": (i32, [P, i32, P, i64, f32, i32, P, C.POINTER(NbrBuf), P, P, P, P]),
     "lw_prior_grid_build": (i32, [C.POINTER(PriorGrid), P]),
     "lw_net_init": (i32, [C.POINTER(InitNet), C.c_uint64, P]),
     "lw_net_forward": (i32, [C.POINTER(InitNet), P, i32, P, P, P, P, P, P]),

@@ -16,7 +16,9 @@ Differences from the reference, all deliberate:
 
 from __future__ import annotations
 
+import ctypes as C
 import threading
+import time
 
 import numpy as np
 import torch
@@ -155,6 +157,9 @@ class Pipeline:
         self.c_t = torch.zeros(n, dtype=torch.float32, device=d)
         self.c_dyn = torch.zeros(n, dtype=torch.int32, device=d)
         self.nrm = torch.zeros((n, 3), dtype=torch.float32, device=d)
+        self.nbr = torch.zeros(n, dtype=torch.int32, device=d)  # point-weighted neighbour counts
+        self.curv = torch.zeros(n, dtype=torch.float32, device=d)
+        self._nb = None  # the neighbourhood pass's buffers, made on first use
         self.gnd = torch.zeros(n, dtype=torch.int32, device=d)
         self.hag = torch.zeros(n, dtype=torch.float32, device=d)
         self.cid = torch.full((n,), -1, dtype=torch.int32, device=d)
@@ -332,8 +337,8 @@ class Pipeline:
         """Classify + compact the map's visible set into c_* in slot order (gpu.py:1466-1512, map mode)."""
         if not map_on:
             raise NotImplementedError("the live-ring visible set is render-side and outside this library's scope")
-        if neighbors:
-            raise NotImplementedError("neighbourhood normals are render-side and outside this library's scope")
+        if neighbors not in ("", "count", "normals"):
+            raise ValueError(f"neighbors must be '', 'count' or 'normals', got {neighbors!r}")
         self.flush_poses()
         _lib.call("lw_map_build", C_ref(self.map_struct), C_ref(view), int(min_count), _lib.ptr(self.c_xyz),
                   _lib.ptr(self.c_attr), _lib.ptr(self.c_t), _lib.ptr(self.c_dyn), _lib.ptr(self._tiles),
@@ -342,7 +347,37 @@ class Pipeline:
         self.count = int(host[0])
         self.map_occupied, self.map_dropped = int(host[1]), int(host[2])
         self.normals_valid = False
+        if neighbors:
+            self.neighborhoods(float(radius), neighbors == "normals", sensor)
         return self.count
+
+    def neighborhoods(self, radius: float, want_normals: bool, sensor):
+        """Fill nbr (and nrm / curv) for the visible points from a voxel summary a third of `radius` wide
+        (gpu.py:1531-1557); build() calls it when asked for neighbours, and it serves load_points() sets too."""
+        n = self.count
+        if self._nb is None:
+            d, cap = self.device, 1 << (2 * self.work_cap - 1).bit_length()
+            self._nb_t = {"keys": torch.full((cap,), -1, dtype=torch.int64, device=d),
+                          "acc": torch.zeros((cap, 4), dtype=torch.int64, device=d),
+                          "vidx": torch.zeros(cap, dtype=torch.int32, device=d),
+                          "v_slot": torch.zeros(cap, dtype=torch.int32, device=d),
+                          "slot_of_pt": torch.zeros(self.work_cap, dtype=torch.int32, device=d),
+                          "v_xyz": torch.zeros((cap, 3), dtype=torch.float32, device=d),
+                          "v_w": torch.zeros(cap, dtype=torch.int32, device=d),
+                          "v_cnt": torch.zeros(cap, dtype=torch.float32, device=d),
+                          "v_nrm": torch.zeros((cap, 3), dtype=torch.float32, device=d),
+                          "v_curv": torch.zeros(cap, dtype=torch.float32, device=d),
+                          "tiles": torch.zeros(cap // 1024 + 2, dtype=torch.int32, device=d),
+                          "m": torch.zeros(1, dtype=torch.int32, device=d)}
+            self._nb = _lib.NbrBuf(*(_lib.ptr(self._nb_t[k]).value for k in _lib.NbrBuf.PTRS), cap, self.work_cap)
+        t0 = time.perf_counter()
+        sen = (C.c_float * 3)(*[float(v) for v in sensor])
+        _lib.call("lw_neighborhoods", _lib.ptr(self.c_xyz), 3, None, int(n), float(radius), int(bool(want_normals)),
+                  sen, C_ref(self._nb), _lib.ptr(self.nbr), _lib.ptr(self.nrm), _lib.ptr(self.curv),
+                  _lib.stream_ptr())
+        self.normals_valid = bool(want_normals)
+        self.nb_voxels = None  # read from the device on demand: int(self._nb_t["m"])
+        self.ms["neighbors"] = (time.perf_counter() - t0) * 1e3
 
     def load_points(self, xyz: np.ndarray):
         """Make an arbitrary world-frame point set the visible set (gpu.py:1522-1529)."""

@@ -938,6 +938,128 @@ void or_prior_distances(const or_grid* g, const float* pts, int64_t n, const dou
 
 }  // extern "C"
 
+// ---- neighbourhoods of the visible points (gpu.py:777-905) --------------------------------------------------------
+// The library's definition: points summed into voxels radius / 3 wide (int64 fixed point), each voxel's neighbours
+// the voxels whose centroid lies within the radius (found among the 7 x 7 x 7 voxel offsets), their weight,
+// weighted offsets and outer products summed in fixed point, the covariance and its eigen-decomposition in float64.
+// The reference uses float atomics and a hash-grid query order instead (its sums depend on thread timing).
+
+extern "C" {
+
+void or_neighborhoods(const float* xyz, int stride, int64_t n, float radius, int want_normals, const float* sensor,
+                      int32_t* out_cnt, float* out_nrm, float* out_curv, int threads) {
+    const float inv_h = 3.0f / radius, r2 = radius * radius;
+    const float FW = (float)1048576.0, FD = (float)1048576.0, FDD = (float)1099511627776.0;
+    std::unordered_map<int64_t, int> vox;
+    std::vector<int64_t> keys, acc;
+    std::vector<int> of_pt(n);
+    for (int64_t i = 0; i < n; ++i) {
+        const float x = xyz[stride * i], y = xyz[stride * i + 1], z = xyz[stride * i + 2];
+        const int64_t key = or_key_ijk((int)std::floor(x * inv_h), (int)std::floor(y * inv_h), (int)std::floor(z * inv_h));
+        auto it = vox.find(key);
+        int v;
+        if (it == vox.end()) {
+            v = (int)keys.size();
+            vox.emplace(key, v);
+            keys.push_back(key);
+            acc.insert(acc.end(), {0, 0, 0, 0});
+        } else {
+            v = it->second;
+        }
+        acc[4 * v + 0] += llrintf(x * FW);
+        acc[4 * v + 1] += llrintf(y * FW);
+        acc[4 * v + 2] += llrintf(z * FW);
+        acc[4 * v + 3] += 1;
+        of_pt[i] = v;
+    }
+    const int m = (int)keys.size();
+    std::vector<float> c(3 * (size_t)m), cnt(m), nrm(3 * (size_t)m), curv(m);
+    for (int v = 0; v < m; ++v) {
+        const double w = (double)acc[4 * v + 3];
+        for (int k = 0; k < 3; ++k) c[3 * v + k] = (float)((double)acc[4 * v + k] / (w * 1048576.0));
+    }
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 64)
+    for (int v = 0; v < m; ++v) {
+        const int64_t key = keys[v];
+        const int ix = (int)(key & 0x1FFFFF) - (1 << 20), iy = (int)((key >> 21) & 0x1FFFFF) - (1 << 20),
+                  iz = (int)((key >> 42) & 0x1FFFFF) - (1 << 20);
+        const float px = c[3 * v], py = c[3 * v + 1], pz = c[3 * v + 2];
+        long long W = 0, s1[3] = {0, 0, 0}, s2[6] = {0, 0, 0, 0, 0, 0};
+        for (int dx = -3; dx <= 3; ++dx)
+            for (int dy = -3; dy <= 3; ++dy)
+                for (int dz = -3; dz <= 3; ++dz) {
+                    auto it = vox.find(or_key_ijk(ix + dx, iy + dy, iz + dz));
+                    if (it == vox.end()) continue;
+                    const int k = it->second;
+                    const float ex = c[3 * k] - px, ey = c[3 * k + 1] - py, ez = c[3 * k + 2] - pz;
+                    if (ex * ex + ey * ey + ez * ez > r2) continue;
+                    const long long wk = acc[4 * k + 3];
+                    W += wk;
+                    s1[0] += wk * llrintf(ex * FD);
+                    s1[1] += wk * llrintf(ey * FD);
+                    s1[2] += wk * llrintf(ez * FD);
+                    s2[0] += wk * llrintf(ex * ex * FDD);
+                    s2[1] += wk * llrintf(ex * ey * FDD);
+                    s2[2] += wk * llrintf(ex * ez * FDD);
+                    s2[3] += wk * llrintf(ey * ey * FDD);
+                    s2[4] += wk * llrintf(ey * ez * FDD);
+                    s2[5] += wk * llrintf(ez * ez * FDD);
+                }
+        cnt[v] = (float)W;
+        if (!want_normals) continue;
+        double tx = (double)sensor[0] - (double)px, ty = (double)sensor[1] - (double)py, tz = (double)sensor[2] - (double)pz;
+        const double tl = std::sqrt(tx * tx + ty * ty + tz * tz);
+        if (tl > 0.0) {
+            tx /= tl;
+            ty /= tl;
+            tz /= tl;
+        }
+        const double inv = 1.0 / std::max((double)W, 1.0);
+        const double mu[3] = {(double)s1[0] / 1048576.0 * inv, (double)s1[1] / 1048576.0 * inv,
+                              (double)s1[2] / 1048576.0 * inv};
+        const int up[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+        double C[9], ev[3], Q[9];
+        for (int r = 0; r < 3; ++r)
+            for (int q = 0; q < 3; ++q) C[r * 3 + q] = (double)s2[up[r * 3 + q]] / 1099511627776.0 * inv - mu[r] * mu[q];
+        jacobi<3>(C, ev, Q);
+        int kmin = 0;
+        if (ev[1] < ev[kmin]) kmin = 1;
+        if (ev[2] < ev[kmin]) kmin = 2;
+        double nx = Q[0 * 3 + kmin], ny = Q[1 * 3 + kmin], nz = Q[2 * 3 + kmin];
+        const double nl = std::sqrt(nx * nx + ny * ny + nz * nz);
+        if (nl > 0.0) {
+            nx /= nl;
+            ny /= nl;
+            nz /= nl;
+        }
+        if (nx * tx + ny * ty + nz * tz < 0.0) {
+            nx = -nx;
+            ny = -ny;
+            nz = -nz;
+        }
+        const double tr = ev[0] + ev[1] + ev[2];
+        if (tr <= 1.0e-12) {
+            nx = tx;
+            ny = ty;
+            nz = tz;
+        }
+        nrm[3 * v] = (float)nx;
+        nrm[3 * v + 1] = (float)ny;
+        nrm[3 * v + 2] = (float)nz;
+        curv[v] = (float)(std::max(ev[kmin], 0.0) / std::max(tr, 1.0e-12));
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        const int v = of_pt[i];
+        out_cnt[i] = (int)(cnt[v] + 0.5f);
+        if (want_normals) {
+            for (int k = 0; k < 3; ++k) out_nrm[3 * i + k] = nrm[3 * v + k];
+            out_curv[i] = curv[v];
+        }
+    }
+}
+
+}  // extern "C"
+
 // ---- coarse hypothesis scores (localize.py:55-123, k_score_grid / k_score_list) --------------------------------
 // Two sums. By default the definition the library computes: the soft count formed exactly from the number of
 // points with d < tau and the sum of their d^2 (integers), rounded once. With ref, the reference's own sum: float32

@@ -88,6 +88,7 @@ def lib() -> C.CDLL:
             "or_prior_distances": (None, [C.POINTER(OrGrid), P, i64, P, P, i32]),
             "or_loc_icp": (None, [C.POINTER(OrGrid), P, P, P, i32, P, i32, P, P, P, f32, i32, P, P, i32]),
             "or_loc_eval": (None, [C.POINTER(OrGrid), P, P, P, i32, P, P, P, i32]),
+            "or_neighborhoods": (None, [P, i32, i64, f32, i32, P, P, P, P, i32]),
             "or_score_grid": (None, [C.POINTER(OrGrid), P, P, i32, P, i64, i32, f32, f32, f32, f32, i32, P, i32]),
             "or_score_list": (None, [C.POINTER(OrGrid), P, P, i32, P, i64, f32, i32, P, i32]),
         }
@@ -254,6 +255,20 @@ def ground(xyz, cell=0.5, thick=0.15, min_sup=3, thresh=0.2, slope_step=0.3, nrm
     lib().or_ground(_p(xyz), xyz.shape[1], None if nrm_a is None else _p(nrm_a), n, cell, thick, min_sup, thresh,
                     slope_step, int(nrm_a is not None), nz_min, _p(gnd), _p(hag))
     return gnd, hag
+
+
+def neighborhoods(xyz, radius: float, want_normals: bool, sensor=(0.0, 0.0, 0.0)):
+    """gpu.py:777-905 as the library defines it (exact voxel sums, neighbours among the 7^3 voxel offsets):
+    (count int32 [n], normal [n, 3], curvature [n])."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+    n = len(xyz)
+    cnt = np.zeros(n, np.int32)
+    nrm = np.zeros((n, 3), np.float32)
+    curv = np.zeros(n, np.float32)
+    sen = np.ascontiguousarray(sensor, dtype=np.float32)
+    lib().or_neighborhoods(_p(xyz), 3, n, float(radius), int(bool(want_normals)), _p(sen), _p(cnt), _p(nrm),
+                           _p(curv), threads())
+    return cnt, nrm, curv
 
 
 def cluster(xyz, gnd=None, voxel=0.1, connect=0.35, min_pts=30, max_out=4096):
