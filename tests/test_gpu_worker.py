@@ -41,7 +41,8 @@ def _collect(w, want, timeout=120.0):
     while len(got) < want and time.time() - t0 < timeout and w._thread.is_alive():
         for r in w.poll():
             arr = r.arrays()  # empty when the output slots were all taken (own-or-drop): the pose still arrives
-            got[r.k] = (r.T, r.m, arr[0].clone() if arr else None, arr[1].clone() if arr else None, r.gen)
+            got[r.k] = (r.T, r.m, arr[0].clone() if arr else None, arr[1].clone() if arr else None, r.gen,
+                        arr[2].cpu().numpy() if arr else None, arr[3].cpu().numpy() if arr else None)
         torch.cuda.current_stream().synchronize()
         w.release_consumed()
         time.sleep(0.002)
@@ -70,9 +71,13 @@ def test_worker_matches_direct_odometry():
     assert sorted(got) == sorted(want) and len(want) == len(frames) - 1  # the last frame is still open
     for k in want:
         T, m, fx, fa = want[k]
-        gT, gm, gx, ga, gen = got[k]
+        gT, gm, gx, ga, gen, gt, gf = got[k]
         assert np.array_equal(gT, T) and gm == m and gen == 1
         assert torch.equal(gx, fx) and torch.equal(ga, fa)
+        # no torn snapshot (check_slam_worker.py:156-163): the frame's points carry its own frame id (or the
+        # previous one, for slightly late points) and times within a frame of it
+        assert np.isin(gf, [k & 0xFFFF, (k - 1) & 0xFFFF]).all()
+        assert ((gt >= (k - 1) * 0.1 - 1e-4) & (gt < (k + 1) * 0.1 + 1e-4)).all()
     assert st["drops"] == {"input_full": 0, "input_own": 0, "output_pool": 0, "stale": 0, "error": 0}, st
     assert st["processed"] == len(frames) and st["frames"] == len(want)
 
