@@ -36,6 +36,11 @@ its own static 360-degree scan of U[2k, 20k] points taken at a free pose (z = 1.
 that pose snapped to a 0.5 m xy grid and a 5 deg heading grid; one step = one batched registration of all 256
 (the schedule (0.40, 8), (0.20, 8), (0.10, 8), (0.05, 10)) plus the evaluation, in one graph-replayed launch.
 
+`--workload coarse` measures the coarse global search (localize.py:426-448): the office prior map at 30 mm, one
+1024-point scan subset, every free position on a 0.25 m xy grid at 8 heights x 180 headings (28M hypotheses) scored
+by the distance-field soft count in one launch; hypotheses/s, with e2e through GlobalLocalizer._coarse_candidates
+(the local maxima found on the device, only the candidates read back).
+
 Multi-GPU: the path does not shard (each frame registers against the map of the frames before it), so
 `--gpus N` runs N independent replicas, one per GPU, and `value` sums their frames.
 """
