@@ -316,6 +316,20 @@ int lw_neighborhoods(const float* xyz, int32_t xyz_stride, const int32_t* n_dev,
                      int32_t want_normals, const float* sensor, lw_nbr_buf* nb, int32_t* out_cnt, float* out_nrm,
                      float* out_curv, void* stream);
 
+/* LVXR recordings (host). lw_lvxr_decode decodes a whole recording held in memory into every firing with its
+ * exact time, the empty ones included (lvxr.py read_firings :189-260, the datagrams of record.rs / point.rs):
+ * n firings of up to R returns each, time-ordered. lw_lvxr_info reports n, R, the device type, the profile and the
+ * firing interval (s); lw_lvxr_copy fills t [n] float64 s, xyz [n*R*3] float32 m (sensor frame, zero where a return
+ * slot is empty), refl / tag / valid [n*R] uint8 and direction [n*3] float32 (NaN where the data gives none); the
+ * decoded recording is host memory owned by the handle until lw_lvxr_free. */
+typedef struct lw_lvxr lw_lvxr;
+int lw_lvxr_decode(const uint8_t* data, int64_t size, lw_lvxr** out);
+int lw_lvxr_info(const lw_lvxr* r, int64_t* n_firings, int32_t* returns, int32_t* dev_type, int32_t* profile,
+                 double* interval_s);
+int lw_lvxr_copy(const lw_lvxr* r, double* t, float* xyz, uint8_t* refl, uint8_t* tag, uint8_t* valid,
+                 float* direction);
+void lw_lvxr_free(lw_lvxr* r);
+
 /* Clear the integration map (gpu.py:1305-1313). */
 int lw_map_clear(lw_map* map, void* stream);
 

@@ -177,6 +177,10 @@ _SIGS = {
     "lw_ground": (i32, [P, i32, P, P, i64, f32, f32, i32, f32, f32, i32, f32, P, P, P, P, P]),
     "lw_cluster": (i32, [P, i32, P, i32, P, i64, f32, f32, f32, i32, C.POINTER(ClusterBuf), P, P]),
     "lw_neighborhoods": (i32, [P, i32, P, i64, f32, i32, P, C.POINTER(NbrBuf), P, P, P, P]),
+    "lw_lvxr_decode": (i32, [P, i64, C.POINTER(P)]),
+    "lw_lvxr_info": (i32, [P, C.POINTER(i64), C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), C.POINTER(f64)]),
+    "lw_lvxr_copy": (i32, [P, P, P, P, P, P, P]),
+    "lw_lvxr_free": (None, [P]),
     "lw_prior_grid_build": (i32, [C.POINTER(PriorGrid), P]),
     "lw_net_init": (i32, [C.POINTER(InitNet), C.c_uint64, P]),
     "lw_net_forward": (i32, [C.POINTER(InitNet), P, i32, P, P, P, P, P, P]),

@@ -11,6 +11,9 @@ device solve:
 
   host_solve.npz    odom.py _sym6, _twist_between, _apply_twist, _body_twist, _twist_matrix, _sensor_basis,
                     _constrained_step; localize.py _twist_apply, _rotz, pose_difference; gpu.py mount_matrix.
+  lvxr.npz          lvxr.py read_firings and Firings.points on seeded synthetic recordings (every record
+                    layout, ns and GPS timestamps, clock jumps, IMU / malformed / truncated datagrams, the Mid-40
+                    dual-return profile, LVXR1); lvxr.py imports only numpy and is loaded from its file.
   prior_prepare.npz mapgrid.py PriorGrid.prepare (a static method, taken out of its class) with
                     horizontal_levels and the module constants it reads (CELL, IDX_BITS, MAX_POINTS, PLANAR; the
                     one Warp call among them, wp.constant, is the identity here).
@@ -153,12 +156,140 @@ def prior_prepare(ref: Path) -> dict:
             "levels_bin": np.float64(lv[2])}
 
 
+# ---- LVXR recordings ---------------------------------------------------------------------------------------------
+# Seeded synthetic recordings in the LVXR format (record.rs: `LVXR2\n`, dev_type, profile, then per datagram
+# host_ns:u64 len:u16 and the datagram; a datagram is an 18-byte data-packet header -- version, slot, id, rsvd,
+# status u32, timestamp type, data type, timestamp u64 -- and its records), decoded by the reference's own reader
+# (lvxr.py imports only numpy, so it is loaded from its file).
+
+REC_SIZE = {0: 13, 1: 9, 2: 14, 3: 10, 4: 28, 5: 16, 7: 42, 8: 22}
+
+
+def _records(rng, dtype: int, n: int) -> bytes:
+    """n random records of a data type; about 15 % of the returns empty (all-zero coordinates or depth)."""
+    out = bytearray()
+    for _ in range(n):
+        def cart():
+            if rng.uniform() < 0.15:
+                return (0).to_bytes(12, "little")
+            return b"".join(int(v).to_bytes(4, "little", signed=True) for v in rng.integers(-20000, 20000, 3))
+
+        def sph_depth():
+            return int(0 if rng.uniform() < 0.15 else rng.integers(300, 40000)).to_bytes(4, "little")
+
+        refl, tag = int(rng.integers(0, 256)), int(rng.integers(0, 4)) << int(rng.integers(0, 3)) * 2
+        if dtype == 0:
+            out += cart() + bytes([refl])
+        elif dtype == 2:
+            out += cart() + bytes([refl, tag])
+        elif dtype in (1, 3):
+            out += sph_depth() + int(rng.integers(0, 18000)).to_bytes(2, "little")
+            out += int(rng.integers(0, 36000)).to_bytes(2, "little") + bytes([refl] + ([tag] if dtype == 3 else []))
+        elif dtype in (4, 7):
+            for _ in range(2 if dtype == 4 else 3):
+                out += cart() + bytes([int(rng.integers(0, 256)), int(rng.integers(0, 4))])
+        else:  # 5, 8
+            out += int(rng.integers(0, 18000)).to_bytes(2, "little") + int(rng.integers(0, 36000)).to_bytes(2, "little")
+            for _ in range(2 if dtype == 5 else 3):
+                out += sph_depth() + bytes([int(rng.integers(0, 256)), int(rng.integers(0, 4))])
+    assert len(out) == n * REC_SIZE[dtype]
+    return bytes(out)
+
+
+def _datagram(ts_type: int, dtype: int, ts: int, body: bytes, gps=None) -> bytes:
+    if gps is not None:  # (hour, microseconds in the hour)
+        stamp = bytes([24, 1, 1, gps[0]]) + int(gps[1]).to_bytes(4, "little")
+    else:
+        stamp = int(ts).to_bytes(8, "little")
+    return bytes([5, 0, 0, 0]) + (0).to_bytes(4, "little") + bytes([ts_type, dtype]) + stamp + body
+
+
+def _frame(dg: bytes, host_ns: int) -> bytes:
+    return int(host_ns).to_bytes(8, "little") + len(dg).to_bytes(2, "little") + dg
+
+
+def lvxr_recordings(seed: int = 11) -> dict:
+    rng = np.random.default_rng(seed)
+    recs = {}
+    # a standard Mid-40 recording: cartesian and spherical packets, an IMU packet, a malformed packet, a forward
+    # clock jump, the clock going backwards (a new base), a truncated last datagram
+    body, t, host = bytearray(b"LVXR2\n" + bytes([1, 0])), 5_000_000_000, 0
+    for k in range(14):
+        dtype = 0 if k % 3 else 1
+        dg = _datagram(0, dtype, t, _records(rng, dtype, 100))
+        if k == 4:
+            dg = _datagram(0, 6, t, bytes(24))  # IMU: skipped
+        if k == 7:
+            dg = dg[:-5]  # malformed: not a whole number of records
+        body += _frame(dg, host)
+        t += 100 * 10_000 + (2_500_000_000 if k == 9 else 0)
+        if k == 11:
+            t = 1_000_000_000  # the clock restarted
+        host += 1_000_000
+    body += _frame(_datagram(0, 0, t, _records(rng, 0, 100)), host)[:-40]  # truncated
+    recs["mid40"] = bytes(body)
+    # a Horizon (fast device) with the extended, dual and triple types, ns and GPS timestamps
+    body, t = bytearray(b"LVXR2\n" + bytes([3, 0])), 7_000_000_000
+    for k in range(16):
+        dtype = [2, 3, 4, 5, 7, 8][k % 6]
+        n_rec = int(rng.integers(20, 96))
+        if k % 5 == 4:
+            hour, us = 2, 1_000_000 + k * 600_000
+            dg = _datagram(3, dtype, 0, _records(rng, dtype, n_rec), gps=(hour, us))
+        else:
+            dg = _datagram(0, dtype, t, _records(rng, dtype, n_rec))
+        body += _frame(dg, k)
+        t += n_rec * 4_167
+    recs["horizon"] = bytes(body)
+    # the Mid-40 dual-return profile: plain records in pairs, 100 per packet; one packet of 98 is rejected
+    body, t = bytearray(b"LVXR2\n" + bytes([1, 1])), 3_000_000_000
+    for k in range(10):
+        dtype = 0 if k % 2 else 1
+        dg = _datagram(0, dtype, t, _records(rng, dtype, 98 if k == 6 else 100))
+        body += _frame(dg, k)
+        t += 50 * 10_000
+    recs["dual"] = bytes(body)
+    # LVXR1: no profile byte
+    body, t = bytearray(b"LVXR1\n" + bytes([1])), 2_000_000_000
+    for k in range(4):
+        body += _frame(_datagram(0, 0, t, _records(rng, 0, 100)), k)
+        t += 100 * 10_000
+    recs["v1"] = bytes(body)
+    return recs
+
+
+def lvxr(ref: Path) -> dict:
+    import importlib.util
+    import tempfile
+
+    spec = importlib.util.spec_from_file_location("ref_lvxr", ref / "python" / "livox_warp" / "lvxr.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["ref_lvxr"] = mod  # its dataclasses look their module up
+    spec.loader.exec_module(mod)
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, data in lvxr_recordings().items():
+            path = Path(tmp) / f"{name}.lvxr"
+            path.write_bytes(data)
+            f = mod.read_firings(path)
+            px, pa, pt, pf = f.points(clean=True, min_range=0.3)
+            out.update({f"{name}_bytes": np.frombuffer(data, np.uint8), f"{name}_t": f.t, f"{name}_xyz": f.xyz,
+                        f"{name}_refl": f.refl, f"{name}_tag": f.tag, f"{name}_valid": f.valid,
+                        f"{name}_direction": f.direction,
+                        f"{name}_meta": np.array([f.dev_type, f.profile], np.int64),
+                        f"{name}_interval": np.float64(f.interval), f"{name}_pts_xyz": px, f"{name}_pts_attr": pa,
+                        f"{name}_pts_t": pt, f"{name}_pts_f": pf})
+    return out
+
+
 def main():
     ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
     np.savez_compressed(HERE / "host_solve.npz", **host_solve(ref))
     print("wrote", HERE / "host_solve.npz")
     np.savez_compressed(HERE / "prior_prepare.npz", **prior_prepare(ref))
     print("wrote", HERE / "prior_prepare.npz")
+    np.savez_compressed(HERE / "lvxr.npz", **lvxr(ref))
+    print("wrote", HERE / "lvxr.npz")
 
 
 if __name__ == "__main__":
