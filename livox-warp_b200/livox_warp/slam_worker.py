@@ -30,7 +30,6 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from . import _lib
 from .gpu import Pipeline
 from .odom import Odometry
 

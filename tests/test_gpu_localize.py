@@ -203,8 +203,6 @@ def test_degenerate_hypotheses_keep_pose(room):
 
 
 def test_argument_errors(room):
-    import ctypes as C
-
     from livox_warp import _lib
     from livox_warp.localize import GlobalLocalizer
 

@@ -4,7 +4,6 @@ the covariance float64 on both sides."""
 
 import numpy as np
 import pytest
-import torch
 
 import common
 from oracle import oracle
