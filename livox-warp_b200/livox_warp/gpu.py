@@ -376,8 +376,12 @@ class Pipeline:
                   sen, C_ref(self._nb), _lib.ptr(self.nbr), _lib.ptr(self.nrm), _lib.ptr(self.curv),
                   _lib.stream_ptr())
         self.normals_valid = bool(want_normals)
-        self.nb_voxels = None  # read from the device on demand: int(self._nb_t["m"])
         self.ms["neighbors"] = (time.perf_counter() - t0) * 1e3
+
+    @property
+    def nb_voxels(self) -> int:
+        """Voxels of the last neighbourhood pass (gpu.py:1547); reading it synchronises the stream."""
+        return 0 if self._nb is None else int(self._nb_t["m"].item())
 
     def load_points(self, xyz: np.ndarray):
         """Make an arbitrary world-frame point set the visible set (gpu.py:1522-1529)."""

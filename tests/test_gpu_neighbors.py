@@ -36,6 +36,7 @@ def test_neighborhoods_bit_exact(radius, normals):
     ocnt, onrm, ocurv = oracle.neighborhoods(xyz, radius, normals, sensor)
     assert np.array_equal(cnt, ocnt)
     assert cnt.min() >= 1 and np.median(cnt) > 5
+    assert 0 < pipe.nb_voxels < n
     assert pipe.normals_valid == normals
     if normals:
         nrm = pipe.nrm[:n].cpu().numpy()
