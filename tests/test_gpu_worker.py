@@ -128,3 +128,33 @@ def test_own_or_drop_and_configure():
     finally:
         w.close()
     assert w.odom.max_iter == 8 and not w._thread.is_alive()
+
+
+def test_restart_clock_keeps_going_on_the_new_clock():
+    """A replay loop: the clock restarts at 0; after restart_clock() the frames of the new clock arrive (new
+    generation, frame ids from 0 again) and nothing of the old clock does."""
+    from livox_warp import gpu
+    from livox_warp.slam_worker import OdomWorker
+
+    frames = common.handheld_frames(8)
+    T0 = common.mid_pose(common.handheld(), 0)
+    pipe = gpu.Pipeline(ring_capacity=1 << 16, map_capacity=1 << 18)
+    w = OdomWorker(pipe, frame_cap=1 << 15, reg_slots=1 << 19, in_slots=64)
+    try:
+        w.configure(reg_voxel=VOXEL)
+        w.reset(T0)
+        for x, a, t in frames:
+            sx, sa, st, sf = pipe.stage(x, a, t, len(t), 10.0)
+            assert w.submit(sx, sa, st, len(t), float(t.min()), float(t.max()))
+        first = _collect(w, 7)
+        w.restart_clock()
+        for x, a, t in frames[:5]:
+            sx, sa, st, sf = pipe.stage(x, a, t, len(t), 10.0)
+            assert w.submit(sx, sa, st, len(t), float(t.min()), float(t.max()))
+        second = _collect(w, 4)
+        gen, st = w.gen, w.status()
+    finally:
+        w.close()
+    assert sorted(first) == list(range(7)) and all(v[4] == 1 for v in first.values())
+    assert gen == 2 and sorted(second) == list(range(4)) and all(v[4] == 2 for v in second.values())
+    assert st["drops"]["error"] == 0
