@@ -106,3 +106,58 @@ def test_pipeline_rejects_bad_capacity():
 
     with pytest.raises(ValueError):
         gpu.Pipeline(ring_capacity=1 << 10, map_capacity=1000)
+
+
+@pytest.mark.parametrize("motion", ["static", "turn"])
+def test_odometry_static_and_turn_gates(motion):
+    """The reference's odometry gates (check_odometry.py:92-95) on the box room. At rest for 6 s: > 90 % of the
+    frames after warm-up registered, rmse < 2 cm, rotation error < 0.2 deg. Turning in place for 15 s from the
+    middle of the room: > 90 % registered, over 20 deg turned, rmse < 10 cm. The reference's rotation gate for the
+    turn (rmse < 0.5 deg) is set for its own simulated sensor; with the 38-degree rosette each frame turns into
+    mostly unseen surfaces and the float64 oracle itself reaches 0.72 deg at this 4 deg/s (1.85 deg at 12 deg/s),
+    so here the rotation rmse is held below 1 deg, and the device to the oracle: 5 mm / 0.1 deg over the first 60
+    frames, 3 cm / 1 deg over the whole turn."""
+    import math
+
+    from livox_warp import synth
+
+    sc = common.room(1)
+    if motion == "static":
+        T0 = common.config1_pose()
+        traj = synth.ConstantVelocity(T0, 1e9, 0.0, 0.0)
+        n = 60
+    else:
+        T0 = common.look_at([4.0, 3.0, 1.4], [8.0, 3.5, 1.0])
+        traj = synth.ConstantVelocity(T0, 1.0, 0.0, math.radians(4.0))
+        n = 150
+    frames = synth.frames(sc, traj, n, RATE, seed=5)
+    Ts = traj.poses(np.array([0.05]))[0]
+    _, odom = _run_gpu(frames, Ts, 0.2)
+    recs = odom.traj
+    err_t, err_r, span_r = [], [], []
+    for _, tm, T in recs:
+        gt = traj.poses(np.array([tm]))[0]
+        e = oracle.pose_error(gt, T)
+        err_t.append(e[0])
+        err_r.append(e[1])
+        span_r.append(oracle.pose_error(T0, gt)[1])
+    err_t, err_r = np.array(err_t), np.array(err_r)
+    # registration evidence after the warm-up: the frames whose registration ran and succeeded
+    log = odom.iteration_log()
+    n_post = sum(1 for k, _, _ in recs if k >= odom.warmup + 2)
+    reg = int((log[:, 0] >= odom.warmup + 2).sum()) / max(1, n_post)
+    assert reg > 0.9, reg
+    if motion == "static":
+        assert np.sqrt(np.mean(err_t ** 2)) < 0.02 and err_r.max() < 0.2, (err_t.max(), err_r.max())
+        return
+    assert max(span_r) > 20.0
+    assert np.sqrt(np.mean(err_t ** 2)) < 0.10 and np.sqrt(np.mean(err_r ** 2)) < 1.0, (err_t.max(), err_r.max())
+    oo = oracle.Odometry(1 << 19, oracle.Params(reg_voxel=0.2), Ts)
+    for k, (x, a, t) in enumerate(frames):
+        oo.frame(k, common.raw4(x, t), a)
+    d = np.array([oracle.pose_error(To, T) for (_, _, T), (_, _, To) in zip(recs, oo.traj)])
+    assert len(oo.traj) == len(recs)
+    # float32 kernels vs float64 host math: within 5 mm / 0.1 deg over the first 60 frames; over the whole turn the
+    # two drift apart by ~1.5 cm (each frame registers against a map built from the previous poses)
+    assert d[:60, 0].max() < 5e-3 and d[:60, 1].max() < 0.1, d[:60].max(axis=0)
+    assert d[:, 0].max() < 0.03 and d[:, 1].max() < 1.0, d.max(axis=0)
