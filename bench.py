@@ -293,8 +293,10 @@ def roofline(res, frames, traj, warmup, steps, peak):
         bytes_per_launch = float(np.mean(per_launch))
     avg_ms = ms / max(cnt, 1)
     achieved = bytes_per_launch / (avg_ms * 1e-3) / 1e9
+    traffic = SEQ_TRAFFIC.get(name)
     return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 3), "peak": peak["hbm_gbs"], "unit": "GB/s",
-            "frac": round(achieved / peak["hbm_gbs"], 5), "traffic": None,
+            "frac": round(achieved / peak["hbm_gbs"], 5), "traffic": traffic,
+            "traffic_source": SEQ_TRAFFIC_SRC if traffic else None,
             "peak_source": peak["source"], "avg_launch_us": round(avg_ms * 1e3, 2), "launches": int(cnt),
             "algorithmic_bytes_per_launch": int(bytes_per_launch),
             "kernel_ms_share": {n: round(prof[n][0] / max(sum(v[0] for v in prof.values()), 1e-9), 4) for n in prof}}
@@ -318,6 +320,14 @@ def pose_drift(odom, traj, oracle_poses: dict) -> dict:
             "gt_max_m": round(float(g[:, 0].max()), 4), "gt_rot_rmse_deg": round(float(np.sqrt((g[:, 1] ** 2).mean())), 3),
             "vs_fp64_oracle_frames": len(orc), "vs_fp64_oracle_max_m": round(float(o[:, 0].max()), 6),
             "vs_fp64_oracle_max_deg": round(float(o[:, 1].max()), 5)}
+
+
+# DRAM bytes (read + write) per launch from one ncu capture of the sequence (profiles/k_gn_k_carve_sequence.md,
+# rounded as summarised there) and of the coarse search (profiles/k_score_grid_office_coarse.md)
+SEQ_TRAFFIC = {"gn": 1_943_000, "carve": 6_928_000}  # carve: both passes (setup + walk)
+SEQ_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_gn_k_carve_sequence.md"
+COARSE_TRAFFIC = 42_780_928 + 71_592_448
+COARSE_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_score_grid_office_coarse.md"
 
 
 def measured_peak():
@@ -1064,7 +1074,8 @@ def run_coarse(a, rank: int, world: int, local: int):
     peak = measured_peak()
     ach = ubytes / (avg_ms * 1e-3) / 1e9
     roof = {"kernel": "k_score_grid", "bound": "hbm", "achieved": round(ach, 3), "peak": peak["hbm_gbs"],
-            "unit": "GB/s", "frac": round(ach / peak["hbm_gbs"], 5), "traffic": None, "peak_source": peak["source"],
+            "unit": "GB/s", "frac": round(ach / peak["hbm_gbs"], 5), "traffic": COARSE_TRAFFIC,
+            "traffic_source": COARSE_TRAFFIC_SRC, "peak_source": peak["source"],
             "avg_launch_us": round(avg_ms * 1e3, 2), "algorithmic_bytes_per_launch": ubytes,
             "byte_gathers_per_launch": int(n_hyp * len(w["pts"])),
             "gathers_per_s": round(n_hyp * len(w["pts"]) / (avg_ms * 1e-3), 1),
