@@ -41,6 +41,11 @@ that pose snapped to a 0.5 m xy grid and a 5 deg heading grid; one step = one ba
 by the distance-field soft count in one launch; hypotheses/s, with e2e through GlobalLocalizer._coarse_candidates
 (the local maxima found on the device, only the candidates read back).
 
+`--workload prior` measures the prior-map builder (prior_map.py:57-219, from_points :358-370): the office's surfaces
+sampled every 10 mm with 2 mm jitter (45.7M points, a building-scale terrestrial scan), voxel means at 20 mm in a
+2^27-slot table (chunks of 2^25 points) and a PCA normal and planarity per mean from its neighbours within 80 mm;
+input points/s, with e2e through prior_map.from_points from host arrays to host arrays.
+
 Multi-GPU: the path does not shard (each frame registers against the map of the frames before it), so
 `--gpus N` runs N independent replicas, one per GPU, and `value` sums their frames.
 """
@@ -1107,6 +1112,147 @@ def run_coarse(a, rank: int, world: int, local: int):
     print(json.dumps(line))
 
 
+PRIOR_SPACING, PRIOR_VOXEL, PRIOR_RADIUS, PRIOR_SLOTS = 0.01, 0.02, 0.08, 27
+
+
+def prior_workload():
+    """The office's surfaces every 10 mm with 2 mm jitter: a building-scale terrestrial scan's density."""
+    from livox_warp import synth
+
+    xyz, _ = synth.sample_surfaces(synth.office(LOC_SEED), PRIOR_SPACING, LOC_SEED, jitter=0.002)
+    return np.ascontiguousarray(xyz, dtype=np.float32)
+
+
+def run_prior(a, rank: int, world: int, local: int):
+    from oracle import oracle as _o
+
+    xyz = prior_workload()
+    n = len(xyz)
+    metric = "prior-map build input points/s (voxel means + PCA normals and planarity)"
+    config = {"workload": f"prior map from a cloud: office 40x30x3 m surfaces every {PRIOR_SPACING * 1e3:.0f} mm "
+                          f"({n:,} pts), voxel {PRIOR_VOXEL * 1e3:.0f} mm (2^{PRIOR_SLOTS} slots, chunks of 2^25), "
+                          f"normal radius {PRIOR_RADIUS * 1e3:.0f} mm (prior_map.py:57-219)",
+              "points": int(n), "l2": "inputs larger than L2, and flushed between steps (256 MB write)",
+              "parallelism": f"replicas x{a.gpus}"}
+    threads = _o.host_cores()
+
+    def cpu_run():
+        t0 = time.perf_counter()
+        vx, _, _, vn = _o.voxel_downsample(xyz, None, None, PRIOR_VOXEL)
+        t1 = time.perf_counter()
+        nrm, pl = _o.normals(vx, PRIOR_RADIUS)
+        return vx, vn, nrm, pl, t1 - t0, time.perf_counter() - t1
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        _, _, _, _, sv, sn = cpu_run()
+        secs = sv + sn
+        v = n / secs
+        print(json.dumps({"impl": "reference", "metric": metric, "value": round(v, 1), "unit": "points/s",
+                          "n_gpus": a.gpus, "steps": 1, "warmup": 0, "ms_per_step": round(1e3 * secs, 3),
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                          "data": "synthetic", "config": config,
+                          "cpu_baseline": {"value": round(v, 1), "unit": "points/s", "cores": threads,
+                                           "kind": "port", "sample": f"the whole cloud once through the CPU "
+                                                                     f"restatement (voxels 1 thread {sv:.1f} s, "
+                                                                     f"normals {threads} threads {sn:.1f} s)"},
+                          "e2e": {"value": round(v, 1), "unit": "points/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+    import torch
+
+    from livox_warp import _lib, prior_map
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    stream = torch.cuda.current_stream(device)
+    x_dev = torch.from_numpy(xyz).to(device)
+    table = prior_map.VoxelTable(PRIOR_VOXEL, PRIOR_SLOTS, 1 << 25, device)
+    table.insert(x_dev)
+    m, dropped = table.totals()
+    assert dropped == 0
+    bufs = prior_map.NormalBuffers(m, device)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    out = {}
+
+    def dev_step():
+        table.clear(stream)
+        table.insert(x_dev, stream=stream)
+        vx, _, _, vn = table.emit(stream, m=m)
+        nrm, pl = prior_map.normals_device(vx, PRIOR_RADIUS, stream, bufs)
+        out.update(vx=vx, vn=vn, nrm=nrm, pl=pl)
+
+    for _ in range(a.warmup):
+        dev_step()
+    torch.cuda.synchronize(device)
+    clocks = Clocks(local)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    _lib.launches(reset=True)
+    _lib.prof_reset()
+    _lib.prof_enable(True)
+    clocks.start()
+    torch.cuda.synchronize(device)
+    for j in range(a.steps):
+        flush.fill_(float(j))
+        evs[j][0].record(stream)
+        dev_step()
+        evs[j][1].record(stream)
+    torch.cuda.synchronize(device)
+    clk = clocks.stop()
+    launches = _lib.launches()
+    kern = {k: _lib.prof_read(k) for k in ("lw_vox_insert", "lw_vox_emit", "lw_normals")}
+    _lib.prof_enable(False)
+    assert table.totals() == (m, 0)
+    step_ms = np.array([x.elapsed_time(y) for x, y in evs])
+    ms_total = max_over_ranks(float(step_ms.sum()), device)
+    value = replica_rate(a.steps * n, world, ms_total)
+    # e2e: the public call from host arrays to host arrays (upload, build, both kernels, read back)
+    for _ in range(2):
+        prior_map.from_points(xyz, PRIOR_VOXEL, PRIOR_RADIUS, device, slots_log2=PRIOR_SLOTS)
+    torch.cuda.synchronize(device)
+    e_steps = max(3, min(a.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        pm = prior_map.from_points(xyz, PRIOR_VOXEL, PRIOR_RADIUS, device, slots_log2=PRIOR_SLOTS)
+    e_s = max_over_ranks(time.perf_counter() - t0, device)
+    if rank != 0:
+        return
+    vx, vn = out["vx"].cpu().numpy(), out["vn"].cpu().numpy()
+    nrm, pl = out["nrm"].cpu().numpy(), out["pl"].cpu().numpy()
+    ox, on, onrm, opl, sv, sn = cpu_run()
+    exact = bool(np.array_equal(vx, ox) and np.array_equal(vn, on) and np.array_equal(nrm, onrm)
+                 and np.array_equal(pl, opl) and np.array_equal(pm["xyz"], ox) and np.array_equal(pm["normal"], onrm))
+    avg_ms = ms_total / a.steps
+    ins_ms, nrm_ms = kern["lw_vox_insert"][0] / a.steps, kern["lw_normals"][0] / a.steps
+    # the insert's algorithmic bytes: each point read once (12 B) and its slot written and read back twice (4 B
+    # x 3), each voxel's table line (keys 8, sums 64, first 8) written once and read by the emit, the order entry
+    peak = measured_peak()
+    ins_bytes = int(n * (12 + 12) + m * (80 + 80 + 4))
+    ach = ins_bytes / (ins_ms * 1e-3) / 1e9
+    roof = {"kernel": "lw_vox_insert (k_vox_insert + first-point compaction)", "bound": "hbm",
+            "achieved": round(ach, 3), "peak": peak["hbm_gbs"], "unit": "GB/s", "frac": round(ach / peak["hbm_gbs"], 5),
+            "traffic": None, "peak_source": peak["source"], "algorithmic_bytes_per_launch": ins_bytes,
+            "avg_ms": round(ins_ms, 4),
+            "limiter": "five int64 atomics per point on its voxel's line (about four points share a 20 mm voxel)"}
+    line = {"metric": metric, "value": round(value, 1), "unit": "points/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(avg_ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 in, int64 fixed-point sums, f64 PCA", "data": "synthetic",
+            "config": config, "voxels": int(m),
+            "kernel_ms": {"lw_vox_insert": round(ins_ms, 4), "lw_vox_emit": round(kern["lw_vox_emit"][0] / a.steps, 4),
+                          "lw_normals": round(nrm_ms, 4)},
+            "normals_points_per_s": round(m / (nrm_ms * 1e-3), 1),
+            "bit_exact_vs_oracle": exact, "roofline": roof,
+            "cpu_baseline": {"value": round(n / (sv + sn), 1), "unit": "points/s", "cores": threads, "kind": "port",
+                             "sample": f"the whole cloud once through the CPU oracle (voxels 1 thread {sv:.1f} s, "
+                                       f"normals {threads} threads {sn:.1f} s)"},
+            "e2e": {"value": round(world * e_steps * n / e_s, 1), "unit": "points/s",
+                    "h2d_bytes_per_step": int(12 * n), "d2h_bytes_per_step": int(m * (12 + 12 + 4 + 4)),
+                    "path": "prior_map.from_points(host xyz) -> host xyz, normal, planarity, count"},
+            "gpu_launches": int(launches), "clocks": clk}
+    print(json.dumps(line))
+
+
 # ---- main -------------------------------------------------------------------------------------------------------
 
 
@@ -1118,7 +1264,7 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=("sequence", "localize", "frame", "learned", "coarse"),
+    ap.add_argument("--workload", choices=("sequence", "localize", "frame", "learned", "coarse", "prior"),
                     default="sequence")
     ap.add_argument("--learn-epochs", type=int, default=40, help="learned: training epochs")
     ap.add_argument("--loc-hyp", type=int, default=256, help="localize: hypotheses (a smaller profiling case)")
@@ -1141,6 +1287,9 @@ def main():
         return
     if a.workload == "coarse":
         run_coarse(a, rank, world, local)
+        return
+    if a.workload == "prior":
+        run_prior(a, rank, world, local)
         return
     n_frames = a.warmup + a.steps + 1
     metric = "ICP sequence odometry frames/s (deskew + GN ICP + keyframe insert + map insert + carve)"

@@ -316,6 +316,68 @@ int lw_neighborhoods(const float* xyz, int32_t xyz_stride, const int32_t* n_dev,
                      int32_t want_normals, const float* sensor, lw_nbr_buf* nb, int32_t* out_cnt, float* out_nrm,
                      float* out_curv, void* stream);
 
+/* Prior-map voxel table (prior_map.py:57-123, voxel_downsample :169-203): cap slots (a power of two, at most
+ * 2^30) filled chunk by chunk. Clear keys to -1 (0xFF bytes), acc and stats to 0 and first to 0x7F bytes before the
+ * first chunk (lw_vox_clear does it). */
+typedef struct lw_vox_buf {
+    int64_t* keys;       /* [cap] voxel keys of floor(p / voxel) (gpu.py voxel_key_ijk), -1 empty */
+    int64_t* acc;        /* [cap*8] per voxel: x, y, z offsets from the voxel centre (units of
+                          * lw_vox_offset_units(voxel) per metre), r, g, b, intensity (LW_VOX_FIX_ATTR units), points */
+    int64_t* first;      /* [cap] lowest point index that reached the voxel */
+    int32_t* order;      /* [cap] slot of the j-th voxel; voxels are numbered in the order of their first point */
+    int32_t* slot_of_pt; /* [pt_cap] scratch: slot of each point of a chunk, -1 when the probe window was full */
+    int32_t* tiles;      /* [pt_cap/1024 + 1] scratch */
+    int64_t* stats;      /* [2] voxels so far, points dropped (probe window full) */
+    int64_t cap, pt_cap;
+} lw_vox_buf;
+
+#define LW_VOX_FIX_ATTR 65536.0 /* prior-map voxel table: units per unit of colour and intensity, 2^16 */
+
+/* Units per metre of a prior-map voxel's offset sums: 2^(30 - e) for the smallest e with voxel < 2^e, so a point's
+ * offset from its voxel centre is below 2^29 units. */
+double lw_vox_offset_units(float voxel);
+
+/* Reset the voxel table for a new cloud. */
+int lw_vox_clear(lw_vox_buf* vb, void* stream);
+
+/* Add n points (n <= pt_cap <= 2^30) to their voxels (k_vox_insert, prior_map.py:57-91), voxel in [1e-6, 1e6] m:
+ * xyz [n*xyz_stride] (stride 3 or 4, finite), intensity [n] and rgb [n*3] optional (NULL sums zeros). index0
+ * is the number of points of the cloud inserted by earlier calls, so that every point has its own index; the
+ * voxels first reached by this chunk are appended to `order` in the order of their first point. A point whose
+ * 128-slot probe window is full counts in stats[1] and is left out (the reference raises on it). */
+int lw_vox_insert(lw_vox_buf* vb, const float* xyz, int32_t xyz_stride, const float* intensity, const float* rgb,
+                  int64_t n, int64_t index0, float voxel, void* stream);
+
+/* The first min(stats[0], m_cap) voxels as dense arrays (k_vox_emit, prior_map.py:100-123): out_xyz [m*3] the
+ * mean position (voxel centre + mean offset), out_rgb [m*3] and out_intensity [m] the mean colour and intensity,
+ * out_cnt [m] the point count; every output may be NULL. */
+int lw_vox_emit(const lw_vox_buf* vb, float voxel, int64_t m_cap, float* out_xyz, float* out_rgb,
+                float* out_intensity, int32_t* out_cnt, void* stream);
+
+/* Buffers of the normal estimation: a table of cells slightly wider than the radius (cap, a power of two, at
+ * least twice the points, at most 2^30) and the points grouped by cell. */
+typedef struct lw_pca_buf {
+    int64_t* keys;       /* [cap] cell keys, -1 empty (cleared by each call) */
+    int32_t* cell_cnt;   /* [cap] points per cell */
+    int32_t* cell_start; /* [cap] first position of each cell's points in `sorted` */
+    int32_t* slot_of_pt; /* [pt_cap] cell slot of each point, -1 when the probe window was full */
+    int32_t* rank_of_pt; /* [pt_cap] position of each point within its cell */
+    float* sorted;       /* [pt_cap*4] the points grouped by cell: x, y, z and the point index (int32 bits) */
+    int32_t* tiles;      /* [cap/1024 + 1] scan scratch */
+    int32_t* stats;      /* [2] points placed, points dropped */
+    int64_t cap, pt_cap;
+} lw_pca_buf;
+
+/* PCA normal and planarity of each of n points (n <= pt_cap <= 2^30) from all points within `radius` (1e-4 to 16 m,
+ * |q - p|^2 <= radius^2 in float32) (k_normals, prior_map.py:126-166, normals :206-219): out_nrm [n*3] the unit
+ * eigenvector of the covariance's smallest eigenvalue, out_planarity [n] (l_mid - l_min) / max(l_max, 1e-12);
+ * both zero for a point with fewer than 4 neighbours (itself included) or one the table could not place. The
+ * neighbour offsets and their products are summed in int64 fixed point (2^20 and 2^40 units of the radius' power
+ * of two), the covariance and its eigen-decomposition are float64: the answers do not depend on thread order.
+ * Exact up to 2^23 neighbours per point. */
+int lw_normals(const float* xyz, int32_t xyz_stride, int64_t n, float radius, lw_pca_buf* pb, float* out_nrm,
+               float* out_planarity, void* stream);
+
 /* LVXR recordings (host). lw_lvxr_decode decodes a whole recording held in memory into every firing with its
  * exact time, the empty ones included (lvxr.py read_firings :189-260, the datagrams of record.rs / point.rs):
  * n firings of up to R returns each, time-ordered. lw_lvxr_info reports n, R, the device type, the profile and the

@@ -70,11 +70,12 @@ __host__ __device__ __forceinline__ int slot_hash(int64_t k) {
     return (int)(h & 0x7FFFFFFFLL);
 }
 
-// Slot holding `key`, or -1 (gpu.py:254-265).
+// Slot holding `key`, or -1 (gpu.py:254-265). P probes (the prior-map table takes 128, prior_map.py:36).
+template <int P = PROBES>
 __device__ __forceinline__ int find_slot(int64_t key, const int64_t* __restrict__ keys, int mask) {
     int h = slot_hash(key) & mask;
 #pragma unroll 1
-    for (int p = 0; p < PROBES; ++p) {
+    for (int p = 0; p < P; ++p) {
         int s = (h + p) & mask;
         int64_t k = __ldg(keys + s);
         if (k == key) return s;
@@ -84,12 +85,13 @@ __device__ __forceinline__ int find_slot(int64_t key, const int64_t* __restrict_
 }
 
 // Find the slot of `key` or claim an empty one. Returns the slot and sets *claimed when this call turned an
-// empty slot into `key`; -1 when the probe window is full (gpu.py:396-412).
+// empty slot into `key`; -1 when the probe window of P slots is full (gpu.py:396-412).
+template <int P = PROBES>
 __device__ __forceinline__ int claim_slot(int64_t key, int64_t* keys, int mask, bool* claimed) {
     int h = slot_hash(key) & mask;
     *claimed = false;
 #pragma unroll 1
-    for (int p = 0; p < PROBES; ++p) {
+    for (int p = 0; p < P; ++p) {
         int s = (h + p) & mask;
         int64_t k = *(volatile int64_t*)(keys + s);
         if (k == key) return s;
@@ -165,6 +167,34 @@ __device__ __forceinline__ int block_rank(int flag, int* smem32, int* tot) {
     __syncthreads();
     int r = smem32[warp] + before;
     *tot = smem32[32];
+    __syncthreads();
+    return r;
+}
+
+// Exclusive scan of per-thread counts over the CTA (blockDim.x <= 1024); the CTA total in *tot.
+__device__ __forceinline__ int block_excl(int v, int* sm, int* tot) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    int inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    if (lane == 31) sm[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        int x = lane < nw ? sm[lane] : 0, xi = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int u = __shfl_up_sync(0xffffffffu, xi, o);
+            if (lane >= o) xi += u;
+        }
+        if (lane < nw) sm[lane] = xi - x;
+        if (lane == 31) sm[32] = xi;
+    }
+    __syncthreads();
+    int r = sm[w] + inc - v;
+    *tot = sm[32];
     __syncthreads();
     return r;
 }

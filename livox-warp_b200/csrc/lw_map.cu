@@ -516,34 +516,6 @@ __device__ __forceinline__ void load_keys(const lw_map& map, int64_t s0, int64_t
     }
 }
 
-// Exclusive scan of per-thread counts over the CTA (blockDim.x <= 1024); the CTA total in *tot.
-__device__ __forceinline__ int block_excl(int v, int* sm, int* tot) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-    int inc = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int u = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += u;
-    }
-    if (lane == 31) sm[w] = inc;
-    __syncthreads();
-    if (w == 0) {
-        int x = lane < nw ? sm[lane] : 0, xi = x;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int u = __shfl_up_sync(0xffffffffu, xi, o);
-            if (lane >= o) xi += u;
-        }
-        if (lane < nw) sm[lane] = xi - x;
-        if (lane == 31) sm[32] = xi;
-    }
-    __syncthreads();
-    int r = sm[w] + inc - v;
-    *tot = sm[32];
-    __syncthreads();
-    return r;
-}
-
 __global__ void __launch_bounds__(CL_THREADS) k_classify_count(lw_map map, lw_view v, int min_count,
                                                                int* __restrict__ tiles) {
     __shared__ int sm[33];

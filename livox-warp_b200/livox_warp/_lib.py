@@ -17,6 +17,7 @@ LIB_PATH = Path(__file__).resolve().parent / "liblivoxb200.so"
 
 LW_OK, LW_EINVAL, LW_ECAPACITY, LW_ETIMEOUT, LW_ECUDA = 0, -1, -2, -3, -4
 FIX_R, FIX_RR, FIX_W = 2.0 ** 32, 2.0 ** 40, 2.0 ** 20
+VOX_FIX_ATTR = 2.0 ** 16
 REG_CAP = MAP_CAP = 4096
 ACC_STRIDE = 64
 REC_FLOATS = 20
@@ -90,6 +91,16 @@ class ClusterBuf(C.Structure):
 
 class NbrBuf(C.Structure):
     PTRS = ("keys", "acc", "vidx", "v_slot", "slot_of_pt", "v_xyz", "v_w", "v_cnt", "v_nrm", "v_curv", "tiles", "m")
+    _fields_ = [(n, P) for n in PTRS] + [("cap", i64), ("pt_cap", i64)]
+
+
+class VoxBuf(C.Structure):
+    PTRS = ("keys", "acc", "first", "order", "slot_of_pt", "tiles", "stats")
+    _fields_ = [(n, P) for n in PTRS] + [("cap", i64), ("pt_cap", i64)]
+
+
+class PcaBuf(C.Structure):
+    PTRS = ("keys", "cell_cnt", "cell_start", "slot_of_pt", "rank_of_pt", "sorted", "tiles", "stats")
     _fields_ = [(n, P) for n in PTRS] + [("cap", i64), ("pt_cap", i64)]
 
 
@@ -177,6 +188,11 @@ _SIGS = {
     "lw_ground": (i32, [P, i32, P, P, i64, f32, f32, i32, f32, f32, i32, f32, P, P, P, P, P]),
     "lw_cluster": (i32, [P, i32, P, i32, P, i64, f32, f32, f32, i32, C.POINTER(ClusterBuf), P, P]),
     "lw_neighborhoods": (i32, [P, i32, P, i64, f32, i32, P, C.POINTER(NbrBuf), P, P, P, P]),
+    "lw_vox_offset_units": (f64, [f32]),
+    "lw_vox_clear": (i32, [C.POINTER(VoxBuf), P]),
+    "lw_vox_insert": (i32, [C.POINTER(VoxBuf), P, i32, P, P, i64, i64, f32, P]),
+    "lw_vox_emit": (i32, [C.POINTER(VoxBuf), f32, i64, P, P, P, P, P]),
+    "lw_normals": (i32, [P, i32, i64, f32, C.POINTER(PcaBuf), P, P, P]),
     "lw_lvxr_decode": (i32, [P, i64, C.POINTER(P)]),
     "lw_lvxr_info": (i32, [P, C.POINTER(i64), C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), C.POINTER(f64)]),
     "lw_lvxr_copy": (i32, [P, P, P, P, P, P, P]),

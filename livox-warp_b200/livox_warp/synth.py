@@ -435,6 +435,30 @@ def spin_scan(scene: Scene, T: np.ndarray, n: int, seed: int, noise: float = 0.0
     return (d * rr[:, None])[ok].astype(np.float32)
 
 
+def tls_scan(scene: Scene, stations, seed: int, step_deg: float = 0.2, elevation_deg=(-60.0, 89.0),
+             noise: float = 0.002, t: float = 0.0) -> np.ndarray:
+    """A terrestrial scanner's capture of the scene (the reference's sources.tls_scan, sources.py:884-899): a
+    spherical grid of rays step_deg apart over the elevation range from each station, Gaussian range noise; the
+    world points (n, 3) float32 of the rays that hit a surface."""
+    rng = np.random.default_rng(seed)
+    st = np.asarray(stations, dtype=np.float64).reshape(-1, 3)
+    n_az = int(round(360.0 / step_deg))
+    n_el = int((elevation_deg[1] - elevation_deg[0]) / step_deg) + 1
+    az = np.radians(np.arange(n_az) * step_deg)
+    el = np.radians(elevation_deg[0] + np.arange(n_el) * step_deg)
+    A, E = np.meshgrid(az, el, indexing="ij")
+    d = np.stack([np.cos(E) * np.cos(A), np.cos(E) * np.sin(A), np.sin(E)], axis=-1).reshape(-1, 3)
+    out = []
+    for o in st:
+        oo = np.broadcast_to(o, d.shape)
+        r = raycast(np.ascontiguousarray(oo), d, scene, np.full(len(d), t), chunk=1 << 15)
+        ok = np.isfinite(r)
+        rr = r[ok] + rng.normal(0.0, noise, int(ok.sum()))
+        out.append(o + d[ok] * rr[:, None])
+    pts = np.concatenate(out) if out else np.zeros((0, 3))
+    return pts[np.abs(pts).max(axis=1) < 1.0e3].astype(np.float32)
+
+
 def free_poses(scene: Scene, n: int, seed: int, z: float = 1.2, margin: float = 0.6, grid: float = 0.0):
     """n sensor poses in free space at height z with yaw uniform in [0, 2 pi): (T (n, 4, 4) sensor to world).
     With grid > 0 the positions lie on that xy grid (distinct cells, drawn without replacement)."""

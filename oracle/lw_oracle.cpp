@@ -9,6 +9,7 @@
 //   carving + local_plane      gpu.py:415-593          map classification  gpu.py:286-299, 596-634, 699-747
 //   ground grid                perception.py:29-111    clusters            perception.py:114-271
 //   prior grid + nearest_point mapgrid.py:35-194       batched ICP + eval  localize.py:126-205, 517-565
+//   prior-map voxel means      prior_map.py:57-123     PCA normals         prior_map.py:126-166
 // The reference's nondeterministic choices are fixed the way the GPU build fixes them: the lowest point index
 // claims a thinning voxel, per-voxel sums are exact int64 fixed point (the units of include/livox_b200.h),
 // and 4096-point caps keep the first points in index order. Float expressions are written in the evaluation
@@ -1316,6 +1317,136 @@ void or_loc_eval(const or_grid* gp, const float* pts4, const int32_t* scan_lo, c
             for (int k = 0; k < 3; ++k) c[k] += d < radii[k];
         }
         for (int k = 0; k < 3; ++k) counts[3 * h + k] = c[k];
+    }
+}
+
+}  // extern "C"
+
+// ---- prior maps: voxel downsample and PCA normals (prior_map.py:57-219) --------------------------------------------
+// The library's definition. Voxel means: offsets from the voxel centre ((i + 0.5) * voxel, float32) summed in int64
+// fixed point (2^(30 - e) units per metre, voxel < 2^e), colour and intensity in 2^16 units, the voxels numbered in
+// the order of their first point; the mean is centre + sum / (count * units) in float64, rounded once. The reference
+// sums float32 offsets with float atomics and emits in hash-slot order. Normals: every point within the radius
+// (|q - p|^2 <= r^2 in float32), its offset and the offset's products summed in fixed point (2^20 and 2^40 units
+// of the radius' power of two), covariance and Jacobi in float64; the reference sums float32 in query order and
+// decomposes with a float32 eig3.
+
+extern "C" {
+
+int64_t or_voxel_downsample(const float* xyz, int64_t n, const float* inten, const float* rgb, float voxel,
+                            float* out_xyz, float* out_rgb, float* out_inten, int32_t* out_cnt) {
+    const float inv_v = (float)(1.0 / (double)voxel);
+    int e = 0;
+    frexpf(voxel, &e);
+    const float fo = (float)ldexp(1.0, 30 - e), fa = 65536.0f;
+    std::unordered_map<int64_t, int64_t> vox;
+    std::vector<int64_t> keys, acc;
+    for (int64_t i = 0; i < n; ++i) {
+        const float x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+        const int ix = ifloor(x * inv_v), iy = ifloor(y * inv_v), iz = ifloor(z * inv_v);
+        const int64_t key = key_ijk(ix, iy, iz);
+        auto it = vox.find(key);
+        int64_t v;
+        if (it == vox.end()) {
+            v = (int64_t)keys.size();
+            vox.emplace(key, v);
+            keys.push_back(key);
+            acc.insert(acc.end(), 8, 0);
+        } else {
+            v = it->second;
+        }
+        int64_t* a = acc.data() + 8 * v;
+        a[0] += llrintf((x - ((float)ix + 0.5f) * voxel) * fo);
+        a[1] += llrintf((y - ((float)iy + 0.5f) * voxel) * fo);
+        a[2] += llrintf((z - ((float)iz + 0.5f) * voxel) * fo);
+        if (rgb)
+            for (int c = 0; c < 3; ++c) a[3 + c] += llrintf(rgb[3 * i + c] * fa);
+        if (inten) a[6] += llrintf(inten[i] * fa);
+        a[7] += 1;
+    }
+    const int64_t m = (int64_t)keys.size();
+    for (int64_t j = 0; j < m; ++j) {
+        const int64_t key = keys[j];
+        const int ix = (int)(key & KMASK) - (int)BIAS, iy = (int)((key >> 21) & KMASK) - (int)BIAS,
+                  iz = (int)((key >> 42) & KMASK) - (int)BIAS;
+        const int64_t* a = acc.data() + 8 * j;
+        const double c = (double)a[7], uo = c * (double)fo, ua = c * 65536.0;
+        out_xyz[3 * j + 0] = (float)((double)(((float)ix + 0.5f) * voxel) + (double)a[0] / uo);
+        out_xyz[3 * j + 1] = (float)((double)(((float)iy + 0.5f) * voxel) + (double)a[1] / uo);
+        out_xyz[3 * j + 2] = (float)((double)(((float)iz + 0.5f) * voxel) + (double)a[2] / uo);
+        for (int k = 0; k < 3; ++k) out_rgb[3 * j + k] = (float)((double)a[3 + k] / ua);
+        out_inten[j] = (float)((double)a[6] / ua);
+        out_cnt[j] = (int32_t)std::min<int64_t>(a[7], 0x7FFFFFFF);
+    }
+    return m;
+}
+
+void or_normals(const float* xyz, int64_t n, float radius, float* out_nrm, float* out_pl, int threads) {
+    const float inv_h = (float)(1.0 / ((double)radius * 1.00390625)), r2 = radius * radius;
+    int e = 0;
+    frexpf(radius, &e);
+    const double fd64 = ldexp(1.0, 20 - e), fdd64 = ldexp(1.0, 40 - 2 * e);
+    const float fd = (float)fd64, fdd = (float)fdd64;
+    std::unordered_map<int64_t, std::vector<int64_t>> cells;
+    for (int64_t i = 0; i < n; ++i) {
+        const float x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+        const int64_t key = key_ijk(ifloor(x * inv_h), ifloor(y * inv_h), ifloor(z * inv_h));
+        cells[key].push_back(i);
+    }
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 256)
+    for (int64_t i = 0; i < n; ++i) {
+        const float px = xyz[3 * i], py = xyz[3 * i + 1], pz = xyz[3 * i + 2];
+        const int ix = ifloor(px * inv_h), iy = ifloor(py * inv_h), iz = ifloor(pz * inv_h);
+        long long cnt = 0, s1[3] = {0, 0, 0}, s2[6] = {0, 0, 0, 0, 0, 0};
+        for (int dx = -1; dx <= 1; ++dx)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dz = -1; dz <= 1; ++dz) {
+                    auto it = cells.find(key_ijk(ix + dx, iy + dy, iz + dz));
+                    if (it == cells.end()) continue;
+                    for (int64_t k : it->second) {
+                        const float ex = xyz[3 * k] - px, ey = xyz[3 * k + 1] - py, ez = xyz[3 * k + 2] - pz;
+                        if (ex * ex + ey * ey + ez * ez > r2) continue;
+                        ++cnt;
+                        s1[0] += llrintf(ex * fd);
+                        s1[1] += llrintf(ey * fd);
+                        s1[2] += llrintf(ez * fd);
+                        s2[0] += llrintf(ex * ex * fdd);
+                        s2[1] += llrintf(ex * ey * fdd);
+                        s2[2] += llrintf(ex * ez * fdd);
+                        s2[3] += llrintf(ey * ey * fdd);
+                        s2[4] += llrintf(ey * ez * fdd);
+                        s2[5] += llrintf(ez * ez * fdd);
+                    }
+                }
+        if (cnt < 4) {
+            out_nrm[3 * i] = out_nrm[3 * i + 1] = out_nrm[3 * i + 2] = 0.0f;
+            out_pl[i] = 0.0f;
+            continue;
+        }
+        const double inv = 1.0 / (double)cnt;
+        const double mu[3] = {(double)s1[0] / fd64 * inv, (double)s1[1] / fd64 * inv, (double)s1[2] / fd64 * inv};
+        const int up[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+        double C[9], ev[3], Q[9];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) C[r * 3 + c] = (double)s2[up[r * 3 + c]] / fdd64 * inv - mu[r] * mu[c];
+        jacobi<3>(C, ev, Q);
+        int lo = 0, hi = 0;  // prior_map.py:157-164
+        for (int a = 1; a < 3; ++a) {
+            if (ev[a] < ev[lo]) lo = a;
+            if (ev[a] > ev[hi]) hi = a;
+        }
+        const int mid = lo == hi ? lo : 3 - lo - hi;
+        double nx = Q[lo], ny = Q[3 + lo], nz = Q[6 + lo];
+        const double nl = std::sqrt(nx * nx + ny * ny + nz * nz);
+        if (nl > 0.0) {
+            nx /= nl;
+            ny /= nl;
+            nz /= nl;
+        }
+        out_nrm[3 * i] = (float)nx;
+        out_nrm[3 * i + 1] = (float)ny;
+        out_nrm[3 * i + 2] = (float)nz;
+        out_pl[i] = (float)((ev[mid] - ev[lo]) / std::max(ev[hi], 1.0e-12));
     }
 }
 

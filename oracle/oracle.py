@@ -91,6 +91,8 @@ def lib() -> C.CDLL:
             "or_neighborhoods": (None, [P, i32, i64, f32, i32, P, P, P, P, i32]),
             "or_score_grid": (None, [C.POINTER(OrGrid), P, P, i32, P, i64, i32, f32, f32, f32, f32, i32, P, i32]),
             "or_score_list": (None, [C.POINTER(OrGrid), P, P, i32, P, i64, f32, i32, P, i32]),
+            "or_voxel_downsample": (i64, [P, i64, P, P, f32, P, P, P, P]),
+            "or_normals": (None, [P, i64, f32, P, P, i32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(_lib, name)
@@ -269,6 +271,33 @@ def neighborhoods(xyz, radius: float, want_normals: bool, sensor=(0.0, 0.0, 0.0)
     lib().or_neighborhoods(_p(xyz), 3, n, float(radius), int(bool(want_normals)), _p(sen), _p(cnt), _p(nrm),
                            _p(curv), threads())
     return cnt, nrm, curv
+
+
+def voxel_downsample(xyz, intensity=None, rgb=None, voxel: float = 0.02):
+    """prior_map.py:57-123, 169-203 as the library defines it (exact fixed-point sums, voxels in the order of their
+    first point): (xyz [m, 3], rgb [m, 3], intensity [m], count int32 [m])."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+    n = len(xyz)
+    it = None if intensity is None else np.ascontiguousarray(intensity, dtype=np.float32).reshape(n)
+    col = None if rgb is None else np.ascontiguousarray(rgb, dtype=np.float32).reshape(n, 3)
+    ox = np.zeros((n, 3), np.float32)
+    oc = np.zeros((n, 3), np.float32)
+    oi = np.zeros(n, np.float32)
+    on = np.zeros(n, np.int32)
+    m = lib().or_voxel_downsample(_p(xyz), n, None if it is None else _p(it), None if col is None else _p(col),
+                                  float(voxel), _p(ox), _p(oc), _p(oi), _p(on))
+    return ox[:m], oc[:m], oi[:m], on[:m]
+
+
+def normals(xyz, radius: float):
+    """prior_map.py:126-166 as the library defines it (every point within the radius, fixed-point sums, float64
+    Jacobi): (normal [n, 3], planarity [n])."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+    n = len(xyz)
+    nrm = np.zeros((n, 3), np.float32)
+    pl = np.zeros(n, np.float32)
+    lib().or_normals(_p(xyz), n, float(radius), _p(nrm), _p(pl), threads())
+    return nrm, pl
 
 
 def cluster(xyz, gnd=None, voxel=0.1, connect=0.35, min_pts=30, max_out=4096):

@@ -51,6 +51,7 @@ def test_struct_layouts_match_header(tmp_path):
                "lw_odom_state": _lib.OdomState, "lw_traj_rec": _lib.TrajRec, "lw_frame_buf": _lib.FrameBuf,
                "lw_gn_scratch": _lib.GnScratch, "lw_pose_table": _lib.PoseTable, "lw_map": _lib.Map,
                "lw_view": _lib.View, "lw_cluster_buf": _lib.ClusterBuf, "lw_nbr_buf": _lib.NbrBuf, "lw_prior_grid": _lib.PriorGrid,
+               "lw_vox_buf": _lib.VoxBuf, "lw_pca_buf": _lib.PcaBuf,
                "lw_loc_batch": _lib.LocBatch, "lw_initnet": _lib.InitNet, "lw_net_scratch": _lib.NetScratch,
                "lw_net_work": _lib.NetWork}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
