@@ -284,6 +284,18 @@ int lw_carve(const float* xyz, int32_t xyz_stride, const uint32_t* attr, const i
 int lw_map_build(const lw_map* map, const lw_view* v, int32_t min_count, float* out_xyz, uint32_t* out_attr,
                  float* out_t, int32_t* out_dyn, int32_t* tiles, int32_t* count_dev, void* stream);
 
+/* The live ring's visible set (k_classify_live, gpu.py:637-697, with the scan + scatter of Pipeline.build
+ * :1466-1504 in live mode), in ring order: every one of the first min(filled, cap) ring slots that is no older
+ * than v->persist (when > 0), passes keep_raw, and -- when v->inv_frame_dt > 0 -- whose frame's pose slot holds
+ * that frame for v->epoch, deskewed by the frame's twist from its time within the frame; posed by its frame's
+ * matrix and inside the crop box. out_* [cap] get the world point, the attribute, the time and, with v->dyn_on,
+ * the Motion label from the map's history (settled_near, gpu.py:596-634), else 0. ring_xyz is [cap*3]; tiles is
+ * [cap/1024 + 2] scratch; writes count_dev[0]. */
+int lw_live_build(const float* ring_xyz, const uint32_t* ring_attr, const float* ring_t, const int32_t* ring_frame,
+                  int64_t cap, int64_t filled, const lw_pose_table* pt, const lw_view* v, const lw_map* map,
+                  float* out_xyz, uint32_t* out_attr, float* out_t, int32_t* out_dyn, int32_t* tiles,
+                  int32_t* count_dev, void* stream);
+
 /* Frame id of each staged point, floor(max(t, 0) * inv_dt), all 0 when inv_dt <= 0 (gpu.py:340-348). */
 int lw_frame_ids(const float* t, int64_t n, float inv_dt, int32_t* out, void* stream);
 

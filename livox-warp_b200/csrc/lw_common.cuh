@@ -125,6 +125,33 @@ __device__ __forceinline__ void xform(const float* __restrict__ T, float x, floa
     oz = T[8] * x + T[9] * y + T[10] * z + T[11];
 }
 
+// deskew (gpu.py:268-283): a point measured a fraction s of a frame after mid-frame, moved to the mid-frame sensor
+// frame by the frame's body motion tw = (rho, theta): rotation by the rotation vector theta * s, then + rho * s.
+// The rotation is evaluated in float64 and rounded once, so the CPU oracle reproduces it exactly.
+__device__ __forceinline__ void deskew_frac(float x, float y, float z, float s, const float* tw, float& ox, float& oy,
+                                            float& oz) {
+    float rx = tw[3] * s, ry = tw[4] * s, rz = tw[5] * s;
+    float a = len3(rx, ry, rz);
+    ox = x;
+    oy = y;
+    oz = z;
+    if (!(a < 1.0e-9f)) {
+        double ad = (double)a;
+        double ux = (double)rx / ad, uy = (double)ry / ad, uz = (double)rz / ad;
+        double sh = sin(0.5 * ad), w = cos(0.5 * ad);
+        double vx = ux * sh, vy = uy * sh, vz = uz * sh;
+        double px = x, py = y, pz = z;
+        // p' = p + w t + v x t with t = 2 (v x p)
+        double tx = 2.0 * (vy * pz - vz * py), ty = 2.0 * (vz * px - vx * pz), tz = 2.0 * (vx * py - vy * px);
+        ox = (float)(px + w * tx + (vy * tz - vz * ty));
+        oy = (float)(py + w * ty + (vz * tx - vx * tz));
+        oz = (float)(pz + w * tz + (vx * ty - vy * tx));
+    }
+    ox = ox + tw[0] * s;
+    oy = oy + tw[1] * s;
+    oz = oz + tw[2] * s;
+}
+
 __device__ __forceinline__ float atomic_min_float(float* a, float v) {
     return v >= 0.0f ? __int_as_float(atomicMin((int*)a, __float_as_int(v)))
                      : __uint_as_float(atomicMax((unsigned int*)a, __float_as_uint(v)));

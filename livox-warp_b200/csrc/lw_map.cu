@@ -616,6 +616,75 @@ __global__ void __launch_bounds__(CL_THREADS) k_classify_scatter(lw_map map, lw_
     }
 }
 
+// =====================================================================================================
+// Visible set of the live ring (k_classify_live, gpu.py:637-697) compacted in ring order: a CTA of LV_TILE
+// threads per tile of ring slots counts its drawn points, one CTA scans the counts, and the scatter pass
+// classifies again and writes each drawn point at its tile's offset plus its rank in the tile.
+// =====================================================================================================
+
+constexpr int LV_TILE = 1024;
+
+struct LiveRing {
+    const float* xyz;      // [cap*3] sensor-frame points as measured
+    const uint32_t* attr;  // [cap]
+    const float* t;        // [cap]
+    const int32_t* frame;  // [cap] frame ids
+    int64_t cap, filled;
+};
+
+// Ring slot i posed into the world; false when it is not drawn (gpu.py:664-690).
+__device__ __forceinline__ bool live_point(const LiveRing& r, const lw_pose_table& pt, const lw_view& v, int64_t i,
+                                           float& wx, float& wy, float& wz) {
+    if (i >= r.filled || i >= r.cap) return false;
+    const float t = r.t[i];
+    if (v.persist > 0.0f && v.now - t > v.persist) return false;
+    float x = r.xyz[3 * i], y = r.xyz[3 * i + 1], z = r.xyz[3 * i + 2];
+    if (!keep_raw(x, y, z, r.attr[i], v)) return false;
+    const int fid = r.frame[i];
+    const int f = fid & (LW_POSE_SLOTS - 1);
+    if (v.inv_frame_dt > 0.0f) {
+        // odometry on: drawn only once the slot holds this frame's pose for the current epoch
+        if (pt.owner_frame[f] != fid || pt.owner_epoch[f] != v.epoch) return false;
+        const float xf = t * v.inv_frame_dt;
+        const float frac = xf - floorf(xf) - 0.5f;  // the point's time from mid-frame, in frames: [-0.5, 0.5)
+        deskew_frac(x, y, z, frac, pt.tw + 6 * (int64_t)f, x, y, z);
+    }
+    xform(pt.poses + 16 * (int64_t)f, x, y, z, wx, wy, wz);
+    return in_crop(wx, wy, wz, v) != 0;
+}
+
+__global__ void __launch_bounds__(LV_TILE) k_live_count(LiveRing r, lw_pose_table pt, lw_view v,
+                                                        int* __restrict__ tiles) {
+    const int64_t i = (int64_t)blockIdx.x * LV_TILE + threadIdx.x;
+    float wx, wy, wz;
+    const int c = __syncthreads_count(live_point(r, pt, v, i, wx, wy, wz) ? 1 : 0);
+    if (threadIdx.x == 0) tiles[blockIdx.x] = c;
+}
+
+__global__ void __launch_bounds__(LV_TILE) k_live_scatter(LiveRing r, lw_pose_table pt, lw_view v, lw_map map,
+                                                          const int* __restrict__ tiles, float* __restrict__ out_xyz,
+                                                          uint32_t* __restrict__ out_attr, float* __restrict__ out_t,
+                                                          int* __restrict__ out_dyn) {
+    __shared__ int sm[33];
+    const int64_t i = (int64_t)blockIdx.x * LV_TILE + threadIdx.x;
+    float wx = 0.0f, wy = 0.0f, wz = 0.0f;
+    const int f = live_point(r, pt, v, i, wx, wy, wz) ? 1 : 0;
+    int tot;
+    const int rank = block_rank(f, sm, &tot);
+    if (!f) return;
+    const int64_t j = (int64_t)tiles[blockIdx.x] + rank;
+    out_xyz[3 * j + 0] = wx;
+    out_xyz[3 * j + 1] = wy;
+    out_xyz[3 * j + 2] = wz;
+    out_attr[j] = r.attr[i];
+    out_t[j] = r.t[i];
+    // static when the map voxel it lands in, or one of its 6 neighbours, is old and no ghost (gpu.py:691-697)
+    out_dyn[j] = v.dyn_on != 0
+                     ? 1 - settled_near(ifloor(wx * v.inv_voxel), ifloor(wy * v.inv_voxel), ifloor(wz * v.inv_voxel), v,
+                                        map)
+                     : 0;
+}
+
 // Frame id of each staged point: floor(max(t, 0) * inv_dt), 0 when inv_dt <= 0 (gpu.py:340-348).
 __global__ void k_frame_of(const float* __restrict__ t, int64_t n, float inv_dt, int32_t* __restrict__ out) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -719,6 +788,35 @@ int lw_map_build(const lw_map* map, const lw_view* v, int32_t min_count, float* 
     k_scan_tiles<<<1, 1024, 0, s>>>(tiles, nt, count_dev);
     k_classify_scatter<<<nt, CL_THREADS, 0, s>>>(*map, *v, min_count, tiles, out_xyz, out_attr, out_t, out_dyn);
     LW_LAUNCHED("lw_map_build");
+    count_launches(3);
+    return LW_OK;
+}
+
+int lw_live_build(const float* ring_xyz, const uint32_t* ring_attr, const float* ring_t, const int32_t* ring_frame,
+                  int64_t cap, int64_t filled, const lw_pose_table* pt, const lw_view* v, const lw_map* map,
+                  float* out_xyz, uint32_t* out_attr, float* out_t, int32_t* out_dyn, int32_t* tiles,
+                  int32_t* count_dev, void* stream) {
+    int r = check_map(map, "lw_live_build");
+    if (r != LW_OK) return r;
+    if (!pt || !pt->poses || !pt->tw || !pt->owner_frame || !pt->owner_epoch || !v || !tiles || !count_dev ||
+        cap < 0 || cap > (1LL << 31) - 1)
+        return set_error(LW_EINVAL, "lw_live_build: bad arguments");
+    if (cap > 0 && (!ring_xyz || !ring_attr || !ring_t || !ring_frame || !out_xyz || !out_attr || !out_t || !out_dyn))
+        return set_error(LW_EINVAL, "lw_live_build: missing ring or output buffers");
+    if (v->dyn_on != 0 && (v->map_mask < 0 || (int64_t)v->map_mask > map->cap - 1))
+        return set_error(LW_EINVAL, "lw_live_build: view map_mask %d does not fit the map's %lld slots", v->map_mask,
+                         (long long)map->cap);
+    cudaStream_t s = (cudaStream_t)stream;
+    LW_CUDA(cudaMemsetAsync(count_dev, 0, sizeof(int32_t), s));
+    if (cap == 0 || filled <= 0) return LW_OK;
+    LiveRing ring{ring_xyz, ring_attr, ring_t, ring_frame, cap, filled < cap ? filled : cap};
+    // only the tiles that hold filled slots: the rest draw nothing
+    const int nt = blocks_for(ring.filled, LV_TILE);
+    ProfScope prof("live_build", s);
+    k_live_count<<<nt, LV_TILE, 0, s>>>(ring, *pt, *v, tiles);
+    k_scan_tiles<<<1, 1024, 0, s>>>(tiles, nt, count_dev);
+    k_live_scatter<<<nt, LV_TILE, 0, s>>>(ring, *pt, *v, *map, tiles, out_xyz, out_attr, out_t, out_dyn);
+    LW_LAUNCHED("lw_live_build");
     count_launches(3);
     return LW_OK;
 }

@@ -89,28 +89,14 @@ __global__ void k_append_total(const int* __restrict__ tiles, int nt, int* count
 }
 
 // =====================================================================================================
-// Deskew (odom.py:163-178 with gpu.py:268-283). The rotation by the rotation vector theta*s is evaluated in
-// float64 and rounded once, so the CPU oracle reproduces it exactly.
+// Deskew (odom.py:163-178 with gpu.py:268-283): s = clamp((t - t_mid) / frame_dt, -1, 1), then deskew_frac.
 // =====================================================================================================
 
 __device__ __forceinline__ float4 deskew_point(float4 p, float t_mid, float inv_dt, const float* tw) {
     float s = fminf(fmaxf((p.w - t_mid) * inv_dt, -1.0f), 1.0f);
-    float rx = tw[3] * s, ry = tw[4] * s, rz = tw[5] * s;
-    float a = len3(rx, ry, rz);
-    float ox = p.x, oy = p.y, oz = p.z;
-    if (!(a < 1.0e-9f)) {
-        double ad = (double)a;
-        double ux = (double)rx / ad, uy = (double)ry / ad, uz = (double)rz / ad;
-        double sh = sin(0.5 * ad), w = cos(0.5 * ad);
-        double vx = ux * sh, vy = uy * sh, vz = uz * sh;
-        double px = p.x, py = p.y, pz = p.z;
-        // p' = p + w t + v x t with t = 2 (v x p)
-        double tx = 2.0 * (vy * pz - vz * py), ty = 2.0 * (vz * px - vx * pz), tz = 2.0 * (vx * py - vy * px);
-        ox = (float)(px + w * tx + (vy * tz - vz * ty));
-        oy = (float)(py + w * ty + (vz * tx - vx * tz));
-        oz = (float)(pz + w * tz + (vx * ty - vy * tx));
-    }
-    return make_float4(ox + tw[0] * s, oy + tw[1] * s, oz + tw[2] * s, p.w);
+    float ox, oy, oz;
+    deskew_frac(p.x, p.y, p.z, s, tw, ox, oy, oz);
+    return make_float4(ox, oy, oz, p.w);
 }
 
 // =====================================================================================================

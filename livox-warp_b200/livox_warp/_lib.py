@@ -184,6 +184,8 @@ _SIGS = {
     "lw_carve": (i32, [P, i32, P, P, P, i64, P, i32, f32, f32, i32, C.POINTER(Map), P, P]),
     "lw_map_build": (i32, [C.POINTER(Map), C.POINTER(View), i32, P, P, P, P, P, P, P]),
     "lw_map_clear": (i32, [C.POINTER(Map), P]),
+    "lw_live_build": (i32, [P, P, P, P, i64, i64, C.POINTER(PoseTable), C.POINTER(View), C.POINTER(Map), P, P, P, P,
+                            P, P, P]),
     "lw_frame_ids": (i32, [P, i64, f32, P, P]),
     "lw_ground": (i32, [P, i32, P, P, i64, f32, f32, i32, f32, f32, i32, f32, P, P, P, P, P]),
     "lw_cluster": (i32, [P, i32, P, i32, P, i64, f32, f32, f32, i32, C.POINTER(ClusterBuf), P, P]),

@@ -10,8 +10,8 @@ Differences from the reference, all deliberate:
   - map_acc holds exact int64 fixed-point sums (units FIX_W per metre, reflectivity in units of 1) instead of
     float32 sums of undefined order: every run gives the same map, bit for bit (map_centroids() decodes it);
   - the first 4096 hits of a voxel in point order are summed (the reference sums whichever 4096 arrive first);
-  - build() supports the map mode (k_classify_map); the live-ring mode and the render-side neighbourhood /
-    shading passes are outside this library's scope.
+  - build() compacts either the map's voxels (k_classify_map, slot order) or the live ring's points
+    (k_classify_live, ring order); the render-side shading passes are outside this library's scope.
 """
 
 from __future__ import annotations
@@ -111,7 +111,7 @@ class Pipeline:
         self.nb_cap = int(nb_capacity)
         self.work_cap = max(self.cap, self.map_cap)
 
-        # live ring (render-side; kept so scripts written for the reference run unchanged)
+        # live ring: the points of the last ring_capacity returns, drawn by build(map_on=False)
         self.ring_xyz = torch.zeros((self.cap, 3), dtype=torch.float32, device=d)
         self.ring_attr = torch.zeros(self.cap, dtype=torch.int32, device=d)
         self.ring_t = torch.zeros(self.cap, dtype=torch.float32, device=d)
@@ -166,7 +166,7 @@ class Pipeline:
         self.cl_vel = torch.zeros((MAX_CLUSTERS, 3), dtype=torch.float32, device=d)
         self.cl_tid = torch.full((MAX_CLUSTERS,), -1, dtype=torch.int32, device=d)
         self._slot = torch.zeros(n, dtype=torch.int32, device=d)  # per-point scratch of the insert passes
-        self._tiles = torch.zeros(m // 1024 + 2, dtype=torch.int32, device=d)
+        self._tiles = torch.zeros(max(m, self.cap) // 1024 + 2, dtype=torch.int32, device=d)
         self.total = torch.zeros(1, dtype=torch.int32, device=d)
 
         self._stage_cap = 0
@@ -334,18 +334,24 @@ class Pipeline:
 
     def build(self, view: View, map_on: bool = True, min_count: int = 1, neighbors: str = "", radius: float = 0.1,
               sensor=(0.0, 0.0, 0.0)) -> int:
-        """Classify + compact the map's visible set into c_* in slot order (gpu.py:1466-1512, map mode)."""
-        if not map_on:
-            raise NotImplementedError("the live-ring visible set is render-side and outside this library's scope")
+        """Classify + compact the visible set into c_* (gpu.py:1466-1512): with map_on the map's voxels in slot
+        order (k_classify_map), else the live ring's points in ring order (k_classify_live)."""
         if neighbors not in ("", "count", "normals"):
             raise ValueError(f"neighbors must be '', 'count' or 'normals', got {neighbors!r}")
         self.flush_poses()
-        _lib.call("lw_map_build", C_ref(self.map_struct), C_ref(view), int(min_count), _lib.ptr(self.c_xyz),
-                  _lib.ptr(self.c_attr), _lib.ptr(self.c_t), _lib.ptr(self.c_dyn), _lib.ptr(self._tiles),
-                  _lib.ptr(self.total), _lib.stream_ptr())
+        if map_on:
+            _lib.call("lw_map_build", C_ref(self.map_struct), C_ref(view), int(min_count), _lib.ptr(self.c_xyz),
+                      _lib.ptr(self.c_attr), _lib.ptr(self.c_t), _lib.ptr(self.c_dyn), _lib.ptr(self._tiles),
+                      _lib.ptr(self.total), _lib.stream_ptr())
+        else:
+            _lib.call("lw_live_build", _lib.ptr(self.ring_xyz), _lib.ptr(self.ring_attr), _lib.ptr(self.ring_t),
+                      _lib.ptr(self.ring_frame), self.cap, self.filled, C_ref(self.pose_table), C_ref(view),
+                      C_ref(self.map_struct), _lib.ptr(self.c_xyz), _lib.ptr(self.c_attr), _lib.ptr(self.c_t),
+                      _lib.ptr(self.c_dyn), _lib.ptr(self._tiles), _lib.ptr(self.total), _lib.stream_ptr())
         host = torch.cat([self.total, self.map_stats]).cpu().numpy()  # the frame's one host sync
         self.count = int(host[0])
-        self.map_occupied, self.map_dropped = int(host[1]), int(host[2])
+        if map_on:
+            self.map_occupied, self.map_dropped = int(host[1]), int(host[2])
         self.normals_valid = False
         if neighbors:
             self.neighborhoods(float(radius), neighbors == "normals", sensor)

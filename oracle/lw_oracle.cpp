@@ -137,27 +137,32 @@ void or_voxel_keys(const float* xyz, int64_t n, float inv, int64_t* out) {
 }
 
 // ---- deskew (odom.py:163-178, gpu.py:268-283); raw/out are [m*4] (x, y, z, t) -----------------------------
+// deskew (gpu.py:268-283) by a fraction s of the frame's motion tw = (rho, theta): rotation in float64, rounded once
+static void deskew_s(float x, float y, float z, float s, const float* tw, float* out) {
+    float rx = tw[3] * s, ry = tw[4] * s, rz = tw[5] * s;
+    float a = len3(rx, ry, rz);
+    float ox = x, oy = y, oz = z;
+    if (!(a < 1.0e-9f)) {
+        double ad = a;
+        double ux = rx / ad, uy = ry / ad, uz = rz / ad;
+        double sh = sin(0.5 * ad), w = cos(0.5 * ad);
+        double vx = ux * sh, vy = uy * sh, vz = uz * sh;
+        double px = x, py = y, pz = z;
+        double tx = 2.0 * (vy * pz - vz * py), ty = 2.0 * (vz * px - vx * pz), tz = 2.0 * (vx * py - vy * px);
+        ox = (float)(px + w * tx + (vy * tz - vz * ty));
+        oy = (float)(py + w * ty + (vz * tx - vx * tz));
+        oz = (float)(pz + w * tz + (vx * ty - vy * tx));
+    }
+    out[0] = ox + tw[0] * s;
+    out[1] = oy + tw[1] * s;
+    out[2] = oz + tw[2] * s;
+}
+
 void or_deskew(const float* raw, int64_t m, float t_mid, float inv_dt, const float* tw, float* out) {
     for (int64_t i = 0; i < m; ++i) {
         const float* p = raw + 4 * i;
         float s = fminf(fmaxf((p[3] - t_mid) * inv_dt, -1.0f), 1.0f);
-        float rx = tw[3] * s, ry = tw[4] * s, rz = tw[5] * s;
-        float a = len3(rx, ry, rz);
-        float ox = p[0], oy = p[1], oz = p[2];
-        if (!(a < 1.0e-9f)) {
-            double ad = a;
-            double ux = rx / ad, uy = ry / ad, uz = rz / ad;
-            double sh = sin(0.5 * ad), w = cos(0.5 * ad);
-            double vx = ux * sh, vy = uy * sh, vz = uz * sh;
-            double px = p[0], py = p[1], pz = p[2];
-            double tx = 2.0 * (vy * pz - vz * py), ty = 2.0 * (vz * px - vx * pz), tz = 2.0 * (vx * py - vy * px);
-            ox = (float)(px + w * tx + (vy * tz - vz * ty));
-            oy = (float)(py + w * ty + (vz * tx - vx * tz));
-            oz = (float)(pz + w * tz + (vx * ty - vy * tx));
-        }
-        out[4 * i + 0] = ox + tw[0] * s;
-        out[4 * i + 1] = oy + tw[1] * s;
-        out[4 * i + 2] = oz + tw[2] * s;
+        deskew_s(p[0], p[1], p[2], s, tw, out + 4 * i);
         out[4 * i + 3] = p[3];
     }
 }
@@ -616,6 +621,73 @@ int64_t or_map_build(int64_t cap, const int64_t* keys, const int32_t* cnt, const
                 }
             }
             dyn = settled ? 0 : 1;
+        }
+        out_dyn[k] = dyn;
+        ++k;
+    }
+    return k;
+}
+
+// ---- live ring visible set (k_classify_live gpu.py:637-697, Pipeline.build live mode :1466-1504) ---------------
+// ring_xyz [cap*3]; poses [65536*16], tw [65536*6], owner_frame / owner_epoch [65536]; map arrays as lw_map (for
+// the Motion label). Writes the drawn points in ring order and returns their count.
+int64_t or_live_build(const float* ring_xyz, const uint32_t* ring_attr, const float* ring_t, const int32_t* ring_frame,
+                      int64_t cap, int64_t filled, const float* poses, const float* tw, const int32_t* owner_frame,
+                      const int32_t* owner_epoch, const View* vp, const int64_t* keys, const int32_t* cnt,
+                      const float* first, const int32_t* miss, float* out_xyz, uint32_t* out_attr, float* out_t,
+                      int32_t* out_dyn) {
+    const View& v = *vp;
+    int64_t k = 0;
+    const int64_t nf = std::min(filled, cap);
+    for (int64_t i = 0; i < nf; ++i) {
+        const float t = ring_t[i];
+        if (v.persist > 0.0f && v.now - t > v.persist) continue;
+        float p[3] = {ring_xyz[3 * i], ring_xyz[3 * i + 1], ring_xyz[3 * i + 2]};
+        const uint32_t a = ring_attr[i];
+        if (!keep_raw(p[0], p[1], p[2], a, v)) continue;
+        const int fid = ring_frame[i];
+        const int f = fid & (POSE_SLOTS - 1);
+        if (v.inv_frame_dt > 0.0f) {
+            if (owner_frame[f] != fid || owner_epoch[f] != v.epoch) continue;
+            const float xf = t * v.inv_frame_dt;
+            const float frac = xf - floorf(xf) - 0.5f;
+            float q[3];
+            deskew_s(p[0], p[1], p[2], frac, tw + 6 * (int64_t)f, q);
+            p[0] = q[0];
+            p[1] = q[1];
+            p[2] = q[2];
+        }
+        float wx, wy, wz;
+        xform(poses + 16 * (int64_t)f, p[0], p[1], p[2], wx, wy, wz);
+        if (v.crop_on != 0) {
+            if (wx < v.crop_lo[0] || wy < v.crop_lo[1] || wz < v.crop_lo[2]) continue;
+            if (wx > v.crop_hi[0] || wy > v.crop_hi[1] || wz > v.crop_hi[2]) continue;
+        }
+        out_xyz[3 * k] = wx;
+        out_xyz[3 * k + 1] = wy;
+        out_xyz[3 * k + 2] = wz;
+        out_attr[k] = a;
+        out_t[k] = t;
+        int dyn = 0;
+        if (v.dyn_on != 0) {
+            const int ix = ifloor(wx * v.inv_voxel), iy = ifloor(wy * v.inv_voxel), iz = ifloor(wz * v.inv_voxel);
+            int settled = 0;
+            for (int nb = 0; nb < 7 && !settled; ++nb) {  // settled_near, gpu.py:596-634
+                int jx = ix, jy = iy, jz = iz;
+                if (nb == 1) jx = ix - 1;
+                else if (nb == 2) jx = ix + 1;
+                else if (nb == 3) jy = iy - 1;
+                else if (nb == 4) jy = iy + 1;
+                else if (nb == 5) jz = iz - 1;
+                else if (nb == 6) jz = iz + 1;
+                const int sn = find_slot(key_ijk(jx, jy, jz), keys, v.map_mask);
+                if (sn >= 0) {
+                    float age = v.now - first[sn];
+                    if (age < 0.0f) age = 1.0e9f;
+                    if (age >= v.dyn_settle && transient(cnt[sn], miss[sn], v) == 0) settled = 1;
+                }
+            }
+            dyn = 1 - settled;
         }
         out_dyn[k] = dyn;
         ++k;

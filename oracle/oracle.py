@@ -81,6 +81,7 @@ def lib() -> C.CDLL:
             "or_map_insert": (None, [P, i32, P, P, P, i64, P, P, f32, i64, P, P, P, P, P, P]),
             "or_carve": (None, [P, i32, P, P, i64, P, i32, f32, f32, i32, i64, P, P, P, P, i32]),
             "or_map_build": (i64, [i64, P, P, P, P, P, P, P, i32, P, P, P, P]),
+            "or_live_build": (i64, [P, P, P, P, i64, i64, P, P, P, P, P, P, P, P, P, P, P, P, P]),
             "or_ground": (None, [P, i32, P, i64, f32, f32, i32, f32, f32, i32, f32, P, P]),
             "or_cluster": (i64, [P, i32, P, i32, i64, f32, f32, f32, i32, P, P, P, P, P, P, P, P]),
             "or_grid_build": (None, [C.POINTER(OrGrid), i64, P, P, i32]),
@@ -236,6 +237,27 @@ class Map:
         dyn = np.zeros(n, np.int32)
         k = lib().or_map_build(self.cap, _p(self.keys), _p(self.cnt), _p(self.acc), _p(self.last), _p(self.first),
                                _p(self.miss), C.byref(view), min_count, _p(xyz), _p(attr), _p(t), _p(dyn))
+        return xyz[:k], attr[:k], t[:k], dyn[:k]
+
+    def live_build(self, ring_xyz, ring_attr, ring_t, ring_frame, filled, poses, tw, owner_frame, owner_epoch, view):
+        """k_classify_live (gpu.py:637-697) over the first `filled` ring slots, in ring order, with this map's
+        history for the Motion label: (xyz, attr, t, dyn)."""
+        rx = np.ascontiguousarray(ring_xyz, dtype=np.float32).reshape(-1, 3)
+        cap = len(rx)
+        ra = np.ascontiguousarray(ring_attr).view(np.uint32).reshape(cap)
+        rt = np.ascontiguousarray(ring_t, dtype=np.float32).reshape(cap)
+        rf = np.ascontiguousarray(ring_frame, dtype=np.int32).reshape(cap)
+        ps = np.ascontiguousarray(poses, dtype=np.float32).reshape(POSE_SLOTS, 16)
+        tws = np.ascontiguousarray(tw, dtype=np.float32).reshape(POSE_SLOTS, 6)
+        of = np.ascontiguousarray(owner_frame, dtype=np.int32).reshape(POSE_SLOTS)
+        oe = np.ascontiguousarray(owner_epoch, dtype=np.int32).reshape(POSE_SLOTS)
+        xyz = np.zeros((cap, 3), np.float32)
+        attr = np.zeros(cap, np.uint32)
+        t = np.zeros(cap, np.float32)
+        dyn = np.zeros(cap, np.int32)
+        k = lib().or_live_build(_p(rx), _p(ra), _p(rt), _p(rf), cap, int(filled), _p(ps), _p(tws), _p(of), _p(oe),
+                                C.byref(view), _p(self.keys), _p(self.cnt), _p(self.first), _p(self.miss), _p(xyz),
+                                _p(attr), _p(t), _p(dyn))
         return xyz[:k], attr[:k], t[:k], dyn[:k]
 
     def as_dict(self):
