@@ -132,3 +132,37 @@ def test_normals_edge_cases():
     p = np.array([[0, 0, 0], [0.01, 0, 0], [0, 0.01, 0]], np.float32)
     nrm, pl = oracle.normals(p, 0.1)
     assert not nrm.any() and not pl.any()
+
+
+def test_offset_units_and_arguments_checked_before_cuda():
+    """lw_vox_offset_units is host arithmetic; the prior-map and live-ring entry points reject bad arguments before
+    any CUDA call, so these run without a GPU."""
+    import ctypes
+
+    from livox_warp import _lib
+
+    lib = _lib.load(require_cuda=False)
+    # 2^(30 - e) with voxel < 2^e: offsets below half a voxel stay below 2^29 units
+    for voxel, e in ((0.02, -5), (0.03125, -4), (0.05, -4), (1.0, 1), (3.0, 2)):
+        assert lib.lw_vox_offset_units(voxel) == 2.0 ** (30 - e)
+        assert np.float32(voxel) < 2.0 ** e and 0.5 * voxel * 2.0 ** (30 - e) <= 2 ** 29
+    fake = ctypes.c_void_p(16)  # never dereferenced: the checks fail first
+    vb = _lib.VoxBuf(*([fake] * len(_lib.VoxBuf.PTRS)), 1000, 8)  # not a power of two
+    assert lib.lw_vox_insert(vb, fake, 3, None, None, 4, 0, 0.05, None) == _lib.LW_EINVAL
+    assert b"power of two" in lib.lw_last_error()
+    vb.cap = 1024
+    assert lib.lw_vox_insert(vb, fake, 3, None, None, 16, 0, 0.05, None) == _lib.LW_ECAPACITY
+    assert lib.lw_vox_insert(vb, fake, 5, None, None, 4, 0, 0.05, None) == _lib.LW_EINVAL
+    assert lib.lw_vox_insert(vb, fake, 3, None, None, 4, -1, 0.05, None) == _lib.LW_EINVAL
+    assert lib.lw_vox_insert(vb, fake, 3, None, None, 4, 0, 1e-9, None) == _lib.LW_EINVAL
+    assert lib.lw_vox_emit(vb, 0.0, 4, None, None, None, None, None) == _lib.LW_EINVAL
+    pb = _lib.PcaBuf(*([fake] * len(_lib.PcaBuf.PTRS)), 1024, 512)
+    assert lib.lw_normals(fake, 3, 16, 0.0, pb, fake, fake, None) == _lib.LW_EINVAL
+    assert b"radius" in lib.lw_last_error()
+    assert lib.lw_normals(fake, 3, 16, 17.0, pb, fake, fake, None) == _lib.LW_EINVAL
+    assert lib.lw_normals(fake, 3, 600, 0.1, pb, fake, fake, None) == _lib.LW_ECAPACITY  # cap < 2n
+    assert lib.lw_normals(fake, 3, 16, 0.1, pb, None, fake, None) == _lib.LW_EINVAL
+    empty_map = _lib.Map(*([None] * 9), 1024)
+    assert lib.lw_live_build(fake, fake, fake, fake, 16, 16, None, None, empty_map, fake, fake, fake, fake, fake,
+                             fake, None) == _lib.LW_EINVAL
+    assert b"lw_live_build" in lib.lw_last_error()
