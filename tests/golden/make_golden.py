@@ -1,7 +1,7 @@
 """Generate the golden fixtures of tests/golden/ from the reference's own code (run in a container that has the
 reference checkout; the fixtures are committed, the GPU tests only read them).
 
-    python tests/golden/make_golden.py /path/to/livox-warp
+    python tests/golden/make_golden.py /path/to/livox-warp [fixture ...]
 
 The reference's modules import NVIDIA Warp at the top, which is not installed, so they cannot be imported.
 Their pure numpy / scipy functions are executed from source instead: this script parses each module with `ast`,
@@ -14,6 +14,10 @@ device solve:
   lvxr.npz          lvxr.py read_firings and Firings.points on seeded synthetic recordings (every record
                     layout, ns and GPS timestamps, clock jumps, IMU / malformed / truncated datagrams, the Mid-40
                     dual-return profile, LVXR1); lvxr.py imports only numpy and is loaded from its file.
+  tracker.npz       perception.py Tracker (the class, pure numpy) driven through a seeded scene of static,
+                    walking and reappearing objects, updates at 10 Hz and 144 Hz mixed, dropouts, shuffled cluster
+                    order and a clock restart: the clusters given, the ids and velocities returned, the confirmed
+                    tracks after every update.
   prior_prepare.npz mapgrid.py PriorGrid.prepare (a static method, taken out of its class) with
                     horizontal_levels and the module constants it reads (CELL, IDX_BITS, MAX_POINTS, PLANAR; the
                     one Warp call among them, wp.constant, is the identity here).
@@ -36,11 +40,11 @@ def extract(src_path: Path, names: list[str], consts: list[str] = ()) -> dict:
     tree = ast.parse(src_path.read_text())
     keep = []
     for node in tree.body:
-        if isinstance(node, ast.FunctionDef) and node.name in names:
+        if isinstance(node, (ast.FunctionDef, ast.ClassDef)) and node.name in names:
             keep.append(node)
         elif isinstance(node, ast.Assign) and any(isinstance(t, ast.Name) and t.id in consts for t in node.targets):
             keep.append(node)
-    found = {n.name for n in keep if isinstance(n, ast.FunctionDef)}
+    found = {n.name for n in keep if isinstance(n, (ast.FunctionDef, ast.ClassDef))}
     missing = set(names) - found
     if missing:
         raise KeyError(f"{src_path.name}: not found {sorted(missing)}")
@@ -282,14 +286,70 @@ def lvxr(ref: Path) -> dict:
     return out
 
 
+def tracker_scene(seed: int = 20261204):
+    """(now, clusters) per update: a static object with a wandering centroid, a large static box, a walker at
+    1 m/s, a second walker that leaves for longer than max_age and comes back, a pair that cross; updates every
+    0.1 s or 1/144 s at random, 10 % cluster dropouts, the clusters in random order, and the clock restarting once."""
+    rng = np.random.default_rng(seed)
+    times, t = [], 0.0
+    while t < 3.2:
+        times.append(t)
+        t += 0.1 if rng.random() < 0.5 else 1.0 / 144.0
+    times += [0.2 + 0.1 * k for k in range(8)]  # the sensor clock restarts (a replay loop)
+    objs = [  # (start, velocity, half extent, visible(t))
+        (np.array([2.0, 1.0, 0.5]), np.zeros(3), 0.2, lambda t: True),
+        (np.array([-4.0, 3.0, 1.0]), np.zeros(3), 1.0, lambda t: True),
+        (np.array([-3.0, -2.0, 0.9]), np.array([1.0, 0.3, 0.0]), 0.3, lambda t: True),
+        (np.array([4.0, -1.0, 0.9]), np.array([-0.8, 0.0, 0.0]), 0.3, lambda t: t < 1.2 or t > 2.3),
+        (np.array([0.0, 4.0, 0.9]), np.array([0.0, -1.2, 0.0]), 0.25, lambda t: True),
+        (np.array([-1.0, 1.5, 0.9]), np.array([0.9, 0.0, 0.0]), 0.25, lambda t: True),
+    ]
+    scene = []
+    for now in times:
+        cl = []
+        for p0, v, h, vis in objs:
+            if not vis(now) or rng.random() < 0.1:
+                continue
+            c = p0 + v * now + rng.normal(0.0, 0.02, 3)
+            e = h * (1.0 + 0.2 * rng.random())
+            cl.append({"cen": c, "lo": c - e, "hi": c + e, "cnt": int(rng.integers(30, 400))})
+        order = rng.permutation(len(cl))
+        scene.append((now, [cl[i] for i in order]))
+    return scene
+
+
+def tracker(ref: Path) -> dict:
+    ns = extract(ref / "python" / "livox_warp" / "perception.py", ["Tracker"])
+    tr = ns["Tracker"]()
+    now_l, n_l, cen, lo, hi, cnt, tid, vel, conf, n_conf = [], [], [], [], [], [], [], [], [], []
+    for now, cl in tracker_scene():
+        ids, v = tr.update(cl, now)
+        now_l.append(now)
+        n_l.append(len(cl))
+        for c in cl:
+            cen.append(c["cen"])
+            lo.append(c["lo"])
+            hi.append(c["hi"])
+            cnt.append(c["cnt"])
+        tid.extend(int(x) for x in ids)
+        vel.extend(v)
+        ok = sorted(int(t) for t, _ in tr.confirmed())
+        conf.extend(ok)
+        n_conf.append(len(ok))
+    return {"now": np.array(now_l), "n": np.array(n_l, np.int64), "cen": np.array(cen), "lo": np.array(lo),
+            "hi": np.array(hi), "cnt": np.array(cnt, np.int64), "tid": np.array(tid, np.int64),
+            "vel": np.array(vel).reshape(-1, 3), "confirmed": np.array(conf, np.int64),
+            "n_confirmed": np.array(n_conf, np.int64)}
+
+
+FIXTURES = {"host_solve": host_solve, "prior_prepare": prior_prepare, "lvxr": lvxr, "tracker": tracker}
+
+
 def main():
     ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
-    np.savez_compressed(HERE / "host_solve.npz", **host_solve(ref))
-    print("wrote", HERE / "host_solve.npz")
-    np.savez_compressed(HERE / "prior_prepare.npz", **prior_prepare(ref))
-    print("wrote", HERE / "prior_prepare.npz")
-    np.savez_compressed(HERE / "lvxr.npz", **lvxr(ref))
-    print("wrote", HERE / "lvxr.npz")
+    for name in sys.argv[2:] or list(FIXTURES):  # optionally only the named fixtures
+        np.savez_compressed(HERE / f"{name}.npz", **FIXTURES[name](ref))
+        print("wrote", HERE / f"{name}.npz")
 
 
 if __name__ == "__main__":
