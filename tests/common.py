@@ -60,3 +60,30 @@ def look_at(p, target) -> np.ndarray:
 def config1_pose() -> np.ndarray:
     """The single-frame ICP case's start pose: a corner of the box room, looking across it and slightly down."""
     return look_at([0.8, 0.8, 1.6], [7.0, 5.0, 1.0])
+
+
+def rule_local_maxima(sc, shape, pool):
+    """The local-maximum rule of localize.py:450-475 in numpy over every score at least the pool-th best: positive
+    and no lower than any in-range (x, y) / wrapped-heading neighbour at the same height. Unordered; the reference
+    takes exactly `pool` candidates, so at a tie on the pool-th score it may leave out some that this keeps
+    (tests/test_local_maxima_cpu.py pins the two against each other)."""
+    nz, nx, ny, nyaw = shape
+    thr = np.partition(sc, len(sc) - pool)[len(sc) - pool] if pool < len(sc) else sc.min()
+    cand = np.nonzero((sc > 0) & (sc >= thr))[0]
+    iyaw = cand % nyaw
+    ip = cand // nyaw
+    iy = ip % ny
+    ix = (ip // ny) % nx
+    iz = ip // (ny * nx)
+    best = np.ones(len(cand), bool)
+    mine = sc[cand]
+    for ox in (-1, 0, 1):
+        for oy in (-1, 0, 1):
+            for oa in (-1, 0, 1):
+                if ox == oy == oa == 0:
+                    continue
+                jx, jy = ix + ox, iy + oy
+                ok = (jx >= 0) & (jx < nx) & (jy >= 0) & (jy < ny)
+                j = ((iz * nx + np.clip(jx, 0, nx - 1)) * ny + np.clip(jy, 0, ny - 1)) * nyaw + (iyaw + oa) % nyaw
+                best &= ~ok | (sc[j] <= mine)
+    return cand[best]

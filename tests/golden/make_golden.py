@@ -18,6 +18,8 @@ device solve:
                     walking and reappearing objects, updates at 10 Hz and 144 Hz mixed, dropouts, shuffled cluster
                     order and a clock restart: the clusters given, the ids and velocities returned, the confirmed
                     tracks after every update.
+  local_maxima.npz  localize.py GlobalLocalizer._local_maxima and _top (the two methods, taken out of the class)
+                    on seeded coarse-score arrays with ties, occupied positions and several pool sizes.
   prior_prepare.npz mapgrid.py PriorGrid.prepare (a static method, taken out of its class) with
                     horizontal_levels and the module constants it reads (CELL, IDX_BITS, MAX_POINTS, PLANAR; the
                     one Warp call among them, wp.constant, is the identity here).
@@ -52,6 +54,20 @@ def extract(src_path: Path, names: list[str], consts: list[str] = ()) -> dict:
     ns = {"np": np, "Rotation": Rotation, "math": __import__("math")}
     exec(compile(mod, str(src_path), "exec"), ns)
     return ns
+
+
+def extract_methods(src_path: Path, cls: str, names: list[str]) -> type:
+    """A class holding only the named methods of `cls` (its other methods and its module's imports are left out)."""
+    tree = ast.parse(src_path.read_text())
+    node = next(n for n in tree.body if isinstance(n, ast.ClassDef) and n.name == cls)
+    body = [m for m in node.body if isinstance(m, ast.FunctionDef) and m.name in names]
+    if {m.name for m in body} != set(names):
+        raise KeyError(f"{src_path.name}: {cls} lacks {sorted(set(names) - {m.name for m in body})}")
+    mod = ast.Module(body=[ast.ClassDef(name=cls, bases=[], keywords=[], body=body, decorator_list=[])],
+                     type_ignores=[])
+    ns = {"np": np, "math": __import__("math")}
+    exec(compile(ast.fix_missing_locations(mod), str(src_path), "exec"), ns)
+    return ns[cls]
 
 
 def random_pose(rng, t_scale=5.0, r_scale=1.0):
@@ -342,7 +358,38 @@ def tracker(ref: Path) -> dict:
             "n_confirmed": np.array(n_conf, np.int64)}
 
 
-FIXTURES = {"host_solve": host_solve, "prior_prepare": prior_prepare, "lvxr": lvxr, "tracker": tracker}
+def local_maxima(ref: Path) -> dict:
+    """GlobalLocalizer._local_maxima and _top (localize.py:450-483) on seeded coarse-score arrays: smooth fields
+    with several modes, quantised so that equal scores occur, negative (occupied) positions, and pools smaller and
+    larger than the array."""
+    Loc = extract_methods(ref / "python" / "livox_warp" / "localize.py", "GlobalLocalizer",
+                          ["_local_maxima", "_top"])
+    rng = np.random.default_rng(20261205)
+    out = {}
+    cases = [((2, 24, 18, 36), 400, 50), ((3, 30, 20, 60), 20000, 1 << 20), ((1, 9, 7, 12), 5000, 7)]
+    for k, (shape, pool, keep) in enumerate(cases):
+        nz, nx, ny, nyaw = shape
+        x = np.linspace(0, 1, nx)[None, :, None, None]
+        y = np.linspace(0, 1, ny)[None, None, :, None]
+        a = np.linspace(0, 2 * np.pi, nyaw, endpoint=False)[None, None, None, :]
+        field = np.zeros(shape)
+        for _ in range(6):
+            cx, cy, ca, w = rng.random(), rng.random(), rng.uniform(0, 2 * np.pi), rng.uniform(100, 900)
+            field = field + w * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / 0.02) * np.exp(np.cos(a - ca) - 1)
+        field = field + rng.normal(0, 5, shape)
+        sc = np.round(field / 4) * 4  # ties
+        sc[rng.random(shape) < 0.15] = -1.0  # positions inside the map
+        sc = sc.astype(np.float32).ravel()
+        loc = Loc()
+        loc._top = lambda scores, pool=pool: Loc._top(scores, pool)
+        out[f"sc{k}"], out[f"shape{k}"] = sc, np.array(shape, np.int64)
+        out[f"pool{k}"], out[f"keep{k}"] = np.int64(pool), np.int64(keep)
+        out[f"idx{k}"] = np.asarray(loc._local_maxima(sc, shape, keep), np.int64)
+    return out
+
+
+FIXTURES = {"host_solve": host_solve, "prior_prepare": prior_prepare, "lvxr": lvxr, "tracker": tracker,
+            "local_maxima": local_maxima}
 
 
 def main():

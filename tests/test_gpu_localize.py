@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 import torch
 
+import common
 from oracle import oracle
 
 pytestmark = pytest.mark.gpu
@@ -299,31 +300,6 @@ def test_score_grid_rejects_too_many_headings(room):
         score_grid(grid, pts, pos, 4, 0.0, 0.01, 25.0, 10.0, out, pos_stride=0)
 
 
-def _rule_local_maxima(sc, shape, pool):
-    """The local-maximum rule of localize.py:450-475 in numpy over every score at least the pool-th best: positive
-    and no lower than any in-range (x, y) / wrapped-heading neighbour at the same height."""
-    nz, nx, ny, nyaw = shape
-    thr = np.partition(sc, len(sc) - pool)[len(sc) - pool] if pool < len(sc) else sc.min()
-    cand = np.nonzero((sc > 0) & (sc >= thr))[0]
-    iyaw = cand % nyaw
-    ip = cand // nyaw
-    iy = ip % ny
-    ix = (ip // ny) % nx
-    iz = ip // (ny * nx)
-    best = np.ones(len(cand), bool)
-    mine = sc[cand]
-    for ox in (-1, 0, 1):
-        for oy in (-1, 0, 1):
-            for oa in (-1, 0, 1):
-                if ox == oy == oa == 0:
-                    continue
-                jx, jy = ix + ox, iy + oy
-                ok = (jx >= 0) & (jx < nx) & (jy >= 0) & (jy < ny)
-                j = ((iz * nx + np.clip(jx, 0, nx - 1)) * ny + np.clip(jy, 0, ny - 1)) * nyaw + (iyaw + oa) % nyaw
-                best &= ~ok | (sc[j] <= mine)
-    return cand[best]
-
-
 def test_coarse_candidates_follow_the_local_maximum_rule(room):
     """lw_score_maxima through GlobalLocalizer._coarse_candidates: every local maximum among the 20000 best scores,
     the same set the reference's rule selects on the full score array, best first."""
@@ -336,7 +312,7 @@ def test_coarse_candidates_follow_the_local_maximum_rule(room):
     pos, shape, dyaw, s = loc._coarse(None, pts, heights)
     pos2, shape2, dyaw2, idx, val = loc._coarse_candidates(None, pts, heights, keep=1 << 20)
     assert shape2 == shape and np.array_equal(pos2, pos)
-    want = _rule_local_maxima(s, shape, 20000)
+    want = common.rule_local_maxima(s, shape, 20000)
     assert len(want) > 10 and set(idx.tolist()) == set(want.tolist())
     assert np.array_equal(val, s[idx]) and np.all(np.diff(val) <= 0)
     top = loc._coarse_candidates(None, pts, heights)[3]
