@@ -1,7 +1,8 @@
 """The reference's behavioural gates for the perception path, restated on this repository's synthetic scenes and
 evaluated on the CPU oracle (the GPU is held bit-exact to it by the -m gpu tests): ground labels and heights
-(check_perception.py:182-183), connected components on long structures (:276-284) and the tracker's static noise
-and speed (:262-263)."""
+(check_perception.py:182-183), connected components on long structures (:276-284), the tracker's static noise
+and speed (:262-263), Motion labels on the live visible set (:226-237) and free-space carving (:95-115, :240-241,
+:265-269)."""
 
 import math
 
@@ -79,3 +80,84 @@ def test_tracker_static_noise_and_speed():
     assert np.percentile(st, 90) < 0.1 and (st > 0.15).mean() < 0.03
     assert abs(np.median(w_speed) - 1.2) < 0.25 * 1.2
     assert len({int(t) for t in tid}) == 4  # four tracks, one per cluster
+
+
+VOXEL_C, PERSIST_C = 0.03, 0.3
+
+
+def _walker_scene():
+    """The reference's simulated room (sources.py:189-210, box_scene :668-677): floor 1.3 m below a static sensor
+    at the origin looking down +x, a crate, a shelf, two pillars, a table and a sign; a 0.9 m walker (a cylinder
+    of the sphere's 0.45 m radius) crossing the far end at x = 12 m, starting mid-lane at y = 0 and walking to
+    y = 2.5 m at 1 m/s (away from its start by 3.5 s, as the reference's sphere is). 3.5 s of the Mid-40 rosette
+    at 100k points/s, 1 cm range noise."""
+    from livox_warp import synth
+
+    walker = synth.Cylinder(np.array([12.0, -2.5]), np.array([12.0, 2.5]), 1.0, radius=0.45, height=0.9, phase=2.5)
+    boxes = np.array([[4.0, -1.8, 0.0, 5.2, -0.6, 1.1], [9.5, 2.6, 0.0, 10.1, 4.4, 2.9],
+                      [2.3, -2.7, 0.0, 2.7, -2.3, 3.9], [10.8, 3.3, 0.0, 11.2, 3.7, 3.9],
+                      [8.0, -3.3, 0.0, 9.2, -2.1, 0.75], [13.8, -0.6, 1.7, 13.99, 0.6, 2.3]])
+    scene = synth.Scene(np.array([-2.0, -4.0, 0.0]), np.array([14.0, 4.5, 3.9]), boxes, [walker])
+    T0 = np.eye(4)
+    T0[:3, 3] = [0.0, 0.0, 1.3]
+    x, a, t = synth.scan(scene, synth.ConstantVelocity(T0, 1e9, 0.0, 0.0), 0.0, 3.5, 100000.0, 7, noise=0.01)
+    return walker, T0, x, a, t
+
+
+def _view_c(now, persist=PERSIST_C, dyn=True, carve=True, settle=2.5):
+    """The reference's viewer settings for Motion labels and carving (check_perception.py:32-36)."""
+    from livox_warp import gpu
+
+    return gpu.make_view(now=now, persist=persist, voxel=VOXEL_C, map_cap=1 << 21, noise_mask=0b0001,
+                         dyn_on=int(dyn), dyn_settle=settle, carve_on=int(carve), carve_ratio=2.0, carve_min=3,
+                         carve_stale=1.0)
+
+
+@pytest.mark.parametrize("every", [1, 2])
+def test_motion_and_carving_gates(every):
+    """Motion labels on the live visible set: > 70 % of the walker's points moving, < 10 % of the far wall's
+    (check_perception.py:226-237). Carving, with every return and with every other return traced: of the map
+    voxels where the walker started, fewer than half survive (and there were > 50), the far wall is all kept
+    (> 97 %), the floor seen at grazing incidence is kept (> 99 %) and < 2 % of it is labelled moving
+    (check_perception.py:95-115)."""
+    walker, T0, x, a, t = _walker_scene()
+    S = oracle.POSE_SLOTS
+    poses = np.tile(np.eye(4, dtype=np.float32).reshape(1, 16), (S, 1))
+    poses[0] = T0.astype(np.float32).reshape(16)
+    fid = np.zeros(len(t), np.int32)  # no odometry: every point is posed by frame 0
+    om = oracle.Map(1 << 21)
+    for k in range(35):  # 0.1 s batches: insert, then carve (check_perception.py:39-47)
+        sel = (t >= 0.1 * k) & (t < 0.1 * (k + 1))
+        om.insert(x[sel], a[sel], t[sel], fid[sel], poses, _view_c(float(t[sel].max())), VOXEL_C)
+        om.carve(x[sel], a[sel], fid[sel], poses, VOXEL_C, every=every)
+    now = float(t.max())
+    if every == 1:
+        lx, _, _, ld = om.live_build(x, a, t, fid, len(t), poses, np.zeros((S, 6), np.float32),
+                                     np.zeros(S, np.int32), np.zeros(S, np.int32), _view_c(now))
+        c = walker.centre(np.array([now - 0.05]))[0]
+        near = (np.linalg.norm(lx[:, :2] - c, axis=1) < 0.6) & (lx[:, 2] < 1.0)
+        wall = (lx[:, 0] > float(np.percentile(lx[:, 0], 99.0)) - 0.5) & (np.abs(lx[:, 1]) > 3.0)
+        assert near.sum() > 100 and wall.sum() > 500
+        assert ld[near].mean() > 0.7 and ld[wall].mean() < 0.1
+    # the map as the viewer shows it, settle 0: 'moving' from carving alone (check_perception.py:50-57)
+    m_all = om.build(_view_c(now, persist=0.0, carve=False, settle=0.0))[0]
+    m_c, _, _, dyn_c = om.build(_view_c(now, persist=0.0, carve=True, settle=0.0))
+    p0 = np.array([*walker.centre(np.array([0.1]))[0], 0.45])
+    x_far = float(np.percentile(m_all[:, 0], 99.0)) - 0.3
+
+    def ghost(m):
+        return np.linalg.norm(m - p0, axis=1) < 0.4
+
+    def wall(m):
+        return (m[:, 0] > x_far) & (np.abs(m[:, 1]) < 2.0)
+
+    def floor(m):
+        return (m[:, 2] < 0.1) & (m[:, 0] > 2.0) & (m[:, 0] < 11.0)
+
+    g0, g1 = ghost(m_all).sum(), ghost(m_c).sum()
+    w0, w1 = wall(m_all).sum(), wall(m_c).sum()
+    f0, f1 = floor(m_all).sum(), floor(m_c).sum()
+    assert g0 > 50 and g1 < 0.5 * g0
+    assert w1 / max(w0, 1) > 0.97 and f0 > 1000 and f1 / max(f0, 1) > 0.99
+    assert dyn_c[floor(m_c)].mean() < 0.02
+
