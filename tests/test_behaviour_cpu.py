@@ -116,7 +116,7 @@ def _view_c(now, persist=PERSIST_C, dyn=True, carve=True, settle=2.5):
 @pytest.mark.parametrize("every", [1, 2])
 def test_motion_and_carving_gates(every):
     """Motion labels on the live visible set: > 70 % of the walker's points moving, < 10 % of the far wall's
-    (check_perception.py:226-237). Carving, with every return and with every other return traced: of the map
+    (check_perception.py:226-237); its clusters: at least 4, the walker in one (:195). Carving, with every return and with every other return traced: of the map
     voxels where the walker started, fewer than half survive (and there were > 50), the far wall is all kept
     (> 97 %), the floor seen at grazing incidence is kept (> 99 %) and < 2 % of it is labelled moving
     (check_perception.py:95-115)."""
@@ -139,6 +139,13 @@ def test_motion_and_carving_gates(every):
         wall = (lx[:, 0] > float(np.percentile(lx[:, 0], 99.0)) - 0.5) & (np.abs(lx[:, 1]) > 3.0)
         assert near.sum() > 100 and wall.sum() > 500
         assert ld[near].mean() > 0.7 and ld[wall].mean() < 0.1
+        # clusters of the live set after ground with normals (check_perception.py:59-62, 187-195): at least 4,
+        # and the walker's points in one of them (> 80 %)
+        _, nrm, _ = oracle.neighborhoods(lx, 0.15, True, (0.0, 0.0, 1.3))
+        gnd, _ = oracle.ground(lx, cell=0.5, thick=0.15, min_sup=3, thresh=0.2, slope_step=0.3, nrm=nrm, nz_min=0.7)
+        cid, _, clusters, _ = oracle.cluster(lx, gnd, voxel=0.1, connect=0.35, min_pts=40)
+        ids, counts = np.unique(cid[near & (cid >= 0)], return_counts=True)
+        assert len(clusters) >= 4 and len(ids) >= 1 and counts.max() / near.sum() > 0.8
     # the map as the viewer shows it, settle 0: 'moving' from carving alone (check_perception.py:50-57)
     m_all = om.build(_view_c(now, persist=0.0, carve=False, settle=0.0))[0]
     m_c, _, _, dyn_c = om.build(_view_c(now, persist=0.0, carve=True, settle=0.0))
