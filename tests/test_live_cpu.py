@@ -1,7 +1,8 @@
 """The live ring's visible set (k_classify_live, gpu.py:637-697) in the oracle against a numpy restatement of the
 reference kernel: which ring slots are drawn (age, keep_raw, the pose slot's owner frame and epoch, the crop box),
 in ring order, their deskewed and posed world points (Rodrigues' rotation in float64 here, the oracle's quaternion
-form there: within 2e-6 m), attributes, times, and the Motion label against an empty map (nothing settled)."""
+form there: within 2e-6 m), attributes, times, and the Motion label against an empty map (nothing settled); and
+the reference's live-window gate of smoke_pipeline.py:43-50."""
 
 import numpy as np
 
@@ -99,3 +100,31 @@ def test_live_build_empty_ring():
                                    np.zeros((S, 16), np.float32), np.zeros((S, 6), np.float32), np.zeros(S, np.int32),
                                    np.zeros(S, np.int32), v)
     assert len(ox) == 0
+
+
+def test_pose_entry_moves_the_live_window():
+    """smoke_pipeline.py:43-50: the live set of a static scan with frame 0's pose at identity, then at a yaw of 90
+    degrees and a (1, 2, 0) m offset (gpu.mount_matrix): the centroid moves as that pose says, within 5 cm."""
+    from livox_warp import gpu, synth
+
+    sc = synth.box_room(1)
+    T = np.eye(4)
+    T[:3, 3] = [4.0, 3.0, 1.5]
+    x = synth.spin_scan(sc, T, 40000, 2)
+    n = len(x)
+    a = np.full(n, 100, np.uint32)
+    t = np.linspace(0.0, 0.4, n).astype(np.float32)
+    S = oracle.POSE_SLOTS
+    tw = np.zeros((S, 6), np.float32)
+    own = np.zeros(S, np.int32)
+    om = oracle.Map(1 << 10)
+    v = _view(now=0.4, persist=0.5, voxel=0.03, map_cap=1 << 10)
+    cents = []
+    for M in (np.eye(4, dtype=np.float32), gpu.mount_matrix(0, 0, 90, 1.0, 2.0, 0.0)):
+        poses = np.tile(np.eye(4, dtype=np.float32).reshape(1, 16), (S, 1))
+        poses[0] = np.asarray(M, np.float32).reshape(16)
+        lx, _, _, _ = om.live_build(x, a, t, np.zeros(n, np.int32), n, poses, tw, own, own, v)
+        assert len(lx) > 0.9 * n
+        cents.append(lx.astype(np.float64).mean(0))
+    c0, c = cents
+    assert abs((c[0] - 1.0) + c0[1]) < 0.05 and abs((c[1] - 2.0) - c0[0]) < 0.05
