@@ -289,8 +289,8 @@ int lw_map_build(const lw_map* map, const lw_view* v, int32_t min_count, float* 
  * than v->persist (when > 0), passes keep_raw, and -- when v->inv_frame_dt > 0 -- whose frame's pose slot holds
  * that frame for v->epoch, deskewed by the frame's twist from its time within the frame; posed by its frame's
  * matrix and inside the crop box. out_* [cap] get the world point, the attribute, the time and, with v->dyn_on,
- * the Motion label from the map's history (settled_near, gpu.py:596-634), else 0. ring_xyz is [cap*3]; tiles is
- * [cap/1024 + 2] scratch; writes count_dev[0]. */
+ * the Motion label from the map's history (settled_near, gpu.py:596-634), else 0. ring_xyz is [cap*3] with
+ * cap <= 2^30; tiles is [cap/1024 + 2] scratch; writes count_dev[0]. */
 int lw_live_build(const float* ring_xyz, const uint32_t* ring_attr, const float* ring_t, const int32_t* ring_frame,
                   int64_t cap, int64_t filled, const lw_pose_table* pt, const lw_view* v, const lw_map* map,
                   float* out_xyz, uint32_t* out_attr, float* out_t, int32_t* out_dyn, int32_t* tiles,

@@ -799,8 +799,8 @@ int lw_live_build(const float* ring_xyz, const uint32_t* ring_attr, const float*
     int r = check_map(map, "lw_live_build");
     if (r != LW_OK) return r;
     if (!pt || !pt->poses || !pt->tw || !pt->owner_frame || !pt->owner_epoch || !v || !tiles || !count_dev ||
-        cap < 0 || cap > (1LL << 31) - 1)
-        return set_error(LW_EINVAL, "lw_live_build: bad arguments");
+        cap < 0 || cap > (1LL << 30))  // at most 2^20 tiles of 1024 slots
+        return set_error(LW_EINVAL, "lw_live_build: bad arguments (ring capacity at most 2^30)");
     if (cap > 0 && (!ring_xyz || !ring_attr || !ring_t || !ring_frame || !out_xyz || !out_attr || !out_t || !out_dyn))
         return set_error(LW_EINVAL, "lw_live_build: missing ring or output buffers");
     if (v->dyn_on != 0 && (v->map_mask < 0 || (int64_t)v->map_mask > map->cap - 1))
