@@ -9,7 +9,7 @@ step (tx, ty, tz, rx, ry, rz) with T = T_pred * [R(r), t]; the Gauss-Newton regi
 anchors its prior at, that pose (Odometry.learned_init).
 
 Training pairs (make_pairs): a sequence is registered by the plain odometry; its converged poses are the
-judges. The registration map is then rebuilt frame by frame from those poses, and before frame k is inserted
+labels. The registration map is then rebuilt frame by frame from those poses, and before frame k is inserted
 its point sets are cut around Gaussian-perturbed copies of its converged pose, the perturbation being the
 target -- so a frame never sees itself in its map patch, as at run time.
 """
