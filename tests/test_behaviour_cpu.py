@@ -1,8 +1,8 @@
 """The reference's behavioural gates for the perception path, restated on this repository's synthetic scenes and
 evaluated on the CPU oracle (the GPU is held bit-exact to it by the -m gpu tests): ground labels and heights
 (check_perception.py:182-183), connected components on long structures (:276-284), the tracker's static noise
-and speed (:262-263), Motion labels on the live visible set (:226-237) and free-space carving (:95-115, :240-241,
-:265-269)."""
+and speed (:262-263), Motion labels on the live visible set (:226-237), free-space carving (:95-115, :240-241,
+:265-269), and the voxel-summary normals against exact PCA (check_normals.py:49-75)."""
 
 import math
 
@@ -168,3 +168,25 @@ def test_motion_and_carving_gates(every):
     assert w1 / max(w0, 1) > 0.97 and f0 > 1000 and f1 / max(f0, 1) > 0.99
     assert dyn_c[floor(m_c)].mean() < 0.02
 
+
+
+def test_voxel_summary_normals_against_exact_pca():
+    """check_normals.py:49-75 on a synthetic handheld sequence instead of a recording: the normals of the voxel
+    summary (Pipeline.neighborhoods, radius 0.1 m) against the smallest eigenvector of every point's exact
+    neighbourhood within the same radius (lw_normals' definition): median angle under 10 degrees."""
+    import common
+
+    frames = common.handheld_frames(10)
+    traj = common.handheld()
+    pts = []
+    for k, (x, a, t) in enumerate(frames):
+        T = common.mid_pose(traj, k)
+        pts.append(x.astype(np.float64) @ T[:3, :3].T + T[:3, 3])
+    xyz = np.concatenate(pts).astype(np.float32)
+    _, vox, _ = oracle.neighborhoods(xyz, 0.1, True, common.mid_pose(traj, 9)[:3, 3])
+    exact, _ = oracle.normals(xyz, 0.1)
+    ok = exact.any(axis=1)  # points with at least 4 neighbours
+    assert ok.mean() > 0.9
+    cos = np.abs((vox[ok].astype(np.float64) * exact[ok]).sum(1))
+    ang = np.degrees(np.arccos(np.clip(cos, 0.0, 1.0)))
+    assert len(ang) > 50000 and np.median(ang) < 10.0
