@@ -2,7 +2,8 @@
 evaluated on the CPU oracle (the GPU is held bit-exact to it by the -m gpu tests): ground labels and heights
 (check_perception.py:182-183), connected components on long structures (:276-284), the tracker's static noise
 and speed (:262-263), Motion labels on the live visible set (:226-237), free-space carving (:95-115, :240-241,
-:265-269), and the voxel-summary normals against exact PCA (check_normals.py:49-75)."""
+:265-269), the voxel-summary normals against exact PCA (check_normals.py:49-75), and global localisation in a
+prior map built here (check_prior_map.py:37-48)."""
 
 import math
 
@@ -190,3 +191,45 @@ def test_voxel_summary_normals_against_exact_pca():
     cos = np.abs((vox[ok].astype(np.float64) * exact[ok]).sum(1))
     ang = np.degrees(np.arccos(np.clip(cos, 0.0, 1.0)))
     assert len(ang) > 50000 and np.median(ang) < 10.0
+
+
+def test_global_localisation_in_a_built_prior_map():
+    """check_prior_map.py:37-48 (global localisation within 2 cm / 0.3 deg of the truth) with a prior map built as
+    prior_map.from_points builds one, on the oracle: a terrestrial scan of the box room from two stations (0.5 deg
+    steps), voxel means at 2 cm, normals and planarity within 8 cm, the prior grid; then for 360-degree scans from
+    three free poses, the coarse search over every position on a 0.25 m grid x 180 headings (1024 spread points,
+    tau 25 cm), its 16 best local maxima refined by the batched ICP (the localisation schedule) and the best by the
+    evaluation kept."""
+    import common
+    from livox_warp import synth
+    from livox_warp.localize import SCHEDULE_ICP, coarse_positions, pose_difference
+
+    sc = synth.box_room(1)
+    cloud = synth.tls_scan(sc, [[2.0, 2.0, 1.5], [6.0, 4.0, 1.6]], seed=0, step_deg=0.5)
+    vx, _, _, _ = oracle.voxel_downsample(cloud, None, None, 0.02)
+    nrm, pl = oracle.normals(vx, 0.08)
+    og = oracle.PriorGrid(oracle.prior_prepare(vx, nrm, pl))
+    pos, nx, ny = coarse_positions(vx.min(0), vx.max(0), [1.2], 0.25)
+    n_yaw, dyaw = 180, math.radians(2.0)
+    for h, T_true in enumerate(synth.free_poses(sc, 3, 5, z=1.2, margin=0.6)):
+        x = synth.spin_scan(sc, T_true, 60000, 11 + h, noise=0.01)
+        x = x[np.linalg.norm(x, axis=1) > 0.3]
+        _, first = np.unique(np.floor(x / 0.15).astype(np.int64), axis=0, return_index=True)
+        spread = x[np.sort(first)]
+        sub = spread[np.random.default_rng(h).choice(len(spread), 1024, replace=False)].astype(np.float32)
+        s = og.score_grid(sub, pos, n_yaw, 0.0, dyaw, 25.0, 10.0)
+        cand = common.rule_local_maxima(s, (1, nx, ny, n_yaw), 20000)
+        cand = cand[np.lexsort((cand, -s[cand]))][:16]
+        T0 = np.tile(np.eye(4), (len(cand), 1, 1))
+        for i, c in enumerate(cand):
+            yaw = (c % n_yaw) * dyaw
+            T0[i, :3, :3] = [[math.cos(yaw), -math.sin(yaw), 0.0], [math.sin(yaw), math.cos(yaw), 0.0], [0, 0, 1]]
+            T0[i, :3, 3] = pos[c // n_yaw]
+        pts = oracle.thin_5cm(x)[:20000]
+        pts4 = np.zeros((len(cand) * len(pts), 4), np.float32)
+        pts4[:, :3] = np.tile(pts, (len(cand), 1))
+        lo = np.arange(len(cand)) * len(pts)
+        T, _, _ = og.icp(pts4, lo, lo + len(pts), T0, SCHEDULE_ICP)
+        ev = og.evaluate(pts4, lo, lo + len(pts), T)
+        dt, dr = pose_difference(T_true, T[int(np.argmax(ev[:, 0]))])
+        assert dt < 0.02 and dr < 0.3, (h, dt, dr)
