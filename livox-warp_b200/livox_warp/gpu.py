@@ -77,6 +77,26 @@ def make_view(now: float = 0.0, persist: float = 0.0, voxel: float = 0.05, map_c
     return v
 
 
+SAMPLE_N = 1 << 16  # points the visible-set statistics sample (gpu.py:1243)
+
+
+def strided_sample(x: torch.Tensor, count: int, m: int = SAMPLE_N) -> torch.Tensor:
+    """Every stride-th of the first `count` rows of x, at most m of them, stride = max(1, count // m)
+    (Pipeline._sample_stride and k_gather_*, gpu.py:1029-1049, 1575-1579)."""
+    stride = max(1, count // m)
+    k = min(m, (count + stride - 1) // stride)
+    return x[:count:stride][:k]
+
+
+def rebase_times(keys: torch.Tensor, first: torch.Tensor, last: torch.Tensor, shift: float):
+    """k_rebase_clock (gpu.py:330-337): the occupied voxels' first / last-seen times onto a restarted clock,
+    new = old - shift in float32; empty slots keep theirs."""
+    occ = keys != -1
+    s = torch.tensor(shift, dtype=first.dtype, device=first.device)
+    first.copy_(torch.where(occ, first - s, first))
+    last.copy_(torch.where(occ, last - s, last))
+
+
 def _as_xyz(x, device) -> torch.Tensor:
     """Device float32 points of shape (n, 3) or (n, 4) (x, y, z, anything)."""
     if isinstance(x, np.ndarray):
@@ -206,6 +226,11 @@ class Pipeline:
     def clear_map(self):
         _lib.call("lw_map_clear", C_ref(self.map_struct), _lib.stream_ptr())
         self.map_occupied = self.map_dropped = 0
+
+    def rebase_clock(self, shift: float):
+        """The live clock restarted (replay loop, sensor reboot): move the map's first / last-seen times onto the new
+        clock, new = old - shift, so persistence, Motion labels and ghosts keep working (gpu.py:1368-1372)."""
+        rebase_times(self.map_keys, self.map_first, self.map_last, float(shift))
 
     # ---- poses ----------------------------------------------------------------------------------------------
 
@@ -409,6 +434,22 @@ class Pipeline:
         nsum = np.minimum(cnt, MAP_COUNT_CAP).astype(np.float64)
         cen = (acc[:, :3].astype(np.float64) / (nsum[:, None] * FIX_W)).astype(np.float32)
         return keys[occ], cen, cnt
+
+    def floor_z(self) -> float | None:
+        """A low (1st) percentile of the visible z, from a strided sample: where the floor usually is
+        (gpu.py:1597-1600)."""
+        if self.count == 0:
+            return None
+        z = strided_sample(self.c_xyz, self.count)[:, 2].cpu().numpy()
+        z = z[np.isfinite(z)]
+        return float(np.percentile(z, 1.0)) if z.size else None
+
+    def bounds(self, lo_pct: float = 2.0, hi_pct: float = 98.0):
+        """Robust (lo, hi) corners of the visible set from a strided sample (gpu.py:1602-1609)."""
+        if self.count == 0:
+            return None
+        pts = strided_sample(self.c_xyz, self.count).cpu().numpy()
+        return np.percentile(pts, lo_pct, axis=0), np.percentile(pts, hi_pct, axis=0)
 
     def export(self):
         n = self.count

@@ -128,3 +128,25 @@ def test_pose_entry_moves_the_live_window():
         cents.append(lx.astype(np.float64).mean(0))
     c0, c = cents
     assert abs((c[0] - 1.0) + c0[1]) < 0.05 and abs((c[1] - 2.0) - c0[0]) < 0.05
+
+
+def test_visible_set_sample_and_clock_rebase():
+    """The strided sample behind Pipeline.bounds / floor_z (gpu.py:1575-1609) and the clock rebase of the map's
+    hit times (k_rebase_clock, gpu.py:330-337), on CPU tensors."""
+    import torch
+
+    from livox_warp.gpu import rebase_times, strided_sample
+
+    x = torch.arange(300000, dtype=torch.float32).reshape(-1, 3)  # 100000 rows
+    s = strided_sample(x, 100000, 1 << 16)
+    assert len(s) == 1 << 16 and torch.equal(s[1], x[1])  # stride 1 (100000 // 65536), first 65536 rows
+    s = strided_sample(x, 100000, 1000)
+    assert len(s) == 1000 and torch.equal(s[3], x[300])
+    s = strided_sample(x, 7, 1 << 16)
+    assert len(s) == 7
+    keys = torch.tensor([5, -1, 9], dtype=torch.int64)
+    first = torch.tensor([10.5, 1.0e30, 3.25], dtype=torch.float32)
+    last = torch.tensor([12.0, 0.0, 4.0], dtype=torch.float32)
+    rebase_times(keys, first, last, 3.0)
+    assert first[0].item() == 7.5 and first[2].item() == 0.25 and first[1].item() > 1e29  # empty slot untouched
+    assert last.tolist() == [9.0, 0.0, 1.0]
