@@ -1,5 +1,10 @@
-"""Batched point-to-plane ICP against a prior map (localize.py): pose tracking (refine) and the registration of
-many pose hypotheses at once (register_batch).
+"""Global localisation in a prior map (localize.py): the search (GlobalLocalizer.localize, Localizer), pose tracking
+(refine) and the registration of many pose hypotheses at once (register_batch).
+
+The search keeps the reference's stages: the scan's gravity candidates from its horizontal planes (ScanPrep, here
+without open3d: 5 cm voxel means, PCA normals from lw_normals, seeded RANSAC planes), the sensor heights where the
+scan's horizontal surfaces line up with the map's, the coarse search with its local maxima on the device, a finer
+local grid scored with more points, non-maximum suppression, then the batched ICP and the evaluation.
 
 The reference runs GlobalLocalizer._icp (localize.py:517-553) as 3 launches, a device-to-host copy and a numpy
 6x6 solve per iteration, for at most 16 poses over one shared scan. Here the whole schedule -- every iteration
@@ -57,6 +62,136 @@ def pose_difference(A: np.ndarray, B: np.ndarray):
     d = np.linalg.inv(A) @ B
     ang = math.degrees(math.acos(np.clip((np.trace(d[:3, :3]) - 1) / 2, -1, 1)))
     return float(np.linalg.norm(A[:3, 3] - B[:3, 3])), ang
+
+
+def rot_to(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Rotation taking unit vector a onto unit vector b (localize.py:211-219)."""
+    a, b = a / np.linalg.norm(a), b / np.linalg.norm(b)
+    v = np.cross(a, b)
+    c = float(np.dot(a, b))
+    if np.linalg.norm(v) < 1e-9:
+        return np.eye(3) if c > 0 else np.diag([1.0, -1.0, -1.0])
+    vx = np.array([[0.0, -v[2], v[1]], [v[2], 0.0, -v[0]], [-v[1], v[0], 0.0]])
+    return np.eye(3) + vx + vx @ vx * (1.0 / (1.0 + c))
+
+
+def voxel_means(xyz: np.ndarray, voxel: float) -> np.ndarray:
+    """The mean of the points in each voxel of a grid anchored at the points' minimum (open3d's
+    voxel_down_sample, which the reference's ScanPrep calls), in the order of each voxel's first point."""
+    p = np.asarray(xyz, dtype=np.float64).reshape(-1, 3)
+    if len(p) == 0:
+        return p
+    k = np.floor((p - p.min(axis=0)) / voxel).astype(np.int64)
+    _, first, inv = np.unique(k, axis=0, return_index=True, return_inverse=True)
+    inv = inv.reshape(-1)
+    rank = np.empty(len(first), np.int64)
+    rank[np.argsort(first, kind="stable")] = np.arange(len(first))
+    vid = rank[inv]
+    out = np.zeros((len(first), 3))
+    np.add.at(out, vid, p)
+    return out / np.bincount(vid, minlength=len(first))[:, None]
+
+
+def ransac_plane(pts: np.ndarray, dist: float, iters: int, rng: np.random.Generator):
+    """The plane through 3 of the points with the most points within `dist` over `iters` seeded draws, refitted
+    to those inliers by least squares (what the reference asks of open3d's segment_plane(dist, 3, iters)):
+    (a, b, c, d) with a unit normal, and the inlier indices."""
+    n = len(pts)
+    tri = rng.integers(0, n, (iters, 3))
+    a, b, c = pts[tri[:, 0]], pts[tri[:, 1]], pts[tri[:, 2]]
+    nrm = np.cross(b - a, c - a)
+    ln = np.linalg.norm(nrm, axis=1)
+    good = ln > 1e-12
+    nrm[good] /= ln[good, None]
+    d = -(nrm * a).sum(axis=1)
+    counts = np.full(iters, -1, np.int64)
+    ok = np.flatnonzero(good)
+    for c0 in range(0, len(ok), 32):  # 32 draws per pass: n x 32 distances at a time
+        j = ok[c0:c0 + 32]
+        counts[j] = (np.abs(pts @ nrm[j].T + d[j]) <= dist).sum(axis=0)
+    if len(ok) == 0:
+        return None, np.zeros(0, np.int64)
+    best = int(np.argmax(counts))  # the first draw with the most inliers
+    inl = np.flatnonzero(np.abs(pts @ nrm[best] + d[best]) <= dist)
+    q = pts[inl]
+    mu = q.mean(axis=0)
+    w, V = np.linalg.eigh((q - mu).T @ (q - mu))
+    m = V[:, 0]
+    if m @ nrm[best] < 0:
+        m = -m
+    dd = -float(m @ mu)
+    inl = np.flatnonzero(np.abs(pts @ m + dd) <= dist)
+    return np.array([m[0], m[1], m[2], dd]), inl
+
+
+class ScanPrep:
+    """Host preparation of a scan in the sensor frame (localize.py:243-316) without open3d: 5 cm voxel means,
+    a PCA normal per point from its neighbours within 0.2 m (lw_normals on the device), and up to 8 planes found
+    by seeded RANSAC (3 cm, 1000 draws, at least 150 inliers) -> up candidates and the height profile.
+    `normals` may supply the normal estimator (a function of (points, radius) returning (normals, planarity))."""
+
+    def __init__(self, xyz: np.ndarray, voxel: float = 0.05, max_tilt_deg: float = 45.0, seed: int = 0,
+                 normals=None):
+        self.pts = voxel_means(xyz, voxel)
+        if normals is None:
+            from . import prior_map
+
+            normals = prior_map.normals
+        nrm, _ = normals(self.pts.astype(np.float32), 0.2)
+        self.normals = np.asarray(nrm, dtype=np.float64)
+        self.planes = []  # (inliers, unit normal, offset, inlier indices)
+        rng = np.random.default_rng(seed)
+        idx = np.arange(len(self.pts))
+        for _ in range(8):
+            if len(idx) < 300:
+                break
+            model, inl = ransac_plane(self.pts[idx], 0.03, 1000, rng)
+            if model is None or len(inl) < 150:
+                break
+            self.planes.append((len(inl), model[:3], float(model[3]), idx[inl]))
+            keep = np.ones(len(idx), bool)
+            keep[inl] = False
+            idx = idx[keep]
+        self.max_tilt = max_tilt_deg
+
+    def up_candidates(self):
+        """[(up unit vector, evidence)] ranked by plane support, both signs of each family (localize.py:275-306):
+        the near-horizontal planes grouped within 10 degrees, one normal fitted to each family's planes together
+        (the smallest eigenvector of their summed scatter about their own centroids), the two best families."""
+        cos_tilt = math.cos(math.radians(self.max_tilt))
+        fams = []  # [support, [plane indices], seed normal]
+        for i, (cnt, n, _, _) in enumerate(self.planes):
+            if abs(n[2]) < cos_tilt:
+                continue  # a wall, for a sensor that is roughly level (or upside down)
+            for f in fams:
+                if abs(float(n @ f[2])) > math.cos(math.radians(10.0)):
+                    f[0] += cnt
+                    f[1].append(i)
+                    break
+            else:
+                fams.append([cnt, [i], n])
+        out = []
+        for support, members, n0 in sorted(fams, key=lambda f: -f[0])[:2]:
+            S = np.zeros((3, 3))
+            for i in members:
+                P = self.pts[self.planes[i][3]]
+                P = P - P.mean(0)
+                S += P.T @ P
+            w, V = np.linalg.eigh(S)
+            n = V[:, 0]
+            if n @ n0 < 0:
+                n = -n
+            out += [(n, support), (-n, support)]
+        if not out:  # no floor or ceiling in view: a level sensor, either way up
+            out = [(np.array([0.0, 0.0, 1.0]), 0), (np.array([0.0, 0.0, -1.0]), 0)]
+        return out
+
+    def height_profile(self, up: np.ndarray, lo: float, n_bins: int, bin_m: float):
+        """Histogram of the heights (along up, from the sensor) of the scan's horizontal points (localize.py:308-313)."""
+        horiz = np.abs(self.normals @ up) > 0.97
+        z = self.pts[horiz] @ up
+        h, _ = np.histogram(z, bins=n_bins, range=(lo, lo + n_bins * bin_m))
+        return h.astype(np.float32)
 
 
 def thin_5cm(xyz: np.ndarray) -> np.ndarray:
@@ -272,6 +407,15 @@ class GlobalLocalizer:
     tau_mid = 12.0
     free_cm = 10.0  # the sensor sits at least this far from any mapped surface
     keep_coarse = 128  # coarse local maxima re-scored on the finer grid (localize.py:367)
+    n_heights = 8  # sensor heights tried per gravity candidate (localize.py:358)
+    n_coarse_pts = 1024
+    n_mid_pts = 2048
+    n_icp = ICP_CAP  # medium winners refined by ICP per gravity candidate (localize.py:368)
+    # unique: inliers (3 cm) at least accept_inliers, and the best answer elsewhere at least accept_gap lower and
+    # below accept_ratio of it (localize.py:369-373)
+    accept_inliers = 0.45
+    accept_gap = 0.15
+    accept_ratio = 0.75
 
     def __init__(self, grid: PriorGrid, device=None, hyp_cap: int = 1024, pts_cap: int = 1 << 23,
                  tuner: Autotuner | None = None):
@@ -337,6 +481,181 @@ class GlobalLocalizer:
         self.last_candidates = k  # local maxima found (and copied to the host) by the last call
         order = np.lexsort((bi, -bv))[:keep]
         return pos, shape, dyaw, bi[order], bv[order]
+
+    # ---- the global search (localize.py:400-424, 476-505, 616-738) -----------------------------------------------
+
+    def _heights(self, prep: ScanPrep, up: np.ndarray):
+        """Sensor heights where the scan's horizontal surfaces line up with the map's, best first: the correlation
+        of the two height profiles (square-rooted, smoothed by +-2 bins) over every shift inside the map's z range,
+        peaks at least 8 cm apart (localize.py:400-424)."""
+        h_map, lo, bin_m = self.grid.levels
+        span = 6.0  # scan heights within +-6 m of the sensor
+        nb = int(round(2 * span / bin_m))
+        h_scan = prep.height_profile(up, -span, nb, bin_m)
+        if h_scan.sum() < 50:
+            return None
+        k = np.array([0.25, 0.5, 1.0, 0.5, 0.25], np.float32)
+        hm = np.convolve(np.sqrt(h_map), k, mode="same")
+        hs = np.convolve(np.sqrt(h_scan), k, mode="same")
+        corr = np.correlate(hm, hs, mode="full")  # corr[j]: a shift of j - (nb - 1) bins
+        shifts = np.arange(len(corr)) - (nb - 1)
+        z_sensor = lo + shifts * bin_m + span
+        ok = (z_sensor >= self.grid.lo[2] - 0.5) & (z_sensor <= self.grid.hi[2] + 0.5)
+        corr = np.where(ok, corr, -1.0)
+        out = []
+        for i in np.argsort(-corr):
+            if corr[i] <= 0 or len(out) >= self.n_heights:
+                break
+            z = float(z_sensor[i])
+            if all(abs(z - o) > 0.08 for o in out):
+                out.append(z)
+        return out
+
+    @staticmethod
+    def _top(scores: np.ndarray, pool: int = 20000) -> np.ndarray:
+        """Indices of the `pool` best scores, best first (localize.py:477-482)."""
+        pool = min(pool, len(scores))
+        idx = np.argpartition(-scores, pool - 1)[:pool] if pool < len(scores) else np.arange(len(scores))
+        return idx[np.argsort(-scores[idx])]
+
+    @staticmethod
+    def _nms(hyps: np.ndarray, scores: np.ndarray, keep: int, dist: float, ang_deg: float) -> np.ndarray:
+        """Greedy non-maximum suppression over (x, y, z, yaw) hypotheses: the survivors' indices, best first
+        (localize.py:484-505)."""
+        chosen = []
+        ang = math.radians(ang_deg)
+        for i in GlobalLocalizer._top(scores):
+            if scores[i] <= 0:
+                break
+            h = hyps[i]
+            ok = True
+            for j in chosen:
+                o = hyps[j]
+                dyaw = abs((h[3] - o[3] + math.pi) % (2 * math.pi) - math.pi)
+                if np.linalg.norm(h[:3] - o[:3]) < dist and dyaw < ang:
+                    ok = False
+                    break
+            if ok:
+                chosen.append(i)
+                if len(chosen) >= keep:
+                    break
+        return np.array(chosen, dtype=np.int64)
+
+    def _unique(self, best: float, alt: float) -> bool:
+        return best >= self.accept_inliers and best - alt >= self.accept_gap and alt <= self.accept_ratio * best
+
+    @staticmethod
+    def _runner_up(results) -> float:
+        """The best 3 cm fit of a result more than 1 m or 15 degrees from the winner's pose (localize.py:733-738)."""
+        best = results[0][3]
+        for r in results[1:]:
+            dt, ang = pose_difference(best, r[3])
+            if dt > 1.0 or ang > 15.0:
+                return r[0]
+        return 0.0
+
+    def localize(self, xyz: np.ndarray, stream=None, up_prior: np.ndarray | None = None, log=print, progress=None,
+                 prep: ScanPrep | None = None):
+        """Sensor-to-map pose (4x4) of a scan given in the sensor frame, plus diagnostics (localize.py:616-728):
+        the gravity candidates of the scan's horizontal planes; per candidate the sensor heights where the scan's
+        and the map's horizontal surfaces line up, the coarse search over every free position x heading with its
+        local maxima (on the device), a finer local grid around each scored with more points and a tighter
+        tolerance, non-maximum suppression, then the batched ICP and the evaluation of the survivors; the search
+        stops early once an answer is good and unique. up_prior (gravity "up" in the sensor frame) only orders
+        the candidates; progress(text) is called between stages; prep may supply a prepared scan."""
+        import time
+
+        t0 = time.perf_counter()
+        say = progress or (lambda s: None)
+        tm = {}
+        rng = np.random.default_rng(self.seed)  # the same scan always gives the same answer
+        prep = prep if prep is not None else ScanPrep(xyz)
+        pts = prep.pts
+        if len(pts) > self.PTS_CAP:
+            pts = pts[rng.choice(len(pts), self.PTS_CAP, replace=False)]
+        n_pts = len(pts)
+        if n_pts < 200:
+            raise RuntimeError(f"scan too sparse to localise ({n_pts} points after 5 cm thinning)")
+        pts32 = pts.astype(np.float32)
+        # coarse / medium subsets: spread evenly over the scan (one per 15 cm voxel first)
+        _, first = np.unique(np.floor(pts / 0.15).astype(np.int64), axis=0, return_index=True)
+        spread = pts[first]
+        sub_c = spread[rng.choice(len(spread), min(self.n_coarse_pts, len(spread)), replace=False)]
+        sub_m = pts[rng.choice(n_pts, min(self.n_mid_pts, n_pts), replace=False)]
+        ups = prep.up_candidates()
+        if up_prior is not None:
+            upp = np.asarray(up_prior, float) / np.linalg.norm(up_prior)
+            ups.sort(key=lambda u: -float(u[0] @ upp))
+        tm["prep"] = time.perf_counter() - t0
+        cands = []
+        t1 = time.perf_counter()
+        n_hyp_total = 0
+        for up, support in ups:
+            say(f"coarse search, up {np.round(up, 2)}")
+            Rg = rot_to(up, np.array([0.0, 0.0, 1.0]))  # sensor -> gravity-aligned sensor frame
+            heights = self._heights(prep, up)
+            if not heights:
+                heights = list(np.arange(self.grid.lo[2], self.grid.hi[2] + 1e-6, self.xy_step))
+            pc = sub_c @ Rg.T
+            pos, shape, dyaw, best, best_sc = self._coarse_candidates(stream, pc, heights, keep=self.keep_coarse)
+            n_yaw = shape[3]
+            n_hyp_total += len(pos) * n_yaw
+            hyps = np.concatenate([pos[best // n_yaw], ((best % n_yaw) * dyaw)[:, None]], 1)
+            cands.append({"up": up, "Rg": Rg, "heights": heights, "coarse": hyps, "coarse_score": best_sc,
+                          "best_coarse": float(best_sc[0]) / len(pc) if len(best) else 0.0, "support": support})
+        tm["coarse"] = time.perf_counter() - t1
+        cands.sort(key=lambda c: -c["best_coarse"])
+        results = []  # (inliers3, inliers5, inliers10, T, candidate index, medium score)
+        tm["mid"] = tm["icp"] = 0.0
+        refined = 0
+        for ci, c in enumerate(cands):
+            if not len(c["coarse"]):
+                continue
+            say(f"refining gravity candidate {ci + 1}/{len(cands)}")
+            tm_a = time.perf_counter()
+            Rg = c["Rg"]
+            pm = sub_m @ Rg.T
+            # +-1 coarse step: two modes a step apart share one coarse local maximum, the window must reach both
+            off = np.arange(-self.xy_step, self.xy_step + 1e-6, self.xy_step / 4)
+            offz = np.array([-0.04, 0.0, 0.04])
+            offy = np.radians(np.arange(-self.yaw_step_deg, self.yaw_step_deg + 1e-6, 0.5))
+            A, B, Cz, D = np.meshgrid(off, off, offz, offy, indexing="ij")
+            local = np.stack([A.ravel(), B.ravel(), Cz.ravel(), D.ravel()], 1)
+            hyps = (c["coarse"][:, None, :] + local[None, :, :]).reshape(-1, 4)
+            ms = self._score_list(stream, pm.astype(np.float32), len(pm), hyps, self.tau_mid)
+            best = self._nms(hyps, ms, self.n_icp, 0.1, 1.5)
+            tm["mid"] += time.perf_counter() - tm_a
+            tm_b = time.perf_counter()
+            Ts = []
+            for i in best:
+                x, y, z, yaw = hyps[i]
+                T = np.eye(4)
+                T[:3, :3] = rotz(yaw) @ Rg
+                T[:3, 3] = (x, y, z)
+                Ts.append(T)
+            Ts = self.icp(pts32, Ts, stream=stream)
+            fr = self.evaluate(pts32, Ts, stream=stream)
+            for j, i in enumerate(best):
+                results.append((float(fr[j, 0]), float(fr[j, 1]), float(fr[j, 2]), Ts[j], ci, float(ms[i]) / len(pm)))
+            tm["icp"] += time.perf_counter() - tm_b
+            refined += 1
+            results.sort(key=lambda r: -r[0])
+            if self._unique(results[0][0], self._runner_up(results)):
+                break  # this candidate's best answer is good and unique
+        results.sort(key=lambda r: -r[0])
+        if not results:
+            raise RuntimeError("no hypothesis survived (is the scan inside the map?)")
+        top = results[0]
+        alt = self._runner_up(results)
+        tm["total"] = time.perf_counter() - t0
+        info = {"inliers": top[0], "inliers5": top[1], "inliers10": top[2], "runner_up": alt,
+                "unique": self._unique(top[0], alt), "up": cands[top[4]]["up"], "heights": cands[top[4]]["heights"],
+                "gravity_candidates": len(cands), "refined_candidates": refined, "hypotheses": n_hyp_total,
+                "scan_points": n_pts, "times": tm}
+        log(f"  {tm['total']:.2f} s (prep {tm['prep']:.2f}, coarse {tm['coarse']:.2f} for {n_hyp_total / 1e6:.1f}M "
+            f"hypotheses, medium {tm['mid']:.2f}, ICP {tm['icp']:.2f}; {refined}/{len(cands)} gravity candidates "
+            f"refined): inliers {top[0]:.3f} within 3 cm (runner-up elsewhere {alt:.3f})")
+        return np.asarray(top[3]), info
 
     def _score_list(self, stream, pts, m: int, hyps: np.ndarray, tau: float) -> np.ndarray:
         """The soft counts of (x, y, z, yaw) hypotheses for the first m points of `pts` (localize.py:507-515)."""
@@ -553,3 +872,27 @@ class GlobalLocalizer:
             return BatchResult(T, ev / n_h[:, None], count, iters, tile, blocks_per_sm)
 
         return replay
+
+
+class Localizer:
+    """Single-threaded convenience wrapper (localize.py:739-763): builds the prior grid and searches on one
+    stream."""
+
+    def __init__(self, map_xyz: np.ndarray, map_normal: np.ndarray, map_planarity: np.ndarray | None = None,
+                 device=None, stream=None):
+        host = {"xyz": map_xyz, "normal": map_normal}
+        if map_planarity is not None:
+            host["planarity"] = map_planarity
+        self.grid = PriorGrid(host, device)
+        self.stream = stream
+        self.grid.build(stream)
+        self.loc = GlobalLocalizer(self.grid, self.grid.device)
+
+    def search(self, xyz: np.ndarray, log=print, up_prior=None):
+        """GlobalLocalizer.localize on this stream: the pose of a sensor-frame scan, and diagnostics."""
+        return self.loc.localize(xyz, self.stream, up_prior=up_prior, log=log)
+
+    def refine(self, xyz: np.ndarray, T0: np.ndarray, **kw):
+        """GlobalLocalizer.refine on this stream: ICP of a point set from the known pose T0."""
+        return self.loc.refine(xyz, T0, self.stream, **kw)
+

@@ -20,6 +20,9 @@ device solve:
                     tracks after every update.
   local_maxima.npz  localize.py GlobalLocalizer._local_maxima and _top (the two methods, taken out of the class)
                     on seeded coarse-score arrays with ties, occupied positions and several pool sizes.
+  localize_host.npz localize.py _rot_to, ScanPrep.up_candidates / height_profile, GlobalLocalizer._heights, _nms,
+                    _top, _runner_up and _unique on seeded inputs (scans with known planes, a map's levels,
+                    clustered hypotheses with ties, result lists).
   prior_prepare.npz mapgrid.py PriorGrid.prepare (a static method, taken out of its class) with
                     horizontal_levels and the module constants it reads (CELL, IDX_BITS, MAX_POINTS, PLANAR; the
                     one Warp call among them, wp.constant, is the identity here).
@@ -388,8 +391,102 @@ def local_maxima(ref: Path) -> dict:
     return out
 
 
+def localize_host(ref: Path) -> dict:
+    """The global search's host stages from localize.py, run from source on seeded inputs: _rot_to; ScanPrep's
+    up_candidates and height_profile on scans with known planes (the methods taken out of the class, the open3d
+    preparation replaced by the planes given); GlobalLocalizer._heights against a map's horizontal levels, _nms
+    with _top, _runner_up and _unique."""
+    src = ref / "python" / "livox_warp" / "localize.py"
+    ns = extract(src, ["_rot_to", "_rotz", "pose_difference"])
+    Prep = extract_methods(src, "ScanPrep", ["up_candidates", "height_profile"])
+    Loc = extract_methods(src, "GlobalLocalizer", ["_heights", "_nms", "_top", "_runner_up", "_unique"])
+    for name in ("pose_difference",):
+        setattr(Loc, name, staticmethod(ns[name]))
+    ns_loc = Loc._runner_up.__globals__
+    ns_loc.update({"pose_difference": ns["pose_difference"], "GlobalLocalizer": Loc})
+    rng = np.random.default_rng(20261206)
+    out = {}
+    # _rot_to: random pairs, a parallel and an antiparallel one
+    a = rng.normal(0, 1, (24, 3))
+    b = rng.normal(0, 1, (24, 3))
+    b[0], b[1] = 2 * a[0], -3 * a[1]
+    out["rot_a"], out["rot_b"] = a, b
+    out["rot_out"] = np.stack([ns["_rot_to"](a[i], b[i]) for i in range(len(a))])
+    # ScanPrep: a tilted floor, a ceiling, two walls and a second floor level, with the planes as open3d would
+    # return them (count, unit normal, offset, indices)
+    for k, tilt in enumerate((0.0, 12.0, 170.0)):
+        R = Rotation.from_rotvec(np.radians(tilt) * np.array([1.0, 0.4, 0.0]) / np.linalg.norm([1.0, 0.4, 0.0]))
+        R = R.as_matrix()
+        parts, normals, planes, start = [], [], [], 0
+        for n_w, off, cnt in (((0, 0, 1), -1.4, 900), ((0, 0, -1), 2.5, 600), ((1, 0, 0), 3.0, 700),
+                              ((0, 1, 0), -2.0, 500), ((0, 0, 1), -0.6, 300), ((0.02, 0, 1), -1.38, 200)):
+            n_w = np.asarray(n_w, float) / np.linalg.norm(n_w)
+            u = np.cross(n_w, [0.3, 0.5, 0.7])
+            u /= np.linalg.norm(u)
+            v = np.cross(n_w, u)
+            P = (-off) * n_w + rng.uniform(-3, 3, (cnt, 1)) * u + rng.uniform(-3, 3, (cnt, 1)) * v
+            P = P + rng.normal(0, 0.005, P.shape)
+            P = P @ R.T
+            n_s = R @ n_w
+            parts.append(P)
+            normals.append(np.tile(n_s, (cnt, 1)) * rng.choice([-1, 1], (cnt, 1)))
+            planes.append((cnt, n_s, float(off), np.arange(start, start + cnt)))
+            start += cnt
+        prep = Prep()
+        prep.pts = np.concatenate(parts)
+        prep.normals = np.concatenate(normals)
+        prep.planes = planes
+        prep.max_tilt = 45.0
+        ups = prep.up_candidates()
+        out[f"prep{k}_pts"], out[f"prep{k}_normals"] = prep.pts, prep.normals
+        out[f"prep{k}_plane_n"] = np.array([p[1] for p in planes])
+        out[f"prep{k}_plane_cnt"] = np.array([p[0] for p in planes], np.int64)
+        out[f"prep{k}_plane_off"] = np.array([p[2] for p in planes])
+        out[f"prep{k}_ups"] = np.array([u[0] for u in ups])
+        out[f"prep{k}_support"] = np.array([u[1] for u in ups], np.int64)
+        out[f"prep{k}_hprof"] = prep.height_profile(ups[0][0], -6.0, 600, 0.02)
+        # _heights against a map whose horizontal levels are the scan's, lifted by 1.5 m
+        lvl, _ = np.histogram(np.concatenate([np.full(900, 0.0), np.full(600, 3.9), np.full(300, 0.8)]),
+                              bins=300, range=(-1.0, 5.0))
+
+        class Grid:
+            levels = (lvl.astype(np.float32), -1.0, 0.02)
+            lo = np.array([0.0, 0.0, -0.2])
+            hi = np.array([20.0, 10.0, 4.0])
+
+        loc = Loc()
+        loc.grid, loc.n_heights = Grid, 8
+        hs = loc._heights(prep, ups[0][0])
+        out[f"prep{k}_heights"] = np.array(hs if hs else [], np.float64)
+    # _nms with _top: clustered hypotheses, ties, non-positive scores
+    hyps = np.concatenate([rng.normal([2, 3, 1.2, 0.5], [0.08, 0.08, 0.02, 0.02], (300, 4)),
+                           rng.normal([6, 1, 1.2, 2.5], [0.3, 0.3, 0.05, 0.05], (300, 4))])
+    sc = np.round(rng.uniform(-5, 100, len(hyps)))
+    out["nms_hyps"], out["nms_scores"] = hyps, sc
+    for j, (keep, dist, ang) in enumerate(((16, 0.1, 1.5), (5, 0.3, 10.0), (100, 0.05, 0.5))):
+        out[f"nms{j}"] = np.asarray(Loc._nms(hyps, sc, keep, dist, ang), np.int64)
+        out[f"nms{j}_args"] = np.array([keep, dist, ang])
+    # _runner_up and _unique
+    poses = []
+    for i in range(12):
+        T = np.eye(4)
+        T[:3, :3] = ns["_rotz"](rng.uniform(-0.4, 0.4) * (i % 3))
+        T[:3, 3] = rng.normal(0, 0.8 * (i % 4), 3)
+        poses.append(T)
+    fits = np.sort(rng.uniform(0.2, 0.9, 12))[::-1]
+    results = [(float(fits[i]), 0.0, 0.0, poses[i], 0, 0.0) for i in range(12)]
+    out["ru_poses"], out["ru_fits"] = np.stack(poses), fits
+    loc = Loc()
+    loc.accept_inliers, loc.accept_gap, loc.accept_ratio = 0.45, 0.15, 0.75
+    out["ru_out"] = np.array([Loc._runner_up(results[i:]) for i in range(11)])
+    pairs = rng.uniform(0, 1, (40, 2))
+    out["uq_pairs"] = pairs
+    out["uq_out"] = np.array([loc._unique(float(p), float(q)) for p, q in pairs])
+    return out
+
+
 FIXTURES = {"host_solve": host_solve, "prior_prepare": prior_prepare, "lvxr": lvxr, "tracker": tracker,
-            "local_maxima": local_maxima}
+            "local_maxima": local_maxima, "localize_host": localize_host}
 
 
 def main():
