@@ -135,3 +135,32 @@ def test_localize_end_to_end_with_the_oracle_for_the_device_stages():
     dt, dr = pose_difference(T_true, T)
     assert dt < 0.02 and dr < 0.3, (dt, dr, info["inliers"], info["runner_up"])
     assert info["unique"] and info["inliers"] > 0.8 and abs(info["up"][2]) > 0.99
+
+
+def test_scan_prep_voxel_means_and_ransac_plane():
+    """The two steps ScanPrep restates from open3d: voxel means on a grid anchored at the points' minimum (each
+    voxel's float64 mean, in the order of its first point), and a seeded RANSAC plane that finds a noisy plane
+    among outliers and returns its least-squares refit and inliers; the same seed gives the same plane."""
+    from livox_warp.localize import ransac_plane, voxel_means
+
+    rng = np.random.default_rng(3)
+    p = rng.uniform(-1, 1, (5000, 3))
+    m = voxel_means(p, 0.25)
+    k = np.floor((p - p.min(0)) / 0.25).astype(np.int64)
+    _, first, inv = np.unique(k, axis=0, return_index=True, return_inverse=True)
+    order = np.argsort(first, kind="stable")
+    want = np.stack([p[inv.reshape(-1) == v].mean(0) for v in order])
+    assert np.allclose(m, want, rtol=0, atol=1e-12)
+    n = np.array([0.2, -0.1, 1.0]) / np.linalg.norm([0.2, -0.1, 1.0])
+    u = np.cross(n, [1.0, 0.0, 0.0])
+    u /= np.linalg.norm(u)
+    v = np.cross(n, u)
+    plane = 0.7 * n + rng.uniform(-2, 2, (3000, 1)) * u + rng.uniform(-2, 2, (3000, 1)) * v
+    plane += rng.normal(0, 0.005, plane.shape) * n
+    pts = np.concatenate([plane, rng.uniform(-2, 2, (1500, 3))])
+    model, inl = ransac_plane(pts, 0.03, 1000, np.random.default_rng(0))
+    assert abs(abs(model[:3] @ n) - 1.0) < 1e-4 and abs(abs(model[3]) - 0.7) < 2e-3
+    # nearly every plane point, and only the few outliers inside the 3 cm slab (about 1.5 % of 1500)
+    assert len(np.intersect1d(inl, np.arange(3000))) > 2990 and len(inl) < 3100
+    again, inl2 = ransac_plane(pts, 0.03, 1000, np.random.default_rng(0))
+    assert np.array_equal(model, again) and np.array_equal(inl, inl2)
