@@ -26,6 +26,10 @@ device solve:
   prior_prepare.npz mapgrid.py PriorGrid.prepare (a static method, taken out of its class) with
                     horizontal_levels and the module constants it reads (CELL, IDX_BITS, MAX_POINTS, PLANAR; the
                     one Warp call among them, wp.constant, is the identity here).
+  ref_odom.npz, ref_map.npz, ref_perception.npz, ref_localize.npz
+                    the reference's Warp kernels themselves (odom.py, gpu.py, perception.py, mapgrid.py,
+                    localize.py), imported unchanged against a serial stand-in for Warp (warp_shim.py) and run on
+                    small seeded inputs; kernel_fixtures.py lists the kernels and how each is driven.
 """
 
 from __future__ import annotations
@@ -487,10 +491,16 @@ def localize_host(ref: Path) -> dict:
 
 FIXTURES = {"host_solve": host_solve, "prior_prepare": prior_prepare, "lvxr": lvxr, "tracker": tracker,
             "local_maxima": local_maxima, "localize_host": localize_host}
+sys.path.insert(0, str(HERE))
+import kernel_fixtures  # noqa: E402 - beside this script
+
+FIXTURES.update(kernel_fixtures.FIXTURES)
 
 
 def main():
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py <reference checkout> [fixture ...]")
+    ref = Path(sys.argv[1])
     for name in sys.argv[2:] or list(FIXTURES):  # optionally only the named fixtures
         np.savez_compressed(HERE / f"{name}.npz", **FIXTURES[name](ref))
         print("wrote", HERE / f"{name}.npz")
