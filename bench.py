@@ -331,6 +331,8 @@ def pose_drift(odom, traj, oracle_poses: dict) -> dict:
 # rounded as summarised there) and of the coarse search (profiles/k_score_grid_office_coarse.md)
 SEQ_TRAFFIC = {"gn": 1_943_000, "carve": 6_928_000}  # carve: both passes (setup + walk)
 SEQ_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_gn_k_carve_sequence.md"
+SINGLE_TRAFFIC: dict = {}  # filled from an ncu capture of the single-frame case
+SINGLE_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_gn_single_frame.md"
 COARSE_TRAFFIC = 42_780_928 + 71_592_448
 COARSE_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_score_grid_office_coarse.md"
 
@@ -711,6 +713,214 @@ def run_frame(a, rank: int, world: int, local: int):
             "e2e": {"value": round(float(np.percentile(lh, 50)), 4), "unit": "ms",
                     "h2d_bytes_per_step": int(h2d / a.steps), "d2h_bytes_per_step": int(d2h / a.steps)},
             "gpu_launches": int(launches), "clocks": clk}
+    print(json.dumps(line))
+
+
+# ---- single-frame scan-to-map ICP (the headline configuration) --------------------------------------------------
+
+SINGLE_VOXEL = 0.2    # registration voxel of the single-frame case
+SINGLE_ITERS = 10     # Gauss-Newton iterations at most
+SINGLE_FRAMES = 8     # distinct seeded frames, cycled over the timed steps
+SINGLE_REG_SLOTS = 1 << 21  # the reference's default registration table (odom.py:461)
+
+
+def single_workload():
+    from livox_warp import synth
+
+    return synth.single_frame_case(synth.box_room(ROOM_SEED), SINGLE_FRAMES, RATE)
+
+
+def _single_oracle_params(_o):
+    return _o.Params(reg_voxel=SINGLE_VOXEL, max_iter=SINGLE_ITERS)
+
+
+def single_oracle(w, threads: int, budget_s: float, max_frames: int):
+    """The float64 oracle on the single-frame case: the map of the static frames, then deskew + thinning +
+    registration of moving frames in turn (cycling) until budget_s of CPU time or max_frames. Returns (frames
+    timed, seconds, {j: T} for every distinct frame registered, {j: stats})."""
+    os.environ["LW_ORACLE_THREADS"] = str(threads)
+    from oracle import oracle as _o
+
+    T0, base, moving = w
+    oreg = _o.RegMap(SINGLE_REG_SLOTS)
+    for x, a, t in base:
+        oreg.insert(np.ascontiguousarray(np.concatenate([x, t[:, None]], 1), dtype=np.float32), a, T0, SINGLE_VOXEL,
+                    60.0, 0b1111)
+    oreg.records(SINGLE_VOXEL, 0.02, 0.05)
+    p = _single_oracle_params(_o)
+    timed, secs, poses, stats = 0, 0.0, {}, {}
+    while timed < max_frames and (secs < budget_s or len(poses) < len(moving)):
+        j = timed % len(moving)
+        x, a, t, t_mid, _ = moving[j]
+        t0 = time.perf_counter()
+        raw = np.ascontiguousarray(np.concatenate([x, t[:, None]], 1), dtype=np.float32)
+        d = _o.deskew(raw, t_mid, 1.0 / FRAME_DT, np.zeros(6, np.float32))
+        ds = _o.thin(d, a, np.float32(2.0 / SINGLE_VOXEL), p.min_range, p.max_range, p.ret_mask)
+        T, ok, st = _o.register(ds, T0, oreg, p, nthreads=threads)
+        secs += time.perf_counter() - t0
+        timed += 1
+        poses[j], stats[j] = T, st
+    return timed, secs, poses, stats
+
+
+def run_single(a, rank: int, world: int, local: int):
+    w = single_workload()  # before any CUDA call
+    T0, base, moving = w
+    pts = int(np.mean([len(f[2]) for f in moving]))
+    metric = "single-frame scan-to-map ICP frames/s (deskew + thinning + <=10 Gauss-Newton iterations, f64 solve)"
+    config = {"workload": "single-frame scan-to-map ICP: box room 8x6x3 m, 20 boxes, rosette 100k pts/s "
+                          f"(~{pts} pts/frame), map of {len(base)} static frames at 0.2 m voxels (2^21 slots), "
+                          "sensor 0.5 m/s + 20 deg/s, constant-velocity start (the rest pose and zero twist of a "
+                          f"sensor that just started moving), <= {SINGLE_ITERS} Gauss-Newton iterations; "
+                          f"{len(moving)} seeded frames cycled",
+              "points_per_frame": pts, "frames_distinct": len(moving),
+              "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{a.gpus}"}
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import oracle as _o
+
+        threads = _o.host_cores()
+        single_oracle(w, threads, 0.0, a.warmup)  # untimed warm-up registrations
+        timed, secs, _, _ = single_oracle(w, threads, 15.0, 1 << 30)
+        v = timed / secs
+        print(json.dumps({"impl": "reference", "metric": metric, "value": round(v, 3), "unit": "frames/s",
+                          "n_gpus": a.gpus, "steps": timed, "warmup": a.warmup,
+                          "ms_per_step": round(1e3 * secs / max(timed, 1), 3), "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+                          "config": config,
+                          "cpu_baseline": {"value": round(v, 3), "unit": "frames/s", "cores": threads, "kind": "port",
+                                           "sample": f"{timed} registrations of the same frames; NVIDIA Warp (the "
+                                                     "reference runtime) is not installed, so this is the CPU "
+                                                     "restatement of its kernels (C++/OpenMP) with the float64 "
+                                                     "host solve"},
+                          "e2e": {"value": round(v, 3), "unit": "frames/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+    import torch
+    import torch.distributed as dist
+
+    from livox_warp import _lib, gpu
+    from livox_warp.odom import Odometry
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+    pipe = gpu.Pipeline(ring_capacity=1 << 16, map_capacity=1 << 16, device=device)
+    odom = Odometry(pipe, reg_slots=SINGLE_REG_SLOTS, frame_cap=1 << 15)
+    odom.reg_voxel, odom.max_iter = SINGLE_VOXEL, SINGLE_ITERS
+    odom.reset(T0)
+    for x, at, t in base:
+        x4 = torch.from_numpy(np.ascontiguousarray(np.concatenate([x, t[:, None]], 1), dtype=np.float32)).to(device)
+        odom.insert_frame(x4, torch.from_numpy(at.view(np.int32)).to(device), T0)
+    dev = [(torch.from_numpy(np.ascontiguousarray(np.concatenate([x, t[:, None]], 1), dtype=np.float32)).to(device),
+            torch.from_numpy(at.view(np.int32)).to(device), t_mid) for x, at, t, t_mid, _ in moving]
+    zero = np.zeros(6, np.float32)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream(device)
+
+    def step(k):
+        x4, at, t_mid = dev[k % len(dev)]
+        odom.register_frame(x4, at, None, t_mid, zero, T0, sync=False)
+
+    for k in range(a.warmup):
+        step(k)
+    torch.cuda.synchronize(device)
+    if world > 1:
+        dist.barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    clocks = Clocks(local)
+    _lib.prof_reset()
+    _lib.prof_enable(True)
+    _lib.launches(reset=True)
+    clocks.start()
+    torch.cuda.synchronize(device)
+    for j in range(a.steps):
+        flush.fill_(float(j))  # L2 flush, outside the step's events
+        evs[j][0].record(stream)
+        step(a.warmup + j)
+        evs[j][1].record(stream)
+    torch.cuda.synchronize(device)
+    clk = clocks.stop()
+    launches = _lib.launches()
+    _lib.prof_enable(False)
+    step_ms = np.array([e0.elapsed_time(e1) for e0, e1 in evs])
+    gn_ms, gn_cnt = _lib.prof_read("gn")
+    ms_total = max_over_ranks(float(step_ms.sum()), device)
+    value = replica_rate(a.steps, world, ms_total)
+    # every distinct frame once more, with its result read back: the poses the oracle checks
+    res = []
+    for j in range(len(dev)):
+        step(j)
+        res.append(odom.registration())
+    # end to end through the public API: host arrays staged (pinned H2D) and the result read back every step
+    for k in range(a.warmup):
+        x, at, t, t_mid, _ = moving[k % len(moving)]
+        odom.register_frame(x, at, t, t_mid, zero, T0)
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for j in range(a.steps):
+        x, at, t, t_mid, _ = moving[(a.warmup + j) % len(moving)]
+        odom.register_frame(x, at, t, t_mid, zero, T0)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    e_ms = max_over_ranks(e0.elapsed_time(e1), device)
+    import ctypes as _ct
+
+    e2e = {"value": round(replica_rate(a.steps, world, e_ms), 3), "unit": "frames/s",
+           "h2d_bytes_per_step": pts * 20, "d2h_bytes_per_step": _ct.sizeof(_lib.OdomState)}
+    reg_keys = odom.reg_keys.cpu().numpy()
+    reg_keys = reg_keys[reg_keys != -1]
+    grid = odom._gn.grid
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    from livox_warp import roofline as rl
+    from oracle import oracle as _o
+
+    threads = _o.host_cores()
+    timed, secs, opose, ostats = single_oracle(w, threads, min(a.cpu_budget, 15.0), 1 << 30)
+    err = np.array([_o.pose_error(opose[j], res[j][0]) for j in range(len(moving))])
+    gt = np.array([_o.pose_error(moving[j][4], res[j][0]) for j in range(len(moving))])
+    iters = np.array([res[j][2]["iters"] for j in range(len(moving))])
+    per_launch = []
+    for j, (x, at, t, t_mid, _) in enumerate(moving):
+        ds = rl.thin_host(x, SINGLE_VOXEL)
+        per_launch.append(rl.gn_bytes(ds, res[j][0], reg_keys, SINGLE_VOXEL, max(int(iters[j]), 1), grid))
+    avg_ms = gn_ms / max(gn_cnt, 1)
+    achieved = float(np.mean(per_launch)) / (avg_ms * 1e-3) / 1e9
+    peak = measured_peak()
+    traffic = SINGLE_TRAFFIC.get("gn")
+    roof = {"kernel": "gn", "bound": "hbm", "achieved": round(achieved, 3), "peak": peak["hbm_gbs"], "unit": "GB/s",
+            "frac": round(achieved / peak["hbm_gbs"], 5), "traffic": traffic,
+            "traffic_source": SINGLE_TRAFFIC_SRC if traffic else None, "peak_source": peak["source"],
+            "avg_launch_us": round(avg_ms * 1e3, 2), "launches": int(gn_cnt),
+            "algorithmic_bytes_per_launch": int(np.mean(per_launch)),
+            "kernel_ms_share": {"gn": round(gn_ms / max(float(step_ms.sum()), 1e-9), 4)}}
+    line = {"metric": metric, "value": round(value, 3), "unit": "frames/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms_total / a.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 solve)", "data": "synthetic",
+            "config": config, "points_per_s": round(value * pts, 1),
+            "step_ms_p50_p99": [round(float(np.percentile(step_ms, 50)), 4),
+                                round(float(np.percentile(step_ms, 99)), 4)],
+            "pose_error_vs_fp64": {"frames": len(moving), "max_m": round(float(err[:, 0].max()), 7),
+                                   "max_deg": round(float(err[:, 1].max()), 6),
+                                   "bound": "1 mm / 0.01 deg", "within_bound": bool((err[:, 0] <= 1e-3).all() and
+                                                                                   (err[:, 1] <= 0.01).all())},
+            "pose_error_vs_truth": {"max_m": round(float(gt[:, 0].max()), 5), "max_deg": round(float(gt[:, 1].max()), 4)},
+            "gn_iterations": {"mean": round(float(iters.mean()), 2),
+                              "oracle_mean": round(float(np.mean([ostats[j]["iters"] for j in ostats])), 2)},
+            "roofline": roof,
+            "cpu_baseline": {"value": round(timed / secs, 3), "unit": "frames/s", "cores": threads, "kind": "port",
+                             "sample": f"{timed} registrations of the same frames through the CPU oracle (C++/OpenMP "
+                                       f"accumulation, numpy float64 solve), {secs:.1f} s"},
+            "e2e": e2e, "gpu_launches": int(launches), "clocks": clk}
     print(json.dumps(line))
 
 
@@ -1264,8 +1474,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=("sequence", "localize", "frame", "learned", "coarse", "prior"),
-                    default="sequence")
+    ap.add_argument("--workload", choices=("single", "sequence", "localize", "frame", "learned", "coarse", "prior"),
+                    default="single")
     ap.add_argument("--learn-epochs", type=int, default=40, help="learned: training epochs")
     ap.add_argument("--loc-hyp", type=int, default=256, help="localize: hypotheses (a smaller profiling case)")
     ap.add_argument("--loc-spacing", type=float, default=0.015, help="localize: prior-map sample spacing (m)")
@@ -1276,6 +1486,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.workload == "single":
+        run_single(a, rank, world, local)
+        return
     if a.workload == "localize":
         run_localize(a, rank, world, local)
         return

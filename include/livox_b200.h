@@ -149,9 +149,12 @@ typedef struct lw_frame_buf {
 /* Scratch of the persistent Gauss-Newton kernel. */
 typedef struct lw_gn_scratch {
     double* part;      /* [2 * grid * LW_ACC_STRIDE] per-CTA partial accumulators, double buffered */
-    uint32_t* bar;     /* [2] grid barrier counter and generation; zero before the first use */
-    int32_t* err;      /* [1] set when a bounded wait gives up */
+    uint32_t* bar;     /* [2] grid barrier counter and generation; zeroed by every launch */
+    int32_t* err;      /* [1] set when a bounded wait gives up (1) or a fixed-point sum overflows (4); sticky */
     int32_t grid;      /* CTAs (<= the SM count, one per SM) */
+    int32_t spin_budget; /* barrier wait limit in ~100 ns sleeps; 0 = the default (~2 s) */
+    int32_t skip_cta;  /* failure injection for tests of the bounded wait: this CTA leaves before the first
+                          barrier, so the others time out and the launch reports err = 1; -1 = none */
 } lw_gn_scratch;
 
 /* Pose table of the Pipeline (gpu.py:1196-1206); written on the device by the odometry. */
@@ -211,7 +214,9 @@ int lw_thin(lw_frame_buf* fb, const int32_t* m_dev, int64_t m_ub, double inv_v, 
  * points per call: more is rejected with LW_ECAPACITY before any work is queued. The first call on a device
  * looks up the array's device address (cudaGetSymbolAddress) with that device current; make that first call
  * before any stream capture. It allocates nothing. Calls share the one array and each clears its tables
- * first, so calls that overlap on the GPU (two streams at once) race: serialise them. */
+ * first, so calls that overlap on the GPU (two streams at once) race: serialise them. xyz4 and ds4_out must
+ * be 16-byte aligned (LW_EINVAL otherwise). The array's address is looked up once per device and kept: after
+ * a cudaDeviceReset of a device, do not call it on that device again in the same process. */
 int lw_thin_noalloc(const float* xyz4, const uint32_t* attr, int64_t m, double inv_v, double min_range,
                     double max_range, int32_t ret_mask, float* ds4_out, int32_t* n_ds_dev, void* stream);
 
@@ -236,6 +241,15 @@ int lw_icp_accumulate(const float* ds4, const int32_t* n_dev, int64_t n_ub, cons
  * st->ok and the stats. One persistent cooperative launch, one grid barrier per iteration. */
 int lw_icp_solve(const float* ds4, const int32_t* n_dev, const lw_odom_params* prm, lw_odom_state* st,
                  const lw_regmap* reg, lw_gn_scratch* gn, void* stream);
+
+/* Deskew and register one frame handed in the caller's device buffers: Odometry._deskew (odom.py:707-709)
+ * then Odometry._register (odom.py:752-803, with _downsample :731-737) from T_pred. raw4 [m*4] holds x, y, z,
+ * t as measured (16-byte aligned), attr [m]; the points are deskewed to t_mid with twist6 (rho, theta) into
+ * fb->f_xyz, thinned into fb->ds_xyz and registered; the result is in st->T_reg, st->ok and the stats
+ * (st->n_ds, iters, corr, rms, cond, degen, weak). Five launches, no host synchronisation. */
+int lw_register_frame(const float* raw4, const uint32_t* attr, int64_t m, double t_mid, const float* twist6_host,
+                      const double* T_pred_host, const lw_odom_params* prm, lw_odom_state* st, lw_frame_buf* fb,
+                      const lw_regmap* reg, lw_gn_scratch* gn, void* stream);
 
 /* ---- integration map (gpu.py:1213-1219) ------------------------------------------------------- */
 typedef struct lw_map {

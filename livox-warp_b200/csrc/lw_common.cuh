@@ -254,10 +254,11 @@ __device__ __forceinline__ void warp_fill_first(const int* __restrict__ pslot, i
 // ---- bounded grid barrier -------------------------------------------------------------------------------
 // bar[0] counts arrivals, bar[1] is the generation. Every CTA of a cooperative launch calls it; a CTA that
 // waits longer than the spin budget sets *err and returns false (the kernel then exits), so a fault can
-// never leave the GPU spinning.
+// never leave the GPU spinning. A launch that gave up leaves bar[0] part counted: the launcher zeroes it
+// before the next launch.
 constexpr long long BARRIER_SPINS = 1LL << 24;  // x ~100 ns sleeps: ~2 s at most
 
-__device__ __forceinline__ bool grid_barrier(uint32_t* bar, int* err, int code) {
+__device__ __forceinline__ bool grid_barrier(uint32_t* bar, int* err, int code, long long budget = BARRIER_SPINS) {
     __shared__ int ok_s;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -273,7 +274,7 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* bar, int* err, int code) 
         } else {
             long long spins = 0;
             while (*gen == g) {
-                if (++spins > BARRIER_SPINS) {
+                if (++spins > budget) {
                     atomicExch(err, code);
                     ok = 0;
                     break;

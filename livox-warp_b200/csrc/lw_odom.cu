@@ -1351,6 +1351,7 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         return;
     }
     const float voxel = (float)prm.reg_voxel;
+    const long long budget = gn.spin_budget > 0 ? (long long)gn.spin_budget : BARRIER_SPINS;
     IcpConsts k;
     k.inv_v = (float)(1.0 / prm.reg_voxel);
     k.mask = mask;
@@ -1365,7 +1366,8 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         // readers passed this barrier) and nobody adds to before the next barrier
         long long* fixed = reinterpret_cast<long long*>(gn.part) + (it % 3) * LW_ACC_STRIDE;
         icp_pass(ds, n, P, k, keys, rec, nullptr, fixed, gn.err);
-        if (!grid_barrier(gn.bar, gn.err, 1)) return;
+        if (it == 0 && (int)blockIdx.x == gn.skip_cta) return;  // injected failure: this CTA never arrives
+        if (!grid_barrier(gn.bar, gn.err, 1, budget)) return;
         if (blockIdx.x == 0 && threadIdx.x < LW_ACC_STRIDE)
             reinterpret_cast<long long*>(gn.part)[((it + 2) % 3) * LW_ACC_STRIDE + threadIdx.x] = 0;
         gn_reduce_fixed(fixed, S);
@@ -1585,6 +1587,30 @@ __global__ void k_predict_poses(int k0, int k1, int current, const lw_odom_state
 
 __global__ void k_reset_state(lw_odom_state* st, lw_odom_state init) { *st = init; }
 
+// The start of a single-frame registration (lw_register_frame): the prediction, the frame's point count, its
+// mid time and the twist it is deskewed with, into the device state.
+struct RegBegin {
+    double T[16];
+    double t_mid;
+    float tw[6];
+    int m;
+};
+
+__global__ void k_reg_begin(lw_odom_state* st, RegBegin b) {
+    const int t = threadIdx.x;
+    if (t < 16) st->T_pred[t] = b.T[t];
+    if (t < 6) st->xi_used[t] = b.tw[t];
+    if (t < 16) st->T_reg[t] = b.T[t];  // what a registration that gives up leaves: the prediction, not ok
+    if (t == 0) {
+        st->t_mid = b.t_mid;
+        st->m = b.m;
+        st->n_ds = 0;
+        st->ok = 0;
+        st->iters = 0;
+        st->corr = 0;
+    }
+}
+
 __global__ void k_zero_count(int* c) { *c = 0; }
 
 __global__ void k_restart_clock(lw_odom_state* st) {
@@ -1651,8 +1677,10 @@ static int launch_gn(const float* ds4, const int32_t* n_dev, const lw_odom_param
     lw_odom_params p = *prm;
     void* args[] = {(void*)&dsp, (void*)&n_dev, (void*)&p, (void*)&st, (void*)&keys, (void*)&rec,
                     (void*)&mask, (void*)&g, (void*)&which};
-    // the fixed-point accumulators of the first two iterations start at zero (the kernel clears the rest)
+    // the fixed-point accumulators of the first two iterations start at zero (the kernel clears the rest), and
+    // the barrier's arrival count too: a launch that gave up at the barrier may have left it part counted
     LW_CUDA(cudaMemsetAsync(gn->part, 0, 3 * LW_ACC_STRIDE * sizeof(long long), s));
+    LW_CUDA(cudaMemsetAsync(gn->bar, 0, 2 * sizeof(uint32_t), s));
     LW_CUDA(cudaLaunchCooperativeKernel((const void*)k_gn, dim3(grid), dim3(GN_THREADS), args, 0, s));
     count_launches(1);
     return LW_OK;
@@ -1820,6 +1848,46 @@ int lw_icp_solve(const float* ds4, const int32_t* n_dev, const lw_odom_params* p
     if (!ds4 || !n_dev || !prm || !st || !reg || !gn) return set_error(LW_EINVAL, "lw_icp_solve: null argument");
     ProfScope prof("gn", (cudaStream_t)stream);
     return launch_gn(ds4, n_dev, prm, st, reg, gn, 2, (cudaStream_t)stream);  // ungated
+}
+
+int lw_register_frame(const float* raw4, const uint32_t* attr, int64_t m, double t_mid, const float* twist6_host,
+                      const double* T_pred_host, const lw_odom_params* prm, lw_odom_state* st, lw_frame_buf* fb,
+                      const lw_regmap* reg, lw_gn_scratch* gn, void* stream) {
+    if (!raw4 || !attr || !twist6_host || !T_pred_host || !prm || !st || !fb || !reg || !gn)
+        return set_error(LW_EINVAL, "lw_register_frame: null argument");
+    if (((uintptr_t)raw4 & 15) != 0) return set_error(LW_EINVAL, "lw_register_frame: raw4 is not 16-byte aligned");
+    if (m < 0 || m > fb->cap)
+        return set_error(LW_ECAPACITY, "lw_register_frame: %lld points, frame capacity %lld", (long long)m,
+                         (long long)fb->cap);
+    cudaStream_t s = (cudaStream_t)stream;
+    RegBegin b;
+    for (int i = 0; i < 16; ++i) b.T[i] = T_pred_host[i];
+    for (int i = 0; i < 6; ++i) b.tw[i] = twist6_host[i];
+    b.t_mid = t_mid;
+    b.m = (int)m;
+    k_reg_begin<<<1, 32, 0, s>>>(st, b);
+    // the frame buffer reads the caller's points in place: pass A deskews them into f_xyz and claims the thinning
+    // voxels, B and C keep the lowest-index point of each and write ds_xyz in point order
+    lw_frame_buf f = *fb;
+    f.f_raw = const_cast<float*>(raw4);
+    f.f_attr = const_cast<uint32_t*>(attr);
+    ThinArgs a = thin_args(prm);
+    a.t_mid = (float)t_mid;
+    Tw6 tw;
+    for (int k = 0; k < 6; ++k) tw.v[k] = twist6_host[k];
+    const int64_t m_ub = m > 0 ? m : 1;
+    int grid = blocks_for(m_ub, 256, 8 * device_sms());
+    int nt = blocks_for(m_ub, TILE);
+    {
+        ProfScope prof("thin", s);
+        k_thin_a<<<grid, 256, 0, s>>>(f, &st->m, a, nullptr, tw, nullptr, nullptr, 1);
+        k_thin_b<<<nt, TILE, 0, s>>>(f, &st->m, nullptr);
+        k_thin_c<<<nt, TILE, 0, s>>>(f, &st->m, &st->n_ds, nullptr);
+    }
+    LW_LAUNCHED("lw_register_frame");
+    count_launches(4);
+    ProfScope prof("gn", s);
+    return launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 2, s);
 }
 
 // The frame's queue of launches; with `net`, the learned start pose replaces the constant-velocity one between
@@ -2003,7 +2071,9 @@ __global__ void k_noalloc_thin_reset(int64_t* keys, int32_t* win, int32_t* m_dev
 }
 
 // The array's device address, looked up once per device with that device current (host code may not use
-// the symbol itself: on the host it names a stand-in, not device memory).
+// the symbol itself: on the host it names a stand-in, not device memory). The address is kept for the life of
+// the process: after cudaDeviceReset the module loads again and the array may move, so a process that resets a
+// device must not call lw_thin_noalloc on it again.
 static int noalloc_thin_scratch(int64_t** out) {
     static std::mutex mu;
     static int64_t* addr[256] = {};
@@ -2027,6 +2097,9 @@ extern "C" int lw_thin_noalloc(const float* xyz4, const uint32_t* attr, int64_t 
                                double max_range, int32_t ret_mask, float* ds4_out, int32_t* n_ds_dev, void* stream) {
     using namespace lw;
     if (!xyz4 || !attr || !ds4_out || !n_ds_dev) return set_error(LW_EINVAL, "lw_thin_noalloc: null argument");
+    // the points are read and written as float4: a misaligned pointer is refused here, not faulted on
+    if (((uintptr_t)xyz4 & 15) != 0 || ((uintptr_t)ds4_out & 15) != 0)
+        return set_error(LW_EINVAL, "lw_thin_noalloc: xyz4 and ds4_out must be 16-byte aligned");
     if (m < 0 || m > NOALLOC_THIN_MAX)
         return set_error(LW_ECAPACITY, "lw_thin_noalloc: %lld points exceed the fixed maximum of %lld per call",
                          (long long)m, (long long)NOALLOC_THIN_MAX);

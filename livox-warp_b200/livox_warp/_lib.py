@@ -70,7 +70,7 @@ class FrameBuf(C.Structure):
 
 
 class GnScratch(C.Structure):
-    _fields_ = [("part", P), ("bar", P), ("err", P), ("grid", i32)]
+    _fields_ = [("part", P), ("bar", P), ("err", P), ("grid", i32), ("spin_budget", i32), ("skip_cta", i32)]
 
 
 class PoseTable(C.Structure):
@@ -180,6 +180,8 @@ _SIGS = {
     "lw_icp_accumulate": (i32, [P, P, i64, C.POINTER(f64), C.POINTER(RegMap), f32, i32, f32, f32,
                                 C.POINTER(GnScratch), P, P]),
     "lw_icp_solve": (i32, [P, P, C.POINTER(OdomParams), P, C.POINTER(RegMap), C.POINTER(GnScratch), P]),
+    "lw_register_frame": (i32, [P, P, i64, f64, C.POINTER(f32), C.POINTER(f64), C.POINTER(OdomParams), P,
+                                C.POINTER(FrameBuf), C.POINTER(RegMap), C.POINTER(GnScratch), P]),
     "lw_map_insert": (i32, [P, i32, P, P, P, P, i64, P, C.POINTER(View), f32, C.POINTER(Map), P, P]),
     "lw_carve": (i32, [P, i32, P, P, P, i64, P, i32, f32, f32, i32, C.POINTER(Map), P, P]),
     "lw_map_build": (i32, [C.POINTER(Map), C.POINTER(View), i32, P, P, P, P, P, P, P]),

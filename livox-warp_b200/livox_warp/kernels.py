@@ -1,7 +1,8 @@
 """The odometry kernels one by one: device tables plus thin wrappers over the C ABI (include/livox_b200.h).
 
-Odometry (odom.py) runs them fused, one lw_odom_finalize per frame; this module exposes each step on its own
-for callers that compose them differently (the parity tests, the single-frame ICP benchmark, batch tools).
+Odometry (odom.py) runs them fused: one lw_odom_finalize per streamed frame, one lw_register_frame per frame handed
+in directly. This module exposes each step on its own for callers that compose them differently (the parity
+tests, batch tools).
 """
 
 from __future__ import annotations
@@ -81,7 +82,9 @@ class RegistrationMap:
 
 
 class GnScratch:
-    """Scratch of the Gauss-Newton kernels: per-CTA partials, the grid barrier and its error flag."""
+    """Scratch of the Gauss-Newton kernels: per-CTA partials, the grid barrier and its error flag. The struct's
+    spin_budget (barrier wait limit, 0 = default) and skip_cta (a CTA that leaves before the first barrier, -1 =
+    none) exist for tests of the bounded wait."""
 
     def __init__(self, device="cuda"):
         d = torch.device(device)
@@ -92,7 +95,7 @@ class GnScratch:
         self.bar = torch.zeros(2, dtype=torch.int32, device=d)
         self.err = torch.zeros(1, dtype=torch.int32, device=d)
         self.struct = _lib.GnScratch(_lib.ptr(self.part).value, _lib.ptr(self.bar).value, _lib.ptr(self.err).value,
-                                     self.grid)
+                                     self.grid, 0, -1)
 
 
 def deskew(raw4: torch.Tensor, t_mid: float, inv_dt: float, twist, stream=None) -> torch.Tensor:

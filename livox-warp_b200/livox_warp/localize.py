@@ -76,12 +76,13 @@ def rot_to(a: np.ndarray, b: np.ndarray) -> np.ndarray:
 
 
 def voxel_means(xyz: np.ndarray, voxel: float) -> np.ndarray:
-    """The mean of the points in each voxel of a grid anchored at the points' minimum (open3d's
-    voxel_down_sample, which the reference's ScanPrep calls), in the order of each voxel's first point."""
+    """The mean of the points in each voxel of a grid whose origin is half a voxel below the points' minimum
+    (open3d's voxel_down_sample anchors its grid there; the reference's ScanPrep calls it), in the order of each
+    voxel's first point (open3d's own order is its hash map's)."""
     p = np.asarray(xyz, dtype=np.float64).reshape(-1, 3)
     if len(p) == 0:
         return p
-    k = np.floor((p - p.min(axis=0)) / voxel).astype(np.int64)
+    k = np.floor((p - (p.min(axis=0) - 0.5 * voxel)) / voxel).astype(np.int64)
     _, first, inv = np.unique(k, axis=0, return_index=True, return_inverse=True)
     inv = inv.reshape(-1)
     rank = np.empty(len(first), np.int64)
@@ -155,36 +156,44 @@ class ScanPrep:
         self.max_tilt = max_tilt_deg
 
     def up_candidates(self):
-        """[(up unit vector, evidence)] ranked by plane support, both signs of each family (localize.py:275-306):
-        the near-horizontal planes grouped within 10 degrees, one normal fitted to each family's planes together
-        (the smallest eigenvector of their summed scatter about their own centroids), the two best families."""
-        cos_tilt = math.cos(math.radians(self.max_tilt))
-        fams = []  # [support, [plane indices], seed normal]
-        for i, (cnt, n, _, _) in enumerate(self.planes):
-            if abs(n[2]) < cos_tilt:
-                continue  # a wall, for a sensor that is roughly level (or upside down)
-            for f in fams:
-                if abs(float(n @ f[2])) > math.cos(math.radians(10.0)):
-                    f[0] += cnt
-                    f[1].append(i)
-                    break
+        """[(up unit vector, evidence)] for the scan's gravity direction (the reference's ScanPrep.up_candidates,
+        localize.py:275-306): the planes within max_tilt of level are floors or ceilings; taken in RANSAC order,
+        each joins the first family whose founding normal lies within 10 degrees of its own (either sign) or founds
+        one. A family's evidence is its planes' inlier count. The two best families give a normal each -- the least
+        spread direction of their planes' points, each plane's points taken about their own centroid -- in both
+        signs, pointing first the way the founding plane did. A scan without such planes gives level, either way
+        up."""
+        level = [(np.array([0.0, 0.0, 1.0]), 0), (np.array([0.0, 0.0, -1.0]), 0)]
+        if not self.planes:
+            return level
+        normals = np.stack([pl[1] for pl in self.planes])
+        inliers = [pl[0] for pl in self.planes]
+        flat = np.flatnonzero(np.abs(normals[:, 2]) >= math.cos(math.radians(self.max_tilt)))
+        same = math.cos(math.radians(10.0))
+        founders: list[np.ndarray] = []
+        families: list[list[int]] = []
+        for i in flat:
+            near = [f for f, n0 in enumerate(founders) if abs(float(normals[i] @ n0)) > same]
+            if near:
+                families[near[0]].append(int(i))
             else:
-                fams.append([cnt, [i], n])
+                founders.append(normals[i])
+                families.append([int(i)])
+        evidence = [sum(inliers[i] for i in fam) for fam in families]
+        ranked = sorted(range(len(families)), key=lambda f: -evidence[f])[:2]  # stable: earlier family on ties
         out = []
-        for support, members, n0 in sorted(fams, key=lambda f: -f[0])[:2]:
-            S = np.zeros((3, 3))
-            for i in members:
-                P = self.pts[self.planes[i][3]]
-                P = P - P.mean(0)
-                S += P.T @ P
-            w, V = np.linalg.eigh(S)
-            n = V[:, 0]
-            if n @ n0 < 0:
-                n = -n
-            out += [(n, support), (-n, support)]
-        if not out:  # no floor or ceiling in view: a level sensor, either way up
-            out = [(np.array([0.0, 0.0, 1.0]), 0), (np.array([0.0, 0.0, -1.0]), 0)]
-        return out
+        for f in ranked:
+            scatter = sum(self._plane_scatter(i) for i in families[f])
+            n = np.linalg.eigh(scatter)[1][:, 0]
+            n = n if n @ founders[f] >= 0 else -n
+            out.extend([(n, evidence[f]), (-n, evidence[f])])
+        return out or level
+
+    def _plane_scatter(self, i: int) -> np.ndarray:
+        """Scatter matrix of plane i's inliers about their centroid."""
+        q = self.pts[self.planes[i][3]]
+        q = q - q.mean(axis=0)
+        return q.T @ q
 
     def height_profile(self, up: np.ndarray, lo: float, n_bins: int, bin_m: float):
         """Histogram of the heights (along up, from the sensor) of the scan's horizontal points (localize.py:308-313)."""
@@ -192,6 +201,28 @@ class ScanPrep:
         z = self.pts[horiz] @ up
         h, _ = np.histogram(z, bins=n_bins, range=(lo, lo + n_bins * bin_m))
         return h.astype(np.float32)
+
+
+def height_candidates(levels: np.ndarray, scan: np.ndarray, z_lo: float, bin_m: float, reach: float, z_range,
+                      n_max: int, min_sep: float = 0.08) -> list:
+    """Sensor heights at which a scan's height profile (horizontal points binned from -reach to +reach about the
+    sensor) lines up with the map's (binned from z_lo), best first: each profile is square-rooted (so a big floor
+    does not drown the rest) and smoothed over +-2 bins, their correlation is taken at every relative shift, shifts
+    putting the sensor outside z_range are dropped, and the best positive ones are picked greedily at least
+    min_sep apart, at most n_max (localize.py:400-424)."""
+    taper = np.array([0.25, 0.5, 1.0, 0.5, 0.25], np.float32)
+    a = np.convolve(np.sqrt(levels), taper, mode="same")
+    b = np.convolve(np.sqrt(scan), taper, mode="same")
+    score = np.correlate(a, b, mode="full")  # score[j]: the scan shifted by j - (len(b) - 1) bins
+    z = z_lo + (np.arange(len(score)) - (len(b) - 1)) * bin_m + reach
+    score = np.where((z >= z_range[0]) & (z <= z_range[1]), score, -1.0)
+    picked: list[float] = []
+    for j in np.argsort(-score):
+        if score[j] <= 0 or len(picked) >= n_max:
+            break
+        if all(abs(float(z[j]) - q) > min_sep for q in picked):
+            picked.append(float(z[j]))
+    return picked
 
 
 def thin_5cm(xyz: np.ndarray) -> np.ndarray:
@@ -485,31 +516,15 @@ class GlobalLocalizer:
     # ---- the global search (localize.py:400-424, 476-505, 616-738) -----------------------------------------------
 
     def _heights(self, prep: ScanPrep, up: np.ndarray):
-        """Sensor heights where the scan's horizontal surfaces line up with the map's, best first: the correlation
-        of the two height profiles (square-rooted, smoothed by +-2 bins) over every shift inside the map's z range,
-        peaks at least 8 cm apart (localize.py:400-424)."""
-        h_map, lo, bin_m = self.grid.levels
-        span = 6.0  # scan heights within +-6 m of the sensor
-        nb = int(round(2 * span / bin_m))
-        h_scan = prep.height_profile(up, -span, nb, bin_m)
-        if h_scan.sum() < 50:
+        """Sensor heights (map z) where the scan's horizontal surfaces line up with the map's, best first, or None
+        when the scan shows too few horizontal points (GlobalLocalizer._heights, localize.py:400-424)."""
+        levels, z_lo, bin_m = self.grid.levels
+        reach = 6.0  # m: the scan's horizontal points are binned within this height of the sensor
+        scan = prep.height_profile(up, -reach, int(round(2 * reach / bin_m)), bin_m)
+        if scan.sum() < 50:
             return None
-        k = np.array([0.25, 0.5, 1.0, 0.5, 0.25], np.float32)
-        hm = np.convolve(np.sqrt(h_map), k, mode="same")
-        hs = np.convolve(np.sqrt(h_scan), k, mode="same")
-        corr = np.correlate(hm, hs, mode="full")  # corr[j]: a shift of j - (nb - 1) bins
-        shifts = np.arange(len(corr)) - (nb - 1)
-        z_sensor = lo + shifts * bin_m + span
-        ok = (z_sensor >= self.grid.lo[2] - 0.5) & (z_sensor <= self.grid.hi[2] + 0.5)
-        corr = np.where(ok, corr, -1.0)
-        out = []
-        for i in np.argsort(-corr):
-            if corr[i] <= 0 or len(out) >= self.n_heights:
-                break
-            z = float(z_sensor[i])
-            if all(abs(z - o) > 0.08 for o in out):
-                out.append(z)
-        return out
+        return height_candidates(levels, scan, z_lo, bin_m, reach, (self.grid.lo[2] - 0.5, self.grid.hi[2] + 0.5),
+                                 self.n_heights)
 
     @staticmethod
     def _top(scores: np.ndarray, pool: int = 20000) -> np.ndarray:
@@ -520,25 +535,24 @@ class GlobalLocalizer:
 
     @staticmethod
     def _nms(hyps: np.ndarray, scores: np.ndarray, keep: int, dist: float, ang_deg: float) -> np.ndarray:
-        """Greedy non-maximum suppression over (x, y, z, yaw) hypotheses: the survivors' indices, best first
-        (localize.py:484-505)."""
-        chosen = []
+        """Greedy non-maximum suppression over (x, y, z, yaw) hypotheses (localize.py:484-505): walking the best
+        scores down (the `_top` pool) until a score is not positive, a hypothesis survives unless an earlier
+        survivor lies within `dist` metres and `ang_deg` degrees of heading of it; at most `keep` survive. Their
+        indices, best first."""
         ang = math.radians(ang_deg)
+        kept = np.empty((0, 4))
+        chosen: list[int] = []
         for i in GlobalLocalizer._top(scores):
-            if scores[i] <= 0:
+            if scores[i] <= 0 or len(chosen) >= keep:
                 break
             h = hyps[i]
-            ok = True
-            for j in chosen:
-                o = hyps[j]
-                dyaw = abs((h[3] - o[3] + math.pi) % (2 * math.pi) - math.pi)
-                if np.linalg.norm(h[:3] - o[:3]) < dist and dyaw < ang:
-                    ok = False
-                    break
-            if ok:
-                chosen.append(i)
-                if len(chosen) >= keep:
-                    break
+            if len(kept):
+                near = np.linalg.norm(kept[:, :3] - h[:3], axis=1) < dist
+                turn = np.abs((h[3] - kept[:, 3] + math.pi) % (2 * math.pi) - math.pi) < ang
+                if np.any(near & turn):
+                    continue
+            chosen.append(int(i))
+            kept = np.vstack([kept, h[None, :]])
         return np.array(chosen, dtype=np.int64)
 
     def _unique(self, best: float, alt: float) -> bool:
@@ -546,116 +560,135 @@ class GlobalLocalizer:
 
     @staticmethod
     def _runner_up(results) -> float:
-        """The best 3 cm fit of a result more than 1 m or 15 degrees from the winner's pose (localize.py:733-738)."""
-        best = results[0][3]
-        for r in results[1:]:
-            dt, ang = pose_difference(best, r[3])
-            if dt > 1.0 or ang > 15.0:
-                return r[0]
-        return 0.0
+        """Fit (3 cm inliers) of the best result that is a different answer -- more than 1 m or 15 degrees from the
+        best result's pose -- or 0 (localize.py:733-738). `results` is sorted best first."""
+        winner = results[0][3]
+        elsewhere = (r[0] for r in results[1:] if any(a > b for a, b in zip(pose_difference(winner, r[3]),
+                                                                             (1.0, 15.0))))
+        return next(elsewhere, 0.0)
 
     def localize(self, xyz: np.ndarray, stream=None, up_prior: np.ndarray | None = None, log=print, progress=None,
                  prep: ScanPrep | None = None):
-        """Sensor-to-map pose (4x4) of a scan given in the sensor frame, plus diagnostics (localize.py:616-728):
-        the gravity candidates of the scan's horizontal planes; per candidate the sensor heights where the scan's
-        and the map's horizontal surfaces line up, the coarse search over every free position x heading with its
-        local maxima (on the device), a finer local grid around each scored with more points and a tighter
-        tolerance, non-maximum suppression, then the batched ICP and the evaluation of the survivors; the search
-        stops early once an answer is good and unique. up_prior (gravity "up" in the sensor frame) only orders
-        the candidates; progress(text) is called between stages; prep may supply a prepared scan."""
+        """Sensor-to-map pose (4x4) of a scan given in the sensor frame, and diagnostics (GlobalLocalizer.localize,
+        localize.py:616-728). Stages: the scan's gravity candidates; for each, the sensor heights that line the
+        scan's horizontal surfaces up with the map's and the coarse search over every free position and heading
+        (its local maxima found on the device); then, best candidate first, a finer local grid around each coarse
+        maximum scored with more points, non-maximum suppression, the batched ICP and the evaluation -- stopping
+        once the best answer is good and unique. up_prior (gravity up in the sensor frame) only orders the
+        candidates; progress(text) is called between stages; prep may supply a prepared scan. The same scan always
+        gives the same answer (the subsets come from a generator seeded with self.seed)."""
         import time
 
-        t0 = time.perf_counter()
-        say = progress or (lambda s: None)
-        tm = {}
-        rng = np.random.default_rng(self.seed)  # the same scan always gives the same answer
+        times: dict = {}
+        t_start = time.perf_counter()
+        say = progress or (lambda text: None)
         prep = prep if prep is not None else ScanPrep(xyz)
+        scan = self._scan_subsets(prep)
+        ups = prep.up_candidates()
+        if up_prior is not None:
+            toward = np.asarray(up_prior, float) / np.linalg.norm(up_prior)
+            ups.sort(key=lambda u: -float(u[0] @ toward))
+        times["prep"] = time.perf_counter() - t_start
+        t0 = time.perf_counter()
+        gravity = [self._coarse_stage(stream, prep, up, support, scan["coarse"], say) for up, support in ups]
+        times["coarse"] = time.perf_counter() - t0
+        gravity.sort(key=lambda c: -c["best_coarse"])
+        results, refined = self._fine_stages(stream, gravity, scan, say, times)
+        if not results:
+            raise RuntimeError("no hypothesis survived (is the scan inside the map?)")
+        best = results[0]
+        alt = self._runner_up(results)
+        times["total"] = time.perf_counter() - t_start
+        n_hyp = sum(c["hypotheses"] for c in gravity)
+        winner = gravity[best[4]]
+        info = {"inliers": best[0], "inliers5": best[1], "inliers10": best[2], "runner_up": alt,
+                "unique": self._unique(best[0], alt), "up": winner["up"], "heights": winner["heights"],
+                "gravity_candidates": len(gravity), "refined_candidates": refined, "hypotheses": n_hyp,
+                "scan_points": scan["n"], "times": times}
+        log(f"  {times['total']:.2f} s (prep {times['prep']:.2f}, coarse {times['coarse']:.2f} for "
+            f"{n_hyp / 1e6:.1f}M hypotheses, medium {times['mid']:.2f}, ICP {times['icp']:.2f}; "
+            f"{refined}/{len(gravity)} gravity candidates refined): inliers {best[0]:.3f} within 3 cm "
+            f"(runner-up elsewhere {alt:.3f})")
+        return np.asarray(best[3]), info
+
+    def _scan_subsets(self, prep: ScanPrep) -> dict:
+        """The scan's points (at most PTS_CAP), the coarse subset (drawn from one point per 15 cm voxel, so it
+        spreads over the scan) and the medium subset, from a generator seeded with self.seed."""
+        rng = np.random.default_rng(self.seed)
         pts = prep.pts
         if len(pts) > self.PTS_CAP:
             pts = pts[rng.choice(len(pts), self.PTS_CAP, replace=False)]
-        n_pts = len(pts)
-        if n_pts < 200:
-            raise RuntimeError(f"scan too sparse to localise ({n_pts} points after 5 cm thinning)")
-        pts32 = pts.astype(np.float32)
-        # coarse / medium subsets: spread evenly over the scan (one per 15 cm voxel first)
+        if len(pts) < 200:
+            raise RuntimeError(f"scan too sparse to localise ({len(pts)} points after 5 cm thinning)")
         _, first = np.unique(np.floor(pts / 0.15).astype(np.int64), axis=0, return_index=True)
         spread = pts[first]
-        sub_c = spread[rng.choice(len(spread), min(self.n_coarse_pts, len(spread)), replace=False)]
-        sub_m = pts[rng.choice(n_pts, min(self.n_mid_pts, n_pts), replace=False)]
-        ups = prep.up_candidates()
-        if up_prior is not None:
-            upp = np.asarray(up_prior, float) / np.linalg.norm(up_prior)
-            ups.sort(key=lambda u: -float(u[0] @ upp))
-        tm["prep"] = time.perf_counter() - t0
-        cands = []
-        t1 = time.perf_counter()
-        n_hyp_total = 0
-        for up, support in ups:
-            say(f"coarse search, up {np.round(up, 2)}")
-            Rg = rot_to(up, np.array([0.0, 0.0, 1.0]))  # sensor -> gravity-aligned sensor frame
-            heights = self._heights(prep, up)
-            if not heights:
-                heights = list(np.arange(self.grid.lo[2], self.grid.hi[2] + 1e-6, self.xy_step))
-            pc = sub_c @ Rg.T
-            pos, shape, dyaw, best, best_sc = self._coarse_candidates(stream, pc, heights, keep=self.keep_coarse)
-            n_yaw = shape[3]
-            n_hyp_total += len(pos) * n_yaw
-            hyps = np.concatenate([pos[best // n_yaw], ((best % n_yaw) * dyaw)[:, None]], 1)
-            cands.append({"up": up, "Rg": Rg, "heights": heights, "coarse": hyps, "coarse_score": best_sc,
-                          "best_coarse": float(best_sc[0]) / len(pc) if len(best) else 0.0, "support": support})
-        tm["coarse"] = time.perf_counter() - t1
-        cands.sort(key=lambda c: -c["best_coarse"])
-        results = []  # (inliers3, inliers5, inliers10, T, candidate index, medium score)
-        tm["mid"] = tm["icp"] = 0.0
+        coarse = spread[rng.choice(len(spread), min(self.n_coarse_pts, len(spread)), replace=False)]
+        mid = pts[rng.choice(len(pts), min(self.n_mid_pts, len(pts)), replace=False)]
+        return {"pts32": pts.astype(np.float32), "coarse": coarse, "mid": mid, "n": len(pts)}
+
+    def _coarse_stage(self, stream, prep: ScanPrep, up: np.ndarray, support, coarse_pts: np.ndarray, say) -> dict:
+        """One gravity candidate's coarse search: its heights (or every height of the map on the xy step when the
+        profiles give none) and the coarse local maxima as (x, y, z, yaw) hypotheses with their scores."""
+        say(f"coarse search, up {np.round(up, 2)}")
+        Rg = rot_to(up, np.array([0.0, 0.0, 1.0]))  # sensor -> gravity-aligned sensor frame
+        heights = self._heights(prep, up) or list(np.arange(self.grid.lo[2], self.grid.hi[2] + 1e-6, self.xy_step))
+        pc = coarse_pts @ Rg.T
+        pos, shape, dyaw, best, best_sc = self._coarse_candidates(stream, pc, heights, keep=self.keep_coarse)
+        n_yaw = shape[3]
+        hyps = np.concatenate([pos[best // n_yaw], ((best % n_yaw) * dyaw)[:, None]], 1)
+        return {"up": up, "Rg": Rg, "heights": heights, "coarse": hyps, "coarse_score": best_sc,
+                "best_coarse": float(best_sc[0]) / len(pc) if len(best) else 0.0, "support": support,
+                "hypotheses": len(pos) * n_yaw}
+
+    def _local_window(self) -> np.ndarray:
+        """(dx, dy, dz, dyaw) offsets of the finer grid scored around each coarse maximum: +-1 coarse step in x and
+        y by quarter steps (two modes a step apart share one coarse maximum), +-4 cm in z, +-one heading step by
+        0.5 degrees."""
+        off = np.arange(-self.xy_step, self.xy_step + 1e-6, self.xy_step / 4)
+        offz = np.array([-0.04, 0.0, 0.04])
+        offy = np.radians(np.arange(-self.yaw_step_deg, self.yaw_step_deg + 1e-6, 0.5))
+        return np.stack([g.ravel() for g in np.meshgrid(off, off, offz, offy, indexing="ij")], 1)
+
+    def _fine_stages(self, stream, gravity: list, scan: dict, say, times: dict):
+        """Medium scores, suppression, ICP and evaluation for each gravity candidate, best first, until the best
+        answer is good and unique. Returns (results best first, candidates refined); a result is (inliers 3 cm,
+        5 cm, 10 cm, pose, candidate index, medium score)."""
+        import time
+
+        times["mid"] = times["icp"] = 0.0
+        window = self._local_window()
+        results: list = []
         refined = 0
-        for ci, c in enumerate(cands):
+        for ci, c in enumerate(gravity):
             if not len(c["coarse"]):
                 continue
-            say(f"refining gravity candidate {ci + 1}/{len(cands)}")
-            tm_a = time.perf_counter()
-            Rg = c["Rg"]
-            pm = sub_m @ Rg.T
-            # +-1 coarse step: two modes a step apart share one coarse local maximum, the window must reach both
-            off = np.arange(-self.xy_step, self.xy_step + 1e-6, self.xy_step / 4)
-            offz = np.array([-0.04, 0.0, 0.04])
-            offy = np.radians(np.arange(-self.yaw_step_deg, self.yaw_step_deg + 1e-6, 0.5))
-            A, B, Cz, D = np.meshgrid(off, off, offz, offy, indexing="ij")
-            local = np.stack([A.ravel(), B.ravel(), Cz.ravel(), D.ravel()], 1)
-            hyps = (c["coarse"][:, None, :] + local[None, :, :]).reshape(-1, 4)
+            say(f"refining gravity candidate {ci + 1}/{len(gravity)}")
+            t0 = time.perf_counter()
+            pm = scan["mid"] @ c["Rg"].T
+            hyps = (c["coarse"][:, None, :] + window[None, :, :]).reshape(-1, 4)
             ms = self._score_list(stream, pm.astype(np.float32), len(pm), hyps, self.tau_mid)
             best = self._nms(hyps, ms, self.n_icp, 0.1, 1.5)
-            tm["mid"] += time.perf_counter() - tm_a
-            tm_b = time.perf_counter()
-            Ts = []
-            for i in best:
-                x, y, z, yaw = hyps[i]
-                T = np.eye(4)
-                T[:3, :3] = rotz(yaw) @ Rg
-                T[:3, 3] = (x, y, z)
-                Ts.append(T)
-            Ts = self.icp(pts32, Ts, stream=stream)
-            fr = self.evaluate(pts32, Ts, stream=stream)
-            for j, i in enumerate(best):
-                results.append((float(fr[j, 0]), float(fr[j, 1]), float(fr[j, 2]), Ts[j], ci, float(ms[i]) / len(pm)))
-            tm["icp"] += time.perf_counter() - tm_b
+            times["mid"] += time.perf_counter() - t0
+            t0 = time.perf_counter()
+            starts = [self._pose_of(hyps[i], c["Rg"]) for i in best]
+            Ts = self.icp(scan["pts32"], starts, stream=stream)
+            fit = self.evaluate(scan["pts32"], Ts, stream=stream)
+            results.extend((float(fit[j, 0]), float(fit[j, 1]), float(fit[j, 2]), Ts[j], ci, float(ms[i]) / len(pm))
+                           for j, i in enumerate(best))
+            times["icp"] += time.perf_counter() - t0
             refined += 1
             results.sort(key=lambda r: -r[0])
             if self._unique(results[0][0], self._runner_up(results)):
-                break  # this candidate's best answer is good and unique
-        results.sort(key=lambda r: -r[0])
-        if not results:
-            raise RuntimeError("no hypothesis survived (is the scan inside the map?)")
-        top = results[0]
-        alt = self._runner_up(results)
-        tm["total"] = time.perf_counter() - t0
-        info = {"inliers": top[0], "inliers5": top[1], "inliers10": top[2], "runner_up": alt,
-                "unique": self._unique(top[0], alt), "up": cands[top[4]]["up"], "heights": cands[top[4]]["heights"],
-                "gravity_candidates": len(cands), "refined_candidates": refined, "hypotheses": n_hyp_total,
-                "scan_points": n_pts, "times": tm}
-        log(f"  {tm['total']:.2f} s (prep {tm['prep']:.2f}, coarse {tm['coarse']:.2f} for {n_hyp_total / 1e6:.1f}M "
-            f"hypotheses, medium {tm['mid']:.2f}, ICP {tm['icp']:.2f}; {refined}/{len(cands)} gravity candidates "
-            f"refined): inliers {top[0]:.3f} within 3 cm (runner-up elsewhere {alt:.3f})")
-        return np.asarray(top[3]), info
+                break
+        return results, refined
+
+    @staticmethod
+    def _pose_of(h: np.ndarray, Rg: np.ndarray) -> np.ndarray:
+        """Sensor-to-map pose of an (x, y, z, yaw) hypothesis in the gravity-aligned frame Rg."""
+        T = np.eye(4)
+        T[:3, :3] = rotz(h[3]) @ Rg
+        T[:3, 3] = h[:3]
+        return T
 
     def _score_list(self, stream, pts, m: int, hyps: np.ndarray, tau: float) -> np.ndarray:
         """The soft counts of (x, y, z, yaw) hypotheses for the first m points of `pts` (localize.py:507-515)."""

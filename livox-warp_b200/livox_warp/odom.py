@@ -111,6 +111,8 @@ class Odometry:
         self._rec_key = None
         self._integrate = None
         self._net = None  # (InitNet, lw_net_work, its buffers) when the learned start pose is on
+        self._reg_pin = None  # pinned staging of register_frame's host frames, and the event of its last copy
+        self._reg_ev = None
         # the frame's point count as the device state holds it (an int32 view into the state buffer)
         off = _lib.OdomState.m.offset
         self._m_dev = self._state[off:off + 4].view(torch.int32)
@@ -320,6 +322,71 @@ class Odometry:
         work = _lib.NetWork(*(_lib.ptr(bufs[k]).value for k in _lib.NetWork.PTRS), float(radius),
                             float(self.reg_voxel) if nearest else 0.0)
         self._net = (net, work, bufs)
+
+    def register_frame(self, xyz, attr, t, t_mid: float, twist, T_pred: np.ndarray, sync: bool = True):
+        """Deskew one frame to t_mid with the body twist (rho, theta) and register it against the map from T_pred:
+        the reference's _deskew then _register (odom.py:707-709, 752-803), for a frame handed in directly instead
+        of cut from a stream. The map is left as it is (no keyframe insert, no velocity update).
+
+        xyz: (m, 3) sensor points with t (m,) separately, or (m, 4) with t in the last column (t is then
+        ignored); attr (m,) uint32. A CUDA tensor (m, 4) float32 is read in place; host arrays are staged into
+        the frame buffer through pinned memory. With sync, returns (T, ok, stats) like the reference's
+        _register plus its stats; without, returns None and registration() reads the result later."""
+        d = self.device
+        if isinstance(xyz, torch.Tensor) and xyz.is_cuda:
+            m = int(xyz.shape[0])
+            raw = xyz if (xyz.dim() == 2 and xyz.shape[1] == 4 and xyz.dtype == torch.float32
+                          and xyz.is_contiguous()) else None
+            if raw is None:
+                raise ValueError("a device frame must be a contiguous (m, 4) float32 tensor (x, y, z, t)")
+            at = attr if isinstance(attr, torch.Tensor) else torch.as_tensor(np.asarray(attr).view(np.int32), device=d)
+        else:
+            x = np.asarray(xyz, np.float32)
+            m = len(x)
+            if m > self.frame_cap:
+                raise ValueError(f"{m} points exceed the frame capacity {self.frame_cap}")
+            if self._reg_pin is None or self._reg_pin[0].shape[0] < m:
+                cap = max(m, 1 << 14)
+                self._reg_pin = (torch.empty((cap, 4), dtype=torch.float32, pin_memory=True),
+                                 torch.empty(cap, dtype=torch.int32, pin_memory=True))
+            hp, ha = self._reg_pin
+            if self._reg_ev is not None:
+                self._reg_ev.synchronize()  # the previous call's copies out of the pinned buffers are done
+            hn = hp.numpy()
+            hn[:m, :3] = x[:, :3]
+            hn[:m, 3] = x[:, 3] if x.shape[1] == 4 else np.asarray(t, np.float32)
+            ha.numpy()[:m] = np.asarray(attr).view(np.int32)
+            with torch.cuda.stream(self.stream):
+                self.f_raw[:m].copy_(hp[:m], non_blocking=True)
+                self.f_attr[:m].copy_(ha[:m], non_blocking=True)
+                self._reg_ev = torch.cuda.Event()
+                self._reg_ev.record(self.stream)
+            raw, at = self.f_raw, self.f_attr
+        if m > self.frame_cap:
+            raise ValueError(f"{m} points exceed the frame capacity {self.frame_cap}")
+        self._sync_records()
+        _lib.call("lw_register_frame", _lib.ptr(raw), _lib.ptr(at), m, float(t_mid),
+                  _lib.f32_array(np.asarray(twist, np.float32).reshape(6)),
+                  _lib.f64_array(np.asarray(T_pred, np.float64).reshape(16)), _byref(self.params()),
+                  _lib.ptr(self._state), _byref(self.fbuf), _byref(self.regmap), _byref(self.gn), self._sp())
+        return self.registration() if sync else None
+
+    def registration(self):
+        """(T, ok, stats) of the last register_frame (synchronises the stream). stats["err"] is non-zero when a
+        registration since the last reset gave up (a bounded wait ran out, or a fixed-point sum overflowed)."""
+        st = self.read_state()
+        with torch.cuda.stream(self.stream):
+            err = int(self._gn.err.cpu()[0])
+        stats = {"ds": st.n_ds, "iters": st.iters, "corr": st.corr, "rms": st.rms, "cond": st.cond,
+                 "weak": bool(st.weak), "degen": st.degen, "err": err}
+        return np.array(st.T_reg, dtype=np.float64).reshape(4, 4), bool(st.ok), stats
+
+    def insert_frame(self, xyz4: torch.Tensor, attr: torch.Tensor, T: np.ndarray):
+        """Add a frame's points (a (m, 4) float32 CUDA tensor), posed by T, to the registration map as a keyframe
+        would be (odom.py:719-727): what builds a prior registration map from frames whose poses are known."""
+        self._sync_records()
+        self.reg.insert(xyz4, attr, T, self.reg_voxel, self.max_range, int(self.ret_mask), self.noise, self.alpha,
+                        stream=self.stream)
 
     def iteration_log(self) -> np.ndarray:
         """(k, iterations of the first registration, iterations of the last) of every logged frame that

@@ -16,11 +16,16 @@ thread spends its time waiting on its stream and the caller's stream never waits
 and frames cross between streams as copies into preallocated device slots, ordered by CUDA events: the consumer
 stream waits for the copy's event, and the producer's next write to the source waits for the same event. Nothing
 is allocated after construction.
+
+Control plane: batches and commands (reset, restart, configure) travel in two deques under one condition variable.
+Every batch carries its submission number, every command the number of batches submitted before it; the worker
+runs a command as soon as no earlier batch is waiting, so commands and batches take effect in the order the caller
+issued them. A new generation (reset, restart) releases the waiting batches of the old one at once.
 """
 
 from __future__ import annotations
 
-import queue
+import collections
 import sys
 import threading
 import time
@@ -96,6 +101,7 @@ class FrameResult:
 
 @dataclass
 class _Batch:
+    seq: int  # submission number
     gen: int
     epoch: int
     snap: _Snap
@@ -105,23 +111,11 @@ class _Batch:
 
 
 @dataclass
-class _Reset:
+class _Command:
+    after: int  # batches submitted before it: it runs once those have been taken
+    kind: str  # "reset", "restart" or "configure"
     gen: int
-    T0: np.ndarray
-
-
-@dataclass
-class _Restart:
-    gen: int
-
-
-@dataclass
-class _Config:
-    params: dict
-
-
-class _Stop:
-    pass
+    arg: object = None
 
 
 class OdomWorker:
@@ -149,21 +143,32 @@ class OdomWorker:
                                [torch.float32, torch.int32, torch.float32, torch.int32], d)
         torch.cuda.synchronize(d)
         self.max_batches = max_batches
-        self.q_in: queue.Queue = queue.Queue()
-        self.q_out: queue.Queue = queue.Queue()
         self.gen = 0  # the caller's generation
         self._worker_gen = 0  # the generation the worker thread is on (written by that thread only)
-        self._pending = 0  # batches queued and not yet processed
-        self._lock = threading.Lock()
+        # work for the worker thread, guarded by _cv: batches and commands, ordered by submission number
+        self._cv = threading.Condition()
+        self._batches: collections.deque[_Batch] = collections.deque()
+        self._commands: collections.deque[_Command] = collections.deque()
+        self._submitted = 0
+        self._running = 0  # batches taken by the worker and not yet finished
+        self._stopping = False
+        # finished frames for the caller
+        self._ready: collections.deque[FrameResult] = collections.deque()
+        self._ready_lock = threading.Lock()
+        self._lock = threading.Lock()  # counters
         self.drops = {"input_full": 0, "input_own": 0, "output_pool": 0, "stale": 0, "error": 0}
         self.processed = 0
         self.frames = 0
         self.last_error = ""
         self.busy_ms = 0.0  # running average of worker time per batch
         self._consumed: list[FrameResult] = []
-        self._stop = False
-        self._thread = threading.Thread(target=self._run, name="livox-odometry", daemon=True)
+        self._closed = False
+        self._thread = threading.Thread(target=self._serve, name="livox-odometry", daemon=True)
         self._thread.start()
+
+    def _count(self, key: str, by: int = 1):
+        with self._lock:
+            self.drops[key] += by
 
     # ---- caller thread ----------------------------------------------------------------------------------
 
@@ -172,89 +177,88 @@ class OdomWorker:
         False = dropped (counted)."""
         if n <= 0:
             return True
-        with self._lock:
-            if self._pending >= self.max_batches:
-                self.drops["input_full"] += 1
-                return False
+        with self._cv:
+            waiting = len(self._batches) + self._running
+        if waiting >= self.max_batches:
+            self._count("input_full")
+            return False
         i = self.in_pool.take() if n <= self.in_cap else None
         if i is None:
-            with self._lock:
-                self.drops["input_own"] += 1
+            self._count("input_own")
             return False
         caller = torch.cuda.current_stream(self.device)
         ev = torch.cuda.Event()
         slot = self.in_pool.bufs[i]
         self.s_in.wait_stream(caller)  # the copy reads what the caller's stream staged
         with torch.cuda.stream(self.s_in):
-            slot[0][:n].copy_(sx[:n, :3], non_blocking=True)
-            slot[1][:n].copy_(sa[:n], non_blocking=True)
-            slot[2][:n].copy_(st[:n], non_blocking=True)
+            for dst, src in zip(slot, (sx[:n, :3], sa[:n], st[:n])):
+                dst[:n].copy_(src, non_blocking=True)
             ev.record(self.s_in)
         caller.wait_event(ev)  # the caller's next write to its staging buffers waits for this copy
-        with self._lock:
-            self._pending += 1
-        self.q_in.put(_Batch(self.gen, int(epoch), _Snap(self.in_pool, i, n, ev), n, float(t_min), float(t_max)))
+        with self._cv:
+            self._batches.append(_Batch(self._submitted, self.gen, int(epoch), _Snap(self.in_pool, i, n, ev), n,
+                                        float(t_min), float(t_max)))
+            self._submitted += 1
+            self._cv.notify()
         return True
 
-    def _new_generation(self):
-        """Bump the generation and drop the batches still queued for the old one (control items keep their order)."""
-        self.gen += 1
-        keep = []
-        while True:
-            try:
-                it = self.q_in.get_nowait()
-            except queue.Empty:
-                break
-            if isinstance(it, _Batch):
-                it.snap.release()
-                with self._lock:
-                    self._pending -= 1
-                    self.drops["stale"] += 1
-            else:
-                keep.append(it)
-        for it in keep:
-            self.q_in.put(it)
-        self._drain_out()
+    def _command(self, kind: str, arg=None, new_generation: bool = False):
+        stale: list[_Batch] = []
+        with self._cv:
+            if new_generation:
+                self.gen += 1
+                stale = [b for b in self._batches if b.gen != self.gen]
+                self._batches = collections.deque(b for b in self._batches if b.gen == self.gen)
+            self._commands.append(_Command(self._submitted, kind, self.gen, arg))
+            self._cv.notify()
+        for b in stale:  # the old generation's batches give their slots back now
+            b.snap.release()
+        if stale:
+            self._count("stale", len(stale))
+        if new_generation:
+            self._take_ready(self.gen)
 
     def reset(self, T0: np.ndarray):
         """Forget map and trajectory; the next frame is posed at T0. Batches and results of the old generation are
         discarded."""
-        self._new_generation()
-        self.q_in.put(_Reset(self.gen, np.array(T0, dtype=np.float64)))
+        self._command("reset", np.array(T0, dtype=np.float64), new_generation=True)
 
     def restart_clock(self):
         """The clock restarted: keep the map and pose, restart frame counting at rest; the old clock's batches and
         results are discarded."""
-        self._new_generation()
-        self.q_in.put(_Restart(self.gen))
+        self._command("restart", new_generation=True)
 
     def configure(self, **params):
         """Set Odometry tuning attributes between batches; an unknown name raises AttributeError here."""
         for name in params:
             if not isinstance(getattr(self.odom, name, None), (int, float, str)):
                 raise AttributeError(f"Odometry has no tuning attribute {name!r}")
-        self.q_in.put(_Config(dict(params)))
+        self._command("configure", dict(params))
+
+    def _take_ready(self, gen: int) -> list[FrameResult]:
+        """The finished frames of generation `gen`; the others are released and counted stale."""
+        with self._ready_lock:
+            items = list(self._ready)
+            self._ready.clear()
+        keep = [r for r in items if r.gen == gen]
+        for r in items:
+            if r.gen != gen:
+                r.release()
+        if len(keep) != len(items):
+            self._count("stale", len(items) - len(keep))
+        return keep
 
     def poll(self) -> list[FrameResult]:
         """Finished frames of the current generation; their arrays are ready for the caller's current stream. Call
         release_consumed() once that stream no longer reads them."""
         caller = torch.cuda.current_stream(self.device)
-        out = []
-        while True:
-            try:
-                r = self.q_out.get_nowait()
-            except queue.Empty:
-                break
-            if r.gen != self.gen:
-                r.release()
-                with self._lock:
-                    self.drops["stale"] += 1
-                continue
+        out = self._take_ready(self.gen)
+        for r in out:
             if r._snap is not None:
                 r._snap.wait(caller)
-            self.frames += 1
-            self._consumed.append(r)
-            out.append(r)
+        with self._lock:
+            self.frames += len(out)
+        self._consumed.extend(out)
         return out
 
     def release_consumed(self):
@@ -263,63 +267,77 @@ class OdomWorker:
             r.release()
         self._consumed.clear()
 
-    def _drain_out(self):
-        while True:
-            try:
-                self.q_out.get_nowait().release()
-            except queue.Empty:
-                break
-
     def status(self) -> dict:
+        with self._cv:
+            pending = len(self._batches) + self._running
         with self._lock:
-            return {"pending": self._pending, "processed": self.processed, "frames": self.frames,
+            return {"pending": pending, "processed": self.processed, "frames": self.frames,
                     "drops": dict(self.drops), "busy_ms": round(self.busy_ms, 2), "last_error": self.last_error,
                     "pool_free": min(self.in_pool.free_slots, self.out_pool.free_slots)}
 
     def close(self):
-        if self._stop:
+        if self._closed:
             return
-        self._stop = True
-        self._new_generation()
-        self.q_in.put(_Stop())
+        self._closed = True
+        with self._cv:
+            self.gen += 1
+            stale = list(self._batches)
+            self._batches.clear()
+            self._commands.clear()
+            self._stopping = True
+            self._cv.notify()
+        for b in stale:
+            b.snap.release()
         self._thread.join(timeout=10.0)
-        self._drain_out()
+        self._take_ready(self.gen)
         self.release_consumed()
         if self._thread.is_alive():
             print("OdomWorker.close: the odometry thread did not stop", file=sys.stderr)
 
     # ---- worker thread ----------------------------------------------------------------------------------
 
-    def _run(self):
+    def _next(self):
+        """Block until there is work: the next command when no earlier batch waits, else the next batch; None to
+        stop."""
+        with self._cv:
+            self._cv.wait_for(lambda: self._stopping or self._batches or self._commands)
+            if self._stopping:
+                return None
+            if self._commands and (not self._batches or self._commands[0].after <= self._batches[0].seq):
+                return self._commands.popleft()
+            self._running += 1
+            return self._batches.popleft()
+
+    def _serve(self):
         torch.cuda.set_device(self.device)
-        while True:
-            item = self.q_in.get()
-            if isinstance(item, _Stop):
-                break
+        while (item := self._next()) is not None:
             try:
-                if isinstance(item, _Reset):
-                    self._worker_gen = item.gen
-                    self.odom.reset(item.T0)
-                    self.odom.synchronize()
-                elif isinstance(item, _Restart):
-                    self._worker_gen = item.gen
-                    self.odom.restart_clock()
-                elif isinstance(item, _Config):
-                    for name, value in item.params.items():
-                        setattr(self.odom, name, value)
-                elif isinstance(item, _Batch):
+                if isinstance(item, _Batch):
                     self._batch(item)
-            except Exception as e:  # one bad batch must not stop the worker
+                else:
+                    self._apply(item)
+            except Exception as e:  # one bad batch or command must not stop the worker
                 with self._lock:
                     self.drops["error"] += 1
                     self.last_error = f"{type(e).__name__}: {e}"
                 traceback.print_exc()
 
+    def _apply(self, c: _Command):
+        if c.kind == "configure":
+            for name, value in c.arg.items():
+                setattr(self.odom, name, value)
+            return
+        self._worker_gen = c.gen
+        if c.kind == "reset":
+            self.odom.reset(c.arg)
+            self.odom.synchronize()
+        else:
+            self.odom.restart_clock()
+
     def _batch(self, item: _Batch):
         try:
             if item.gen != self._worker_gen:
-                with self._lock:
-                    self.drops["stale"] += 1
+                self._count("stale")
                 return
             t0 = time.perf_counter()
             s = self.s_odom
@@ -335,8 +353,8 @@ class OdomWorker:
                 self.busy_ms = dt if self.processed == 1 else 0.9 * self.busy_ms + 0.1 * dt
         finally:
             item.snap.release()
-            with self._lock:
-                self._pending -= 1
+            with self._cv:
+                self._running -= 1
 
     def _on_frame(self, k, T, fx, fa, ft, ff, m):
         """On the worker thread when a frame's pose is final: copy its points out for the caller."""
@@ -346,8 +364,7 @@ class OdomWorker:
         snap = None
         i = self.out_pool.take() if m <= o.frame_cap else None
         if i is None:
-            with self._lock:
-                self.drops["output_pool"] += 1
+            self._count("output_pool")
         else:
             ev = torch.cuda.Event()
             slot = self.out_pool.bufs[i]
@@ -361,4 +378,5 @@ class OdomWorker:
         r = FrameResult(self._worker_gen, int(k), np.array(T, dtype=np.float64), xi, int(m),
                         snap.arrays if snap else None, dict(o.stats))
         r._snap = snap
-        self.q_out.put(r)
+        with self._ready_lock:
+            self._ready.append(r)

@@ -499,3 +499,34 @@ def perturb(T: np.ndarray, seed: int, trans: float, yaw_deg: float, tilt_deg: fl
         T[i, :3, :3] = R @ T[i, :3, :3]
         T[i, :2, 3] += dxy[i]
     return T
+
+
+def look_at(p, target) -> np.ndarray:
+    """Sensor-to-world pose at p with the sensor's x axis toward target (no roll)."""
+    p = np.asarray(p, np.float64)
+    d = np.asarray(target, np.float64) - p
+    yaw = math.atan2(d[1], d[0])
+    pitch = -math.atan2(d[2], np.linalg.norm(d[:2]))
+    T = np.eye(4)
+    T[:3, :3] = Rotation.from_euler("zyx", [yaw, pitch, 0.0]).as_matrix()
+    T[:3, 3] = p
+    return T
+
+
+def single_frame_case(scene: Scene, n_frames: int, rate: float = 100000.0, map_frames: int = 10,
+                      v: float = 0.5, yaw_rate_deg: float = 20.0, map_seed: int = 21, seed: int = 100):
+    """The single-frame scan-to-map ICP case: a sensor in a corner of the box room, looking across it and slightly
+    down, holds still for map_frames frames (they build the map), then moves at v m/s forward while turning at
+    yaw_rate_deg deg/s. Returns (T0, map frames [(xyz, attr, t)], moving frames [(xyz, attr, t, t_mid, T_true)]):
+    moving frame j is the first 0.1 s of motion of a sensor that starts moving at 1.0 + 0.1 j s, so each is a
+    fresh rosette pattern taken while moving, its points in the sensor frame at their own firing times."""
+    T0 = look_at([0.8, 0.8, 1.6], [7.0, 5.0, 1.0])
+    static = ConstantVelocity(T0, 1e9, 0.0, 0.0)
+    base = frames(scene, static, map_frames, rate, map_seed)
+    moving = []
+    for j in range(n_frames):
+        t0 = 0.1 * map_frames + 0.1 * j
+        mover = ConstantVelocity(T0, t0, v, math.radians(yaw_rate_deg))
+        x, a, t = scan(scene, mover, t0, t0 + 0.1, rate, seed + j)
+        moving.append((x, a, t, t0 + 0.05, mover.poses(np.array([t0 + 0.05]))[0]))
+    return T0, base, moving

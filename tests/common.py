@@ -43,18 +43,7 @@ def raw4(xyz, t) -> np.ndarray:
 
 def look_at(p, target) -> np.ndarray:
     """Sensor-to-world pose at p with the sensor's x axis toward target (no roll)."""
-    import math
-
-    from scipy.spatial.transform import Rotation
-
-    p = np.asarray(p, np.float64)
-    d = np.asarray(target, np.float64) - p
-    yaw = math.atan2(d[1], d[0])
-    pitch = -math.atan2(d[2], np.linalg.norm(d[:2]))
-    T = np.eye(4)
-    T[:3, :3] = Rotation.from_euler("zyx", [yaw, pitch, 0.0]).as_matrix()
-    T[:3, 3] = p
-    return T
+    return synth.look_at(p, target)
 
 
 def config1_pose() -> np.ndarray:

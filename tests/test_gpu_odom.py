@@ -215,3 +215,44 @@ def test_register_degenerate_corridor_matches_oracle():
     assert abs(Tg[0, 3] - Tp[0, 3]) < 0.002  # the corridor direction stays at the prediction
     assert abs(Tg[1, 3] - T0[1, 3]) < 0.01 and abs(Tg[2, 3] - T0[2, 3]) < 0.01  # the constrained ones converge
     assert abs(sg["cond"] - so["cond"]) <= 1e-6 + 0.05 * abs(so["cond"])  # float32 sums of H: ~1e-3 relative
+
+
+def test_register_frame_single_case_matches_float64_oracle():
+    """The single-frame case through Odometry.register_frame (deskew + thinning + Gauss-Newton in one call, from
+    host arrays and from device tensors): every one of its 8 seeded frames lands within 1 mm / 0.01 deg of the
+    float64 oracle registering the same thinned frame from the same start, and within 3 cm / 1 deg of the truth."""
+    from livox_warp import gpu, synth
+    from livox_warp.odom import Odometry
+
+    voxel = 0.2
+    T0, base, moving = synth.single_frame_case(common.room(1), 8, RATE)
+    oreg = oracle.RegMap(1 << 18)
+    pipe = gpu.Pipeline(ring_capacity=1 << 14, map_capacity=1 << 14)
+    odom = Odometry(pipe, reg_slots=1 << 18, frame_cap=1 << 15)
+    odom.reg_voxel, odom.max_iter = voxel, 10
+    odom.reset(T0)
+    for x, a, t in base:
+        x4 = common.raw4(x, t)
+        oreg.insert(x4, a, T0, voxel, 60.0, 0b1111)
+        odom.insert_frame(torch.from_numpy(x4).cuda(), torch.from_numpy(a.view(np.int32)).cuda(), T0)
+    oreg.records(voxel, 0.02, 0.05)
+    g, o = odom.reg.as_dict(), oreg.as_dict()
+    assert g == o
+    p = oracle.Params(reg_voxel=voxel, max_iter=10)
+    zero = np.zeros(6, np.float32)
+    for j, (x, a, t, t_mid, T_true) in enumerate(moving):
+        x4 = common.raw4(x, t)
+        ds = oracle.thin(oracle.deskew(x4, t_mid, 10.0, zero), a, np.float32(2.0 / voxel), 0.3, 60.0, 0b1111)
+        To, ok_o, so = oracle.register(ds, T0, oreg, p)
+        if j % 2:
+            Tg, ok_g, sg = odom.register_frame(x, a, t, t_mid, zero, T0)
+        else:
+            Tg, ok_g, sg = odom.register_frame(torch.from_numpy(x4).cuda(), torch.from_numpy(a.view(np.int32)).cuda(),
+                                               None, t_mid, zero, T0)
+        assert ok_g and ok_o
+        assert sg["ds"] == len(ds) and sg["iters"] == so["iters"], (sg, so)
+        assert np.array_equal(odom.ds_xyz[:len(ds)].cpu().numpy(), ds)
+        dt, dr = oracle.pose_error(To, Tg)
+        assert dt <= 1e-3 and dr <= 0.01, (j, dt, dr)
+        et, er = oracle.pose_error(T_true, Tg)
+        assert et < 0.03 and er < 1.0, (j, et, er)

@@ -138,15 +138,16 @@ def test_localize_end_to_end_with_the_oracle_for_the_device_stages():
 
 
 def test_scan_prep_voxel_means_and_ransac_plane():
-    """The two steps ScanPrep restates from open3d: voxel means on a grid anchored at the points' minimum (each
-    voxel's float64 mean, in the order of its first point), and a seeded RANSAC plane that finds a noisy plane
+    """The two steps ScanPrep restates from open3d: voxel means on a grid anchored half a voxel below the points'
+    minimum, as open3d anchors it (each voxel's float64 mean, in the order of its first point), and a seeded
+    RANSAC plane that finds a noisy plane
     among outliers and returns its least-squares refit and inliers; the same seed gives the same plane."""
     from livox_warp.localize import ransac_plane, voxel_means
 
     rng = np.random.default_rng(3)
     p = rng.uniform(-1, 1, (5000, 3))
     m = voxel_means(p, 0.25)
-    k = np.floor((p - p.min(0)) / 0.25).astype(np.int64)
+    k = np.floor((p - (p.min(0) - 0.125)) / 0.25).astype(np.int64)
     _, first, inv = np.unique(k, axis=0, return_index=True, return_inverse=True)
     order = np.argsort(first, kind="stable")
     want = np.stack([p[inv.reshape(-1) == v].mean(0) for v in order])
