@@ -1,20 +1,29 @@
 #!/usr/bin/env python
-"""Benchmark of the per-frame SLAM hot path on B200: sequence odometry frames/s.
+"""Benchmark of the per-frame SLAM hot path on B200.
 
-Workload (the sequence-odometry configuration): a seeded 8 x 6 x 3 m box room with 20 boxes, a Mid-40-like
-rosette at 100k points/s (about 10k points per 0.1 s frame) along a smooth handheld trajectory (a spline
-through random waypoints, <= 1 m/s and <= 60 deg/s, after 1 s at rest). Each step is one frame through the
-whole path: frame cut, deskew, half-voxel thinning, scan-to-map Gauss-Newton (float64 6x6 solve on the device),
-re-deskew, keyframe insert into the 0.15 m registration map, velocity update, then insertion of the frame into
-the 0.1 m integration map (2^22 slots) and free-space carving of every ray.
+Default workload (`--workload single`, the single-frame scan-to-map ICP configuration): a seeded 8 x 6 x 3 m box
+room with 20 boxes and a Mid-40-like rosette (r = 0.5 fov sin(7/3 phi), fov 38.4 deg) at 100k points/s; the
+registration map (0.2 m voxels, 2^21 slots) is built from 10 frames of a sensor holding still in a corner, then
+the sensor moves at 0.5 m/s forward and 20 deg/s yaw. A step registers one 10k-point frame taken in the first
+0.1 s of that motion: deskew with the constant-velocity prediction (a sensor that was at rest: its pose and a
+zero twist), half-voxel thinning, and at most 10 Gauss-Newton iterations with the float64 6x6 solve on the device
+(Odometry.register_frame, the reference's _deskew + _register, odom.py:707-709, 752-803). Eight seeded frames are
+cycled. The line reports frames/s and points/s, each distinct frame's pose against the float64 oracle registering
+the same thinned frame from the same start (the metric's <= 1 mm / 0.01 deg) and against the truth.
 
   value  frames/s with the frames already resident in HBM, device time (CUDA events per step), L2 flushed
          between steps by a 256 MB write outside the timed events;
-  e2e    the same through the public API from host (numpy) buffers: pinned H2D of each frame, the pose read
+  e2e    the same through the public API from host (numpy) buffers: pinned H2D of each frame, the result read
          back (D2H) every frame, CUDA events around all steps;
   roofline  the dominant kernel's algorithmic bytes / its live average launch time vs the measured HBM peak;
   cpu_baseline  the CPU oracle (a C++ / numpy restatement of the reference's kernels and host solve, OpenMP)
          on a bounded sample of the same frames.
+
+`--workload sequence` measures sequence odometry: the same room and rosette along a smooth handheld trajectory (a
+spline through random waypoints, <= 1 m/s and <= 60 deg/s, after 1 s at rest). Each step is one frame through the
+whole path: frame cut, deskew, half-voxel thinning, scan-to-map Gauss-Newton, re-deskew, keyframe insert into the
+0.15 m registration map, velocity update, then insertion of the frame into the 0.1 m integration map (2^22 slots)
+and free-space carving of every ray; the timed frames start after the at-rest second and the ramp to cruise speed.
 
 `--impl reference` times the reference's CPU implementation of the path instead: NVIDIA Warp (the reference's
 only runtime) is not installed, so that arm runs the CPU restatement, on every host core.
@@ -24,11 +33,13 @@ points per frame) on a handheld path through a seeded 40 x 30 x 3 m office with 
 (walker ghosts), the map's visible set, the 0.5 m ground grid (slope allowance 0.3) and clusters of the non-ground
 points at 0.2 m voxels (connect 0.35 m, 30 points), read back to the host; latency p50 / p99 per frame.
 
-`--workload learned` measures the learned start pose: 50k training pairs cut from plain-odometry runs of seeded
-fast handheld paths (<= 2 m/s, <= 120 deg/s) in the box room, the network trained on the GPU by the library's bf16
-kernels, then held-out 600-frame paths registered twice -- from the constant-velocity prediction and from the
-network's proposal -- comparing Gauss-Newton iterations of the first registration and the pose error against the
-ground truth.
+`--workload learned` measures the learned start pose: fast handheld paths in the box room (<= 2 m/s, <= 120 deg/s),
+every frame registered against a map of the frames before it (inserted at their true poses) three times -- from
+the constant-velocity prediction, from the network's proposal made at that prediction, and from the true pose
+(the converged registration that judges the other two). The network is trained on the GPU by the library's bf16
+kernels on ~48k pairs from 8 paths (each frame's prediction and 9 perturbations of its converged pose); 3 held-out
+600-frame paths compare the Gauss-Newton iterations each start needs to reach the converged pose within
+1 mm / 0.01 deg, and their final errors.
 
 `--workload localize` measures the batched global localisation instead: a 20.3M-point prior map sampled every
 15 mm on the surfaces of a seeded 40 x 30 x 3 m office (walls with doors, 200 boxes), 256 hypotheses, each with
@@ -79,6 +90,7 @@ ROOM_SEED = 1   # the box room
 PATH_SEED = 31  # the handheld path (a sequence the float64 oracle tracks for the whole 60 s)
 SCAN_SEED = 3
 L2_FLUSH_BYTES = 256 << 20
+SEQ_SKIP = 20  # sequence frames never timed: 1 s at rest and the 1 s ramp to cruise speed
 LOC_SEED = 1          # the office
 LOC_SPACING = 0.015   # prior-map sample spacing: 20.3M points on the office's surfaces
 LOC_HYP = 256
@@ -414,10 +426,11 @@ def _oracle_view(oracle):
 
 # ---- learned start pose ------------------------------------------------------------------------------------------
 
-LEARN_TRAIN_SEEDS = tuple(range(101, 109))  # 8 paths x 625 frames = 5000 frames, 10 pairs each
+LEARN_TRAIN_SEEDS = tuple(range(101, 109))  # 8 paths x 600 frames, 10 pairs per frame
 LEARN_EVAL_SEEDS = (201, 202, 203)
-LEARN_FRAMES = 625
-LEARN_V, LEARN_W = 1.0, 60.0  # the sequence configuration's path limits (cruise 0.7 m/s)
+LEARN_FRAMES = 600
+LEARN_V, LEARN_W = 2.0, 120.0  # path limits: <= 2 m/s (cruise 1.4 m/s), <= 120 deg/s
+LEARN_SIGMA = (0.03, 0.03, 0.03, 0.02, 0.02, 0.02)  # m, rad: perturbations of the converged pose for training
 
 
 def _learn_chunk(args):
@@ -433,7 +446,7 @@ def learn_sequences(seeds, n_frames: int, procs: int | None = None):
     """{seed: (frames, trajectory)} of fast handheld paths in the box room (generated before any CUDA call)."""
     from livox_warp import synth
 
-    procs = procs or min(8, os.cpu_count() or 1)
+    procs = procs or min(16, os.cpu_count() or 1)
     step = max(1, math.ceil(n_frames / 8))
     jobs = [(sd, n_frames, k, min(k + step, n_frames)) for sd in seeds for k in range(0, n_frames, step)]
     with mp.get_context("spawn").Pool(procs) as pool:
@@ -447,11 +460,11 @@ def learn_sequences(seeds, n_frames: int, procs: int | None = None):
 
 
 def run_learned(a, rank: int, world: int, local: int):
+    """The learned start pose against the constant-velocity one, frame by frame (initnet.FrameByFrame)."""
     import torch
 
     from livox_warp import gpu
-    from livox_warp.initnet import InitNet, make_pairs
-    from livox_warp.localize import pose_difference
+    from livox_warp.initnet import FrameByFrame, InitNet
     from livox_warp.odom import Odometry
 
     seqs = learn_sequences(LEARN_TRAIN_SEEDS + LEARN_EVAL_SEEDS, LEARN_FRAMES)
@@ -460,24 +473,19 @@ def run_learned(a, rank: int, world: int, local: int):
     pipe = gpu.Pipeline(ring_capacity=1 << 16, map_capacity=1 << 16, device=device)
     odom = Odometry(pipe, reg_slots=REG_SLOTS, frame_cap=FRAME_CAP)
     odom.reg_voxel = REG_VOXEL
+    fbf = FrameByFrame(odom, nearest=True)
     t0 = time.perf_counter()
-    sigma = (0.02, 0.02, 0.02, 0.012, 0.012, 0.012)
-    all_sets, all_tg, n_frames, vetoed = [], [], 0, 0
+    all_sets, all_tg = [], []
     for sd in LEARN_TRAIN_SEEDS:
         frames, traj = seqs[sd]
-        T0 = traj.poses(np.array([0.5 * FRAME_DT]))[0]
-
-        sets, tg, info = make_pairs(frames, odom, T0, per_frame=10, sigma=sigma, seed=sd, nearest=True)
-        vetoed += info["vetoed"]
+        _, sets, tg = fbf.run(frames, traj.poses, per_frame=10, sigma=LEARN_SIGMA, seed=sd)
         all_sets.append(sets)
         all_tg.append(tg)
-        n_frames += info["frames"]
     sets = torch.cat(all_sets)
     tg = torch.cat(all_tg)
     del all_sets, all_tg
     n_pairs = int(tg.shape[0])
     gen_s = time.perf_counter() - t0
-    # shuffle the pairs once so the held-out tail mixes every path
     perm = torch.randperm(n_pairs, generator=torch.Generator().manual_seed(0)).to(device)
     sets = sets.view(n_pairs, 2, -1, 4).index_select(0, perm).view(2 * n_pairs, -1, 4)
     tg = tg.index_select(0, perm)
@@ -488,50 +496,52 @@ def run_learned(a, rank: int, world: int, local: int):
     torch.cuda.synchronize(device)
     train_s = time.perf_counter() - t1
     del sets
-    # evaluation: each held-out path from the constant-velocity prediction and from the network
     rows = []
     for sd in LEARN_EVAL_SEEDS:
         frames, traj = seqs[sd]
-        T0 = traj.poses(np.array([0.5 * FRAME_DT]))[0]
-        res = {}
-        for mode in ("plain", "learned"):
-            odom.reset(T0)
-            odom.learned_init(net if mode == "learned" else None, nearest=True)
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            ev0.record()
-            for k, (x, at, t) in enumerate(frames):
-                sx, sa, st_, sf = pipe.stage(x, at, t, len(t), 1.0 / FRAME_DT)
-                odom.push(sx, sa, st_, len(t), float(t.min()), float(t.max()))
-            odom.flush()
-            ev1.record()
-            ev1.synchronize()
-            it = odom.iteration_log()
-            err = np.array([pose_difference(traj.poses(np.array([tm]))[0], T) for _, tm, T in odom.traj])
-            res[mode] = {"iters_first_mean": float(it[:, 1].mean()), "iters_last_mean": float(it[:, 2].mean()),
-                         "frames": int(len(it)), "rmse_m": float(np.sqrt((err[:, 0] ** 2).mean())),
-                         "max_m": float(err[:, 0].max()), "rot_rmse_deg": float(np.sqrt((err[:, 1] ** 2).mean())),
-                         "ms_per_frame": ev0.elapsed_time(ev1) / len(frames)}
-        odom.learned_init(None)
-        rows.append({"seed": sd, **{f"{m}_{k}": round(v, 5) for m in res for k, v in res[m].items()}})
+        r, _, _ = fbf.run(frames, traj.poses, net=net)
+        rows.extend(dict(x, seed=sd) for x in r)
     if rank != 0:
         return
-    pl = np.mean([r["plain_iters_first_mean"] for r in rows])
-    le = np.mean([r["learned_iters_first_mean"] for r in rows])
-    line = {"metric": "mean Gauss-Newton iterations of the first registration: constant-velocity / learned start",
-            "value": round(pl / le, 4), "unit": "x fewer iterations", "n_gpus": world, "steps": len(rows),
-            "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "bf16 network (fp32 accumulate), f32/f64 registration", "data": "synthetic",
-            "config": {"workload": f"learned start pose: box room, handheld paths cruising at {0.7 * LEARN_V:.1f} m/s, <= {LEARN_W} deg/s, "
-                                   f"{len(LEARN_TRAIN_SEEDS)} training paths x {LEARN_FRAMES} frames x 10 Gaussian "
-                                   f"perturbations (sigma {sigma}), {len(LEARN_EVAL_SEEDS)} held-out paths",
-                       "pairs": n_pairs, "train_frames": n_frames, "vetoed_frames": vetoed, "epochs": a.learn_epochs,
-                       "batch": 256},
-            "iters_first": {"constant_velocity": round(float(pl), 4), "learned": round(float(le), 4)},
-            "ceiling_note": "from the converged pose itself the registration still runs ~7.9 iterations (the "
-                            "robust-kernel width decays over the first iterations), so no start pose can save more "
-                            "than ~1.5x on this schedule",
-            "eval": rows, "train_loss": [round(x, 4) for x in hist["train"][::max(1, len(hist['train']) // 10)]],
-            "val_loss": [round(x, 4) for x in hist["val"][::max(1, len(hist['val']) // 10)]],
+    ok = [r for r in rows if r["ok"]]
+
+    def mean(key):
+        return float(np.mean([r[key] for r in ok]))
+
+    def pct(key, i, q):
+        return float(np.percentile([r[key][i] for r in ok], q))
+
+    to_cv, to_net = mean("to_acc_cv"), mean("to_acc_net")
+    line = {"metric": "mean Gauss-Newton iterations to reach the converged pose (1 mm / 0.01 deg): constant-velocity "
+                      "start / learned start",
+            "value": round(to_cv / max(to_net, 1e-9), 4), "unit": "x fewer iterations", "n_gpus": world,
+            "steps": len(ok), "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 network (fp32 accumulate), f32/f64 registration", "data": "synthetic",
+            "config": {"workload": f"learned start pose: box room 8x6x3 m, 20 boxes, handheld paths <= {LEARN_V} m/s "
+                                   f"(cruise {0.7 * LEARN_V:.1f}), <= {LEARN_W} deg/s; each frame registered against the "
+                                   "map of the frames before it (at their true poses) from the constant-velocity "
+                                   "prediction and from the network's proposal; the registration from the true pose "
+                                   "is the judge",
+                       "train_paths": len(LEARN_TRAIN_SEEDS), "eval_paths": len(LEARN_EVAL_SEEDS),
+                       "frames_per_path": LEARN_FRAMES, "pairs": n_pairs, "sigma": LEARN_SIGMA,
+                       "epochs": a.learn_epochs, "batch": 256, "max_iter": odom.max_iter},
+            "iterations_to_converged": {"constant_velocity": round(to_cv, 3), "learned": round(to_net, 3)},
+            "iterations_to_own_final": {"constant_velocity": round(mean("to_own_cv"), 3),
+                                        "learned": round(mean("to_own_net"), 3)},
+            "iterations_to_stop_test": {"constant_velocity": round(mean("iters_cv"), 3),
+                                        "learned": round(mean("iters_net"), 3)},
+            "start_error_vs_converged": {"constant_velocity_p50_m_deg": [round(pct("start_cv", 0, 50), 4),
+                                                                         round(pct("start_cv", 1, 50), 3)],
+                                         "learned_p50_m_deg": [round(pct("start_net", 0, 50), 4),
+                                                               round(pct("start_net", 1, 50), 3)]},
+            "final_error_vs_converged": {"constant_velocity_p95_m_deg": [round(pct("final_cv", 0, 95), 5),
+                                                                         round(pct("final_cv", 1, 95), 4)],
+                                         "learned_p95_m_deg": [round(pct("final_net", 0, 95), 5),
+                                                               round(pct("final_net", 1, 95), 4)]},
+            "judge_vs_truth_p50_m_deg": [round(pct("truth_judge", 0, 50), 4), round(pct("truth_judge", 1, 50), 3)],
+            "frames_evaluated": len(ok), "frames_failed": len(rows) - len(ok),
+            "train_loss": [round(x, 4) for x in hist["train"][::max(1, len(hist["train"]) // 10)]],
+            "val_loss": [round(x, 4) for x in hist["val"][::max(1, len(hist["val"]) // 10)]],
             "pair_gen_s": round(gen_s, 2), "train_s": round(train_s, 2),
             "train_pairs_per_s": round(n_pairs * a.learn_epochs / max(train_s, 1e-9), 1)}
     print(json.dumps(line))
@@ -1504,31 +1514,35 @@ def main():
     if a.workload == "prior":
         run_prior(a, rank, world, local)
         return
-    n_frames = a.warmup + a.steps + 1
+    # the at-rest second and the first second of motion (the ramp to cruise speed) are never timed
+    skip = max(a.warmup, SEQ_SKIP)
+    n_frames = skip + a.steps + 1
     metric = "ICP sequence odometry frames/s (deskew + GN ICP + keyframe insert + map insert + carve)"
     config = {"workload": "sequence odometry: box room 8x6x3 m, 20 boxes, rosette 100k pts/s (~10k pts/frame), "
                           "handheld spline <=1 m/s <=60 deg/s, reg voxel 0.15 m (2^21 slots), "
                           "integration voxel 0.1 m (2^22 slots), carve every ray",
-              "frames": n_frames, "points_per_frame": None, "l2": "flushed between steps (256 MB write)",
+              "frames": n_frames, "timed_frames": [skip, skip + a.steps - 1], "points_per_frame": None,
+              "l2": "flushed between steps (256 MB write)",
               "parallelism": f"replicas x{a.gpus}"}
 
     if a.impl == "reference":
         if rank != 0:
             return
         frames, traj = workload(n_frames)
+        config["points_per_frame"] = int(np.mean([len(f[2]) for f in frames]))
         from oracle import oracle as _o
 
         threads = _o.host_cores()
         budget = max(30.0, min(150.0, 0.25 * a.steps))
-        timed, secs, _ = cpu_pipeline(frames, traj, a.warmup, budget, a.steps, threads)
+        timed, secs, _ = cpu_pipeline(frames, traj, skip, budget, a.steps, threads)
         v = timed / secs
         line = {"impl": "reference", "metric": metric, "value": round(v, 3), "unit": "frames/s", "n_gpus": a.gpus,
                 "steps": timed, "warmup": a.warmup, "ms_per_step": round(1e3 * secs / max(timed, 1), 3),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
                 "data": "synthetic", "config": config,
                 "cpu_baseline": {"value": round(v, 3), "unit": "frames/s", "cores": threads, "kind": "port",
-                                 "sample": f"frames {a.warmup}..{a.warmup + timed - 1} of the sequence after "
-                                           f"{a.warmup} untimed frames; NVIDIA Warp (the reference runtime) is not "
+                                 "sample": f"frames {skip}..{skip + timed - 1} of the sequence after "
+                                           f"{skip} untimed frames; NVIDIA Warp (the reference runtime) is not "
                                            "installed, so this is the CPU restatement of its kernels and host "
                                            "solve"},
                 "e2e": {"value": round(v, 3), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -1550,12 +1564,12 @@ def main():
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(device)
-    res = run_device(frames, traj, a.warmup, a.steps, device, clocks)
+    res = run_device(frames, traj, skip, a.steps, device, clocks)
     ms_total = max_over_ranks(float(res["step_ms"].sum()), device)
     value = replica_rate(a.steps, world, ms_total)
     e2e = None
     if not a.no_e2e:
-        e = run_e2e(frames, traj, a.warmup, a.steps, device)
+        e = run_e2e(frames, traj, skip, a.steps, device)
         e_ms = max_over_ranks(e["ms"], device)
         e2e = {"value": round(replica_rate(a.steps, world, e_ms), 3), "unit": "frames/s",
                "h2d_bytes_per_step": e["h2d"], "d2h_bytes_per_step": e["d2h"]}
@@ -1564,12 +1578,12 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
-    roof = roofline(res, frames, traj, a.warmup, a.steps, measured_peak())
+    roof = roofline(res, frames, traj, skip, a.steps, measured_peak())
     from oracle import oracle as _o
 
     threads = _o.host_cores()
     n_cpu = max(3, min(60, a.steps))
-    timed, secs, opose = cpu_pipeline(frames, traj, a.warmup, a.cpu_budget, n_cpu, threads)
+    timed, secs, opose = cpu_pipeline(frames, traj, skip, a.cpu_budget, n_cpu, threads)
     pts = config["points_per_frame"]
     drift = pose_drift(res["odom"], traj, opose)
     line = {"metric": metric, "value": round(value, 3), "unit": "frames/s", "n_gpus": world, "steps": a.steps,
@@ -1580,7 +1594,7 @@ def main():
                                 round(float(np.percentile(res["step_ms"], 99)), 4)],
             "roofline": roof,
             "cpu_baseline": {"value": round(timed / secs, 3), "unit": "frames/s", "cores": threads, "kind": "port",
-                             "sample": f"{timed} frames ({a.warmup}..{a.warmup + timed - 1}) of the same sequence "
+                             "sample": f"{timed} frames ({skip}..{skip + timed - 1}) of the same sequence "
                                        f"through the CPU oracle (C++/OpenMP kernels + numpy float64 solve), "
                                        f"{secs:.1f} s"},
             "e2e": e2e, "gpu_launches": int(res["launches"]), "clocks": res["clocks"], "pose_drift": drift}

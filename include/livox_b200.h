@@ -44,6 +44,7 @@ extern "C" {
 #define LW_REG_CAP 4096              /* points a registration voxel sums (odom.py:83) */
 #define LW_MAP_CAP 4096              /* points an integration voxel sums (gpu.py:55) */
 #define LW_ACC_STRIDE 64             /* entries of one Gauss-Newton accumulator (odom.py:72-82) */
+#define LW_GN_TRACE 17               /* poses a Gauss-Newton trace holds: the start and up to 16 iterations */
 #define LW_REC_FLOATS 20             /* floats of a registration voxel's derived record */
 #define LW_POSE_SLOTS 65536          /* pose table entries (gpu.py:56) */
 
@@ -155,6 +156,8 @@ typedef struct lw_gn_scratch {
     int32_t spin_budget; /* barrier wait limit in ~100 ns sleeps; 0 = the default (~2 s) */
     int32_t skip_cta;  /* failure injection for tests of the bounded wait: this CTA leaves before the first
                           barrier, so the others time out and the launch reports err = 1; -1 = none */
+    double* trace;     /* NULL, or [LW_GN_TRACE * 12]: the start pose and the pose after each iteration (the top
+                          3 rows of the 4x4, row major), for studies of how fast a registration converges */
 } lw_gn_scratch;
 
 /* Pose table of the Pipeline (gpu.py:1196-1206); written on the device by the odometry. */

@@ -405,15 +405,16 @@ __global__ void k_reg_refresh_all(lw_regmap reg, lw_rec_params rp) {
 }
 
 // =====================================================================================================
-// Gauss-Newton accumulation (odom.py:275-375). A group of G lanes serves one thinned point: the lanes split
-// the (2 reach + 1)^3 neighbour voxels between them (independent probes in flight per lane), reduce to the
-// closest mean in reference order, and the group leader adds the point's weighted terms. The Jacobian is taken
-// about a point near the frame (the predicted sensor position) so float32 keeps its precision far from the
+// Gauss-Newton accumulation (odom.py:275-375). A group of G lanes serves one thinned point: the lanes split the
+// (2 reach + 1)^3 neighbour voxels between them, B probes in flight per lane (G = 16, B = 8 for the 125 voxels of
+// the wide search; G = 8, B = 4 for the 27 of the narrow one, so one batch of independent loads per lane covers a
+// point), reduce to the closest mean in reference order by shuffles, and then split the point's 53 weighted terms
+// between them (a term per lane per G, from the matched voxel's record that every lane reads). The Jacobian is
+// taken about a point near the frame (the predicted sensor position) so float32 keeps its precision far from the
 // world origin; the float64 reduction maps H, b and Hg back to the reference's twist about the world origin.
 // =====================================================================================================
 
 constexpr int GN_THREADS = 256;
-constexpr int GN_G = 16;  // lanes per point
 constexpr int NTERMS = 53;
 
 struct IcpPose {
@@ -438,14 +439,14 @@ __device__ __forceinline__ int probe_rest(int64_t key, int h, int mask, const in
     return -1;
 }
 
-template <int R>
+// The closest occupied voxel mean among this lane's share (offsets lane_g, lane_g + G, ...) of the neighbourhood.
+template <int R, int G, int B>
 __device__ __forceinline__ void icp_search(int lane_g, float wx, float wy, float wz, const IcpConsts& k,
                                            const int64_t* __restrict__ keys, const float* __restrict__ rec,
                                            float& best_d2, int& best_o, int& best_s) {
     constexpr int S = 2 * R + 1;
     constexpr int N = S * S * S;
-    constexpr int PER = (N + GN_G - 1) / GN_G;
-    constexpr int B = 4;
+    constexpr int PER = (N + G - 1) / G;
     const int bx = ifloor(wx * k.inv_v), by = ifloor(wy * k.inv_v), bz = ifloor(wz * k.inv_v);
 #pragma unroll
     for (int j0 = 0; j0 < PER; j0 += B) {
@@ -456,7 +457,7 @@ __device__ __forceinline__ void icp_search(int lane_g, float wx, float wy, float
         bool val[B];
 #pragma unroll
         for (int u = 0; u < B; ++u) {
-            o[u] = lane_g + (j0 + u) * GN_G;
+            o[u] = lane_g + (j0 + u) * G;
             val[u] = (j0 + u) < PER && o[u] < N;
             if (val[u]) {
                 int dz = o[u] % S - R, dy = (o[u] / S) % S - R, dx = o[u] / (S * S) - R;
@@ -493,95 +494,89 @@ __device__ __forceinline__ void icp_search(int lane_g, float wx, float wy, float
     }
 }
 
-// Accumulate one point's terms (odom.py:233-272, 335-375) into a[NTERMS].
-__device__ __forceinline__ void icp_terms(float* a, const float* __restrict__ rec, int s, float wx, float wy, float wz,
-                                          float lx, float ly, float lz, float range, float kappa2) {
-    const float* rr = rec + (int64_t)s * LW_REC_FLOATS;
-    float4 h0 = __ldg(reinterpret_cast<const float4*>(rr));
-    float4 h1 = __ldg(reinterpret_cast<const float4*>(rr + 4));
-    float4 h2 = __ldg(reinterpret_cast<const float4*>(rr + 8));
-    float4 h3 = __ldg(reinterpret_cast<const float4*>(rr + 12));
-    float4 h4 = __ldg(reinterpret_cast<const float4*>(rr + 16));
-    const float M[6] = {h1.x, h1.y, h1.z, h1.w, h2.x, h2.y};
-    const float Mg[6] = {h2.z, h2.w, h3.x, h3.y, h3.z, h3.w};
-    float r0 = wx - h0.x, r1 = wy - h0.y, r2 = wz - h0.z;
-    // M r
-    float Mr0 = fmaf(M[0], r0, fmaf(M[1], r1, M[2] * r2));
-    float Mr1 = fmaf(M[1], r0, fmaf(M[3], r1, M[4] * r2));
-    float Mr2 = fmaf(M[2], r0, fmaf(M[4], r1, M[5] * r2));
-    float d2 = fmaf(r0, Mr0, fmaf(r1, Mr1, r2 * Mr2));
-    float wgt = 1.0f / (1.0f + d2 / kappa2);
-    wgt = wgt * wgt;  // Geman-McClure
-    float rn = (h4.w > 0.5f) ? fmaf(r0, h4.x, fmaf(r1, h4.y, r2 * h4.z)) : sqrtf(fmaf(r0, r0, fmaf(r1, r1, r2 * r2)));
-    // Jacobian columns (odom.py:305-307) at the re-centred point l
-    const float C[6][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f},
-                           {0.f, -lz, ly},  {lz, 0.f, -lx}, {-ly, lx, 0.f}};
-    float MC[6][3], GC[6][3];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-        MC[q][0] = fmaf(M[0], C[q][0], fmaf(M[1], C[q][1], M[2] * C[q][2]));
-        MC[q][1] = fmaf(M[1], C[q][0], fmaf(M[3], C[q][1], M[4] * C[q][2]));
-        MC[q][2] = fmaf(M[2], C[q][0], fmaf(M[4], C[q][1], M[5] * C[q][2]));
-        GC[q][0] = fmaf(Mg[0], C[q][0], fmaf(Mg[1], C[q][1], Mg[2] * C[q][2]));
-        GC[q][1] = fmaf(Mg[1], C[q][0], fmaf(Mg[3], C[q][1], Mg[4] * C[q][2]));
-        GC[q][2] = fmaf(Mg[2], C[q][0], fmaf(Mg[4], C[q][1], Mg[5] * C[q][2]));
-    }
-    int idx = 0;
-#pragma unroll
-    for (int p = 0; p < 6; ++p)
-#pragma unroll
-        for (int q = p; q < 6; ++q) {
-            a[LW_ACC_H + idx] = fmaf(wgt, fmaf(C[p][0], MC[q][0], fmaf(C[p][1], MC[q][1], C[p][2] * MC[q][2])), a[LW_ACC_H + idx]);
-            a[LW_ACC_HG + idx] = fmaf(wgt, fmaf(C[p][0], GC[q][0], fmaf(C[p][1], GC[q][1], C[p][2] * GC[q][2])), a[LW_ACC_HG + idx]);
-            ++idx;
-        }
-#pragma unroll
-    for (int p = 0; p < 6; ++p)
-        a[LW_ACC_B + p] = fmaf(wgt, fmaf(C[p][0], Mr0, fmaf(C[p][1], Mr1, C[p][2] * Mr2)), a[LW_ACC_B + p]);
-    a[LW_ACC_COUNT] += 1.0f;
-    a[LW_ACC_ERR] = fmaf(wgt, d2, a[LW_ACC_ERR]);
-    a[LW_ACC_RMS] = fmaf(wgt, rn * rn, a[LW_ACC_RMS]);
-    a[LW_ACC_WEIGHT] += wgt;
-    a[LW_ACC_RANGE] += range;
+// Row p of the Jacobian columns at the re-centred point l (odom.py:305-307): e_p for p < 3, then the rows of
+// -[l]x: (0, -lz, ly), (lz, 0, -lx), (-ly, lx, 0).
+__device__ __forceinline__ void jac_row(int p, float lx, float ly, float lz, float& a, float& b, float& c) {
+    a = p == 0 ? 1.0f : (p == 4 ? lz : (p == 5 ? -ly : 0.0f));
+    b = p == 1 ? 1.0f : (p == 3 ? -lz : (p == 5 ? lx : 0.0f));
+    c = p == 2 ? 1.0f : (p == 3 ? ly : (p == 4 ? -lx : 0.0f));
 }
 
-// One accumulation pass of this CTA over its share of the thinned points; writes the CTA's float64 partial.
+// (p, q) of the upper-triangle entries in row-major order, 3 bits each.
+__host__ __device__ constexpr uint64_t triu_code(bool want_p) {
+    uint64_t v = 0;
+    int t = 0;
+    for (int p = 0; p < 6; ++p)
+        for (int q = p; q < 6; ++q) {
+            v |= (uint64_t)(want_p ? p : q) << (3 * t);
+            ++t;
+        }
+    return v;
+}
+constexpr uint64_t TRIU_P = triu_code(true);
+constexpr uint64_t TRIU_Q = triu_code(false);
+
+// What one lane adds for accumulator entry t (LW_ACC_* layout): kind 0 = an entry of H (precision M), 1 = of b,
+// 2 = count, 3 = weighted error, 4 = rms along the tight direction, 5 = weight, 6 = range, 7 = an entry of Hg
+// (the tight precision Mg), 8 = none.
+struct TermSel {
+    int kind, p, q;
+};
+
+__device__ __forceinline__ TermSel term_of(int t) {
+    TermSel r{8, 0, 0};
+    if (t < LW_ACC_B) {
+        r = {0, (int)((TRIU_P >> (3 * t)) & 7), (int)((TRIU_Q >> (3 * t)) & 7)};
+    } else if (t < LW_ACC_COUNT) {
+        r = {1, t - LW_ACC_B, 0};
+    } else if (t < LW_ACC_HG) {
+        r = {2 + (t - LW_ACC_COUNT), 0, 0};
+    } else if (t < NTERMS) {
+        const int u = t - LW_ACC_HG;
+        r = {7, (int)((TRIU_P >> (3 * u)) & 7), (int)((TRIU_Q >> (3 * u)) & 7)};
+    }
+    return r;
+}
+
 // Fixed point of the cross-CTA sums of the Gauss-Newton loop: 2^-16 units. The largest term a frame can produce
 // (rotation block of H: weight 1 x precision <= 2500 m^-2 x lever arm^2 <= 3600 m^2 x 2^18 points) is 2.4e12, so
 // the sum of all CTAs' terms stays below 2^62; a partial that would not fit flags an error instead of wrapping.
 constexpr double GN_FIX = 65536.0;
 constexpr double GN_FIX_MAX = 4.0e18 / 256.0;  // per-CTA bound: 256 CTAs stay below 2^62
 
-__device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P, const IcpConsts& k,
-                         const int64_t* __restrict__ keys, const float* __restrict__ rec, double* __restrict__ part,
-                         long long* __restrict__ fixed = nullptr, int* err = nullptr) {
-    constexpr int GROUPS = GN_THREADS / GN_G;
-    // one row of float accumulators per group, written by the group's leader lane (registers stay free for the
-    // search); summed over the groups in a fixed order at the end
-    __shared__ float gacc[GROUPS][NTERMS + 1];
-    for (int e = threadIdx.x; e < GROUPS * (NTERMS + 1); e += blockDim.x) (&gacc[0][0])[e] = 0.0f;
-    __syncthreads();
+// One accumulation pass of this CTA over its share of the thinned points with groups of G lanes; writes the CTA's
+// float64 partial (part) or adds it in fixed point (fixed).
+template <int R, int G, int B>
+__device__ void icp_pass_g(const float4* __restrict__ ds, int n, const IcpPose& P, const IcpConsts& k,
+                           const int64_t* __restrict__ keys, const float* __restrict__ rec, double* __restrict__ part,
+                           long long* __restrict__ fixed, int* err) {
+    constexpr int GROUPS = GN_THREADS / G;
+    constexpr int TPL = (NTERMS + G - 1) / G;  // terms per lane
+    __shared__ float tacc[GN_THREADS / 8][LW_ACC_STRIDE];
     const int lane = threadIdx.x & 31;
-    const int lane_g = lane & (GN_G - 1);
-    const int gl = threadIdx.x / GN_G;
+    const int lane_g = lane & (G - 1);
+    const int gl = threadIdx.x / G;
     const int group = blockIdx.x * GROUPS + gl;
     const int ngroups = gridDim.x * GROUPS;
-    // groups of one warp may run different trip counts: shuffle within this group's lanes only
-    const unsigned gmask = (GN_G == 32 ? 0xffffffffu : ((1u << GN_G) - 1u)) << (lane & ~(GN_G - 1));
+    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane & ~(G - 1));
+    TermSel sel[TPL];
+    float acc[TPL];
+#pragma unroll
+    for (int u = 0; u < TPL; ++u) {
+        sel[u] = term_of(lane_g + u * G);
+        acc[u] = 0.0f;
+    }
     for (int j = group; j < n; j += ngroups) {
-        float4 p = __ldg(ds + j);
-        float lx = P.R[0] * p.x + P.R[1] * p.y + P.R[2] * p.z + P.tr[0];
-        float ly = P.R[3] * p.x + P.R[4] * p.y + P.R[5] * p.z + P.tr[1];
-        float lz = P.R[6] * p.x + P.R[7] * p.y + P.R[8] * p.z + P.tr[2];
-        float wx = lx + P.c[0], wy = ly + P.c[1], wz = lz + P.c[2];
+        const float4 p = __ldg(ds + j);
+        const float lx = P.R[0] * p.x + P.R[1] * p.y + P.R[2] * p.z + P.tr[0];
+        const float ly = P.R[3] * p.x + P.R[4] * p.y + P.R[5] * p.z + P.tr[1];
+        const float lz = P.R[6] * p.x + P.R[7] * p.y + P.R[8] * p.z + P.tr[2];
+        const float wx = lx + P.c[0], wy = ly + P.c[1], wz = lz + P.c[2];
         float bd = k.max_d2;
         int bo = 0x7FFFFFFF, bs = -1;
-        if (k.reach == 2)
-            icp_search<2>(lane_g, wx, wy, wz, k, keys, rec, bd, bo, bs);
-        else
-            icp_search<1>(lane_g, wx, wy, wz, k, keys, rec, bd, bo, bs);
+        icp_search<R, G, B>(lane_g, wx, wy, wz, k, keys, rec, bd, bo, bs);
 #pragma unroll
-        for (int off = GN_G / 2; off > 0; off >>= 1) {
+        for (int off = G / 2; off > 0; off >>= 1) {
             float od = __shfl_xor_sync(gmask, bd, off);
             int oo = __shfl_xor_sync(gmask, bo, off);
             int os = __shfl_xor_sync(gmask, bs, off);
@@ -591,26 +586,84 @@ __device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P,
                 bs = os;
             }
         }
-        if (lane_g == 0 && bs >= 0) icp_terms(gacc[gl], rec, bs, wx, wy, wz, lx, ly, lz, p.w, k.kappa2);
+        if (bs < 0) continue;  // uniform over the group after the reduction
+        // the matched voxel's record (odom.py:335-368, hoisted to the insert): every lane of the group reads it
+        const float* rr = rec + (int64_t)bs * LW_REC_FLOATS;
+        const float4 h0 = __ldg(reinterpret_cast<const float4*>(rr));
+        const float4 h1 = __ldg(reinterpret_cast<const float4*>(rr + 4));
+        const float4 h2 = __ldg(reinterpret_cast<const float4*>(rr + 8));
+        const float4 h3 = __ldg(reinterpret_cast<const float4*>(rr + 12));
+        const float4 h4 = __ldg(reinterpret_cast<const float4*>(rr + 16));
+        const float M[6] = {h1.x, h1.y, h1.z, h1.w, h2.x, h2.y};
+        const float Mg[6] = {h2.z, h2.w, h3.x, h3.y, h3.z, h3.w};
+        const float r0 = wx - h0.x, r1 = wy - h0.y, r2 = wz - h0.z;
+        const float Mr0 = fmaf(M[0], r0, fmaf(M[1], r1, M[2] * r2));
+        const float Mr1 = fmaf(M[1], r0, fmaf(M[3], r1, M[4] * r2));
+        const float Mr2 = fmaf(M[2], r0, fmaf(M[4], r1, M[5] * r2));
+        const float d2 = fmaf(r0, Mr0, fmaf(r1, Mr1, r2 * Mr2));
+        float wgt = 1.0f / (1.0f + d2 / k.kappa2);
+        wgt = wgt * wgt;  // Geman-McClure
+        const float rn = (h4.w > 0.5f) ? fmaf(r0, h4.x, fmaf(r1, h4.y, r2 * h4.z))
+                                       : sqrtf(fmaf(r0, r0, fmaf(r1, r1, r2 * r2)));
+#pragma unroll
+        for (int u = 0; u < TPL; ++u) {
+            const TermSel& t = sel[u];
+            const float* W = t.kind == 7 ? Mg : M;
+            float ua, ub, uc, va, vb, vc;
+            jac_row(t.p, lx, ly, lz, ua, ub, uc);
+            jac_row(t.q, lx, ly, lz, va, vb, vc);
+            if (t.kind == 1) {
+                va = r0;
+                vb = r1;
+                vc = r2;
+            }
+            // u^T W v with W symmetric, stored xx, xy, xz, yy, yz, zz
+            const float wv0 = fmaf(W[0], va, fmaf(W[1], vb, W[2] * vc));
+            const float wv1 = fmaf(W[1], va, fmaf(W[3], vb, W[4] * vc));
+            const float wv2 = fmaf(W[2], va, fmaf(W[4], vb, W[5] * vc));
+            float x = wgt * fmaf(ua, wv0, fmaf(ub, wv1, uc * wv2));
+            x = t.kind == 2 ? 1.0f : x;
+            x = t.kind == 3 ? wgt * d2 : x;
+            x = t.kind == 4 ? wgt * (rn * rn) : x;
+            x = t.kind == 5 ? wgt : x;
+            x = t.kind == 6 ? p.w : x;
+            acc[u] += t.kind == 8 ? 0.0f : x;
+        }
+    }
+    // the CTA's sums: each term over the groups in a fixed order, in float64
+#pragma unroll
+    for (int u = 0; u < TPL; ++u) {
+        const int t = lane_g + u * G;
+        if (t < LW_ACC_STRIDE) tacc[gl][t] = acc[u];
     }
     __syncthreads();
     if (threadIdx.x < NTERMS) {
-        double s = 0.0;
-#pragma unroll
-        for (int g = 0; g < GROUPS; ++g) s += (double)gacc[g][threadIdx.x];
+        double sum = 0.0;
+#pragma unroll 4
+        for (int g = 0; g < GROUPS; ++g) sum += (double)tacc[g][threadIdx.x];
         if (fixed) {
             // integer atomics commute: every CTA reads back the same exact sum, whatever the arrival order
-            double q = rint(s * GN_FIX);
+            double q = rint(sum * GN_FIX);
             if (!(fabs(q) < GN_FIX_MAX)) {
                 atomicExch(err, 4);
                 q = 0.0;
             }
             atomicAdd((unsigned long long*)(fixed + threadIdx.x), (unsigned long long)(long long)q);
         } else {
-            part[threadIdx.x] = s;
+            part[threadIdx.x] = sum;
         }
     }
     __syncthreads();
+}
+
+__device__ __forceinline__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P, const IcpConsts& k,
+                                         const int64_t* __restrict__ keys, const float* __restrict__ rec,
+                                         double* __restrict__ part, long long* __restrict__ fixed = nullptr,
+                                         int* err = nullptr) {
+    if (k.reach == 2)
+        icp_pass_g<2, 16, 8>(ds, n, P, k, keys, rec, part, fixed, err);
+    else
+        icp_pass_g<1, 8, 4>(ds, n, P, k, keys, rec, part, fixed, err);
 }
 
 __device__ __forceinline__ void sym6_from(const double* up, double* H) {
@@ -983,67 +1036,62 @@ __device__ __forceinline__ void chol6_solve(const double* Lf, const double* rhs,
     }
 }
 
-// A = L L^T (positive definite) and the solution of A x = rhs, with one reciprocal per column: out of line so the
-// factor stays in registers (the caller's register budget is spent on the correspondence search).
-__device__ __noinline__ int chol6_solve_nl(const double* __restrict__ A, const double* __restrict__ rhs, double* x) {
-    double Lf[36], inv[6];
+// A - shift I = L D L^T with L unit lower triangular (Crout order, on the packed lower triangle): no square root,
+// one reciprocal per pivot, and about half the live registers of an L L^T factor. Returns 0 unless every pivot is
+// positive (A - shift I positive definite). L holds the 15 entries below the diagonal, row i from i (i - 1) / 2.
+__device__ __forceinline__ int ldl6(const double* __restrict__ A, double shift, double* L, double* rd) {
+    double D[6];
 #pragma unroll
     for (int j = 0; j < 6; ++j) {
-        double d = A[j * 6 + j];
+        double v[6];
+        double d = A[j * 6 + j] - shift;
 #pragma unroll
-        for (int k = 0; k < j; ++k) d -= Lf[j * 6 + k] * Lf[j * 6 + k];
+        for (int k = 0; k < j; ++k) {
+            v[k] = L[j * (j - 1) / 2 + k] * D[k];
+            d -= L[j * (j - 1) / 2 + k] * v[k];
+        }
         if (!(d > 0.0)) return 0;
-        const double l = sqrt(d);
-        const double r = 1.0 / l;
-        Lf[j * 6 + j] = l;
-        inv[j] = r;
+        D[j] = d;
+        const double r = 1.0 / d;
+        rd[j] = r;
 #pragma unroll
         for (int i = j + 1; i < 6; ++i) {
-            double v = A[i * 6 + j];
+            double x = A[i * 6 + j];
 #pragma unroll
-            for (int k = 0; k < j; ++k) v -= Lf[i * 6 + k] * Lf[j * 6 + k];
-            Lf[i * 6 + j] = v * r;
+            for (int k = 0; k < j; ++k) x -= L[i * (i - 1) / 2 + k] * v[k];
+            L[i * (i - 1) / 2 + j] = x * r;
         }
     }
+    return 1;
+}
+
+// A = L D L^T (positive definite) and the solution of A x = rhs: out of line so the factor stays in registers
+// (the caller's register budget is spent on the correspondence search). 0 when A is not positive definite.
+__device__ __noinline__ int chol6_solve_nl(const double* __restrict__ A, const double* __restrict__ rhs, double* x) {
+    double L[15], rd[6];
+    if (!ldl6(A, 0.0, L, rd)) return 0;
     double y[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
         double v = rhs[i];
 #pragma unroll
-        for (int k = 0; k < i; ++k) v -= Lf[i * 6 + k] * y[k];
-        y[i] = v * inv[i];
+        for (int k = 0; k < i; ++k) v -= L[i * (i - 1) / 2 + k] * y[k];
+        y[i] = v;
     }
 #pragma unroll
     for (int i = 5; i >= 0; --i) {
-        double v = y[i];
+        double v = y[i] * rd[i];
 #pragma unroll
-        for (int k = i + 1; k < 6; ++k) v -= Lf[k * 6 + i] * x[k];
-        x[i] = v * inv[i];
+        for (int k = i + 1; k < 6; ++k) v -= L[k * (k - 1) / 2 + i] * x[k];
+        x[i] = v;
     }
     return 1;
 }
 
-// Whether M - shift I is positive definite (a Cholesky factorisation succeeds), out of line like the solve.
+// Whether M - shift I is positive definite (its L D L^T pivots are all positive), out of line like the solve.
 __device__ __noinline__ int chol6_pd_nl(const double* __restrict__ M, double shift) {
-    double Lf[36];
-#pragma unroll
-    for (int j = 0; j < 6; ++j) {
-        double d = M[j * 6 + j] - shift;
-#pragma unroll
-        for (int k = 0; k < j; ++k) d -= Lf[j * 6 + k] * Lf[j * 6 + k];
-        if (!(d > 0.0)) return 0;
-        const double l = sqrt(d);
-        const double r = 1.0 / l;
-        Lf[j * 6 + j] = l;
-#pragma unroll
-        for (int i = j + 1; i < 6; ++i) {
-            double v = M[i * 6 + j];
-#pragma unroll
-            for (int k = 0; k < j; ++k) v -= Lf[i * 6 + k] * Lf[j * 6 + k];
-            Lf[i * 6 + j] = v * r;
-        }
-    }
-    return 1;
+    double L[15], rd[6];
+    return ldl6(M, shift, L, rd);
 }
 
 // The degenerate branch of odom.py:436-455 (some direction below degen_thr): with G's eigen-decomposition in
@@ -1331,6 +1379,8 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
     const int n = *n_dev;
     if (threadIdx.x == 0) {
         for (int i = 0; i < 16; ++i) S.T[i] = S.Tp[i] = st->T_pred[i];
+        if (gn.trace && blockIdx.x == 0)
+            for (int i = 0; i < 12; ++i) gn.trace[i] = st->T_pred[i];  // the start pose
         S.c[0] = st->T_pred[3];
         S.c[1] = st->T_pred[7];
         S.c[2] = st->T_pred[11];
@@ -1372,6 +1422,8 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
             reinterpret_cast<long long*>(gn.part)[((it + 2) % 3) * LW_ACC_STRIDE + threadIdx.x] = 0;
         gn_reduce_fixed(fixed, S);
         gn_step_block(S, prm);
+        if (gn.trace && blockIdx.x == 0 && threadIdx.x < 12 && it + 1 < LW_GN_TRACE)
+            gn.trace[(it + 1) * 12 + threadIdx.x] = S.T[threadIdx.x];  // the pose after iteration it
         if (threadIdx.x == 0) {
             s_corr = S.corr;
             if (S.status != 2) s_rms = S.rms;

@@ -20,6 +20,7 @@ FIX_R, FIX_RR, FIX_W = 2.0 ** 32, 2.0 ** 40, 2.0 ** 20
 VOX_FIX_ATTR = 2.0 ** 16
 REG_CAP = MAP_CAP = 4096
 ACC_STRIDE = 64
+GN_TRACE = 17  # poses a Gauss-Newton trace holds (LW_GN_TRACE)
 REC_FLOATS = 20
 POSE_SLOTS = 1 << 16
 ACC_H, ACC_B, ACC_COUNT, ACC_ERR, ACC_RMS, ACC_WEIGHT, ACC_RANGE, ACC_HG = 0, 21, 27, 28, 29, 30, 31, 32
@@ -70,7 +71,8 @@ class FrameBuf(C.Structure):
 
 
 class GnScratch(C.Structure):
-    _fields_ = [("part", P), ("bar", P), ("err", P), ("grid", i32), ("spin_budget", i32), ("skip_cta", i32)]
+    _fields_ = [("part", P), ("bar", P), ("err", P), ("grid", i32), ("spin_budget", i32), ("skip_cta", i32),
+                ("trace", P)]
 
 
 class PoseTable(C.Structure):

@@ -257,3 +257,121 @@ def _perturbed(T: np.ndarray, s: np.ndarray) -> np.ndarray:
     out[:3, :3] = R
     out[:3, 3] = T[:3, 3] - R @ s[:3]
     return out
+
+
+# ---- frame by frame: training pairs and the evaluation on paths the registration is judged on ----------------
+
+
+def iterations_to(poses: np.ndarray, target: np.ndarray, tol_m: float = 1e-3, tol_deg: float = 0.01) -> int:
+    """The first Gauss-Newton iteration from which a registration's traced poses (start first) all stay within
+    tol_m / tol_deg of `target`; len(poses) when they never settle there."""
+    def close(T):
+        d = np.linalg.inv(target) @ T
+        ang = math.degrees(np.linalg.norm(Rotation.from_matrix(d[:3, :3]).as_rotvec()))
+        return np.linalg.norm(d[:3, 3]) <= tol_m and ang <= tol_deg
+
+    ok = [close(T) for T in poses]
+    first = len(poses)
+    for i in range(len(poses) - 1, -1, -1):
+        if not ok[i]:
+            break
+        first = i
+    return first
+
+
+def pose_gap(A: np.ndarray, B: np.ndarray) -> tuple:
+    """(metres, degrees) from pose A to pose B."""
+    d = np.linalg.inv(A) @ B
+    return float(np.linalg.norm(d[:3, 3])), float(math.degrees(np.linalg.norm(Rotation.from_matrix(d[:3, :3]).as_rotvec())))
+
+
+class FrameByFrame:
+    """A path's frames registered one at a time against a registration map of the frames before them, inserted at
+    their true poses: each frame from the constant-velocity prediction (the motion between the two previous true
+    poses carried on; deskewed with it), from the network's proposal made at that prediction, and from its true
+    pose -- the converged registration that judges the other two. Both starts see the same map and the same
+    deskewed, thinned frame, so what differs is only where the registration starts (and anchors its prior).
+
+    Drives Odometry.register_frame with its Gauss-Newton trace on; `radius` / `nearest` choose the network's map
+    set as in Odometry.learned_init."""
+
+    def __init__(self, odom, radius: float = 12.0, nearest: bool = True):
+        self.odom = odom
+        self.radius, self.nearest = radius, nearest
+        d = odom.device
+        self.scratch = {"cand": torch.zeros(odom.reg_cap, dtype=torch.int32, device=d),
+                        "tiles": torch.zeros(odom.reg_cap // 1024 + 2, dtype=torch.int32, device=d),
+                        "count": torch.zeros(2, dtype=torch.int32, device=d)}
+        odom._gn.trace_on(True)
+
+    def _register(self, raw4, attr, t_mid, twist, T):
+        Tr, ok, st = self.odom.register_frame(raw4, attr, None, t_mid, twist, T)
+        return Tr, ok, st, self.odom._gn.poses(st["iters"])
+
+    def sets_at(self, T: np.ndarray, out: torch.Tensor):
+        """The network's two point sets for the frame last thinned by register_frame, at pose T, into out."""
+        o = self.odom
+        off = _lib.OdomState.n_ds.offset
+        n_ds = o._state[off:off + 4].view(torch.int32)
+        Td = torch.from_numpy(np.asarray(T, np.float64).reshape(16).copy()).to(o.device)
+        frame_sets(o.ds_xyz, n_ds, o.reg, Td, self.radius, out, self.scratch,
+                   o.reg_voxel if self.nearest else 0.0, o.stream)
+
+    def run(self, frames, truth, net=None, warm: int = 10, per_frame: int = 0, sigma=None, seed: int = 0,
+            tol_m: float = 1e-3, tol_deg: float = 0.01):
+        """Frames [(xyz, attr, t)] of a path and truth(t) -> 4x4 poses. The first `warm` frames only build the map.
+        Without per_frame: each later frame is registered from both starts (the network's: `net`'s proposal, or
+        the prediction itself when net is None) and a row of results is kept. With per_frame > 0: training pairs
+        instead -- the prediction and per_frame - 1 Gaussian perturbations (sigma) of the converged pose, each with
+        its point sets and its step to the converged pose. Returns (rows, sets, targets)."""
+        o = self.odom
+        dt = o.frame_dt
+        rng = np.random.default_rng(seed)
+        rows, sets, targets = [], [], []
+        zero = np.zeros(6, np.float32)
+        o.reset(np.eye(4))
+        for k, (x, a, t) in enumerate(frames):
+            t_mid = (k + 0.5) * dt
+            T_true = truth(np.array([t_mid]))[0]
+            raw4 = torch.from_numpy(np.ascontiguousarray(np.concatenate([x, t[:, None]], 1), dtype=np.float32))
+            raw4 = raw4.to(o.device)
+            at = torch.from_numpy(np.asarray(a).view(np.int32)).to(o.device)
+            if k < max(warm, 2):
+                o.register_frame(raw4, at, None, t_mid, zero, T_true, sync=False)  # deskew only; map at the truth
+                o.insert_frame(o.f_xyz[:len(t)], at, T_true)
+                continue
+            T1, T2 = truth(np.array([t_mid - dt, t_mid - 2 * dt]))
+            delta = np.linalg.inv(T2) @ T1
+            T_cv = T1 @ delta
+            tw = np.concatenate([delta[:3, 3], Rotation.from_matrix(delta[:3, :3]).as_rotvec()]).astype(np.float32)
+            T_star, ok_s, _, _ = self._register(raw4, at, t_mid, tw, T_true)  # the judge
+            if per_frame > 0:
+                if ok_s:
+                    starts = [T_cv] + [_perturbed(T_star, rng.normal(0.0, 1.0, 6) * np.asarray(sigma))
+                                       for _ in range(per_frame - 1)]
+                    buf = torch.zeros((2 * len(starts), P, 4), dtype=torch.float32, device=o.device)
+                    for q, T0 in enumerate(starts):
+                        self.sets_at(T0, buf[2 * q:2 * q + 2])
+                        targets.append(step_between(T0, T_star))
+                    sets.append(buf)
+            else:
+                T_a, ok_a, st_a, tr_a = self._register(raw4, at, t_mid, tw, T_cv)
+                buf = torch.zeros((2, P, 4), dtype=torch.float32, device=o.device)
+                self.sets_at(T_cv, buf)
+                step = net.predict(buf, 1)[0] if net is not None else np.zeros(6)
+                T_l = apply_step(T_cv, step)
+                T_b, ok_b, st_b, tr_b = self._register(raw4, at, t_mid, tw, T_l)
+                rows.append({"k": k, "ok": bool(ok_s and ok_a and ok_b),
+                             "start_cv": pose_gap(T_star, T_cv), "start_net": pose_gap(T_star, T_l),
+                             "final_cv": pose_gap(T_star, T_a), "final_net": pose_gap(T_star, T_b),
+                             "truth_judge": pose_gap(T_true, T_star),
+                             "iters_cv": int(st_a["iters"]), "iters_net": int(st_b["iters"]),
+                             "to_acc_cv": iterations_to(tr_a, T_star, tol_m, tol_deg),
+                             "to_acc_net": iterations_to(tr_b, T_star, tol_m, tol_deg),
+                             "to_own_cv": iterations_to(tr_a, T_a, tol_m, tol_deg),
+                             "to_own_net": iterations_to(tr_b, T_b, tol_m, tol_deg)})
+            o.insert_frame(o.f_xyz[:len(t)], at, T_true)
+        if per_frame > 0:
+            return rows, (torch.cat(sets) if sets else None), torch.tensor(np.array(targets), dtype=torch.float32,
+                                                                          device=o.device)
+        return rows, None, None

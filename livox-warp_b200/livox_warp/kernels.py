@@ -95,7 +95,21 @@ class GnScratch:
         self.bar = torch.zeros(2, dtype=torch.int32, device=d)
         self.err = torch.zeros(1, dtype=torch.int32, device=d)
         self.struct = _lib.GnScratch(_lib.ptr(self.part).value, _lib.ptr(self.bar).value, _lib.ptr(self.err).value,
-                                     self.grid, 0, -1)
+                                     self.grid, 0, -1, None)
+        self.trace = None
+
+    def trace_on(self, on: bool = True):
+        """Record the start pose and the pose after each Gauss-Newton iteration (read with poses())."""
+        if on and self.trace is None:
+            self.trace = torch.zeros(_lib.GN_TRACE * 12, dtype=torch.float64, device=self.part.device)
+        self.struct.trace = _lib.ptr(self.trace).value if on else None
+
+    def poses(self, iters: int) -> np.ndarray:
+        """The traced poses: (iters + 1, 4, 4), the start first (synchronises)."""
+        t = self.trace.cpu().numpy().reshape(_lib.GN_TRACE, 3, 4)[:iters + 1]
+        out = np.tile(np.eye(4), (len(t), 1, 1))
+        out[:, :3, :] = t
+        return out
 
 
 def deskew(raw4: torch.Tensor, t_mid: float, inv_dt: float, twist, stream=None) -> torch.Tensor:
