@@ -337,3 +337,36 @@ def test_score_empty_inputs(room):
     h = torch.zeros((0, 4), dtype=torch.float32, device="cuda")
     score_list(grid, none, h, 12.0, out)
     assert bool((out == 7.0).all())
+
+
+def test_global_search_end_to_end_on_the_device():
+    """GlobalLocalizer.localize (localize.py:616-728) with every stage on the B200: the prior map built by the
+    library from a simulated terrestrial scan (voxel means and normals on the device), the grid flooded on the
+    device, the coarse search with its local maxima, the list scores, the batched ICP and the evaluation. A
+    360-degree scan is placed within 2 cm / 0.3 deg of the truth and the answer is unique; the same search with
+    the oracle answering the device stages (tests/test_localize_host_cpu.py) reaches the same pose within 1 mm."""
+    from livox_warp import prior_map, synth
+    from livox_warp.localize import Localizer, ScanPrep, pose_difference
+
+    sc = synth.box_room(3, size=(9.0, 6.5, 3.2), n_boxes=25, side=(0.3, 2.4))
+    stations = [T[:3, 3] for T in synth.free_poses(sc, 2, 4, z=1.5, margin=0.6)]
+    cloud = synth.tls_scan(sc, stations, seed=0, step_deg=0.5)
+    pm = prior_map.from_points(cloud, voxel=0.02, normal_radius=0.08)
+    loc = Localizer(pm["xyz"], pm["normal"], pm["planarity"])
+    T_true = synth.free_poses(sc, 1, 8, z=1.4, margin=0.6)[0]
+    x = synth.spin_scan(sc, T_true, 80000, 21, noise=0.01)
+    x = x[np.linalg.norm(x, axis=1) > 0.3]
+    T, info = loc.search(x, log=lambda *a: None)
+    dt, dr = pose_difference(T_true, T)
+    assert dt < 0.02 and dr < 0.3, (dt, dr, info["inliers"], info["runner_up"])
+    assert info["unique"] and info["inliers"] > 0.8 and abs(info["up"][2]) > 0.99
+    assert info["times"]["total"] < 30.0
+    # the oracle's stages on the same prepared scan and map
+    prep = ScanPrep(x)
+    og = oracle.PriorGrid(oracle.prior_prepare(pm["xyz"], pm["normal"], pm["planarity"]))
+    pts4 = np.zeros((len(prep.pts), 4), np.float32)
+    pts4[:, :3] = prep.pts
+    T_o, _, _ = og.icp(pts4, np.zeros(1, np.int32), np.full(1, len(pts4), np.int32), T[None].copy(),
+                       ((0.05, 10),))
+    do, ro = pose_difference(T_o[0], T)
+    assert do < 1e-3 and ro < 0.02, (do, ro)
