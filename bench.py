@@ -90,6 +90,10 @@ ROOM_SEED = 1   # the box room
 PATH_SEED = 31  # the handheld path (a sequence the float64 oracle tracks for the whole 60 s)
 SCAN_SEED = 3
 L2_FLUSH_BYTES = 256 << 20
+SEQ_DURATION = 62.1  # s: the handheld path of the 600-frame sequence (the float64 oracle tracks all of it)
+SOAK_S = 0.6  # s of untimed steps after a short timed region, so the clock sampler sees the load
+SEQ_SOAK_FRAMES = 600  # sequence frames generated after the timed ones, for the clock soak
+SEQ_MAX_FRAMES = 620
 SEQ_SKIP = 20  # sequence frames never timed: 1 s at rest and the 1 s ramp to cruise speed
 LOC_SEED = 1          # the office
 LOC_SPACING = 0.015   # prior-map sample spacing: 20.3M points on the office's surfaces
@@ -118,7 +122,7 @@ def workload(n_frames: int, procs: int | None = None):
     """The frames 0 .. n_frames-1 of the sequence (generated in a spawn pool before any CUDA call)."""
     from livox_warp import synth
 
-    duration = max(n_frames * FRAME_DT + 2.0, 62.0)  # the path of the 600-frame sequence, whatever n_frames
+    duration = SEQ_DURATION  # the path of the 600-frame sequence, whatever n_frames
     procs = procs or min(8, os.cpu_count() or 1)
     step = max(1, math.ceil(n_frames / (procs * 4)))
     chunks = [(duration, k, min(k + step, n_frames)) for k in range(0, n_frames, step)]
@@ -149,6 +153,7 @@ class Clocks:
         self.path = tempfile.mktemp(suffix=".csv")
 
     def start(self):
+        """Start sampling; returns once the sampler has written its first row (or after 3 s)."""
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
@@ -156,6 +161,11 @@ class Clocks:
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        t_end = time.time() + 3.0
+        while time.time() < t_end and os.path.getsize(self.path) == 0:
+            time.sleep(0.02)
+        self.skip = sum(1 for _ in open(self.path))  # rows written before the timed region (idle clocks)
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -167,9 +177,9 @@ class Clocks:
             self.proc.kill()
         self.f.close()
         rows = []
-        for line in open(self.path):
+        for i, line in enumerate(open(self.path)):
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
+            if len(parts) >= 9 and i >= getattr(self, "skip", 0):
                 rows.append(parts)
         os.unlink(self.path)
         if not rows:
@@ -234,12 +244,23 @@ def run_device(frames, traj, warmup: int, steps: int, device, clocks: "Clocks | 
         step(warmup + j)
         evs[j][1].record(stream)
     torch.cuda.synchronize(device)
-    clk = clocks.stop() if clocks else None
     launches = _lib.launches()
     _lib.prof_enable(False)
     step_ms = np.array([a.elapsed_time(b) for a, b in evs])
     names = ("gn", "carve", "map_insert", "thin", "reg_insert", "frame_append", "control")
     prof = {n: _lib.prof_read(n) for n in names}
+    clk = None
+    if clocks:
+        # the sequence goes on, untimed, so the clock sampler (100 ms period) sees this load for SOAK_S more
+        k, t_soak = warmup + steps, time.time() + SOAK_S
+        while time.time() < t_soak and k < len(dev):
+            step(k)
+            k += 1
+            if k % 20 == 0:
+                torch.cuda.synchronize(device)
+        torch.cuda.synchronize(device)
+        clk = clocks.stop()
+        clk["window"] = f"the timed frames and {k - warmup - steps} more frames of the sequence"
     odom.flush()
     torch.cuda.synchronize(device)
     return {"step_ms": step_ms, "prof": prof, "launches": launches, "clocks": clk, "odom": odom, "pipe": pipe}
@@ -353,8 +374,11 @@ def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured (MEASURED_PEAKS.json)"}
-    return {"hbm_gbs": 6650.0, "source": "fallback 6.65 TB/s"}
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d.get("bf16_tflops", 1590.0)),
+                "bf16_tflops_sustained": float(d.get("bf16_tflops_sustained", d.get("bf16_tflops", 1400.0))),
+                "source": "measured (MEASURED_PEAKS.json)"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+            "source": "fallback 6.65 TB/s, 1.59 PFLOP/s"}
 
 
 # ---- replicas ---------------------------------------------------------------------------------------------------
@@ -463,7 +487,7 @@ def run_learned(a, rank: int, world: int, local: int):
     """The learned start pose against the constant-velocity one, frame by frame (initnet.FrameByFrame)."""
     import torch
 
-    from livox_warp import gpu
+    from livox_warp import _lib, gpu
     from livox_warp.initnet import FrameByFrame, InitNet
     from livox_warp.odom import Odometry
 
@@ -491,16 +515,46 @@ def run_learned(a, rank: int, world: int, local: int):
     tg = tg.index_select(0, perm)
     net = InitNet(device, seed=0, batch_cap=256)
     torch.cuda.synchronize(device)
+    clocks = Clocks(local)
+    clocks.start()
+    _lib.prof_reset()
+    _lib.prof_enable(True)
     t1 = time.perf_counter()
     hist = net.fit(sets, tg, epochs=a.learn_epochs, batch=256, lr=1e-3, val_frac=0.05)
     torch.cuda.synchronize(device)
     train_s = time.perf_counter() - t1
+    _lib.prof_enable(False)
+    clk = clocks.stop()
+    clk["window"] = "the network's training"
+    fwd_ms, fwd_n = _lib.prof_read("net_forward")
+    # a CPU sample of the same training step: the float64 oracle's forward and backward of a few pairs
+    from oracle import oracle as _o
+
+    w_host = net.w.cpu().numpy().view(np.uint16)
+    sc = net.out_scale.cpu().numpy()
+    n_cpu, cpu_s = 0, 0.0
+    sample = sets.view(n_pairs, 2, -1, 4)[:64].cpu().numpy()
+    tgt = tg[:64].cpu().numpy()
+    t_cpu = time.perf_counter()
+    while n_cpu < len(sample) and time.perf_counter() - t_cpu < 10.0:
+        f = _o.net_forward(w_host, sample[n_cpu:n_cpu + 1].reshape(2, -1, 4), net.in_scale, sc)
+        _o.net_backward(w_host, sample[n_cpu:n_cpu + 1].reshape(2, -1, 4), f, tgt[n_cpu:n_cpu + 1], np.ones(6), sc)
+        n_cpu += 1
+    cpu_s = time.perf_counter() - t_cpu
     del sets
     rows = []
+    _lib.launches(reset=True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
     for sd in LEARN_EVAL_SEEDS:
         frames, traj = seqs[sd]
         r, _, _ = fbf.run(frames, traj.poses, net=net)
         rows.extend(dict(x, seed=sd) for x in r)
+    e1.record()
+    torch.cuda.synchronize(device)
+    eval_ms = e0.elapsed_time(e1)
+    launches = _lib.launches()
     if rank != 0:
         return
     ok = [r for r in rows if r["ok"]]
@@ -544,6 +598,26 @@ def run_learned(a, rank: int, world: int, local: int):
             "val_loss": [round(x, 4) for x in hist["val"][::max(1, len(hist["val"]) // 10)]],
             "pair_gen_s": round(gen_s, 2), "train_s": round(train_s, 2),
             "train_pairs_per_s": round(n_pairs * a.learn_epochs / max(train_s, 1e-9), 1)}
+    peak = measured_peak()
+    flops = 256 * 2 * 2 * _lib.NET_P * (3 * 64 + 64 * 128 + 128 * 256)  # one training batch's two point sets
+    achieved = flops / (fwd_ms / max(fwd_n, 1) * 1e-3) / 1e12
+    line["roofline"] = {"kernel": "net_forward (k_net_mlp + k_net_head, batch 256)", "bound": "tensor",
+                        "achieved": round(achieved, 2), "peak": peak["bf16_tflops"], "unit": "TFLOP/s",
+                        "frac": round(achieved / peak["bf16_tflops"], 5), "traffic": None,
+                        "peak_source": peak["source"] + " bf16 burst", "launches": int(fwd_n),
+                        "avg_launch_us": round(fwd_ms / max(fwd_n, 1) * 1e3, 2),
+                        "flops_per_launch": flops}
+    line["cpu_baseline"] = {"value": round(n_cpu / max(cpu_s, 1e-9), 3), "unit": "training pairs/s",
+                            "cores": 1, "kind": "port",
+                            "sample": f"{n_cpu} pairs through the float64 oracle's network forward and backward "
+                                      f"({cpu_s:.1f} s); the device trains {line['train_pairs_per_s']} pairs/s"}
+    line["e2e"] = {"value": line["value"], "unit": line["unit"],
+                   "h2d_bytes_per_step": int(np.mean([len(f[2]) for sd in LEARN_EVAL_SEEDS for f in seqs[sd][0]]) * 20),
+                   "d2h_bytes_per_step": 3 * 976 + 3 * 12 * 8 * 17,
+                   "note": "measured through Odometry.register_frame from host frames (each frame copied to the "
+                           f"device and three registrations read back); evaluation {eval_ms / 1e3:.1f} s"}
+    line["gpu_launches"] = int(launches)
+    line["clocks"] = clk
     print(json.dumps(line))
 
 
@@ -671,6 +745,8 @@ def run_frame(a, rank: int, world: int, local: int):
     clocks = Clocks(local)
     clocks.start()
     _lib.launches(reset=True)
+    _lib.prof_reset()
+    _lib.prof_enable(True)
     h2d = d2h = 0
     for j in range(a.steps):
         k = a.warmup + j
@@ -687,6 +763,9 @@ def run_frame(a, rank: int, world: int, local: int):
         d2h += 12 + len(cl) * 40 + 12
     clk = clocks.stop()
     launches = _lib.launches()
+    _lib.prof_enable(False)
+    prof = {n: _lib.prof_read(n) for n in ("gn", "carve", "map_insert", "thin", "reg_insert", "frame_append", "control",
+                                           "map_build", "ground", "cluster")}
     if rank != 0:
         return
     # parity of the last frame's labels: the oracle's ground and clusters on the same visible set
@@ -705,6 +784,11 @@ def run_frame(a, rank: int, world: int, local: int):
     from livox_warp.localize import pose_difference
 
     gt = np.array([pose_difference(traj.poses(np.array([tm]))[0], T) for _, tm, T in recs])
+    top = {n: prof[n] for n in ("gn", "carve", "map_insert")}  # the kernels roofline() has byte counts for
+    roof = roofline({"prof": top, "odom": odom, "pipe": pipe}, frames, traj, a.warmup, a.steps, measured_peak())
+    total_ms = sum(v[0] for v in prof.values())
+    roof["kernel_ms_share"] = {n: round(v[0] / max(total_ms, 1e-9), 4) for n, v in prof.items()}
+    roof["traffic"], roof["traffic_source"] = None, None  # the ncu traffic figures are the sequence's
     line = {"metric": metric, "value": round(float(np.percentile(lh, 50)), 4), "unit": "ms", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(float(lh.mean()), 4),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 solve)",
@@ -717,6 +801,7 @@ def run_frame(a, rank: int, world: int, local: int):
             "labels_bit_exact_last_frame": {"gnd": gnd_ok, "cid": cid_ok},
             "pose_vs_gt": {"rmse_m": round(float(np.sqrt((gt[:, 0] ** 2).mean())), 4),
                            "max_m": round(float(gt[:, 0].max()), 4), "max_deg": round(float(gt[:, 1].max()), 3)},
+            "roofline": roof,
             "cpu_baseline": {"value": round(1e3 * secs / max(timed, 1), 3), "unit": "ms", "cores": threads,
                              "kind": "port", "sample": f"{timed} frames of the same sequence through the CPU oracle "
                                                        f"(odometry, insert, carve, visible set, ground, clusters)"},
@@ -854,11 +939,22 @@ def run_single(a, rank: int, world: int, local: int):
         step(a.warmup + j)
         evs[j][1].record(stream)
     torch.cuda.synchronize(device)
-    clk = clocks.stop()
     launches = _lib.launches()
     _lib.prof_enable(False)
-    step_ms = np.array([e0.elapsed_time(e1) for e0, e1 in evs])
     gn_ms, gn_cnt = _lib.prof_read("gn")
+    # the timed steps last milliseconds, less than the sampler's 100 ms period: the same steps go on, untimed,
+    # for SOAK_S more so that the clock samples see this load
+    t_soak = time.time() + SOAK_S
+    j = 0
+    while time.time() < t_soak:
+        for _ in range(20):
+            flush.fill_(float(j))
+            step(j)
+            j += 1
+        torch.cuda.synchronize(device)
+    clk = clocks.stop()
+    clk["window"] = f"the timed steps and {SOAK_S} s more of the same steps"
+    step_ms = np.array([e0.elapsed_time(e1) for e0, e1 in evs])
     ms_total = max_over_ranks(float(step_ms.sum()), device)
     value = replica_rate(a.steps, world, ms_total)
     # every distinct frame once more, with its result read back: the poses the oracle checks
@@ -1517,6 +1613,7 @@ def main():
     # the at-rest second and the first second of motion (the ramp to cruise speed) are never timed
     skip = max(a.warmup, SEQ_SKIP)
     n_frames = skip + a.steps + 1
+    n_gen = min(max(n_frames + SEQ_SOAK_FRAMES, n_frames), SEQ_MAX_FRAMES)  # frames after the timed ones: the clock soak
     metric = "ICP sequence odometry frames/s (deskew + GN ICP + keyframe insert + map insert + carve)"
     config = {"workload": "sequence odometry: box room 8x6x3 m, 20 boxes, rosette 100k pts/s (~10k pts/frame), "
                           "handheld spline <=1 m/s <=60 deg/s, reg voxel 0.15 m (2^21 slots), "
@@ -1549,7 +1646,7 @@ def main():
         print(json.dumps(line))
         return
 
-    frames, traj = workload(n_frames)  # before any CUDA call (spawn pool)
+    frames, traj = workload(n_gen)  # before any CUDA call (spawn pool)
     config["points_per_frame"] = int(np.mean([len(f[2]) for f in frames]))
     import torch
     import torch.distributed as dist

@@ -293,6 +293,50 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* bar, int* err, int code, 
     return ok_s != 0;
 }
 
+// An arrival-count grid barrier for kernels that meet many times in one launch. *count only grows during a launch
+// (the launcher zeroes it): every CTA adds 1 with release semantics after its writes, and episode e of a grid of G
+// CTAs is over once the count reaches (e + 1) G, read with acquire semantics -- no reset, no generation word, so the
+// last arrival releases the others with its one atomic. While thread 0 waits, thread 32 runs side() (work of
+// this CTA that does not depend on the other CTAs). A wait longer than `budget` spins (~100 ns each) sets *err
+// and returns false; so does a wait during which another CTA gave up.
+struct NoSide {
+    __device__ void operator()() const {}
+};
+
+template <class Side = NoSide>
+__device__ __forceinline__ bool grid_sync(uint32_t* count, uint32_t target, int* err, int code, long long budget,
+                                          const Side& side = Side()) {
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();  // the CTA's writes and atomics before its arrival
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
+        int ok = 1;
+        long long spins = 0;
+        while (true) {
+            uint32_t v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+            if ((int32_t)(v - target) >= 0) break;
+            if (++spins > budget) {
+                atomicExch(err, code);
+                ok = 0;
+                break;
+            }
+            if ((spins & 31) == 0 && *(volatile int*)err != 0) {
+                ok = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+        ok_s = ok;
+    } else if (threadIdx.x == 32) {
+        side();
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
 // ---- grid sizing -----------------------------------------------------------------------------------------
 inline int blocks_for(int64_t n, int threads, int cap = 1 << 20) {
     int64_t b = (n + threads - 1) / threads;

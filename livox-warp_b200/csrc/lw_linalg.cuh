@@ -260,12 +260,15 @@ __device__ __forceinline__ bool lu_solve(const double* A_in, const double* b, do
 // angles, then the quaternion's matrix.
 __device__ __forceinline__ void rotvec_to_mat(const double* rv, double* R) {
     double a2 = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2];
-    double a = sqrt(a2);
     double scale, w;
-    if (a <= 1e-3) {
-        scale = 0.5 - a2 / 48.0 + a2 * a2 / 3840.0;
-        w = cos(0.5 * a);
+    if (a2 <= 1e-2) {
+        // angles up to 0.1 rad (every Gauss-Newton step): the Maclaurin series of sin(a/2)/a and cos(a/2) in a^2,
+        // truncated where the next term is below 1e-20 -- no square root, sine or cosine on the step's chain
+        scale = 0.5 + a2 * (-1.0 / 48.0 + a2 * (1.0 / 3840.0 + a2 * (-1.0 / 645120.0 + a2 * (1.0 / 185794560.0))));
+        w = 1.0 + a2 * (-1.0 / 8.0 + a2 * (1.0 / 384.0 + a2 * (-1.0 / 46080.0 + a2 * (1.0 / 10321920.0 +
+                                                                                   a2 * (-1.0 / 3715891200.0)))));
     } else {
+        const double a = sqrt(a2);
         scale = sin(0.5 * a) / a;
         w = cos(0.5 * a);
     }

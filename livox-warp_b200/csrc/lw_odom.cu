@@ -405,11 +405,12 @@ __global__ void k_reg_refresh_all(lw_regmap reg, lw_rec_params rp) {
 }
 
 // =====================================================================================================
-// Gauss-Newton accumulation (odom.py:275-375). A group of G lanes serves one thinned point: the lanes split the
-// (2 reach + 1)^3 neighbour voxels between them, B probes in flight per lane (G = 16, B = 8 for the 125 voxels of
-// the wide search; G = 8, B = 4 for the 27 of the narrow one, so one batch of independent loads per lane covers a
-// point), reduce to the closest mean in reference order by shuffles, and then split the point's 53 weighted terms
-// between them (a term per lane per G, from the matched voxel's record that every lane reads). The Jacobian is
+// Gauss-Newton accumulation (odom.py:275-375). A group of G = 8 lanes serves one thinned point: the lanes split the
+// (2 reach + 1)^3 neighbour voxels between them, B probes in flight per lane (B = 8: two batches of independent
+// loads cover the 125 voxels of the wide search; B = 4: one batch the 27 of the narrow one; with 4736 groups a
+// frame's points need a single round), reduce to the closest mean in reference order by shuffles, and then split
+// the point's 53 weighted terms between them by column pairs of H and Hg (term_index), from the matched voxel's
+// record that every lane reads. The Jacobian is
 // taken about a point near the frame (the predicted sensor position) so float32 keeps its precision far from the
 // world origin; the float64 reduction maps H, b and Hg back to the reference's twist about the world origin.
 // =====================================================================================================
@@ -424,7 +425,7 @@ struct IcpPose {
 };
 
 struct IcpConsts {
-    float inv_v, max_d2, kappa2;
+    float inv_v, max_d2, kappa2, inv_kappa2;
     int reach, mask;
 };
 
@@ -502,40 +503,35 @@ __device__ __forceinline__ void jac_row(int p, float lx, float ly, float lz, flo
     c = p == 2 ? 1.0f : (p == 3 ? ly : (p == 4 ? -lx : 0.0f));
 }
 
-// (p, q) of the upper-triangle entries in row-major order, 3 bits each.
-__host__ __device__ constexpr uint64_t triu_code(bool want_p) {
-    uint64_t v = 0;
-    int t = 0;
-    for (int p = 0; p < 6; ++p)
-        for (int q = p; q < 6; ++q) {
-            v |= (uint64_t)(want_p ? p : q) << (3 * t);
-            ++t;
+// How a group of 8 lanes splits a point's 53 accumulator terms, 7 per lane: lanes 0-2 take column pairs (0, 5),
+// (1, 4), (2, 3) of H = sum w J^T M J (1 + 6, 2 + 5, 3 + 4 upper-triangle entries), lanes 3-5 the same of Hg
+// (precision Mg), lane 6 b = sum w J^T M r and the count, lane 7 the weighted error, rms, weight and range. Each of
+// lanes 0-6 forms its two matrix-vector products W v once and then dots them with the Jacobian rows.
+constexpr int TERM_LANES = 8;
+constexpr int TERMS_PER_LANE = 7;
+
+__device__ __forceinline__ int triu6(int p, int q) { return p * 6 - (p * (p - 1)) / 2 + (q - p); }
+
+// Accumulator index of lane lg's term u (LW_ACC_* layout), -1 for none; p / q receive the H entry's row / column.
+__device__ __forceinline__ int term_index(int lg, int u, int& p, int& q) {
+    p = 0;
+    q = 0;
+    if (lg < 6) {
+        const int qa = lg % 3, qb = 5 - qa;
+        if (u <= qa) {
+            p = u;
+            q = qa;
+        } else {
+            p = u - qa - 1;
+            q = qb;
         }
-    return v;
-}
-constexpr uint64_t TRIU_P = triu_code(true);
-constexpr uint64_t TRIU_Q = triu_code(false);
-
-// What one lane adds for accumulator entry t (LW_ACC_* layout): kind 0 = an entry of H (precision M), 1 = of b,
-// 2 = count, 3 = weighted error, 4 = rms along the tight direction, 5 = weight, 6 = range, 7 = an entry of Hg
-// (the tight precision Mg), 8 = none.
-struct TermSel {
-    int kind, p, q;
-};
-
-__device__ __forceinline__ TermSel term_of(int t) {
-    TermSel r{8, 0, 0};
-    if (t < LW_ACC_B) {
-        r = {0, (int)((TRIU_P >> (3 * t)) & 7), (int)((TRIU_Q >> (3 * t)) & 7)};
-    } else if (t < LW_ACC_COUNT) {
-        r = {1, t - LW_ACC_B, 0};
-    } else if (t < LW_ACC_HG) {
-        r = {2 + (t - LW_ACC_COUNT), 0, 0};
-    } else if (t < NTERMS) {
-        const int u = t - LW_ACC_HG;
-        r = {7, (int)((TRIU_P >> (3 * u)) & 7), (int)((TRIU_Q >> (3 * u)) & 7)};
+        return (lg < 3 ? LW_ACC_H : LW_ACC_HG) + triu6(p, q);
     }
-    return r;
+    if (lg == 6) {
+        p = u;
+        return u < 6 ? LW_ACC_B + u : LW_ACC_COUNT;
+    }
+    return u < 4 ? LW_ACC_ERR + u : -1;  // err, rms, weight, range
 }
 
 // Fixed point of the cross-CTA sums of the Gauss-Newton loop: 2^-16 units. The largest term a frame can produce
@@ -551,21 +547,18 @@ __device__ void icp_pass_g(const float4* __restrict__ ds, int n, const IcpPose& 
                            const int64_t* __restrict__ keys, const float* __restrict__ rec, double* __restrict__ part,
                            long long* __restrict__ fixed, int* err) {
     constexpr int GROUPS = GN_THREADS / G;
-    constexpr int TPL = (NTERMS + G - 1) / G;  // terms per lane
-    __shared__ float tacc[GN_THREADS / 8][LW_ACC_STRIDE];
+    constexpr int TPL = TERMS_PER_LANE;  // terms per lane
+    static_assert(G == TERM_LANES, "the terms are split over groups of 8 lanes");
+    __shared__ float tacc[GN_THREADS / 32][LW_ACC_STRIDE];
     const int lane = threadIdx.x & 31;
     const int lane_g = lane & (G - 1);
     const int gl = threadIdx.x / G;
     const int group = blockIdx.x * GROUPS + gl;
     const int ngroups = gridDim.x * GROUPS;
     const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane & ~(G - 1));
-    TermSel sel[TPL];
     float acc[TPL];
 #pragma unroll
-    for (int u = 0; u < TPL; ++u) {
-        sel[u] = term_of(lane_g + u * G);
-        acc[u] = 0.0f;
-    }
+    for (int u = 0; u < TPL; ++u) acc[u] = 0.0f;
     for (int j = group; j < n; j += ngroups) {
         const float4 p = __ldg(ds + j);
         const float lx = P.R[0] * p.x + P.R[1] * p.y + P.R[2] * p.z + P.tr[0];
@@ -601,46 +594,61 @@ __device__ void icp_pass_g(const float4* __restrict__ ds, int n, const IcpPose& 
         const float Mr1 = fmaf(M[1], r0, fmaf(M[3], r1, M[4] * r2));
         const float Mr2 = fmaf(M[2], r0, fmaf(M[4], r1, M[5] * r2));
         const float d2 = fmaf(r0, Mr0, fmaf(r1, Mr1, r2 * Mr2));
-        float wgt = 1.0f / (1.0f + d2 / k.kappa2);
+        float wgt = __frcp_rn(fmaf(d2, k.inv_kappa2, 1.0f));
         wgt = wgt * wgt;  // Geman-McClure
         const float rn = (h4.w > 0.5f) ? fmaf(r0, h4.x, fmaf(r1, h4.y, r2 * h4.z))
                                        : sqrtf(fmaf(r0, r0, fmaf(r1, r1, r2 * r2)));
+        // this lane's two matrix-vector products: W (M for H and b, Mg for Hg) times its two columns' vectors
+        // (Jacobian rows qa, qb; the residual r for the b lane)
+        const int qa = lane_g % 3, qb = 5 - qa;
+        const float* W = (lane_g >= 3 && lane_g < 6) ? Mg : M;
+        float va, vb, vc, xa, xb, xc;
+        jac_row(qa, lx, ly, lz, va, vb, vc);
+        jac_row(qb, lx, ly, lz, xa, xb, xc);
+        if (lane_g == 6) {
+            va = r0;
+            vb = r1;
+            vc = r2;
+        }
+        const float wa0 = fmaf(W[0], va, fmaf(W[1], vb, W[2] * vc));
+        const float wa1 = fmaf(W[1], va, fmaf(W[3], vb, W[4] * vc));
+        const float wa2 = fmaf(W[2], va, fmaf(W[4], vb, W[5] * vc));
+        const float wb0 = fmaf(W[0], xa, fmaf(W[1], xb, W[2] * xc));
+        const float wb1 = fmaf(W[1], xa, fmaf(W[3], xb, W[4] * xc));
+        const float wb2 = fmaf(W[2], xa, fmaf(W[4], xb, W[5] * xc));
 #pragma unroll
         for (int u = 0; u < TPL; ++u) {
-            const TermSel& t = sel[u];
-            const float* W = t.kind == 7 ? Mg : M;
-            float ua, ub, uc, va, vb, vc;
-            jac_row(t.p, lx, ly, lz, ua, ub, uc);
-            jac_row(t.q, lx, ly, lz, va, vb, vc);
-            if (t.kind == 1) {
-                va = r0;
-                vb = r1;
-                vc = r2;
-            }
-            // u^T W v with W symmetric, stored xx, xy, xz, yy, yz, zz
-            const float wv0 = fmaf(W[0], va, fmaf(W[1], vb, W[2] * vc));
-            const float wv1 = fmaf(W[1], va, fmaf(W[3], vb, W[4] * vc));
-            const float wv2 = fmaf(W[2], va, fmaf(W[4], vb, W[5] * vc));
-            float x = wgt * fmaf(ua, wv0, fmaf(ub, wv1, uc * wv2));
-            x = t.kind == 2 ? 1.0f : x;
-            x = t.kind == 3 ? wgt * d2 : x;
-            x = t.kind == 4 ? wgt * (rn * rn) : x;
-            x = t.kind == 5 ? wgt : x;
-            x = t.kind == 6 ? p.w : x;
-            acc[u] += t.kind == 8 ? 0.0f : x;
+            const bool first = lane_g == 6 || u <= qa;
+            const int pr = lane_g == 6 ? u : (u <= qa ? u : u - qa - 1);
+            float ua, ub, uc;
+            jac_row(pr, lx, ly, lz, ua, ub, uc);
+            float x = first ? fmaf(ua, wa0, fmaf(ub, wa1, uc * wa2)) : fmaf(ua, wb0, fmaf(ub, wb1, uc * wb2));
+            x *= wgt;
+            if (lane_g == 6 && u == 6) x = 1.0f;  // the count
+            if (lane_g == 7) x = u == 0 ? wgt * d2 : (u == 1 ? wgt * (rn * rn) : (u == 2 ? wgt : (u == 3 ? p.w : 0.0f)));
+            acc[u] += x;
         }
     }
-    // the CTA's sums: each term over the groups in a fixed order, in float64
+    // the CTA's sums: the groups of a warp by shuffles (a fixed butterfly), then each term over the warps in a
+    // fixed order, in float64
 #pragma unroll
-    for (int u = 0; u < TPL; ++u) {
-        const int t = lane_g + u * G;
-        if (t < LW_ACC_STRIDE) tacc[gl][t] = acc[u];
+    for (int u = 0; u < TPL; ++u)
+#pragma unroll
+        for (int off = G; off < 32; off <<= 1) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], off);
+    const int warp = threadIdx.x >> 5;
+    if (lane < G) {
+#pragma unroll
+        for (int u = 0; u < TPL; ++u) {
+            int tp, tq;
+            const int t = term_index(lane_g, u, tp, tq);
+            if (t >= 0) tacc[warp][t] = acc[u];
+        }
     }
     __syncthreads();
     if (threadIdx.x < NTERMS) {
         double sum = 0.0;
-#pragma unroll 4
-        for (int g = 0; g < GROUPS; ++g) sum += (double)tacc[g][threadIdx.x];
+#pragma unroll
+        for (int w = 0; w < GN_THREADS / 32; ++w) sum += (double)tacc[w][threadIdx.x];
         if (fixed) {
             // integer atomics commute: every CTA reads back the same exact sum, whatever the arrival order
             double q = rint(sum * GN_FIX);
@@ -661,7 +669,7 @@ __device__ __forceinline__ void icp_pass(const float4* __restrict__ ds, int n, c
                                          double* __restrict__ part, long long* __restrict__ fixed = nullptr,
                                          int* err = nullptr) {
     if (k.reach == 2)
-        icp_pass_g<2, 16, 8>(ds, n, P, k, keys, rec, part, fixed, err);
+        icp_pass_g<2, 8, 8>(ds, n, P, k, keys, rec, part, fixed, err);
     else
         icp_pass_g<1, 8, 4>(ds, n, P, k, keys, rec, part, fixed, err);
 }
@@ -731,11 +739,15 @@ __device__ void make_pose(const double* T, const double* c, IcpPose& P) {
     }
 }
 
+// 6 x 0.7^it, the Geman-McClure scale's decay (odom.py:86, 767), by repeated multiplication at compile time
+__host__ __device__ constexpr double kappa_raw(int it) { return it <= 0 ? 6.0 : 0.7 * kappa_raw(it - 1); }
+
 __device__ __forceinline__ void schedule(int it, float voxel, int& reach, float& max_d2, float& kappa) {
     reach = it < 3 ? 2 : 1;  // wide search first, then local refinement (odom.py:765-767)
     float d = ((float)reach + 0.5f) * voxel;
     max_d2 = d * d;
-    kappa = fmaxf(2.0f, (float)(6.0 * pow(0.7, (double)it)));
+    kappa = it >= 4 ? 2.0f : fmaxf(2.0f, (float)(it == 0 ? kappa_raw(0) : it == 1 ? kappa_raw(1)
+                                                 : it == 2 ? kappa_raw(2) : kappa_raw(3)));
 }
 
 // ---- the float64 step (odom.py:772-796) ----------------------------------------------------------------
@@ -934,21 +946,57 @@ struct GnSmem {
     double wv[6][6];                        // the degenerate step's vectors
     int have_v, dstat;                      // EV holds an earlier iteration's vectors; the degenerate step's status
     double T[16], Tp[16], c[3];
-    double L, rms, dmean;
+    double SB0[36], P0[36], P0xi[6];       // from the pose alone, formed while the grid barrier waits
+    double L, invL, rms, dmean;
     int status, corr, degen;
 };
 
-// The cross-CTA sums from the fixed-point accumulator (one load per term); a thread without a term forms the twist
-// from the current pose back to the prediction meanwhile (odom.py:397-401).
+// What the step needs from the current pose alone, formed by one thread while the grid barrier waits: the twist
+// from the current pose back to the prediction (odom.py:397-401), the sensor basis without its 1/L scaling,
+// SB0 = [[R, C R], [0, R]] (C = [c]x, c the sensor position; odom.py:425-433), and the prior's information without
+// its L^2 term, P0 = prior_info [[I, -C], [C, C^T C]] (the closed form of SB^-T SB^-1, R R^T = I), with P0 xi.
+struct StepPrep {
+    GnSmem* S;
+    double prior;
+    __device__ void operator()() const {
+        double Ti[16], Mp[16];
+        mat44_inv_rigid(S->T, Ti);
+        mat44_mul(S->Tp, Ti, Mp);
+        body_twist(Mp, S->xi);
+        const double* T = S->T;
+        const double c0 = T[3], c1 = T[7], c2 = T[11];
+        const double C[9] = {0.0, -c2, c1, c2, 0.0, -c0, -c1, c0, 0.0};
+        const double cc = c0 * c0 + c1 * c1 + c2 * c2;
+        const double cv[3] = {c0, c1, c2};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const double r = T[i * 4 + j];
+                const double cr = C[i * 3 + 0] * T[0 * 4 + j] + C[i * 3 + 1] * T[1 * 4 + j] + C[i * 3 + 2] * T[2 * 4 + j];
+                S->SB0[i * 6 + j] = r;
+                S->SB0[i * 6 + j + 3] = cr;
+                S->SB0[(i + 3) * 6 + j] = 0.0;
+                S->SB0[(i + 3) * 6 + j + 3] = r;
+                S->P0[i * 6 + j] = i == j ? prior : 0.0;
+                S->P0[i * 6 + j + 3] = -prior * C[i * 3 + j];
+                S->P0[(i + 3) * 6 + j] = prior * C[i * 3 + j];
+                S->P0[(i + 3) * 6 + j + 3] = prior * ((i == j ? cc : 0.0) - cv[i] * cv[j]);
+            }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            double x = 0.0;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) x += S->P0[i * 6 + k] * S->xi[k];
+            S->P0xi[i] = x;
+        }
+    }
+};
+
+// The cross-CTA sums from the fixed-point accumulator (one load per term).
 __device__ void gn_reduce_fixed(const long long* __restrict__ fixed, GnSmem& S) {
     const int t = threadIdx.x;
     if (t < LW_ACC_STRIDE) S.v[t] = t < NTERMS ? (double)__ldcg(fixed + t) * (1.0 / GN_FIX) : 0.0;
-    if (t == GN_THREADS - 1) {
-        double Ti[16], Mp[16];
-        mat44_inv_rigid(S.T, Ti);
-        mat44_mul(S.Tp, Ti, Mp);
-        body_twist(Mp, S.xi);
-    }
     __syncthreads();
 }
 
@@ -968,33 +1016,6 @@ __device__ __forceinline__ double kmat(const double* c, int i, int j) {
     return K[i * 3 + j];
 }
 
-// H = A^T H_c A, Hg likewise, b = A^T b_c with A = [[I, -[c]x], [0, I]] (odom.py's twist is about the origin).
-__device__ void gn_world(GnSmem& S) {
-    const int tid = threadIdx.x;
-    if (tid < 72) {
-        const int w = tid / 36, e = tid % 36, p = e / 6, q = e % 6;
-        const double* up = S.v + (w == 0 ? LW_ACC_H : LW_ACC_HG);
-        double x = up[sym_idx(p, q)];
-        if (q >= 3)
-            for (int k = 0; k < 3; ++k) x += up[sym_idx(p, k)] * kmat(S.c, k, q - 3);
-        S.HA[w][e] = x;
-    }
-    __syncthreads();
-    if (tid < 72) {
-        const int w = tid / 36, e = tid % 36, p = e / 6, q = e % 6;
-        double x = S.HA[w][e];
-        if (p >= 3)
-            for (int k = 0; k < 3; ++k) x += kmat(S.c, k, p - 3) * S.HA[w][k * 6 + q];
-        (w == 0 ? S.H : S.Hg)[e] = x;
-    } else if (tid < 78) {
-        const int p = tid - 72;
-        double x = S.v[LW_ACC_B + p];
-        if (p >= 3)
-            for (int k = 0; k < 3; ++k) x += kmat(S.c, k, p - 3) * S.v[LW_ACC_B + k];
-        S.b[p] = x;
-    }
-    __syncthreads();
-}
 
 // Cholesky of a symmetric 6x6 (row major) shifted by -shift on the diagonal, in registers; false unless it is
 // positive definite.
@@ -1227,143 +1248,162 @@ __device__ void gn_degenerate_warp(GnSmem& S, double thr) {
 
 // One Gauss-Newton update of S.T (odom.py:769-796) by the whole block. S.status: 0 continue, 1 converged,
 // 2 too few correspondences, 3 singular.
-__device__ void gn_step_block(GnSmem& S, const lw_odom_params& prm) {
+// -[c]x, entry (k, m), without an indexed local array.
+__device__ __forceinline__ double kneg(const double* c, int k, int m) {
+    return k == m ? 0.0
+                  : (k == 0 ? (m == 1 ? c[2] : -c[1]) : (k == 1 ? (m == 0 ? -c[2] : c[0]) : (m == 0 ? c[1] : -c[0])));
+}
+
+__device__ __forceinline__ void pair_sync() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
+
+// The float64 step of odom.py:772-796 on warps 0 and 1 (the other warps go straight to the block barrier after it):
+// warp 0 maps the sums to the world-origin twist, forms A, rhs and the sensor-basis information G, then its lane 0
+// solves A delta = rhs by L D L^T while thread 32 tests G - thr I for positive definiteness; warp 0 then takes the
+// degenerate step if a direction is below the threshold, and applies the twist. Named barrier 1 orders the two warps.
+__device__ void gn_step_pair(GnSmem& S, const lw_odom_params& prm) {
     const int tid = threadIdx.x;
-    gn_world(S);
-    if (tid == 0) {
-        S.corr = (int)S.v[LW_ACC_COUNT];
-        S.status = S.corr < prm.min_corr ? 2 : 0;
-        S.degen = 0;
-        if (S.status == 0) {
-            S.L = fmax(S.v[LW_ACC_RANGE] / (double)S.corr, 1.0);
-            S.rms = sqrt(fmax(S.v[LW_ACC_RMS], 0.0) / fmax(S.v[LW_ACC_WEIGHT], 1e-9));
-            double dm = 0.0;
-            for (int k = 0; k < 6; ++k) dm += S.H[k * 7];
-            S.dmean = dm / 6.0;  // S.xi (the twist back onto the prediction) was formed during the reduce
+    const int lane = tid & 31;
+    __shared__ int s_g_ok, s_a_ok;
+    if (tid < 32) {
+        // world-origin twist: H = A^T H_c A, Hg likewise, b = A^T b_c with A = [[I, K], [0, I]], K = -[c]x
+        for (int e = lane; e < 72; e += 32) {
+            const int w = e / 36, f = e % 36, p = f / 6, q = f % 6;
+            const double* up = S.v + (w == 0 ? LW_ACC_H : LW_ACC_HG);
+            double x = up[sym_idx(p, q)];
+            if (q >= 3)
+                for (int k = 0; k < 3; ++k) x += up[sym_idx(p, k)] * kneg(S.c, k, q - 3);
+            S.HA[w][f] = x;
         }
-    }
-    __syncthreads();
-    if (S.status != 0) return;
-    if (tid < 36) {
-        const int p = tid / 6, q = tid % 6, bi = p / 3, bj = q / 3, i = p % 3, j = q % 3;
-        double a = S.H[tid];
-        if (p == q) a += 1e-9 * S.dmean + prm.damping * S.H[tid];
-        S.A[tid] = a;
-        // sensor basis (odom.py:425-433): SB = [[R, [c]x R / L], [0, R / L]], SB^-1 = [[R^T, -R^T [c]x], [0, L R^T]]
-        const double c0 = S.T[3], c1 = S.T[7], c2 = S.T[11];
-        const double cx[9] = {0.0, -c2, c1, c2, 0.0, -c0, -c1, c0, 0.0};
-        double sb = 0.0, sbi = 0.0;
-        if (bi == 0 && bj == 0) {
-            sb = S.T[i * 4 + j];
-            sbi = S.T[j * 4 + i];
-        } else if (bi == 0 && bj == 1) {
-            double cr = 0.0, rc = 0.0;
-            for (int k = 0; k < 3; ++k) {
-                cr += cx[i * 3 + k] * S.T[k * 4 + j];
-                rc += S.T[k * 4 + i] * cx[k * 3 + j];
-            }
-            sb = cr / S.L;
-            sbi = -rc;
-        } else if (bi == 1 && bj == 1) {
-            sb = S.T[i * 4 + j] / S.L;
-            sbi = S.L * S.T[j * 4 + i];
-        }
-        S.SB[tid] = sb;
-        S.SBi[tid] = sbi;
-    } else if (tid < 42) {
-        S.rhs[tid - 36] = -S.b[tid - 36];
-    }
-    __syncthreads();
-    if (tid < 36) {
-        const int p = tid / 6, q = tid % 6;
-        double y = 0.0;
-        for (int k = 0; k < 6; ++k) y += S.Hg[p * 6 + k] * S.SB[k * 6 + q];
-        S.tmp[tid] = y;
-        // SBi^T SBi in closed form (R R^T = I): [[I, -C], [C, C^T C + L^2 I]] with C = [c]x
-        const int bi = p / 3, bj = q / 3, i = p % 3, j = q % 3;
-        const double c[3] = {S.T[3], S.T[7], S.T[11]};
-        double x;
-        if (bi == 0 && bj == 0) {
-            x = i == j ? 1.0 : 0.0;
-        } else if (bi == 0) {
-            x = kmat(c, i, j);  // -C[i][j] (kmat holds -C)
-        } else if (bj == 0) {
-            x = -kmat(c, i, j);
-        } else {
-            // (C^T C)[i][j] = |c|^2 delta_ij - c_i c_j
-            x = (i == j ? c[0] * c[0] + c[1] * c[1] + c[2] * c[2] + S.L * S.L : 0.0) - c[i] * c[j];
-        }
-        S.P[tid] = prm.prior_info > 0.0 ? prm.prior_info * x : 0.0;
-    }
-    __syncthreads();
-    if (tid < 36) {
-        const int p = tid / 6, q = tid % 6;
-        double g = 0.0;
-        for (int k = 0; k < 6; ++k) g += S.SB[k * 6 + p] * S.tmp[k * 6 + q];
-        S.G[tid] = g;
-        if (prm.prior_info > 0.0) S.A[tid] += S.P[tid];
-    } else if (tid < 42 && prm.prior_info > 0.0) {
-        const int i = tid - 36;
-        double x = 0.0;
-        for (int k = 0; k < 6; ++k) x += S.P[i * 6 + k] * S.xi[k];
-        S.rhs[i] += x;
-    }
-    __syncthreads();
-    // the degeneracy test (G - thr I positive definite) on another warp while thread 0 factors A
-    __shared__ int s_g_ok;
-    if (tid == 32) s_g_ok = !(prm.degen_thr > 0.0) || chol6_pd_nl(S.G, prm.degen_thr);
-    double delta[6];
-    int a_ok = 0;
-    if (tid == 0) a_ok = chol6_solve_nl(S.A, S.rhs, delta);
-    __syncthreads();
-    if (!s_g_ok) {  // block-uniform: some direction below the threshold, warp 0 takes the degenerate step
-        if (tid < 32) {
-            const bool warm = S.have_v != 0;
-            if (warm) {
-                // start from an earlier iteration's vectors: V^T G V is nearly diagonal, so fewer sweeps
-                for (int e = tid; e < 36; e += 32) {
-                    const int i = e / 6, j = e % 6;
-                    double t = 0.0;
-                    for (int k = 0; k < 6; ++k) t += S.G[i * 6 + k] * S.EV[k * 6 + j];
-                    S.tmp[e] = t;
-                }
-                __syncwarp();
-                for (int e = tid; e < 36; e += 32) {
-                    const int i = e / 6, j = e % 6;
-                    if (i > j) continue;
-                    double t = 0.0;
-                    for (int k = 0; k < 6; ++k) t += S.EV[k * 6 + i] * S.tmp[k * 6 + j];
-                    S.EA[i * 6 + j] = t;
-                    S.EA[j * 6 + i] = t;
-                }
+        __syncwarp();
+        for (int e = lane; e < 78; e += 32) {
+            if (e < 72) {
+                const int w = e / 36, f = e % 36, p = f / 6, q = f % 6;
+                double x = S.HA[w][f];
+                if (p >= 3)
+                    for (int k = 0; k < 3; ++k) x += kneg(S.c, k, p - 3) * S.HA[w][k * 6 + q];
+                (w == 0 ? S.H : S.Hg)[f] = x;
             } else {
-                S.EA[tid] = S.G[tid];
-                if (tid < 4) S.EA[tid + 32] = S.G[tid + 32];
+                const int p = e - 72;
+                double x = S.v[LW_ACC_B + p];
+                if (p >= 3)
+                    for (int k = 0; k < 3; ++k) x += kneg(S.c, k, p - 3) * S.v[LW_ACC_B + k];
+                S.b[p] = x;
+            }
+        }
+        __syncwarp();
+        // the stats (odom.py:769-772): the mean diagonal by a shuffle sum, the mean range L, the rms off the path
+        double dg = lane < 6 ? S.H[lane * 7] : 0.0;
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1) dg += __shfl_xor_sync(0xffffffffu, dg, off);
+        if (lane == 0) {
+            S.corr = (int)S.v[LW_ACC_COUNT];
+            S.status = S.corr < prm.min_corr ? 2 : 0;
+            S.degen = 0;
+            if (S.status == 0) {
+                S.L = fmax(S.v[LW_ACC_RANGE] / (double)S.corr, 1.0);
+                S.invL = 1.0 / S.L;
+                S.dmean = dg / 6.0;
+            }
+        } else if (lane == 1 && S.v[LW_ACC_COUNT] >= prm.min_corr) {
+            S.rms = sqrt(fmax(S.v[LW_ACC_RMS], 0.0) / fmax(S.v[LW_ACC_WEIGHT], 1e-9));
+        }
+        __syncwarp();
+        if (S.status == 0) {
+            // A = H + LM damping + prior, rhs = -b + prior (xi), and tmp = Hg SB0
+            const double pl2 = prm.prior_info > 0.0 ? prm.prior_info * S.L * S.L : 0.0;
+            for (int e = lane; e < 36; e += 32) {
+                const int p = e / 6, q = e % 6;
+                double a = S.H[e];
+                if (p == q) a += 1e-9 * S.dmean + prm.damping * S.H[e];
+                a += S.P0[e];
+                if (p == q && p >= 3) a += pl2;
+                S.A[e] = a;
+                double y = 0.0;
+                for (int k = 0; k < 6; ++k) y += S.Hg[p * 6 + k] * S.SB0[k * 6 + q];
+                S.tmp[e] = y;
+            }
+            if (lane < 6) S.rhs[lane] = -S.b[lane] + S.P0xi[lane] + (lane >= 3 ? pl2 * S.xi[lane] : 0.0);
+            __syncwarp();
+            // G = SB^T Hg SB with SB = SB0 diag(1, 1, 1, 1/L, 1/L, 1/L)
+            for (int e = lane; e < 36; e += 32) {
+                const int p = e / 6, q = e % 6;
+                double g = 0.0;
+                for (int k = 0; k < 6; ++k) g += S.SB0[k * 6 + p] * S.tmp[k * 6 + q];
+                S.G[e] = g * (p >= 3 ? S.invL : 1.0) * (q >= 3 ? S.invL : 1.0);
             }
             __syncwarp();
-            jacobi6_warp<true>(S.EA, S.EV, S.ev, S.rot, warm);
-            if (tid == 0) S.have_v = 1;
-            gn_degenerate_warp(S, prm.degen_thr);
         }
-        __syncthreads();
     }
-    if (tid == 0) {
+    pair_sync();
+    if (S.status != 0) return;  // uniform over the two warps
+    // the degeneracy test on warp 1 while warp 0 solves
+    double delta[6];
+    if (tid == 32) s_g_ok = !(prm.degen_thr > 0.0) || chol6_pd_nl(S.G, prm.degen_thr);
+    if (tid == 0) s_a_ok = chol6_solve_nl(S.A, S.rhs, delta);
+    pair_sync();
+    if (tid >= 32) return;
+    const int g_ok = s_g_ok;
+    if (!g_ok) {
+        // the sensor basis and its inverse, which the degenerate step works in (odom.py:425-433, 436-455)
+        for (int e = lane; e < 36; e += 32) {
+            const int p = e / 6, q = e % 6, i = p % 3, j = q % 3;
+            S.SB[e] = S.SB0[e] * (q >= 3 ? S.invL : 1.0);
+            double sbi = 0.0;
+            if (p < 3 && q < 3) {
+                sbi = S.T[j * 4 + i];
+            } else if (p < 3) {
+                double rc = 0.0;  // (R^T [c]x)[i][j]
+                for (int k = 0; k < 3; ++k) rc -= S.T[k * 4 + i] * kneg(S.c, k, j);
+                sbi = -rc;
+            } else if (q >= 3) {
+                sbi = S.L * S.T[j * 4 + i];
+            }
+            S.SBi[e] = sbi;
+        }
+        __syncwarp();
+        const bool warm = S.have_v != 0;
+        if (warm) {
+            // start from an earlier iteration's vectors: V^T G V is nearly diagonal, so fewer sweeps
+            for (int e = lane; e < 36; e += 32) {
+                const int i = e / 6, j = e % 6;
+                double t = 0.0;
+                for (int k = 0; k < 6; ++k) t += S.G[i * 6 + k] * S.EV[k * 6 + j];
+                S.tmp[e] = t;
+            }
+            __syncwarp();
+            for (int e = lane; e < 36; e += 32) {
+                const int i = e / 6, j = e % 6;
+                if (i > j) continue;
+                double t = 0.0;
+                for (int k = 0; k < 6; ++k) t += S.EV[k * 6 + i] * S.tmp[k * 6 + j];
+                S.EA[i * 6 + j] = t;
+                S.EA[j * 6 + i] = t;
+            }
+        } else {
+            S.EA[lane] = S.G[lane];
+            if (lane < 4) S.EA[lane + 32] = S.G[lane + 32];
+        }
+        __syncwarp();
+        jacobi6_warp<true>(S.EA, S.EV, S.ev, S.rot, warm);
+        if (lane == 0) S.have_v = 1;
+        gn_degenerate_warp(S, prm.degen_thr);
+    }
+    if (lane == 0) {
         int st = 0;
-        if (!s_g_ok) {
+        if (!g_ok) {
             st = S.dstat;
             for (int i = 0; i < 6; ++i) delta[i] = S.delta[i];
-        } else if (!a_ok) {
+        } else if (!s_a_ok) {
             st = 3;
         }
         if (st == 0) {
             apply_twist(S.T, delta);
-            double nt = sqrt(delta[0] * delta[0] + delta[1] * delta[1] + delta[2] * delta[2]);
-            double nr = sqrt(delta[3] * delta[3] + delta[4] * delta[4] + delta[5] * delta[5]);
-            st = (nt < 1e-4 && nr < 1e-4) ? 1 : 0;  // STEP_TOL (odom.py:88)
+            const double nt = delta[0] * delta[0] + delta[1] * delta[1] + delta[2] * delta[2];
+            const double nr = delta[3] * delta[3] + delta[4] * delta[4] + delta[5] * delta[5];
+            st = (nt < 1e-8 && nr < 1e-8) ? 1 : 0;  // |step| < STEP_TOL (odom.py:88), squared
         }
         S.status = st;
     }
-    __syncthreads();
 }
 
 // The whole registration loop (odom.py:752-803) in one cooperative launch. Every CTA reduces the partials
@@ -1409,6 +1449,7 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         float kappa;
         schedule(it, voxel, k.reach, k.max_d2, kappa);
         k.kappa2 = kappa * kappa;
+        k.inv_kappa2 = 1.0f / k.kappa2;
         IcpPose P;
         make_pose(S.T, S.c, P);
         // cross-CTA sums in fixed point, three buffers in turn: iteration `it` adds into buffer it % 3 before the
@@ -1417,11 +1458,15 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         long long* fixed = reinterpret_cast<long long*>(gn.part) + (it % 3) * LW_ACC_STRIDE;
         icp_pass(ds, n, P, k, keys, rec, nullptr, fixed, gn.err);
         if (it == 0 && (int)blockIdx.x == gn.skip_cta) return;  // injected failure: this CTA never arrives
-        if (!grid_barrier(gn.bar, gn.err, 1, budget)) return;
+        // while thread 0 waits, thread 32 prepares what the step needs from the pose alone
+        if (!grid_sync(gn.bar, (uint32_t)(it + 1) * gridDim.x, gn.err, 1, budget,
+                       StepPrep{&S, prm.prior_info > 0.0 ? prm.prior_info : 0.0}))
+            return;
         if (blockIdx.x == 0 && threadIdx.x < LW_ACC_STRIDE)
             reinterpret_cast<long long*>(gn.part)[((it + 2) % 3) * LW_ACC_STRIDE + threadIdx.x] = 0;
         gn_reduce_fixed(fixed, S);
-        gn_step_block(S, prm);
+        if (threadIdx.x < 64) gn_step_pair(S, prm);
+        __syncthreads();
         if (gn.trace && blockIdx.x == 0 && threadIdx.x < 12 && it + 1 < LW_GN_TRACE)
             gn.trace[(it + 1) * 12 + threadIdx.x] = S.T[threadIdx.x];  // the pose after iteration it
         if (threadIdx.x == 0) {
@@ -1885,6 +1930,7 @@ int lw_icp_accumulate(const float* ds4, const int32_t* n_dev, int64_t n_ub, cons
     k.inv_v = (float)(1.0 / (double)voxel);
     k.max_d2 = max_d2;
     k.kappa2 = kappa * kappa;
+    k.inv_kappa2 = 1.0f / k.kappa2;
     k.reach = reach;
     k.mask = (int)(reg->cap - 1);
     k_acc_once<<<grid, GN_THREADS, 0, s>>>(reinterpret_cast<const float4*>(ds4), n_dev, n_ub, P, k, reg->keys,

@@ -283,8 +283,7 @@ class OdomWorker:
             self.gen += 1
             stale = list(self._batches)
             self._batches.clear()
-            self._commands.clear()
-            self._stopping = True
+            self._stopping = True  # the commands already issued still run, then the thread ends
             self._cv.notify()
         for b in stale:
             b.snap.release()
@@ -297,14 +296,14 @@ class OdomWorker:
     # ---- worker thread ----------------------------------------------------------------------------------
 
     def _next(self):
-        """Block until there is work: the next command when no earlier batch waits, else the next batch; None to
-        stop."""
+        """Block until there is work: the next command when no earlier batch waits, else the next batch; None once
+        close() has been called and the commands issued before it have run."""
         with self._cv:
             self._cv.wait_for(lambda: self._stopping or self._batches or self._commands)
-            if self._stopping:
-                return None
             if self._commands and (not self._batches or self._commands[0].after <= self._batches[0].seq):
                 return self._commands.popleft()
+            if self._stopping:
+                return None
             self._running += 1
             return self._batches.popleft()
 

@@ -253,14 +253,38 @@ class Handheld:
         # sample the spline densely, arc-length parametrise, time at a speed profile under v_max
         us = np.linspace(0, len(P) - 3, (len(P) - 3) * 200 + 1)
         xyz = self._spline(us)
+        # a hand does not turn a corner instantly: where the spline kinks at a waypoint, round it off -- resample
+        # every 1 cm of arc length and smooth with a Gaussian of 0.25 m along the path (the ends held)
+        seglen = np.linalg.norm(np.diff(xyz, axis=0), axis=1)
+        s = np.concatenate([[0.0], np.cumsum(seglen)])
+        su = np.arange(0.0, s[-1], 0.01)
+        xyz = np.stack([np.interp(su, s, xyz[:, k]) for k in range(3)], 1)
+        g = np.exp(-0.5 * (np.arange(-75, 76) / 25.0) ** 2)
+        g /= g.sum()
+        pad = np.concatenate([np.repeat(xyz[:1], 75, 0), xyz, np.repeat(xyz[-1:], 75, 0)])
+        xyz = np.stack([np.convolve(pad[:, k], g, mode="valid") for k in range(3)], 1)
         seglen = np.linalg.norm(np.diff(xyz, axis=0), axis=1)
         s = np.concatenate([[0.0], np.cumsum(seglen)])
         T_move = duration - rest
         v = min(v_max * 0.7, s[-1] / max(T_move * 0.6, 1e-3))  # cruise; the spline's bends stay under v_max
         ramp = 0.8  # s to reach cruise speed, so the first moving frames look like a hand starting to move
+        # speed along the path: the cruise speed, slower in bends (sideways acceleration at most a_lat), speeding up
+        # and slowing down at most a_lon (the ramp's), from rest at the start
+        a_lon, a_lat = v / ramp, 2.5 * max(v_max, 1.0)
+        d1 = np.gradient(xyz, s, axis=0)
+        d2 = np.gradient(d1, s, axis=0)
+        kappa = np.linalg.norm(np.cross(d1, d2), axis=1) / np.maximum(np.linalg.norm(d1, axis=1) ** 3, 1e-12)
+        vv = np.minimum(v, np.sqrt(a_lat / np.maximum(kappa, 1e-9)))
+        vv[0] = 0.0
+        ds = np.diff(s)
+        for i in range(1, len(vv)):
+            vv[i] = min(vv[i], math.sqrt(vv[i - 1] ** 2 + 2.0 * a_lon * ds[i - 1]))
+        for i in range(len(vv) - 2, 0, -1):
+            vv[i] = min(vv[i], math.sqrt(vv[i + 1] ** 2 + 2.0 * a_lon * ds[i]))
+        t_of_s = np.concatenate([[0.0], np.cumsum(2.0 * ds / np.maximum(vv[1:] + vv[:-1], 1e-6))])
+
         def s_of(tau):
-            tau = np.clip(tau, 0, None)
-            return np.where(tau < ramp, v * tau * tau / (2 * ramp), v * (tau - ramp / 2))
+            return np.interp(np.clip(tau, 0, None), t_of_s, s)
         self._s, self._xyz, self._s_of = s, xyz, s_of
         # yaw: a handheld scan keeps the room in view -- the sensor points from where it is toward a look-at
         # point that drifts around the room's middle, smoothed over 1 s (causal) and rate-limited to w_max, plus
