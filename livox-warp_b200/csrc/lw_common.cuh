@@ -296,9 +296,12 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* bar, int* err, int code, 
 // An arrival-count grid barrier for kernels that meet many times in one launch. *count only grows during a launch
 // (the launcher zeroes it): every CTA adds 1 with release semantics after its writes, and episode e of a grid of G
 // CTAs is over once the count reaches (e + 1) G, read with acquire semantics -- no reset, no generation word, so the
-// last arrival releases the others with its one atomic. While thread 0 waits, thread 32 runs side() (work of
-// this CTA that does not depend on the other CTAs). A wait longer than `budget` spins (~100 ns each) sets *err
-// and returns false; so does a wait during which another CTA gave up.
+// last arrival releases the others with its one atomic. No separate fences: the block barrier orders the CTA's
+// writes before thread 0's release add (release is cumulative), and the acquire load that sees the final count
+// synchronises with every arrival's release, whose writes the closing block barrier then hands to the whole CTA.
+// While thread 0 waits, thread 32 runs side() (work of this CTA that does not depend on the other CTAs). A wait
+// longer than `budget` spins (~100 ns each) sets *err and returns false; so does a wait during which another CTA
+// gave up.
 struct NoSide {
     __device__ void operator()() const {}
 };
@@ -309,7 +312,6 @@ __device__ __forceinline__ bool grid_sync(uint32_t* count, uint32_t target, int*
     __shared__ int ok_s;
     __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();  // the CTA's writes and atomics before its arrival
         asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
         int ok = 1;
         long long spins = 0;
@@ -328,7 +330,6 @@ __device__ __forceinline__ bool grid_sync(uint32_t* count, uint32_t target, int*
             }
             __nanosleep(32);
         }
-        __threadfence();
         ok_s = ok;
     } else if (threadIdx.x == 32) {
         side();

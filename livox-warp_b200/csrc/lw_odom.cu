@@ -930,16 +930,18 @@ __device__ __noinline__ double conditioning(const double* H) {
     return fmax(lo, 0.0) / fmax(hi, 1e-12);
 }
 
-// ---- the block-cooperative float64 step --------------------------------------------------------------------
+// ---- the float64 step --------------------------------------------------------------------------------------
 // Every CTA of the persistent kernel runs the same step on the same reduced accumulator (so one grid barrier per
-// iteration suffices). The 6x6 products are spread over 36 threads (one element each); the positive-definiteness
-// tests and solves are 6x6 Cholesky factorisations held in registers. Only a frame with a degenerate direction
-// takes the eigen-decomposition path (odom.py:436-455) on one thread.
+// iteration suffices). The step is a chain of dependent float64 operations, so its cost is latency: the 6x6
+// products are one element per thread with compile-time indices and no divergent branches, the positive-
+// definiteness test and the solve are L D L^T factorisations held in registers on two threads of different warps.
+// Only a frame with a degenerate direction takes the eigen-decomposition path (odom.py:436-455).
 
 struct GnSmem {
     double v[LW_ACC_STRIDE];
-    double HA[2][36];
-    double H[36], Hg[36], b[6];
+    double Ac[36];   // [[I, -[c]x], [0, I]]: the re-centred twist's columns in the world-origin twist (per launch)
+    double W[36];    // Ac SB0: the sensor basis (without 1/L) seen from the re-centred twist (per iteration)
+    double H[36], b[6];
     double A[36], SB[36], SBi[36], P[36], tmp[36], G[36];
     double rhs[6], xi[6], delta[6];
     double EA[36], EV[36], ev[6], rot[6];  // the warp eigen-decomposition (degenerate branch, conditioning)
@@ -953,8 +955,9 @@ struct GnSmem {
 
 // What the step needs from the current pose alone, formed by one thread while the grid barrier waits: the twist
 // from the current pose back to the prediction (odom.py:397-401), the sensor basis without its 1/L scaling,
-// SB0 = [[R, C R], [0, R]] (C = [c]x, c the sensor position; odom.py:425-433), and the prior's information without
-// its L^2 term, P0 = prior_info [[I, -C], [C, C^T C]] (the closed form of SB^-T SB^-1, R R^T = I), with P0 xi.
+// SB0 = [[R, C R], [0, R]] (C = [c]x, c the sensor position; odom.py:425-433), the same seen from the twist about
+// the pass centre c0, W = [[I, -[c0]x], [0, I]] SB0 = [[R, [c - c0]x R], [0, R]], and the prior's information
+// without its L^2 term, P0 = prior_info [[I, -C], [C, C^T C]] (the closed form of SB^-T SB^-1, R R^T = I), with P0 xi.
 struct StepPrep {
     GnSmem* S;
     double prior;
@@ -968,16 +971,23 @@ struct StepPrep {
         const double C[9] = {0.0, -c2, c1, c2, 0.0, -c0, -c1, c0, 0.0};
         const double cc = c0 * c0 + c1 * c1 + c2 * c2;
         const double cv[3] = {c0, c1, c2};
+        const double d0 = c0 - S->c[0], d1 = c1 - S->c[1], d2 = c2 - S->c[2];
+        const double D[9] = {0.0, -d2, d1, d2, 0.0, -d0, -d1, d0, 0.0};
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
                 const double r = T[i * 4 + j];
                 const double cr = C[i * 3 + 0] * T[0 * 4 + j] + C[i * 3 + 1] * T[1 * 4 + j] + C[i * 3 + 2] * T[2 * 4 + j];
+                const double dr = D[i * 3 + 0] * T[0 * 4 + j] + D[i * 3 + 1] * T[1 * 4 + j] + D[i * 3 + 2] * T[2 * 4 + j];
                 S->SB0[i * 6 + j] = r;
                 S->SB0[i * 6 + j + 3] = cr;
                 S->SB0[(i + 3) * 6 + j] = 0.0;
                 S->SB0[(i + 3) * 6 + j + 3] = r;
+                S->W[i * 6 + j] = r;
+                S->W[i * 6 + j + 3] = dr;
+                S->W[(i + 3) * 6 + j] = 0.0;
+                S->W[(i + 3) * 6 + j + 3] = r;
                 S->P0[i * 6 + j] = i == j ? prior : 0.0;
                 S->P0[i * 6 + j + 3] = -prior * C[i * 3 + j];
                 S->P0[(i + 3) * 6 + j] = prior * C[i * 3 + j];
@@ -1069,7 +1079,7 @@ __device__ __forceinline__ int ldl6(const double* __restrict__ A, double shift, 
 #pragma unroll
         for (int k = 0; k < j; ++k) {
             v[k] = L[j * (j - 1) / 2 + k] * D[k];
-            d -= L[j * (j - 1) / 2 + k] * v[k];
+            d = fma(-L[j * (j - 1) / 2 + k], v[k], d);
         }
         if (!(d > 0.0)) return 0;
         D[j] = d;
@@ -1079,16 +1089,16 @@ __device__ __forceinline__ int ldl6(const double* __restrict__ A, double shift, 
         for (int i = j + 1; i < 6; ++i) {
             double x = A[i * 6 + j];
 #pragma unroll
-            for (int k = 0; k < j; ++k) x -= L[i * (i - 1) / 2 + k] * v[k];
+            for (int k = 0; k < j; ++k) x = fma(-L[i * (i - 1) / 2 + k], v[k], x);
             L[i * (i - 1) / 2 + j] = x * r;
         }
     }
     return 1;
 }
 
-// A = L D L^T (positive definite) and the solution of A x = rhs: out of line so the factor stays in registers
-// (the caller's register budget is spent on the correspondence search). 0 when A is not positive definite.
-__device__ __noinline__ int chol6_solve_nl(const double* __restrict__ A, const double* __restrict__ rhs, double* x) {
+// The solution of A x = rhs from A = L D L^T (positive definite), in registers when A and rhs are. 0 when A is not
+// positive definite.
+__device__ __forceinline__ int ldl6_solve(const double* __restrict__ A, const double* __restrict__ rhs, double* x) {
     double L[15], rd[6];
     if (!ldl6(A, 0.0, L, rd)) return 0;
     double y[6];
@@ -1096,23 +1106,17 @@ __device__ __noinline__ int chol6_solve_nl(const double* __restrict__ A, const d
     for (int i = 0; i < 6; ++i) {
         double v = rhs[i];
 #pragma unroll
-        for (int k = 0; k < i; ++k) v -= L[i * (i - 1) / 2 + k] * y[k];
+        for (int k = 0; k < i; ++k) v = fma(-L[i * (i - 1) / 2 + k], y[k], v);
         y[i] = v;
     }
 #pragma unroll
     for (int i = 5; i >= 0; --i) {
         double v = y[i] * rd[i];
 #pragma unroll
-        for (int k = i + 1; k < 6; ++k) v -= L[k * (k - 1) / 2 + i] * x[k];
+        for (int k = i + 1; k < 6; ++k) v = fma(-L[k * (k - 1) / 2 + i], x[k], v);
         x[i] = v;
     }
     return 1;
-}
-
-// Whether M - shift I is positive definite (its L D L^T pivots are all positive), out of line like the solve.
-__device__ __noinline__ int chol6_pd_nl(const double* __restrict__ M, double shift) {
-    double L[15], rd[6];
-    return ldl6(M, shift, L, rd);
 }
 
 // The degenerate branch of odom.py:436-455 (some direction below degen_thr): with G's eigen-decomposition in
@@ -1246,8 +1250,6 @@ __device__ void gn_degenerate_warp(GnSmem& S, double thr) {
     __syncwarp();
 }
 
-// One Gauss-Newton update of S.T (odom.py:769-796) by the whole block. S.status: 0 continue, 1 converged,
-// 2 too few correspondences, 3 singular.
 // -[c]x, entry (k, m), without an indexed local array.
 __device__ __forceinline__ double kneg(const double* c, int k, int m) {
     return k == m ? 0.0
@@ -1256,95 +1258,120 @@ __device__ __forceinline__ double kneg(const double* c, int k, int m) {
 
 __device__ __forceinline__ void pair_sync() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
 
-// The float64 step of odom.py:772-796 on warps 0 and 1 (the other warps go straight to the block barrier after it):
-// warp 0 maps the sums to the world-origin twist, forms A, rhs and the sensor-basis information G, then its lane 0
-// solves A delta = rhs by L D L^T while thread 32 tests G - thr I for positive definiteness; warp 0 then takes the
-// degenerate step if a direction is below the threshold, and applies the twist. Named barrier 1 orders the two warps.
+// (p, q) of the 21 upper-triangle entries of a symmetric 6x6 in row-major order (the accumulator's layout), 3 bits
+// each.
+__host__ __device__ constexpr uint64_t triu6_code(bool want_q) {
+    uint64_t v = 0;
+    int t = 0;
+    for (int p = 0; p < 6; ++p)
+        for (int q = p; q < 6; ++q, ++t) v |= (uint64_t)(want_q ? q : p) << (3 * t);
+    return v;
+}
+constexpr uint64_t TRIU6_P = triu6_code(false);
+constexpr uint64_t TRIU6_Q = triu6_code(true);
+__host__ __device__ constexpr int triu6c(int i, int j) {
+    return i <= j ? i * 6 - (i * (i - 1)) / 2 + (j - i) : j * 6 - (j * (j - 1)) / 2 + (i - j);
+}
+
+// u^T M v for a symmetric 6x6 M stored as its packed upper triangle: unrolled, every load of M is a fixed offset and
+// the six row sums are independent chains.
+__device__ __forceinline__ double sym_bilinear(const double* M, const double (&u)[6], const double (&v)[6]) {
+    double r[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double t = 0.0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) t = fma(M[triu6c(i, j)], v[j], t);
+        r[i] = u[i] * t;
+    }
+    return ((r[0] + r[1]) + (r[2] + r[3])) + (r[4] + r[5]);
+}
+
+// A = H + LM damping + prior information and rhs = -b + prior (xi) (odom.py:772-785), formed in registers by one
+// thread and solved by L D L^T; A and rhs also go to shared memory for the degenerate branch. 0 when A is not
+// positive definite.
+__device__ __forceinline__ int gn_solve_thread(GnSmem& S, const lw_odom_params& prm, double* delta) {
+    const double pl2 = prm.prior_info > 0.0 ? prm.prior_info * S.L * S.L : 0.0;
+    const double dmean = ((S.H[0] + S.H[7]) + (S.H[14] + S.H[21]) + (S.H[28] + S.H[35])) / 6.0;
+    S.dmean = dmean;
+    double a[36], rhs[6];
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+#pragma unroll
+        for (int q = p; q < 6; ++q) {
+            double x = S.H[p * 6 + q] + S.P0[p * 6 + q];
+            if (p == q) x += fma(prm.damping, S.H[p * 7], 1e-9 * dmean) + (p >= 3 ? pl2 : 0.0);
+            a[p * 6 + q] = x;
+            a[q * 6 + p] = x;
+            S.A[p * 6 + q] = x;
+            S.A[q * 6 + p] = x;
+        }
+        rhs[p] = -S.b[p] + S.P0xi[p] + (p >= 3 ? pl2 * S.xi[p] : 0.0);
+        S.rhs[p] = rhs[p];
+    }
+    return ldl6_solve(a, rhs, delta);
+}
+
+// One Gauss-Newton update of S.T (odom.py:769-796) on warps 0 and 1 (the other warps go straight to the block
+// barrier after it). S.status: 0 continue, 1 converged, 2 too few correspondences, 3 singular.
+//   1. one output per thread: threads 0-20 the world-origin H = Ac^T Hc Ac (the sums were taken about the pass
+//      centre; odom.py's twist is about the origin), 21-41 the sensor-basis information G = SB^T Hg SB = diag(s)
+//      W^T Hg_c W diag(s) (s = 1, 1, 1, 1/L, 1/L, 1/L), 42-47 b = Ac^T b_c, 48-49 the stats (odom.py:769-772);
+//   2. thread 0 forms A and rhs and solves A delta = rhs by L D L^T while thread 32 tests G - thr I for positive
+//      definiteness the same way;
+//   3. warp 0 takes the degenerate step if a direction is below the threshold, then applies the twist.
+// Named barrier 1 orders the two warps.
 __device__ void gn_step_pair(GnSmem& S, const lw_odom_params& prm) {
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     __shared__ int s_g_ok, s_a_ok;
-    if (tid < 32) {
-        // world-origin twist: H = A^T H_c A, Hg likewise, b = A^T b_c with A = [[I, K], [0, I]], K = -[c]x
-        for (int e = lane; e < 72; e += 32) {
-            const int w = e / 36, f = e % 36, p = f / 6, q = f % 6;
-            const double* up = S.v + (w == 0 ? LW_ACC_H : LW_ACC_HG);
-            double x = up[sym_idx(p, q)];
-            if (q >= 3)
-                for (int k = 0; k < 3; ++k) x += up[sym_idx(p, k)] * kneg(S.c, k, q - 3);
-            S.HA[w][f] = x;
-        }
-        __syncwarp();
-        for (int e = lane; e < 78; e += 32) {
-            if (e < 72) {
-                const int w = e / 36, f = e % 36, p = f / 6, q = f % 6;
-                double x = S.HA[w][f];
-                if (p >= 3)
-                    for (int k = 0; k < 3; ++k) x += kneg(S.c, k, p - 3) * S.HA[w][k * 6 + q];
-                (w == 0 ? S.H : S.Hg)[f] = x;
-            } else {
-                const int p = e - 72;
-                double x = S.v[LW_ACC_B + p];
-                if (p >= 3)
-                    for (int k = 0; k < 3; ++k) x += kneg(S.c, k, p - 3) * S.v[LW_ACC_B + k];
-                S.b[p] = x;
-            }
-        }
-        __syncwarp();
-        // the stats (odom.py:769-772): the mean diagonal by a shuffle sum, the mean range L, the rms off the path
-        double dg = lane < 6 ? S.H[lane * 7] : 0.0;
+    if (tid < 42) {
+        const bool is_h = tid < 21;
+        const int u = is_h ? tid : tid - 21;
+        const int p = (int)((TRIU6_P >> (3 * u)) & 7u), q = (int)((TRIU6_Q >> (3 * u)) & 7u);
+        const double* U = is_h ? S.Ac : S.W;
+        double up[6], uq[6];
 #pragma unroll
-        for (int off = 4; off > 0; off >>= 1) dg += __shfl_xor_sync(0xffffffffu, dg, off);
-        if (lane == 0) {
-            S.corr = (int)S.v[LW_ACC_COUNT];
-            S.status = S.corr < prm.min_corr ? 2 : 0;
-            S.degen = 0;
-            if (S.status == 0) {
-                S.L = fmax(S.v[LW_ACC_RANGE] / (double)S.corr, 1.0);
-                S.invL = 1.0 / S.L;
-                S.dmean = dg / 6.0;
-            }
-        } else if (lane == 1 && S.v[LW_ACC_COUNT] >= prm.min_corr) {
-            S.rms = sqrt(fmax(S.v[LW_ACC_RMS], 0.0) / fmax(S.v[LW_ACC_WEIGHT], 1e-9));
+        for (int i = 0; i < 6; ++i) {
+            up[i] = U[i * 6 + p];
+            uq[i] = U[i * 6 + q];
         }
-        __syncwarp();
-        if (S.status == 0) {
-            // A = H + LM damping + prior, rhs = -b + prior (xi), and tmp = Hg SB0
-            const double pl2 = prm.prior_info > 0.0 ? prm.prior_info * S.L * S.L : 0.0;
-            for (int e = lane; e < 36; e += 32) {
-                const int p = e / 6, q = e % 6;
-                double a = S.H[e];
-                if (p == q) a += 1e-9 * S.dmean + prm.damping * S.H[e];
-                a += S.P0[e];
-                if (p == q && p >= 3) a += pl2;
-                S.A[e] = a;
-                double y = 0.0;
-                for (int k = 0; k < 6; ++k) y += S.Hg[p * 6 + k] * S.SB0[k * 6 + q];
-                S.tmp[e] = y;
-            }
-            if (lane < 6) S.rhs[lane] = -S.b[lane] + S.P0xi[lane] + (lane >= 3 ? pl2 * S.xi[lane] : 0.0);
-            __syncwarp();
-            // G = SB^T Hg SB with SB = SB0 diag(1, 1, 1, 1/L, 1/L, 1/L)
-            for (int e = lane; e < 36; e += 32) {
-                const int p = e / 6, q = e % 6;
-                double g = 0.0;
-                for (int k = 0; k < 6; ++k) g += S.SB0[k * 6 + p] * S.tmp[k * 6 + q];
-                S.G[e] = g * (p >= 3 ? S.invL : 1.0) * (q >= 3 ? S.invL : 1.0);
-            }
-            __syncwarp();
-        }
+        double x = sym_bilinear(S.v + (is_h ? LW_ACC_H : LW_ACC_HG), up, uq);
+        const double iL = 1.0 / fmax(S.v[LW_ACC_RANGE] / S.v[LW_ACC_COUNT], 1.0);
+        x *= is_h ? 1.0 : (p >= 3 ? iL : 1.0) * (q >= 3 ? iL : 1.0);
+        double* out = is_h ? S.H : S.G;
+        out[p * 6 + q] = x;
+        out[q * 6 + p] = x;
+    } else if (tid < 48) {
+        const int p = tid - 42;
+        double x = 0.0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) x = fma(S.Ac[i * 6 + p], S.v[LW_ACC_B + i], x);
+        S.b[p] = x;
+    } else if (tid == 48) {
+        S.corr = (int)S.v[LW_ACC_COUNT];
+        S.status = S.corr < prm.min_corr ? 2 : 0;
+        S.degen = 0;
+        S.L = fmax(S.v[LW_ACC_RANGE] / (double)S.corr, 1.0);
+        S.invL = 1.0 / S.L;
+    } else if (tid == 49 && S.v[LW_ACC_COUNT] >= prm.min_corr) {
+        S.rms = sqrt(fmax(S.v[LW_ACC_RMS], 0.0) / fmax(S.v[LW_ACC_WEIGHT], 1e-9));
     }
     pair_sync();
     if (S.status != 0) return;  // uniform over the two warps
-    // the degeneracy test on warp 1 while warp 0 solves
     double delta[6];
-    if (tid == 32) s_g_ok = !(prm.degen_thr > 0.0) || chol6_pd_nl(S.G, prm.degen_thr);
-    if (tid == 0) s_a_ok = chol6_solve_nl(S.A, S.rhs, delta);
+    if (tid == 0) s_a_ok = gn_solve_thread(S, prm, delta);
+    if (tid == 32) {
+        double Lg[15], rg[6];
+        s_g_ok = !(prm.degen_thr > 0.0) || ldl6(S.G, prm.degen_thr, Lg, rg);
+    }
     pair_sync();
     if (tid >= 32) return;
     const int g_ok = s_g_ok;
     if (!g_ok) {
-        // the sensor basis and its inverse, which the degenerate step works in (odom.py:425-433, 436-455)
+        // the sensor basis and its inverse, which the degenerate step works in (odom.py:425-433, 436-455), at
+        // the current pose's position (not the pass centre S.c, which stays at the prediction)
+        const double cT[3] = {S.T[3], S.T[7], S.T[11]};
         for (int e = lane; e < 36; e += 32) {
             const int p = e / 6, q = e % 6, i = p % 3, j = q % 3;
             S.SB[e] = S.SB0[e] * (q >= 3 ? S.invL : 1.0);
@@ -1353,7 +1380,7 @@ __device__ void gn_step_pair(GnSmem& S, const lw_odom_params& prm) {
                 sbi = S.T[j * 4 + i];
             } else if (p < 3) {
                 double rc = 0.0;  // (R^T [c]x)[i][j]
-                for (int k = 0; k < 3; ++k) rc -= S.T[k * 4 + i] * kneg(S.c, k, j);
+                for (int k = 0; k < 3; ++k) rc -= S.T[k * 4 + i] * kneg(cT, k, j);
                 sbi = -rc;
             } else if (q >= 3) {
                 sbi = S.L * S.T[j * 4 + i];
@@ -1424,6 +1451,9 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         S.c[0] = st->T_pred[3];
         S.c[1] = st->T_pred[7];
         S.c[2] = st->T_pred[11];
+        for (int i = 0; i < 6; ++i)
+            for (int j = 0; j < 6; ++j)
+                S.Ac[i * 6 + j] = i == j ? 1.0 : (i < 3 && j >= 3 ? kneg(S.c, i, j - 3) : 0.0);
         s_iters = 0;
         s_degen = 0;
         s_corr = 0;

@@ -100,3 +100,17 @@ def test_no_cpu_fallback():
             _lib.load(require_cuda=True)
     finally:
         _lib._lib = saved
+
+
+def test_noalloc_thinning_refuses_misaligned_points_without_a_gpu():
+    """lw_thin_noalloc reads and writes float4 points: a pointer off a 16-byte boundary is refused with LW_EINVAL
+    before any device work (so this runs without a GPU; the pointers are never dereferenced)."""
+    from livox_warp import _lib
+
+    lib = _lib.load(require_cuda=False)
+    good, bad = 0x10000, 0x10004
+    for xyz, out in ((bad, good), (good, bad)):
+        rc = lib.lw_thin_noalloc(ctypes.c_void_p(xyz), ctypes.c_void_p(good), 100, 10.0, 0.3, 60.0, 15,
+                                 ctypes.c_void_p(out), ctypes.c_void_p(good), None)
+        assert rc == _lib.LW_EINVAL
+        assert b"16-byte" in lib.lw_last_error()
