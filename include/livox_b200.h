@@ -83,7 +83,7 @@ typedef struct lw_regmap {
     int32_t* bcnt;   /* [cap] scratch, 0 between calls */
     int32_t* first;  /* [cap] scratch, INT32_MAX between calls */
     int32_t* stats;  /* [2] voxels claimed, points that found no slot in the probe window */
-    int64_t cap;     /* slots, a power of two */
+    int64_t cap;     /* slots, a power of two; at most 2^25 for the Gauss-Newton entry points */
 } lw_regmap;
 
 /* What a registration voxel's record is derived with (odom.py:337-368, 759-761). */
@@ -153,7 +153,7 @@ typedef struct lw_gn_scratch {
     uint32_t* bar;     /* [2] grid barrier counter and generation; zeroed by every launch */
     int32_t* err;      /* [1] set when a bounded wait gives up (1) or a fixed-point sum overflows (4); sticky */
     int32_t grid;      /* CTAs (<= the SM count, one per SM) */
-    int32_t spin_budget; /* barrier wait limit in ~100 ns sleeps; 0 = the default (~2 s) */
+    int32_t spin_budget; /* barrier wait limit in polls (~0.1-0.3 us each); 0 = the default (2^24 polls) */
     int32_t skip_cta;  /* failure injection for tests of the bounded wait: this CTA leaves before the first
                           barrier, so the others time out and the launch reports err = 1; -1 = none */
     double* trace;     /* NULL, or [LW_GN_TRACE * 12]: the start pose and the pose after each iteration (the top

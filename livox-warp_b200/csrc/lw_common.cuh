@@ -299,9 +299,10 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* bar, int* err, int code, 
 // last arrival releases the others with its one atomic. No separate fences: the block barrier orders the CTA's
 // writes before thread 0's release add (release is cumulative), and the acquire load that sees the final count
 // synchronises with every arrival's release, whose writes the closing block barrier then hands to the whole CTA.
-// While thread 0 waits, thread 32 runs side() (work of this CTA that does not depend on the other CTAs). A wait
-// longer than `budget` spins (~100 ns each) sets *err and returns false; so does a wait during which another CTA
-// gave up.
+// While thread 0 waits, thread 32 runs side() (work of this CTA that does not depend on the other CTAs). Thread 0
+// polls without sleeping (each poll is one L2 round trip, ~0.2 us), so every CTA leaves within a round trip of the
+// last arrival. A wait longer than `budget` polls sets *err and returns false; so does a wait during which another
+// CTA gave up.
 struct NoSide {
     __device__ void operator()() const {}
 };
@@ -328,7 +329,6 @@ __device__ __forceinline__ bool grid_sync(uint32_t* count, uint32_t target, int*
                 ok = 0;
                 break;
             }
-            __nanosleep(32);
         }
         ok_s = ok;
     } else if (threadIdx.x == 32) {

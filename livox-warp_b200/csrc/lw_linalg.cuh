@@ -264,24 +264,24 @@ __device__ __forceinline__ void rotvec_to_mat(const double* rv, double* R) {
     if (a2 <= 1e-2) {
         // angles up to 0.1 rad (every Gauss-Newton step): the Maclaurin series of sin(a/2)/a and cos(a/2) in a^2,
         // truncated where the next term is below 1e-20 -- no square root, sine or cosine on the step's chain
-        scale = 0.5 + a2 * (-1.0 / 48.0 + a2 * (1.0 / 3840.0 + a2 * (-1.0 / 645120.0 + a2 * (1.0 / 185794560.0))));
-        w = 1.0 + a2 * (-1.0 / 8.0 + a2 * (1.0 / 384.0 + a2 * (-1.0 / 46080.0 + a2 * (1.0 / 10321920.0 +
-                                                                                   a2 * (-1.0 / 3715891200.0)))));
+        scale = fma(a2, fma(a2, fma(a2, fma(a2, 1.0 / 185794560.0, -1.0 / 645120.0), 1.0 / 3840.0), -1.0 / 48.0), 0.5);
+        w = fma(a2, fma(a2, fma(a2, fma(a2, fma(a2, -1.0 / 3715891200.0, 1.0 / 10321920.0), -1.0 / 46080.0),
+                                1.0 / 384.0), -1.0 / 8.0), 1.0);
     } else {
         const double a = sqrt(a2);
         scale = sin(0.5 * a) / a;
         w = cos(0.5 * a);
     }
     double x = rv[0] * scale, y = rv[1] * scale, z = rv[2] * scale;
-    R[0] = 1.0 - 2.0 * (y * y + z * z);
-    R[1] = 2.0 * (x * y - z * w);
-    R[2] = 2.0 * (x * z + y * w);
-    R[3] = 2.0 * (x * y + z * w);
-    R[4] = 1.0 - 2.0 * (x * x + z * z);
-    R[5] = 2.0 * (y * z - x * w);
-    R[6] = 2.0 * (x * z - y * w);
-    R[7] = 2.0 * (y * z + x * w);
-    R[8] = 1.0 - 2.0 * (x * x + y * y);
+    R[0] = fma(-2.0, fma(y, y, z * z), 1.0);
+    R[1] = 2.0 * fma(x, y, -z * w);
+    R[2] = 2.0 * fma(x, z, y * w);
+    R[3] = 2.0 * fma(x, y, z * w);
+    R[4] = fma(-2.0, fma(x, x, z * z), 1.0);
+    R[5] = 2.0 * fma(y, z, -x * w);
+    R[6] = 2.0 * fma(x, z, -y * w);
+    R[7] = 2.0 * fma(y, z, x * w);
+    R[8] = fma(-2.0, fma(x, x, y * y), 1.0);
 }
 
 // Rotation vector of a rotation matrix: quaternion by the largest of (trace, diagonal) (Shepperd's method),
@@ -382,8 +382,9 @@ __device__ __forceinline__ void apply_twist(double* T, const double* delta) {
     rotvec_to_mat(delta + 3, Rz);
     double o[12];
     for (int i = 0; i < 3; ++i) {
-        for (int j = 0; j < 3; ++j) o[i * 4 + j] = Rz[i * 3 + 0] * T[0 * 4 + j] + Rz[i * 3 + 1] * T[1 * 4 + j] + Rz[i * 3 + 2] * T[2 * 4 + j];
-        o[i * 4 + 3] = Rz[i * 3 + 0] * T[3] + Rz[i * 3 + 1] * T[7] + Rz[i * 3 + 2] * T[11] + delta[i];
+        for (int j = 0; j < 3; ++j)
+            o[i * 4 + j] = fma(Rz[i * 3 + 0], T[0 * 4 + j], fma(Rz[i * 3 + 1], T[1 * 4 + j], Rz[i * 3 + 2] * T[2 * 4 + j]));
+        o[i * 4 + 3] = fma(Rz[i * 3 + 0], T[3], fma(Rz[i * 3 + 1], T[7], fma(Rz[i * 3 + 2], T[11], delta[i])));
     }
     for (int i = 0; i < 12; ++i) T[i] = o[i];
 }

@@ -429,6 +429,39 @@ struct IcpConsts {
     int reach, mask;
 };
 
+// A launch-long memo, in shared memory, of what the first point of each group read from global memory. Within one
+// Gauss-Newton launch the map and the thinned points do not change, and a point moves by millimetres between
+// iterations. The memo keeps the group's point, the 5 x 5 x 5 window of hash slots and means that its last wide
+// search gathered around base voxel `tag`, and the record of its last matched voxel. A wide search from the same
+// base voxel, and every narrow search whose 3 x 3 x 3 neighbourhood lies inside the window (base voxel within one of
+// the tag's), then reads shared memory instead of making dependent global loads -- the same values, so the sums
+// are exactly those of the uncached pass.
+constexpr int GN_GROUPS = GN_THREADS / 8;
+constexpr int WIN = 128;  // 5^3 = 125 window entries per group, padded
+struct IcpCache {
+    float4* mean;  // [GN_GROUPS][WIN] means (x, y, z, occupancy weight) of the window's slots
+    float4* brec;  // [GN_GROUPS][5] the record of the group's last matched voxel
+    float4* pt;    // [GN_GROUPS] the group's first point
+    int4* tag;     // [GN_GROUPS] the window's base voxel (x, y, z); w = 0: no window yet
+    int* slot;     // [GN_GROUPS][WIN] the window's slots (-1: not in the map), offset (dx + 2) 25 + (dy + 2) 5 + dz + 2
+    int* best;     // [GN_GROUPS] the group's last matched slot (-1: none)
+    int pt_ok;     // pt holds the points (every pass after the launch's first)
+};
+constexpr size_t GN_DYN_SMEM = (size_t)(GN_GROUPS * WIN + GN_GROUPS * 5 + GN_GROUPS * 2) * sizeof(float4) +
+                               (size_t)(GN_GROUPS * WIN + GN_GROUPS) * sizeof(int);
+
+__device__ __forceinline__ IcpCache icp_cache_carve(float4* base) {
+    IcpCache C;
+    C.mean = base;
+    C.brec = C.mean + GN_GROUPS * WIN;
+    C.pt = C.brec + GN_GROUPS * 5;
+    C.tag = reinterpret_cast<int4*>(C.pt + GN_GROUPS);
+    C.slot = reinterpret_cast<int*>(C.tag + GN_GROUPS);
+    C.best = C.slot + GN_GROUPS * WIN;
+    C.pt_ok = 0;
+    return C;
+}
+
 __device__ __forceinline__ int probe_rest(int64_t key, int h, int mask, const int64_t* __restrict__ keys) {
 #pragma unroll 1
     for (int p = 1; p < PROBES; ++p) {
@@ -440,56 +473,96 @@ __device__ __forceinline__ int probe_rest(int64_t key, int h, int mask, const in
     return -1;
 }
 
-// The closest occupied voxel mean among this lane's share (offsets lane_g, lane_g + G, ...) of the neighbourhood.
-template <int R, int G, int B>
-__device__ __forceinline__ void icp_search(int lane_g, float wx, float wy, float wz, const IcpConsts& k,
-                                           const int64_t* __restrict__ keys, const float* __restrict__ rec,
-                                           float& best_d2, int& best_o, int& best_s) {
-    constexpr int S = 2 * R + 1;
-    constexpr int N = S * S * S;
-    constexpr int PER = (N + G - 1) / G;
-    const int bx = ifloor(wx * k.inv_v), by = ifloor(wy * k.inv_v), bz = ifloor(wz * k.inv_v);
+// Squared distance from w to a voxel mean, one expression wherever candidates are compared (bit-identical d2).
+__device__ __forceinline__ float mean_d2(float wx, float wy, float wz, const float4& m) {
+    const float dx = wx - m.x, dy = wy - m.y, dz = wz - m.z;
+    return dx * dx + dy * dy + dz * dz;
+}
+
+// The slot of `key` (hashing to h) and, when it is in the map, its mean: -1 when absent.
+__device__ __forceinline__ int lookup_mean(int64_t key, const IcpConsts& k, const int64_t* __restrict__ keys,
+                                           const float* __restrict__ rec, float4& hd) {
+    const int h = slot_hash(key) & k.mask;
+    const int64_t k0 = __ldg(keys + h);
+    int s = -1;
+    if (k0 == key) s = h;
+    else if (k0 != EMPTY_KEY) s = probe_rest(key, h, k.mask, keys);
+    if (s >= 0) hd = __ldg(reinterpret_cast<const float4*>(rec + (int64_t)s * LW_REC_FLOATS));
+    return s;
+}
+
+// Phase A of a search: the closest occupied voxel mean among this lane's share (i = lane_g, lane_g + 8, ...) of the
+// 27 voxels around base voxel (bx, by, bz), four lookups in flight per lane. o numbers a voxel as the reference's
+// loop visits the reach's whole neighbourhood ((dx + R) (2R + 1)^2 + (dy + R) (2R + 1) + dz + R), which breaks ties.
+// ws / wm: the group's memo window, based (ox, oy, oz) voxels from (bx, by, bz); with use, entries come from it (an
+// entry not gathered yet, -2, is looked up and then kept); otherwise from the hash table and records, and with store
+// they are written to it.
+__device__ __forceinline__ void icp_search27(int lane_g, int R, int bx, int by, int bz, float wx, float wy, float wz,
+                                             const IcpConsts& k, const int64_t* __restrict__ keys,
+                                             const float* __restrict__ rec, int* ws, float4* wm, int ox, int oy,
+                                             int oz, bool use, bool store, float& best_d2, int& best_o, int& best_s) {
+    constexpr int B = 4;
+    const int S = 2 * R + 1;
+    int s[B], o[B], w[B];
+    int64_t key[B];
+    float4 hd[B];
+    bool val[B], need[B];
 #pragma unroll
-    for (int j0 = 0; j0 < PER; j0 += B) {
-        int64_t key[B];
-        int h[B];
-        int64_t k0[B];
-        int o[B];
-        bool val[B];
+    for (int u = 0; u < B; ++u) {
+        const int i = lane_g + 8 * u;
+        val[u] = i < 27;
+        const int dx = i / 9 - 1, dy = (i / 3) % 3 - 1, dz = i % 3 - 1;
+        o[u] = (dx + R) * S * S + (dy + R) * S + (dz + R);
+        w[u] = (dx + ox + 2) * 25 + (dy + oy + 2) * 5 + (dz + oz + 2);
+        s[u] = -1;
+        need[u] = val[u];
+        if (use && val[u]) {
+            s[u] = ws[w[u]];
+            need[u] = s[u] == -2;
+            if (s[u] >= 0) hd[u] = wm[w[u]];
+        }
+    }
+    // the lookups not served by the window: first every probe's head key, then the records
+    int h[B];
+    int64_t k0[B];
+    if (need[0] || need[1] || need[2] || need[3]) {
 #pragma unroll
-        for (int u = 0; u < B; ++u) {
-            o[u] = lane_g + (j0 + u) * G;
-            val[u] = (j0 + u) < PER && o[u] < N;
-            if (val[u]) {
-                int dz = o[u] % S - R, dy = (o[u] / S) % S - R, dx = o[u] / (S * S) - R;
-                key[u] = key_ijk(bx + dx, by + dy, bz + dz);
+        for (int u = 0; u < B; ++u)
+            if (need[u]) {
+                const int i = lane_g + 8 * u;
+                key[u] = key_ijk(bx + i / 9 - 1, by + (i / 3) % 3 - 1, bz + i % 3 - 1);
                 h[u] = slot_hash(key[u]) & k.mask;
                 k0[u] = __ldg(keys + h[u]);
             }
-        }
-        int s[B];
 #pragma unroll
-        for (int u = 0; u < B; ++u) {
-            s[u] = -1;
-            if (val[u]) {
+        for (int u = 0; u < B; ++u)
+            if (need[u]) {
+                s[u] = -1;
                 if (k0[u] == key[u]) s[u] = h[u];
                 else if (k0[u] != EMPTY_KEY) s[u] = probe_rest(key[u], h[u], k.mask, keys);
             }
-        }
-        float4 hd[B];
 #pragma unroll
         for (int u = 0; u < B; ++u)
-            if (s[u] >= 0) hd[u] = __ldg(reinterpret_cast<const float4*>(rec + (int64_t)s[u] * LW_REC_FLOATS));
+            if (need[u] && s[u] >= 0)
+                hd[u] = __ldg(reinterpret_cast<const float4*>(rec + (int64_t)s[u] * LW_REC_FLOATS));
+        if (ws && (store || use)) {
 #pragma unroll
-        for (int u = 0; u < B; ++u) {
-            if (s[u] >= 0 && hd[u].w > 0.0f) {
-                float dx = wx - hd[u].x, dy = wy - hd[u].y, dz = wz - hd[u].z;
-                float d2 = dx * dx + dy * dy + dz * dz;
-                if (d2 < best_d2) {
-                    best_d2 = d2;
-                    best_o = o[u];
-                    best_s = s[u];
+            for (int u = 0; u < B; ++u)
+                if (need[u]) {
+                    ws[w[u]] = s[u];
+                    if (s[u] >= 0) wm[w[u]] = hd[u];
                 }
+        }
+    }
+    // this lane's candidates come in increasing o, so the first of equal distances stays
+#pragma unroll
+    for (int u = 0; u < B; ++u) {
+        if (val[u] && s[u] >= 0 && hd[u].w > 0.0f) {
+            const float d2 = mean_d2(wx, wy, wz, hd[u]);
+            if (d2 < best_d2) {
+                best_d2 = d2;
+                best_o = o[u];
+                best_s = s[u];
             }
         }
     }
@@ -540,34 +613,116 @@ __device__ __forceinline__ int term_index(int lg, int u, int& p, int& q) {
 constexpr double GN_FIX = 65536.0;
 constexpr double GN_FIX_MAX = 4.0e18 / 256.0;  // per-CTA bound: 256 CTAs stay below 2^62
 
-// One accumulation pass of this CTA over its share of the thinned points with groups of G lanes; writes the CTA's
-// float64 partial (part) or adds it in fixed point (fixed).
-template <int R, int G, int B>
-__device__ void icp_pass_g(const float4* __restrict__ ds, int n, const IcpPose& P, const IcpConsts& k,
-                           const int64_t* __restrict__ keys, const float* __restrict__ rec, double* __restrict__ part,
-                           long long* __restrict__ fixed, int* err) {
+// Phase B of a wide search, for the points whose best mean among their 27 inner voxels is not closer than the outer
+// shell of their 5 x 5 x 5 neighbourhood (few: those far from the map's surfaces). The whole CTA splits their outer
+// voxels; a voxel whose box (widened by a millimetre, more than the rounding of a mean) is farther than the point's
+// current best cannot hold a closer or tying mean and is skipped, and each candidate that may win is folded in by
+// an atomic minimum of (d2, o, slot) packed into 64 bits -- the order the reference's loop picks in.
+constexpr int SLOT_BITS = 25;  // a registration map of up to 2^25 slots
+__device__ __forceinline__ unsigned long long pack_best(float d2, int o, int s) {
+    return ((unsigned long long)__float_as_uint(d2) << 32) | ((unsigned long long)(o & 127) << SLOT_BITS) |
+           (unsigned long long)(s < 0 ? (1 << SLOT_BITS) - 1 : s);
+}
+
+struct NeedyPoint {
+    float wx, wy, wz;
+    int bx, by, bz;
+};
+
+__device__ void outer_shell(const NeedyPoint* __restrict__ q, unsigned long long* best, int nq, const IcpConsts& k,
+                            float voxel, const int64_t* __restrict__ keys, const float* __restrict__ rec) {
+    for (int it = threadIdx.x; it < nq * 128; it += blockDim.x) {
+        const int qi = it >> 7, o = it & 127;
+        const int dx = o / 25 - 2, dy = (o / 5) % 5 - 2, dz = o % 5 - 2;
+        if (o >= 125 || (abs(dx) <= 1 && abs(dy) <= 1 && abs(dz) <= 1)) continue;
+        const NeedyPoint p = q[qi];
+        const float slack = 1e-3f;
+        const float lx = (float)(p.bx + dx) * voxel - slack, hx = (float)(p.bx + dx + 1) * voxel + slack;
+        const float ly = (float)(p.by + dy) * voxel - slack, hy = (float)(p.by + dy + 1) * voxel + slack;
+        const float lz = (float)(p.bz + dz) * voxel - slack, hz = (float)(p.bz + dz + 1) * voxel + slack;
+        const float gx = fmaxf(0.0f, fmaxf(lx - p.wx, p.wx - hx));
+        const float gy = fmaxf(0.0f, fmaxf(ly - p.wy, p.wy - hy));
+        const float gz = fmaxf(0.0f, fmaxf(lz - p.wz, p.wz - hz));
+        const float box2 = gx * gx + gy * gy + gz * gz;
+        const float cur = __uint_as_float((unsigned)(*(volatile unsigned long long*)(best + qi) >> 32));
+        if (box2 > cur) continue;
+        float4 hd;
+        const int s = lookup_mean(key_ijk(p.bx + dx, p.by + dy, p.bz + dz), k, keys, rec, hd);
+        if (s < 0 || !(hd.w > 0.0f)) continue;
+        const float d2 = mean_d2(p.wx, p.wy, p.wz, hd);
+        if (d2 < k.max_d2) atomicMin(best + qi, pack_best(d2, o, s));
+    }
+}
+
+// One accumulation pass of this CTA over its share of the thinned points, a group of 8 lanes per point; writes the
+// CTA's float64 partial (part) or adds it in fixed point (fixed). The rounds over the points are uniform across the
+// CTA (a round's phase B needs every thread).
+__device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P, const IcpConsts& k,
+                         const int64_t* __restrict__ keys, const float* __restrict__ rec, double* __restrict__ part,
+                         long long* __restrict__ fixed = nullptr, int* err = nullptr, const IcpCache* C = nullptr) {
+    constexpr int G = 8;
     constexpr int GROUPS = GN_THREADS / G;
     constexpr int TPL = TERMS_PER_LANE;  // terms per lane
     static_assert(G == TERM_LANES, "the terms are split over groups of 8 lanes");
     __shared__ float tacc[GN_THREADS / 32][LW_ACC_STRIDE];
+    __shared__ NeedyPoint s_need[2][GROUPS];
+    __shared__ unsigned long long s_best[2][GROUPS];
+    __shared__ int s_nq[3];
+    const int R = k.reach;
     const int lane = threadIdx.x & 31;
     const int lane_g = lane & (G - 1);
     const int gl = threadIdx.x / G;
-    const int group = blockIdx.x * GROUPS + gl;
     const int ngroups = gridDim.x * GROUPS;
-    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane & ~(G - 1));
+    const unsigned gmask = 0xFFu << (lane & ~(G - 1));
+    const float voxel = 1.0f / k.inv_v;
+    if (R == 2) {
+        if (threadIdx.x < 3) s_nq[threadIdx.x] = 0;
+        __syncthreads();
+    }
     float acc[TPL];
 #pragma unroll
     for (int u = 0; u < TPL; ++u) acc[u] = 0.0f;
-    for (int j = group; j < n; j += ngroups) {
-        const float4 p = __ldg(ds + j);
+    int round = 0;
+    for (int j0 = blockIdx.x * GROUPS; j0 < n; j0 += ngroups, ++round) {
+        const int j = j0 + gl;
+        const bool active = j < n;
+        const bool memo = C != nullptr && j0 == blockIdx.x * GROUPS;  // the memo serves each group's first point
+        float4 p = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (active) p = memo && C->pt_ok ? C->pt[gl] : __ldg(ds + j);
+        if (active && memo && !C->pt_ok && lane_g == 0) C->pt[gl] = p;
         const float lx = P.R[0] * p.x + P.R[1] * p.y + P.R[2] * p.z + P.tr[0];
         const float ly = P.R[3] * p.x + P.R[4] * p.y + P.R[5] * p.z + P.tr[1];
         const float lz = P.R[6] * p.x + P.R[7] * p.y + P.R[8] * p.z + P.tr[2];
         const float wx = lx + P.c[0], wy = ly + P.c[1], wz = lz + P.c[2];
+        const int bx = ifloor(wx * k.inv_v), by = ifloor(wy * k.inv_v), bz = ifloor(wz * k.inv_v);
+        // the window serves the wide search from its own base voxel and the narrow one from within one voxel of it
+        bool use = false, store = false;
+        int ox = 0, oy = 0, oz = 0;
+        if (active && memo) {
+            const int4 tg = C->tag[gl];
+            ox = bx - tg.x;
+            oy = by - tg.y;
+            oz = bz - tg.z;
+            const int lim = 2 - R;
+            use = tg.w != 0 && abs(ox) <= lim && abs(oy) <= lim && abs(oz) <= lim;
+            store = !use && R == 2;
+            if (!use) ox = oy = oz = 0;
+        }
+        int* ws = memo ? C->slot + gl * WIN : nullptr;
+        float4* wm = memo ? C->mean + gl * WIN : nullptr;
+        if (store) {
+            __syncwarp(gmask);  // every lane of the group has read the old tag
+            // a new window: its outer shell is not gathered yet (the inner 27 are written by the search below)
+            for (int e = lane_g; e < 125; e += G) {
+                const int ex = e / 25 - 2, ey = (e / 5) % 5 - 2, ez = e % 5 - 2;
+                if (abs(ex) == 2 || abs(ey) == 2 || abs(ez) == 2) ws[e] = -2;
+            }
+            if (lane_g == 0) C->tag[gl] = make_int4(bx, by, bz, 1);
+        }
         float bd = k.max_d2;
         int bo = 0x7FFFFFFF, bs = -1;
-        icp_search<R, G, B>(lane_g, wx, wy, wz, k, keys, rec, bd, bo, bs);
+        if (active)
+            icp_search27(lane_g, R, bx, by, bz, wx, wy, wz, k, keys, rec, ws, wm, ox, oy, oz, use, store, bd, bo, bs);
 #pragma unroll
         for (int off = G / 2; off > 0; off >>= 1) {
             float od = __shfl_xor_sync(gmask, bd, off);
@@ -579,14 +734,67 @@ __device__ void icp_pass_g(const float4* __restrict__ ds, int n, const IcpPose& 
                 bs = os;
             }
         }
-        if (bs < 0) continue;  // uniform over the group after the reduction
+        if (R == 2) {
+            // phase B: may a mean in the outer shell be at least as close as the inner best? (the nearest outer
+            // voxel is a whole voxel or more away along one axis)
+            const float fx = wx * k.inv_v - (float)bx, fy = wy * k.inv_v - (float)by, fz = wz * k.inv_v - (float)bz;
+            const float gap = fmaxf(0.0f, fminf(fminf(fminf(2.0f - fx, 1.0f + fx), fminf(2.0f - fy, 1.0f + fy)),
+                                                 fminf(2.0f - fz, 1.0f + fz)) * voxel - 2e-3f);
+            const bool needy = active && gap * gap <= bd;
+            const int buf = round & 1;
+            int qi = 0;
+            if (needy && lane_g == 0) {
+                qi = atomicAdd(&s_nq[round % 3], 1);
+                s_need[buf][qi] = NeedyPoint{wx, wy, wz, bx, by, bz};
+                s_best[buf][qi] = pack_best(bd, bo, bs);
+            }
+            __syncthreads();
+            const int nq = s_nq[round % 3];
+            if (threadIdx.x == 0) s_nq[(round + 2) % 3] = 0;  // last used two rounds ago; next used after a barrier
+            if (nq > 0) {
+                outer_shell(s_need[buf], s_best[buf], nq, k, voxel, keys, rec);
+                __syncthreads();
+                if (needy) {
+                    qi = __shfl_sync(gmask, qi, lane & ~(G - 1));
+                    const unsigned long long b = s_best[buf][qi];
+                    bd = __uint_as_float((unsigned)(b >> 32));
+                    bo = (int)((b >> SLOT_BITS) & 127u);
+                    bs = (int)(b & ((1u << SLOT_BITS) - 1u));
+                    if (bs == (1 << SLOT_BITS) - 1) bs = -1;
+                }
+            }
+        }
+        if (!active || bs < 0) continue;  // uniform over the group after the reduction
         // the matched voxel's record (odom.py:335-368, hoisted to the insert): every lane of the group reads it
-        const float* rr = rec + (int64_t)bs * LW_REC_FLOATS;
-        const float4 h0 = __ldg(reinterpret_cast<const float4*>(rr));
-        const float4 h1 = __ldg(reinterpret_cast<const float4*>(rr + 4));
-        const float4 h2 = __ldg(reinterpret_cast<const float4*>(rr + 8));
-        const float4 h3 = __ldg(reinterpret_cast<const float4*>(rr + 12));
-        const float4 h4 = __ldg(reinterpret_cast<const float4*>(rr + 16));
+        float4 h0, h1, h2, h3, h4;
+        const bool rec_memo = memo && C->best[gl] == bs;
+        if (rec_memo) {
+            const float4* cr = C->brec + gl * 5;
+            h0 = cr[0];
+            h1 = cr[1];
+            h2 = cr[2];
+            h3 = cr[3];
+            h4 = cr[4];
+        } else {
+            const float* rr = rec + (int64_t)bs * LW_REC_FLOATS;
+            h0 = __ldg(reinterpret_cast<const float4*>(rr));
+            h1 = __ldg(reinterpret_cast<const float4*>(rr + 4));
+            h2 = __ldg(reinterpret_cast<const float4*>(rr + 8));
+            h3 = __ldg(reinterpret_cast<const float4*>(rr + 12));
+            h4 = __ldg(reinterpret_cast<const float4*>(rr + 16));
+            if (memo) {
+                __syncwarp(gmask);  // every lane of the group has read the old matched slot
+                if (lane_g == 0) {
+                    float4* cr = C->brec + gl * 5;
+                    cr[0] = h0;
+                    cr[1] = h1;
+                    cr[2] = h2;
+                    cr[3] = h3;
+                    cr[4] = h4;
+                    C->best[gl] = bs;
+                }
+            }
+        }
         const float M[6] = {h1.x, h1.y, h1.z, h1.w, h2.x, h2.y};
         const float Mg[6] = {h2.z, h2.w, h3.x, h3.y, h3.z, h3.w};
         const float r0 = wx - h0.x, r1 = wy - h0.y, r2 = wz - h0.z;
@@ -664,15 +872,6 @@ __device__ void icp_pass_g(const float4* __restrict__ ds, int n, const IcpPose& 
     __syncthreads();
 }
 
-__device__ __forceinline__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P, const IcpConsts& k,
-                                         const int64_t* __restrict__ keys, const float* __restrict__ rec,
-                                         double* __restrict__ part, long long* __restrict__ fixed = nullptr,
-                                         int* err = nullptr) {
-    if (k.reach == 2)
-        icp_pass_g<2, 8, 8>(ds, n, P, k, keys, rec, part, fixed, err);
-    else
-        icp_pass_g<1, 8, 4>(ds, n, P, k, keys, rec, part, fixed, err);
-}
 
 __device__ __forceinline__ void sym6_from(const double* up, double* H) {
     int idx = 0;
@@ -1067,6 +1266,19 @@ __device__ __forceinline__ void chol6_solve(const double* Lf, const double* rhs,
     }
 }
 
+// 1 / d for d > 0 on a chain of dependent operations: the PTX approximate reciprocal refined by two Newton-Raphson
+// steps r <- r + r (1 - d r), each of which doubles the number of correct bits, to within an ulp or so of the
+// rounded quotient. Outside the normal range (where the approximation flushes) the division itself.
+__device__ __forceinline__ double rcp_newton(double d) {
+    if (!(d > 1e-300 && d < 1e300)) return 1.0 / d;
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+    double e = fma(-d, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-d, r, 1.0);
+    return fma(r, e, r);
+}
+
 // A - shift I = L D L^T with L unit lower triangular (Crout order, on the packed lower triangle): no square root,
 // one reciprocal per pivot, and about half the live registers of an L L^T factor. Returns 0 unless every pivot is
 // positive (A - shift I positive definite). L holds the 15 entries below the diagonal, row i from i (i - 1) / 2.
@@ -1083,7 +1295,7 @@ __device__ __forceinline__ int ldl6(const double* __restrict__ A, double shift, 
         }
         if (!(d > 0.0)) return 0;
         D[j] = d;
-        const double r = 1.0 / d;
+        const double r = rcp_newton(d);
         rd[j] = r;
 #pragma unroll
         for (int i = j + 1; i < 6; ++i) {
@@ -1443,6 +1655,12 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
     __shared__ GnSmem S;
     __shared__ int s_iters, s_degen, s_corr;
     __shared__ double s_rms;
+    extern __shared__ float4 gn_dyn[];
+    IcpCache memo = icp_cache_carve(gn_dyn);
+    if (threadIdx.x < GN_GROUPS) {
+        memo.tag[threadIdx.x] = make_int4(0, 0, 0, 0);
+        memo.best[threadIdx.x] = -1;
+    }
     const int n = *n_dev;
     if (threadIdx.x == 0) {
         for (int i = 0; i < 16; ++i) S.T[i] = S.Tp[i] = st->T_pred[i];
@@ -1486,7 +1704,8 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         // barrier and reads it after; CTA 0 then clears buffer (it + 2) % 3, which nobody reads any more (its last
         // readers passed this barrier) and nobody adds to before the next barrier
         long long* fixed = reinterpret_cast<long long*>(gn.part) + (it % 3) * LW_ACC_STRIDE;
-        icp_pass(ds, n, P, k, keys, rec, nullptr, fixed, gn.err);
+        memo.pt_ok = it > 0;
+        icp_pass(ds, n, P, k, keys, rec, nullptr, fixed, gn.err, &memo);
         if (it == 0 && (int)blockIdx.x == gn.skip_cta) return;  // injected failure: this CTA never arrives
         // while thread 0 waits, thread 32 prepares what the step needs from the pose alone
         if (!grid_sync(gn.bar, (uint32_t)(it + 1) * gridDim.x, gn.err, 1, budget,
@@ -1794,6 +2013,8 @@ static lw_rec_params rec_params(const lw_odom_params* prm) {
 
 static int launch_gn(const float* ds4, const int32_t* n_dev, const lw_odom_params* prm, lw_odom_state* st,
                      const lw_regmap* reg, lw_gn_scratch* gn, int which, cudaStream_t s) {
+    if (reg->cap > (1LL << SLOT_BITS))
+        return set_error(LW_EINVAL, "Gauss-Newton: a registration map of %lld slots (at most 2^25)", (long long)reg->cap);
     int grid = gn_grid(gn);
     lw_gn_scratch g = *gn;
     g.grid = grid;
@@ -1808,7 +2029,14 @@ static int launch_gn(const float* ds4, const int32_t* n_dev, const lw_odom_param
     // the barrier's arrival count too: a launch that gave up at the barrier may have left it part counted
     LW_CUDA(cudaMemsetAsync(gn->part, 0, 3 * LW_ACC_STRIDE * sizeof(long long), s));
     LW_CUDA(cudaMemsetAsync(gn->bar, 0, 2 * sizeof(uint32_t), s));
-    LW_CUDA(cudaLaunchCooperativeKernel((const void*)k_gn, dim3(grid), dim3(GN_THREADS), args, 0, s));
+    static bool smem_set[64] = {};  // the memo's dynamic shared memory is above the default 48 KB
+    int dev = 0;
+    LW_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || !smem_set[dev]) {
+        LW_CUDA(cudaFuncSetAttribute((const void*)k_gn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GN_DYN_SMEM));
+        if (dev >= 0 && dev < 64) smem_set[dev] = true;
+    }
+    LW_CUDA(cudaLaunchCooperativeKernel((const void*)k_gn, dim3(grid), dim3(GN_THREADS), args, GN_DYN_SMEM, s));
     count_launches(1);
     return LW_OK;
 }
@@ -1946,6 +2174,8 @@ int lw_icp_accumulate(const float* ds4, const int32_t* n_dev, int64_t n_ub, cons
                       void* stream) {
     if (!ds4 || !T_host || !reg || !gn || !out64) return set_error(LW_EINVAL, "lw_icp_accumulate: null argument");
     if (reach != 1 && reach != 2) return set_error(LW_EINVAL, "lw_icp_accumulate: reach must be 1 or 2");
+    if (reg->cap > (1LL << SLOT_BITS))
+        return set_error(LW_EINVAL, "lw_icp_accumulate: a registration map of %lld slots (at most 2^25)", (long long)reg->cap);
     cudaStream_t s = (cudaStream_t)stream;
     int grid = gn_grid(gn);
     IcpPose P;

@@ -38,7 +38,7 @@ def test_barrier_wait_runs_out_and_the_context_stays_usable():
     odom, oreg, T0, (x, a, t, t_mid, _), voxel = _case()
     zero = np.zeros(6, np.float32)
     gn = odom._gn
-    gn.struct.spin_budget = 2000   # ~0.2 ms of sleeps instead of ~2 s
+    gn.struct.spin_budget = 2000   # ~0.5 ms of polls instead of seconds
     gn.struct.skip_cta = gn.grid - 1
     t0 = time.perf_counter()
     _, ok, st = odom.register_frame(x, a, t, t_mid, zero, T0)
