@@ -712,11 +712,10 @@ __device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P,
         float4* wm = memo ? C->mean + gl * WIN : nullptr;
         if (store) {
             __syncwarp(gmask);  // every lane of the group has read the old tag
-            // a new window: its outer shell is not gathered yet (the inner 27 are written by the search below)
-            for (int e = lane_g; e < 125; e += G) {
-                const int ex = e / 25 - 2, ey = (e / 5) % 5 - 2, ez = e % 5 - 2;
-                if (abs(ex) == 2 || abs(ey) == 2 || abs(ez) == 2) ws[e] = -2;
-            }
+            // a new window: nothing gathered yet (the search below writes the inner 27)
+            int4* w4 = reinterpret_cast<int4*>(ws);
+            for (int e = lane_g; e < WIN / 4; e += G) w4[e] = make_int4(-2, -2, -2, -2);
+            __syncwarp(gmask);
             if (lane_g == 0) C->tag[gl] = make_int4(bx, by, bz, 1);
         }
         float bd = k.max_d2;
@@ -1279,54 +1278,47 @@ __device__ __forceinline__ double rcp_newton(double d) {
     return fma(r, e, r);
 }
 
-// A - shift I = L D L^T with L unit lower triangular (Crout order, on the packed lower triangle): no square root,
-// one reciprocal per pivot, and about half the live registers of an L L^T factor. Returns 0 unless every pivot is
-// positive (A - shift I positive definite). L holds the 15 entries below the diagonal, row i from i (i - 1) / 2.
-__device__ __forceinline__ int ldl6(const double* __restrict__ A, double shift, double* L, double* rd) {
-    double D[6];
-#pragma unroll
-    for (int j = 0; j < 6; ++j) {
-        double v[6];
-        double d = A[j * 6 + j] - shift;
-#pragma unroll
-        for (int k = 0; k < j; ++k) {
-            v[k] = L[j * (j - 1) / 2 + k] * D[k];
-            d = fma(-L[j * (j - 1) / 2 + k], v[k], d);
-        }
-        if (!(d > 0.0)) return 0;
-        D[j] = d;
-        const double r = rcp_newton(d);
-        rd[j] = r;
-#pragma unroll
-        for (int i = j + 1; i < 6; ++i) {
-            double x = A[i * 6 + j];
-#pragma unroll
-            for (int k = 0; k < j; ++k) x = fma(-L[i * (i - 1) / 2 + k], v[k], x);
-            L[i * (i - 1) / 2 + j] = x * r;
-        }
-    }
-    return 1;
+// Gaussian elimination of a symmetric 6x6 (row major, in registers) shifted by diag(st, st, st, sr, sr, sr), with
+// no division on its chain: step k replaces each trailing row by p_k row_i - a_ik row_k, where p_k is the pivot
+// times the power of two that brings it to [1, 2) (an exact scaling, so the entries keep their range); the update
+// p A - a a^T keeps the trailing block symmetric, so only its upper triangle is formed, and it scales each Schur
+// complement by a positive factor, so the pivots carry the signs of the L D L^T pivots. Returns 0 unless every
+// pivot is positive (the shifted matrix positive definite). With rhs, the right-hand side is carried along and
+// x receives the solution: the six reciprocals are taken together, then the back substitution only multiplies.
+__device__ __forceinline__ double pow2_below(double p) {  // 2^-e for p = m 2^e, m in [1, 2), p normal and positive
+    const int e = ((__double2hiint(p) >> 20) & 0x7FF) - 1023;
+    return __hiloint2double((1023 - e) << 20, 0);
 }
 
-// The solution of A x = rhs from A = L D L^T (positive definite), in registers when A and rhs are. 0 when A is not
-// positive definite.
-__device__ __forceinline__ int ldl6_solve(const double* __restrict__ A, const double* __restrict__ rhs, double* x) {
-    double L[15], rd[6];
-    if (!ldl6(A, 0.0, L, rd)) return 0;
-    double y[6];
+__device__ __forceinline__ int elim6(double* a, double st, double sr, double* rhs, double* x) {
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        double v = rhs[i];
+    for (int k = 0; k < 6; ++k) a[k * 7] -= k < 3 ? st : sr;
 #pragma unroll
-        for (int k = 0; k < i; ++k) v = fma(-L[i * (i - 1) / 2 + k], y[k], v);
-        y[i] = v;
+    for (int k = 0; k < 6; ++k) {
+        const double p = a[k * 7];
+        if (!(p > 1e-300 && p < 1e300)) return 0;
+        const double sc = pow2_below(p);
+        const double ps = p * sc;
+#pragma unroll
+        for (int i = k + 1; i < 6; ++i) {
+            const double f = a[k * 6 + i] * sc;  // a_ik, by symmetry
+#pragma unroll
+            for (int j = i; j < 6; ++j) a[i * 6 + j] = fma(ps, a[i * 6 + j], -(f * a[k * 6 + j]));
+            if (rhs) rhs[i] = fma(ps, rhs[i], -(f * rhs[k]));
+        }
     }
+    if (!rhs) return 1;
+    double r[6];
 #pragma unroll
-    for (int i = 5; i >= 0; --i) {
-        double v = y[i] * rd[i];
+    for (int k = 0; k < 6; ++k) r[k] = rcp_newton(a[k * 7]);
+    double acc[6];
 #pragma unroll
-        for (int k = i + 1; k < 6; ++k) v = fma(-L[k * (k - 1) / 2 + i], x[k], v);
-        x[i] = v;
+    for (int k = 0; k < 6; ++k) acc[k] = rhs[k];
+#pragma unroll
+    for (int k = 5; k >= 0; --k) {
+        x[k] = acc[k] * r[k];
+#pragma unroll
+        for (int i = 0; i < k; ++i) acc[i] = fma(-a[i * 6 + k], x[k], acc[i]);
     }
     return 1;
 }
@@ -1500,11 +1492,11 @@ __device__ __forceinline__ double sym_bilinear(const double* M, const double (&u
 }
 
 // A = H + LM damping + prior information and rhs = -b + prior (xi) (odom.py:772-785), formed in registers by one
-// thread and solved by L D L^T; A and rhs also go to shared memory for the degenerate branch. 0 when A is not
-// positive definite.
+// thread and solved by elimination (elim6); A and rhs also go to shared memory for the degenerate branch. 0 when A
+// is not positive definite.
 __device__ __forceinline__ int gn_solve_thread(GnSmem& S, const lw_odom_params& prm, double* delta) {
     const double pl2 = prm.prior_info > 0.0 ? prm.prior_info * S.L * S.L : 0.0;
-    const double dmean = ((S.H[0] + S.H[7]) + (S.H[14] + S.H[21]) + (S.H[28] + S.H[35])) / 6.0;
+    const double dmean = ((S.H[0] + S.H[7]) + (S.H[14] + S.H[21]) + (S.H[28] + S.H[35])) * (1.0 / 6.0);
     S.dmean = dmean;
     double a[36], rhs[6];
 #pragma unroll
@@ -1521,16 +1513,17 @@ __device__ __forceinline__ int gn_solve_thread(GnSmem& S, const lw_odom_params& 
         rhs[p] = -S.b[p] + S.P0xi[p] + (p >= 3 ? pl2 * S.xi[p] : 0.0);
         S.rhs[p] = rhs[p];
     }
-    return ldl6_solve(a, rhs, delta);
+    return elim6(a, 0.0, 0.0, rhs, delta);
 }
 
 // One Gauss-Newton update of S.T (odom.py:769-796) on warps 0 and 1 (the other warps go straight to the block
 // barrier after it). S.status: 0 continue, 1 converged, 2 too few correspondences, 3 singular.
-//   1. one output per thread: threads 0-20 the world-origin H = Ac^T Hc Ac (the sums were taken about the pass
-//      centre; odom.py's twist is about the origin), 21-41 the sensor-basis information G = SB^T Hg SB = diag(s)
-//      W^T Hg_c W diag(s) (s = 1, 1, 1, 1/L, 1/L, 1/L), 42-47 b = Ac^T b_c, 48-49 the stats (odom.py:769-772);
-//   2. thread 0 forms A and rhs and solves A delta = rhs by L D L^T while thread 32 tests G - thr I for positive
-//      definiteness the same way;
+//   1. one output per thread, no division on the way: threads 0-20 the world-origin H = Ac^T Hc Ac (the sums were
+//      taken about the pass centre; odom.py's twist is about the origin), 21-41 G0 = W^T Hg_c W, of which the
+//      sensor-basis information is G = SB^T Hg SB = diag(s) G0 diag(s) (s = 1, 1, 1, 1/L, 1/L, 1/L), 42-47
+//      b = Ac^T b_c, 48 the count and the mean range L (odom.py:769-772);
+//   2. thread 0 forms A and rhs and solves A delta = rhs (elim6) while thread 32 tests G for the threshold by the
+//      same elimination and thread 33 takes the rms;
 //   3. warp 0 takes the degenerate step if a direction is below the threshold, then applies the twist.
 // Named barrier 1 orders the two warps.
 __device__ void gn_step_pair(GnSmem& S, const lw_odom_params& prm) {
@@ -1548,9 +1541,7 @@ __device__ void gn_step_pair(GnSmem& S, const lw_odom_params& prm) {
             up[i] = U[i * 6 + p];
             uq[i] = U[i * 6 + q];
         }
-        double x = sym_bilinear(S.v + (is_h ? LW_ACC_H : LW_ACC_HG), up, uq);
-        const double iL = 1.0 / fmax(S.v[LW_ACC_RANGE] / S.v[LW_ACC_COUNT], 1.0);
-        x *= is_h ? 1.0 : (p >= 3 ? iL : 1.0) * (q >= 3 ? iL : 1.0);
+        const double x = sym_bilinear(S.v + (is_h ? LW_ACC_H : LW_ACC_HG), up, uq);
         double* out = is_h ? S.H : S.G;
         out[p * 6 + q] = x;
         out[q * 6 + p] = x;
@@ -1565,17 +1556,25 @@ __device__ void gn_step_pair(GnSmem& S, const lw_odom_params& prm) {
         S.status = S.corr < prm.min_corr ? 2 : 0;
         S.degen = 0;
         S.L = fmax(S.v[LW_ACC_RANGE] / (double)S.corr, 1.0);
-        S.invL = 1.0 / S.L;
-    } else if (tid == 49 && S.v[LW_ACC_COUNT] >= prm.min_corr) {
-        S.rms = sqrt(fmax(S.v[LW_ACC_RMS], 0.0) / fmax(S.v[LW_ACC_WEIGHT], 1e-9));
     }
     pair_sync();
     if (S.status != 0) return;  // uniform over the two warps
     double delta[6];
     if (tid == 0) s_a_ok = gn_solve_thread(S, prm, delta);
     if (tid == 32) {
-        double Lg[15], rg[6];
-        s_g_ok = !(prm.degen_thr > 0.0) || ldl6(S.G, prm.degen_thr, Lg, rg);
+        // G = diag(s) G0 diag(s) with s = (1, 1, 1, 1/L, 1/L, 1/L): G - thr I is positive definite exactly when
+        // G0 - thr diag(1, 1, 1, L^2, L^2, L^2) is (a congruence), so the test needs no scaling
+        int ok = 1;
+        if (prm.degen_thr > 0.0) {
+            double g[36];
+#pragma unroll
+            for (int e = 0; e < 36; ++e) g[e] = S.G[e];
+            ok = elim6(g, prm.degen_thr, prm.degen_thr * S.L * S.L, nullptr, nullptr);
+        }
+        s_g_ok = ok;
+    } else if (tid == 33) {
+        S.invL = 1.0 / S.L;
+        S.rms = sqrt(fmax(S.v[LW_ACC_RMS], 0.0) / fmax(S.v[LW_ACC_WEIGHT], 1e-9));
     }
     pair_sync();
     if (tid >= 32) return;
@@ -1586,6 +1585,7 @@ __device__ void gn_step_pair(GnSmem& S, const lw_odom_params& prm) {
         const double cT[3] = {S.T[3], S.T[7], S.T[11]};
         for (int e = lane; e < 36; e += 32) {
             const int p = e / 6, q = e % 6, i = p % 3, j = q % 3;
+            S.G[e] *= (p >= 3 ? S.invL : 1.0) * (q >= 3 ? S.invL : 1.0);  // the sensor-basis scaling of G
             S.SB[e] = S.SB0[e] * (q >= 3 ? S.invL : 1.0);
             double sbi = 0.0;
             if (p < 3 && q < 3) {
