@@ -110,6 +110,9 @@ class Odometry:
         self.epoch = 0
         self._rec_key = None
         self._integrate = None
+        self.side_stream = None  # integration's stream when it overlaps registration (integrate(overlap=True))
+        self._snap = None
+        self._pending = None
         self._net = None  # (InitNet, lw_net_work, its buffers) when the learned start pose is on
         self._reg_pin = None  # pinned staging of register_frame's host frames, and the event of its last copy
         self._reg_ev = None
@@ -167,6 +170,7 @@ class Odometry:
 
     def reset(self, T0: np.ndarray):
         """Forget the map and the trajectory; the next frame is posed at T0 (odom.py:561-579)."""
+        self._issue_pending()
         T0 = np.asarray(T0, dtype=np.float64).reshape(16)
         _lib.call("lw_odom_reset", _lib.f64_array(T0), _lib.ptr(self._state), _byref(self.regmap), 1, self._sp())
         with torch.cuda.stream(self.stream):
@@ -294,12 +298,52 @@ class Odometry:
             self._poses(self.k_open, self.k_open + 1, 0)
             self.k_pred = max(self.k_pred, self.k_open)
 
-    def integrate(self, view, voxel: float, carve_every: int = 1, max_range: float = 40.0, max_steps: int = 4096):
+    def integrate(self, view, voxel: float, carve_every: int = 1, max_range: float = 40.0, max_steps: int = 4096,
+                  overlap: bool = False):
         """Insert every finalised frame into the pipeline's integration map and carve its rays, on the device,
         straight after registration (what the viewer's on_frame does: app.py:557-563) -- without a host round
-        trip. carve_every = 0 inserts without carving; view = None turns it off."""
+        trip. carve_every = 0 inserts without carving; view = None turns it off.
+
+        overlap: run each frame's insert and carve on a second stream (`side_stream`) one frame later, from a copy
+        of the frame, while the next frame registers on `stream`. The map then trails the newest pose by one frame
+        until flush(); it ends up the same. Work on `stream` that reads the map should first wait for side_stream
+        (flush() does that)."""
+        self._issue_pending()
         self._integrate = None if view is None else (view, float(voxel), int(carve_every), float(max_range),
                                                      int(max_steps))
+        self.side_stream = None
+        self._snap = None
+        self._pending = None
+        if view is not None and overlap:
+            d, cap = self.device, self.frame_cap
+            self.side_stream = torch.cuda.Stream(d)
+            # two copies of the frame buffers: frame k is copied while frame k - 1's copy may still be integrating
+            self._snap = [{"xyz": torch.zeros((cap, 4), dtype=torch.float32, device=d),
+                           "attr": torch.zeros(cap, dtype=torch.int32, device=d),
+                           "t": torch.zeros(cap, dtype=torch.float32, device=d),
+                           "frame": torch.zeros(cap, dtype=torch.int32, device=d),
+                           "m": torch.zeros(1, dtype=torch.int32, device=d),
+                           "copied": torch.cuda.Event(), "done": None, "m_ub": 0} for _ in range(2)]
+            self._snap_next = 0
+
+    def _run_integration(self, xyz, attr, t, frame, m_ub: int, m_dev):
+        view, voxel, every, max_range, max_steps = self._integrate
+        self.pipe.map_insert(xyz, attr, t, frame, m_ub, view, voxel, n_dev=m_dev)
+        if every > 0:
+            self.pipe.carve(xyz, attr, frame, m_ub, voxel, every, max_range, max_steps, n_dev=m_dev)
+
+    def _issue_pending(self):
+        """Start the deferred integration of the last copied frame on the side stream."""
+        snap = self._pending
+        if snap is None:
+            return
+        self._pending = None
+        side = self.side_stream
+        side.wait_event(snap["copied"])
+        with torch.cuda.stream(side):
+            self._run_integration(snap["xyz"], snap["attr"], snap["t"], snap["frame"], snap["m_ub"], snap["m"])
+        snap["done"] = torch.cuda.Event()
+        snap["done"].record(side)
 
     def learned_init(self, net, radius: float = 12.0, nearest: bool = True):
         """Start each frame's registration from the network's proposal (livox_warp.initnet.InitNet) instead of
@@ -401,13 +445,18 @@ class Odometry:
         return np.array(rows, dtype=np.int64).reshape(-1, 3)
 
     def flush(self, on_frame=None):
-        """Finalise the open frame now (the end of a recording)."""
+        """Finalise the open frame now (the end of a recording); with overlapped integration, also integrate the
+        last frame and order `stream` after the side stream."""
         if self.k_open is not None and self._m_ub > 0:
             self._finalize(self.k_open, on_frame)
             self.k_open = None
+        self._issue_pending()
+        if self.side_stream is not None:
+            self.stream.wait_stream(self.side_stream)
 
     def _finalize(self, k: int, on_frame):
         t0 = time.perf_counter()
+        self._issue_pending()  # the previous frame's insert and carve run beside this frame's registration
         if self._net is None:
             _lib.call("lw_odom_finalize", int(k), max(self._m_ub, 1), _byref(self.params()), _lib.ptr(self._state),
                       _byref(self.fbuf), _byref(self.regmap), _byref(self.gn), _byref(self.pipe.pose_table),
@@ -419,14 +468,24 @@ class Odometry:
                       _byref(self.pipe.pose_table), self.epoch, _lib.ptr(self._traj), TRAJ_CAP, _byref(net.struct),
                       _byref(work), self._sp())
         if self._integrate is not None:
-            view, voxel, every, max_range, max_steps = self._integrate
             m_ub = max(self._m_ub, 1)
-            with torch.cuda.stream(self.stream):
-                self.pipe.map_insert(self.f_xyz, self.f_attr, self.f_t, self.f_frame, m_ub, view, voxel,
-                                     n_dev=self._m_dev)
-                if every > 0:
-                    self.pipe.carve(self.f_xyz, self.f_attr, self.f_frame, m_ub, voxel, every, max_range, max_steps,
-                                    n_dev=self._m_dev)
+            if self._snap is None:
+                with torch.cuda.stream(self.stream):
+                    self._run_integration(self.f_xyz, self.f_attr, self.f_t, self.f_frame, m_ub, self._m_dev)
+            else:
+                snap = self._snap[self._snap_next]
+                self._snap_next ^= 1
+                if snap["done"] is not None:
+                    self.stream.wait_event(snap["done"])  # the copy two frames back has been integrated
+                with torch.cuda.stream(self.stream):
+                    snap["xyz"][:m_ub].copy_(self.f_xyz[:m_ub])
+                    snap["attr"][:m_ub].copy_(self.f_attr[:m_ub])
+                    snap["t"][:m_ub].copy_(self.f_t[:m_ub])
+                    snap["frame"][:m_ub].copy_(self.f_frame[:m_ub])
+                    snap["m"].copy_(self._m_dev)
+                snap["copied"].record(self.stream)
+                snap["m_ub"] = m_ub
+                self._pending = snap
         if on_frame is not None:
             st = self.read_state()
             self._ms = (time.perf_counter() - t0) * 1e3

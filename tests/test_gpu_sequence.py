@@ -77,7 +77,11 @@ def test_every_registration_of_the_sequence_within_1mm_of_float64():
     assert (np.abs(e[:, 2] - e[:, 3]) <= 1).all()  # the stop test fires at the same iteration, or one apart
 
 
-def test_integration_map_and_carving_at_size_bit_exact():
+@pytest.mark.parametrize("overlap", [False, True])
+def test_integration_map_and_carving_at_size_bit_exact(overlap):
+    """200 frames inserted and carved (every ray) into a 2^22-slot map, keys, counts, sums and misses equal to the
+    oracle's replay of the same frames at the device's poses; with overlap the insert and carve of each frame run on
+    the side stream one frame later, and the map must come out the same."""
     from livox_warp import gpu
     from livox_warp.odom import Odometry
 
@@ -88,7 +92,7 @@ def test_integration_map_and_carving_at_size_bit_exact():
     odom = Odometry(pipe, reg_slots=1 << 21, frame_cap=1 << 15)
     odom.reg_voxel = 0.15
     view = gpu.make_view(now=0.0, voxel=0.1, map_cap=cap)
-    odom.integrate(view, 0.1, carve_every=1)
+    odom.integrate(view, 0.1, carve_every=1, overlap=overlap)
     odom.reset(traj.poses(np.array([0.5 * FRAME_DT]))[0])
     got = []
 
