@@ -369,7 +369,7 @@ def pose_drift(odom, traj, oracle_poses: dict) -> dict:
 # rounded as summarised there) and of the coarse search (profiles/k_score_grid_office_coarse.md)
 SEQ_TRAFFIC = {"gn": 1_943_000, "carve": 6_928_000}  # carve: both passes (setup + walk)
 SEQ_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_gn_k_carve_sequence.md"
-SINGLE_TRAFFIC: dict = {}  # filled from an ncu capture of the single-frame case
+SINGLE_TRAFFIC = {"gn": 975_616}  # ncu, one timed launch of the single-frame case (975,360 B read + 256 B written)
 SINGLE_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_gn_single_frame.md"
 COARSE_TRAFFIC = 42_780_928 + 71_592_448
 COARSE_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_score_grid_office_coarse.md"

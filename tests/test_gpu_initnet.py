@@ -62,6 +62,25 @@ def test_forward_matches_oracle(net):
     assert np.all(np.abs(step - o["step"]) <= 2e-3 * sc)
 
 
+def test_forward_training_batch(net):
+    """The training batch's shape (256 pairs: 512 CTAs, about 3.5 waves on 148 SMs): the first and last pairs
+    against the oracle, and every pair equal to the same pair run in a small batch (the CTAs are independent)."""
+    n = 256
+    sets = _sets(n, 5)
+    dev = torch.from_numpy(sets).cuda()
+    for _ in range(2):
+        f = net.forward(dev, n)
+        pooled = f["pooled"].cpu().numpy().reshape(2 * n, 256)
+        assert int(f["err"].cpu()[0]) == 0
+    pick = [0, n - 1]
+    idx = np.array([[2 * q, 2 * q + 1] for q in pick]).reshape(-1)
+    o = oracle.net_forward(_w(net), sets[idx], net.in_scale, net.out_scale.cpu().numpy())
+    scale = np.abs(o["pooled"]).max()
+    assert (np.abs(pooled[idx] - o["pooled"]) <= 1e-3 * scale).mean() >= 0.99
+    small = net.forward(torch.from_numpy(np.ascontiguousarray(sets[idx])).cuda(), len(pick))
+    assert np.array_equal(small["pooled"].cpu().numpy().reshape(-1, 256), pooled[idx])
+
+
 def test_backward_matches_oracle(net):
     n = 4
     sets = _sets(n, 2)
