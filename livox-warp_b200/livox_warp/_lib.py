@@ -11,6 +11,8 @@ import ctypes as C
 import os
 from pathlib import Path
 
+import numpy as np
+
 import torch
 
 LIB_PATH = Path(__file__).resolve().parent / "liblivoxb200.so"
@@ -269,13 +271,13 @@ def stream_ptr(stream=None) -> C.c_void_p:
 
 
 def f64_array(values) -> C.Array:
-    vals = [float(v) for v in values]
-    return (f64 * len(vals))(*vals)
+    a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+    return (f64 * a.size).from_buffer_copy(a)
 
 
 def f32_array(values) -> C.Array:
-    vals = [float(v) for v in values]
-    return (f32 * len(vals))(*vals)
+    a = np.ascontiguousarray(values, dtype=np.float32).reshape(-1)
+    return (f32 * a.size).from_buffer_copy(a)
 
 
 def prof_enable(on: bool = True):

@@ -84,6 +84,9 @@ class Odometry:
         self._gn = GnScratch(d)
         self.gn = self._gn.struct
         self._state = torch.zeros(ctypes.sizeof(_lib.OdomState), dtype=torch.uint8, device=d)
+        # pinned landing buffers for the state and the registration's error flag: one stream sync per readback
+        self._state_host = torch.empty(ctypes.sizeof(_lib.OdomState), dtype=torch.uint8, pin_memory=True)
+        self._err_host = torch.empty(1, dtype=torch.int32, pin_memory=True)
         self._traj = torch.zeros(TRAJ_CAP * ctypes.sizeof(_lib.TrajRec), dtype=torch.uint8, device=d)
 
         # tuning (odom.py:499-525)
@@ -159,8 +162,9 @@ class Odometry:
     def read_state(self) -> _lib.OdomState:
         """The device state (synchronises the stream)."""
         with torch.cuda.stream(self.stream):
-            host = self._state.cpu()
-        return _lib.OdomState.from_buffer_copy(host.numpy().tobytes())
+            self._state_host.copy_(self._state, non_blocking=True)
+        self.stream.synchronize()
+        return _lib.OdomState.from_buffer_copy(self._state_host.numpy())
 
     @staticmethod
     def empty_stats() -> dict:
@@ -389,20 +393,31 @@ class Odometry:
             m = len(x)
             if m > self.frame_cap:
                 raise ValueError(f"{m} points exceed the frame capacity {self.frame_cap}")
-            if self._reg_pin is None or self._reg_pin[0].shape[0] < m:
+            if self._reg_pin is None or self._reg_pin["x4"].shape[0] < m:
                 cap = max(m, 1 << 14)
-                self._reg_pin = (torch.empty((cap, 4), dtype=torch.float32, pin_memory=True),
-                                 torch.empty(cap, dtype=torch.int32, pin_memory=True))
-            hp, ha = self._reg_pin
+                self._reg_pin = {"x4": torch.empty((cap, 4), dtype=torch.float32, pin_memory=True),
+                                 "x3": torch.empty((cap, 3), dtype=torch.float32, pin_memory=True),
+                                 "t": torch.empty(cap, dtype=torch.float32, pin_memory=True),
+                                 "a": torch.empty(cap, dtype=torch.int32, pin_memory=True),
+                                 "d3": torch.empty((cap, 3), dtype=torch.float32, device=d),
+                                 "dt": torch.empty(cap, dtype=torch.float32, device=d)}
+            pin = self._reg_pin
             if self._reg_ev is not None:
                 self._reg_ev.synchronize()  # the previous call's copies out of the pinned buffers are done
-            hn = hp.numpy()
-            hn[:m, :3] = x[:, :3]
-            hn[:m, 3] = x[:, 3] if x.shape[1] == 4 else np.asarray(t, np.float32)
-            ha.numpy()[:m] = np.asarray(attr).view(np.int32)
+            pin["a"].numpy()[:m] = np.asarray(attr).view(np.int32)
             with torch.cuda.stream(self.stream):
-                self.f_raw[:m].copy_(hp[:m], non_blocking=True)
-                self.f_attr[:m].copy_(ha[:m], non_blocking=True)
+                if x.ndim == 2 and x.shape[1] == 4:  # x, y, z, t already interleaved: one copy
+                    pin["x4"].numpy()[:m] = x
+                    self.f_raw[:m].copy_(pin["x4"][:m], non_blocking=True)
+                else:
+                    # contiguous host copies only; the interleave is two strided copies on the device
+                    pin["x3"].numpy()[:m] = x[:, :3]
+                    pin["t"].numpy()[:m] = np.asarray(t, np.float32)
+                    pin["d3"][:m].copy_(pin["x3"][:m], non_blocking=True)
+                    pin["dt"][:m].copy_(pin["t"][:m], non_blocking=True)
+                    self.f_raw[:m, :3].copy_(pin["d3"][:m])
+                    self.f_raw[:m, 3].copy_(pin["dt"][:m])
+                self.f_attr[:m].copy_(pin["a"][:m], non_blocking=True)
                 self._reg_ev = torch.cuda.Event()
                 self._reg_ev.record(self.stream)
             raw, at = self.f_raw, self.f_attr
@@ -418,9 +433,12 @@ class Odometry:
     def registration(self):
         """(T, ok, stats) of the last register_frame (synchronises the stream). stats["err"] is non-zero when a
         registration since the last reset gave up (a bounded wait ran out, or a fixed-point sum overflowed)."""
-        st = self.read_state()
         with torch.cuda.stream(self.stream):
-            err = int(self._gn.err.cpu()[0])
+            self._state_host.copy_(self._state, non_blocking=True)
+            self._err_host.copy_(self._gn.err, non_blocking=True)
+        self.stream.synchronize()
+        st = _lib.OdomState.from_buffer_copy(self._state_host.numpy())
+        err = int(self._err_host[0])
         stats = {"ds": st.n_ds, "iters": st.iters, "corr": st.corr, "rms": st.rms, "cond": st.cond,
                  "weak": bool(st.weak), "degen": st.degen, "err": err}
         return np.array(st.T_reg, dtype=np.float64).reshape(4, 4), bool(st.ok), stats
