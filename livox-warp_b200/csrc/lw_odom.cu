@@ -409,7 +409,7 @@ __global__ void k_reg_refresh_all(lw_regmap reg, lw_rec_params rp) {
 // (2 reach + 1)^3 neighbour voxels between them, B probes in flight per lane (B = 8: two batches of independent
 // loads cover the 125 voxels of the wide search; B = 4: one batch the 27 of the narrow one; with 4736 groups a
 // frame's points need a single round), reduce to the closest mean in reference order by shuffles, and then split
-// the point's 53 weighted terms between them by column pairs of H and Hg (term_index), from the matched voxel's
+// the point's 53 weighted terms between them by column pairs of H and Hg (term_slot), from the matched voxel's
 // record that every lane reads. The Jacobian is
 // taken about a point near the frame (the predicted sensor position) so float32 keeps its precision far from the
 // world origin; the float64 reduction maps H, b and Hg back to the reference's twist about the world origin.
@@ -568,43 +568,42 @@ __device__ __forceinline__ void icp_search27(int lane_g, int R, int bx, int by, 
     }
 }
 
-// Row p of the Jacobian columns at the re-centred point l (odom.py:305-307): e_p for p < 3, then the rows of
-// -[l]x: (0, -lz, ly), (lz, 0, -lx), (-ly, lx, 0).
-__device__ __forceinline__ void jac_row(int p, float lx, float ly, float lz, float& a, float& b, float& c) {
-    a = p == 0 ? 1.0f : (p == 4 ? lz : (p == 5 ? -ly : 0.0f));
-    b = p == 1 ? 1.0f : (p == 3 ? -lz : (p == 5 ? lx : 0.0f));
-    c = p == 2 ? 1.0f : (p == 3 ? ly : (p == 4 ? -lx : 0.0f));
-}
-
 // How a group of 8 lanes splits a point's 53 accumulator terms, 7 per lane: lanes 0-2 take column pairs (0, 5),
 // (1, 4), (2, 3) of H = sum w J^T M J (1 + 6, 2 + 5, 3 + 4 upper-triangle entries), lanes 3-5 the same of Hg
 // (precision Mg), lane 6 b = sum w J^T M r and the count, lane 7 the weighted error, rms, weight and range. Each of
-// lanes 0-6 forms its two matrix-vector products W v once and then dots them with the Jacobian rows.
+// lanes 0-6 forms its two matrix-vector products W v once and then every Jacobian row against both (J w = (w, w x l)
+// at the re-centred point l; odom.py:305-307), and picks its seven.
 constexpr int TERM_LANES = 8;
 constexpr int TERMS_PER_LANE = 7;
 
 __device__ __forceinline__ int triu6(int p, int q) { return p * 6 - (p * (p - 1)) / 2 + (q - p); }
 
-// Accumulator index of lane lg's term u (LW_ACC_* layout), -1 for none; p / q receive the H entry's row / column.
-__device__ __forceinline__ int term_index(int lg, int u, int& p, int& q) {
-    p = 0;
-    q = 0;
-    if (lg < 6) {
-        const int qa = lg % 3, qb = 5 - qa;
-        if (u <= qa) {
-            p = u;
-            q = qa;
-        } else {
-            p = u - qa - 1;
-            q = qb;
-        }
-        return (lg < 3 ? LW_ACC_H : LW_ACC_HG) + triu6(p, q);
+// (p, q) of the 21 upper-triangle entries of a symmetric 6x6 in row-major order (the accumulator's layout), 3 bits
+// each.
+__host__ __device__ constexpr uint64_t triu6_code(bool want_q) {
+    uint64_t v = 0;
+    int t = 0;
+    for (int p = 0; p < 6; ++p)
+        for (int q = p; q < 6; ++q, ++t) v |= (uint64_t)(want_q ? q : p) << (3 * t);
+    return v;
+}
+constexpr uint64_t TRIU6_P = triu6_code(false);
+constexpr uint64_t TRIU6_Q = triu6_code(true);
+__host__ __device__ constexpr int triu6c(int i, int j) {
+    return i <= j ? i * 6 - (i * (i - 1)) / 2 + (j - i) : j * 6 - (j * (j - 1)) / 2 + (i - j);
+}
+
+// Where lane lg of a group keeps its term u in the CTA's term rows (lg * 7 + u), seen from accumulator entry t:
+// lanes 0-2 hold H's column pairs (q, 5 - q), lanes 3-5 Hg's, lane 6 b and the count, lane 7 the stats.
+__device__ __forceinline__ int term_slot(int t) {
+    if (t < LW_ACC_B || (t >= LW_ACC_HG && t < NTERMS)) {
+        const int e = t < LW_ACC_B ? t : t - LW_ACC_HG;
+        const int p = (int)((TRIU6_P >> (3 * e)) & 7u), q = (int)((TRIU6_Q >> (3 * e)) & 7u);  // p <= q
+        const int qa = q < 3 ? q : 5 - q;
+        return ((t < LW_ACC_B ? 0 : 3) + qa) * TERMS_PER_LANE + (q == qa ? p : qa + 1 + p);
     }
-    if (lg == 6) {
-        p = u;
-        return u < 6 ? LW_ACC_B + u : LW_ACC_COUNT;
-    }
-    return u < 4 ? LW_ACC_ERR + u : -1;  // err, rms, weight, range
+    if (t <= LW_ACC_COUNT) return 6 * TERMS_PER_LANE + (t - LW_ACC_B);  // b, then the count
+    return 7 * TERMS_PER_LANE + (t - LW_ACC_ERR);                       // err, rms, weight, range
 }
 
 // Fixed point of the cross-CTA sums of the Gauss-Newton loop: 2^-16 units. The largest term a frame can produce
@@ -805,31 +804,41 @@ __device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P,
         wgt = wgt * wgt;  // Geman-McClure
         const float rn = (h4.w > 0.5f) ? fmaf(r0, h4.x, fmaf(r1, h4.y, r2 * h4.z))
                                        : sqrtf(fmaf(r0, r0, fmaf(r1, r1, r2 * r2)));
-        // this lane's two matrix-vector products: W (M for H and b, Mg for Hg) times its two columns' vectors
-        // (Jacobian rows qa, qb; the residual r for the b lane)
-        const int qa = lane_g % 3, qb = 5 - qa;
-        const float* W = (lane_g >= 3 && lane_g < 6) ? Mg : M;
-        float va, vb, vc, xa, xb, xc;
-        jac_row(qa, lx, ly, lz, va, vb, vc);
-        jac_row(qb, lx, ly, lz, xa, xb, xc);
+        // this lane's two matrix-vector products: W (M for H and b, Mg for Hg) times its two columns' vectors,
+        // Jacobian rows qa and qb (the residual r for the b lane); a unit row picks W's column as it is
+        const int qa = lane_g % 3;
+        const bool hg = lane_g >= 3 && lane_g < 6;
+        float W[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) W[i] = hg ? Mg[i] : M[i];
+        float wa0 = qa == 0 ? W[0] : (qa == 1 ? W[1] : W[2]);
+        float wa1 = qa == 0 ? W[1] : (qa == 1 ? W[3] : W[4]);
+        float wa2 = qa == 0 ? W[2] : (qa == 1 ? W[4] : W[5]);
         if (lane_g == 6) {
-            va = r0;
-            vb = r1;
-            vc = r2;
+            wa0 = Mr0;
+            wa1 = Mr1;
+            wa2 = Mr2;
         }
-        const float wa0 = fmaf(W[0], va, fmaf(W[1], vb, W[2] * vc));
-        const float wa1 = fmaf(W[1], va, fmaf(W[3], vb, W[4] * vc));
-        const float wa2 = fmaf(W[2], va, fmaf(W[4], vb, W[5] * vc));
+        // row qb = 5 - qa of J: (0, -lz, ly), (lz, 0, -lx) or (-ly, lx, 0)
+        const float xa = qa == 2 ? 0.0f : (qa == 1 ? lz : -ly);
+        const float xb = qa == 2 ? -lz : (qa == 1 ? 0.0f : lx);
+        const float xc = qa == 2 ? ly : (qa == 1 ? -lx : 0.0f);
         const float wb0 = fmaf(W[0], xa, fmaf(W[1], xb, W[2] * xc));
         const float wb1 = fmaf(W[1], xa, fmaf(W[3], xb, W[4] * xc));
         const float wb2 = fmaf(W[2], xa, fmaf(W[4], xb, W[5] * xc));
+        // every Jacobian row against both products: J w = (w, w x l) in the rows' own expressions
+        const float A[6] = {wa0, wa1, wa2, fmaf(-lz, wa1, ly * wa2), fmaf(lz, wa0, -lx * wa2),
+                            fmaf(-ly, wa0, lx * wa1)};
+        const float Bv[6] = {wb0, wb1, wb2, fmaf(-lz, wb1, ly * wb2), fmaf(lz, wb0, -lx * wb2),
+                             fmaf(-ly, wb0, lx * wb1)};
 #pragma unroll
         for (int u = 0; u < TPL; ++u) {
-            const bool first = lane_g == 6 || u <= qa;
-            const int pr = lane_g == 6 ? u : (u <= qa ? u : u - qa - 1);
-            float ua, ub, uc;
-            jac_row(pr, lx, ly, lz, ua, ub, uc);
-            float x = first ? fmaf(ua, wa0, fmaf(ub, wa1, uc * wa2)) : fmaf(ua, wb0, fmaf(ub, wb1, uc * wb2));
+            // term u: row u against column qa while u <= qa, then rows 0.. against column qb (the b lane: rows
+            // against M r, then the count)
+            const float b1 = u >= 1 ? Bv[u - 1] : 0.0f, b2 = u >= 2 ? Bv[u - 2] : 0.0f, b3 = u >= 3 ? Bv[u - 3] : 0.0f;
+            const float bsel = qa == 0 ? b1 : (qa == 1 ? b2 : b3);
+            const float asel = u < 6 ? A[u < 6 ? u : 0] : 0.0f;
+            float x = (u <= qa || (lane_g == 6 && u < 6)) ? asel : bsel;
             x *= wgt;
             if (lane_g == 6 && u == 6) x = 1.0f;  // the count
             if (lane_g == 7) x = u == 0 ? wgt * d2 : (u == 1 ? wgt * (rn * rn) : (u == 2 ? wgt : (u == 3 ? p.w : 0.0f)));
@@ -845,17 +854,14 @@ __device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P,
     const int warp = threadIdx.x >> 5;
     if (lane < G) {
 #pragma unroll
-        for (int u = 0; u < TPL; ++u) {
-            int tp, tq;
-            const int t = term_index(lane_g, u, tp, tq);
-            if (t >= 0) tacc[warp][t] = acc[u];
-        }
+        for (int u = 0; u < TPL; ++u) tacc[warp][lane * TPL + u] = acc[u];
     }
     __syncthreads();
     if (threadIdx.x < NTERMS) {
+        const int slot = term_slot(threadIdx.x);
         double sum = 0.0;
 #pragma unroll
-        for (int w = 0; w < GN_THREADS / 32; ++w) sum += (double)tacc[w][threadIdx.x];
+        for (int w = 0; w < GN_THREADS / 32; ++w) sum += (double)tacc[w][slot];
         if (fixed) {
             // integer atomics commute: every CTA reads back the same exact sum, whatever the arrival order
             double q = rint(sum * GN_FIX);
@@ -1461,21 +1467,6 @@ __device__ __forceinline__ double kneg(const double* c, int k, int m) {
 }
 
 __device__ __forceinline__ void pair_sync() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
-
-// (p, q) of the 21 upper-triangle entries of a symmetric 6x6 in row-major order (the accumulator's layout), 3 bits
-// each.
-__host__ __device__ constexpr uint64_t triu6_code(bool want_q) {
-    uint64_t v = 0;
-    int t = 0;
-    for (int p = 0; p < 6; ++p)
-        for (int q = p; q < 6; ++q, ++t) v |= (uint64_t)(want_q ? q : p) << (3 * t);
-    return v;
-}
-constexpr uint64_t TRIU6_P = triu6_code(false);
-constexpr uint64_t TRIU6_Q = triu6_code(true);
-__host__ __device__ constexpr int triu6c(int i, int j) {
-    return i <= j ? i * 6 - (i * (i - 1)) / 2 + (j - i) : j * 6 - (j * (j - 1)) / 2 + (i - j);
-}
 
 // u^T M v for a symmetric 6x6 M stored as its packed upper triangle: unrolled, every load of M is a fixed offset and
 // the six row sums are independent chains.
