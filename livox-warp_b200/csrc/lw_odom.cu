@@ -110,7 +110,38 @@ struct ThinArgs {
     int ret_mask;
     int deskew;      // 1: pass A deskews f_raw into f_xyz first
     float t_mid, inv_dt;
+    // with pf_keys set, pass A also warms L2 for the Gauss-Newton pass that follows (prefetch_neighbourhood)
+    const int64_t* pf_keys;
+    const float* pf_rec;
+    const double* pf_T;  // the predicted pose (device)
+    int pf_mask;
+    float pf_inv_v;      // 1 / registration voxel
 };
+
+__device__ __forceinline__ void prefetch_l2(const void* ptr) { asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr)); }
+
+// A hint for the registration that follows the thinning, whose first pass would otherwise meet a cold L2: prefetch
+// the hash slot where the point's registration voxel (at the predicted pose) is first looked for and that slot's
+// record, and for every fourth point the first slots of the 26 neighbouring voxels too. Nothing is read back, so
+// an imprecise voxel or a key stored further along its probe sequence only leaves a miss for later.
+__device__ __forceinline__ void prefetch_neighbourhood(const ThinArgs& a, const float4& p, int64_t i) {
+    const double* T = a.pf_T;
+    const float wx = (float)T[0] * p.x + (float)T[1] * p.y + (float)T[2] * p.z + (float)T[3];
+    const float wy = (float)T[4] * p.x + (float)T[5] * p.y + (float)T[6] * p.z + (float)T[7];
+    const float wz = (float)T[8] * p.x + (float)T[9] * p.y + (float)T[10] * p.z + (float)T[11];
+    const int bx = ifloor(wx * a.pf_inv_v), by = ifloor(wy * a.pf_inv_v), bz = ifloor(wz * a.pf_inv_v);
+    const int h = slot_hash(key_ijk(bx, by, bz)) & a.pf_mask;
+    prefetch_l2(a.pf_keys + h);
+    prefetch_l2(a.pf_rec + (int64_t)h * LW_REC_FLOATS);
+    if ((i & 3) == 0) {
+#pragma unroll 1
+        for (int o = 0; o < 27; ++o) {
+            if (o == 13) continue;  // the voxel itself
+            const int hn = slot_hash(key_ijk(bx + o / 9 - 1, by + (o / 3) % 3 - 1, bz + o % 3 - 1)) & a.pf_mask;
+            prefetch_l2(a.pf_keys + hn);
+        }
+    }
+}
 
 // The frame's point count and twist come from the state when `st` is set, else from the arguments.
 struct Tw6 {
@@ -147,6 +178,7 @@ __global__ void k_thin_a(lw_frame_buf fb, const int* __restrict__ m_dev, ThinArg
         float r = len3(p.x, p.y, p.z);
         uint32_t at = fb.f_attr[i];
         if (!(r < a.min_range || r > a.max_range) && tag_of(at) == 0 && ((1 << ret_of(at)) & a.ret_mask) != 0) {
+            if (a.pf_keys) prefetch_neighbourhood(a, p, i);
             int64_t key = key_ijk(ifloor(p.x * a.inv_v), ifloor(p.y * a.inv_v), ifloor(p.z * a.inv_v));
             bool claimed;
             slot = claim_slot(key, fb.ds_keys, mask, &claimed);
@@ -1134,6 +1166,82 @@ __device__ __noinline__ double conditioning(const double* H) {
     return fmax(lo, 0.0) / fmax(hi, 1e-12);
 }
 
+__device__ __forceinline__ double pow2_below(double p) {  // 2^-e for p = m 2^e, m in [1, 2), p normal and positive
+    const int e = ((__double2hiint(p) >> 20) & 0x7FF) - 1023;
+    return __hiloint2double((1023 - e) << 20, 0);
+}
+
+// ---- the conditioning statistic -------------------------------------------------------------------------------
+// How many pivots of the elimination of A - x I (symmetric 6x6, in registers) are negative: by Sylvester's law of
+// inertia, the number of A's eigenvalues below x. Each step forms |p| row_i - sign(p) a_ik row_k with |p| scaled
+// by a power of two -- a positive multiple of the Schur complement, so its signs are kept -- and no division; a
+// zero or non-finite pivot is counted as negative and the elimination goes on from -1.
+__device__ __forceinline__ int neg_count6(const double* __restrict__ A, double x) {
+    double a[36];
+#pragma unroll
+    for (int e = 0; e < 36; ++e) a[e] = A[e];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) a[k * 7] -= x;
+    int neg = 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        double p = a[k * 7];
+        if (!(p > 0.0)) {
+            ++neg;
+            if (!(p < -1e-290 && p > -1e290)) p = -1.0;
+        } else if (!(p > 1e-290 && p < 1e290)) {
+            p = 1.0;
+        }
+        const double ap = fabs(p);
+        const double sc = pow2_below(ap);
+        const double ps = ap * sc;
+        const double sg = p > 0.0 ? sc : -sc;
+#pragma unroll
+        for (int i = k + 1; i < 6; ++i) {
+            const double f = a[k * 6 + i] * sg;
+#pragma unroll
+            for (int j = i; j < 6; ++j) a[i * 6 + j] = fma(ps, a[i * 6 + j], -(f * a[k * 6 + j]));
+        }
+    }
+    return neg;
+}
+
+// min(lambda) / max(lambda) of a positive semi-definite 6x6 with unit diagonal (H normalised by its diagonal,
+// odom.py:797-800), on one warp, without an eigen-decomposition: with a unit diagonal lambda_min <= 1 <= lambda_max
+// <= 6, and the count of eigenvalues below a shift brackets each end. Every round, lanes 0-15 try 16 shifts on a
+// logarithmic grid over lambda_min's bracket (from 2^-46.5 ~ 1e-14 up to 1) and lanes 16-31 16 shifts on a linear
+// grid over lambda_max's (1 to 6); each end keeps the sixteenth of its bracket where the count first reaches 1
+// (respectively 6). Four rounds leave lambda_max within ~1e-4 and lambda_min within ~5e-4 relative; a lambda_min
+// below the grid's floor is taken as 0. Every lane returns the ratio.
+__device__ double cond6_warp(const double* __restrict__ A) {
+    constexpr float LOG2_FLOOR = -46.5f;
+    const int lane = threadIdx.x & 31;
+    const bool low = lane < 16;
+    const int kk = lane & 15;
+    float lo = low ? LOG2_FLOOR : 1.0f, hi = low ? 0.0f : 6.0f;
+#pragma unroll 1
+    for (int r = 0; r < 4; ++r) {
+        const float g = lo + (hi - lo) * (float)(kk + 1) * (1.0f / 16.0f);
+        const double x = low ? (double)exp2f(g) : (double)g;
+        const int c = neg_count6(A, x);
+        const unsigned m = __ballot_sync(0xffffffffu, low ? c >= 1 : c >= 6);
+        const unsigned mine = low ? (m & 0xFFFFu) : (m >> 16);
+        if (mine == 0u) {
+            lo = hi;  // above the bracket's top (rounding): pin it there
+        } else {
+            const int k = __ffs(mine) - 1;
+            const float w = (hi - lo) * (1.0f / 16.0f);
+            lo = lo + w * (float)k;
+            hi = lo + w;
+        }
+    }
+    const float l0 = __shfl_sync(0xffffffffu, lo, 0), h0 = __shfl_sync(0xffffffffu, hi, 0);
+    const float l1 = __shfl_sync(0xffffffffu, lo, 16), h1 = __shfl_sync(0xffffffffu, hi, 16);
+    const double lmin = l0 <= LOG2_FLOOR ? 0.0 : (double)exp2f(0.5f * (l0 + h0));
+    const double lmax = 0.5 * ((double)l1 + (double)h1);
+    return fmax(lmin, 0.0) / fmax(lmax, 1e-12);
+}
+
 // ---- the float64 step --------------------------------------------------------------------------------------
 // Every CTA of the persistent kernel runs the same step on the same reduced accumulator (so one grid barrier per
 // iteration suffices). The step is a chain of dependent float64 operations, so its cost is latency: the 6x6
@@ -1291,10 +1399,6 @@ __device__ __forceinline__ double rcp_newton(double d) {
 // complement by a positive factor, so the pivots carry the signs of the L D L^T pivots. Returns 0 unless every
 // pivot is positive (the shifted matrix positive definite). With rhs, the right-hand side is carried along and
 // x receives the solution: the six reciprocals are taken together, then the back substitution only multiplies.
-__device__ __forceinline__ double pow2_below(double p) {  // 2^-e for p = m 2^e, m in [1, 2), p normal and positive
-    const int e = ((__double2hiint(p) >> 20) & 0x7FF) - 1023;
-    return __hiloint2double((1023 - e) << 20, 0);
-}
 
 __device__ __forceinline__ int elim6(double* a, double st, double sr, double* rhs, double* x) {
 #pragma unroll
@@ -1727,19 +1831,13 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
             S.EA[e] = S.H[e] / (sqrt(fmax(S.H[i * 7], 1e-12)) * sqrt(fmax(S.H[j * 7], 1e-12)));
         }
         __syncwarp();
-        jacobi6_warp<false>(S.EA, nullptr, S.ev, S.rot, false);
+        const double c = cond6_warp(S.EA);
+        if (threadIdx.x == 0) S.ev[0] = c;
     }
+    __syncthreads();
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         bool ok = s_corr >= prm.min_corr;
-        double cond = st->cond;
-        if (ok) {
-            double lo = S.ev[0], hi = S.ev[0];
-            for (int k = 1; k < 6; ++k) {
-                lo = fmin(lo, S.ev[k]);
-                hi = fmax(hi, S.ev[k]);
-            }
-            cond = fmax(lo, 0.0) / fmax(hi, 1e-12);
-        }
+        const double cond = ok ? S.ev[0] : st->cond;
         for (int i = 0; i < 16; ++i) st->T_reg[i] = S.T[i];
         st->ok = ok ? 1 : 0;
         st->n_ds = n;
@@ -1989,6 +2087,22 @@ static ThinArgs thin_args(const lw_odom_params* prm) {
     a.deskew = 1;
     a.t_mid = 0.0f;
     a.inv_dt = (float)(1.0 / prm->frame_dt);
+    a.pf_keys = nullptr;
+    a.pf_rec = nullptr;
+    a.pf_T = nullptr;
+    a.pf_mask = 0;
+    a.pf_inv_v = 0.0f;
+    return a;
+}
+
+// thin_args with the L2 prefetch for the registration against `reg` from the predicted pose in `st`
+static ThinArgs thin_args_prefetch(const lw_odom_params* prm, const lw_regmap* reg, const lw_odom_state* st) {
+    ThinArgs a = thin_args(prm);
+    a.pf_keys = reg->keys;
+    a.pf_rec = reg->rec;
+    a.pf_T = st->T_pred;
+    a.pf_mask = (int)(reg->cap - 1);
+    a.pf_inv_v = (float)(1.0 / prm->reg_voxel);
     return a;
 }
 
@@ -2220,7 +2334,7 @@ int lw_register_frame(const float* raw4, const uint32_t* attr, int64_t m, double
     lw_frame_buf f = *fb;
     f.f_raw = const_cast<float*>(raw4);
     f.f_attr = const_cast<uint32_t*>(attr);
-    ThinArgs a = thin_args(prm);
+    ThinArgs a = thin_args_prefetch(prm, reg, st);
     a.t_mid = (float)t_mid;
     Tw6 tw;
     for (int k = 0; k < 6; ++k) tw.v[k] = twist6_host[k];
@@ -2265,7 +2379,7 @@ static int finalize_impl(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_
     // first registration: deskew with the predicted motion, thin, Gauss-Newton
     {
         ProfScope prof("thin", s);
-        k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, ta, st, tw, nullptr, &st->run_reg, 1);
+        k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, thin_args_prefetch(prm, reg, st), st, tw, nullptr, &st->run_reg, 1);
         k_thin_b<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->run_reg);
         k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->run_reg);
     }
