@@ -1379,11 +1379,10 @@ __device__ __forceinline__ void chol6_solve(const double* Lf, const double* rhs,
     }
 }
 
-// 1 / d for d > 0 on a chain of dependent operations: the PTX approximate reciprocal refined by two Newton-Raphson
-// steps r <- r + r (1 - d r), each of which doubles the number of correct bits, to within an ulp or so of the
-// rounded quotient. Outside the normal range (where the approximation flushes) the division itself.
-__device__ __forceinline__ double rcp_newton(double d) {
-    if (!(d > 1e-300 && d < 1e300)) return 1.0 / d;
+// 1 / d for a normal d of moderate size (the caller has checked it) on a chain of dependent operations: the PTX
+// approximate reciprocal refined by two Newton-Raphson steps r <- r + r (1 - d r), each of which doubles the number
+// of correct bits, to within an ulp or so of the rounded quotient.
+__device__ __forceinline__ double rcp_newton_normal(double d) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
     double e = fma(-d, r, 1.0);
@@ -1403,10 +1402,13 @@ __device__ __forceinline__ double rcp_newton(double d) {
 __device__ __forceinline__ int elim6(double* a, double st, double sr, double* rhs, double* x) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) a[k * 7] -= k < 3 ? st : sr;
+    int ok = 1;  // no early exit: a branch per pivot would hold the next steps back
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-        const double p = a[k * 7];
-        if (!(p > 1e-300 && p < 1e300)) return 0;
+        double p = a[k * 7];
+        const bool good = p > 1e-300 && p < 1e300;
+        ok &= good ? 1 : 0;
+        p = good ? p : 1.0;  // a failed factor goes on with finite numbers and is discarded
         const double sc = pow2_below(p);
         const double ps = p * sc;
 #pragma unroll
@@ -1417,10 +1419,10 @@ __device__ __forceinline__ int elim6(double* a, double st, double sr, double* rh
             if (rhs) rhs[i] = fma(ps, rhs[i], -(f * rhs[k]));
         }
     }
-    if (!rhs) return 1;
+    if (!rhs) return ok;
     double r[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) r[k] = rcp_newton(a[k * 7]);
+    for (int k = 0; k < 6; ++k) r[k] = rcp_newton_normal(a[k * 7]);  // the pivots passed the range test
     double acc[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) acc[k] = rhs[k];
@@ -1430,7 +1432,7 @@ __device__ __forceinline__ int elim6(double* a, double st, double sr, double* rh
 #pragma unroll
         for (int i = 0; i < k; ++i) acc[i] = fma(-a[i * 6 + k], x[k], acc[i]);
     }
-    return 1;
+    return ok;
 }
 
 // The degenerate branch of odom.py:436-455 (some direction below degen_thr): with G's eigen-decomposition in
