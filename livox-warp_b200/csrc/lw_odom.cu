@@ -113,7 +113,8 @@ struct ThinArgs {
     // with pf_keys set, pass A also warms L2 for the Gauss-Newton pass that follows (prefetch_neighbourhood)
     const int64_t* pf_keys;
     const float* pf_rec;
-    const double* pf_T;  // the predicted pose (device)
+    const double* pf_T;  // the predicted pose (device), or null to use pf_Tv
+    float pf_Tv[12];     // the predicted pose's first three rows, by value
     int pf_mask;
     float pf_inv_v;      // 1 / registration voxel
 };
@@ -125,10 +126,12 @@ __device__ __forceinline__ void prefetch_l2(const void* ptr) { asm volatile("pre
 // record, and for every fourth point the first slots of the 26 neighbouring voxels too. Nothing is read back, so
 // an imprecise voxel or a key stored further along its probe sequence only leaves a miss for later.
 __device__ __forceinline__ void prefetch_neighbourhood(const ThinArgs& a, const float4& p, int64_t i) {
-    const double* T = a.pf_T;
-    const float wx = (float)T[0] * p.x + (float)T[1] * p.y + (float)T[2] * p.z + (float)T[3];
-    const float wy = (float)T[4] * p.x + (float)T[5] * p.y + (float)T[6] * p.z + (float)T[7];
-    const float wz = (float)T[8] * p.x + (float)T[9] * p.y + (float)T[10] * p.z + (float)T[11];
+    float T[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) T[i] = a.pf_T ? (float)a.pf_T[i] : a.pf_Tv[i];
+    const float wx = T[0] * p.x + T[1] * p.y + T[2] * p.z + T[3];
+    const float wy = T[4] * p.x + T[5] * p.y + T[6] * p.z + T[7];
+    const float wz = T[8] * p.x + T[9] * p.y + T[10] * p.z + T[11];
     const int bx = ifloor(wx * a.pf_inv_v), by = ifloor(wy * a.pf_inv_v), bz = ifloor(wz * a.pf_inv_v);
     const int h = slot_hash(key_ijk(bx, by, bz)) & a.pf_mask;
     prefetch_l2(a.pf_keys + h);
@@ -148,11 +151,49 @@ struct Tw6 {
     float v[6];
 };
 
+struct RegBegin {
+    double T[16];
+    double t_mid;
+    float tw[6];
+    int m;
+};
+
+// What a single-frame registration sets up before its first pass (lw_register_frame), done by block 0 of the first
+// thinning pass instead of kernels of its own: the registration's start state, and the Gauss-Newton launch's
+// fixed-point accumulators and barrier count cleared. With `on`, the pass takes its point count from `m`.
+struct ThinBegin {
+    lw_odom_state* st;
+    long long* part;  // [3 * LW_ACC_STRIDE] to clear
+    uint32_t* bar;    // [2] to clear
+    RegBegin b;
+    int on;
+};
+
+__device__ __forceinline__ void reg_begin(lw_odom_state* st, const RegBegin& b) {
+    const int t = threadIdx.x;
+    if (t < 16) st->T_pred[t] = b.T[t];
+    if (t < 6) st->xi_used[t] = b.tw[t];
+    if (t < 16) st->T_reg[t] = b.T[t];  // what a registration that gives up leaves: the prediction, not ok
+    if (t == 0) {
+        st->t_mid = b.t_mid;
+        st->m = b.m;
+        st->n_ds = 0;
+        st->ok = 0;
+        st->iters = 0;
+        st->corr = 0;
+    }
+}
+
 __global__ void k_thin_a(lw_frame_buf fb, const int* __restrict__ m_dev, ThinArgs a, const lw_odom_state* st,
-                         Tw6 tw_arg, const int* gate_deskew, const int* gate_thin, int thin_on) {
+                         Tw6 tw_arg, const int* gate_deskew, const int* gate_thin, int thin_on, ThinBegin bg) {
+    if (bg.on && blockIdx.x == 0) {
+        reg_begin(bg.st, bg.b);
+        for (int e = threadIdx.x; e < 3 * LW_ACC_STRIDE; e += blockDim.x) bg.part[e] = 0;
+        if (threadIdx.x < 2) bg.bar[threadIdx.x] = 0;
+    }
     if (gate_deskew && *gate_deskew == 0) return;
     const bool thin = thin_on && !(gate_thin && *gate_thin == 0);
-    int64_t m = *m_dev;
+    int64_t m = bg.on ? (int64_t)bg.b.m : (int64_t)*m_dev;
     if (m > fb.cap) m = fb.cap;
     float tw[6];
     float t_mid = a.t_mid;
@@ -2026,27 +2067,8 @@ __global__ void k_reset_state(lw_odom_state* st, lw_odom_state init) { *st = ini
 
 // The start of a single-frame registration (lw_register_frame): the prediction, the frame's point count, its
 // mid time and the twist it is deskewed with, into the device state.
-struct RegBegin {
-    double T[16];
-    double t_mid;
-    float tw[6];
-    int m;
-};
 
-__global__ void k_reg_begin(lw_odom_state* st, RegBegin b) {
-    const int t = threadIdx.x;
-    if (t < 16) st->T_pred[t] = b.T[t];
-    if (t < 6) st->xi_used[t] = b.tw[t];
-    if (t < 16) st->T_reg[t] = b.T[t];  // what a registration that gives up leaves: the prediction, not ok
-    if (t == 0) {
-        st->t_mid = b.t_mid;
-        st->m = b.m;
-        st->n_ds = 0;
-        st->ok = 0;
-        st->iters = 0;
-        st->corr = 0;
-    }
-}
+__global__ void k_reg_begin(lw_odom_state* st, RegBegin b) { reg_begin(st, b); }
 
 __global__ void k_zero_count(int* c) { *c = 0; }
 
@@ -2119,7 +2141,7 @@ static lw_rec_params rec_params(const lw_odom_params* prm) {
 }
 
 static int launch_gn(const float* ds4, const int32_t* n_dev, const lw_odom_params* prm, lw_odom_state* st,
-                     const lw_regmap* reg, lw_gn_scratch* gn, int which, cudaStream_t s) {
+                     const lw_regmap* reg, lw_gn_scratch* gn, int which, cudaStream_t s, bool cleared = false) {
     if (reg->cap > (1LL << SLOT_BITS))
         return set_error(LW_EINVAL, "Gauss-Newton: a registration map of %lld slots (at most 2^25)", (long long)reg->cap);
     int grid = gn_grid(gn);
@@ -2134,8 +2156,10 @@ static int launch_gn(const float* ds4, const int32_t* n_dev, const lw_odom_param
                     (void*)&mask, (void*)&g, (void*)&which};
     // the fixed-point accumulators of the first two iterations start at zero (the kernel clears the rest), and
     // the barrier's arrival count too: a launch that gave up at the barrier may have left it part counted
-    LW_CUDA(cudaMemsetAsync(gn->part, 0, 3 * LW_ACC_STRIDE * sizeof(long long), s));
-    LW_CUDA(cudaMemsetAsync(gn->bar, 0, 2 * sizeof(uint32_t), s));
+    if (!cleared) {
+        LW_CUDA(cudaMemsetAsync(gn->part, 0, 3 * LW_ACC_STRIDE * sizeof(long long), s));
+        LW_CUDA(cudaMemsetAsync(gn->bar, 0, 2 * sizeof(uint32_t), s));
+    }
     static bool smem_set[64] = {};  // the memo's dynamic shared memory is above the default 48 KB
     int dev = 0;
     LW_CUDA(cudaGetDevice(&dev));
@@ -2205,7 +2229,7 @@ int lw_deskew(const float* raw, float* out, const int32_t* m_dev, int64_t m_ub, 
     Tw6 tw;
     for (int k = 0; k < 6; ++k) tw.v[k] = twist6_host[k];
     int grid = blocks_for(m_ub, 256, 8 * device_sms());
-    k_thin_a<<<grid, 256, 0, (cudaStream_t)stream>>>(fb, m_dev, a, nullptr, tw, nullptr, nullptr, 0);
+    k_thin_a<<<grid, 256, 0, (cudaStream_t)stream>>>(fb, m_dev, a, nullptr, tw, nullptr, nullptr, 0, ThinBegin{});
     LW_LAUNCHED("lw_deskew");
     count_launches(1);
     return LW_OK;
@@ -2225,7 +2249,7 @@ int lw_thin(lw_frame_buf* fb, const int32_t* m_dev, int64_t m_ub, double inv_v, 
     Tw6 tw{};
     int grid = blocks_for(m_ub, 256, 8 * device_sms());
     int nt = blocks_for(m_ub, TILE);
-    k_thin_a<<<grid, 256, 0, s>>>(*fb, m_dev, a, nullptr, tw, nullptr, nullptr, 1);
+    k_thin_a<<<grid, 256, 0, s>>>(*fb, m_dev, a, nullptr, tw, nullptr, nullptr, 1, ThinBegin{});
     k_thin_b<<<nt, TILE, 0, s>>>(*fb, m_dev, nullptr);
     k_thin_c<<<nt, TILE, 0, s>>>(*fb, m_dev, n_ds_dev, nullptr);
     LW_LAUNCHED("lw_thin");
@@ -2330,14 +2354,22 @@ int lw_register_frame(const float* raw4, const uint32_t* attr, int64_t m, double
     for (int i = 0; i < 6; ++i) b.tw[i] = twist6_host[i];
     b.t_mid = t_mid;
     b.m = (int)m;
-    k_reg_begin<<<1, 32, 0, s>>>(st, b);
-    // the frame buffer reads the caller's points in place: pass A deskews them into f_xyz and claims the thinning
-    // voxels, B and C keep the lowest-index point of each and write ds_xyz in point order
+    // the frame buffer reads the caller's points in place: pass A (whose block 0 also sets up the registration's
+    // state and clears the Gauss-Newton sums) deskews them into f_xyz and claims the thinning voxels, B and C keep
+    // the lowest-index point of each and write ds_xyz in point order
     lw_frame_buf f = *fb;
     f.f_raw = const_cast<float*>(raw4);
     f.f_attr = const_cast<uint32_t*>(attr);
     ThinArgs a = thin_args_prefetch(prm, reg, st);
+    a.pf_T = nullptr;  // the prediction by value: the state's copy is written by this same launch
+    for (int i = 0; i < 12; ++i) a.pf_Tv[i] = (float)T_pred_host[i];
     a.t_mid = (float)t_mid;
+    ThinBegin bg;
+    bg.st = st;
+    bg.part = reinterpret_cast<long long*>(gn->part);
+    bg.bar = gn->bar;
+    bg.b = b;
+    bg.on = 1;
     Tw6 tw;
     for (int k = 0; k < 6; ++k) tw.v[k] = twist6_host[k];
     const int64_t m_ub = m > 0 ? m : 1;
@@ -2345,14 +2377,14 @@ int lw_register_frame(const float* raw4, const uint32_t* attr, int64_t m, double
     int nt = blocks_for(m_ub, TILE);
     {
         ProfScope prof("thin", s);
-        k_thin_a<<<grid, 256, 0, s>>>(f, &st->m, a, nullptr, tw, nullptr, nullptr, 1);
+        k_thin_a<<<grid, 256, 0, s>>>(f, &st->m, a, nullptr, tw, nullptr, nullptr, 1, bg);
         k_thin_b<<<nt, TILE, 0, s>>>(f, &st->m, nullptr);
         k_thin_c<<<nt, TILE, 0, s>>>(f, &st->m, &st->n_ds, nullptr);
     }
     LW_LAUNCHED("lw_register_frame");
-    count_launches(4);
+    count_launches(3);
     ProfScope prof("gn", s);
-    return launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 2, s);
+    return launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 2, s, /*cleared=*/true);
 }
 
 // The frame's queue of launches; with `net`, the learned start pose replaces the constant-velocity one between
@@ -2381,7 +2413,8 @@ static int finalize_impl(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_
     // first registration: deskew with the predicted motion, thin, Gauss-Newton
     {
         ProfScope prof("thin", s);
-        k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, thin_args_prefetch(prm, reg, st), st, tw, nullptr, &st->run_reg, 1);
+        k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, thin_args_prefetch(prm, reg, st), st, tw, nullptr, &st->run_reg, 1,
+                                      ThinBegin{});
         k_thin_b<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->run_reg);
         k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->run_reg);
     }
@@ -2409,7 +2442,7 @@ static int finalize_impl(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_
     }
     {
         ProfScope prof("thin", s);
-        k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, ta, st, tw, &st->redo, &st->redo, 1);
+        k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, ta, st, tw, &st->redo, &st->redo, 1, ThinBegin{});
         k_thin_b<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->redo);
         k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->redo);
     }
@@ -2599,7 +2632,7 @@ extern "C" int lw_thin_noalloc(const float* xyz4, const uint32_t* attr, int64_t 
     int64_t mu = m > 0 ? m : 1;
     int grid = blocks_for(mu, 256, 8 * device_sms());
     int nt = blocks_for(mu, TILE);
-    k_thin_a<<<grid, 256, 0, s>>>(fb, m_dev, a, nullptr, tw, nullptr, nullptr, 1);
+    k_thin_a<<<grid, 256, 0, s>>>(fb, m_dev, a, nullptr, tw, nullptr, nullptr, 1, ThinBegin{});
     k_thin_b<<<nt, TILE, 0, s>>>(fb, m_dev, nullptr);
     k_thin_c<<<nt, TILE, 0, s>>>(fb, m_dev, n_ds_dev, nullptr);
     LW_LAUNCHED("lw_thin_noalloc");
