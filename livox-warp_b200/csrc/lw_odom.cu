@@ -1856,7 +1856,7 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         __syncthreads();
         if (gn.trace && blockIdx.x == 0 && threadIdx.x < 12 && it + 1 < LW_GN_TRACE)
             gn.trace[(it + 1) * 12 + threadIdx.x] = S.T[threadIdx.x];  // the pose after iteration it
-        if (threadIdx.x == 0) {
+        if (threadIdx.x == 0) {  // read after the loop only (past the barrier below it)
             s_corr = S.corr;
             if (S.status != 2) s_rms = S.rms;
             if (S.status == 0 || S.status == 1) {
@@ -1864,9 +1864,9 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
                 s_degen = S.degen;
             }
         }
-        __syncthreads();
-        if (S.status != 0) break;
+        if (S.status != 0) break;  // S.status was written before the block barrier above
     }
+    __syncthreads();  // thread 0's last s_corr, s_rms, s_iters, s_degen
     if (blockIdx.x == 0 && threadIdx.x < 32 && s_corr >= prm.min_corr) {
         // min/max eigenvalue of H normalised by its diagonal (odom.py:797-800), by warp 0
         for (int e = threadIdx.x; e < 36; e += 32) {
@@ -1913,7 +1913,17 @@ __global__ void k_acc_reduce(const double* part, int grid, double c0, double c1,
 // Frame state machine (odom.py:642-694, 712-727) on one thread.
 // =====================================================================================================
 
-__global__ void k_ctl_begin(int k, lw_odom_params prm, lw_odom_state* st, const int* count) {
+// The Gauss-Newton launch that follows a control kernel needs its fixed-point sums and barrier count at zero; the
+// control kernel's threads clear them, so the launch needs no memsets of its own.
+__device__ __forceinline__ void clear_gn_sums(long long* part, uint32_t* bar) {
+    for (int e = threadIdx.x; e < 3 * LW_ACC_STRIDE; e += blockDim.x) part[e] = 0;
+    if (threadIdx.x < 2) bar[threadIdx.x] = 0;
+}
+
+__global__ void k_ctl_begin(int k, lw_odom_params prm, lw_odom_state* st, const int* count, long long* part,
+                            uint32_t* bar) {
+    clear_gn_sums(part, bar);
+    if (threadIdx.x != 0) return;
     int m = *count;
     if (m > prm.frame_cap) m = prm.frame_cap;
     st->m = m;
@@ -1944,7 +1954,9 @@ __global__ void k_ctl_begin(int k, lw_odom_params prm, lw_odom_state* st, const 
 }
 
 // After the first registration: deskew again with the frame's own motion when it differs (odom.py:673-679).
-__global__ void k_ctl_mid(lw_odom_params prm, lw_odom_state* st) {
+__global__ void k_ctl_mid(lw_odom_params prm, lw_odom_state* st, long long* part, uint32_t* bar) {
+    clear_gn_sums(part, bar);
+    if (threadIdx.x != 0) return;
     st->redo = 0;
     if (!(st->run_reg && st->ok && prm.deskew && prm.redeskew && st->has_prev)) return;
     double Ti[16], D[16], xn[6];
@@ -2408,7 +2420,7 @@ static int finalize_impl(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_
 
     {
         ProfScope prof("control", s);
-        k_ctl_begin<<<1, 1, 0, s>>>(k, *prm, st, fb->count);
+        k_ctl_begin<<<1, 64, 0, s>>>(k, *prm, st, fb->count, reinterpret_cast<long long*>(gn->part), gn->bar);
     }
     // first registration: deskew with the predicted motion, thin, Gauss-Newton
     {
@@ -2432,13 +2444,13 @@ static int finalize_impl(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_
     }
     {
         ProfScope prof("gn", s);
-        r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 0, s);
+        r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 0, s, /*cleared=*/true);
     }
     if (r != LW_OK) return r;
     // re-deskew with the solved motion and register again when it moved enough
     {
         ProfScope prof("control", s);
-        k_ctl_mid<<<1, 1, 0, s>>>(*prm, st);
+        k_ctl_mid<<<1, 64, 0, s>>>(*prm, st, reinterpret_cast<long long*>(gn->part), gn->bar);
     }
     {
         ProfScope prof("thin", s);
@@ -2448,7 +2460,7 @@ static int finalize_impl(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_
     }
     {
         ProfScope prof("gn", s);
-        r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 1, s);
+        r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 1, s, /*cleared=*/true);
     }
     if (r != LW_OK) return r;
     // keyframe, velocity, pose table, trajectory
