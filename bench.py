@@ -459,7 +459,7 @@ LEARN_TRAIN_SEEDS = tuple(range(101, 109))  # 8 paths x 600 frames, 10 pairs per
 LEARN_EVAL_SEEDS = (201, 202, 203)
 LEARN_FRAMES = 600
 LEARN_V, LEARN_W = 2.0, 120.0  # path limits: <= 2 m/s (cruise 1.4 m/s), <= 120 deg/s
-LEARN_SIGMA = (0.03, 0.03, 0.03, 0.02, 0.02, 0.02)  # m, rad: perturbations of the converged pose for training
+LEARN_SIGMA = (0.015, 0.015, 0.015, 0.006, 0.006, 0.006)  # m, rad: perturbations of the converged pose for training
 
 
 def _learn_chunk(args):
