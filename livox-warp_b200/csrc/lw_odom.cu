@@ -1302,7 +1302,7 @@ struct GnSmem {
     int have_v, dstat;                      // EV holds an earlier iteration's vectors; the degenerate step's status
     double T[16], Tp[16], c[3];
     double SB0[36], P0[36], P0xi[6];       // from the pose alone, formed while the grid barrier waits
-    double L, invL, rms, dmean;
+    double L;
     int status, corr, degen;
 };
 
@@ -1629,39 +1629,38 @@ __device__ __forceinline__ double sym_bilinear(const double* M, const double (&u
     return ((r[0] + r[1]) + (r[2] + r[3])) + (r[4] + r[5]);
 }
 
-// A = H + LM damping + prior information and rhs = -b + prior (xi) (odom.py:772-785), formed in registers by one
-// thread and solved by elimination (elim6); A and rhs also go to shared memory for the degenerate branch. 0 when A
-// is not positive definite.
+// A = H + LM damping + prior information and rhs = -b + prior (xi) (odom.py:772-785), from the first phase's threads
+// plus the 1e-9 mean-diagonal term and the prior's L^2 terms, solved in registers by one thread (elim6); what it
+// adds goes back to shared memory for the degenerate branch. 0 when A is not positive definite.
 __device__ __forceinline__ int gn_solve_thread(GnSmem& S, const lw_odom_params& prm, double* delta) {
-    const double pl2 = prm.prior_info > 0.0 ? prm.prior_info * S.L * S.L : 0.0;
-    const double dmean = ((S.H[0] + S.H[7]) + (S.H[14] + S.H[21]) + (S.H[28] + S.H[35])) * (1.0 / 6.0);
-    S.dmean = dmean;
+    const double dm = ((S.H[0] + S.H[7]) + (S.H[14] + S.H[21]) + (S.H[28] + S.H[35])) * (1e-9 / 6.0);
+    const double pl2 = prm.prior_info > 0.0 ? prm.prior_info * S.L * S.L : 0.0;  // the prior's L^2 term
     double a[36], rhs[6];
 #pragma unroll
     for (int p = 0; p < 6; ++p) {
 #pragma unroll
-        for (int q = p; q < 6; ++q) {
-            double x = S.H[p * 6 + q] + S.P0[p * 6 + q];
-            if (p == q) x += fma(prm.damping, S.H[p * 7], 1e-9 * dmean) + (p >= 3 ? pl2 : 0.0);
-            a[p * 6 + q] = x;
-            a[q * 6 + p] = x;
-            S.A[p * 6 + q] = x;
-            S.A[q * 6 + p] = x;
-        }
-        rhs[p] = -S.b[p] + S.P0xi[p] + (p >= 3 ? pl2 * S.xi[p] : 0.0);
-        S.rhs[p] = rhs[p];
+        for (int q = p; q < 6; ++q) a[p * 6 + q] = S.A[p * 6 + q];
+        rhs[p] = S.rhs[p] + (p >= 3 ? pl2 * S.xi[p] : 0.0);
     }
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+        a[p * 7] += dm + (p >= 3 ? pl2 : 0.0);
+        S.A[p * 7] = a[p * 7];
+    }
+#pragma unroll
+    for (int p = 3; p < 6; ++p) S.rhs[p] = rhs[p];
     return elim6(a, 0.0, 0.0, rhs, delta);
 }
 
 // One Gauss-Newton update of S.T (odom.py:769-796) on warps 0 and 1 (the other warps go straight to the block
 // barrier after it). S.status: 0 continue, 1 converged, 2 too few correspondences, 3 singular.
-//   1. one output per thread, no division on the way: threads 0-20 the world-origin H = Ac^T Hc Ac (the sums were
+//   1. one output per thread: threads 0-20 the world-origin H = Ac^T Hc Ac (the sums were
 //      taken about the pass centre; odom.py's twist is about the origin), 21-41 G0 = W^T Hg_c W, of which the
 //      sensor-basis information is G = SB^T Hg SB = diag(s) G0 diag(s) (s = 1, 1, 1, 1/L, 1/L, 1/L), 42-47
-//      b = Ac^T b_c, 48 the count and the mean range L (odom.py:769-772);
-//   2. thread 0 forms A and rhs and solves A delta = rhs (elim6) while thread 32 tests G for the threshold by the
-//      same elimination and thread 33 takes the rms;
+//      b = Ac^T b_c, 48 the count and the mean range L (odom.py:769-772); the H threads also form A and the b
+//      threads rhs;
+//   2. thread 0 solves A delta = rhs (elim6; A and rhs formed in phase 1) while thread 32 tests G for the threshold
+//      by the same elimination;
 //   3. warp 0 takes the degenerate step if a direction is below the threshold, then applies the twist.
 // Named barrier 1 orders the two warps.
 __device__ void gn_step_pair(GnSmem& S, const lw_odom_params& prm) {
@@ -1683,12 +1682,21 @@ __device__ void gn_step_pair(GnSmem& S, const lw_odom_params& prm) {
         double* out = is_h ? S.H : S.G;
         out[p * 6 + q] = x;
         out[q * 6 + p] = x;
+        if (is_h) {
+            // A = H + LM damping + prior information, but for the 1e-9 mean-diagonal term and the prior's L^2 term
+            // (the solve adds those)
+            double a = x + S.P0[p * 6 + q];
+            if (p == q) a += prm.damping * x;
+            S.A[p * 6 + q] = a;
+            S.A[q * 6 + p] = a;
+        }
     } else if (tid < 48) {
         const int p = tid - 42;
         double x = 0.0;
 #pragma unroll
         for (int i = 0; i < 6; ++i) x = fma(S.Ac[i * 6 + p], S.v[LW_ACC_B + i], x);
         S.b[p] = x;
+        S.rhs[p] = -x + S.P0xi[p];  // -b + prior (xi), but for the prior's L^2 term
     } else if (tid == 48) {
         S.corr = (int)S.v[LW_ACC_COUNT];
         S.status = S.corr < prm.min_corr ? 2 : 0;
@@ -1710,9 +1718,6 @@ __device__ void gn_step_pair(GnSmem& S, const lw_odom_params& prm) {
             ok = elim6(g, prm.degen_thr, prm.degen_thr * S.L * S.L, nullptr, nullptr);
         }
         s_g_ok = ok;
-    } else if (tid == 33) {
-        S.invL = 1.0 / S.L;
-        S.rms = sqrt(fmax(S.v[LW_ACC_RMS], 0.0) / fmax(S.v[LW_ACC_WEIGHT], 1e-9));
     }
     pair_sync();
     if (tid >= 32) return;
@@ -1721,10 +1726,11 @@ __device__ void gn_step_pair(GnSmem& S, const lw_odom_params& prm) {
         // the sensor basis and its inverse, which the degenerate step works in (odom.py:425-433, 436-455), at
         // the current pose's position (not the pass centre S.c, which stays at the prediction)
         const double cT[3] = {S.T[3], S.T[7], S.T[11]};
+        const double invL = 1.0 / S.L;
         for (int e = lane; e < 36; e += 32) {
             const int p = e / 6, q = e % 6, i = p % 3, j = q % 3;
-            S.G[e] *= (p >= 3 ? S.invL : 1.0) * (q >= 3 ? S.invL : 1.0);  // the sensor-basis scaling of G
-            S.SB[e] = S.SB0[e] * (q >= 3 ? S.invL : 1.0);
+            S.G[e] *= (p >= 3 ? invL : 1.0) * (q >= 3 ? invL : 1.0);  // the sensor-basis scaling of G
+            S.SB[e] = S.SB0[e] * (q >= 3 ? invL : 1.0);
             double sbi = 0.0;
             if (p < 3 && q < 3) {
                 sbi = S.T[j * 4 + i];
@@ -1792,7 +1798,7 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
     if (gate && *gate == 0) return;  // uniform: every CTA reads the same flag before any barrier
     __shared__ GnSmem S;
     __shared__ int s_iters, s_degen, s_corr;
-    __shared__ double s_rms;
+    __shared__ double s_rms_num, s_rms_den;
     extern __shared__ float4 gn_dyn[];
     IcpCache memo = icp_cache_carve(gn_dyn);
     if (threadIdx.x < GN_GROUPS) {
@@ -1813,7 +1819,8 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         s_iters = 0;
         s_degen = 0;
         s_corr = 0;
-        s_rms = 0.0;
+        s_rms_num = 0.0;
+        s_rms_den = 1.0;
         for (int i = 0; i < 36; ++i) S.H[i] = (i % 7 == 0) ? 1.0 : 0.0;
         S.have_v = 0;
     }
@@ -1858,7 +1865,10 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
             gn.trace[(it + 1) * 12 + threadIdx.x] = S.T[threadIdx.x];  // the pose after iteration it
         if (threadIdx.x == 0) {  // read after the loop only (past the barrier below it)
             s_corr = S.corr;
-            if (S.status != 2) s_rms = S.rms;
+            if (S.status != 2) {  // the rms of the last accumulation with enough matches, taken after the loop
+                s_rms_num = S.v[LW_ACC_RMS];
+                s_rms_den = S.v[LW_ACC_WEIGHT];
+            }
             if (S.status == 0 || S.status == 1) {
                 s_iters = it + 1;
                 s_degen = S.degen;
@@ -1866,7 +1876,7 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         }
         if (S.status != 0) break;  // S.status was written before the block barrier above
     }
-    __syncthreads();  // thread 0's last s_corr, s_rms, s_iters, s_degen
+    __syncthreads();  // thread 0's last s_corr, s_rms_num / _den, s_iters, s_degen
     if (blockIdx.x == 0 && threadIdx.x < 32 && s_corr >= prm.min_corr) {
         // min/max eigenvalue of H normalised by its diagonal (odom.py:797-800), by warp 0
         for (int e = threadIdx.x; e < 36; e += 32) {
@@ -1887,7 +1897,7 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         st->iters = s_iters;
         if (which == 0) st->iters_first = s_iters;
         st->corr = s_corr;
-        st->rms = s_rms;
+        st->rms = sqrt(fmax(s_rms_num, 0.0) / fmax(s_rms_den, 1e-9));
         st->cond = cond;
         st->degen = s_degen;
         st->weak = (cond < 1e-3 || s_degen > 0) ? 1 : 0;  // WEAK_COND (odom.py:90)
