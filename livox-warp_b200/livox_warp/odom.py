@@ -87,7 +87,6 @@ class Odometry:
         # pinned landing buffers for the state and the registration's error flag: one stream sync per readback
         self._state_host = torch.empty(ctypes.sizeof(_lib.OdomState), dtype=torch.uint8, pin_memory=True)
         self._err_host = torch.empty(1, dtype=torch.int32, pin_memory=True)
-        self._ready = torch.cuda.Event()
         self._traj = torch.zeros(TRAJ_CAP * ctypes.sizeof(_lib.TrajRec), dtype=torch.uint8, device=d)
 
         # tuning (odom.py:499-525)
@@ -160,18 +159,11 @@ class Odometry:
     def synchronize(self):
         self.stream.synchronize()
 
-    def _wait(self):
-        """Wait for the work queued on the stream so far by polling an event: a registration's result is wanted as
-        soon as it lands, and a blocking synchronise adds the thread's wake-up (tens of microseconds) to each frame."""
-        self._ready.record(self.stream)
-        while not self._ready.query():
-            pass
-
     def read_state(self) -> _lib.OdomState:
         """The device state (synchronises the stream)."""
         with torch.cuda.stream(self.stream):
             self._state_host.copy_(self._state, non_blocking=True)
-        self._wait()
+        self.stream.synchronize()
         return _lib.OdomState.from_buffer_copy(self._state_host.numpy())
 
     @staticmethod
@@ -444,7 +436,7 @@ class Odometry:
         with torch.cuda.stream(self.stream):
             self._state_host.copy_(self._state, non_blocking=True)
             self._err_host.copy_(self._gn.err, non_blocking=True)
-        self._wait()
+        self.stream.synchronize()
         st = _lib.OdomState.from_buffer_copy(self._state_host.numpy())
         err = int(self._err_host[0])
         stats = {"ds": st.n_ds, "iters": st.iters, "corr": st.corr, "rms": st.rms, "cond": st.cond,
