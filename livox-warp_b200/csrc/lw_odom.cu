@@ -110,41 +110,7 @@ struct ThinArgs {
     int ret_mask;
     int deskew;      // 1: pass A deskews f_raw into f_xyz first
     float t_mid, inv_dt;
-    // with pf_keys set, pass A also warms L2 for the Gauss-Newton pass that follows (prefetch_neighbourhood)
-    const int64_t* pf_keys;
-    const float* pf_rec;
-    const double* pf_T;  // the predicted pose (device), or null to use pf_Tv
-    float pf_Tv[12];     // the predicted pose's first three rows, by value
-    int pf_mask;
-    float pf_inv_v;      // 1 / registration voxel
 };
-
-__device__ __forceinline__ void prefetch_l2(const void* ptr) { asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr)); }
-
-// A hint for the registration that follows the thinning, whose first pass would otherwise meet a cold L2: prefetch
-// the hash slot where the point's registration voxel (at the predicted pose) is first looked for and that slot's
-// record, and for every fourth point the first slots of the 26 neighbouring voxels too. Nothing is read back, so
-// an imprecise voxel or a key stored further along its probe sequence only leaves a miss for later.
-__device__ __forceinline__ void prefetch_neighbourhood(const ThinArgs& a, const float4& p, int64_t i) {
-    float T[12];
-#pragma unroll
-    for (int i = 0; i < 12; ++i) T[i] = a.pf_T ? (float)a.pf_T[i] : a.pf_Tv[i];
-    const float wx = T[0] * p.x + T[1] * p.y + T[2] * p.z + T[3];
-    const float wy = T[4] * p.x + T[5] * p.y + T[6] * p.z + T[7];
-    const float wz = T[8] * p.x + T[9] * p.y + T[10] * p.z + T[11];
-    const int bx = ifloor(wx * a.pf_inv_v), by = ifloor(wy * a.pf_inv_v), bz = ifloor(wz * a.pf_inv_v);
-    const int h = slot_hash(key_ijk(bx, by, bz)) & a.pf_mask;
-    prefetch_l2(a.pf_keys + h);
-    prefetch_l2(a.pf_rec + (int64_t)h * LW_REC_FLOATS);
-    if ((i & 3) == 0) {
-#pragma unroll 1
-        for (int o = 0; o < 27; ++o) {
-            if (o == 13) continue;  // the voxel itself
-            const int hn = slot_hash(key_ijk(bx + o / 9 - 1, by + (o / 3) % 3 - 1, bz + o % 3 - 1)) & a.pf_mask;
-            prefetch_l2(a.pf_keys + hn);
-        }
-    }
-}
 
 // The frame's point count and twist come from the state when `st` is set, else from the arguments.
 struct Tw6 {
@@ -219,7 +185,6 @@ __global__ void k_thin_a(lw_frame_buf fb, const int* __restrict__ m_dev, ThinArg
         float r = len3(p.x, p.y, p.z);
         uint32_t at = fb.f_attr[i];
         if (!(r < a.min_range || r > a.max_range) && tag_of(at) == 0 && ((1 << ret_of(at)) & a.ret_mask) != 0) {
-            if (a.pf_keys) prefetch_neighbourhood(a, p, i);
             int64_t key = key_ijk(ifloor(p.x * a.inv_v), ifloor(p.y * a.inv_v), ifloor(p.z * a.inv_v));
             bool claimed;
             slot = claim_slot(key, fb.ds_keys, mask, &claimed);
@@ -2133,22 +2098,6 @@ static ThinArgs thin_args(const lw_odom_params* prm) {
     a.deskew = 1;
     a.t_mid = 0.0f;
     a.inv_dt = (float)(1.0 / prm->frame_dt);
-    a.pf_keys = nullptr;
-    a.pf_rec = nullptr;
-    a.pf_T = nullptr;
-    a.pf_mask = 0;
-    a.pf_inv_v = 0.0f;
-    return a;
-}
-
-// thin_args with the L2 prefetch for the registration against `reg` from the predicted pose in `st`
-static ThinArgs thin_args_prefetch(const lw_odom_params* prm, const lw_regmap* reg, const lw_odom_state* st) {
-    ThinArgs a = thin_args(prm);
-    a.pf_keys = reg->keys;
-    a.pf_rec = reg->rec;
-    a.pf_T = st->T_pred;
-    a.pf_mask = (int)(reg->cap - 1);
-    a.pf_inv_v = (float)(1.0 / prm->reg_voxel);
     return a;
 }
 
@@ -2382,9 +2331,7 @@ int lw_register_frame(const float* raw4, const uint32_t* attr, int64_t m, double
     lw_frame_buf f = *fb;
     f.f_raw = const_cast<float*>(raw4);
     f.f_attr = const_cast<uint32_t*>(attr);
-    ThinArgs a = thin_args_prefetch(prm, reg, st);
-    a.pf_T = nullptr;  // the prediction by value: the state's copy is written by this same launch
-    for (int i = 0; i < 12; ++i) a.pf_Tv[i] = (float)T_pred_host[i];
+    ThinArgs a = thin_args(prm);
     a.t_mid = (float)t_mid;
     ThinBegin bg;
     bg.st = st;
@@ -2435,8 +2382,7 @@ static int finalize_impl(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_
     // first registration: deskew with the predicted motion, thin, Gauss-Newton
     {
         ProfScope prof("thin", s);
-        k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, thin_args_prefetch(prm, reg, st), st, tw, nullptr, &st->run_reg, 1,
-                                      ThinBegin{});
+        k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, ta, st, tw, nullptr, &st->run_reg, 1, ThinBegin{});
         k_thin_b<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->run_reg);
         k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->run_reg);
     }
