@@ -393,10 +393,9 @@ class Odometry:
             m = len(x)
             if m > self.frame_cap:
                 raise ValueError(f"{m} points exceed the frame capacity {self.frame_cap}")
-            if self._reg_pin is None or self._reg_pin["x4"].shape[0] < m:
+            if self._reg_pin is None or self._reg_pin["x3"].shape[0] < m:
                 cap = max(m, 1 << 14)
-                self._reg_pin = {"x4": torch.empty((cap, 4), dtype=torch.float32, pin_memory=True),
-                                 "x3": torch.empty((cap, 3), dtype=torch.float32, pin_memory=True),
+                self._reg_pin = {"x3": torch.empty((cap, 3), dtype=torch.float32, pin_memory=True),
                                  "t": torch.empty(cap, dtype=torch.float32, pin_memory=True),
                                  "a": torch.empty(cap, dtype=torch.int32, pin_memory=True),
                                  "d3": torch.empty((cap, 3), dtype=torch.float32, device=d),
@@ -404,22 +403,19 @@ class Odometry:
             pin = self._reg_pin
             if self._reg_ev is not None:
                 self._reg_ev.synchronize()  # the previous call's copies out of the pinned buffers are done
+            # contiguous host copies into pinned memory, then one call: three copies and the interleave on the device
             pin["a"].numpy()[:m] = np.asarray(attr).view(np.int32)
-            with torch.cuda.stream(self.stream):
-                if x.ndim == 2 and x.shape[1] == 4:  # x, y, z, t already interleaved: one copy
-                    pin["x4"].numpy()[:m] = x
-                    self.f_raw[:m].copy_(pin["x4"][:m], non_blocking=True)
-                else:
-                    # contiguous host copies only; the interleave is two strided copies on the device
-                    pin["x3"].numpy()[:m] = x[:, :3]
-                    pin["t"].numpy()[:m] = np.asarray(t, np.float32)
-                    pin["d3"][:m].copy_(pin["x3"][:m], non_blocking=True)
-                    pin["dt"][:m].copy_(pin["t"][:m], non_blocking=True)
-                    self.f_raw[:m, :3].copy_(pin["d3"][:m])
-                    self.f_raw[:m, 3].copy_(pin["dt"][:m])
-                self.f_attr[:m].copy_(pin["a"][:m], non_blocking=True)
+            if x.ndim == 2 and x.shape[1] == 4:
+                pin["x3"].numpy()[:m] = x[:, :3]
+                pin["t"].numpy()[:m] = x[:, 3]
+            else:
+                pin["x3"].numpy()[:m] = x[:, :3]
+                pin["t"].numpy()[:m] = np.asarray(t, np.float32)
+            _lib.call("lw_stage_frame", _lib.ptr(pin["x3"]), _lib.ptr(pin["t"]), _lib.ptr(pin["a"]), m,
+                      _lib.ptr(pin["d3"]), _lib.ptr(pin["dt"]), _lib.ptr(self.f_raw), _lib.ptr(self.f_attr), self._sp())
+            if self._reg_ev is None:
                 self._reg_ev = torch.cuda.Event()
-                self._reg_ev.record(self.stream)
+            self._reg_ev.record(self.stream)
             raw, at = self.f_raw, self.f_attr
         if m > self.frame_cap:
             raise ValueError(f"{m} points exceed the frame capacity {self.frame_cap}")
