@@ -245,6 +245,12 @@ int lw_icp_accumulate(const float* ds4, const int32_t* n_dev, int64_t n_ub, cons
 int lw_icp_solve(const float* ds4, const int32_t* n_dev, const lw_odom_params* prm, lw_odom_state* st,
                  const lw_regmap* reg, lw_gn_scratch* gn, void* stream);
 
+/* The odometry state (and, with err_dev, the Gauss-Newton error flag) copied to host memory, after everything
+ * queued on the stream: the state behind Odometry.stats (odom.py:550-559), in one call. Synchronises the
+ * stream. */
+int lw_read_state(const lw_odom_state* st_dev, const int32_t* err_dev, lw_odom_state* st_host, int32_t* err_host,
+                  void* stream);
+
 /* Stage a host frame for lw_register_frame: copy xyz3_host [m*3], t_host [m] and attr_host [m] (pinned host
  * memory for an asynchronous copy) into the device buffers xyz3_dev, t_dev and attr_dev, and interleave the first
  * two into raw4_dev [m*4] (x, y, z, t; 16-byte aligned). The reference stages host batches through Pipeline.stage
@@ -323,6 +329,12 @@ int lw_live_build(const float* ring_xyz, const uint32_t* ring_attr, const float*
 
 /* Frame id of each staged point, floor(max(t, 0) * inv_dt), all 0 when inv_dt <= 0 (gpu.py:340-348). */
 int lw_frame_ids(const float* t, int64_t n, float inv_dt, int32_t* out, void* stream);
+
+/* Pipeline.stage (gpu.py:1376-1401) in one call: copy a host batch -- xyz_host [n*3], attr_host [n], t_host [n],
+ * pinned for an asynchronous copy -- into the device staging buffers and compute its frame ids (frame_dev [n]) with
+ * inv_dt as lw_frame_ids does. Three copies and one launch, no host synchronisation. */
+int lw_stage_batch(const float* xyz_host, const uint32_t* attr_host, const float* t_host, int64_t n, float* xyz_dev,
+                   uint32_t* attr_dev, float* t_dev, float inv_dt, int32_t* frame_dev, void* stream);
 
 /* Buffers of the neighbourhood pass: an open-addressed voxel table of cap (a power of two) slots and the dense
  * per-voxel arrays (at most one voxel per point). */

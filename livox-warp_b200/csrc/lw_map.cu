@@ -830,6 +830,22 @@ int lw_frame_ids(const float* t, int64_t n, float inv_dt, int32_t* out, void* st
     return LW_OK;
 }
 
+int lw_stage_batch(const float* xyz_host, const uint32_t* attr_host, const float* t_host, int64_t n, float* xyz_dev,
+                   uint32_t* attr_dev, float* t_dev, float inv_dt, int32_t* frame_dev, void* stream) {
+    if (n < 0) return set_error(LW_EINVAL, "lw_stage_batch: negative point count");
+    if (n == 0) return LW_OK;
+    if (!xyz_host || !attr_host || !t_host || !xyz_dev || !attr_dev || !t_dev || !frame_dev)
+        return set_error(LW_EINVAL, "lw_stage_batch: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    LW_CUDA(cudaMemcpyAsync(xyz_dev, xyz_host, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, s));
+    LW_CUDA(cudaMemcpyAsync(attr_dev, attr_host, (size_t)n * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    LW_CUDA(cudaMemcpyAsync(t_dev, t_host, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, s));
+    k_frame_of<<<blocks_for(n, 256, 8 * device_sms()), 256, 0, s>>>(t_dev, n, inv_dt, frame_dev);
+    LW_LAUNCHED("lw_stage_batch");
+    count_launches(1);
+    return LW_OK;
+}
+
 int lw_map_clear(lw_map* map, void* stream) {
     int r = check_map(map, "lw_map_clear");
     if (r != LW_OK) return r;

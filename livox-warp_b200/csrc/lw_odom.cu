@@ -2317,6 +2317,16 @@ int lw_icp_solve(const float* ds4, const int32_t* n_dev, const lw_odom_params* p
     return launch_gn(ds4, n_dev, prm, st, reg, gn, 2, (cudaStream_t)stream);  // ungated
 }
 
+int lw_read_state(const lw_odom_state* st_dev, const int32_t* err_dev, lw_odom_state* st_host, int32_t* err_host,
+                  void* stream) {
+    if (!st_dev || !st_host) return set_error(LW_EINVAL, "lw_read_state: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    LW_CUDA(cudaMemcpyAsync(st_host, st_dev, sizeof(lw_odom_state), cudaMemcpyDeviceToHost, s));
+    if (err_dev && err_host) LW_CUDA(cudaMemcpyAsync(err_host, err_dev, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    LW_CUDA(cudaStreamSynchronize(s));
+    return LW_OK;
+}
+
 int lw_stage_frame(const float* xyz3_host, const float* t_host, const uint32_t* attr_host, int64_t m, float* xyz3_dev,
                    float* t_dev, float* raw4_dev, uint32_t* attr_dev, void* stream) {
     if (m < 0) return set_error(LW_EINVAL, "lw_stage_frame: negative point count");

@@ -184,6 +184,8 @@ _SIGS = {
     "lw_icp_accumulate": (i32, [P, P, i64, C.POINTER(f64), C.POINTER(RegMap), f32, i32, f32, f32,
                                 C.POINTER(GnScratch), P, P]),
     "lw_icp_solve": (i32, [P, P, C.POINTER(OdomParams), P, C.POINTER(RegMap), C.POINTER(GnScratch), P]),
+    "lw_read_state": (i32, [P, P, P, P, P]),
+    "lw_stage_batch": (i32, [P, P, P, i64, P, P, P, f32, P, P]),
     "lw_stage_frame": (i32, [P, P, P, i64, P, P, P, P, P]),
     "lw_register_frame": (i32, [P, P, i64, f64, C.POINTER(f32), C.POINTER(f64), C.POINTER(OdomParams), P,
                                 C.POINTER(FrameBuf), C.POINTER(RegMap), C.POINTER(GnScratch), P]),

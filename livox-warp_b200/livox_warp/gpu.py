@@ -287,15 +287,17 @@ class Pipeline:
             if self._pin_ev is not None:
                 self._pin_ev.synchronize()  # the previous batch's copy may still read the pinned buffers
             self._ensure_stage(n)
-            self._pin_xyz[:n].numpy()[:] = np.asarray(xyz, dtype=np.float32).reshape(-1, 3)[:n]
-            self._pin_attr[:n].numpy()[:] = np.asarray(attr)[:n].view(np.int32)
-            self._pin_t[:n].numpy()[:] = np.asarray(t, dtype=np.float32)[:n]
-            self._stage_xyz[:n].copy_(self._pin_xyz[:n], non_blocking=True)
-            self._stage_attr[:n].copy_(self._pin_attr[:n], non_blocking=True)
-            self._stage_t[:n].copy_(self._pin_t[:n], non_blocking=True)
-            self._pin_ev = torch.cuda.Event()
+            self._pin_xyz.numpy()[:n] = np.asarray(xyz, dtype=np.float32).reshape(-1, 3)[:n]
+            self._pin_attr.numpy()[:n] = np.asarray(attr)[:n].view(np.int32)
+            self._pin_t.numpy()[:n] = np.asarray(t, dtype=np.float32)[:n]
+            sx, sa, st, sf = self._stage_xyz, self._stage_attr, self._stage_t, self._stage_frame
+            # the three copies and the frame ids in one call
+            _lib.call("lw_stage_batch", _lib.ptr(self._pin_xyz), _lib.ptr(self._pin_attr), _lib.ptr(self._pin_t), n,
+                      _lib.ptr(sx), _lib.ptr(sa), _lib.ptr(st), float(inv_frame_dt), _lib.ptr(sf), _lib.stream_ptr(s))
+            if self._pin_ev is None:
+                self._pin_ev = torch.cuda.Event()
             self._pin_ev.record(s)
-            sx, sa, st = self._stage_xyz, self._stage_attr, self._stage_t
+            return sx, sa, st, sf
         else:
             self._ensure_stage(n)
             sx, sa, st = _as_xyz(xyz, self.device), attr, t

@@ -161,9 +161,7 @@ class Odometry:
 
     def read_state(self) -> _lib.OdomState:
         """The device state (synchronises the stream)."""
-        with torch.cuda.stream(self.stream):
-            self._state_host.copy_(self._state, non_blocking=True)
-        self.stream.synchronize()
+        _lib.call("lw_read_state", _lib.ptr(self._state), None, _lib.ptr(self._state_host), None, self._sp())
         return _lib.OdomState.from_buffer_copy(self._state_host.numpy())
 
     @staticmethod
@@ -429,10 +427,8 @@ class Odometry:
     def registration(self):
         """(T, ok, stats) of the last register_frame (synchronises the stream). stats["err"] is non-zero when a
         registration since the last reset gave up (a bounded wait ran out, or a fixed-point sum overflowed)."""
-        with torch.cuda.stream(self.stream):
-            self._state_host.copy_(self._state, non_blocking=True)
-            self._err_host.copy_(self._gn.err, non_blocking=True)
-        self.stream.synchronize()
+        _lib.call("lw_read_state", _lib.ptr(self._state), _lib.ptr(self._gn.err), _lib.ptr(self._state_host),
+                  _lib.ptr(self._err_host), self._sp())
         st = _lib.OdomState.from_buffer_copy(self._state_host.numpy())
         err = int(self._err_host[0])
         stats = {"ds": st.n_ds, "iters": st.iters, "corr": st.corr, "rms": st.rms, "cond": st.cond,
