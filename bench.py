@@ -367,9 +367,9 @@ def pose_drift(odom, traj, oracle_poses: dict) -> dict:
 
 # DRAM bytes (read + write) per launch from one ncu capture of the sequence (profiles/k_gn_k_carve_sequence.md,
 # rounded as summarised there) and of the coarse search (profiles/k_score_grid_office_coarse.md)
-SEQ_TRAFFIC = {"gn": 1_943_000, "carve": 6_928_000}  # carve: both passes (setup + walk)
+SEQ_TRAFFIC = {"gn": 1_245_952, "carve": 6_774_848}  # carve: both passes (setup + walk)
 SEQ_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_gn_k_carve_sequence.md"
-SINGLE_TRAFFIC = {"gn": 975_616}  # ncu, one timed launch of the single-frame case (975,360 B read + 256 B written)
+SINGLE_TRAFFIC = {"gn": 963_072}  # ncu, one timed launch of the single-frame case (963,072 B read, 0 written)
 SINGLE_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_gn_single_frame.md"
 COARSE_TRAFFIC = 42_780_928 + 71_592_448
 COARSE_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_score_grid_office_coarse.md"
