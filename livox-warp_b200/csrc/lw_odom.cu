@@ -664,10 +664,12 @@ __device__ __forceinline__ unsigned long long pack_best(float d2, int o, int s) 
 struct NeedyPoint {
     float wx, wy, wz;
     int bx, by, bz;
+    int win;  // the group whose memo window is based at (bx, by, bz), or -1: outer entries are read and kept there
 };
 
 __device__ void outer_shell(const NeedyPoint* __restrict__ q, unsigned long long* best, int nq, const IcpConsts& k,
-                            float voxel, const int64_t* __restrict__ keys, const float* __restrict__ rec) {
+                            float voxel, const int64_t* __restrict__ keys, const float* __restrict__ rec,
+                            const IcpCache* C) {
     for (int it = threadIdx.x; it < nq * 128; it += blockDim.x) {
         const int qi = it >> 7, o = it & 127;
         const int dx = o / 25 - 2, dy = (o / 5) % 5 - 2, dz = o % 5 - 2;
@@ -684,7 +686,22 @@ __device__ void outer_shell(const NeedyPoint* __restrict__ q, unsigned long long
         const float cur = __uint_as_float((unsigned)(*(volatile unsigned long long*)(best + qi) >> 32));
         if (box2 > cur) continue;
         float4 hd;
-        const int s = lookup_mean(key_ijk(p.bx + dx, p.by + dy, p.bz + dz), k, keys, rec, hd);
+        int s = -2;
+        int* ws = nullptr;
+        float4* wm = nullptr;
+        if (C && p.win >= 0) {  // one thread per (point, voxel): no other thread touches this entry now
+            ws = C->slot + p.win * WIN;
+            wm = C->mean + p.win * WIN;
+            s = ws[o];
+            if (s >= 0) hd = wm[o];
+        }
+        if (s == -2) {
+            s = lookup_mean(key_ijk(p.bx + dx, p.by + dy, p.bz + dz), k, keys, rec, hd);
+            if (ws) {
+                ws[o] = s;
+                if (s >= 0) wm[o] = hd;
+            }
+        }
         if (s < 0 || !(hd.w > 0.0f)) continue;
         const float d2 = mean_d2(p.wx, p.wy, p.wz, hd);
         if (d2 < k.max_d2) atomicMin(best + qi, pack_best(d2, o, s));
@@ -781,14 +798,15 @@ __device__ void icp_pass(const float4* __restrict__ ds, int n, const IcpPose& P,
             int qi = 0;
             if (needy && lane_g == 0) {
                 qi = atomicAdd(&s_nq[round % 3], 1);
-                s_need[buf][qi] = NeedyPoint{wx, wy, wz, bx, by, bz};
+                // the group's window is based at this point's voxel when it was gathered or used at reach 2 now
+                s_need[buf][qi] = NeedyPoint{wx, wy, wz, bx, by, bz, (use || store) ? gl : -1};
                 s_best[buf][qi] = pack_best(bd, bo, bs);
             }
             __syncthreads();
             const int nq = s_nq[round % 3];
             if (threadIdx.x == 0) s_nq[(round + 2) % 3] = 0;  // last used two rounds ago; next used after a barrier
             if (nq > 0) {
-                outer_shell(s_need[buf], s_best[buf], nq, k, voxel, keys, rec);
+                outer_shell(s_need[buf], s_best[buf], nq, k, voxel, keys, rec, C);
                 __syncthreads();
                 if (needy) {
                     qi = __shfl_sync(gmask, qi, lane & ~(G - 1));
