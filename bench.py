@@ -324,7 +324,8 @@ def roofline(res, frames, traj, warmup, steps, peak):
         x = frames[k][0]
         if name == "gn":
             ds = rl.thin_host(x, REG_VOXEL)
-            per_launch.append(rl.gn_bytes(ds, T, reg_keys, REG_VOXEL, max(iters, 1), odom._gn.grid))
+            per_launch.append(rl.gn_bytes(ds, T, reg_keys, REG_VOXEL, max(iters, 1), odom._gn.grid,
+                                          frame_points=len(x)))
         elif name == "carve":
             per_launch.append(rl.carve_bytes(x, T, map_keys, MAP_VOXEL))
         else:
@@ -1003,7 +1004,8 @@ def run_single(a, rank: int, world: int, local: int):
     per_launch = []
     for j, (x, at, t, t_mid, _) in enumerate(moving):
         ds = rl.thin_host(x, SINGLE_VOXEL)
-        per_launch.append(rl.gn_bytes(ds, res[j][0], reg_keys, SINGLE_VOXEL, max(int(iters[j]), 1), grid))
+        per_launch.append(rl.gn_bytes(ds, res[j][0], reg_keys, SINGLE_VOXEL, max(int(iters[j]), 1), grid,
+                                      frame_points=len(x)))
     avg_ms = gn_ms / max(gn_cnt, 1)
     achieved = float(np.mean(per_launch)) / (avg_ms * 1e-3) / 1e9
     peak = measured_peak()

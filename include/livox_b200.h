@@ -149,10 +149,12 @@ typedef struct lw_frame_buf {
 
 /* Scratch of the persistent Gauss-Newton kernel. */
 typedef struct lw_gn_scratch {
-    double* part;      /* [2 * grid * LW_ACC_STRIDE] per-CTA partial accumulators, double buffered */
-    uint32_t* bar;     /* [2] grid barrier counter and generation; zeroed by every launch */
+    double* part;      /* [2 * grid * LW_ACC_STRIDE] per-CTA partials (lw_icp_accumulate); the Gauss-Newton loop's
+                          fixed-point sums and the thinning's per-CTA counts (grid >= 2) */
+    uint32_t* bar;     /* [2] grid barrier count and exit count; zero before the first launch, and every launch
+                          leaves both zero */
     int32_t* err;      /* [1] set when a bounded wait gives up (1) or a fixed-point sum overflows (4); sticky */
-    int32_t grid;      /* CTAs (<= the SM count, one per SM) */
+    int32_t grid;      /* CTAs (2 .. the SM count, one per SM) */
     int32_t spin_budget; /* barrier wait limit in polls (~0.1-0.3 us each); 0 = the default (2^24 polls) */
     int32_t skip_cta;  /* failure injection for tests of the bounded wait: this CTA leaves before the first
                           barrier, so the others time out and the launch reports err = 1; -1 = none */
@@ -263,7 +265,8 @@ int lw_stage_frame(const float* xyz3_host, const float* t_host, const uint32_t* 
  * then Odometry._register (odom.py:752-803, with _downsample :731-737) from T_pred. raw4 [m*4] holds x, y, z,
  * t as measured (16-byte aligned), attr [m]; the points are deskewed to t_mid with twist6 (rho, theta) into
  * fb->f_xyz, thinned into fb->ds_xyz and registered; the result is in st->T_reg, st->ok and the stats
- * (st->n_ds, iters, corr, rms, cond, degen, weak). Four launches, no host synchronisation. */
+ * (st->n_ds, iters, corr, rms, cond, degen, weak). One launch (the Gauss-Newton kernel deskews and thins the
+ * frame before its loop), no host synchronisation. */
 int lw_register_frame(const float* raw4, const uint32_t* attr, int64_t m, double t_mid, const float* twist6_host,
                       const double* T_pred_host, const lw_odom_params* prm, lw_odom_state* st, lw_frame_buf* fb,
                       const lw_regmap* reg, lw_gn_scratch* gn, void* stream);

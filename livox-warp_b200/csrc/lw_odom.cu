@@ -1772,13 +1772,195 @@ __device__ void gn_step_pair(GnSmem& S, const lw_odom_params& prm) {
     }
 }
 
-// The whole registration loop (odom.py:752-803) in one cooperative launch. Every CTA reduces the partials
-// and computes the same float64 step, so one grid barrier per iteration suffices.
-__global__ void __launch_bounds__(GN_THREADS, 1)
-    k_gn(const float4* __restrict__ ds, const int* __restrict__ n_dev, lw_odom_params prm, lw_odom_state* st,
-         const int64_t* __restrict__ keys, const float* __restrict__ rec, int mask, lw_gn_scratch gn, int which) {
+// The frame's deskew and thinning (odom.py:126-178), run by the registration's own launch as its first three
+// grid-barrier episodes instead of as three kernels before it. Each CTA takes a contiguous run of the frame's
+// points, a thread every 256th of them:
+//   A  deskews f_raw into f_xyz and claims each point's half-voxel, keeping the lowest claiming index per slot;
+//   B  keeps the points that won their slot and publishes the CTA's count;
+//   C  writes the kept points to ds_xyz at the CTA's offset (the counts of the CTAs before it) in point order,
+//      and clears the slots for the next frame.
+// The result is the kernels' (k_thin_a/b/c): the same points in the same order.
+struct GnThin {
+    lw_frame_buf fb;
+    ThinArgs a;      // a.deskew: deskew f_raw into f_xyz in pass A
+    Tw6 tw;          // the deskew twist unless from_state
+    RegBegin b;      // begin: the registration's start state and the frame's size
+    int on;          // 0: no thinning, the launch registers ds and *n_dev as given
+    int from_state;  // 1: twist, t_mid and the point count from the state (the sequence's frames)
+    int begin;       // 1: CTA 0 writes b into the state (reg_begin) and the launch starts from b.T
+};
+
+// Counts out every CTA after its last barrier read; the last one out zeroes the barrier words, so the next launch
+// starts from a clean count whether or not this one completed.
+__device__ __forceinline__ void gn_exit(uint32_t* bar) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t prev = atomicAdd(bar + 1, 1u);
+        if (prev == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            atomicExch(bar + 1, 0u);
+        }
+    }
+}
+
+// Passes A-C; returns the number of thinned points, or -1 when the launch ends here (thinning not gated in, or a
+// barrier gave up). `run`: the launch's gate; pass A still deskews without it for the first registration of a
+// sequence frame (the frame's map insert reads f_xyz).
+__device__ __forceinline__ int gn_thin(const GnThin& th, lw_odom_state* st, const lw_gn_scratch& gn, int which,
+                                       bool run, long long budget) {
+    const lw_frame_buf& fb = th.fb;
+    const bool deskew = th.a.deskew && (run || which != 1);
+    if (!deskew && !run) return -1;
+    int64_t m = th.from_state ? (int64_t)st->m : (int64_t)th.b.m;
+    if (m > fb.cap) m = fb.cap;
+    if (m < 0) m = 0;
+    float tw[6];
+    float t_mid = th.a.t_mid;
+    if (th.from_state) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) tw[k] = st->xi_used[k];
+        t_mid = (float)st->t_mid;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) tw[k] = th.tw.v[k];
+    }
+    const int G = gridDim.x;
+    const int64_t chunk = (m + G - 1) / G;
+    const int64_t lo = (int64_t)blockIdx.x * chunk;
+    const int64_t hi = lo + chunk < m ? lo + chunk : m;
+    const int tid = threadIdx.x;
+    const int mask = (int)(fb.ds_cap - 1);
+    long long* fixed = reinterpret_cast<long long*>(gn.part);
+    int* counts = reinterpret_cast<int*>(fixed + 3 * LW_ACC_STRIDE);  // [G] kept points per CTA
+    __shared__ int s_sm[33];
+    __shared__ int s_base, s_total;
+    if (blockIdx.x == 0) {
+        if (th.begin) reg_begin(st, th.b);
+        // the fixed-point sums of the first two iterations start at zero (the loop clears the third)
+        if (run && tid < 2 * LW_ACC_STRIDE) fixed[tid] = 0;
+    }
+    // A: deskew, claim; the thread's first point and slot stay in registers for B and C, the rest go to ds_slot
+    float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f);
+    int slot0 = -1;
+    for (int64_t i = lo + tid; i < hi; i += GN_THREADS) {
+        float4 p;
+        if (deskew) {
+            p = deskew_point(reinterpret_cast<const float4*>(fb.f_raw)[i], t_mid, th.a.inv_dt, tw);
+            reinterpret_cast<float4*>(fb.f_xyz)[i] = p;
+        } else {
+            p = reinterpret_cast<const float4*>(fb.f_xyz)[i];
+        }
+        if (!run) continue;
+        int slot = -1;
+        const float r = len3(p.x, p.y, p.z);
+        const uint32_t at = fb.f_attr[i];
+        if (!(r < th.a.min_range || r > th.a.max_range) && tag_of(at) == 0 && ((1 << ret_of(at)) & th.a.ret_mask) != 0) {
+            const int64_t key = key_ijk(ifloor(p.x * th.a.inv_v), ifloor(p.y * th.a.inv_v), ifloor(p.z * th.a.inv_v));
+            bool claimed;
+            slot = claim_slot(key, fb.ds_keys, mask, &claimed);
+            if (slot >= 0) atomicMin(fb.ds_win + slot, (int)i);
+        }
+        if (i == lo + tid) {
+            p0 = p;
+            slot0 = slot;
+        } else {
+            fb.ds_slot[i] = slot;
+        }
+    }
+    if (!run) return -1;
+    // a barrier that gives up leaves the pass unfinished: every CTA then empties the slots its points claimed, so
+    // the table is clear for the next frame whichever CTAs got how far (a slot is emptied by each of its claimers)
+    auto give_up = [&]() {
+        for (int64_t i = lo + tid; i < hi; i += GN_THREADS) {
+            const int slot = i == lo + tid ? slot0 : fb.ds_slot[i];
+            if (slot >= 0) {
+                fb.ds_keys[slot] = EMPTY_KEY;
+                fb.ds_win[slot] = NO_INDEX;
+            }
+        }
+        return -1;
+    };
+    if ((int)blockIdx.x == gn.skip_cta) return give_up();  // injected failure: this CTA never arrives
+    if (!grid_sync(gn.bar, (uint32_t)G, gn.err, 1, budget)) return give_up();
+    // B: the lowest claiming index of a slot is kept; the CTA's count goes to counts[blockIdx.x]
+    int keep0 = 0, kept = 0;
+    for (int64_t r0 = lo; r0 < hi; r0 += GN_THREADS) {  // uniform over the CTA
+        const int64_t i = r0 + tid;
+        int keep = 0;
+        if (i < hi) {
+            const int slot = r0 == lo ? slot0 : fb.ds_slot[i];
+            keep = (slot >= 0 && fb.ds_win[slot] == (int)i) ? 1 : 0;
+            if (r0 == lo) keep0 = keep;
+        }
+        kept += __syncthreads_count(keep);
+    }
+    if (tid == 0) counts[blockIdx.x] = kept;
+    if (!grid_sync(gn.bar, 2u * (uint32_t)G, gn.err, 1, budget)) return give_up();
+    // C: this CTA's offset and the total, then the kept points in order. Each kept point empties its slot; a point
+    // that is not kept reads an index other than its own there, whether or not the kept point has emptied it yet.
+    if (tid < 32) {
+        int before = 0, all = 0;
+        for (int j = tid; j < G; j += 32) {
+            const int c = *(volatile int*)(counts + j);
+            all += c;
+            if (j < (int)blockIdx.x) before += c;
+        }
+        before = warp_sum_i(before);
+        all = warp_sum_i(all);
+        if (tid == 0) {
+            s_base = before;
+            s_total = all;
+        }
+    }
+    __syncthreads();
+    int run_base = s_base;
+    const int n = s_total;
+    for (int64_t r0 = lo; r0 < hi; r0 += GN_THREADS) {
+        const int64_t i = r0 + tid;
+        int slot = -1;
+        if (i < hi) {
+            if (r0 == lo) {
+                slot = keep0 ? slot0 : -1;
+            } else {
+                slot = fb.ds_slot[i];
+                if (slot >= 0 && fb.ds_win[slot] != (int)i) slot = -1;
+            }
+        }
+        const int keep = slot >= 0;
+        int tot;
+        const int rk = block_rank(keep, s_sm, &tot);
+        if (keep) {
+            const float4 p = r0 == lo ? p0 : reinterpret_cast<const float4*>(fb.f_xyz)[i];
+            reinterpret_cast<float4*>(fb.ds_xyz)[run_base + rk] = make_float4(p.x, p.y, p.z, len3(p.x, p.y, p.z));
+            fb.ds_keys[slot] = EMPTY_KEY;
+            fb.ds_win[slot] = NO_INDEX;
+        }
+        run_base += tot;
+    }
+    if (!grid_sync(gn.bar, 3u * (uint32_t)G, gn.err, 1, budget)) return give_up();
+    return n;
+}
+
+// The whole registration loop (odom.py:752-803) in one cooperative launch, with the frame's thinning before it
+// when th.on. Every CTA reduces the partials and computes the same float64 step, so one grid barrier per iteration
+// suffices.
+__device__ __forceinline__ void gn_run(const float4* __restrict__ ds, const int* __restrict__ n_dev,
+                                       const lw_odom_params& prm, lw_odom_state* st, const int64_t* __restrict__ keys,
+                                       const float* __restrict__ rec, int mask, const lw_gn_scratch& gn, int which,
+                                       const GnThin& th) {
     const int* gate = which == 0 ? &st->run_reg : (which == 1 ? &st->redo : nullptr);
-    if (gate && *gate == 0) return;  // uniform: every CTA reads the same flag before any barrier
+    const bool run = !(gate && *gate == 0);  // uniform: every CTA reads the same flag before any barrier
+    const long long budget = gn.spin_budget > 0 ? (long long)gn.spin_budget : BARRIER_SPINS;
+    int n;
+    uint32_t ep0 = 0;  // grid-barrier episodes before the loop's
+    if (th.on) {
+        n = gn_thin(th, st, gn, which, run, budget);
+        if (n < 0) return;
+        ep0 = 3;
+    } else {
+        if (!run) return;
+        n = *n_dev;
+    }
     __shared__ GnSmem S;
     __shared__ int s_iters, s_degen, s_corr;
     __shared__ double s_rms_num, s_rms_den;
@@ -1788,14 +1970,13 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         memo.tag[threadIdx.x] = make_int4(0, 0, 0, 0);
         memo.best[threadIdx.x] = -1;
     }
-    const int n = *n_dev;
     if (threadIdx.x == 0) {
-        for (int i = 0; i < 16; ++i) S.T[i] = S.Tp[i] = st->T_pred[i];
+        for (int i = 0; i < 16; ++i) S.T[i] = S.Tp[i] = th.on && th.begin ? th.b.T[i] : st->T_pred[i];
         if (gn.trace && blockIdx.x == 0)
-            for (int i = 0; i < 12; ++i) gn.trace[i] = st->T_pred[i];  // the start pose
-        S.c[0] = st->T_pred[3];
-        S.c[1] = st->T_pred[7];
-        S.c[2] = st->T_pred[11];
+            for (int i = 0; i < 12; ++i) gn.trace[i] = S.Tp[i];  // the start pose
+        S.c[0] = S.Tp[3];
+        S.c[1] = S.Tp[7];
+        S.c[2] = S.Tp[11];
         for (int i = 0; i < 6; ++i)
             for (int j = 0; j < 6; ++j)
                 S.Ac[i * 6 + j] = i == j ? 1.0 : (i < 3 && j >= 3 ? kneg(S.c, i, j - 3) : 0.0);
@@ -1817,7 +1998,6 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         return;
     }
     const float voxel = (float)prm.reg_voxel;
-    const long long budget = gn.spin_budget > 0 ? (long long)gn.spin_budget : BARRIER_SPINS;
     IcpConsts k;
     k.inv_v = (float)(1.0 / prm.reg_voxel);
     k.mask = mask;
@@ -1834,9 +2014,9 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         long long* fixed = reinterpret_cast<long long*>(gn.part) + (it % 3) * LW_ACC_STRIDE;
         memo.pt_ok = it > 0;
         icp_pass(ds, n, P, k, keys, rec, nullptr, fixed, gn.err, &memo);
-        if (it == 0 && (int)blockIdx.x == gn.skip_cta) return;  // injected failure: this CTA never arrives
+        if (it == 0 && !th.on && (int)blockIdx.x == gn.skip_cta) return;  // injected failure: never arrives
         // while thread 0 waits, thread 32 prepares what the step needs from the pose alone
-        if (!grid_sync(gn.bar, (uint32_t)(it + 1) * gridDim.x, gn.err, 1, budget,
+        if (!grid_sync(gn.bar, (ep0 + (uint32_t)it + 1u) * gridDim.x, gn.err, 1, budget,
                        StepPrep{&S, prm.prior_info > 0.0 ? prm.prior_info : 0.0}))
             return;
         if (blockIdx.x == 0 && threadIdx.x < LW_ACC_STRIDE)
@@ -1885,6 +2065,14 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
         st->degen = s_degen;
         st->weak = (cond < 1e-3 || s_degen > 0) ? 1 : 0;  // WEAK_COND (odom.py:90)
     }
+}
+
+__global__ void __launch_bounds__(GN_THREADS, 1)
+    k_gn(const float4* __restrict__ ds, const int* __restrict__ n_dev, lw_odom_params prm, lw_odom_state* st,
+         const int64_t* __restrict__ keys, const float* __restrict__ rec, int mask, lw_gn_scratch gn, int which,
+         GnThin th) {
+    gn_run(ds, n_dev, prm, st, keys, rec, mask, gn, which, th);
+    gn_exit(gn.bar);
 }
 
 // Standalone accumulation at a host pose, for the parity tests and the batched callers.
@@ -2136,10 +2324,16 @@ static lw_rec_params rec_params(const lw_odom_params* prm) {
     return rp;
 }
 
+// th: the frame's thinning, done by the launch before its loop (th->on), or nullptr to register ds4 and *n_dev as
+// they are. cleared: the fixed-point sums of the first two iterations are already zero (a thinning launch clears
+// them itself).
 static int launch_gn(const float* ds4, const int32_t* n_dev, const lw_odom_params* prm, lw_odom_state* st,
-                     const lw_regmap* reg, lw_gn_scratch* gn, int which, cudaStream_t s, bool cleared = false) {
+                     const lw_regmap* reg, lw_gn_scratch* gn, int which, cudaStream_t s, bool cleared = false,
+                     const GnThin* th = nullptr) {
     if (reg->cap > (1LL << SLOT_BITS))
         return set_error(LW_EINVAL, "Gauss-Newton: a registration map of %lld slots (at most 2^25)", (long long)reg->cap);
+    if (gn->grid < 2)  // the scratch holds 2 * grid accumulators; the loop's sums and the thinning counts need 4
+        return set_error(LW_EINVAL, "Gauss-Newton: a scratch of %d CTAs (at least two)", (int)gn->grid);
     int grid = gn_grid(gn);
     lw_gn_scratch g = *gn;
     g.grid = grid;
@@ -2148,11 +2342,13 @@ static int launch_gn(const float* ds4, const int32_t* n_dev, const lw_odom_param
     const int64_t* keys = reg->keys;
     const float* rec = reg->rec;
     lw_odom_params p = *prm;
+    GnThin t{};
+    if (th) t = *th;
     void* args[] = {(void*)&dsp, (void*)&n_dev, (void*)&p, (void*)&st, (void*)&keys, (void*)&rec,
-                    (void*)&mask, (void*)&g, (void*)&which};
-    // the fixed-point accumulators of the first two iterations start at zero (the kernel clears the rest), and
-    // the barrier's arrival count too: a launch that gave up at the barrier may have left it part counted
-    if (!cleared) {
+                    (void*)&mask, (void*)&g, (void*)&which, (void*)&t};
+    // the fixed-point accumulators of the first two iterations start at zero (the kernel clears the rest; a
+    // thinning launch clears them all); the barrier words are zero from the previous launch's exit
+    if (!cleared && !t.on) {
         LW_CUDA(cudaMemsetAsync(gn->part, 0, 3 * LW_ACC_STRIDE * sizeof(long long), s));
         LW_CUDA(cudaMemsetAsync(gn->bar, 0, 2 * sizeof(uint32_t), s));
     }
@@ -2303,6 +2499,7 @@ int lw_icp_accumulate(const float* ds4, const int32_t* n_dev, int64_t n_ub, cons
     if (reach != 1 && reach != 2) return set_error(LW_EINVAL, "lw_icp_accumulate: reach must be 1 or 2");
     if (reg->cap > (1LL << SLOT_BITS))
         return set_error(LW_EINVAL, "lw_icp_accumulate: a registration map of %lld slots (at most 2^25)", (long long)reg->cap);
+    if (gn->grid < 1) return set_error(LW_EINVAL, "lw_icp_accumulate: a scratch of %d CTAs", (int)gn->grid);
     cudaStream_t s = (cudaStream_t)stream;
     int grid = gn_grid(gn);
     IcpPose P;
@@ -2377,35 +2574,21 @@ int lw_register_frame(const float* raw4, const uint32_t* attr, int64_t m, double
     for (int i = 0; i < 6; ++i) b.tw[i] = twist6_host[i];
     b.t_mid = t_mid;
     b.m = (int)m;
-    // the frame buffer reads the caller's points in place: pass A (whose block 0 also sets up the registration's
-    // state and clears the Gauss-Newton sums) deskews them into f_xyz and claims the thinning voxels, B and C keep
-    // the lowest-index point of each and write ds_xyz in point order
-    lw_frame_buf f = *fb;
-    f.f_raw = const_cast<float*>(raw4);
-    f.f_attr = const_cast<uint32_t*>(attr);
-    ThinArgs a = thin_args(prm);
-    a.t_mid = (float)t_mid;
-    ThinBegin bg;
-    bg.st = st;
-    bg.part = reinterpret_cast<long long*>(gn->part);
-    bg.bar = gn->bar;
-    bg.b = b;
-    bg.on = 1;
-    Tw6 tw;
-    for (int k = 0; k < 6; ++k) tw.v[k] = twist6_host[k];
-    const int64_t m_ub = m > 0 ? m : 1;
-    int grid = blocks_for(m_ub, 256, 8 * device_sms());
-    int nt = blocks_for(m_ub, TILE);
-    {
-        ProfScope prof("thin", s);
-        k_thin_a<<<grid, 256, 0, s>>>(f, &st->m, a, nullptr, tw, nullptr, nullptr, 1, bg);
-        k_thin_b<<<nt, TILE, 0, s>>>(f, &st->m, nullptr);
-        k_thin_c<<<nt, TILE, 0, s>>>(f, &st->m, &st->n_ds, nullptr);
-    }
-    LW_LAUNCHED("lw_register_frame");
-    count_launches(3);
+    // the frame buffer reads the caller's points in place; the launch deskews them into f_xyz and thins them into
+    // ds_xyz (its CTA 0 also sets up the registration's state) before the Gauss-Newton loop
+    GnThin th{};
+    th.fb = *fb;
+    th.fb.f_raw = const_cast<float*>(raw4);
+    th.fb.f_attr = const_cast<uint32_t*>(attr);
+    th.a = thin_args(prm);
+    th.a.t_mid = (float)t_mid;
+    for (int k = 0; k < 6; ++k) th.tw.v[k] = twist6_host[k];
+    th.b = b;
+    th.on = 1;
+    th.from_state = 0;
+    th.begin = 1;
     ProfScope prof("gn", s);
-    return launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 2, s, /*cleared=*/true);
+    return launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 2, s, /*cleared=*/true, &th);
 }
 
 // The frame's queue of launches; with `net`, the learned start pose replaces the constant-velocity one between
@@ -2431,16 +2614,25 @@ static int finalize_impl(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_
         ProfScope prof("control", s);
         k_ctl_begin<<<1, 64, 0, s>>>(k, *prm, st, fb->count, reinterpret_cast<long long*>(gn->part), gn->bar);
     }
-    // first registration: deskew with the predicted motion, thin, Gauss-Newton
-    {
-        ProfScope prof("thin", s);
-        k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, ta, st, tw, nullptr, &st->run_reg, 1, ThinBegin{});
-        k_thin_b<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->run_reg);
-        k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->run_reg);
-    }
+    // the Gauss-Newton launches deskew and thin the frame themselves (from the state's twist, t_mid and count)
+    GnThin th{};
+    th.fb = *fb;
+    th.a = thin_args(prm);
+    th.on = 1;
+    th.from_state = 1;
+    th.begin = 0;
     int r;
+    int nl = 6;  // the three control kernels and the keyframe insert's three passes
     if (net) {
-        // the network sees the frame and the map patch around the constant-velocity prediction
+        // first registration: deskew with the predicted motion and thin in kernels of their own, so that the
+        // network sees the frame and the map patch around the constant-velocity prediction before the loop starts
+        {
+            ProfScope prof("thin", s);
+            k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, ta, st, tw, nullptr, &st->run_reg, 1, ThinBegin{});
+            k_thin_b<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->run_reg);
+            k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->run_reg);
+        }
+        nl += 3;
         ProfScope prof("net", s);
         r = net_sets_launch(fb->ds_xyz, &st->n_ds, *reg, st->T_pred, work->radius, work->voxel, work->sets,
                             work->cand, work->tiles, work->count, s);
@@ -2451,8 +2643,9 @@ static int finalize_impl(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_
         if (r != LW_OK) return r;
     }
     {
+        // first registration (after deskewing with the predicted motion and thinning, unless done above)
         ProfScope prof("gn", s);
-        r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 0, s, /*cleared=*/true);
+        r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 0, s, /*cleared=*/true, net ? nullptr : &th);
     }
     if (r != LW_OK) return r;
     // re-deskew with the solved motion and register again when it moved enough
@@ -2461,14 +2654,8 @@ static int finalize_impl(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_
         k_ctl_mid<<<1, 64, 0, s>>>(*prm, st, reinterpret_cast<long long*>(gn->part), gn->bar);
     }
     {
-        ProfScope prof("thin", s);
-        k_thin_a<<<grid, 256, 0, s>>>(*fb, &st->m, ta, st, tw, &st->redo, &st->redo, 1, ThinBegin{});
-        k_thin_b<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->redo);
-        k_thin_c<<<nt, TILE, 0, s>>>(*fb, &st->m, &st->n_ds, &st->redo);
-    }
-    {
         ProfScope prof("gn", s);
-        r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 1, s, /*cleared=*/true);
+        r = launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 1, s, /*cleared=*/true, &th);
     }
     if (r != LW_OK) return r;
     // keyframe, velocity, pose table, trajectory
@@ -2486,7 +2673,7 @@ static int finalize_impl(int32_t k, int64_t m_ub, const lw_odom_params* prm, lw_
         k_reg_d<<<grid, 256, 0, s>>>(&st->m, m_ub, *reg, fb->ds_slot, rp, &st->do_insert);
     }
     LW_LAUNCHED("lw_odom_finalize");
-    count_launches(12);  // plus the two Gauss-Newton launches counted by launch_gn
+    count_launches(nl);  // plus the two Gauss-Newton launches counted by launch_gn
     return LW_OK;
 }
 

@@ -10,6 +10,9 @@ from the frame's points, its solved pose and the table's occupied keys, per kern
     + 16 B per distinct occupied voxel among them (its mean and count)
     + 64 B per distinct voxel a point is matched to (its precision record)
     + 2 * 64 * 8 B per CTA (the float64 partials written and read back)
+  and once per launch, for the frame's deskew and thinning that the launch runs before its loop:
+      36 B per frame point (x, y, z, t and attr read, the deskewed x, y, z, t written)
+    + 40 B per thinned point (x, y, z, range written; its half-voxel's key and index claimed and emptied)
   carving (one launch = one frame's rays):
       20 B per traced ray (x, y, z, attr, frame id)
     + 12 B per distinct voxel the rays visit (key + hit count)
@@ -60,8 +63,9 @@ def thin_host(xyz_sensor: np.ndarray, voxel: float, min_range: float = 0.3, max_
 
 
 def gn_bytes(ds_sensor: np.ndarray, T: np.ndarray, occupied_keys: np.ndarray, voxel: float, iters: int,
-             grid: int, wide_iters: int = 3) -> float:
-    """Compulsory bytes of one registration launch (all its iterations)."""
+             grid: int, wide_iters: int = 3, frame_points: int = 0) -> float:
+    """Compulsory bytes of one registration launch (all its iterations, and the thinning of a frame of
+    frame_points points when it has one)."""
     w = _world(ds_sensor, T)
     base = np.floor(w / voxel).astype(np.int64)
     occ = np.sort(occupied_keys)
@@ -78,6 +82,8 @@ def gn_bytes(ds_sensor: np.ndarray, T: np.ndarray, occupied_keys: np.ndarray, vo
         v_occ = np.count_nonzero(np.isin(probed, occ))
         per_it = 16 * len(ds_sensor) + 8 * len(probed) + 16 * v_occ + 64 * len(matched) + 2 * grid * 64 * 8
         total += n_it * per_it
+    if frame_points:
+        total += 36 * frame_points + 40 * len(ds_sensor)
     return float(total)
 
 

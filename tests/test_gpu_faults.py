@@ -45,7 +45,8 @@ def test_barrier_wait_runs_out_and_the_context_stays_usable():
     waited = time.perf_counter() - t0
     assert st["err"] == 1 and not ok
     assert waited < 2.0  # the short limit, not the default one
-    # the next launch re-zeroes the barrier; clear the sticky flag as reset() does and register normally
+    # the failed launch left the barrier words zero on its way out (and the thinning table empty); clear the sticky
+    # flag as reset() does and register normally
     gn.struct.spin_budget, gn.struct.skip_cta = 0, -1
     gn.err.zero_()
     Tg, ok, st = odom.register_frame(x, a, t, t_mid, zero, T0)
@@ -58,8 +59,8 @@ def test_barrier_wait_runs_out_and_the_context_stays_usable():
 
 
 def test_every_cta_but_one_gives_up_in_turn():
-    """Whichever CTA is missing, the launch ends with the error set (CTA 0 included, which clears the rotating
-    accumulators after the barrier)."""
+    """Whichever CTA is missing, the launch ends with the error set (CTA 0 included, which sets up the start state
+    and clears the accumulators before the first barrier)."""
     odom, _, T0, (x, a, t, t_mid, _), _ = _case()
     zero = np.zeros(6, np.float32)
     gn = odom._gn
@@ -73,3 +74,28 @@ def test_every_cta_but_one_gives_up_in_turn():
     gn.err.zero_()
     _, ok, st = odom.register_frame(x, a, t, t_mid, zero, T0)
     assert ok and st["err"] == 0
+
+
+def test_launches_that_give_up_leave_the_thinning_table_empty():
+    """A launch that gives up at its first barrier has claimed the frame's thinning slots already: each CTA empties
+    the slots its points claimed on the way out. After three such launches the same frame registers as the oracle
+    does, with the oracle's thinned point count, so no slot was left behind."""
+    odom, oreg, T0, (x, a, t, t_mid, _), voxel = _case()
+    zero = np.zeros(6, np.float32)
+    gn = odom._gn
+    gn.struct.spin_budget = 2000
+    for skip in (1, gn.grid // 3, gn.grid - 2):
+        gn.err.zero_()
+        gn.struct.skip_cta = skip
+        _, ok, st = odom.register_frame(x, a, t, t_mid, zero, T0)
+        assert st["err"] == 1 and not ok
+    gn.struct.skip_cta, gn.struct.spin_budget = -1, 0
+    gn.err.zero_()
+    Tg, ok, st = odom.register_frame(x, a, t, t_mid, zero, T0)
+    assert ok and st["err"] == 0
+    ds = oracle.thin(oracle.deskew(common.raw4(x, t), t_mid, 10.0, zero), a, np.float32(2.0 / voxel), 0.3, 60.0,
+                     0b1111)
+    assert st["ds"] == len(ds)
+    To, ok_o, _ = oracle.register(ds, T0, oreg, oracle.Params(reg_voxel=voxel, max_iter=10))
+    dt, dr = oracle.pose_error(To, Tg)
+    assert ok_o and dt <= 1e-3 and dr <= 0.01

@@ -224,6 +224,45 @@ def test_register_degenerate_corridor_matches_oracle(yaw_deg):
     assert abs(sg["cond"] - so["cond"]) <= 1e-6 + 0.05 * abs(so["cond"])  # float32 sums of H: ~1e-3 relative
 
 
+@pytest.mark.parametrize("rate", [1.5e6, 0.0])
+def test_register_frame_deskews_and_thins_like_the_oracle(rate):
+    """The registration launch deskews and thins the frame itself: a 150k-point frame (several points per thread
+    of every CTA) with a turning twist leaves f_xyz and ds_xyz bit-exact with the oracle's deskew and thinning,
+    the table empty for the next frame (a second, different frame thins exactly too), and an empty frame leaves
+    no registration."""
+    from livox_warp import gpu, synth
+    from livox_warp.odom import Odometry
+
+    voxel = 0.2
+    T0, base, moving = synth.single_frame_case(common.room(1), 2, max(rate, RATE), map_frames=3)
+    pipe = gpu.Pipeline(ring_capacity=1 << 14, map_capacity=1 << 14)
+    odom = Odometry(pipe, reg_slots=1 << 18, frame_cap=1 << 18)
+    odom.reg_voxel, odom.max_iter = voxel, 10
+    odom.reset(T0)
+    oreg = oracle.RegMap(1 << 18)
+    for x, a, t in base:
+        x4 = common.raw4(x, t)
+        oreg.insert(x4, a, T0, voxel, 60.0, 0b1111)
+        odom.insert_frame(torch.from_numpy(x4).cuda(), torch.from_numpy(a.view(np.int32)).cuda(), T0)
+    tw = np.array([0.05, -0.02, 0.0, 0.0, 0.01, np.radians(2.0)], np.float32)
+    if rate == 0.0:
+        e = np.zeros((0, 3), np.float32)
+        Tg, ok, st = odom.register_frame(e, np.zeros(0, np.uint32), np.zeros(0, np.float32), 1.0, tw, T0)
+        assert not ok and st["ds"] == 0 and st["err"] == 0
+        assert np.array_equal(Tg, T0)
+        return
+    for x, a, t, t_mid, _ in moving:
+        assert len(t) > 148 * 256 * 3
+        x4 = common.raw4(x, t)
+        d_o = oracle.deskew(x4, t_mid, 10.0, tw)
+        ds = oracle.thin(d_o, a, np.float32(2.0 / voxel), 0.3, 60.0, 0b1111)
+        _, _, st = odom.register_frame(x, a, t, t_mid, tw, T0)
+        assert st["err"] == 0 and st["ds"] == len(ds)
+        assert np.array_equal(odom.f_xyz[:len(t)].cpu().numpy(), d_o)
+        assert np.array_equal(odom.ds_xyz[:len(ds)].cpu().numpy(), ds)
+    assert bool((odom.ds_keys == -1).all()) and bool((odom._ds_win == np.iinfo(np.int32).max).all())
+
+
 def test_register_frame_single_case_matches_float64_oracle():
     """The single-frame case through Odometry.register_frame (deskew + thinning + Gauss-Newton in one call, from
     host arrays and from device tensors): every one of its 8 seeded frames lands within 1 mm / 0.01 deg of the
