@@ -167,6 +167,22 @@ __device__ __forceinline__ void atomic_add_i64(int64_t* a, int64_t v) {
 __device__ __forceinline__ int64_t to_fix(float v, float scale) { return __float2ll_rn(v * scale); }
 
 // ---- reductions --------------------------------------------------------------------------------------------
+// claim_slot with the compare-and-swap as the probe: one atomic round trip per probed slot, where a load first
+// costs two for a slot found empty. The same slot results (a key is in at most one slot of its probe sequence:
+// a probe stops at the first slot that holds the key or that it turns from empty into the key).
+template <int P = PROBES>
+__device__ __forceinline__ int claim_slot_cas(int64_t key, int64_t* keys, int mask) {
+    int h = slot_hash(key) & mask;
+#pragma unroll 1
+    for (int p = 0; p < P; ++p) {
+        int s = (h + p) & mask;
+        unsigned long long prev = atomicCAS((unsigned long long*)(keys + s), (unsigned long long)EMPTY_KEY,
+                                            (unsigned long long)key);
+        if ((int64_t)prev == EMPTY_KEY || (int64_t)prev == key) return s;
+    }
+    return -1;
+}
+
 __device__ __forceinline__ int warp_sum_i(int v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -1856,8 +1856,7 @@ __device__ __forceinline__ int gn_thin(const GnThin& th, lw_odom_state* st, cons
         const uint32_t at = fb.f_attr[i];
         if (!(r < th.a.min_range || r > th.a.max_range) && tag_of(at) == 0 && ((1 << ret_of(at)) & th.a.ret_mask) != 0) {
             const int64_t key = key_ijk(ifloor(p.x * th.a.inv_v), ifloor(p.y * th.a.inv_v), ifloor(p.z * th.a.inv_v));
-            bool claimed;
-            slot = claim_slot(key, fb.ds_keys, mask, &claimed);
+            slot = claim_slot_cas(key, fb.ds_keys, mask);
             if (slot >= 0) atomicMin(fb.ds_win + slot, (int)i);
         }
         if (i == lo + tid) {
@@ -1951,16 +1950,6 @@ __device__ __forceinline__ void gn_run(const float4* __restrict__ ds, const int*
     const int* gate = which == 0 ? &st->run_reg : (which == 1 ? &st->redo : nullptr);
     const bool run = !(gate && *gate == 0);  // uniform: every CTA reads the same flag before any barrier
     const long long budget = gn.spin_budget > 0 ? (long long)gn.spin_budget : BARRIER_SPINS;
-    int n;
-    uint32_t ep0 = 0;  // grid-barrier episodes before the loop's
-    if (th.on) {
-        n = gn_thin(th, st, gn, which, run, budget);
-        if (n < 0) return;
-        ep0 = 3;
-    } else {
-        if (!run) return;
-        n = *n_dev;
-    }
     __shared__ GnSmem S;
     __shared__ int s_iters, s_degen, s_corr;
     __shared__ double s_rms_num, s_rms_den;
@@ -1970,9 +1959,11 @@ __device__ __forceinline__ void gn_run(const float4* __restrict__ ds, const int*
         memo.tag[threadIdx.x] = make_int4(0, 0, 0, 0);
         memo.best[threadIdx.x] = -1;
     }
-    if (threadIdx.x == 0) {
+    // the loop's start state, set up by a thread of the last warp (the one with the least thinning work) while the
+    // others thin the frame
+    if (threadIdx.x == GN_THREADS - 32) {
         for (int i = 0; i < 16; ++i) S.T[i] = S.Tp[i] = th.on && th.begin ? th.b.T[i] : st->T_pred[i];
-        if (gn.trace && blockIdx.x == 0)
+        if (gn.trace && blockIdx.x == 0 && run)
             for (int i = 0; i < 12; ++i) gn.trace[i] = S.Tp[i];  // the start pose
         S.c[0] = S.Tp[3];
         S.c[1] = S.Tp[7];
@@ -1987,6 +1978,16 @@ __device__ __forceinline__ void gn_run(const float4* __restrict__ ds, const int*
         s_rms_den = 1.0;
         for (int i = 0; i < 36; ++i) S.H[i] = (i % 7 == 0) ? 1.0 : 0.0;
         S.have_v = 0;
+    }
+    int n;
+    uint32_t ep0 = 0;  // grid-barrier episodes before the loop's
+    if (th.on) {
+        n = gn_thin(th, st, gn, which, run, budget);
+        if (n < 0) return;
+        ep0 = 3;
+    } else {
+        if (!run) return;
+        n = *n_dev;
     }
     __syncthreads();
     if (n < prm.min_corr) {  // odom.py:754-757
