@@ -370,7 +370,7 @@ def pose_drift(odom, traj, oracle_poses: dict) -> dict:
 # rounded as summarised there) and of the coarse search (profiles/k_score_grid_office_coarse.md)
 SEQ_TRAFFIC = {"gn": 1_245_952, "carve": 6_774_848}  # carve: both passes (setup + walk)
 SEQ_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_gn_k_carve_sequence.md"
-SINGLE_TRAFFIC = {"gn": 963_072}  # ncu, one timed launch of the single-frame case (963,072 B read, 0 written)
+SINGLE_TRAFFIC = {"gn": 1_387_776}  # ncu, one timed launch of the single-frame case (1,387,520 B read, 256 written)
 SINGLE_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_gn_single_frame.md"
 COARSE_TRAFFIC = 42_780_928 + 71_592_448
 COARSE_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_score_grid_office_coarse.md"
