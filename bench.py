@@ -368,7 +368,7 @@ def pose_drift(odom, traj, oracle_poses: dict) -> dict:
 
 # DRAM bytes (read + write) per launch from one ncu capture of the sequence (profiles/k_gn_k_carve_sequence.md,
 # rounded as summarised there) and of the coarse search (profiles/k_score_grid_office_coarse.md)
-SEQ_TRAFFIC = {"gn": 1_245_952, "carve": 6_774_848}  # carve: both passes (setup + walk)
+SEQ_TRAFFIC = {"gn": 2_186_752, "carve": 6_774_848}  # gn: thinning + iterations (mean of two full launches); carve: setup + walk
 SEQ_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_gn_k_carve_sequence.md"
 SINGLE_TRAFFIC = {"gn": 1_387_776}  # ncu, one timed launch of the single-frame case (1,387,520 B read, 256 written)
 SINGLE_TRAFFIC_SRC = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/k_gn_single_frame.md"
@@ -968,7 +968,8 @@ def run_single(a, rank: int, world: int, local: int):
     for j in range(len(dev)):
         step(j)
         res.append(odom.registration())
-    # end to end through the public API: host arrays staged (pinned H2D) and the result read back every step
+    # end to end through the public API: host arrays copied to pinned memory, read by the launch over the bus, and
+    # the result read back every step
     for k in range(a.warmup):
         x, at, t, t_mid, _ = moving[k % len(moving)]
         odom.register_frame(x, at, t, t_mid, zero, T0)

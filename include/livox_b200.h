@@ -271,6 +271,18 @@ int lw_register_frame(const float* raw4, const uint32_t* attr, int64_t m, double
                       const double* T_pred_host, const lw_odom_params* prm, lw_odom_state* st, lw_frame_buf* fb,
                       const lw_regmap* reg, lw_gn_scratch* gn, void* stream);
 
+/* lw_register_frame for a frame in the caller's pinned host memory (cudaHostAlloc / cudaHostRegister, mapped for
+ * the device), with its result returned there too: the same deskew, thinning and registration (odom.py:707-709,
+ * 731-737, 752-803), where the host-side staging of Pipeline.stage (gpu.py:1376-1420) and the state read-back are
+ * not separate copies. xyz3 [m*3] (x, y, z), t [m] and attr [m] are read by the launch itself; at its end it
+ * writes the state (as lw_read_state would read it) to st_out and the error flag (gn->err) to err_out, also when
+ * it gives up. The input buffers must not change and st_out / err_out must not be read until the stream has
+ * passed the launch. One launch, no host synchronisation; LW_EINVAL when a buffer is not mapped pinned memory. */
+int lw_register_frame_host(const float* xyz3, const float* t, const uint32_t* attr, int64_t m, double t_mid,
+                           const float* twist6_host, const double* T_pred_host, const lw_odom_params* prm,
+                           lw_odom_state* st, lw_frame_buf* fb, const lw_regmap* reg, lw_gn_scratch* gn,
+                           lw_odom_state* st_out, int32_t* err_out, void* stream);
+
 /* ---- integration map (gpu.py:1213-1219) ------------------------------------------------------- */
 typedef struct lw_map {
     int64_t* keys;   /* [cap] */

@@ -1788,18 +1788,41 @@ struct GnThin {
     int on;          // 0: no thinning, the launch registers ds and *n_dev as given
     int from_state;  // 1: twist, t_mid and the point count from the state (the sequence's frames)
     int begin;       // 1: CTA 0 writes b into the state (reg_begin) and the launch starts from b.T
+    // a frame read from the host: pass A reads x, y, z [m*3], t [m] and attr [m] through these device pointers of
+    // pinned host memory instead of f_raw and f_attr (null: from the frame buffer)
+    const float* src3;
+    const float* src_t;
+    const uint32_t* src_attr;
+    // the state and the error flag written to pinned host memory at the end of the launch (null: not)
+    lw_odom_state* out_st;
+    int32_t* out_err;
 };
 
 // Counts out every CTA after its last barrier read; the last one out zeroes the barrier words, so the next launch
-// starts from a clean count whether or not this one completed.
-__device__ __forceinline__ void gn_exit(uint32_t* bar) {
+// starts from a clean count whether or not this one completed. With th.out_st, the last one out also copies the
+// state and the error flag to the caller's pinned host memory: every CTA's writes to them (the state by CTA 0, the
+// flag by any CTA that gave up) precede its count by a fence, and the last CTA's fence follows all the counts.
+__device__ __forceinline__ void gn_exit(uint32_t* bar, const lw_odom_state* st, const int32_t* err, const GnThin& th) {
+    __shared__ int s_last;
     __syncthreads();
     if (threadIdx.x == 0) {
+        if (th.out_st) __threadfence();
         const uint32_t prev = atomicAdd(bar + 1, 1u);
-        if (prev == gridDim.x - 1) {
+        const int last = prev == gridDim.x - 1;
+        if (last) {
             atomicExch(bar, 0u);
             atomicExch(bar + 1, 0u);
+            if (th.out_st) __threadfence();
         }
+        s_last = last;
+    }
+    __syncthreads();
+    if (th.out_st && s_last && threadIdx.x < 32) {
+        const unsigned long long* a = reinterpret_cast<const unsigned long long*>(st);
+        unsigned long long* o = reinterpret_cast<unsigned long long*>(th.out_st);
+        constexpr int W = (int)(sizeof(lw_odom_state) / 8);
+        for (int e = threadIdx.x; e < W; e += 32) o[e] = *(volatile const unsigned long long*)(a + e);
+        if (threadIdx.x == 0 && th.out_err) *th.out_err = *(volatile const int32_t*)err;
     }
 }
 
@@ -1839,21 +1862,51 @@ __device__ __forceinline__ int gn_thin(const GnThin& th, lw_odom_state* st, cons
         // the fixed-point sums of the first two iterations start at zero (the loop clears the third)
         if (run && tid < 2 * LW_ACC_STRIDE) fixed[tid] = 0;
     }
-    // A: deskew, claim; the thread's first point and slot stay in registers for B and C, the rest go to ds_slot
+    // A: deskew, claim; the thread's first point and slot stay in registers for B and C, the rest go to ds_slot. A
+    // warp takes 32 consecutive points per round (the rounds are uniform over the warp).
     float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f);
     int slot0 = -1;
-    for (int64_t i = lo + tid; i < hi; i += GN_THREADS) {
-        float4 p;
-        if (deskew) {
-            p = deskew_point(reinterpret_cast<const float4*>(fb.f_raw)[i], t_mid, th.a.inv_dt, tw);
-            reinterpret_cast<float4*>(fb.f_xyz)[i] = p;
-        } else {
-            p = reinterpret_cast<const float4*>(fb.f_xyz)[i];
+    const int lane = tid & 31;
+    for (int64_t b0 = lo + (tid & ~31); b0 < hi; b0 += GN_THREADS) {
+        const int64_t i = b0 + lane;
+        const bool valid = i < hi;
+        float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t at = 0;
+        if (th.src3) {
+            // from pinned host memory, every byte crossing the bus once: the warp's points' x, y, z are 96
+            // consecutive floats, read as three coalesced rows and handed to their lanes by shuffles
+            float v[3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const int64_t e = 3 * b0 + 32 * r + lane;
+                v[r] = e < 3 * hi ? th.src3[e] : 0.0f;
+            }
+            float c[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int e = 3 * lane + k;
+                const float a0 = __shfl_sync(0xffffffffu, v[0], e & 31);
+                const float a1 = __shfl_sync(0xffffffffu, v[1], e & 31);
+                const float a2 = __shfl_sync(0xffffffffu, v[2], e & 31);
+                c[k] = e < 32 ? a0 : (e < 64 ? a1 : a2);
+            }
+            if (valid) {
+                at = th.src_attr[i];
+                p = deskew_point(make_float4(c[0], c[1], c[2], th.src_t[i]), t_mid, th.a.inv_dt, tw);
+                reinterpret_cast<float4*>(fb.f_xyz)[i] = p;
+            }
+        } else if (valid) {
+            if (deskew) {
+                p = deskew_point(reinterpret_cast<const float4*>(fb.f_raw)[i], t_mid, th.a.inv_dt, tw);
+                reinterpret_cast<float4*>(fb.f_xyz)[i] = p;
+            } else {
+                p = reinterpret_cast<const float4*>(fb.f_xyz)[i];
+            }
         }
-        if (!run) continue;
+        if (!run || !valid) continue;
+        if (!th.src3) at = fb.f_attr[i];
         int slot = -1;
         const float r = len3(p.x, p.y, p.z);
-        const uint32_t at = fb.f_attr[i];
         if (!(r < th.a.min_range || r > th.a.max_range) && tag_of(at) == 0 && ((1 << ret_of(at)) & th.a.ret_mask) != 0) {
             const int64_t key = key_ijk(ifloor(p.x * th.a.inv_v), ifloor(p.y * th.a.inv_v), ifloor(p.z * th.a.inv_v));
             slot = claim_slot_cas(key, fb.ds_keys, mask);
@@ -2073,7 +2126,7 @@ __global__ void __launch_bounds__(GN_THREADS, 1)
          const int64_t* __restrict__ keys, const float* __restrict__ rec, int mask, lw_gn_scratch gn, int which,
          GnThin th) {
     gn_run(ds, n_dev, prm, st, keys, rec, mask, gn, which, th);
-    gn_exit(gn.bar);
+    gn_exit(gn.bar, st, gn.err, th);
 }
 
 // Standalone accumulation at a host pose, for the parity tests and the batched callers.
@@ -2585,6 +2638,51 @@ int lw_register_frame(const float* raw4, const uint32_t* attr, int64_t m, double
     th.a.t_mid = (float)t_mid;
     for (int k = 0; k < 6; ++k) th.tw.v[k] = twist6_host[k];
     th.b = b;
+    th.on = 1;
+    th.from_state = 0;
+    th.begin = 1;
+    ProfScope prof("gn", s);
+    return launch_gn(fb->ds_xyz, &st->n_ds, prm, st, reg, gn, 2, s, /*cleared=*/true, &th);
+}
+
+// A device pointer for pinned host memory (the caller's buffer as the kernel reads or writes it), or null with the
+// error set when the memory is not pinned host memory this device can reach.
+static void* mapped(const void* host, const char* what) {
+    void* dev = nullptr;
+    cudaError_t e = cudaHostGetDevicePointer(&dev, const_cast<void*>(host), 0);
+    if (e != cudaSuccess || !dev) {
+        cudaGetLastError();
+        set_error(LW_EINVAL, "lw_register_frame_host: %s is not pinned host memory mapped for the device", what);
+        return nullptr;
+    }
+    return dev;
+}
+
+int lw_register_frame_host(const float* xyz3, const float* t, const uint32_t* attr, int64_t m, double t_mid,
+                           const float* twist6_host, const double* T_pred_host, const lw_odom_params* prm,
+                           lw_odom_state* st, lw_frame_buf* fb, const lw_regmap* reg, lw_gn_scratch* gn,
+                           lw_odom_state* st_out, int32_t* err_out, void* stream) {
+    if (!xyz3 || !t || !attr || !twist6_host || !T_pred_host || !prm || !st || !fb || !reg || !gn || !st_out || !err_out)
+        return set_error(LW_EINVAL, "lw_register_frame_host: null argument");
+    if (m < 0 || m > fb->cap)
+        return set_error(LW_ECAPACITY, "lw_register_frame_host: %lld points, frame capacity %lld", (long long)m,
+                         (long long)fb->cap);
+    GnThin th{};
+    th.src3 = static_cast<const float*>(mapped(xyz3, "xyz3"));
+    th.src_t = static_cast<const float*>(mapped(t, "t"));
+    th.src_attr = static_cast<const uint32_t*>(mapped(attr, "attr"));
+    th.out_st = static_cast<lw_odom_state*>(mapped(st_out, "st_out"));
+    th.out_err = static_cast<int32_t*>(mapped(err_out, "err_out"));
+    if (!th.src3 || !th.src_t || !th.src_attr || !th.out_st || !th.out_err) return LW_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int i = 0; i < 16; ++i) th.b.T[i] = T_pred_host[i];
+    for (int i = 0; i < 6; ++i) th.b.tw[i] = twist6_host[i];
+    th.b.t_mid = t_mid;
+    th.b.m = (int)m;
+    th.fb = *fb;
+    th.a = thin_args(prm);
+    th.a.t_mid = (float)t_mid;
+    for (int k = 0; k < 6; ++k) th.tw.v[k] = twist6_host[k];
     th.on = 1;
     th.from_state = 0;
     th.begin = 1;

@@ -189,6 +189,8 @@ _SIGS = {
     "lw_stage_frame": (i32, [P, P, P, i64, P, P, P, P, P]),
     "lw_register_frame": (i32, [P, P, i64, f64, C.POINTER(f32), C.POINTER(f64), C.POINTER(OdomParams), P,
                                 C.POINTER(FrameBuf), C.POINTER(RegMap), C.POINTER(GnScratch), P]),
+    "lw_register_frame_host": (i32, [P, P, P, i64, f64, C.POINTER(f32), C.POINTER(f64), C.POINTER(OdomParams), P,
+                                     C.POINTER(FrameBuf), C.POINTER(RegMap), C.POINTER(GnScratch), P, P, P]),
     "lw_map_insert": (i32, [P, i32, P, P, P, P, i64, P, C.POINTER(View), f32, C.POINTER(Map), P, P]),
     "lw_carve": (i32, [P, i32, P, P, P, i64, P, i32, f32, f32, i32, C.POINTER(Map), P, P]),
     "lw_map_build": (i32, [C.POINTER(Map), C.POINTER(View), i32, P, P, P, P, P, P, P]),

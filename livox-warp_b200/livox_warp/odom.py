@@ -87,6 +87,10 @@ class Odometry:
         # pinned landing buffers for the state and the registration's error flag: one stream sync per readback
         self._state_host = torch.empty(ctypes.sizeof(_lib.OdomState), dtype=torch.uint8, pin_memory=True)
         self._err_host = torch.empty(1, dtype=torch.int32, pin_memory=True)
+        # where a host frame's registration launch writes its result (lw_register_frame_host)
+        self._reg_out = torch.empty(ctypes.sizeof(_lib.OdomState), dtype=torch.uint8, pin_memory=True)
+        self._reg_err = torch.empty(1, dtype=torch.int32, pin_memory=True)
+        self._out_pending = False
         self._traj = torch.zeros(TRAJ_CAP * ctypes.sizeof(_lib.TrajRec), dtype=torch.uint8, device=d)
 
         # tuning (odom.py:499-525)
@@ -375,9 +379,10 @@ class Odometry:
         of cut from a stream. The map is left as it is (no keyframe insert, no velocity update).
 
         xyz: (m, 3) sensor points with t (m,) separately, or (m, 4) with t in the last column (t is then
-        ignored); attr (m,) uint32. A CUDA tensor (m, 4) float32 is read in place; host arrays are staged into
-        the frame buffer through pinned memory. With sync, returns (T, ok, stats) like the reference's
-        _register plus its stats; without, returns None and registration() reads the result later."""
+        ignored); attr (m,) uint32. A CUDA tensor (m, 4) float32 is read in place; host arrays are copied into
+        pinned memory, which the registration launch reads itself (and where it leaves its result). With sync,
+        returns (T, ok, stats) like the reference's _register plus its stats; without, returns None and
+        registration() reads the result later."""
         d = self.device
         if isinstance(xyz, torch.Tensor) and xyz.is_cuda:
             m = int(xyz.shape[0])
@@ -395,13 +400,12 @@ class Odometry:
                 cap = max(m, 1 << 14)
                 self._reg_pin = {"x3": torch.empty((cap, 3), dtype=torch.float32, pin_memory=True),
                                  "t": torch.empty(cap, dtype=torch.float32, pin_memory=True),
-                                 "a": torch.empty(cap, dtype=torch.int32, pin_memory=True),
-                                 "d3": torch.empty((cap, 3), dtype=torch.float32, device=d),
-                                 "dt": torch.empty(cap, dtype=torch.float32, device=d)}
+                                 "a": torch.empty(cap, dtype=torch.int32, pin_memory=True)}
             pin = self._reg_pin
             if self._reg_ev is not None:
-                self._reg_ev.synchronize()  # the previous call's copies out of the pinned buffers are done
-            # contiguous host copies into pinned memory, then one call: three copies and the interleave on the device
+                self._reg_ev.synchronize()  # the previous launch has read the pinned frame
+            # contiguous host copies into pinned memory; the registration launch reads them from there itself and
+            # writes its result to pinned memory at its end (one launch, nothing else on the stream)
             pin["a"].numpy()[:m] = np.asarray(attr).view(np.int32)
             if x.ndim == 2 and x.shape[1] == 4:
                 pin["x3"].numpy()[:m] = x[:, :3]
@@ -409,12 +413,17 @@ class Odometry:
             else:
                 pin["x3"].numpy()[:m] = x[:, :3]
                 pin["t"].numpy()[:m] = np.asarray(t, np.float32)
-            _lib.call("lw_stage_frame", _lib.ptr(pin["x3"]), _lib.ptr(pin["t"]), _lib.ptr(pin["a"]), m,
-                      _lib.ptr(pin["d3"]), _lib.ptr(pin["dt"]), _lib.ptr(self.f_raw), _lib.ptr(self.f_attr), self._sp())
+            self._sync_records()
+            _lib.call("lw_register_frame_host", _lib.ptr(pin["x3"]), _lib.ptr(pin["t"]), _lib.ptr(pin["a"]), m,
+                      float(t_mid), _lib.f32_array(np.asarray(twist, np.float32).reshape(6)),
+                      _lib.f64_array(np.asarray(T_pred, np.float64).reshape(16)), _byref(self.params()),
+                      _lib.ptr(self._state), _byref(self.fbuf), _byref(self.regmap), _byref(self.gn),
+                      _lib.ptr(self._reg_out), _lib.ptr(self._reg_err), self._sp())
             if self._reg_ev is None:
                 self._reg_ev = torch.cuda.Event()
             self._reg_ev.record(self.stream)
-            raw, at = self.f_raw, self.f_attr
+            self._out_pending = True
+            return self.registration() if sync else None
         if m > self.frame_cap:
             raise ValueError(f"{m} points exceed the frame capacity {self.frame_cap}")
         self._sync_records()
@@ -422,15 +431,21 @@ class Odometry:
                   _lib.f32_array(np.asarray(twist, np.float32).reshape(6)),
                   _lib.f64_array(np.asarray(T_pred, np.float64).reshape(16)), _byref(self.params()),
                   _lib.ptr(self._state), _byref(self.fbuf), _byref(self.regmap), _byref(self.gn), self._sp())
+        self._out_pending = False
         return self.registration() if sync else None
 
     def registration(self):
         """(T, ok, stats) of the last register_frame (synchronises the stream). stats["err"] is non-zero when a
         registration since the last reset gave up (a bounded wait ran out, or a fixed-point sum overflowed)."""
-        _lib.call("lw_read_state", _lib.ptr(self._state), _lib.ptr(self._gn.err), _lib.ptr(self._state_host),
-                  _lib.ptr(self._err_host), self._sp())
-        st = _lib.OdomState.from_buffer_copy(self._state_host.numpy())
-        err = int(self._err_host[0])
+        if self._out_pending:  # a host frame's launch wrote its result to pinned memory
+            self._reg_ev.synchronize()
+            st = _lib.OdomState.from_buffer_copy(self._reg_out.numpy())
+            err = int(self._reg_err[0])
+        else:
+            _lib.call("lw_read_state", _lib.ptr(self._state), _lib.ptr(self._gn.err), _lib.ptr(self._state_host),
+                      _lib.ptr(self._err_host), self._sp())
+            st = _lib.OdomState.from_buffer_copy(self._state_host.numpy())
+            err = int(self._err_host[0])
         stats = {"ds": st.n_ds, "iters": st.iters, "corr": st.corr, "rms": st.rms, "cond": st.cond,
                  "weak": bool(st.weak), "degen": st.degen, "err": err}
         return np.array(st.T_reg, dtype=np.float64).reshape(4, 4), bool(st.ok), stats

@@ -263,6 +263,39 @@ def test_register_frame_deskews_and_thins_like_the_oracle(rate):
     assert bool((odom.ds_keys == -1).all()) and bool((odom._ds_win == np.iinfo(np.int32).max).all())
 
 
+def test_register_frame_host_refuses_memory_that_is_not_pinned():
+    """lw_register_frame_host reads the frame and writes its result through device pointers of pinned host memory;
+    pageable memory is refused before anything is launched, and the next call with pinned buffers registers."""
+    import ctypes
+
+    from livox_warp import _lib, gpu, synth
+    from livox_warp.odom import Odometry
+
+    T0, base, moving = synth.single_frame_case(common.room(1), 1, RATE, map_frames=2)
+    pipe = gpu.Pipeline(ring_capacity=1 << 14, map_capacity=1 << 14)
+    odom = Odometry(pipe, reg_slots=1 << 18, frame_cap=1 << 15)
+    odom.reg_voxel, odom.max_iter = 0.2, 10
+    odom.reset(T0)
+    for x, a, t in base:
+        odom.insert_frame(torch.from_numpy(common.raw4(x, t)).cuda(), torch.from_numpy(a.view(np.int32)).cuda(), T0)
+    x, a, t, t_mid, _ = moving[0]
+    m = len(t)
+    x3 = np.ascontiguousarray(x[:, :3], np.float32)
+    tt = np.ascontiguousarray(t, np.float32)
+    aa = np.ascontiguousarray(a, np.uint32)
+    out = np.zeros(ctypes.sizeof(_lib.OdomState), np.uint8)
+    err = np.zeros(1, np.int32)
+    vp = lambda arr: ctypes.c_void_p(arr.ctypes.data)  # noqa: E731
+    with pytest.raises(_lib.LwError, match="not pinned"):
+        _lib.call("lw_register_frame_host", vp(x3), vp(tt), vp(aa), m, float(t_mid),
+                  _lib.f32_array(np.zeros(6, np.float32)), _lib.f64_array(T0.reshape(16)),
+                  ctypes.byref(odom.params()), _lib.ptr(odom._state), ctypes.byref(odom.fbuf),
+                  ctypes.byref(odom.regmap), ctypes.byref(odom.gn), vp(out), vp(err), odom._sp())
+    torch.cuda.synchronize()
+    _, ok, st = odom.register_frame(x, a, t, t_mid, np.zeros(6, np.float32), T0)
+    assert ok and st["err"] == 0 and st["ds"] > 0
+
+
 def test_register_frame_single_case_matches_float64_oracle():
     """The single-frame case through Odometry.register_frame (deskew + thinning + Gauss-Newton in one call, from
     host arrays and from device tensors): every one of its 8 seeded frames lands within 1 mm / 0.01 deg of the
