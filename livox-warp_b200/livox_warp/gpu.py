@@ -98,14 +98,21 @@ def rebase_times(keys: torch.Tensor, first: torch.Tensor, last: torch.Tensor, sh
 
 
 def _as_xyz(x, device) -> torch.Tensor:
-    """Device float32 points of shape (n, 3) or (n, 4) (x, y, z, anything)."""
+    """Device float32 points of shape (n, 3) or (n, 4) (x, y, z, anything), contiguous, or the (n, 3) x, y, z
+    columns of an (n, 4) buffer (rows 4 floats apart: the frame an on_frame callback is handed)."""
     if isinstance(x, np.ndarray):
         x = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 3))
     if x.device.type != "cuda":
         x = x.to(device, non_blocking=True)
-    if x.dtype != torch.float32 or not x.is_contiguous() or x.dim() != 2 or x.shape[1] not in (3, 4):
-        raise ValueError("points must be a contiguous float32 (n, 3) or (n, 4) array")
+    if (x.dtype != torch.float32 or x.dim() != 2 or x.shape[1] not in (3, 4) or x.stride(1) != 1
+            or x.stride(0) not in (3, 4) or x.stride(0) < x.shape[1]):
+        raise ValueError("points must be a float32 (n, 3) or (n, 4) array with rows of 3 or 4 floats")
     return x
+
+
+def row_stride(x: torch.Tensor) -> int:
+    """Floats from one point to the next (3 or 4) of points accepted by _as_xyz."""
+    return int(x.stride(0)) if x.shape[0] > 1 else int(max(x.stride(0), x.shape[1]))
 
 
 class Pipeline:
@@ -332,7 +339,7 @@ class Pipeline:
             return
         self.flush_poses()
         sx = _as_xyz(sx, self.device)
-        _lib.call("lw_map_insert", _lib.ptr(sx), sx.shape[1], _lib.ptr(sa), _lib.ptr(st), _lib.ptr(sf),
+        _lib.call("lw_map_insert", _lib.ptr(sx), row_stride(sx), _lib.ptr(sa), _lib.ptr(st), _lib.ptr(sf),
                   _lib.ptr(n_dev), n, _lib.ptr(self.poses), C_ref(view), 1.0 / max(voxel, 1e-4),
                   C_ref(self.map_struct), _lib.ptr(self._scratch(n)), _lib.stream_ptr())
 
@@ -344,7 +351,7 @@ class Pipeline:
             return
         self.flush_poses()
         sx = _as_xyz(sx, self.device)
-        _lib.call("lw_carve", _lib.ptr(sx), sx.shape[1], _lib.ptr(sa), _lib.ptr(sf), _lib.ptr(n_dev), n,
+        _lib.call("lw_carve", _lib.ptr(sx), row_stride(sx), _lib.ptr(sa), _lib.ptr(sf), _lib.ptr(n_dev), n,
                   _lib.ptr(self.poses), max(1, int(every)), 1.0 / max(voxel, 1e-4), float(max_range), int(max_steps),
                   C_ref(self.map_struct), _lib.ptr(self._scratch(n)), _lib.stream_ptr())
 

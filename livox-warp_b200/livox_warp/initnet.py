@@ -205,8 +205,9 @@ def make_pairs(frames, odom, T0: np.ndarray, per_frame: int, sigma, seed: int, r
         st = odom.read_state()
         n = int(st.n_ds)
         if st.ok and st.run_reg and n >= 200:
+            # the frame's float4 rows (x, y, z, t), which the registration map's insert reads
             ds_list.append((k, odom.ds_xyz[:n].clone(), np.array(st.T, dtype=np.float64).reshape(4, 4),
-                            f_xyz[:m].clone(), f_attr[:m].clone()))
+                            odom.f_xyz[:m].clone(), f_attr[:m].clone()))
 
     pipe = odom.pipe
     for k, (x, a, t) in enumerate(frames):

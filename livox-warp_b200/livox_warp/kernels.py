@@ -62,6 +62,9 @@ class RegistrationMap:
                ret_mask: int = 0b1111, noise: float = 0.02, alpha: float = 0.05, n_dev: torch.Tensor | None = None,
                stream=None):
         """Add points (n, 4) posed by T and refresh the touched voxels' records (odom.py:186-230, 719-727)."""
+        if (xyz4.dtype != torch.float32 or xyz4.dim() != 2 or xyz4.shape[1] != 4 or not xyz4.is_contiguous()
+                or not xyz4.is_cuda):
+            raise ValueError("registration map points must be a contiguous float32 (n, 4) CUDA tensor")
         n = int(xyz4.shape[0])
         if n > self._pslot.numel():
             self._pslot = torch.zeros(n, dtype=torch.int32, device=self.keys.device)

@@ -23,7 +23,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .gpu import Pipeline
+from .gpu import Pipeline, _as_xyz, row_stride
 from .kernels import GnScratch, RegistrationMap
 
 ACC_SLOTS = 64
@@ -254,8 +254,8 @@ class Odometry:
                       self.epoch, self._sp())
 
     def _append(self, sx, sa, st, n, inv_dt, k_min, k_open):
-        xyz = sx if isinstance(sx, torch.Tensor) else torch.as_tensor(sx)
-        _lib.call("lw_frame_append", _lib.ptr(xyz), int(xyz.shape[1]), _lib.ptr(sa), _lib.ptr(st), int(n),
+        xyz = _as_xyz(sx if isinstance(sx, torch.Tensor) else torch.as_tensor(sx), self.device)
+        _lib.call("lw_frame_append", _lib.ptr(xyz), row_stride(xyz), _lib.ptr(sa), _lib.ptr(st), int(n),
                   float(inv_dt), int(k_min), int(k_open), _byref(self.fbuf), self._sp())
         self._m_ub = min(self._m_ub + int(n), self.frame_cap)
 
@@ -515,4 +515,5 @@ class Odometry:
             st = self.read_state()
             self._ms = (time.perf_counter() - t0) * 1e3
             T = np.array(st.T, dtype=np.float64).reshape(4, 4)
-            on_frame(k, T, self.f_xyz, self.f_attr, self.f_t, self.f_frame, int(st.m))
+            # f_xyz as the reference hands it (a vec3 per point): the x, y, z columns of the float4 frame buffer
+            on_frame(k, T, self.f_xyz[:, :3], self.f_attr, self.f_t, self.f_frame, int(st.m))

@@ -84,7 +84,7 @@ class FrameResult:
     T: np.ndarray  # sensor-to-world at mid-frame
     xi: np.ndarray  # body-frame motion over the frame (rho, theta)
     m: int  # points in the frame
-    snaps: list | None  # [xyz4, attr, t, frame] of the deskewed frame (device tensors), or None if dropped
+    snaps: list | None  # [xyz (x, y, z), attr, t, frame] of the deskewed frame (device tensors), or None if dropped
     stats: dict = field(default_factory=dict)
 
     def arrays(self):
@@ -139,7 +139,7 @@ class OdomWorker:
         self.in_cap = int(in_cap)
         self.in_pool = _Slots(in_slots, [(in_cap, 3), (in_cap,), (in_cap,)],
                               [torch.float32, torch.int32, torch.float32], d)
-        self.out_pool = _Slots(out_slots, [(frame_cap, 4), (frame_cap,), (frame_cap,), (frame_cap,)],
+        self.out_pool = _Slots(out_slots, [(frame_cap, 3), (frame_cap,), (frame_cap,), (frame_cap,)],
                                [torch.float32, torch.int32, torch.float32, torch.int32], d)
         torch.cuda.synchronize(d)
         self.max_batches = max_batches
