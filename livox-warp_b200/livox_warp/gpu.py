@@ -97,22 +97,29 @@ def rebase_times(keys: torch.Tensor, first: torch.Tensor, last: torch.Tensor, sh
     last.copy_(torch.where(occ, last - s, last))
 
 
+def row_stride(x: torch.Tensor) -> int:
+    """Floats from one point to the next of an (n, 3) or (n, 4) float32 point array; 0 when the kernels cannot
+    read it as it is (rows must be 3 or 4 floats apart, at least as wide as a row, columns adjacent)."""
+    if x.dtype != torch.float32 or x.dim() != 2 or x.shape[1] not in (3, 4):
+        return 0
+    if x.shape[0] <= 1:  # a single row's stride is not meaningful
+        return int(x.shape[1]) if x.shape[0] == 0 or x.stride(1) == 1 else 0
+    s = int(x.stride(0))
+    return s if x.stride(1) == 1 and s in (3, 4) and s >= x.shape[1] else 0
+
+
 def _as_xyz(x, device) -> torch.Tensor:
     """Device float32 points of shape (n, 3) or (n, 4) (x, y, z, anything), contiguous, or the (n, 3) x, y, z
     columns of an (n, 4) buffer (rows 4 floats apart: the frame an on_frame callback is handed)."""
     if isinstance(x, np.ndarray):
         x = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 3))
+    if row_stride(x) == 0:
+        raise ValueError("points must be a float32 (n, 3) or (n, 4) array with rows of 3 or 4 floats")
     if x.device.type != "cuda":
         x = x.to(device, non_blocking=True)
-    if (x.dtype != torch.float32 or x.dim() != 2 or x.shape[1] not in (3, 4) or x.stride(1) != 1
-            or x.stride(0) not in (3, 4) or x.stride(0) < x.shape[1]):
-        raise ValueError("points must be a float32 (n, 3) or (n, 4) array with rows of 3 or 4 floats")
+        if row_stride(x) == 0:
+            x = x.contiguous()
     return x
-
-
-def row_stride(x: torch.Tensor) -> int:
-    """Floats from one point to the next (3 or 4) of points accepted by _as_xyz."""
-    return int(x.stride(0)) if x.shape[0] > 1 else int(max(x.stride(0), x.shape[1]))
 
 
 class Pipeline:
