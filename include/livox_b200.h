@@ -253,14 +253,6 @@ int lw_icp_solve(const float* ds4, const int32_t* n_dev, const lw_odom_params* p
 int lw_read_state(const lw_odom_state* st_dev, const int32_t* err_dev, lw_odom_state* st_host, int32_t* err_host,
                   void* stream);
 
-/* Stage a host frame for lw_register_frame: copy xyz3_host [m*3], t_host [m] and attr_host [m] (pinned host
- * memory for an asynchronous copy) into the device buffers xyz3_dev, t_dev and attr_dev, and interleave the first
- * two into raw4_dev [m*4] (x, y, z, t; 16-byte aligned). The reference stages host batches through Pipeline.stage
- * (gpu.py:1376-1420); this is that step for a single frame, in one call instead of a copy per array plus a copy
- * kernel per column from the host. Three copies and one launch, no host synchronisation. */
-int lw_stage_frame(const float* xyz3_host, const float* t_host, const uint32_t* attr_host, int64_t m, float* xyz3_dev,
-                   float* t_dev, float* raw4_dev, uint32_t* attr_dev, void* stream);
-
 /* Deskew and register one frame handed in the caller's device buffers: Odometry._deskew (odom.py:707-709)
  * then Odometry._register (odom.py:752-803, with _downsample :731-737) from T_pred. raw4 [m*4] holds x, y, z,
  * t as measured (16-byte aligned), attr [m]; the points are deskewed to t_mid with twist6 (rho, theta) into

@@ -2337,13 +2337,6 @@ __global__ void k_fill_i32(int32_t* a, int64_t n, int32_t v) {
 
 }  // namespace lw
 
-// x, y, z (stride 3) and t into float4 points.
-__global__ void k_interleave4(const float* __restrict__ xyz3, const float* __restrict__ t, float4* __restrict__ raw4,
-                              int64_t m) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
-        raw4[i] = make_float4(xyz3[i * 3], xyz3[i * 3 + 1], xyz3[i * 3 + 2], t[i]);
-}
-
 // =========================================================================================================
 // C ABI
 // =========================================================================================================
@@ -2593,23 +2586,6 @@ int lw_read_state(const lw_odom_state* st_dev, const int32_t* err_dev, lw_odom_s
     LW_CUDA(cudaMemcpyAsync(st_host, st_dev, sizeof(lw_odom_state), cudaMemcpyDeviceToHost, s));
     if (err_dev && err_host) LW_CUDA(cudaMemcpyAsync(err_host, err_dev, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     LW_CUDA(cudaStreamSynchronize(s));
-    return LW_OK;
-}
-
-int lw_stage_frame(const float* xyz3_host, const float* t_host, const uint32_t* attr_host, int64_t m, float* xyz3_dev,
-                   float* t_dev, float* raw4_dev, uint32_t* attr_dev, void* stream) {
-    if (m < 0) return set_error(LW_EINVAL, "lw_stage_frame: negative point count");
-    if (m == 0) return LW_OK;
-    if (!xyz3_host || !t_host || !attr_host || !xyz3_dev || !t_dev || !raw4_dev || !attr_dev)
-        return set_error(LW_EINVAL, "lw_stage_frame: null argument");
-    if (((uintptr_t)raw4_dev & 15) != 0) return set_error(LW_EINVAL, "lw_stage_frame: raw4_dev is not 16-byte aligned");
-    cudaStream_t s = (cudaStream_t)stream;
-    LW_CUDA(cudaMemcpyAsync(xyz3_dev, xyz3_host, (size_t)m * 3 * sizeof(float), cudaMemcpyHostToDevice, s));
-    LW_CUDA(cudaMemcpyAsync(t_dev, t_host, (size_t)m * sizeof(float), cudaMemcpyHostToDevice, s));
-    LW_CUDA(cudaMemcpyAsync(attr_dev, attr_host, (size_t)m * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-    k_interleave4<<<blocks_for(m, 256), 256, 0, s>>>(xyz3_dev, t_dev, reinterpret_cast<float4*>(raw4_dev), m);
-    LW_LAUNCHED("lw_stage_frame");
-    count_launches(1);
     return LW_OK;
 }
 

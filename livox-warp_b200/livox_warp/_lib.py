@@ -186,7 +186,6 @@ _SIGS = {
     "lw_icp_solve": (i32, [P, P, C.POINTER(OdomParams), P, C.POINTER(RegMap), C.POINTER(GnScratch), P]),
     "lw_read_state": (i32, [P, P, P, P, P]),
     "lw_stage_batch": (i32, [P, P, P, i64, P, P, P, f32, P, P]),
-    "lw_stage_frame": (i32, [P, P, P, i64, P, P, P, P, P]),
     "lw_register_frame": (i32, [P, P, i64, f64, C.POINTER(f32), C.POINTER(f64), C.POINTER(OdomParams), P,
                                 C.POINTER(FrameBuf), C.POINTER(RegMap), C.POINTER(GnScratch), P]),
     "lw_register_frame_host": (i32, [P, P, P, i64, f64, C.POINTER(f32), C.POINTER(f64), C.POINTER(OdomParams), P,
