@@ -5,6 +5,7 @@ import ctypes
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
@@ -114,3 +115,29 @@ def test_noalloc_thinning_refuses_misaligned_points_without_a_gpu():
                                  ctypes.c_void_p(out), ctypes.c_void_p(good), None)
         assert rc == _lib.LW_EINVAL
         assert b"16-byte" in lib.lw_last_error()
+
+
+def test_register_frame_host_refuses_bad_arguments_without_a_gpu():
+    """lw_register_frame_host checks its arguments before it asks CUDA for anything: a null buffer is LW_EINVAL and
+    a frame above the frame buffer's capacity LW_ECAPACITY (so this runs without a GPU; no pointer is used)."""
+    from livox_warp import _lib
+
+    lib = _lib.load(require_cuda=False)
+    dummy = ctypes.c_void_p(0x10000)
+    tw = _lib.f32_array(np.zeros(6, np.float32))
+    T = _lib.f64_array(np.eye(4).reshape(16))
+    prm = _lib.OdomParams()
+    fb = _lib.FrameBuf()
+    fb.cap = 16
+    reg = _lib.RegMap()
+    gn = _lib.GnScratch()
+
+    def call(xyz3, m):
+        return lib.lw_register_frame_host(xyz3, dummy, dummy, m, 0.0, tw, T, ctypes.byref(prm), dummy,
+                                          ctypes.byref(fb), ctypes.byref(reg), ctypes.byref(gn), dummy, dummy, None)
+
+    assert call(None, 8) == _lib.LW_EINVAL
+    assert b"null" in lib.lw_last_error()
+    assert call(dummy, 32) == _lib.LW_ECAPACITY
+    assert b"capacity" in lib.lw_last_error()
+    assert call(dummy, -1) == _lib.LW_ECAPACITY
