@@ -263,6 +263,30 @@ def test_register_frame_deskews_and_thins_like_the_oracle(rate):
     assert bool((odom.ds_keys == -1).all()) and bool((odom._ds_win == np.iinfo(np.int32).max).all())
 
 
+def test_register_frame_host_frames_queued_without_sync():
+    """Host frames queued back to back (sync=False) register as they do one at a time: each call waits until the
+    previous launch has read the pinned frame before refilling it, and registration() returns the last frame's
+    result from the pinned result buffer."""
+    from livox_warp import gpu, synth
+    from livox_warp.odom import Odometry
+
+    T0, base, moving = synth.single_frame_case(common.room(1), 3, RATE, map_frames=3)
+    pipe = gpu.Pipeline(ring_capacity=1 << 14, map_capacity=1 << 14)
+    odom = Odometry(pipe, reg_slots=1 << 18, frame_cap=1 << 15)
+    odom.reg_voxel, odom.max_iter = 0.2, 10
+    odom.reset(T0)
+    for x, a, t in base:
+        odom.insert_frame(torch.from_numpy(common.raw4(x, t)).cuda(), torch.from_numpy(a.view(np.int32)).cuda(), T0)
+    zero = np.zeros(6, np.float32)
+    one_by_one = [odom.register_frame(x, a, t, t_mid, zero, T0) for x, a, t, t_mid, _ in moving]
+    for j in range(len(moving)):
+        for x, a, t, t_mid, _ in moving[:j + 1]:
+            assert odom.register_frame(x, a, t, t_mid, zero, T0, sync=False) is None
+        T, ok, st = odom.registration()
+        Tj, okj, stj = one_by_one[j]
+        assert ok == okj and np.array_equal(T, Tj) and st == stj
+
+
 def test_register_frame_host_refuses_memory_that_is_not_pinned():
     """lw_register_frame_host reads the frame and writes its result through device pointers of pinned host memory;
     pageable memory is refused before anything is launched, and the next call with pinned buffers registers."""
