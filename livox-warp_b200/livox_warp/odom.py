@@ -90,6 +90,7 @@ class Odometry:
         # where a host frame's registration launch writes its result (lw_register_frame_host)
         self._reg_out = torch.empty(ctypes.sizeof(_lib.OdomState), dtype=torch.uint8, pin_memory=True)
         self._reg_err = torch.empty(1, dtype=torch.int32, pin_memory=True)
+        self._reg_out_np, self._reg_err_np = self._reg_out.numpy(), self._reg_err.numpy()
         self._out_pending = False
         self._traj = torch.zeros(TRAJ_CAP * ctypes.sizeof(_lib.TrajRec), dtype=torch.uint8, device=d)
 
@@ -401,18 +402,16 @@ class Odometry:
                 self._reg_pin = {"x3": torch.empty((cap, 3), dtype=torch.float32, pin_memory=True),
                                  "t": torch.empty(cap, dtype=torch.float32, pin_memory=True),
                                  "a": torch.empty(cap, dtype=torch.int32, pin_memory=True)}
+                # numpy views of the pinned buffers, made once (a tensor's .numpy() costs microseconds per call)
+                self._reg_pin.update({k + "_np": self._reg_pin[k].numpy() for k in ("x3", "t", "a")})
             pin = self._reg_pin
             if self._reg_ev is not None:
                 self._reg_ev.synchronize()  # the previous launch has read the pinned frame
             # contiguous host copies into pinned memory; the registration launch reads them from there itself and
             # writes its result to pinned memory at its end (one launch, nothing else on the stream)
-            pin["a"].numpy()[:m] = np.asarray(attr).view(np.int32)
-            if x.ndim == 2 and x.shape[1] == 4:
-                pin["x3"].numpy()[:m] = x[:, :3]
-                pin["t"].numpy()[:m] = x[:, 3]
-            else:
-                pin["x3"].numpy()[:m] = x[:, :3]
-                pin["t"].numpy()[:m] = np.asarray(t, np.float32)
+            pin["a_np"][:m] = np.asarray(attr).view(np.int32)
+            pin["x3_np"][:m] = x[:, :3]
+            pin["t_np"][:m] = x[:, 3] if x.ndim == 2 and x.shape[1] == 4 else np.asarray(t, np.float32)
             self._sync_records()
             _lib.call("lw_register_frame_host", _lib.ptr(pin["x3"]), _lib.ptr(pin["t"]), _lib.ptr(pin["a"]), m,
                       float(t_mid), _lib.f32_array(np.asarray(twist, np.float32).reshape(6)),
@@ -439,8 +438,8 @@ class Odometry:
         registration since the last reset gave up (a bounded wait ran out, or a fixed-point sum overflowed)."""
         if self._out_pending:  # a host frame's launch wrote its result to pinned memory
             self._reg_ev.synchronize()
-            st = _lib.OdomState.from_buffer_copy(self._reg_out.numpy())
-            err = int(self._reg_err[0])
+            st = _lib.OdomState.from_buffer_copy(self._reg_out_np)
+            err = int(self._reg_err_np[0])
         else:
             _lib.call("lw_read_state", _lib.ptr(self._state), _lib.ptr(self._gn.err), _lib.ptr(self._state_host),
                       _lib.ptr(self._err_host), self._sp())
